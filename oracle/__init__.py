@@ -1,0 +1,318 @@
+"""CPU oracle for the Daubechies-16 local-Hamiltonian path.
+
+TEST INFRASTRUCTURE ONLY.  The parity tests, ``__graft_entry__.smoke()`` and
+the CPU-baseline leg of ``bench.py`` use this module as the checker; the
+product library never imports it.
+
+``wvl_oracle.c`` restates the reference's FP64 CPU convolutions (Fortran,
+``bigdft/src/orbitals/convolut_simple_per.f90`` and friends) and the
+compositions of its OpenCL backend (``bigdft/src/OpenCL/*.c``); each C routine
+cites the reference lines it follows.  Parity pins:
+
+* the magic filter is checked against the reference's own C implementation
+  (``bigdft/src/convolutions-c/MagicFilter_sse.c``) compiled into
+  ``oracle/_ref`` (see ``Makefile``), and against golden vectors generated
+  from it (``tests/golden``);
+* the rest is pinned by the reference's mathematical known-answer checks
+  (orthonormality of DB16, analysis after synthesis = identity, magic-filter
+  adjointness, kinetic symmetry, agreement of the fine-grid kinetic with the
+  wavelet-basis ``ConvolkineticT`` filters, analytic Laplacian of a Gaussian),
+  since the reference stores no golden vectors for this path.
+"""
+import ctypes as C
+import os
+import subprocess
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+LIB = HERE / "_build" / "liboracle.so"
+REF_MF = HERE / "_ref" / "libref_magicfilter.so"
+
+_lib = None
+
+i32p = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
+f64p = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
+u8p = np.ctypeslib.ndpointer(dtype=np.uint8, flags="C_CONTIGUOUS")
+ip = C.POINTER(C.c_int)
+dp = C.POINTER(C.c_double)
+
+
+def build():
+    subprocess.run(["make", "-s", "-C", str(HERE)], check=True)
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not LIB.exists():
+            build()
+        L = C.CDLL(str(LIB))
+        L.wo_num_segkeys.argtypes = [C.c_int, C.c_int, C.c_int, u8p, ip, ip]
+        L.wo_segkeys.argtypes = [C.c_int, C.c_int, C.c_int, u8p, i32p, i32p]
+        L.wo_uncompress.argtypes = [C.c_int] * 3 + [C.c_int, i32p, i32p, C.c_int, i32p, i32p, f64p, f64p, C.c_void_p, f64p]
+        L.wo_compress.argtypes = [C.c_int] * 3 + [C.c_int, i32p, i32p, C.c_int, i32p, i32p, f64p, C.c_void_p, C.c_int, f64p, f64p]
+        for nm in ("wo_ana_rot_per", "wo_syn_rot_per", "wo_convrot_n_per", "wo_convrot_t_per",
+                   "wo_syn_grow_rot", "wo_ana_shrink_rot", "wo_mf_grow_rot", "wo_mf_shrink_rot"):
+            getattr(L, nm).argtypes = [C.c_int, C.c_int, f64p, f64p]
+        L.wo_kinetic_per_T.argtypes = [C.c_int] * 3 + [f64p, f64p, f64p, dp]
+        L.wo_kinetic_generic.argtypes = [C.c_int] * 3 + [i32p, f64p, f64p, f64p, dp]
+        L.wo_kinetic_wavelet.argtypes = [i32p, i32p, f64p, f64p, f64p, dp]
+        L.wo_synthese_generic.argtypes = [i32p, i32p, f64p, f64p, f64p]
+        L.wo_analyse_generic.argtypes = [i32p, i32p, f64p, f64p, f64p]
+        L.wo_magic_generic.argtypes = [i32p, i32p, f64p, f64p, f64p]
+        L.wo_magic_t_generic.argtypes = [i32p, i32p, f64p, f64p, f64p]
+        L.wo_locham_per.argtypes = [C.c_int] * 3 + [f64p, C.c_int, i32p, i32p, C.c_int, i32p, i32p,
+                                                    f64p, f64p, f64p, f64p, f64p, dp, dp]
+        L.wo_locham_generic.argtypes = [i32p, i32p, f64p, C.c_int, i32p, i32p, C.c_int, i32p, i32p,
+                                        f64p, f64p, f64p, f64p, f64p, dp, dp]
+        L.wo_locden_generic.argtypes = [i32p, i32p, C.c_int, i32p, i32p, C.c_int, i32p, i32p,
+                                        f64p, f64p, C.c_double, f64p]
+        L.wo_precond_scal.argtypes = [f64p, C.c_double, f64p]
+        L.wo_precond_generic.argtypes = [i32p, i32p, f64p, C.c_double, C.c_int,
+                                         C.c_int, C.c_int, i32p, i32p, C.c_int, C.c_int, i32p, i32p,
+                                         f64p, f64p, f64p]
+        L.wo_overlap.argtypes = [C.c_int, C.c_int, f64p, f64p]
+        L.wo_cholesky.argtypes = [C.c_int, f64p]
+        L.wo_cholesky.restype = C.c_int
+        L.wo_apply_potential.argtypes = [C.c_size_t, f64p, f64p]
+        L.wo_apply_potential.restype = C.c_double
+        _lib = L
+    return _lib
+
+
+def threads(n):
+    """Set the OpenMP thread count used by the oracle (for timing)."""
+    os.environ["OMP_NUM_THREADS"] = str(n)
+
+
+# ---------------------------------------------------------------- keys
+def segkeys(mask):
+    """mask[i3,i2,i1] (uint8) -> (keyg (nseg,2) int32 1-based, keyv (nseg,) int32)."""
+    mask = np.ascontiguousarray(mask, dtype=np.uint8)
+    n3, n2, n1 = (s - 1 for s in mask.shape)
+    ms, mv = C.c_int(), C.c_int()
+    lib().wo_num_segkeys(n1, n2, n3, mask, C.byref(ms), C.byref(mv))
+    keyg = np.zeros((ms.value, 2), np.int32)
+    keyv = np.zeros(ms.value, np.int32)
+    if ms.value:
+        lib().wo_segkeys(n1, n2, n3, mask, keyg, keyv)
+    return keyg, keyv
+
+
+def _k(a):
+    return np.ascontiguousarray(a, dtype=np.int32)
+
+
+class Desc:
+    """Wavefunction descriptor: coarse counts N=(N1,N2,N3), per-dim periodicity,
+    coarse and fine keys (1-based, as the reference)."""
+
+    def __init__(self, N, periodic, keyg_c, keyv_c, keyg_f, keyv_f):
+        self.N = np.asarray(N, np.int32)
+        self.per = np.asarray(periodic, np.int32)
+        self.keyg_c, self.keyv_c = _k(keyg_c), _k(keyv_c)
+        self.keyg_f, self.keyv_f = _k(keyg_f), _k(keyv_f)
+        self.nseg_c, self.nseg_f = len(self.keyv_c), len(self.keyv_f)
+        self.nvctr_c = int((self.keyg_c[:, 1] - self.keyg_c[:, 0] + 1).sum()) if self.nseg_c else 0
+        self.nvctr_f = int((self.keyg_f[:, 1] - self.keyg_f[:, 0] + 1).sum()) if self.nseg_f else 0
+
+    @property
+    def F(self):
+        return np.where(self.per == 1, 2 * self.N, 2 * self.N + 14)
+
+    @property
+    def I(self):
+        return np.where(self.per == 1, 2 * self.N, 2 * self.N + 29)
+
+    def args(self):
+        return (self.nseg_c, self.keyg_c, self.keyv_c, self.nseg_f, self.keyg_f, self.keyv_f)
+
+
+def desc_from_masks(mask_c, mask_f, periodic):
+    kc, vc = segkeys(mask_c)
+    kf, vf = segkeys(mask_f)
+    N = mask_c.shape[::-1]
+    return Desc(N, periodic, kc, vc, kf, vf)
+
+
+# ---------------------------------------------------------------- 1D passes
+def _rot(fn, n, ndat, x, lout):
+    x = np.ascontiguousarray(x, np.float64)
+    y = np.empty(ndat * lout, np.float64)
+    getattr(lib(), fn)(n, ndat, x, y)
+    return y
+
+
+def syn_rot_per(n, ndat, x):
+    return _rot("wo_syn_rot_per", n, ndat, x, 2 * n + 2)
+
+
+def ana_rot_per(n, ndat, x):
+    return _rot("wo_ana_rot_per", n, ndat, x, 2 * n + 2)
+
+
+def convrot_n_per(n1, ndat, x):
+    return _rot("wo_convrot_n_per", n1, ndat, x, n1 + 1)
+
+
+def convrot_t_per(n1, ndat, x):
+    return _rot("wo_convrot_t_per", n1, ndat, x, n1 + 1)
+
+
+def syn_grow_rot(N, ndat, x):
+    return _rot("wo_syn_grow_rot", N, ndat, x, 2 * N + 14)
+
+
+def ana_shrink_rot(N, ndat, x):
+    return _rot("wo_ana_shrink_rot", N, ndat, x, 2 * N)
+
+
+def mf_grow_rot(Lf, ndat, x):
+    return _rot("wo_mf_grow_rot", Lf, ndat, x, Lf + 15)
+
+
+def mf_shrink_rot(Lf, ndat, x):
+    return _rot("wo_mf_shrink_rot", Lf, ndat, x, Lf)
+
+
+# ---------------------------------------------------------------- 3D ops
+def uncompress(d, psi_c, psi_f, scal=None):
+    N = d.N
+    out = np.empty(8 * int(np.prod(N)), np.float64)
+    sc = None if scal is None else np.ascontiguousarray(scal, np.float64).ctypes.data
+    lib().wo_uncompress(int(N[0]) - 1, int(N[1]) - 1, int(N[2]) - 1, *d.args(),
+                        np.ascontiguousarray(psi_c, np.float64), np.ascontiguousarray(psi_f, np.float64), sc, out)
+    return out
+
+
+def compress(d, psig, scal=None, acc=False, psi_c=None, psi_f=None):
+    N = d.N
+    pc = np.zeros(d.nvctr_c) if psi_c is None else np.array(psi_c, np.float64)
+    pf = np.zeros(7 * d.nvctr_f) if psi_f is None else np.array(psi_f, np.float64)
+    sc = None if scal is None else np.ascontiguousarray(scal, np.float64).ctypes.data
+    lib().wo_compress(int(N[0]) - 1, int(N[1]) - 1, int(N[2]) - 1, *d.args(),
+                      np.ascontiguousarray(psig, np.float64), sc, int(acc), pc, pf)
+    return pc, pf
+
+
+def synthese(d, psig):
+    n = int(np.prod(d.I))
+    out, w = np.empty(n), np.empty(n)
+    lib().wo_synthese_generic(d.N, d.per, np.ascontiguousarray(psig, np.float64), out, w)
+    return out[: int(np.prod(d.F))]
+
+
+def analyse(d, y):
+    n = int(np.prod(d.I))
+    out, w = np.empty(n), np.empty(n)
+    lib().wo_analyse_generic(d.N, d.per, np.ascontiguousarray(y, np.float64), out, w)
+    return out[: 8 * int(np.prod(d.N))]
+
+
+def magic(d, x):
+    n = int(np.prod(d.I))
+    out, w = np.empty(n), np.empty(n)
+    lib().wo_magic_generic(np.asarray(d.F, np.int32), d.per, np.ascontiguousarray(x, np.float64), out, w)
+    return out
+
+
+def magic_t(d, r):
+    n = int(np.prod(d.I))
+    out, w = np.empty(n), np.empty(n)
+    lib().wo_magic_t_generic(np.asarray(d.F, np.int32), d.per, np.ascontiguousarray(r, np.float64), out, w)
+    return out[: int(np.prod(d.F))]
+
+
+def kinetic(d, hgrid_fine, x, y=None):
+    F = d.F
+    x = np.ascontiguousarray(x, np.float64)
+    y = np.zeros_like(x) if y is None else np.array(y, np.float64)
+    ek = C.c_double()
+    lib().wo_kinetic_generic(int(F[0]), int(F[1]), int(F[2]), d.per,
+                             np.asarray(hgrid_fine, np.float64), x, y, C.byref(ek))
+    return y, ek.value
+
+
+def kinetic_wavelet(d, hgrid_coarse, psig):
+    y = np.zeros(8 * int(np.prod(d.N)))
+    ek = C.c_double()
+    lib().wo_kinetic_wavelet(d.N, d.per, np.asarray(hgrid_coarse, np.float64),
+                             np.ascontiguousarray(psig, np.float64), y, C.byref(ek))
+    return y, ek.value
+
+
+def locham_per(d, hgrid, psi_c, psi_f, pot):
+    """Fortran-chain periodic Hpsi (hpsi accumulated from zero)."""
+    N = d.N
+    hc, hf = np.zeros(d.nvctr_c), np.zeros(7 * d.nvctr_f)
+    ek, ep = C.c_double(), C.c_double()
+    lib().wo_locham_per(int(N[0]) - 1, int(N[1]) - 1, int(N[2]) - 1, np.asarray(hgrid, np.float64), *d.args(),
+                        np.ascontiguousarray(psi_c, np.float64), np.ascontiguousarray(psi_f, np.float64),
+                        np.ascontiguousarray(pot, np.float64), hc, hf, C.byref(ek), C.byref(ep))
+    return hc, hf, ek.value, ep.value
+
+
+def locham(d, hgrid, psi_c, psi_f, pot):
+    """OpenCL-composition Hpsi for any per-dimension BC (hpsi overwritten)."""
+    hc, hf = np.zeros(d.nvctr_c), np.zeros(7 * d.nvctr_f)
+    ek, ep = C.c_double(), C.c_double()
+    lib().wo_locham_generic(d.N, d.per, np.asarray(hgrid, np.float64), *d.args(),
+                            np.ascontiguousarray(psi_c, np.float64), np.ascontiguousarray(psi_f, np.float64),
+                            np.ascontiguousarray(pot, np.float64), hc, hf, C.byref(ek), C.byref(ep))
+    return hc, hf, ek.value, ep.value
+
+
+def locden(d, psi_c, psi_f, hfac, rho=None):
+    n = int(np.prod(d.I))
+    rho = np.zeros(n) if rho is None else np.array(rho, np.float64)
+    lib().wo_locden_generic(d.N, d.per, *d.args(), np.ascontiguousarray(psi_c, np.float64),
+                            np.ascontiguousarray(psi_f, np.float64), float(hfac), rho)
+    return rho
+
+
+def precond_scal(h_fine, c):
+    s = np.empty(8)
+    lib().wo_precond_scal(np.asarray(h_fine, np.float64), float(c), s)
+    return s
+
+
+def precond(d, h_fine, c, ncong, x, b):
+    """ocl_preconditioner_generic: returns (x_out, rnorm[ncong+1])."""
+    x = np.array(x, np.float64)
+    b = np.array(b, np.float64)
+    rn = np.zeros(ncong + 1)
+    lib().wo_precond_generic(d.N, d.per, np.asarray(h_fine, np.float64), float(c), int(ncong),
+                             d.nseg_c, d.nvctr_c, d.keyg_c, d.keyv_c, d.nseg_f, d.nvctr_f, d.keyg_f, d.keyv_f,
+                             x, b, rn)
+    return x, rn
+
+
+def overlap(psi):
+    """psi (norb, nvctr) row-major == (nvctr, norb) column-major -> S (norb,norb)."""
+    psi = np.ascontiguousarray(psi, np.float64)
+    norb, nv = psi.shape
+    S = np.empty((norb, norb))
+    lib().wo_overlap(nv, norb, psi, S)
+    return S
+
+
+def cholesky_lower(S):
+    """Returns L (row-major numpy) with S = L L^T."""
+    A = np.array(S, np.float64, order="C")
+    info = lib().wo_cholesky(A.shape[0], A)  # operates column-major: A^T viewed
+    if info:
+        raise np.linalg.LinAlgError("not positive definite at %d" % info)
+    return A.T.copy()
+
+
+# ---------------------------------------------------------------- reference pin
+def ref_magicfilter():
+    """ctypes handle to the reference's own C magic filter, or None."""
+    if not REF_MF.exists():
+        return None
+    L = C.CDLL(str(REF_MF))
+    for nm in ("magicfilter1d_naive_", "magicfilter1d_t_naive_", "magicfilter1d_sse_", "magicfilter1d_t_sse_"):
+        getattr(L, nm).argtypes = [C.POINTER(C.c_uint), C.POINTER(C.c_uint), f64p, f64p]
+    return L
