@@ -1,0 +1,268 @@
+// Common device code of the wvlh library: filter constants, boundary helpers
+// and the register-blocked 1D line passes every kernel is built from.
+//
+// A "line pass" applies one 1D operator of the Daubechies-16 local
+// Hamiltonian (synthesis, analysis, magic filter, transposed magic filter,
+// 29-tap kinetic) along lines of a shared-memory buffer.  Lines are addressed
+// as base + line*ls + p*ps, so the same code walks rows, columns or z-pencils.
+// Each thread owns a segment of SEG consecutive outputs of one line, loads
+// the input window for the whole segment into registers once, and issues
+// SEG*taps FMAs from registers; the filter taps are compile-time immediates.
+//
+// Operator definitions (the math of the reference, Fortran indices):
+//  syn  (orbitals/convolut_simple_per.f90:89-103, free: OpenCL syngrow1d):
+//       y(2i+o) = sum_{l=-4..4} ch(2l+o) s(i-l) + cg(2l+o) w(i-l)
+//  ana  (convolut_simple_per.f90:11-57, free: OpenCL anashrink1d):
+//       c(i) = sum_{l=-7..8} ch(l) y(2i+l),  d(i) = sum cg(l) y(2i+l)
+//  mf   (convrot_n_per :200-243):  r(i) = sum_{l=-8..7} fil(l) x(i+l)
+//  mft  (convrot_t_per :246-291):  x(i) = sum_{l=-7..8} fil(-l) r(i+l)
+//  kin  (convolut_kinetic_per_T :377-460):
+//       y(i) += -1/(2h^2) sum_{l=-14..14} a(|l|) x(i+l)
+// Periodic lines wrap; free lines are zero outside and grow/shrink:
+// fine grid f in [-7, 2N+6] (stored at q=f+7), ISF grid in [-14, 2N+14]
+// (stored at r+14), exactly the OpenCL grow/shrink kernels' extents.
+//
+// FP32 energies: E_kin is accumulated in FP64 from the FP32 stencil result
+// with the FP64 scale -1/(2h^2) and a low-order correction for the rounding of
+// the five largest kinetic taps to FP32 (tap = hi + lo, lo applied to the
+// already formed pair sums), which removes the systematic O(1e-8) relative
+// bias that FP32 constants would put on the energy.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "wvl_filters.h"
+
+namespace wvlh {
+
+template <class T> struct Filt {
+    static __device__ __forceinline__ constexpr T ch(int i) { return (T)(WVL_CH_AT(i)); }
+    static __device__ __forceinline__ constexpr T cg(int i) { return (T)(WVL_CG_AT(i)); }
+    static __device__ __forceinline__ constexpr T mf(int i) { return (T)(WVL_MF_AT(i)); }
+    static __device__ __forceinline__ constexpr T kin(int i) { return (T)(WVL_KIN_AT(i)); }
+    // residual of the T-rounded kinetic tap (zero in FP64)
+    static __device__ __forceinline__ constexpr T kin_lo(int i)
+    {
+        return (T)((WVL_KIN_AT(i)) - (double)(T)(WVL_KIN_AT(i)));
+    }
+};
+
+// Fine-grid and ISF-grid extents of one dimension with N coarse cells.
+__host__ __device__ __forceinline__ int fine_len(int N, int per) { return per ? 2 * N : 2 * N + 14; }
+__host__ __device__ __forceinline__ int isf_len(int N, int per) { return per ? 2 * N : 2 * N + 29; }
+
+__device__ __forceinline__ int wrapi(int p, int L)
+{
+    if ((unsigned)p < (unsigned)L) return p;
+    p %= L;
+    return p < 0 ? p + L : p;
+}
+
+// Load x[k] = line(p0 + k), k < W, with periodic wrap or zero padding; the
+// common interior case takes a single base address and constant strides.
+template <class T, int W>
+__device__ __forceinline__ void load_window(T (&x)[W], const T *in, int ps, int p0, int L, int per)
+{
+    if (p0 >= 0 && p0 + W <= L) {
+        const T *b = in + p0 * ps;
+#pragma unroll
+        for (int k = 0; k < W; ++k) x[k] = b[k * ps];
+    } else if (per) {
+#pragma unroll
+        for (int k = 0; k < W; ++k) x[k] = in[wrapi(p0 + k, L) * ps];
+    } else {
+#pragma unroll
+        for (int k = 0; k < W; ++k) {
+            const int p = p0 + k;
+            x[k] = ((unsigned)p < (unsigned)L) ? in[p * ps] : T(0);
+        }
+    }
+}
+
+// Distribute (line, segment) work items over the block: consecutive threads
+// take consecutive lines so that x-passes (lanes = rows, odd pitch) and
+// y/z-passes (lanes = contiguous columns) are both bank-conflict free.
+template <class F>
+__device__ __forceinline__ void for_items(int nlines, int nseg, F &&f)
+{
+    const int items = nlines * nseg;
+    for (int it = threadIdx.x; it < items; it += blockDim.x) {
+        const int s = it / nlines;
+        f(it - s * nlines, s);
+    }
+}
+
+struct LineGeom {
+    int nlines;
+    int src_ls, src_ps;
+    int dst_ls, dst_ps;
+};
+
+// ---------------------------------------------------------------- synthesis
+// src line: [s(0..N-1) | w(0..N-1)], dst line: F = fine_len(N,per) values.
+template <class T, int SEG>
+__device__ void pass_syn(const T *src, T *dst, const LineGeom g, int N, int per)
+{
+    static_assert(SEG % 2 == 0, "even segment");
+    constexpr int W = SEG / 2 + 8;
+    const int F = fine_len(N, per);
+    const int off = per ? 0 : 7;      // storage index q = f + off
+    const int fstart = per ? 0 : -8;  // even start in Fortran fine coordinates
+    const int nseg = (F + off - fstart + SEG - 1) / SEG;
+    for_items(g.nlines, nseg, [&](int line, int s) {
+        const T *in = src + line * g.src_ls;
+        T *out = dst + line * g.dst_ls;
+        const int f0 = fstart + s * SEG;
+        const int ib = f0 / 2 - 4;  // f0 is even, so f0/2 is exact
+        T xs[W], xw[W];
+        load_window<T, W>(xs, in, g.src_ps, ib, N, per);
+        load_window<T, W>(xw, in + N * g.src_ps, g.src_ps, ib, N, per);
+#pragma unroll
+        for (int t = 0; t < SEG; ++t) {
+            const int q = f0 + t + off;
+            const int o = t & 1;
+            const int ic = t / 2 + 4;  // window index of coarse position i0 + t/2
+            T acc = T(0);
+#pragma unroll
+            for (int l = -4; l <= 4; ++l) {
+                const int m = 2 * l + o;  // ch_syn(m) = ch(m) for m in [-7,8]
+                if (m < -7 || m > 8) continue;
+                acc = fma(Filt<T>::ch(m + 7), xs[ic - l], acc);
+                acc = fma(Filt<T>::cg(m + 7), xw[ic - l], acc);
+            }
+            if ((unsigned)q < (unsigned)F) out[q * g.dst_ps] = acc;
+        }
+    });
+}
+
+// ---------------------------------------------------------------- analysis
+// src line: F fine values; dst line: [c(0..N-1) | d(0..N-1)]
+template <class T, int SEG>
+__device__ void pass_ana(const T *src, T *dst, const LineGeom g, int N, int per)
+{
+    static_assert(SEG % 2 == 0, "even segment");
+    constexpr int H = SEG / 2;
+    constexpr int W = SEG + 14;
+    const int F = fine_len(N, per);
+    const int off = per ? 0 : 7;
+    const int nseg = (N + H - 1) / H;
+    for_items(g.nlines, nseg, [&](int line, int s) {
+        const T *in = src + line * g.src_ls;
+        T *out = dst + line * g.dst_ls;
+        const int i0 = s * H;
+        T x[W];
+        load_window<T, W>(x, in, g.src_ps, 2 * i0 - 7 + off, F, per);
+#pragma unroll
+        for (int t = 0; t < H; ++t) {
+            T ci = T(0), di = T(0);
+#pragma unroll
+            for (int l = 0; l < 16; ++l) {
+                ci = fma(Filt<T>::ch(l), x[2 * t + l], ci);
+                di = fma(Filt<T>::cg(l), x[2 * t + l], di);
+            }
+            const int i = i0 + t;
+            if (i < N) {
+                out[i * g.dst_ps] = ci;
+                out[(i + N) * g.dst_ps] = di;
+            }
+        }
+    });
+}
+
+// ---------------------------------------------------------------- magic filter
+// MODE 0: mf periodic, 1: mft periodic, 2: mf grow (F -> F+15), 3: mft shrink (F+15 -> F)
+template <class T, int SEG, int MODE>
+__device__ void pass_mf(const T *src, T *dst, const LineGeom g, int Lin, int Lout)
+{
+    constexpr int W = SEG + 15;
+    constexpr int shift = MODE == 0 ? -8 : MODE == 1 ? -7 : MODE == 2 ? -15 : 0;
+    constexpr bool rev = (MODE == 1 || MODE == 3);
+    constexpr int per = (MODE <= 1);
+    const int nseg = (Lout + SEG - 1) / SEG;
+    for_items(g.nlines, nseg, [&](int line, int s) {
+        const T *in = src + line * g.src_ls;
+        T *out = dst + line * g.dst_ls;
+        const int q0 = s * SEG;
+        T x[W];
+        load_window<T, W>(x, in, g.src_ps, q0 + shift, Lin, per);
+#pragma unroll
+        for (int t = 0; t < SEG; ++t) {
+            T acc = T(0);
+#pragma unroll
+            for (int k = 0; k < 16; ++k) acc = fma(Filt<T>::mf(rev ? 15 - k : k), x[t + k], acc);
+            const int q = q0 + t;
+            if (q < Lout) out[q * g.dst_ps] = acc;
+        }
+    });
+}
+
+// ---------------------------------------------------------------- kinetic
+// dst(q) = (ACC ? dst(q) : cshift * src(q)) + scale * sum_l a(|l|) src(q+l)
+// with scale = -1/(2h^2) (cshift: the preconditioner's c of (T + c),
+// OpenCL/Preconditioner.c:108); ekin += src(q) * scale * conv in FP64.
+template <class T, int SEG, bool ACC>
+__device__ void pass_kin(const T *src, T *dst, const LineGeom g, int L, int per, double scale_d, T cshift,
+                         double *ekin)
+{
+    constexpr int W = SEG + 28;
+    const T scale = (T)scale_d;
+    const int nseg = (L + SEG - 1) / SEG;
+    double e = 0.0;
+    for_items(g.nlines, nseg, [&](int line, int s) {
+        const T *in = src + line * g.src_ls;
+        T *out = dst + line * g.dst_ls;
+        const int q0 = s * SEG;
+        T x[W];
+        load_window<T, W>(x, in, g.src_ps, q0 - 14, L, per);
+#pragma unroll
+        for (int t = 0; t < SEG; ++t) {
+            T conv = Filt<T>::kin(0) * x[t + 14];
+            T lo = T(0);
+            if constexpr (sizeof(T) == 4) lo = Filt<T>::kin_lo(0) * x[t + 14];
+#pragma unroll
+            for (int l = 1; l <= 14; ++l) {
+                const T pr = x[t + 14 + l] + x[t + 14 - l];
+                conv = fma(Filt<T>::kin(l), pr, conv);
+                if constexpr (sizeof(T) == 4) {
+                    if (l <= 4) lo = fma(Filt<T>::kin_lo(l), pr, lo);
+                }
+            }
+            const int q = q0 + t;
+            if (q < L) {
+                if (ekin) {
+                    if constexpr (sizeof(T) == 4) e += (double)x[t + 14] * (((double)conv + (double)lo) * scale_d);
+                    else e += x[t + 14] * (conv * scale_d);
+                }
+                const T base = ACC ? out[q * g.dst_ps] : cshift * x[t + 14];
+                out[q * g.dst_ps] = fma(scale, conv, base);
+            }
+        }
+    });
+    if (ekin) *ekin += e;
+}
+
+// ---------------------------------------------------------------- reductions
+__device__ __forceinline__ double warp_sum(double v)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// block-wide sum, result valid in thread 0; red must hold 32 doubles
+__device__ __forceinline__ double block_sum(double v, double *red)
+{
+    v = warp_sum(v);
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    __syncthreads();
+    if (lane == 0) red[wid] = v;
+    __syncthreads();
+    double r = 0.0;
+    if (wid == 0) {
+        r = (lane < (int)(blockDim.x >> 5)) ? red[lane] : 0.0;
+        r = warp_sum(r);
+    }
+    return r;
+}
+
+}  // namespace wvlh

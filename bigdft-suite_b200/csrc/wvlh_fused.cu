@@ -1,0 +1,427 @@
+// Fused, batched local Hamiltonian (Hpsi, E_kin, E_pot) for many orbitals
+// and many localisation regions in three kernels, FP32 or FP64.
+//
+// The reference applies locham to one orbital at a time as 13 full-array
+// passes (uncompress, 3x syn, 3x MF, xV, 3x MF^T, 3x kinetic, 3x ana,
+// compress: orbitals/daubisf.f90:214-331, locregs/locreg_operations.f90:2502-2937,
+// OpenCL/Hamiltonian.c:105-172).  Because every 1D operator acts on one
+// axis, the chain factorises as
+//     Hpsi = A_x A_y [ Mt_x Mt_y Z1 + Z2 + (K_x + K_y) P ]
+//     P  = S_x S_y psi,    Q = M_x M_y P                       (plane kernel K1)
+//     Z1 = A_z Mt_z V M_z S_z Q,   Z2 = A_z K_z S_z P            (z kernel K2)
+// (S syn, A ana, M magic filter, K kinetic) so that each kernel keeps a whole
+// xy-plane or a whole z-pencil tile in shared memory and chains its 1D passes
+// there.  E_pot = sum V r^2 comes from K2; E_kin = sum_d <X|K_d X> with
+// X = S^3 psi: the z part from K2 on X itself, the x,y parts from K3 on P
+// (<X|K_x X> = <P|K_x P> because S_z is an isometry).  Energies are reduced
+// in FP64 into per-CTA partial slots and summed in a fixed order.
+#include <cuda_runtime.h>
+
+#include "wvlh_common.cuh"
+#include "wvlh_internal.h"
+
+namespace wvlh {
+
+constexpr int TX = TX_;
+constexpr int TY = TY_;
+constexpr int TC = TX * TY;
+
+template <class T> struct Seg;
+template <> struct Seg<float> { static constexpr int v = 8; };
+template <> struct Seg<double> { static constexpr int v = 4; };
+
+struct Dims {
+    int N1, N2, N3, p1, p2, p3;
+    int G1, G2, G3, F1, F2, F3, I1, I2, I3;
+    __device__ __forceinline__ explicit Dims(const LrDev &L)
+    {
+        N1 = L.N[0]; N2 = L.N[1]; N3 = L.N[2];
+        p1 = L.per[0]; p2 = L.per[1]; p3 = L.per[2];
+        G1 = 2 * N1; G2 = 2 * N2; G3 = 2 * N3;
+        F1 = fine_len(N1, p1); F2 = fine_len(N2, p2); F3 = fine_len(N3, p3);
+        I1 = isf_len(N1, p1); I2 = isf_len(N2, p2); I3 = isf_len(N3, p3);
+    }
+    __device__ __forceinline__ int pitch() const { return (max(G1, max(F1, I1))) | 1; }
+    __device__ __forceinline__ int rows() const { return max(G2, max(F2, I2)); }
+};
+
+__device__ __forceinline__ LineGeom rows_geom(int nrows, int pitch)
+{
+    return LineGeom{nrows, pitch, 1, pitch, 1};
+}
+__device__ __forceinline__ LineGeom cols_geom(int ncols, int pitch)
+{
+    return LineGeom{ncols, 1, pitch, 1, pitch};
+}
+
+// fine component c=1..7 of psi_f -> (s1,s2,s3) bits (wavelib/un-compress.f90:930-936)
+__device__ __forceinline__ int fs1(int c) { return c & 1; }
+__device__ __forceinline__ int fs2(int c) { return (c >> 1) & 1; }
+__device__ __forceinline__ int fs3(int c) { return (c >> 2) & 1; }
+
+// Scatter the compressed coefficients of wavelet-basis plane kz into the
+// (G2 x G1, pitch) buffer A, which must be zero.  psi points at [psi_c|psi_f].
+template <class T, class TI>
+__device__ void gather_plane(T *A, int pitch, const LrDev &L, int kz, const TI *psi)
+{
+    const int N1 = L.N[0], N2 = L.N[1], N3 = L.N[2];
+    const int s3 = kz >= N3;
+    const int i3 = kz - s3 * N3;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    if (!s3) {
+        const int a = L.plane_c[i3], b = L.plane_c[i3 + 1];
+        for (int sg = a + warp; sg < b; sg += nw) {
+            const int4 d = L.seg_c[sg];
+            for (int t = lane; t < d.z; t += 32) A[d.y * pitch + d.x + t] = (T)psi[d.w + t];
+        }
+    }
+    const TI *pf = psi + L.nvctr_c;
+    const int a = L.plane_f[i3], b = L.plane_f[i3 + 1];
+    for (int sg = a + warp; sg < b; sg += nw) {
+        const int4 d = L.seg_f[sg];
+        for (int t = lane; t < d.z; t += 32) {
+            const TI *src = pf + 7 * (size_t)(d.w + t);
+#pragma unroll
+            for (int c = 1; c <= 7; ++c) {
+                if (fs3(c) != s3) continue;
+                A[(fs2(c) * N2 + d.y) * pitch + fs1(c) * N1 + d.x + t] = (T)src[c - 1];
+            }
+        }
+    }
+}
+
+// Inverse of gather_plane: write (or add into) the compressed output.
+template <class T, class TO>
+__device__ void scatter_plane(const T *A, int pitch, const LrDev &L, int kz, TO *out, bool accumulate)
+{
+    const int N1 = L.N[0], N2 = L.N[1], N3 = L.N[2];
+    const int s3 = kz >= N3;
+    const int i3 = kz - s3 * N3;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    if (!s3) {
+        const int a = L.plane_c[i3], b = L.plane_c[i3 + 1];
+        for (int sg = a + warp; sg < b; sg += nw) {
+            const int4 d = L.seg_c[sg];
+            for (int t = lane; t < d.z; t += 32) {
+                const TO v = (TO)A[d.y * pitch + d.x + t];
+                out[d.w + t] = accumulate ? out[d.w + t] + v : v;
+            }
+        }
+    }
+    TO *pf = out + L.nvctr_c;
+    const int a = L.plane_f[i3], b = L.plane_f[i3 + 1];
+    for (int sg = a + warp; sg < b; sg += nw) {
+        const int4 d = L.seg_f[sg];
+        for (int t = lane; t < d.z; t += 32) {
+            TO *dst = pf + 7 * (size_t)(d.w + t);
+#pragma unroll
+            for (int c = 1; c <= 7; ++c) {
+                if (fs3(c) != s3) continue;
+                const TO v = (TO)A[(fs2(c) * N2 + d.y) * pitch + fs1(c) * N1 + d.x + t];
+                dst[c - 1] = accumulate ? dst[c - 1] + v : v;
+            }
+        }
+    }
+}
+
+template <class T>
+__device__ __forceinline__ void zero_region(T *A, int rows, int cols, int pitch)
+{
+    for (int i = threadIdx.x; i < rows * pitch; i += blockDim.x) A[i] = T(0);
+    (void)cols;
+}
+
+template <class T>
+__device__ __forceinline__ void store_plane(const T *A, int pitch, int rows, int cols, T *g)
+{
+    for (int i = threadIdx.x; i < rows * cols; i += blockDim.x) {
+        const int r = i / cols, c = i - r * cols;
+        g[i] = A[r * pitch + c];
+    }
+}
+
+template <class T>
+__device__ __forceinline__ void load_plane(T *A, int pitch, int rows, int cols, const T *g)
+{
+    for (int i = threadIdx.x; i < rows * cols; i += blockDim.x) {
+        const int r = i / cols, c = i - r * cols;
+        A[r * pitch + c] = g[i];
+    }
+}
+
+// ---------------------------------------------------------------------------
+// K1: compressed psi -> P = S_x S_y psi and Q = M_x M_y P for one z-plane.
+// TI is the storage type of psi (may differ from compute type T).
+template <class T, class TI>
+__global__ void __launch_bounds__(256) k1_plane_forward(const LrDev *__restrict__ lrs, const OrbDev *__restrict__ orbs,
+                                                        const int2 *__restrict__ work, const TI *__restrict__ psi,
+                                                        T *__restrict__ scratch)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int2 w = work[blockIdx.x];
+    const OrbDev o = orbs[w.x];
+    const LrDev L = lrs[o.lr];
+    const Dims d(L);
+    const int kz = w.y;
+    const int pitch = d.pitch();
+    T *A = reinterpret_cast<T *>(smem_raw);
+    T *B = A + (size_t)d.rows() * pitch;
+    constexpr int SEG = Seg<T>::v;
+
+    zero_region(A, d.G2, d.G1, pitch);
+    __syncthreads();
+    gather_plane<T, TI>(A, pitch, L, kz, psi + o.psi);
+    __syncthreads();
+    pass_syn<T, SEG>(A, B, rows_geom(d.G2, pitch), d.N1, d.p1);   // S_x: G2 rows, G1 -> F1
+    __syncthreads();
+    pass_syn<T, SEG>(B, A, cols_geom(d.F1, pitch), d.N2, d.p2);   // S_y: F1 cols, G2 -> F2
+    __syncthreads();
+    store_plane(A, pitch, d.F2, d.F1, scratch + o.sP + (size_t)kz * d.F2 * d.F1);
+    if (d.p1) pass_mf<T, SEG, 0>(A, B, rows_geom(d.F2, pitch), d.F1, d.I1);
+    else pass_mf<T, SEG, 2>(A, B, rows_geom(d.F2, pitch), d.F1, d.I1);
+    __syncthreads();
+    if (d.p2) pass_mf<T, SEG, 0>(B, A, cols_geom(d.I1, pitch), d.F2, d.I2);
+    else pass_mf<T, SEG, 2>(B, A, cols_geom(d.I1, pitch), d.F2, d.I2);
+    __syncthreads();
+    store_plane(A, pitch, d.I2, d.I1, scratch + o.sQ + (size_t)kz * d.I2 * d.I1);
+}
+
+// ---------------------------------------------------------------------------
+// K2: z-pencil tiles.  chain 0: Z1 = A_z Mt_z (V . M_z S_z Q) in place of Q,
+// E_pot partial.  chain 1: Z2 = A_z K_z S_z P, E_kin(z) partial.
+template <class T, class TV>
+__global__ void __launch_bounds__(256) k2_zpencil(const LrDev *__restrict__ lrs, const OrbDev *__restrict__ orbs,
+                                                  const int4 *__restrict__ work, const int *__restrict__ slots,
+                                                  const TV *__restrict__ pot, T *__restrict__ scratch,
+                                                  double *__restrict__ part_pot, double *__restrict__ part_kin,
+                                                  int part_stride)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ double red[32];
+    const int4 w = work[blockIdx.x];
+    const OrbDev o = orbs[w.x];
+    const LrDev L = lrs[o.lr];
+    const Dims d(L);
+    const int chain = w.y, x0 = w.z, y0 = w.w;
+    const int zl = max(d.G3, max(d.F3, d.I3));
+    T *A = reinterpret_cast<T *>(smem_raw);
+    T *B = A + (size_t)zl * TC;
+    constexpr int SEG = Seg<T>::v;
+    const int W = chain == 0 ? d.I1 : d.F1;   // plane width/height of the data
+    const int H = chain == 0 ? d.I2 : d.F2;
+    T *g = scratch + (chain == 0 ? o.sQ : o.sP);
+    T *gz = scratch + (chain == 0 ? o.sQ : o.sZ);
+    const size_t plane = (size_t)W * H;
+
+    // load the tile: TC columns x G3 z' rows, zero outside the plane
+    for (int i = threadIdx.x; i < d.G3 * TC; i += blockDim.x) {
+        const int z = i / TC, c = i - z * TC;
+        const int x = x0 + (c % TX), y = y0 + (c / TX);
+        A[i] = (x < W && y < H) ? g[(size_t)z * plane + (size_t)y * W + x] : T(0);
+    }
+    __syncthreads();
+    const LineGeom zg{TC, 1, TC, 1, TC};
+    double e = 0.0;
+    pass_syn<T, SEG>(A, B, zg, d.N3, d.p3);                      // S_z: G3 -> F3
+    __syncthreads();
+    if (chain == 0) {
+        if (d.p3) pass_mf<T, SEG, 0>(B, A, zg, d.F3, d.I3);       // M_z: F3 -> I3
+        else pass_mf<T, SEG, 2>(B, A, zg, d.F3, d.I3);
+        __syncthreads();
+        // psir <- V psir, epot += V psir^2 (orbitals/potential.f90:1011-1031)
+        const TV *V = pot + o.pot;
+        for (int i = threadIdx.x; i < d.I3 * TC; i += blockDim.x) {
+            const int z = i / TC, c = i - z * TC;
+            const int x = x0 + (c % TX), y = y0 + (c / TX);
+            if (x < W && y < H) {
+                const T r = A[i];
+                const T wv = (T)V[((size_t)z * d.I2 + y) * d.I1 + x] * r;
+                e += (double)wv * (double)r;
+                A[i] = wv;
+            } else {
+                A[i] = T(0);
+            }
+        }
+        __syncthreads();
+        if (d.p3) pass_mf<T, SEG, 1>(A, B, zg, d.I3, d.F3);       // Mt_z: I3 -> F3
+        else pass_mf<T, SEG, 3>(A, B, zg, d.I3, d.F3);
+        __syncthreads();
+        pass_ana<T, SEG>(B, A, zg, d.N3, d.p3);                  // A_z: F3 -> G3
+    } else {
+        const double scale = -0.5 / ((0.5 * L.hgrid[2]) * (0.5 * L.hgrid[2]));
+        pass_kin<T, SEG, false>(B, A, zg, d.F3, d.p3, scale, T(0), &e);   // K_z X
+        __syncthreads();
+        pass_ana<T, SEG>(A, B, zg, d.N3, d.p3);                  // A_z: F3 -> G3
+        __syncthreads();
+        T *t = A; A = B; B = t;                                   // result in A
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < d.G3 * TC; i += blockDim.x) {
+        const int z = i / TC, c = i - z * TC;
+        const int x = x0 + (c % TX), y = y0 + (c / TX);
+        if (x < W && y < H) gz[(size_t)z * plane + (size_t)y * W + x] = A[i];
+    }
+    const double s = block_sum(e, red);
+    if (threadIdx.x == 0) (chain == 0 ? part_pot : part_kin)[(size_t)w.x * part_stride + slots[blockIdx.x]] = s;
+}
+
+// ---------------------------------------------------------------------------
+// K3: Hpsi plane kz = A_x A_y [Mt_x Mt_y Z1 + Z2 + (K_x + K_y) P]
+template <class T, class TO>
+__global__ void __launch_bounds__(256) k3_plane_backward(const LrDev *__restrict__ lrs, const OrbDev *__restrict__ orbs,
+                                                         const int2 *__restrict__ work, const int *__restrict__ slots,
+                                                         const T *__restrict__ scratch, TO *__restrict__ hpsi,
+                                                         double *__restrict__ part_kin, int part_stride, int accumulate)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ double red[32];
+    const int2 w = work[blockIdx.x];
+    const OrbDev o = orbs[w.x];
+    const LrDev L = lrs[o.lr];
+    const Dims d(L);
+    const int kz = w.y;
+    const int pitch = d.pitch();
+    T *A = reinterpret_cast<T *>(smem_raw);
+    T *B = A + (size_t)d.rows() * pitch;
+    constexpr int SEG = Seg<T>::v;
+
+    load_plane(A, pitch, d.I2, d.I1, scratch + o.sQ + (size_t)kz * d.I2 * d.I1);
+    __syncthreads();
+    if (d.p1) pass_mf<T, SEG, 1>(A, B, rows_geom(d.I2, pitch), d.I1, d.F1);   // Mt_x
+    else pass_mf<T, SEG, 3>(A, B, rows_geom(d.I2, pitch), d.I1, d.F1);
+    __syncthreads();
+    if (d.p2) pass_mf<T, SEG, 1>(B, A, cols_geom(d.F1, pitch), d.I2, d.F2);   // Mt_y
+    else pass_mf<T, SEG, 3>(B, A, cols_geom(d.F1, pitch), d.I2, d.F2);
+    __syncthreads();
+    {
+        const T *z2 = scratch + o.sZ + (size_t)kz * d.F2 * d.F1;
+        const T *p = scratch + o.sP + (size_t)kz * d.F2 * d.F1;
+        for (int i = threadIdx.x; i < d.F2 * d.F1; i += blockDim.x) {
+            const int r = i / d.F1, c = i - r * d.F1;
+            A[r * pitch + c] += z2[i];
+            B[r * pitch + c] = p[i];
+        }
+    }
+    __syncthreads();
+    double e = 0.0;
+    const double sx = -0.5 / ((0.5 * L.hgrid[0]) * (0.5 * L.hgrid[0]));
+    const double sy = -0.5 / ((0.5 * L.hgrid[1]) * (0.5 * L.hgrid[1]));
+    pass_kin<T, SEG, true>(B, A, rows_geom(d.F2, pitch), d.F1, d.p1, sx, T(0), &e);   // += K_x P
+    __syncthreads();
+    pass_kin<T, SEG, true>(B, A, cols_geom(d.F1, pitch), d.F2, d.p2, sy, T(0), &e);   // += K_y P
+    __syncthreads();
+    pass_ana<T, SEG>(A, B, rows_geom(d.F2, pitch), d.N1, d.p1);   // A_x: F1 -> G1
+    __syncthreads();
+    pass_ana<T, SEG>(B, A, cols_geom(d.G1, pitch), d.N2, d.p2);   // A_y: F2 -> G2
+    __syncthreads();
+    scatter_plane<T, TO>(A, pitch, L, kz, hpsi + o.psi, accumulate != 0);
+    const double s = block_sum(e, red);
+    if (threadIdx.x == 0) part_kin[(size_t)w.x * part_stride + slots[blockIdx.x]] = s;
+}
+
+// fixed-order per-orbital sum of the energy partial slots
+__global__ void k_reduce_energies(const double *__restrict__ part_pot, const double *__restrict__ part_kin,
+                                  int part_stride, int norb, double *__restrict__ ekin, double *__restrict__ epot)
+{
+    __shared__ double red[32];
+    const int orb = blockIdx.x;
+    if (orb >= norb) return;
+    double a = 0.0, b = 0.0;
+    for (int i = threadIdx.x; i < part_stride; i += blockDim.x) {
+        a += part_kin[(size_t)orb * part_stride + i];
+        b += part_pot[(size_t)orb * part_stride + i];
+    }
+    const double sa = block_sum(a, red);
+    __syncthreads();
+    const double sb = block_sum(b, red);
+    if (threadIdx.x == 0) {
+        if (ekin) ekin[orb] = sa;
+        if (epot) epot[orb] = sb;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// host launchers
+template <class T, class TIO>
+cudaError_t launch_locham(const Plan &p, const TIO *psi, const TIO *pot, TIO *hpsi, T *scratch, double *part_pot,
+                          double *part_kin, double *ekin, double *epot, int accumulate, cudaStream_t st,
+                          cudaEvent_t *ev)
+{
+    const int fp = sizeof(T) == 8 ? 1 : 0;
+    const size_t sm13 = p.smem13[fp], sm2 = p.smem2[fp];
+    cudaError_t err;
+    err = cudaFuncSetAttribute(k1_plane_forward<T, TIO>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm13);
+    if (err != cudaSuccess) return err;
+    err = cudaFuncSetAttribute(k2_zpencil<T, TIO>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm2);
+    if (err != cudaSuccess) return err;
+    err = cudaFuncSetAttribute(k3_plane_backward<T, TIO>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm13);
+    if (err != cudaSuccess) return err;
+    cudaMemsetAsync(part_pot, 0, sizeof(double) * (size_t)p.norb * p.part_stride, st);
+    cudaMemsetAsync(part_kin, 0, sizeof(double) * (size_t)p.norb * p.part_stride, st);
+    // optional per-kernel timing: ev[0..4] bracket K1, K2, K3 and the reduction
+    if (ev) cudaEventRecord(ev[0], st);
+    k1_plane_forward<T, TIO><<<p.n_work13, 256, sm13, st>>>(p.d_lr, p.d_orb, p.d_work13, psi, scratch);
+    if (ev) cudaEventRecord(ev[1], st);
+    k2_zpencil<T, TIO><<<p.n_work2, 256, sm2, st>>>(p.d_lr, p.d_orb, p.d_work2, p.d_part_slot2, pot, scratch,
+                                                    part_pot, part_kin, p.part_stride);
+    if (ev) cudaEventRecord(ev[2], st);
+    k3_plane_backward<T, TIO><<<p.n_work13, 256, sm13, st>>>(p.d_lr, p.d_orb, p.d_work13, p.d_part_slot13, scratch,
+                                                             hpsi, part_kin, p.part_stride, accumulate);
+    if (ev) cudaEventRecord(ev[3], st);
+    k_reduce_energies<<<p.norb, 128, 0, st>>>(part_pot, part_kin, p.part_stride, p.norb, ekin, epot);
+    if (ev) cudaEventRecord(ev[4], st);
+    return cudaGetLastError();
+}
+
+template cudaError_t launch_locham<float, float>(const Plan &, const float *, const float *, float *, float *,
+                                                 double *, double *, double *, double *, int, cudaStream_t,
+                                                 cudaEvent_t *);
+template cudaError_t launch_locham<double, double>(const Plan &, const double *, const double *, double *, double *,
+                                                   double *, double *, double *, double *, int, cudaStream_t,
+                                                   cudaEvent_t *);
+
+// FP32/FP64 FMA throughput probe: independent FMA chains held in registers.
+template <class T>
+__global__ void __launch_bounds__(256) k_fma_probe(T *out, int iters, T a, T b)
+{
+    T x[16];
+#pragma unroll
+    for (int k = 0; k < 16; ++k) x[k] = T(threadIdx.x + k) * T(1e-3);
+    for (int i = 0; i < iters; ++i) {
+#pragma unroll
+        for (int k = 0; k < 16; ++k) x[k] = fma(x[k], a, b);
+    }
+    T s = T(0);
+#pragma unroll
+    for (int k = 0; k < 16; ++k) s += x[k];
+    if (s == T(12345.678)) out[blockIdx.x] = s;  // keep the chains alive
+}
+
+cudaError_t fma_probe(int precision, int iters, float *ms, double *flops, cudaStream_t st)
+{
+    int dev = 0, nsm = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    const int blocks = nsm * 8;
+    void *buf = nullptr;
+    cudaError_t e = cudaMalloc(&buf, 8 * (size_t)blocks);
+    if (e) return e;
+    cudaEvent_t a, b;
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+    for (int rep = 0; rep < 2; ++rep) {  // first launch warms up
+        cudaEventRecord(a, st);
+        if (precision == 64) k_fma_probe<double><<<blocks, 256, 0, st>>>((double *)buf, iters, 0.999999, 1e-7);
+        else k_fma_probe<float><<<blocks, 256, 0, st>>>((float *)buf, iters, 0.999999f, 1e-7f);
+        cudaEventRecord(b, st);
+    }
+    cudaEventSynchronize(b);
+    cudaEventElapsedTime(ms, a, b);
+    *flops = 2.0 * 16.0 * (double)iters * 256.0 * blocks;
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    cudaFree(buf);
+    return cudaGetLastError();
+}
+
+}  // namespace wvlh

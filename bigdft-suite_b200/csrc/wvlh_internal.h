@@ -1,0 +1,68 @@
+// Internal host/device structures of the wvlh library (not part of the C ABI).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+#include <vector>
+
+namespace wvlh {
+
+// z-kernel tile: TX_ consecutive x by TY_ rows of columns
+constexpr int TX_ = 32;
+constexpr int TY_ = 2;
+
+// One localisation region (box + compressed-key tables) as seen by kernels.
+// Segments are decoded once on upload from the reference's 1-based keyg/keyv
+// (wavelib/un-compress.f90:896-905 arithmetic) into {i0, i2, len, jj0}, with
+// jj0 the 0-based compressed position; plane_c/plane_f[i3..i3+1] delimit the
+// segments of coarse z-plane i3 (keys are sorted by linear index).
+struct LrDev {
+    int N[3];
+    int per[3];
+    int nseg_c, nseg_f;
+    int nvctr_c, nvctr_f;
+    const int4 *seg_c;
+    const int4 *seg_f;
+    const int *plane_c;  // N3+1 entries
+    const int *plane_f;  // N3+1 entries
+    double hgrid[3];     // coarse grid spacing
+};
+
+// One orbital job of a batch.
+struct OrbDev {
+    int lr;
+    int pad;
+    long long psi;   // element offset of [psi_c | psi_f] in the psi/hpsi arrays
+    long long pot;   // element offset of this orbital's potential (ISF grid)
+    long long sP;    // scratch element offsets: P (G3*F2*F1)
+    long long sQ;    //   Q / Z1 (G3*I2*I1)
+    long long sZ;    //   Z2 (G3*F2*F1)
+    double c;        // shift of (T + c), preconditioner only
+};
+
+// Host view of an uploaded batch (plan) — owned by the context.
+struct Plan {
+    int nlr = 0, norb = 0;
+    std::vector<int> lr_N;  // 3*nlr
+    std::vector<int> lr_per;
+    std::vector<int> orb_lr;
+    std::vector<long long> orb_psi;  // element offsets
+    long long psi_total = 0;
+    long long scratch_elems = 0;     // per "chunk" of all orbitals (full batch)
+    // device tables
+    LrDev *d_lr = nullptr;
+    OrbDev *d_orb = nullptr;
+    int2 *d_work13 = nullptr;  // (orb, kz) for the plane kernels
+    int4 *d_work2 = nullptr;   // (orb, chain, x0, y0) for the z kernel
+    int n_work13 = 0, n_work2 = 0;
+    int *d_part_slot13 = nullptr;  // slot of each plane CTA in the energy partials
+    int *d_part_slot2 = nullptr;
+    int part_stride = 0;           // energy partial slots per orbital
+    size_t smem13[2] = {0, 0};     // dynamic smem bytes (float, double)
+    size_t smem2[2] = {0, 0};
+    int pitch_max = 0, rows_max = 0, zlen_max = 0;
+    std::vector<void *> owned;     // device allocations to free
+};
+
+}  // namespace wvlh

@@ -1,0 +1,152 @@
+"""Batched local Hamiltonian over many orbitals and localisation regions.
+
+The batch is the B200 form of the reference's orbital loop
+(``LocalHamiltonianApplication``, ``bigdft/src/hpsiortho.f90:934-958``: for
+each locreg, for each orbital, ``local_hamiltonian_ket``): all orbitals of all
+regions go through one fused three-kernel launch sequence.  Coefficients of
+orbital ``o`` are packed ``[psi_c | psi_f]`` (``nvctr_c + 7*nvctr_f`` values,
+the reference's ``psi(nvctr_c+7*nvctr_f, norb)`` layout) starting at
+``Batch.psi_offset(o)``; the potential of orbital ``o`` is an ISF grid (x
+fastest) starting at ``pot_offset[o]``.
+"""
+import ctypes as C
+
+import numpy as np
+
+from ._lib import LocregDesc, WvlhError, check, lib, require_cuda
+
+
+def _ptr(t):
+    return C.c_void_p(t.data_ptr()) if t is not None else None
+
+
+class Context:
+    """One device, one stream (the torch current stream at creation by default)."""
+
+    def __init__(self, device=0, stream=None):
+        torch = require_cuda()
+        self.torch = torch
+        self.device = device
+        h = C.c_void_p()
+        check(lib().wvlh_ctx_create(device, C.byref(h)), "wvlh_ctx_create")
+        self.h = h
+        s = stream if stream is not None else torch.cuda.current_stream(device)
+        self.set_stream(s)
+
+    def set_stream(self, stream):
+        self.stream = stream
+        check(lib().wvlh_ctx_set_stream(self.h, C.c_void_p(stream.cuda_stream)), "wvlh_ctx_set_stream")
+
+    def synchronize(self):
+        check(lib().wvlh_ctx_synchronize(self.h), "wvlh_ctx_synchronize")
+
+    def close(self):
+        if self.h:
+            lib().wvlh_ctx_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Batch:
+    def __init__(self, ctx, locregs, orb_lr, pot_offset=None):
+        self.ctx = ctx
+        self.locregs = list(locregs)
+        self.orb_lr = np.ascontiguousarray(orb_lr, np.int32)
+        self.norb = len(self.orb_lr)
+        descs = (LocregDesc * len(self.locregs))()
+        self._keep = []
+        for i, L in enumerate(self.locregs):
+            d = descs[i]
+            d.n[:] = list(L.n)
+            d.periodic[:] = list(L.periodic)
+            d.hgrid[:] = list(L.hgrid)
+            d.nseg_c, d.nseg_f = len(L.keyv_c), len(L.keyv_f)
+            for nm in ("keyg_c", "keyv_c", "keyg_f", "keyv_f"):
+                arr = np.ascontiguousarray(getattr(L, nm), np.int32)
+                self._keep.append(arr)
+                setattr(d, nm, arr.ctypes.data_as(C.POINTER(C.c_int32)))
+        if pot_offset is None:
+            po = None
+            self.pot_offset = np.zeros(self.norb, np.int64)
+        else:
+            self.pot_offset = np.ascontiguousarray(pot_offset, np.int64)
+            po = self.pot_offset.ctypes.data_as(C.POINTER(C.c_int64))
+        h = C.c_void_p()
+        rc = lib().wvlh_batch_create(ctx.h, len(self.locregs), descs, self.norb,
+                                     self.orb_lr.ctypes.data_as(C.POINTER(C.c_int32)), po, C.byref(h))
+        check(rc, "wvlh_batch_create")
+        self.h = h
+        self.psi_size = int(lib().wvlh_batch_psi_size(h))
+        self.offsets = np.array([lib().wvlh_batch_psi_offset(h, o) for o in range(self.norb)], np.int64)
+
+    def psi_offset(self, o):
+        return int(self.offsets[o])
+
+    def scratch_bytes(self, precision):
+        return int(lib().wvlh_batch_scratch_bytes(self.h, precision))
+
+    @property
+    def pot_size(self):
+        return int(max(self.pot_offset[o] + self.locregs[self.orb_lr[o]].nisf for o in range(self.norb)))
+
+    @property
+    def coarse_cells(self):
+        return sum(self.locregs[l].coarse_cells for l in self.orb_lr)
+
+    def locham(self, psi, pot, hpsi=None, ekin=None, epot=None, accumulate=False):
+        """Device tensors; precision follows psi's dtype (float32 or float64)."""
+        torch = self.ctx.torch
+        prec = {torch.float32: 32, torch.float64: 64}.get(psi.dtype)
+        if prec is None or pot.dtype != psi.dtype:
+            raise WvlhError("psi and pot must both be float32 or float64")
+        if psi.numel() < self.psi_size or pot.numel() < self.pot_size:
+            raise WvlhError("psi/pot smaller than the batch layout")
+        if hpsi is None:
+            hpsi = torch.zeros_like(psi)
+        if ekin is None:
+            ekin = torch.empty(self.norb, dtype=torch.float64, device=psi.device)
+        if epot is None:
+            epot = torch.empty(self.norb, dtype=torch.float64, device=psi.device)
+        rc = lib().wvlh_locham_batched(self.h, prec, _ptr(psi), _ptr(pot), _ptr(hpsi), _ptr(ekin), _ptr(epot),
+                                       int(bool(accumulate)))
+        check(rc, "wvlh_locham_batched")
+        return hpsi, ekin, epot
+
+    def locham_host(self, psi, pot, hpsi, ekin, epot, precision):
+        """Host buffers (numpy arrays or CPU tensors, ideally pinned)."""
+        def addr(a):
+            return C.c_void_p(a.data_ptr() if hasattr(a, "data_ptr") else a.ctypes.data)
+        rc = lib().wvlh_locham_batched_host(self.h, precision, addr(psi), addr(pot), addr(hpsi), addr(ekin),
+                                            addr(epot))
+        check(rc, "wvlh_locham_batched_host")
+
+    def locham_plain(self, psi, pot, hpsi=None, ekin=None, epot=None):
+        """FP64, one kernel per 1D pass (the OpenCL backend's structure)."""
+        torch = self.ctx.torch
+        if psi.dtype != torch.float64 or pot.dtype != torch.float64:
+            raise WvlhError("the plain path is FP64")
+        if hpsi is None:
+            hpsi = torch.zeros_like(psi)
+        if ekin is None:
+            ekin = torch.empty(self.norb, dtype=torch.float64, device=psi.device)
+        if epot is None:
+            epot = torch.empty(self.norb, dtype=torch.float64, device=psi.device)
+        rc = lib().wvlh_locham_plain_batched(self.h, _ptr(psi), _ptr(pot), _ptr(hpsi), _ptr(ekin), _ptr(epot))
+        check(rc, "wvlh_locham_plain_batched")
+        return hpsi, ekin, epot
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().wvlh_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -1,0 +1,277 @@
+/*
+ * wvlh — B200-native Daubechies-16 wavelet local Hamiltonian.
+ *
+ * C ABI.  Two groups of entry points:
+ *
+ *  1. Drop-in replacements for the accelerator wrappers BigDFT's Fortran host
+ *     already calls (bigdft/src/OpenCL/OpenCL_wrappers.h, FC_FUNC_ mangling:
+ *     lower case + trailing underscore, every argument by pointer).  Buffers
+ *     (cl_mem) are opaque handles to device allocations owned by the caller,
+ *     exactly as in the reference (interface_ocl.f90:43-190 allocates, :196-260
+ *     frees).  Keys are device buffers of 1-based uint32 keyg(2,nseg)/keyv(nseg).
+ *     Errors never exit(): they are recorded on the queue (sticky) and in a
+ *     process-wide slot read by wvlh_get_last_error().  Only the Gamma point
+ *     (nspinor == 1) is supported by the *_k entry points; nspinor == 2 records
+ *     WVLH_ERR_UNSUPPORTED.
+ *
+ *  2. New batched entry points (wvlh_*): many orbitals and many localisation
+ *     regions per call, FP32 or FP64 compute, device pointers, returning an
+ *     int status (0 = success).
+ *
+ * All FP64 results match the reference's CPU convolutions within 1e-13
+ * relative L2; FP32 forms keep energies, densities and scalar products in FP64.
+ */
+#ifndef WVLH_H
+#define WVLH_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef uint32_t cl_uint;
+typedef int32_t cl_int;
+typedef double cl_double;
+typedef struct wvlh_mem *cl_mem;
+typedef struct wvlh_ocl_context *bigdft_context;
+typedef struct wvlh_ocl_queue *bigdft_command_queue;
+
+enum {
+    WVLH_OK = 0,
+    WVLH_ERR_CUDA = 1,
+    WVLH_ERR_ARG = 2,
+    WVLH_ERR_KEYS = 3,
+    WVLH_ERR_NOMEM = 4,
+    WVLH_ERR_UNSUPPORTED = 5,
+    WVLH_ERR_TOO_LARGE = 6
+};
+
+/* --------------------------------------------------------------------- */
+/* 1. drop-in OpenCL-wrapper ABI                                          */
+/* --------------------------------------------------------------------- */
+
+/* lifecycle: OpenCL_wrappers.h:309-381 */
+void ocl_create_context_(bigdft_context *context, const char *platform, const char *devices, cl_int *device_type,
+                         cl_uint *device_number);                                       /* :315 */
+void ocl_create_gpu_context_(bigdft_context *context, cl_uint *device_number);         /* :317 */
+void ocl_build_programs_(bigdft_context *context);                                     /* :313 */
+void ocl_create_command_queue_(bigdft_command_queue *command_queue, bigdft_context *context); /* :370 */
+void ocl_create_command_queue_id_(bigdft_command_queue *command_queue, bigdft_context *context,
+                                  cl_uint *index);                                     /* :372 */
+void ocl_create_read_buffer_(bigdft_context *context, cl_uint *size, cl_mem *buff_ptr);        /* :325 */
+void ocl_create_write_buffer_(bigdft_context *context, cl_uint *size, cl_mem *buff_ptr);       /* :338 */
+void ocl_create_read_write_buffer_(bigdft_context *context, cl_uint *size, cl_mem *buff_ptr);  /* :331 */
+void ocl_create_read_buffer_and_copy_(bigdft_context *context, cl_uint *size, void *host_ptr,
+                                      cl_mem *buff_ptr);                               /* :332 */
+void ocl_release_mem_object_(cl_mem *buff_ptr);                                         /* :340 */
+void ocl_enqueue_read_buffer_(bigdft_command_queue *command_queue, cl_mem *buffer, cl_uint *size,
+                              void *host_ptr);                                         /* :347 */
+void ocl_enqueue_write_buffer_(bigdft_command_queue *command_queue, cl_mem *buffer, cl_uint *size,
+                               const void *host_ptr);                                  /* :354 */
+void ocl_enqueue_read_buffer_async_(bigdft_command_queue *command_queue, cl_mem *buffer, cl_uint *size,
+                                    void *host_ptr);                                   /* :361 */
+void ocl_enqueue_write_buffer_async_(bigdft_command_queue *command_queue, cl_mem *buffer, cl_uint *size,
+                                     const void *host_ptr);                            /* :368 */
+void ocl_finish_(bigdft_command_queue *command_queue);                                  /* :374 */
+void ocl_enqueue_barrier_(bigdft_command_queue *command_queue);                         /* :377 */
+void ocl_clean_command_queue_(bigdft_command_queue *command_queue);                     /* :379 */
+void ocl_clean_(bigdft_context *context);                                               /* :381 */
+void init_event_list_(bigdft_context *context);                                         /* :309 */
+void print_event_list_(bigdft_context *context);                                        /* :311 */
+
+/* compress / uncompress: OpenCL_wrappers.h:814-905 (Uncompress.c:596-640) */
+void uncompress_d_(bigdft_command_queue *command_queue, cl_uint *dimensions, cl_uint *nseg_c, cl_uint *nvctr_c,
+                   cl_mem *keyg_c, cl_mem *keyv_c, cl_uint *nseg_f, cl_uint *nvctr_f, cl_mem *keyg_f,
+                   cl_mem *keyv_f, cl_mem *psi_c, cl_mem *psi_f, cl_mem *psi_out);          /* :814 */
+void compress_d_(bigdft_command_queue *command_queue, cl_uint *dimensions, cl_uint *nseg_c, cl_uint *nvctr_c,
+                 cl_mem *keyg_c, cl_mem *keyv_c, cl_uint *nseg_f, cl_uint *nvctr_f, cl_mem *keyg_f,
+                 cl_mem *keyv_f, cl_mem *psi_c, cl_mem *psi_f, cl_mem *psi);                /* :833 */
+void uncompress_scale_d_(bigdft_command_queue *command_queue, cl_uint *dimensions, cl_double *h, cl_double *c,
+                         cl_uint *nseg_c, cl_uint *nvctr_c, cl_mem *keyg_c, cl_mem *keyv_c, cl_uint *nseg_f,
+                         cl_uint *nvctr_f, cl_mem *keyg_f, cl_mem *keyv_f, cl_mem *psi_c, cl_mem *psi_f,
+                         cl_mem *psi_out);                                                 /* :864 */
+void compress_scale_d_(bigdft_command_queue *command_queue, cl_uint *dimensions, cl_double *h, cl_double *c,
+                       cl_uint *nseg_c, cl_uint *nvctr_c, cl_mem *keyg_c, cl_mem *keyv_c, cl_uint *nseg_f,
+                       cl_uint *nvctr_f, cl_mem *keyg_f, cl_mem *keyv_f, cl_mem *psi_c, cl_mem *psi_f,
+                       cl_mem *psi);                                                       /* :885 */
+void scale_psi_d_(bigdft_command_queue *command_queue, cl_uint *nvctr_c, cl_uint *nvctr_f, cl_double *h,
+                  cl_double *c, cl_mem *psi_c, cl_mem *psi_f);                               /* :846 */
+
+/* 1D rotated passes: OpenCL_wrappers.h:390-512, 619 */
+void syn1d_d_(bigdft_command_queue *command_queue, cl_uint *n, cl_uint *ndat, cl_mem *psi, cl_mem *out);      /* :431 */
+void syngrow1d_d_(bigdft_command_queue *command_queue, cl_uint *n, cl_uint *ndat, cl_mem *psi, cl_mem *out);  /* :439 */
+void ana1d_d_(bigdft_command_queue *command_queue, cl_uint *n, cl_uint *ndat, cl_mem *psi, cl_mem *out);      /* :390 */
+void anashrink1d_d_(bigdft_command_queue *command_queue, cl_uint *n, cl_uint *ndat, cl_mem *psi, cl_mem *out); /* :398 */
+void magicfilter1d_d_(bigdft_command_queue *command_queue, cl_uint *n, cl_uint *ndat, cl_mem *psi, cl_mem *out); /* :469 */
+void magicfiltergrow1d_d_(bigdft_command_queue *command_queue, cl_uint *n, cl_uint *ndat, cl_mem *psi,
+                          cl_mem *out);                                                    /* :477 */
+void magicfilter1d_t_d_(bigdft_command_queue *command_queue, cl_uint *n, cl_uint *ndat, cl_mem *psi,
+                        cl_mem *out);                                                      /* :485 */
+void magicfiltershrink1d_d_(bigdft_command_queue *command_queue, cl_uint *n, cl_uint *ndat, cl_mem *psi,
+                            cl_mem *out);                                                  /* :493 */
+void magicfilter1d_pot_d_(bigdft_command_queue *command_queue, cl_uint *n, cl_uint *ndat, cl_mem *psi,
+                          cl_mem *pot, cl_mem *out);                                       /* :512 */
+void kinetic1d_d_(bigdft_command_queue *command_queue, cl_uint *n, cl_uint *ndat, cl_double *h, cl_double *c,
+                  cl_mem *x, cl_mem *y, cl_mem *workx, cl_mem *worky, cl_double *ekin);    /* :619 */
+
+/* 3D operators: OpenCL_wrappers.h:419-574, 629-639, 1228-1229 */
+void syn_self_d_(bigdft_command_queue *command_queue, cl_uint *dimensions, cl_mem *psi, cl_mem *out);        /* :458 */
+void ana_self_d_(bigdft_command_queue *command_queue, cl_uint *dimensions, cl_mem *psi, cl_mem *out);        /* :421 */
+void syn_self_d_generic_(bigdft_command_queue *command_queue, cl_uint *dimensions, cl_uint *periodic,
+                         cl_mem *psi, cl_mem *out);                                        /* :460 */
+void ana_self_d_generic_(bigdft_command_queue *command_queue, cl_uint *dimensions, cl_uint *periodic,
+                         cl_mem *psi, cl_mem *out);                                        /* :423 */
+void syn_d_generic_(bigdft_command_queue *command_queue, cl_uint *dimensions, cl_uint *periodic, cl_mem *tmp,
+                    cl_mem *psi, cl_mem *out);                                             /* :456 */
+void ana_d_generic_(bigdft_command_queue *command_queue, cl_uint *dimensions, cl_uint *periodic, cl_mem *tmp,
+                    cl_mem *psi, cl_mem *out);                                             /* :419 */
+void magic_filter_3d_generic_(bigdft_command_queue *command_queue, cl_uint *dimensions, cl_uint *periodic,
+                              cl_mem *tmp, cl_mem *tmp_dot, cl_mem *psi, cl_mem *out);     /* :1229 */
+void magic_filter_t_3d_generic_(bigdft_command_queue *command_queue, cl_uint *dimensions, cl_uint *periodic,
+                                cl_mem *tmp, cl_mem *tmp_dot, cl_mem *psi, cl_mem *out);   /* :1228 */
+void potential_application_d_generic_(bigdft_command_queue *command_queue, cl_uint *dimensions,
+                                      cl_uint *periodic, cl_mem *tmp, cl_mem *tmp_dot, cl_mem *psi, cl_mem *out,
+                                      cl_mem *pot, cl_double *epot);                       /* :574 */
+void kinetic_d_generic_(bigdft_command_queue *command_queue, cl_uint *dimensions, cl_uint *periodic,
+                        cl_double *h, cl_mem *x, cl_mem *y, cl_mem *work_x, cl_mem *work_y);  /* :639 */
+void kinetic_d_(bigdft_command_queue *command_queue, cl_uint *dimensions, cl_double *h, cl_mem *x, cl_mem *y,
+                cl_mem *work_x, cl_mem *work_y);                                           /* :629 */
+void magicfilter_den_d_generic_(bigdft_command_queue *command_queue, cl_uint *dimensions, cl_uint *periodic,
+                                cl_mem *tmp, cl_mem *psi, cl_mem *out);                    /* :542 */
+
+/* BLAS-1 with FP64 reductions: OpenCL_wrappers.h:663-767 */
+void dot_d_(bigdft_command_queue *command_queue, cl_uint *n, cl_mem *x, cl_mem *y, cl_mem *work1, cl_mem *work2,
+            cl_double *out);                                                              /* :718 */
+void dot_d_async_(bigdft_command_queue *command_queue, cl_uint *n, cl_mem *x, cl_mem *y, cl_mem *work1,
+                  cl_mem *work2, cl_double *out);                                         /* :728 */
+void nrm2sq_d_(bigdft_command_queue *command_queue, cl_uint *n, cl_mem *in, cl_mem *work1, cl_mem *work2,
+               cl_double *out);                                                           /* :674 */
+void axpy_d_(bigdft_command_queue *command_queue, cl_uint *n, cl_double *alpha, cl_mem *x, cl_mem *y,
+             cl_mem *z);                                                                  /* :685 */
+void axpy_self_d_(bigdft_command_queue *command_queue, cl_uint *n, cl_double *alpha, cl_mem *x, cl_mem *y); /* :693 */
+void scal_d_(bigdft_command_queue *command_queue, cl_uint *n, cl_double *alpha, cl_mem *x, cl_mem *y);      /* :701 */
+void scal_self_d_(bigdft_command_queue *command_queue, cl_uint *n, cl_double *alpha, cl_mem *x);            /* :708 */
+void copy_d_(bigdft_command_queue *command_queue, cl_uint *n, cl_mem *x, cl_mem *y);                        /* :742 */
+void set_d_(bigdft_command_queue *command_queue, cl_uint *n, cl_double *value, cl_mem *x);                  /* :735 */
+
+/* compositions: OpenCL/Hamiltonian.c:41-172, Density.c:37-55, Preconditioner.c:130-360 */
+void ocl_fulllocham_generic_(bigdft_command_queue *command_queue, cl_uint *dimensions, cl_uint *periodic,
+                             cl_double *h, cl_uint *nseg_c, cl_uint *nvctr_c, cl_mem *keyg_c, cl_mem *keyv_c,
+                             cl_uint *nseg_f, cl_uint *nvctr_f, cl_mem *keyg_f, cl_mem *keyv_f, cl_mem *psi_c,
+                             cl_mem *psi_f, cl_mem *pot, cl_mem *psi, cl_mem *out, cl_mem *work, cl_mem *kinres,
+                             cl_double *epot, cl_double *ekinpot);                          /* Hamiltonian.c:41 */
+void ocl_fulllocham_generic_k_(bigdft_command_queue *command_queue, cl_uint *dimensions, cl_uint *periodic,
+                               cl_double *h, cl_double *k, cl_uint *nseg_c, cl_uint *nvctr_c, cl_mem *keyg_c,
+                               cl_mem *keyv_c, cl_uint *nseg_f, cl_uint *nvctr_f, cl_mem *keyg_f, cl_mem *keyv_f,
+                               cl_mem *psi_c_r, cl_mem *psi_f_r, cl_mem *psi_c_i, cl_mem *psi_f_i, cl_mem *pot,
+                               cl_mem *psi_r, cl_mem *out_r, cl_mem *work_r, cl_mem *psi_i, cl_mem *out_i,
+                               cl_mem *work_i, cl_mem *kinres_r, cl_mem *kinres_i, cl_uint *nspinor,
+                               cl_double *epot, cl_double *ekinpot);                        /* Hamiltonian.c:105 */
+void ocl_daub_to_isf_(bigdft_command_queue *command_queue, cl_uint *dimensions, cl_uint *periodic,
+                      cl_uint *nseg_c, cl_uint *nvctr_c, cl_mem *keyg_c, cl_mem *keyv_c, cl_uint *nseg_f,
+                      cl_uint *nvctr_f, cl_mem *keyg_f, cl_mem *keyv_f, cl_mem *psi_c, cl_mem *psi_f,
+                      cl_mem *psi, cl_mem *out, cl_mem *work, cl_mem *kinres);              /* Hamiltonian.c:89 */
+void ocl_isf_to_daub_(bigdft_command_queue *command_queue, cl_uint *dimensions, cl_uint *periodic,
+                      cl_uint *nseg_c, cl_uint *nvctr_c, cl_mem *keyg_c, cl_mem *keyv_c, cl_uint *nseg_f,
+                      cl_uint *nvctr_f, cl_mem *keyg_f, cl_mem *keyv_f, cl_mem *psi_c, cl_mem *psi_f,
+                      cl_mem *psi, cl_mem *out, cl_mem *work, cl_mem *kinres);              /* Hamiltonian.c:74 */
+void ocl_locden_generic_(bigdft_command_queue *command_queue, cl_uint *dimensions, cl_uint *periodic,
+                         cl_double *hfac, cl_uint *nseg_c, cl_uint *nvctr_c, cl_mem *keyg_c, cl_mem *keyv_c,
+                         cl_uint *nseg_f, cl_uint *nvctr_f, cl_mem *keyg_f, cl_mem *keyv_f, cl_mem *psi_c,
+                         cl_mem *psi_f, cl_mem *psi, cl_mem *out, cl_mem *work, cl_mem *pot); /* Density.c:37 */
+void ocl_preconditioner_generic_(bigdft_command_queue *command_queue, cl_uint *dimensions, cl_uint *periodic,
+                                 cl_double *h, cl_double *c, cl_uint *ncong, cl_uint *nseg_c, cl_uint *nvctr_c,
+                                 cl_mem *keyg_c, cl_mem *keyv_c, cl_uint *nseg_f, cl_uint *nvctr_f,
+                                 cl_mem *keyg_f, cl_mem *keyv_f, cl_mem *psi_c, cl_mem *psi_f, cl_mem *psi_c_r,
+                                 cl_mem *psi_f_r, cl_mem *psi_c_b, cl_mem *psi_f_b, cl_mem *psi_c_d,
+                                 cl_mem *psi_f_d, cl_mem *work1, cl_mem *work2, cl_mem *work3,
+                                 cl_mem *work4);                                           /* Preconditioner.c:130 */
+void ocl_preconditioner_generic_k_(bigdft_command_queue *command_queue, cl_uint *dimensions, cl_uint *periodic,
+                                   cl_double *h, cl_double *k, cl_double *c, cl_uint *ncong, cl_uint *nseg_c,
+                                   cl_uint *nvctr_c, cl_mem *keyg_c, cl_mem *keyv_c, cl_uint *nseg_f,
+                                   cl_uint *nvctr_f, cl_mem *keyg_f, cl_mem *keyv_f, cl_mem *psi_c_r,
+                                   cl_mem *psi_f_r, cl_mem *psi_c_i, cl_mem *psi_f_i, cl_mem *psi_c_r_r,
+                                   cl_mem *psi_f_r_r, cl_mem *psi_c_r_i, cl_mem *psi_f_r_i, cl_mem *psi_c_b_r,
+                                   cl_mem *psi_f_b_r, cl_mem *psi_c_b_i, cl_mem *psi_f_b_i, cl_mem *psi_c_d_r,
+                                   cl_mem *psi_f_d_r, cl_mem *psi_c_d_i, cl_mem *psi_f_d_i, cl_mem *work1_r,
+                                   cl_mem *work2_r, cl_mem *work3_r, cl_mem *work4_r, cl_mem *work1_i,
+                                   cl_mem *work2_i, cl_mem *work3_i, cl_mem *work4_i, cl_uint *nspinor,
+                                   cl_double *norm_sq_cf);                                 /* Preconditioner.c:247 */
+
+/* last error recorded by any entry point of the process, then reset to 0
+ * (no counterpart in the reference, which exits on error) */
+int wvlh_get_last_error(void);
+const char *wvlh_error_string(int code);
+/* device pointer of a buffer handle (for interoperability and tests) */
+void *wvlh_mem_ptr(cl_mem mem);
+
+/* --------------------------------------------------------------------- */
+/* 2. batched ABI (new)                                                   */
+/* --------------------------------------------------------------------- */
+typedef struct wvlh_ctx wvlh_ctx;
+typedef struct wvlh_batch wvlh_batch;
+
+/* One localisation region: coarse cells per dimension (n1+1, n2+1, n3+1),
+ * periodicity, coarse grid spacing and the reference's 1-based keys (HOST
+ * arrays, keyg(2,nseg) / keyv(nseg), wavelib compression.f90:29-39). */
+typedef struct {
+    int n[3];
+    int periodic[3];
+    double hgrid[3];
+    int nseg_c, nseg_f;
+    const int32_t *keyg_c, *keyv_c;
+    const int32_t *keyg_f, *keyv_f;
+} wvlh_locreg;
+
+int wvlh_ctx_create(int device, wvlh_ctx **ctx);
+int wvlh_ctx_destroy(wvlh_ctx *ctx);
+/* stream (cudaStream_t) all calls of this context are issued on; 0 = legacy */
+int wvlh_ctx_set_stream(wvlh_ctx *ctx, void *stream);
+int wvlh_ctx_synchronize(wvlh_ctx *ctx);
+
+/* Validate and upload the keys of nlr regions and lay out norb orbitals:
+ * orbital o lives in region orb_lr[o]; its coefficients [psi_c | psi_f]
+ * start at wvlh_batch_psi_offset(o) (orbitals packed in order); its local
+ * potential / density grid (ISF points, x fastest) starts at element
+ * pot_offset[o] of the pot/rho arrays (NULL: all orbitals at offset 0). */
+int wvlh_batch_create(wvlh_ctx *ctx, int nlr, const wvlh_locreg *lrs, int norb, const int32_t *orb_lr,
+                      const int64_t *pot_offset, wvlh_batch **batch);
+int wvlh_batch_destroy(wvlh_batch *batch);
+int64_t wvlh_batch_psi_size(const wvlh_batch *batch);    /* total coefficient count */
+int64_t wvlh_batch_psi_offset(const wvlh_batch *batch, int orb);
+int64_t wvlh_batch_scratch_bytes(const wvlh_batch *batch, int precision);
+
+/* Hpsi for all orbitals of the batch.  precision 32: psi/pot/hpsi are float,
+ * 64: double.  Device pointers.  ekin/epot: device arrays of norb doubles
+ * (<psi|T|psi> and <psi|V|psi> per orbital, the reference's per-orbital ekin
+ * and epot of local_hamiltonian_ket).  accumulate != 0 adds into hpsi like
+ * compress_and_accumulate_mixed; 0 overwrites like compress_d. */
+int wvlh_locham_batched(wvlh_batch *batch, int precision, const void *psi, const void *pot, void *hpsi,
+                        double *ekin, double *epot, int accumulate);
+/* same with HOST buffers: copies in, computes, copies out, synchronises */
+int wvlh_locham_batched_host(wvlh_batch *batch, int precision, const void *psi, const void *pot, void *hpsi,
+                             double *ekin, double *epot);
+/* FP64, one kernel per 1D pass (the OpenCL backend's structure) */
+int wvlh_locham_plain_batched(wvlh_batch *batch, const double *psi, const double *pot, double *hpsi,
+                              double *ekin, double *epot);
+
+/* Optional per-kernel timing with CUDA events recorded on the context's
+ * stream around the fused kernels (K1 plane-forward, K2 z-pencil, K3
+ * plane-backward, energy reduction).  While on, each wvlh_locham_batched call
+ * waits for its own events; times accumulate until re-enabled. */
+int wvlh_ctx_enable_timing(wvlh_ctx *ctx, int on);
+int wvlh_ctx_kernel_times(wvlh_ctx *ctx, double *ms4, long long *ncalls);
+/* FMA-pipe throughput of this GPU (TFLOP/s) from a register-resident FMA
+ * chain kernel, the compute roof of the fused stencils (precision 32 or 64). */
+int wvlh_measure_fma_peak(int precision, int iters, double *tflops);
+
+/* pinned host memory helpers */
+void *wvlh_host_alloc(size_t bytes);
+void wvlh_host_free(void *p);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
