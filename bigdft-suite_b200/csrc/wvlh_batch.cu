@@ -298,6 +298,8 @@ extern "C" int wvlh_batch_create(wvlh_ctx *ctx, int nlr, const wvlh_locreg *lrs,
         sm2_elems = std::max(sm2_elems, (size_t)2 * zl * TX_ * TY_);
     }
     p.psi_total = psi_off;
+    p.all_periodic = true;
+    for (int v : p.lr_per) p.all_periodic = p.all_periodic && v == 1;
     p.scratch_elems = scr;
     p.part_stride = stride;
     p.smem13[0] = sm13_elems * sizeof(float);

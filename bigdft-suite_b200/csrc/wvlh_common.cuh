@@ -24,9 +24,12 @@
 //
 // FP32 energies: E_kin is accumulated in FP64 from the FP32 stencil result
 // with the FP64 scale -1/(2h^2) and a low-order correction for the rounding of
-// the five largest kinetic taps to FP32 (tap = hi + lo, lo applied to the
-// already formed pair sums), which removes the systematic O(1e-8) relative
-// bias that FP32 constants would put on the energy.
+// the six largest kinetic taps to FP32 (tap = hi + lo, lo applied to the
+// already formed pair sums).  The synthesis and forward magic-filter passes,
+// whose outputs feed E_kin and E_pot, start each FMA chain from the low-order
+// parts of their largest taps, so the expectation of every rounded output
+// carries the FP64 tap values.  Together these remove the systematic O(1e-8)
+// relative bias that FP32-rounded constants put on the energies.
 #pragma once
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -40,12 +43,18 @@ template <class T> struct Filt {
     static __device__ __forceinline__ constexpr T cg(int i) { return (T)(WVL_CG_AT(i)); }
     static __device__ __forceinline__ constexpr T mf(int i) { return (T)(WVL_MF_AT(i)); }
     static __device__ __forceinline__ constexpr T kin(int i) { return (T)(WVL_KIN_AT(i)); }
-    // residual of the T-rounded kinetic tap (zero in FP64)
+    // residuals of the T-rounded taps (zero in FP64)
     static __device__ __forceinline__ constexpr T kin_lo(int i)
     {
         return (T)((WVL_KIN_AT(i)) - (double)(T)(WVL_KIN_AT(i)));
     }
+    static __device__ __forceinline__ constexpr T ch_lo(int i) { return (T)((WVL_CH_AT(i)) - (double)(T)(WVL_CH_AT(i))); }
+    static __device__ __forceinline__ constexpr T cg_lo(int i) { return (T)((WVL_CG_AT(i)) - (double)(T)(WVL_CG_AT(i))); }
+    static __device__ __forceinline__ constexpr T mf_lo(int i) { return (T)((WVL_MF_AT(i)) - (double)(T)(WVL_MF_AT(i))); }
 };
+
+// taps whose FP32 rounding residual is carried (see the header comment)
+__host__ __device__ constexpr bool big_tap(double v, double thr) { return v > thr || v < -thr; }
 
 // Fine-grid and ISF-grid extents of one dimension with N coarse cells.
 __host__ __device__ __forceinline__ int fine_len(int N, int per) { return per ? 2 * N : 2 * N + 14; }
@@ -123,6 +132,16 @@ __device__ void pass_syn(const T *src, T *dst, const LineGeom g, int N, int per)
             const int o = t & 1;
             const int ic = t / 2 + 4;  // window index of coarse position i0 + t/2
             T acc = T(0);
+            if constexpr (sizeof(T) == 4) {
+                // low-order parts of the largest taps (|c| > 0.04) seed the FMA chain
+#pragma unroll
+                for (int l = -4; l <= 4; ++l) {
+                    const int m = 2 * l + o;
+                    if (m < -7 || m > 8) continue;
+                    if (big_tap(WVL_CH_AT(m + 7), 0.04)) acc = fma(Filt<T>::ch_lo(m + 7), xs[ic - l], acc);
+                    if (big_tap(WVL_CG_AT(m + 7), 0.04)) acc = fma(Filt<T>::cg_lo(m + 7), xw[ic - l], acc);
+                }
+            }
 #pragma unroll
             for (int l = -4; l <= 4; ++l) {
                 const int m = 2 * l + o;  // ch_syn(m) = ch(m) for m in [-7,8]
@@ -188,6 +207,13 @@ __device__ void pass_mf(const T *src, T *dst, const LineGeom g, int Lin, int Lou
 #pragma unroll
         for (int t = 0; t < SEG; ++t) {
             T acc = T(0);
+            if constexpr (sizeof(T) == 4 && !rev) {
+                // forward magic filter feeds E_pot: seed with the residuals of
+                // its largest taps (|c| > 0.02)
+#pragma unroll
+                for (int k = 0; k < 16; ++k)
+                    if (big_tap(WVL_MF_AT(k), 0.02)) acc = fma(Filt<T>::mf_lo(k), x[t + k], acc);
+            }
 #pragma unroll
             for (int k = 0; k < 16; ++k) acc = fma(Filt<T>::mf(rev ? 15 - k : k), x[t + k], acc);
             const int q = q0 + t;
@@ -214,6 +240,9 @@ __device__ void pass_kin(const T *src, T *dst, const LineGeom g, int L, int per,
         const int q0 = s * SEG;
         T x[W];
         load_window<T, W>(x, in, g.src_ps, q0 - 14, L, per);
+        // per-segment partial sums of x.conv (and of x.lo in FP32), converted
+        // to FP64 once per segment; the rounding of these short sums is unbiased
+        T es = T(0), el = T(0);
 #pragma unroll
         for (int t = 0; t < SEG; ++t) {
             T conv = Filt<T>::kin(0) * x[t + 14];
@@ -224,19 +253,18 @@ __device__ void pass_kin(const T *src, T *dst, const LineGeom g, int L, int per,
                 const T pr = x[t + 14 + l] + x[t + 14 - l];
                 conv = fma(Filt<T>::kin(l), pr, conv);
                 if constexpr (sizeof(T) == 4) {
-                    if (l <= 4) lo = fma(Filt<T>::kin_lo(l), pr, lo);
+                    if (l <= 5) lo = fma(Filt<T>::kin_lo(l), pr, lo);
                 }
             }
             const int q = q0 + t;
             if (q < L) {
-                if (ekin) {
-                    if constexpr (sizeof(T) == 4) e += (double)x[t + 14] * (((double)conv + (double)lo) * scale_d);
-                    else e += x[t + 14] * (conv * scale_d);
-                }
+                es = fma(x[t + 14], conv, es);
+                if constexpr (sizeof(T) == 4) el = fma(x[t + 14], lo, el);
                 const T base = ACC ? out[q * g.dst_ps] : cshift * x[t + 14];
                 out[q * g.dst_ps] = fma(scale, conv, base);
             }
         }
+        e += ((double)es + (double)el) * scale_d;
     });
     if (ekin) *ekin += e;
 }

@@ -33,10 +33,14 @@ template <> struct Seg<double> { static constexpr int v = 4; };
 struct Dims {
     int N1, N2, N3, p1, p2, p3;
     int G1, G2, G3, F1, F2, F3, I1, I2, I3;
-    __device__ __forceinline__ explicit Dims(const LrDev &L)
+    // allper: the batch is known to be periodic in every direction, which lets
+    // the compiler drop the free-boundary variants from the kernel
+    __device__ __forceinline__ Dims(const LrDev &L, bool allper)
     {
         N1 = L.N[0]; N2 = L.N[1]; N3 = L.N[2];
-        p1 = L.per[0]; p2 = L.per[1]; p3 = L.per[2];
+        p1 = allper ? 1 : L.per[0];
+        p2 = allper ? 1 : L.per[1];
+        p3 = allper ? 1 : L.per[2];
         G1 = 2 * N1; G2 = 2 * N2; G3 = 2 * N3;
         F1 = fine_len(N1, p1); F2 = fine_len(N2, p2); F3 = fine_len(N3, p3);
         I1 = isf_len(N1, p1); I2 = isf_len(N2, p2); I3 = isf_len(N3, p3);
@@ -152,16 +156,17 @@ __device__ __forceinline__ void load_plane(T *A, int pitch, int rows, int cols, 
 // ---------------------------------------------------------------------------
 // K1: compressed psi -> P = S_x S_y psi and Q = M_x M_y P for one z-plane.
 // TI is the storage type of psi (may differ from compute type T).
-template <class T, class TI>
-__global__ void __launch_bounds__(256) k1_plane_forward(const LrDev *__restrict__ lrs, const OrbDev *__restrict__ orbs,
-                                                        const int2 *__restrict__ work, const TI *__restrict__ psi,
-                                                        T *__restrict__ scratch)
+template <class T, class TI, bool ALLPER>
+__global__ void __launch_bounds__(kPlaneThreads) k1_plane_forward(const LrDev *__restrict__ lrs,
+                                                                  const OrbDev *__restrict__ orbs,
+                                                                  const int2 *__restrict__ work,
+                                                                  const TI *__restrict__ psi, T *__restrict__ scratch)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int2 w = work[blockIdx.x];
     const OrbDev o = orbs[w.x];
     const LrDev L = lrs[o.lr];
-    const Dims d(L);
+    const Dims d(L, ALLPER);
     const int kz = w.y;
     const int pitch = d.pitch();
     T *A = reinterpret_cast<T *>(smem_raw);
@@ -189,19 +194,19 @@ __global__ void __launch_bounds__(256) k1_plane_forward(const LrDev *__restrict_
 // ---------------------------------------------------------------------------
 // K2: z-pencil tiles.  chain 0: Z1 = A_z Mt_z (V . M_z S_z Q) in place of Q,
 // E_pot partial.  chain 1: Z2 = A_z K_z S_z P, E_kin(z) partial.
-template <class T, class TV>
-__global__ void __launch_bounds__(256) k2_zpencil(const LrDev *__restrict__ lrs, const OrbDev *__restrict__ orbs,
-                                                  const int4 *__restrict__ work, const int *__restrict__ slots,
-                                                  const TV *__restrict__ pot, T *__restrict__ scratch,
-                                                  double *__restrict__ part_pot, double *__restrict__ part_kin,
-                                                  int part_stride)
+template <class T, class TV, bool ALLPER>
+__global__ void __launch_bounds__(kZThreads) k2_zpencil(const LrDev *__restrict__ lrs, const OrbDev *__restrict__ orbs,
+                                                        const int4 *__restrict__ work, const int *__restrict__ slots,
+                                                        const TV *__restrict__ pot, T *__restrict__ scratch,
+                                                        double *__restrict__ part_pot, double *__restrict__ part_kin,
+                                                        int part_stride)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ double red[32];
     const int4 w = work[blockIdx.x];
     const OrbDev o = orbs[w.x];
     const LrDev L = lrs[o.lr];
-    const Dims d(L);
+    const Dims d(L, ALLPER);
     const int chain = w.y, x0 = w.z, y0 = w.w;
     const int zl = max(d.G3, max(d.F3, d.I3));
     T *A = reinterpret_cast<T *>(smem_raw);
@@ -228,20 +233,23 @@ __global__ void __launch_bounds__(256) k2_zpencil(const LrDev *__restrict__ lrs,
         if (d.p3) pass_mf<T, SEG, 0>(B, A, zg, d.F3, d.I3);       // M_z: F3 -> I3
         else pass_mf<T, SEG, 2>(B, A, zg, d.F3, d.I3);
         __syncthreads();
-        // psir <- V psir, epot += V psir^2 (orbitals/potential.f90:1011-1031)
+        // psir <- V psir, epot += V psir^2 (orbitals/potential.f90:1011-1031);
+        // per-thread partial sum in T, one FP64 conversion per thread
         const TV *V = pot + o.pot;
+        T ep = T(0);
         for (int i = threadIdx.x; i < d.I3 * TC; i += blockDim.x) {
             const int z = i / TC, c = i - z * TC;
             const int x = x0 + (c % TX), y = y0 + (c / TX);
             if (x < W && y < H) {
                 const T r = A[i];
                 const T wv = (T)V[((size_t)z * d.I2 + y) * d.I1 + x] * r;
-                e += (double)wv * (double)r;
+                ep = fma(wv, r, ep);
                 A[i] = wv;
             } else {
                 A[i] = T(0);
             }
         }
+        e += (double)ep;
         __syncthreads();
         if (d.p3) pass_mf<T, SEG, 1>(A, B, zg, d.I3, d.F3);       // Mt_z: I3 -> F3
         else pass_mf<T, SEG, 3>(A, B, zg, d.I3, d.F3);
@@ -267,18 +275,21 @@ __global__ void __launch_bounds__(256) k2_zpencil(const LrDev *__restrict__ lrs,
 
 // ---------------------------------------------------------------------------
 // K3: Hpsi plane kz = A_x A_y [Mt_x Mt_y Z1 + Z2 + (K_x + K_y) P]
-template <class T, class TO>
-__global__ void __launch_bounds__(256) k3_plane_backward(const LrDev *__restrict__ lrs, const OrbDev *__restrict__ orbs,
-                                                         const int2 *__restrict__ work, const int *__restrict__ slots,
-                                                         const T *__restrict__ scratch, TO *__restrict__ hpsi,
-                                                         double *__restrict__ part_kin, int part_stride, int accumulate)
+template <class T, class TO, bool ALLPER>
+__global__ void __launch_bounds__(kPlaneThreads) k3_plane_backward(const LrDev *__restrict__ lrs,
+                                                                   const OrbDev *__restrict__ orbs,
+                                                                   const int2 *__restrict__ work,
+                                                                   const int *__restrict__ slots,
+                                                                   const T *__restrict__ scratch, TO *__restrict__ hpsi,
+                                                                   double *__restrict__ part_kin, int part_stride,
+                                                                   int accumulate)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ double red[32];
     const int2 w = work[blockIdx.x];
     const OrbDev o = orbs[w.x];
     const LrDev L = lrs[o.lr];
-    const Dims d(L);
+    const Dims d(L, ALLPER);
     const int kz = w.y;
     const int pitch = d.pitch();
     T *A = reinterpret_cast<T *>(smem_raw);
@@ -342,35 +353,50 @@ __global__ void k_reduce_energies(const double *__restrict__ part_pot, const dou
 
 // ---------------------------------------------------------------------------
 // host launchers
-template <class T, class TIO>
-cudaError_t launch_locham(const Plan &p, const TIO *psi, const TIO *pot, TIO *hpsi, T *scratch, double *part_pot,
-                          double *part_kin, double *ekin, double *epot, int accumulate, cudaStream_t st,
-                          cudaEvent_t *ev)
+template <class T, class TIO, bool ALLPER>
+static cudaError_t launch_locham_bc(const Plan &p, const TIO *psi, const TIO *pot, TIO *hpsi, T *scratch,
+                                    double *part_pot, double *part_kin, double *ekin, double *epot, int accumulate,
+                                    cudaStream_t st, cudaEvent_t *ev)
 {
     const int fp = sizeof(T) == 8 ? 1 : 0;
     const size_t sm13 = p.smem13[fp], sm2 = p.smem2[fp];
     cudaError_t err;
-    err = cudaFuncSetAttribute(k1_plane_forward<T, TIO>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm13);
+    err = cudaFuncSetAttribute(k1_plane_forward<T, TIO, ALLPER>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)sm13);
     if (err != cudaSuccess) return err;
-    err = cudaFuncSetAttribute(k2_zpencil<T, TIO>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm2);
+    err = cudaFuncSetAttribute(k2_zpencil<T, TIO, ALLPER>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm2);
     if (err != cudaSuccess) return err;
-    err = cudaFuncSetAttribute(k3_plane_backward<T, TIO>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm13);
+    err = cudaFuncSetAttribute(k3_plane_backward<T, TIO, ALLPER>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)sm13);
     if (err != cudaSuccess) return err;
     cudaMemsetAsync(part_pot, 0, sizeof(double) * (size_t)p.norb * p.part_stride, st);
     cudaMemsetAsync(part_kin, 0, sizeof(double) * (size_t)p.norb * p.part_stride, st);
     // optional per-kernel timing: ev[0..4] bracket K1, K2, K3 and the reduction
     if (ev) cudaEventRecord(ev[0], st);
-    k1_plane_forward<T, TIO><<<p.n_work13, 256, sm13, st>>>(p.d_lr, p.d_orb, p.d_work13, psi, scratch);
+    k1_plane_forward<T, TIO, ALLPER><<<p.n_work13, kPlaneThreads, sm13, st>>>(p.d_lr, p.d_orb, p.d_work13, psi,
+                                                                             scratch);
     if (ev) cudaEventRecord(ev[1], st);
-    k2_zpencil<T, TIO><<<p.n_work2, 256, sm2, st>>>(p.d_lr, p.d_orb, p.d_work2, p.d_part_slot2, pot, scratch,
-                                                    part_pot, part_kin, p.part_stride);
+    k2_zpencil<T, TIO, ALLPER><<<p.n_work2, kZThreads, sm2, st>>>(p.d_lr, p.d_orb, p.d_work2, p.d_part_slot2, pot,
+                                                                 scratch, part_pot, part_kin, p.part_stride);
     if (ev) cudaEventRecord(ev[2], st);
-    k3_plane_backward<T, TIO><<<p.n_work13, 256, sm13, st>>>(p.d_lr, p.d_orb, p.d_work13, p.d_part_slot13, scratch,
-                                                             hpsi, part_kin, p.part_stride, accumulate);
+    k3_plane_backward<T, TIO, ALLPER><<<p.n_work13, kPlaneThreads, sm13, st>>>(
+        p.d_lr, p.d_orb, p.d_work13, p.d_part_slot13, scratch, hpsi, part_kin, p.part_stride, accumulate);
     if (ev) cudaEventRecord(ev[3], st);
     k_reduce_energies<<<p.norb, 128, 0, st>>>(part_pot, part_kin, p.part_stride, p.norb, ekin, epot);
     if (ev) cudaEventRecord(ev[4], st);
     return cudaGetLastError();
+}
+
+template <class T, class TIO>
+cudaError_t launch_locham(const Plan &p, const TIO *psi, const TIO *pot, TIO *hpsi, T *scratch, double *part_pot,
+                          double *part_kin, double *ekin, double *epot, int accumulate, cudaStream_t st,
+                          cudaEvent_t *ev)
+{
+    if (p.all_periodic)
+        return launch_locham_bc<T, TIO, true>(p, psi, pot, hpsi, scratch, part_pot, part_kin, ekin, epot,
+                                              accumulate, st, ev);
+    return launch_locham_bc<T, TIO, false>(p, psi, pot, hpsi, scratch, part_pot, part_kin, ekin, epot, accumulate,
+                                           st, ev);
 }
 
 template cudaError_t launch_locham<float, float>(const Plan &, const float *, const float *, float *, float *,

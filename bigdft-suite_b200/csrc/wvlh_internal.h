@@ -11,6 +11,10 @@ namespace wvlh {
 // z-kernel tile: TX_ consecutive x by TY_ rows of columns
 constexpr int TX_ = 32;
 constexpr int TY_ = 2;
+// block sizes of the plane kernels (K1, K3) and of the z-pencil kernel (K2);
+// 384 threads give 3 line-segment items per thread on 96-point planes
+constexpr int kPlaneThreads = 384;
+constexpr int kZThreads = 256;
 
 // One localisation region (box + compressed-key tables) as seen by kernels.
 // Segments are decoded once on upload from the reference's 1-based keyg/keyv
@@ -44,6 +48,7 @@ struct OrbDev {
 // Host view of an uploaded batch (plan) — owned by the context.
 struct Plan {
     int nlr = 0, norb = 0;
+    bool all_periodic = false;  // every region periodic in x, y and z
     std::vector<int> lr_N;  // 3*nlr
     std::vector<int> lr_per;
     std::vector<int> orb_lr;
