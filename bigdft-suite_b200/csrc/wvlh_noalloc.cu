@@ -1,0 +1,284 @@
+// Local Hamiltonian of one orbital without any device allocation.
+//
+// Some callers cannot call cudaMalloc at all: code running under a memory
+// manager that owns every device allocation (a host program whose allocator
+// hands out one fixed pool, or a runtime that forbids allocation once it has
+// started capturing work), and library layers that must not grow the device
+// footprint behind their host's back.  For them this file gives one entry
+// point that runs the same fused kernels as wvlh_locham_batched, with every
+// table and all of its scratch (the P, Q/Z1 and Z2 planes and the energy
+// partials) carved out of a file-scope static device array of fixed size.
+// The caller passes only its own inputs and outputs.
+#include <cuda_runtime.h>
+
+#include <mutex>
+
+#include "../../include/wvlh.h"
+#include "wvlh_common.cuh"
+#include "wvlh_internal.h"
+
+namespace wvlh {
+template <class T, class TIO>
+cudaError_t launch_locham(const Plan &p, const TIO *psi, const TIO *pot, TIO *hpsi, T *scratch, double *part_pot,
+                          double *part_kin, double *ekin, double *epot, int accumulate, cudaStream_t st,
+                          cudaEvent_t *ev);
+void set_last_error(int code);
+}  // namespace wvlh
+
+using namespace wvlh;
+
+// The static scratch: 64 MiB on every device the entry point is used on, held
+// until the process exits.  Host code never dereferences this symbol: its
+// address on the current device is obtained with cudaGetSymbolAddress.
+constexpr size_t kNoAllocBytes = size_t(64) << 20;
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
+
+namespace {
+
+constexpr int kMaxDevices = 64;
+std::mutex g_setup_mutex;
+void *g_scratch_addr[kMaxDevices] = {nullptr};
+
+// decoded segment {i0, i2, len, jj0} from 1-based keys (un-compress.f90:896-905)
+__global__ void k_decode_segments(int n1, int n2, int nseg, const int32_t *__restrict__ keyg,
+                                  const int32_t *__restrict__ keyv, int4 *__restrict__ seg)
+{
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= nseg) return;
+    const int j0 = keyg[2 * s], j1 = keyg[2 * s + 1];
+    int ii = j0 - 1;
+    const int i3 = ii / (n1 * n2);
+    ii -= i3 * n1 * n2;
+    const int i2 = ii / n1;
+    seg[s] = make_int4(ii - i2 * n1, i2, j1 - j0 + 1, keyv[s] - 1);
+}
+
+// first segment of each coarse z-plane (keys are sorted by linear index)
+__global__ void k_plane_ranges(int n12, int n3, int nseg, const int32_t *__restrict__ keyg, int *__restrict__ plane)
+{
+    const int i3 = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i3 > n3) return;
+    int lo = 0, hi = nseg;  // first s with (keyg[2s]-1)/n12 >= i3
+    while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        if ((keyg[2 * mid] - 1) / n12 < i3) lo = mid + 1; else hi = mid;
+    }
+    plane[i3] = lo;
+}
+
+// work lists of one orbital: plane kernels (kz) and z-pencil tiles
+__global__ void k_work_lists(int G3, int ntx0, int nty0, int ntx1, int nty1, int2 *w13, int *s13, int4 *w2, int *s2)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int n0 = ntx0 * nty0, n1 = ntx1 * nty1;
+    if (i < G3) {
+        w13[i] = make_int2(0, i);
+        s13[i] = n1 + i;
+    }
+    if (i < n0) {
+        w2[i] = make_int4(0, 0, (i % ntx0) * TX_, (i / ntx0) * TY_);
+        s2[i] = i;
+    } else if (i < n0 + n1) {
+        const int k = i - n0;
+        w2[i] = make_int4(0, 1, (k % ntx1) * TX_, (k / ntx1) * TY_);
+        s2[i] = k;
+    }
+}
+
+inline size_t up256(size_t b) { return (b + 255) & ~size_t(255); }
+
+// host-side validation of the reference's keys, without allocating
+int check_keys(const int *N, int nseg, const int32_t *keyg, const int32_t *keyv)
+{
+    const long long n12 = (long long)N[0] * N[1], ntot = n12 * N[2];
+    long long prev = 0, cum = 0;
+    for (int s = 0; s < nseg; ++s) {
+        const long long j0 = keyg[2 * s], j1 = keyg[2 * s + 1];
+        if (j0 < 1 || j1 < j0 || j1 > ntot || j0 <= prev) return WVLH_ERR_KEYS;
+        if ((j0 - 1) / N[0] != (j1 - 1) / N[0]) return WVLH_ERR_KEYS;
+        if ((long long)keyv[s] != cum + 1) return WVLH_ERR_KEYS;
+        cum += j1 - j0 + 1;
+        prev = j1;
+    }
+    return WVLH_OK;
+}
+
+}  // namespace
+
+extern "C" size_t wvlh_noalloc_capacity(void) { return kNoAllocBytes; }
+
+extern "C" int wvlh_locham_noalloc(int precision, const int n[3], const int periodic[3], const double hgrid[3],
+                                   int nseg_c, const int32_t *keyg_c, const int32_t *keyv_c, int nseg_f,
+                                   const int32_t *keyg_f, const int32_t *keyv_f, const void *psi, const void *pot,
+                                   void *hpsi, double *ekin, double *epot, void *stream)
+{
+    if ((precision != 32 && precision != 64) || !n || !periodic || !hgrid || !psi || !pot || !hpsi || !ekin ||
+        !epot || nseg_c < 0 || nseg_f < 0 || (nseg_c && (!keyg_c || !keyv_c)) || (nseg_f && (!keyg_f || !keyv_f))) {
+        set_last_error(WVLH_ERR_ARG);
+        return WVLH_ERR_ARG;
+    }
+    int N[3], per[3];
+    for (int k = 0; k < 3; ++k) {
+        N[k] = n[k];
+        per[k] = periodic[k] ? 1 : 0;
+        if (N[k] < 1 || N[k] > 1024 || (per[k] && N[k] < 8)) {
+            set_last_error(WVLH_ERR_ARG);
+            return WVLH_ERR_ARG;
+        }
+    }
+    int rc = check_keys(N, nseg_c, keyg_c, keyv_c);
+    if (!rc) rc = check_keys(N, nseg_f, keyg_f, keyv_f);
+    if (rc) {
+        set_last_error(rc);
+        return rc;
+    }
+    const int G[3] = {2 * N[0], 2 * N[1], 2 * N[2]};
+    int F[3], I[3];
+    for (int k = 0; k < 3; ++k) {
+        F[k] = fine_len(N[k], per[k]);
+        I[k] = isf_len(N[k], per[k]);
+    }
+    const size_t es = precision == 32 ? 4 : 8;
+    const int ntx0 = (I[0] + TX_ - 1) / TX_, nty0 = (I[1] + TY_ - 1) / TY_;
+    const int ntx1 = (F[0] + TX_ - 1) / TX_, nty1 = (F[1] + TY_ - 1) / TY_;
+    const int nw2 = ntx0 * nty0 + ntx1 * nty1;
+    const int stride = (ntx0 * nty0 > ntx1 * nty1 + G[2]) ? ntx0 * nty0 : ntx1 * nty1 + G[2];
+    const long long sP = (long long)G[2] * F[1] * F[0], sQ = (long long)G[2] * I[1] * I[0];
+    // layout of the static array
+    size_t off = 0;
+    const size_t o_lr = off; off = up256(off + sizeof(LrDev));
+    const size_t o_orb = off; off = up256(off + sizeof(OrbDev));
+    const size_t o_kc = off; off = up256(off + 8 * (size_t)nseg_c + 4 * (size_t)nseg_c);
+    const size_t o_kf = off; off = up256(off + 8 * (size_t)nseg_f + 4 * (size_t)nseg_f);
+    const size_t o_sc = off; off = up256(off + 16 * (size_t)nseg_c);
+    const size_t o_sf = off; off = up256(off + 16 * (size_t)nseg_f);
+    const size_t o_pc = off; off = up256(off + 4 * (size_t)(N[2] + 1));
+    const size_t o_pf = off; off = up256(off + 4 * (size_t)(N[2] + 1));
+    const size_t o_w13 = off; off = up256(off + 8 * (size_t)G[2]);
+    const size_t o_s13 = off; off = up256(off + 4 * (size_t)G[2]);
+    const size_t o_w2 = off; off = up256(off + 16 * (size_t)nw2);
+    const size_t o_s2 = off; off = up256(off + 4 * (size_t)nw2);
+    const size_t o_pp = off; off = up256(off + 8 * (size_t)stride);
+    const size_t o_pk = off; off = up256(off + 8 * (size_t)stride);
+    const size_t o_scr = off; off = up256(off + es * (size_t)(2 * sP + sQ));
+    if (off > kNoAllocBytes) {
+        set_last_error(WVLH_ERR_TOO_LARGE);
+        return WVLH_ERR_TOO_LARGE;
+    }
+    const size_t pitch = (size_t)((G[0] > F[0] ? (G[0] > I[0] ? G[0] : I[0]) : (F[0] > I[0] ? F[0] : I[0])) | 1);
+    const size_t rows = (size_t)(G[1] > F[1] ? (G[1] > I[1] ? G[1] : I[1]) : (F[1] > I[1] ? F[1] : I[1]));
+    const size_t zl = (size_t)(G[2] > F[2] ? (G[2] > I[2] ? G[2] : I[2]) : (F[2] > I[2] ? F[2] : I[2]));
+    int dev = 0, smax = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) {
+        set_last_error(WVLH_ERR_CUDA);
+        return WVLH_ERR_CUDA;
+    }
+    cudaDeviceGetAttribute(&smax, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    if (2 * rows * pitch * es > (size_t)smax - 1024 || 2 * zl * TX_ * TY_ * es > (size_t)smax - 1024) {
+        set_last_error(WVLH_ERR_TOO_LARGE);
+        return WVLH_ERR_TOO_LARGE;
+    }
+    // one-time set-up on this device: the device address of the static array
+    unsigned char *base;
+    {
+        std::lock_guard<std::mutex> lock(g_setup_mutex);
+        if (!g_scratch_addr[dev]) {
+            void *a = nullptr;
+            if (cudaGetSymbolAddress(&a, g_noalloc_scratch) != cudaSuccess || !a) {
+                set_last_error(WVLH_ERR_CUDA);
+                return WVLH_ERR_CUDA;
+            }
+            g_scratch_addr[dev] = a;
+        }
+        base = (unsigned char *)g_scratch_addr[dev];
+    }
+    cudaStream_t st = (cudaStream_t)stream;
+    LrDev L;
+    for (int k = 0; k < 3; ++k) {
+        L.N[k] = N[k];
+        L.per[k] = per[k];
+        L.hgrid[k] = hgrid[k];
+    }
+    L.nseg_c = nseg_c;
+    L.nseg_f = nseg_f;
+    long long nvc = 0, nvf = 0;
+    for (int s = 0; s < nseg_c; ++s) nvc += keyg_c[2 * s + 1] - keyg_c[2 * s] + 1;
+    for (int s = 0; s < nseg_f; ++s) nvf += keyg_f[2 * s + 1] - keyg_f[2 * s] + 1;
+    L.nvctr_c = (int)nvc;
+    L.nvctr_f = (int)nvf;
+    L.seg_c = (const int4 *)(base + o_sc);
+    L.seg_f = (const int4 *)(base + o_sf);
+    L.plane_c = (const int *)(base + o_pc);
+    L.plane_f = (const int *)(base + o_pf);
+    OrbDev O;
+    O.lr = 0;
+    O.pad = 0;
+    O.psi = 0;
+    O.pot = 0;
+    O.sP = 0;
+    O.sQ = sP;
+    O.sZ = sP + sQ;
+    O.c = 0.0;
+    cudaError_t e = cudaSuccess;
+#define NA_CK(x)                                  \
+    do {                                          \
+        if ((e = (x)) != cudaSuccess) {           \
+            set_last_error(WVLH_ERR_CUDA);        \
+            return WVLH_ERR_CUDA;                 \
+        }                                         \
+    } while (0)
+    NA_CK(cudaMemcpyAsync(base + o_lr, &L, sizeof(L), cudaMemcpyHostToDevice, st));
+    NA_CK(cudaMemcpyAsync(base + o_orb, &O, sizeof(O), cudaMemcpyHostToDevice, st));
+    int32_t *dkc = (int32_t *)(base + o_kc), *dkf = (int32_t *)(base + o_kf);
+    if (nseg_c) {
+        NA_CK(cudaMemcpyAsync(dkc, keyg_c, 8 * (size_t)nseg_c, cudaMemcpyHostToDevice, st));
+        NA_CK(cudaMemcpyAsync(dkc + 2 * nseg_c, keyv_c, 4 * (size_t)nseg_c, cudaMemcpyHostToDevice, st));
+        k_decode_segments<<<(nseg_c + 255) / 256, 256, 0, st>>>(N[0], N[1], nseg_c, dkc, dkc + 2 * nseg_c,
+                                                                (int4 *)(base + o_sc));
+    }
+    if (nseg_f) {
+        NA_CK(cudaMemcpyAsync(dkf, keyg_f, 8 * (size_t)nseg_f, cudaMemcpyHostToDevice, st));
+        NA_CK(cudaMemcpyAsync(dkf + 2 * nseg_f, keyv_f, 4 * (size_t)nseg_f, cudaMemcpyHostToDevice, st));
+        k_decode_segments<<<(nseg_f + 255) / 256, 256, 0, st>>>(N[0], N[1], nseg_f, dkf, dkf + 2 * nseg_f,
+                                                                (int4 *)(base + o_sf));
+    }
+    k_plane_ranges<<<(N[2] + 256) / 256, 256, 0, st>>>(N[0] * N[1], N[2], nseg_c, dkc, (int *)(base + o_pc));
+    k_plane_ranges<<<(N[2] + 256) / 256, 256, 0, st>>>(N[0] * N[1], N[2], nseg_f, dkf, (int *)(base + o_pf));
+    const int nl = G[2] > nw2 ? G[2] : nw2;
+    k_work_lists<<<(nl + 255) / 256, 256, 0, st>>>(G[2], ntx0, nty0, ntx1, nty1, (int2 *)(base + o_w13),
+                                                   (int *)(base + o_s13), (int4 *)(base + o_w2),
+                                                   (int *)(base + o_s2));
+    NA_CK(cudaGetLastError());
+    // the launch plan lives on the host stack; its device tables point into the static array
+    Plan p;
+    p.nlr = 1;
+    p.norb = 1;
+    p.all_periodic = per[0] && per[1] && per[2];
+    p.d_lr = (LrDev *)(base + o_lr);
+    p.d_orb = (OrbDev *)(base + o_orb);
+    p.d_work13 = (int2 *)(base + o_w13);
+    p.d_part_slot13 = (int *)(base + o_s13);
+    p.d_work2 = (int4 *)(base + o_w2);
+    p.d_part_slot2 = (int *)(base + o_s2);
+    p.n_work13 = G[2];
+    p.n_work2 = nw2;
+    p.part_stride = stride;
+    p.smem13[0] = 2 * rows * pitch * 4;
+    p.smem13[1] = 2 * rows * pitch * 8;
+    p.smem2[0] = 2 * zl * TX_ * TY_ * 4;
+    p.smem2[1] = 2 * zl * TX_ * TY_ * 8;
+    // the energy partials are cleared by the launcher; P, Q/Z1, Z2 are fully
+    // overwritten before they are read, so stale contents of an earlier call
+    // never leak into this one
+    if (precision == 64)
+        e = launch_locham<double, double>(p, (const double *)psi, (const double *)pot, (double *)hpsi,
+                                          (double *)(base + o_scr), (double *)(base + o_pp), (double *)(base + o_pk),
+                                          ekin, epot, 0, st, nullptr);
+    else
+        e = launch_locham<float, float>(p, (const float *)psi, (const float *)pot, (float *)hpsi,
+                                        (float *)(base + o_scr), (double *)(base + o_pp), (double *)(base + o_pk),
+                                        ekin, epot, 0, st, nullptr);
+    NA_CK(e);
+#undef NA_CK
+    return WVLH_OK;
+}

@@ -67,6 +67,7 @@ WVLH_SYMBOLS = [
     "wvlh_batch_psi_size", "wvlh_batch_psi_offset", "wvlh_batch_scratch_bytes", "wvlh_locham_batched",
     "wvlh_locham_batched_host", "wvlh_locham_plain_batched", "wvlh_host_alloc", "wvlh_host_free",
     "wvlh_ctx_enable_timing", "wvlh_ctx_kernel_times", "wvlh_measure_fma_peak",
+    "wvlh_locham_noalloc", "wvlh_noalloc_capacity",
 ]
 
 
@@ -102,6 +103,10 @@ def lib():
     L.wvlh_ctx_enable_timing.argtypes = [vp, C.c_int]
     L.wvlh_ctx_kernel_times.argtypes = [vp, dp, C.POINTER(C.c_longlong)]
     L.wvlh_measure_fma_peak.argtypes = [C.c_int, C.c_int, dp]
+    i32p = C.POINTER(C.c_int32)
+    L.wvlh_locham_noalloc.argtypes = [C.c_int, ip, ip, dp, C.c_int, i32p, i32p, C.c_int, i32p, i32p,
+                                      vp, vp, vp, vp, vp, vp]
+    L.wvlh_noalloc_capacity.restype = C.c_size_t
     L.wvlh_host_alloc.restype = vp
     L.wvlh_host_alloc.argtypes = [C.c_size_t]
     L.wvlh_host_free.argtypes = [vp]

@@ -267,6 +267,27 @@ int wvlh_ctx_kernel_times(wvlh_ctx *ctx, double *ms4, long long *ncalls);
  * chain kernel, the compute roof of the fused stencils (precision 32 or 64). */
 int wvlh_measure_fma_peak(int precision, int iters, double *tflops);
 
+/* Local Hamiltonian of ONE orbital that allocates nothing.  No counterpart in
+ * the reference.  For callers that cannot call cudaMalloc (an application
+ * whose memory manager owns every device allocation, a layer that must not
+ * grow the device footprint on its own): all tables and scratch of the fused
+ * kernels live in a static device array of wvlh_noalloc_capacity() bytes
+ * (64 MiB), held on each GPU where this entry point has been used until the
+ * process exits.  psi/pot/hpsi/ekin/epot are the caller's DEVICE buffers
+ * (precision 32: float, 64: double; ekin/epot one double each); the keys are
+ * HOST arrays, 1-based as in the reference, read by copies queued on `stream`
+ * (keep them unchanged until the stream reaches the call).  Boxes whose
+ * scratch exceeds the capacity return WVLH_ERR_TOO_LARGE.  The first call on
+ * a device looks up the device address of the static array (set-up): make
+ * that first call before any stream capture.  Every call uses the same array,
+ * so calls that overlap on the GPU (other streams, other host threads) race:
+ * serialise them. */
+int wvlh_locham_noalloc(int precision, const int n[3], const int periodic[3], const double hgrid[3], int nseg_c,
+                        const int32_t *keyg_c, const int32_t *keyv_c, int nseg_f, const int32_t *keyg_f,
+                        const int32_t *keyv_f, const void *psi, const void *pot, void *hpsi, double *ekin,
+                        double *epot, void *stream);
+size_t wvlh_noalloc_capacity(void);
+
 /* pinned host memory helpers */
 void *wvlh_host_alloc(size_t bytes);
 void wvlh_host_free(void *p);
