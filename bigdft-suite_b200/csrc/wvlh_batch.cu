@@ -48,6 +48,7 @@ struct DevBuf {
 struct wvlh_ctx {
     int device = 0;
     cudaStream_t stream = 0;
+    DevBuf cg_r, cg_d, cg_ad, cg_scal, den_part;
     // optional per-kernel timing of the fused locham (K1, K2, K3, reduction)
     int timing = 0;
     cudaEvent_t ev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
@@ -60,6 +61,7 @@ struct wvlh_batch {
     wvlh_ctx *ctx = nullptr;
     Plan plan;
     std::vector<int64_t> pot_off;
+    bool density_ok = true;  // orbitals sharing a density grid share its region
     // raw 1-based keys per region on the device (plain path)
     std::vector<uint32_t *> d_keyg_c, d_keyv_c, d_keyg_f, d_keyv_f;
     std::vector<int> nvc, nvf, nsc, nsf;
@@ -104,6 +106,11 @@ extern "C" int wvlh_ctx_destroy(wvlh_ctx *ctx)
     ctx->io_e.release();
     for (auto &b : ctx->plain) b.release();
     ctx->dotpart.release();
+    ctx->cg_r.release();
+    ctx->cg_d.release();
+    ctx->cg_ad.release();
+    ctx->cg_scal.release();
+    ctx->den_part.release();
     for (auto &e : ctx->ev)
         if (e) cudaEventDestroy(e);
     delete ctx;
@@ -242,8 +249,9 @@ extern "C" int wvlh_batch_create(wvlh_ctx *ctx, int nlr, const wvlh_locreg *lrs,
     std::vector<OrbDev> od(norb);
     std::vector<int2> w13;
     std::vector<int> s13;
-    std::vector<int4> w2;
-    std::vector<int> s2;
+    std::vector<int4> w2, w2p;
+    std::vector<int> s2, s2p, orb_len;
+    std::vector<long long> orb_off;
     long long psi_off = 0, scr = 0;
     int stride = 0;
     size_t sm13_elems = 0, sm2_elems = 0;
@@ -285,7 +293,11 @@ extern "C" int wvlh_batch_create(wvlh_ctx *ctx, int nlr, const wvlh_locreg *lrs,
             for (int tx = 0; tx < ntx1; ++tx) {
                 w2.push_back(make_int4(o, 1, tx * TX_, ty * TY_));
                 s2.push_back(ty * ntx1 + tx);
+                w2p.push_back(make_int4(o, 1, tx * TX_, ty * TY_));
+                s2p.push_back(ty * ntx1 + tx);
             }
+        orb_off.push_back(psi_off - (d.nvctr_c + 7LL * d.nvctr_f));
+        orb_len.push_back(d.nvctr_c + 7 * d.nvctr_f);
         for (int kz = 0; kz < G3; ++kz) {
             w13.push_back(make_int2(o, kz));
             s13.push_back(ntx1 * nty1 + kz);
@@ -308,9 +320,64 @@ extern "C" int wvlh_batch_create(wvlh_ctx *ctx, int nlr, const wvlh_locreg *lrs,
     p.smem2[1] = sm2_elems * sizeof(double);
     p.n_work13 = (int)w13.size();
     p.n_work2 = (int)w2.size();
+    p.n_work2p = (int)w2p.size();
+    // density: group the orbitals by density grid (same region and offset),
+    // split each group in chunks of at most kDenChunk orbitals
+    constexpr int kDenChunk = 32;
+    std::vector<int> order(norb);
+    for (int o = 0; o < norb; ++o) order[o] = o;
+    std::stable_sort(order.begin(), order.end(), [&](int a, int c) {
+        return b->pot_off[a] != b->pot_off[c] ? b->pot_off[a] < b->pot_off[c] : orb_lr[a] < orb_lr[c];
+    });
+    std::vector<int> chunk_start, chunk_orbs, group_chunk_start, group_n;
+    std::vector<long long> chunk_part, group_rho;
+    std::vector<int4> wd;
+    long long den = 0;
+    b->density_ok = true;
+    for (int i = 0; i < norb;) {
+        int j = i;
+        while (j < norb && b->pot_off[order[j]] == b->pot_off[order[i]]) {
+            if (orb_lr[order[j]] != orb_lr[order[i]]) b->density_ok = false;  // one grid, one region
+            ++j;
+        }
+        const LrDev &d = lrd[orb_lr[order[i]]];
+        const int I1 = isf_len(d.N[0], d.per[0]), I2 = isf_len(d.N[1], d.per[1]), I3 = isf_len(d.N[2], d.per[2]);
+        if (I3 * TX_ * TY_ > 32 * kZThreads) b->density_ok = false;   // accumulators of kd_density
+        group_chunk_start.push_back((int)chunk_start.size());
+        group_rho.push_back(b->pot_off[order[i]]);
+        group_n.push_back(I1 * I2 * I3);
+        p.max_group_n = std::max(p.max_group_n, I1 * I2 * I3);
+        // a group of many orbitals is split in up to 8 chunks (one partial
+        // density each) so that its tiles fill the GPU
+        const int n = j - i;
+        const int nch = std::min(n, std::max(8, (n + kDenChunk - 1) / kDenChunk));
+        const int per_chunk = (n + nch - 1) / nch;
+        for (int k = i; k < j; k += per_chunk) {
+            const int c = (int)chunk_start.size();
+            chunk_start.push_back((int)chunk_orbs.size());
+            for (int m = k; m < std::min(j, k + per_chunk); ++m) chunk_orbs.push_back(order[m]);
+            chunk_part.push_back(den);
+            den += (long long)I1 * I2 * I3;
+            const int ntx = (I1 + TX_ - 1) / TX_, nty = (I2 + TY_ - 1) / TY_;
+            for (int ty = 0; ty < nty; ++ty)
+                for (int tx = 0; tx < ntx; ++tx) wd.push_back(make_int4(c, tx * TX_, ty * TY_, 0));
+        }
+        i = j;
+    }
+    chunk_start.push_back((int)chunk_orbs.size());
+    group_chunk_start.push_back((int)chunk_part.size());
+    p.nchunk = (int)chunk_part.size();
+    p.ngroup = (int)group_rho.size();
+    p.part_den_elems = den;
+    p.n_workd = (int)wd.size();
     if ((rc = upload(p, lrd, &p.d_lr)) || (rc = upload(p, od, &p.d_orb)) || (rc = upload(p, w13, &p.d_work13)) ||
         (rc = upload(p, s13, &p.d_part_slot13)) || (rc = upload(p, w2, &p.d_work2)) ||
-        (rc = upload(p, s2, &p.d_part_slot2))) {
+        (rc = upload(p, s2, &p.d_part_slot2)) || (rc = upload(p, w2p, &p.d_work2p)) ||
+        (rc = upload(p, s2p, &p.d_part_slot2p)) || (rc = upload(p, wd, &p.d_workd)) ||
+        (rc = upload(p, chunk_start, &p.d_chunk_orb_start)) || (rc = upload(p, chunk_orbs, &p.d_chunk_orbs)) ||
+        (rc = upload(p, chunk_part, &p.d_chunk_part)) || (rc = upload(p, group_chunk_start, &p.d_group_chunk_start)) ||
+        (rc = upload(p, group_rho, &p.d_group_rho)) || (rc = upload(p, group_n, &p.d_group_n)) ||
+        (rc = upload(p, orb_off, &p.d_orb_off)) || (rc = upload(p, orb_len, &p.d_orb_len))) {
         wvlh_batch_destroy(b);
         return fail(rc);
     }
@@ -410,6 +477,64 @@ extern "C" int wvlh_measure_fma_peak(int precision, int iters, double *tflops)
     double flops = 0.0;
     CK(fma_probe(precision, iters, &ms, &flops, 0));
     *tflops = flops / (ms * 1e-3) / 1e12;
+    return WVLH_OK;
+}
+
+namespace wvlh {
+template <class T>
+cudaError_t launch_locden(const Plan &p, const T *psi, const double *hfac, double *rho, T *scratch, double *part,
+                          cudaStream_t st);
+template <class T>
+cudaError_t launch_precond(const Plan &p, int ncong, const double *cprec, T *x, const T *b, T *r, T *dvec, T *ad,
+                           T *scratch, double *scal, double *hist, cudaStream_t st);
+}  // namespace wvlh
+
+extern "C" int wvlh_locden_batched(wvlh_batch *b, int precision, const void *psi, const double *hfac, double *rho)
+{
+    if (!b || !psi || !hfac || !rho || (precision != 32 && precision != 64)) return fail(WVLH_ERR_ARG);
+    if (!b->density_ok) return fail(WVLH_ERR_UNSUPPORTED);
+    wvlh_ctx *c = b->ctx;
+    CK(cudaSetDevice(c->device));
+    const Plan &p = b->plan;
+    const int fp = precision == 64;
+    const size_t lim = sm_limit() - 1024;
+    if (p.smem13[fp] > lim || p.smem2[fp] > lim) return fail(WVLH_ERR_TOO_LARGE);
+    int rc;
+    if ((rc = c->scratch.ensure(p.scratch_elems * (fp ? 8 : 4))) ||
+        (rc = c->den_part.ensure(sizeof(double) * (size_t)p.part_den_elems)))
+        return fail(rc);
+    cudaError_t e = fp ? launch_locden<double>(p, (const double *)psi, hfac, rho, (double *)c->scratch.p,
+                                               (double *)c->den_part.p, c->stream)
+                       : launch_locden<float>(p, (const float *)psi, hfac, rho, (float *)c->scratch.p,
+                                              (double *)c->den_part.p, c->stream);
+    CK(e);
+    return WVLH_OK;
+}
+
+extern "C" int wvlh_precond_batched(wvlh_batch *b, int precision, int ncong, const double *cprec, void *x,
+                                    const void *rhs, double *hist)
+{
+    if (!b || !cprec || !x || !rhs || ncong < 0 || (precision != 32 && precision != 64)) return fail(WVLH_ERR_ARG);
+    wvlh_ctx *c = b->ctx;
+    CK(cudaSetDevice(c->device));
+    const Plan &p = b->plan;
+    const int fp = precision == 64;
+    const size_t lim = sm_limit() - 1024;
+    if (p.smem13[fp] > lim || p.smem2[fp] > lim) return fail(WVLH_ERR_TOO_LARGE);
+    const size_t es = fp ? 8 : 4;
+    const size_t nv = (size_t)p.psi_total * es;
+    int rc;
+    if ((rc = c->scratch.ensure(p.scratch_elems * es)) || (rc = c->cg_r.ensure(nv)) || (rc = c->cg_d.ensure(nv)) ||
+        (rc = c->cg_ad.ensure(nv)) || (rc = c->cg_scal.ensure(sizeof(double) * (size_t)p.norb * (5 + 16))))
+        return fail(rc);
+    cudaError_t e =
+        fp ? launch_precond<double>(p, ncong, cprec, (double *)x, (const double *)rhs, (double *)c->cg_r.p,
+                                    (double *)c->cg_d.p, (double *)c->cg_ad.p, (double *)c->scratch.p,
+                                    (double *)c->cg_scal.p, hist, c->stream)
+           : launch_precond<float>(p, ncong, cprec, (float *)x, (const float *)rhs, (float *)c->cg_r.p,
+                                   (float *)c->cg_d.p, (float *)c->cg_ad.p, (float *)c->scratch.p,
+                                   (double *)c->cg_scal.p, hist, c->stream);
+    CK(e);
     return WVLH_OK;
 }
 

@@ -1,5 +1,6 @@
-// Fused, batched local Hamiltonian (Hpsi, E_kin, E_pot) for many orbitals
-// and many localisation regions in three kernels, FP32 or FP64.
+// Fused, batched local Hamiltonian (Hpsi, E_kin, E_pot), density and
+// preconditioner operator for many orbitals and many localisation regions,
+// FP32 or FP64.
 //
 // The reference applies locham to one orbital at a time as 13 full-array
 // passes (uncompress, 3x syn, 3x MF, xV, 3x MF^T, 3x kinetic, 3x ana,
@@ -15,6 +16,13 @@
 // X = S^3 psi: the z part from K2 on X itself, the x,y parts from K3 on P
 // (<X|K_x X> = <P|K_x P> because S_z is an isometry).  Energies are reduced
 // in FP64 into per-CTA partial slots and summed in a fixed order.
+//
+// The same kernels in MODE_LOCDEN give the density rho += hfac (M^3 S^3 psi)^2
+// (OpenCL/Density.c:37-55, sumrho.f90:472-577) through K1 (Q only) and a
+// z-kernel that loops over the orbitals sharing a density grid, and in
+// MODE_PRECOND the preconditioner operator D^-1/2 A (c + T) S D^-1/2 of
+// OpenCL/Preconditioner.c:98-128 through K1 (scaled gather, P only), the
+// kinetic chain of K2 and K3 (Z2 + c P + (K_x+K_y) P, scaled scatter).
 #include <cuda_runtime.h>
 
 #include "wvlh_common.cuh"
@@ -63,20 +71,34 @@ __device__ __forceinline__ int fs1(int c) { return c & 1; }
 __device__ __forceinline__ int fs2(int c) { return (c >> 1) & 1; }
 __device__ __forceinline__ int fs3(int c) { return (c >> 2) & 1; }
 
+// Preconditioner diagonal D^-1/2 per component k = s1 + 2 s2 + 4 s3: GPUscal0..7
+// of OpenCL/Uncompress.c:380-470 with h = hgrid/2 (the host passes 0.5*hgrid).
+__device__ __forceinline__ double prec_scal(const LrDev &L, double c, int k)
+{
+    double s = c;
+    for (int d = 0; d < 3; ++d) {
+        const double h = 0.5 * L.hgrid[d];
+        s += (((k >> d) & 1) ? WVL_B2 : WVL_A2) * (0.125 / (h * h));
+    }
+    return 1.0 / sqrt(s);
+}
+
 // Scatter the compressed coefficients of wavelet-basis plane kz into the
-// (G2 x G1, pitch) buffer A, which must be zero.  psi points at [psi_c|psi_f].
+// (G2 x G1, pitch) buffer A, which must be zero.  psi points at [psi_c|psi_f];
+// sc (8 factors) scales each component when non-null.
 template <class T, class TI>
-__device__ void gather_plane(T *A, int pitch, const LrDev &L, int kz, const TI *psi)
+__device__ void gather_plane(T *A, int pitch, const LrDev &L, int kz, const TI *psi, const T *sc)
 {
     const int N1 = L.N[0], N2 = L.N[1], N3 = L.N[2];
     const int s3 = kz >= N3;
     const int i3 = kz - s3 * N3;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
     if (!s3) {
+        const T s0 = sc ? sc[0] : T(1);
         const int a = L.plane_c[i3], b = L.plane_c[i3 + 1];
         for (int sg = a + warp; sg < b; sg += nw) {
             const int4 d = L.seg_c[sg];
-            for (int t = lane; t < d.z; t += 32) A[d.y * pitch + d.x + t] = (T)psi[d.w + t];
+            for (int t = lane; t < d.z; t += 32) A[d.y * pitch + d.x + t] = (T)psi[d.w + t] * s0;
         }
     }
     const TI *pf = psi + L.nvctr_c;
@@ -88,7 +110,7 @@ __device__ void gather_plane(T *A, int pitch, const LrDev &L, int kz, const TI *
 #pragma unroll
             for (int c = 1; c <= 7; ++c) {
                 if (fs3(c) != s3) continue;
-                A[(fs2(c) * N2 + d.y) * pitch + fs1(c) * N1 + d.x + t] = (T)src[c - 1];
+                A[(fs2(c) * N2 + d.y) * pitch + fs1(c) * N1 + d.x + t] = (T)src[c - 1] * (sc ? sc[c] : T(1));
             }
         }
     }
@@ -96,18 +118,19 @@ __device__ void gather_plane(T *A, int pitch, const LrDev &L, int kz, const TI *
 
 // Inverse of gather_plane: write (or add into) the compressed output.
 template <class T, class TO>
-__device__ void scatter_plane(const T *A, int pitch, const LrDev &L, int kz, TO *out, bool accumulate)
+__device__ void scatter_plane(const T *A, int pitch, const LrDev &L, int kz, TO *out, bool accumulate, const T *sc)
 {
     const int N1 = L.N[0], N2 = L.N[1], N3 = L.N[2];
     const int s3 = kz >= N3;
     const int i3 = kz - s3 * N3;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
     if (!s3) {
+        const T s0 = sc ? sc[0] : T(1);
         const int a = L.plane_c[i3], b = L.plane_c[i3 + 1];
         for (int sg = a + warp; sg < b; sg += nw) {
             const int4 d = L.seg_c[sg];
             for (int t = lane; t < d.z; t += 32) {
-                const TO v = (TO)A[d.y * pitch + d.x + t];
+                const TO v = (TO)(A[d.y * pitch + d.x + t] * s0);
                 out[d.w + t] = accumulate ? out[d.w + t] + v : v;
             }
         }
@@ -121,7 +144,7 @@ __device__ void scatter_plane(const T *A, int pitch, const LrDev &L, int kz, TO 
 #pragma unroll
             for (int c = 1; c <= 7; ++c) {
                 if (fs3(c) != s3) continue;
-                const TO v = (TO)A[(fs2(c) * N2 + d.y) * pitch + fs1(c) * N1 + d.x + t];
+                const TO v = (TO)(A[(fs2(c) * N2 + d.y) * pitch + fs1(c) * N1 + d.x + t] * (sc ? sc[c] : T(1)));
                 dst[c - 1] = accumulate ? dst[c - 1] + v : v;
             }
         }
@@ -129,10 +152,9 @@ __device__ void scatter_plane(const T *A, int pitch, const LrDev &L, int kz, TO 
 }
 
 template <class T>
-__device__ __forceinline__ void zero_region(T *A, int rows, int cols, int pitch)
+__device__ __forceinline__ void zero_region(T *A, int rows, int pitch)
 {
     for (int i = threadIdx.x; i < rows * pitch; i += blockDim.x) A[i] = T(0);
-    (void)cols;
 }
 
 template <class T>
@@ -153,16 +175,29 @@ __device__ __forceinline__ void load_plane(T *A, int pitch, int rows, int cols, 
     }
 }
 
+template <class TI>
+__device__ __forceinline__ const TI *in_ptr(const OrbDev &o, const TI *base)
+{
+    return o.in_ptr ? (const TI *)o.in_ptr : base + o.psi;
+}
+template <class TO>
+__device__ __forceinline__ TO *out_ptr(const OrbDev &o, TO *base)
+{
+    return o.out_ptr ? (TO *)o.out_ptr : base + o.psi;
+}
+
 // ---------------------------------------------------------------------------
-// K1: compressed psi -> P = S_x S_y psi and Q = M_x M_y P for one z-plane.
-// TI is the storage type of psi (may differ from compute type T).
-template <class T, class TI, bool ALLPER>
+// K1: compressed psi -> P = S_x S_y psi (not in MODE_LOCDEN) and
+// Q = M_x M_y P (not in MODE_PRECOND) for one wavelet z-plane.
+template <class T, class TI, bool ALLPER, int MODE>
 __global__ void __launch_bounds__(kPlaneThreads) k1_plane_forward(const LrDev *__restrict__ lrs,
                                                                   const OrbDev *__restrict__ orbs,
                                                                   const int2 *__restrict__ work,
-                                                                  const TI *__restrict__ psi, T *__restrict__ scratch)
+                                                                  const TI *__restrict__ psi, T *__restrict__ scratch,
+                                                                  const double *__restrict__ cprec)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ T sc[8];
     const int2 w = work[blockIdx.x];
     const OrbDev o = orbs[w.x];
     const LrDev L = lrs[o.lr];
@@ -170,18 +205,20 @@ __global__ void __launch_bounds__(kPlaneThreads) k1_plane_forward(const LrDev *_
     const int kz = w.y;
     const int pitch = d.pitch();
     T *A = reinterpret_cast<T *>(smem_raw);
-    T *B = A + (size_t)d.rows() * pitch;
+    T *B = A + d.rows() * pitch;
     constexpr int SEG = Seg<T>::v;
 
-    zero_region(A, d.G2, d.G1, pitch);
+    if (MODE == MODE_PRECOND && threadIdx.x < 8) sc[threadIdx.x] = (T)prec_scal(L, cprec[w.x], threadIdx.x);
+    zero_region(A, d.G2, pitch);
     __syncthreads();
-    gather_plane<T, TI>(A, pitch, L, kz, psi + o.psi);
+    gather_plane<T, TI>(A, pitch, L, kz, in_ptr(o, psi), MODE == MODE_PRECOND ? sc : nullptr);
     __syncthreads();
     pass_syn<T, SEG>(A, B, rows_geom(d.G2, pitch), d.N1, d.p1);   // S_x: G2 rows, G1 -> F1
     __syncthreads();
     pass_syn<T, SEG>(B, A, cols_geom(d.F1, pitch), d.N2, d.p2);   // S_y: F1 cols, G2 -> F2
     __syncthreads();
-    store_plane(A, pitch, d.F2, d.F1, scratch + o.sP + (size_t)kz * d.F2 * d.F1);
+    if (MODE != MODE_LOCDEN) store_plane(A, pitch, d.F2, d.F1, scratch + o.sP + (size_t)kz * d.F2 * d.F1);
+    if (MODE == MODE_PRECOND) return;
     if (d.p1) pass_mf<T, SEG, 0>(A, B, rows_geom(d.F2, pitch), d.F1, d.I1);
     else pass_mf<T, SEG, 2>(A, B, rows_geom(d.F2, pitch), d.F1, d.I1);
     __syncthreads();
@@ -210,7 +247,7 @@ __global__ void __launch_bounds__(kZThreads) k2_zpencil(const LrDev *__restrict_
     const int chain = w.y, x0 = w.z, y0 = w.w;
     const int zl = max(d.G3, max(d.F3, d.I3));
     T *A = reinterpret_cast<T *>(smem_raw);
-    T *B = A + (size_t)zl * TC;
+    T *B = A + zl * TC;
     constexpr int SEG = Seg<T>::v;
     const int W = chain == 0 ? d.I1 : d.F1;   // plane width/height of the data
     const int H = chain == 0 ? d.I2 : d.F2;
@@ -235,7 +272,7 @@ __global__ void __launch_bounds__(kZThreads) k2_zpencil(const LrDev *__restrict_
         __syncthreads();
         // psir <- V psir, epot += V psir^2 (orbitals/potential.f90:1011-1031);
         // per-thread partial sum in T, one FP64 conversion per thread
-        const TV *V = pot + o.pot;
+        const TV *V = o.pot_ptr ? (const TV *)o.pot_ptr : pot + o.pot;
         T ep = T(0);
         for (int i = threadIdx.x; i < d.I3 * TC; i += blockDim.x) {
             const int z = i / TC, c = i - z * TC;
@@ -270,22 +307,25 @@ __global__ void __launch_bounds__(kZThreads) k2_zpencil(const LrDev *__restrict_
         if (x < W && y < H) gz[(size_t)z * plane + (size_t)y * W + x] = A[i];
     }
     const double s = block_sum(e, red);
-    if (threadIdx.x == 0) (chain == 0 ? part_pot : part_kin)[(size_t)w.x * part_stride + slots[blockIdx.x]] = s;
+    if (threadIdx.x == 0 && part_kin)
+        (chain == 0 ? part_pot : part_kin)[(size_t)w.x * part_stride + slots[blockIdx.x]] = s;
 }
 
 // ---------------------------------------------------------------------------
-// K3: Hpsi plane kz = A_x A_y [Mt_x Mt_y Z1 + Z2 + (K_x + K_y) P]
-template <class T, class TO, bool ALLPER>
+// K3 (MODE_LOCHAM): Hpsi plane kz = A_x A_y [Mt_x Mt_y Z1 + Z2 + (K_x + K_y) P]
+// K3 (MODE_PRECOND): D^-1/2 A_x A_y [Z2 + c P + (K_x + K_y) P]
+template <class T, class TO, bool ALLPER, int MODE>
 __global__ void __launch_bounds__(kPlaneThreads) k3_plane_backward(const LrDev *__restrict__ lrs,
                                                                    const OrbDev *__restrict__ orbs,
                                                                    const int2 *__restrict__ work,
                                                                    const int *__restrict__ slots,
                                                                    const T *__restrict__ scratch, TO *__restrict__ hpsi,
                                                                    double *__restrict__ part_kin, int part_stride,
-                                                                   int accumulate)
+                                                                   int accumulate, const double *__restrict__ cprec)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ double red[32];
+    __shared__ T sc[8];
     const int2 w = work[blockIdx.x];
     const OrbDev o = orbs[w.x];
     const LrDev L = lrs[o.lr];
@@ -293,24 +333,32 @@ __global__ void __launch_bounds__(kPlaneThreads) k3_plane_backward(const LrDev *
     const int kz = w.y;
     const int pitch = d.pitch();
     T *A = reinterpret_cast<T *>(smem_raw);
-    T *B = A + (size_t)d.rows() * pitch;
+    T *B = A + d.rows() * pitch;
     constexpr int SEG = Seg<T>::v;
 
-    load_plane(A, pitch, d.I2, d.I1, scratch + o.sQ + (size_t)kz * d.I2 * d.I1);
-    __syncthreads();
-    if (d.p1) pass_mf<T, SEG, 1>(A, B, rows_geom(d.I2, pitch), d.I1, d.F1);   // Mt_x
-    else pass_mf<T, SEG, 3>(A, B, rows_geom(d.I2, pitch), d.I1, d.F1);
-    __syncthreads();
-    if (d.p2) pass_mf<T, SEG, 1>(B, A, cols_geom(d.F1, pitch), d.I2, d.F2);   // Mt_y
-    else pass_mf<T, SEG, 3>(B, A, cols_geom(d.F1, pitch), d.I2, d.F2);
-    __syncthreads();
+    T cshift = T(0);
+    if (MODE == MODE_PRECOND) {
+        cshift = (T)cprec[w.x];
+        if (threadIdx.x < 8) sc[threadIdx.x] = (T)prec_scal(L, cprec[w.x], threadIdx.x);
+    } else {
+        load_plane(A, pitch, d.I2, d.I1, scratch + o.sQ + (size_t)kz * d.I2 * d.I1);
+        __syncthreads();
+        if (d.p1) pass_mf<T, SEG, 1>(A, B, rows_geom(d.I2, pitch), d.I1, d.F1);   // Mt_x
+        else pass_mf<T, SEG, 3>(A, B, rows_geom(d.I2, pitch), d.I1, d.F1);
+        __syncthreads();
+        if (d.p2) pass_mf<T, SEG, 1>(B, A, cols_geom(d.F1, pitch), d.I2, d.F2);   // Mt_y
+        else pass_mf<T, SEG, 3>(B, A, cols_geom(d.F1, pitch), d.I2, d.F2);
+        __syncthreads();
+    }
     {
         const T *z2 = scratch + o.sZ + (size_t)kz * d.F2 * d.F1;
         const T *p = scratch + o.sP + (size_t)kz * d.F2 * d.F1;
         for (int i = threadIdx.x; i < d.F2 * d.F1; i += blockDim.x) {
             const int r = i / d.F1, c = i - r * d.F1;
-            A[r * pitch + c] += z2[i];
-            B[r * pitch + c] = p[i];
+            const T pv = p[i];
+            if (MODE == MODE_PRECOND) A[r * pitch + c] = fma(cshift, pv, z2[i]);
+            else A[r * pitch + c] += z2[i];
+            B[r * pitch + c] = pv;
         }
     }
     __syncthreads();
@@ -325,9 +373,10 @@ __global__ void __launch_bounds__(kPlaneThreads) k3_plane_backward(const LrDev *
     __syncthreads();
     pass_ana<T, SEG>(B, A, cols_geom(d.G1, pitch), d.N2, d.p2);   // A_y: F2 -> G2
     __syncthreads();
-    scatter_plane<T, TO>(A, pitch, L, kz, hpsi + o.psi, accumulate != 0);
+    scatter_plane<T, TO>(A, pitch, L, kz, out_ptr(o, hpsi), accumulate != 0,
+                         MODE == MODE_PRECOND ? sc : nullptr);
     const double s = block_sum(e, red);
-    if (threadIdx.x == 0) part_kin[(size_t)w.x * part_stride + slots[blockIdx.x]] = s;
+    if (threadIdx.x == 0 && part_kin) part_kin[(size_t)w.x * part_stride + slots[blockIdx.x]] = s;
 }
 
 // fixed-order per-orbital sum of the energy partial slots
@@ -352,6 +401,191 @@ __global__ void k_reduce_energies(const double *__restrict__ part_pot, const dou
 }
 
 // ---------------------------------------------------------------------------
+// Density z-kernel: for a tile of ISF columns, loop over the orbitals of one
+// chunk: R = M_z S_z Q, acc += hfac R^2 (FP64), then write the chunk partial.
+template <class T, bool ALLPER>
+__global__ void __launch_bounds__(kZThreads) kd_density(const LrDev *__restrict__ lrs,
+                                                        const OrbDev *__restrict__ orbs,
+                                                        const int4 *__restrict__ work,
+                                                        const int *__restrict__ chunk_orb_start,
+                                                        const int *__restrict__ chunk_orbs,
+                                                        const long long *__restrict__ chunk_part,
+                                                        const T *__restrict__ scratch, const double *__restrict__ hfac,
+                                                        double *__restrict__ part)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    constexpr int MAXP = 32;   // accumulators per thread (I3 * TC / kZThreads <= MAXP)
+    const int4 w = work[blockIdx.x];
+    const int chunk = w.x, x0 = w.y, y0 = w.z;
+    const int ob = chunk_orb_start[chunk], oe = chunk_orb_start[chunk + 1];
+    const OrbDev o0 = orbs[chunk_orbs[ob]];
+    const LrDev L = lrs[o0.lr];
+    const Dims d(L, ALLPER);
+    const int zl = max(d.G3, max(d.F3, d.I3));
+    T *A = reinterpret_cast<T *>(smem_raw);
+    T *B = A + zl * TC;
+    constexpr int SEG = Seg<T>::v;
+    const int W = d.I1, H = d.I2;
+    const size_t plane = (size_t)W * H;
+    const LineGeom zg{TC, 1, TC, 1, TC};
+    double acc[MAXP];
+#pragma unroll
+    for (int k = 0; k < MAXP; ++k) acc[k] = 0.0;
+    for (int oi = ob; oi < oe; ++oi) {
+        const int orb = chunk_orbs[oi];
+        const OrbDev o = orbs[orb];
+        const T *g = scratch + o.sQ;
+        __syncthreads();
+        for (int i = threadIdx.x; i < d.G3 * TC; i += blockDim.x) {
+            const int z = i / TC, c = i - z * TC;
+            const int x = x0 + (c % TX), y = y0 + (c / TX);
+            A[i] = (x < W && y < H) ? g[(size_t)z * plane + (size_t)y * W + x] : T(0);
+        }
+        __syncthreads();
+        pass_syn<T, SEG>(A, B, zg, d.N3, d.p3);                  // S_z
+        __syncthreads();
+        if (d.p3) pass_mf<T, SEG, 0>(B, A, zg, d.F3, d.I3);       // M_z
+        else pass_mf<T, SEG, 2>(B, A, zg, d.F3, d.I3);
+        __syncthreads();
+        const double hf = hfac[orb];
+#pragma unroll
+        for (int k = 0; k < MAXP; ++k) {
+            const int i = threadIdx.x + k * blockDim.x;
+            if (i < d.I3 * TC) {
+                const double r = (double)A[i];
+                acc[k] = fma(hf * r, r, acc[k]);
+            }
+        }
+    }
+    double *out = part + chunk_part[chunk];
+#pragma unroll
+    for (int k = 0; k < MAXP; ++k) {
+        const int i = threadIdx.x + k * blockDim.x;
+        if (i < d.I3 * TC) {
+            const int z = i / TC, c = i - z * TC;
+            const int x = x0 + (c % TX), y = y0 + (c / TX);
+            if (x < W && y < H) out[((size_t)z * H + y) * W + x] = acc[k];
+        }
+    }
+}
+
+// rho[group] += sum of the group's chunk partials, in chunk order
+__global__ void k_density_reduce(const int *__restrict__ group_chunk_start, const long long *__restrict__ group_rho,
+                                 const int *__restrict__ group_n, const long long *__restrict__ chunk_part,
+                                 const double *__restrict__ part, double *__restrict__ rho)
+{
+    const int g = blockIdx.y;
+    const int n = group_n[g];
+    const int cb = group_chunk_start[g], ce = group_chunk_start[g + 1];
+    double *r = rho + group_rho[g];
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        double s = r[i];
+        for (int c = cb; c < ce; ++c) s += part[chunk_part[c] + i];
+        r[i] = s;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Batched CG vector kernels (OpenCL/Preconditioner.c:130-195 with per-orbital
+// scalars kept on the device).  Vectors are [psi_c | psi_f] per orbital at
+// off[o], len[o] values; grid.y = orbital, grid.x = chunks of the vector.
+constexpr int kCgChunks = 16;
+
+template <class T>
+__global__ void k_cg_dot(const long long *__restrict__ off, const int *__restrict__ len, const T *__restrict__ x,
+                         const T *__restrict__ y, double *__restrict__ part)
+{
+    __shared__ double red[32];
+    const int o = blockIdx.y;
+    const long long b = off[o];
+    const int n = len[o];
+    double s = 0.0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        s += (double)x[b + i] * (double)y[b + i];
+    const double t = block_sum(s, red);
+    if (threadIdx.x == 0) part[o * kCgChunks + blockIdx.x] = t;
+}
+
+// out[o] = sum of its chunk partials (fixed order); optionally copy into hist
+__global__ void k_cg_sum(int norb, const double *__restrict__ part, double *__restrict__ out,
+                         double *__restrict__ hist)
+{
+    const int o = blockIdx.x * blockDim.x + threadIdx.x;
+    if (o >= norb) return;
+    double s = 0.0;
+    for (int c = 0; c < kCgChunks; ++c) s += part[o * kCgChunks + c];
+    out[o] = s;
+    if (hist) hist[o] = s;
+}
+
+// r = b - Ax; d = r
+template <class T>
+__global__ void k_cg_init(const long long *__restrict__ off, const int *__restrict__ len, const T *__restrict__ b,
+                          const T *__restrict__ ax, T *__restrict__ r, T *__restrict__ d)
+{
+    const int o = blockIdx.y;
+    const long long base = off[o];
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < len[o]; i += gridDim.x * blockDim.x) {
+        const T v = b[base + i] - ax[base + i];
+        r[base + i] = v;
+        d[base + i] = v;
+    }
+}
+
+// alpha = rr/dAd; x += alpha d; if (update_r) r -= alpha Ad
+template <class T>
+__global__ void k_cg_step(const long long *__restrict__ off, const int *__restrict__ len,
+                          const double *__restrict__ rr, const double *__restrict__ dad, T *__restrict__ x,
+                          const T *__restrict__ d, T *__restrict__ r, const T *__restrict__ ad, int update_r)
+{
+    const int o = blockIdx.y;
+    const long long base = off[o];
+    const T alpha = (T)(rr[o] / dad[o]);
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < len[o]; i += gridDim.x * blockDim.x) {
+        x[base + i] = fma(alpha, d[base + i], x[base + i]);
+        if (update_r) r[base + i] = fma(-alpha, ad[base + i], r[base + i]);
+    }
+}
+
+// beta = rr_new/rr; d = beta d + r; rr = rr_new
+template <class T>
+__global__ void k_cg_dir(const long long *__restrict__ off, const int *__restrict__ len, double *__restrict__ rr,
+                         const double *__restrict__ rr_new, T *__restrict__ d, const T *__restrict__ r)
+{
+    const int o = blockIdx.y;
+    const long long base = off[o];
+    const T beta = (T)(rr_new[o] / rr[o]);
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < len[o]; i += gridDim.x * blockDim.x)
+        d[base + i] = fma(beta, d[base + i], r[base + i]);
+}
+
+__global__ void k_copy_scalars(int n, const double *__restrict__ a, double *__restrict__ b)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) b[i] = a[i];
+}
+
+// x *= D^-1/2 per component (scale_psi_d, OpenCL/Uncompress.c:596)
+template <class T>
+__global__ void k_cg_scale(const LrDev *__restrict__ lrs, const OrbDev *__restrict__ orbs,
+                           const long long *__restrict__ off, const int *__restrict__ len,
+                           const double *__restrict__ cprec, T *__restrict__ x)
+{
+    const int o = blockIdx.y;
+    const OrbDev ob = orbs[o];
+    const LrDev L = lrs[ob.lr];
+    T sc[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) sc[k] = (T)prec_scal(L, cprec[o], k);
+    const long long base = off[o];
+    const int nc = L.nvctr_c;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < len[o]; i += gridDim.x * blockDim.x) {
+        const int k = i < nc ? 0 : 1 + (i - nc) % 7;
+        x[base + i] *= sc[k];
+    }
+}
+
+// ---------------------------------------------------------------------------
 // host launchers
 template <class T, class TIO, bool ALLPER>
 static cudaError_t launch_locham_bc(const Plan &p, const TIO *psi, const TIO *pot, TIO *hpsi, T *scratch,
@@ -361,26 +595,23 @@ static cudaError_t launch_locham_bc(const Plan &p, const TIO *psi, const TIO *po
     const int fp = sizeof(T) == 8 ? 1 : 0;
     const size_t sm13 = p.smem13[fp], sm2 = p.smem2[fp];
     cudaError_t err;
-    err = cudaFuncSetAttribute(k1_plane_forward<T, TIO, ALLPER>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               (int)sm13);
-    if (err != cudaSuccess) return err;
-    err = cudaFuncSetAttribute(k2_zpencil<T, TIO, ALLPER>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm2);
-    if (err != cudaSuccess) return err;
-    err = cudaFuncSetAttribute(k3_plane_backward<T, TIO, ALLPER>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               (int)sm13);
-    if (err != cudaSuccess) return err;
+    auto k1 = k1_plane_forward<T, TIO, ALLPER, MODE_LOCHAM>;
+    auto k2 = k2_zpencil<T, TIO, ALLPER>;
+    auto k3 = k3_plane_backward<T, TIO, ALLPER, MODE_LOCHAM>;
+    if ((err = cudaFuncSetAttribute(k1, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm13))) return err;
+    if ((err = cudaFuncSetAttribute(k2, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm2))) return err;
+    if ((err = cudaFuncSetAttribute(k3, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm13))) return err;
     cudaMemsetAsync(part_pot, 0, sizeof(double) * (size_t)p.norb * p.part_stride, st);
     cudaMemsetAsync(part_kin, 0, sizeof(double) * (size_t)p.norb * p.part_stride, st);
     // optional per-kernel timing: ev[0..4] bracket K1, K2, K3 and the reduction
     if (ev) cudaEventRecord(ev[0], st);
-    k1_plane_forward<T, TIO, ALLPER><<<p.n_work13, kPlaneThreads, sm13, st>>>(p.d_lr, p.d_orb, p.d_work13, psi,
-                                                                             scratch);
+    k1<<<p.n_work13, kPlaneThreads, sm13, st>>>(p.d_lr, p.d_orb, p.d_work13, psi, scratch, nullptr);
     if (ev) cudaEventRecord(ev[1], st);
-    k2_zpencil<T, TIO, ALLPER><<<p.n_work2, kZThreads, sm2, st>>>(p.d_lr, p.d_orb, p.d_work2, p.d_part_slot2, pot,
-                                                                 scratch, part_pot, part_kin, p.part_stride);
+    k2<<<p.n_work2, kZThreads, sm2, st>>>(p.d_lr, p.d_orb, p.d_work2, p.d_part_slot2, pot, scratch, part_pot,
+                                          part_kin, p.part_stride);
     if (ev) cudaEventRecord(ev[2], st);
-    k3_plane_backward<T, TIO, ALLPER><<<p.n_work13, kPlaneThreads, sm13, st>>>(
-        p.d_lr, p.d_orb, p.d_work13, p.d_part_slot13, scratch, hpsi, part_kin, p.part_stride, accumulate);
+    k3<<<p.n_work13, kPlaneThreads, sm13, st>>>(p.d_lr, p.d_orb, p.d_work13, p.d_part_slot13, scratch, hpsi,
+                                                part_kin, p.part_stride, accumulate, nullptr);
     if (ev) cudaEventRecord(ev[3], st);
     k_reduce_energies<<<p.norb, 128, 0, st>>>(part_pot, part_kin, p.part_stride, p.norb, ekin, epot);
     if (ev) cudaEventRecord(ev[4], st);
@@ -405,6 +636,100 @@ template cudaError_t launch_locham<float, float>(const Plan &, const float *, co
 template cudaError_t launch_locham<double, double>(const Plan &, const double *, const double *, double *, double *,
                                                    double *, double *, double *, double *, int, cudaStream_t,
                                                    cudaEvent_t *);
+
+template <class T, bool ALLPER>
+static cudaError_t launch_locden_bc(const Plan &p, const T *psi, const double *hfac, double *rho, T *scratch,
+                                    double *part, cudaStream_t st)
+{
+    const int fp = sizeof(T) == 8 ? 1 : 0;
+    const size_t sm13 = p.smem13[fp], sm2 = p.smem2[fp];
+    cudaError_t err;
+    auto k1 = k1_plane_forward<T, T, ALLPER, MODE_LOCDEN>;
+    auto kd = kd_density<T, ALLPER>;
+    if ((err = cudaFuncSetAttribute(k1, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm13))) return err;
+    if ((err = cudaFuncSetAttribute(kd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm2))) return err;
+    k1<<<p.n_work13, kPlaneThreads, sm13, st>>>(p.d_lr, p.d_orb, p.d_work13, psi, scratch, nullptr);
+    kd<<<p.n_workd, kZThreads, sm2, st>>>(p.d_lr, p.d_orb, p.d_workd, p.d_chunk_orb_start, p.d_chunk_orbs,
+                                          p.d_chunk_part, scratch, hfac, part);
+    dim3 g((p.max_group_n + 255) / 256 < 4096 ? (p.max_group_n + 255) / 256 : 4096, p.ngroup);
+    k_density_reduce<<<g, 256, 0, st>>>(p.d_group_chunk_start, p.d_group_rho, p.d_group_n, p.d_chunk_part, part,
+                                        rho);
+    return cudaGetLastError();
+}
+
+template <class T>
+cudaError_t launch_locden(const Plan &p, const T *psi, const double *hfac, double *rho, T *scratch, double *part,
+                          cudaStream_t st)
+{
+    if (p.all_periodic) return launch_locden_bc<T, true>(p, psi, hfac, rho, scratch, part, st);
+    return launch_locden_bc<T, false>(p, psi, hfac, rho, scratch, part, st);
+}
+template cudaError_t launch_locden<float>(const Plan &, const float *, const double *, double *, float *, double *,
+                                          cudaStream_t);
+template cudaError_t launch_locden<double>(const Plan &, const double *, const double *, double *, double *,
+                                           double *, cudaStream_t);
+
+// preconditioner operator y = D^-1/2 A (c + T) S D^-1/2 x for every orbital
+template <class T, bool ALLPER>
+static cudaError_t launch_prec_apply_bc(const Plan &p, const T *x, T *y, const double *cprec, T *scratch,
+                                        cudaStream_t st)
+{
+    const int fp = sizeof(T) == 8 ? 1 : 0;
+    const size_t sm13 = p.smem13[fp], sm2 = p.smem2[fp];
+    cudaError_t err;
+    auto k1 = k1_plane_forward<T, T, ALLPER, MODE_PRECOND>;
+    auto k2 = k2_zpencil<T, T, ALLPER>;
+    auto k3 = k3_plane_backward<T, T, ALLPER, MODE_PRECOND>;
+    if ((err = cudaFuncSetAttribute(k1, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm13))) return err;
+    if ((err = cudaFuncSetAttribute(k2, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm2))) return err;
+    if ((err = cudaFuncSetAttribute(k3, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm13))) return err;
+    k1<<<p.n_work13, kPlaneThreads, sm13, st>>>(p.d_lr, p.d_orb, p.d_work13, x, scratch, cprec);
+    k2<<<p.n_work2p, kZThreads, sm2, st>>>(p.d_lr, p.d_orb, p.d_work2p, p.d_part_slot2p, (const T *)nullptr,
+                                           scratch, nullptr, nullptr, 0);
+    k3<<<p.n_work13, kPlaneThreads, sm13, st>>>(p.d_lr, p.d_orb, p.d_work13, p.d_part_slot13, scratch, y, nullptr, 0,
+                                                0, cprec);
+    return cudaGetLastError();
+}
+
+// Batched CG of ocl_preconditioner_generic: x (in: initial guess, out:
+// preconditioned), b right-hand side; work: r, d, ad vectors; scal: 5*norb
+// doubles + kCgChunks*norb partials; hist (optional): (ncong+1)*norb squared
+// residual norms, entry 0 the initial one.
+template <class T>
+cudaError_t launch_precond(const Plan &p, int ncong, const double *cprec, T *x, const T *b, T *r, T *dvec, T *ad,
+                           T *scratch, double *scal, double *hist, cudaStream_t st)
+{
+    double *rr = scal, *dad = scal + p.norb, *rrn = scal + 2 * p.norb, *part = scal + 5 * p.norb;
+    const dim3 vg(kCgChunks, p.norb);
+    auto apply = [&](const T *in, T *out) {
+        return p.all_periodic ? launch_prec_apply_bc<T, true>(p, in, out, cprec, scratch, st)
+                              : launch_prec_apply_bc<T, false>(p, in, out, cprec, scratch, st);
+    };
+    cudaError_t err;
+    if ((err = apply(x, ad))) return err;
+    k_cg_init<T><<<vg, 256, 0, st>>>(p.d_orb_off, p.d_orb_len, b, ad, r, dvec);
+    k_cg_dot<T><<<vg, 256, 0, st>>>(p.d_orb_off, p.d_orb_len, r, r, part);
+    k_cg_sum<<<(p.norb + 127) / 128, 128, 0, st>>>(p.norb, part, rr, hist);
+    for (int it = 0; it < ncong; ++it) {
+        if ((err = apply(dvec, ad))) return err;
+        k_cg_dot<T><<<vg, 256, 0, st>>>(p.d_orb_off, p.d_orb_len, dvec, ad, part);
+        k_cg_sum<<<(p.norb + 127) / 128, 128, 0, st>>>(p.norb, part, dad, nullptr);
+        k_cg_step<T><<<vg, 256, 0, st>>>(p.d_orb_off, p.d_orb_len, rr, dad, x, dvec, r, ad, 1);
+        k_cg_dot<T><<<vg, 256, 0, st>>>(p.d_orb_off, p.d_orb_len, r, r, part);
+        k_cg_sum<<<(p.norb + 127) / 128, 128, 0, st>>>(p.norb, part, rrn,
+                                                      hist ? hist + (size_t)(it + 1) * p.norb : nullptr);
+        if (it != ncong - 1) {
+            k_cg_dir<T><<<vg, 256, 0, st>>>(p.d_orb_off, p.d_orb_len, rr, rrn, dvec, r);
+            k_copy_scalars<<<(p.norb + 127) / 128, 128, 0, st>>>(p.norb, rrn, rr);
+        }
+    }
+    k_cg_scale<T><<<vg, 256, 0, st>>>(p.d_lr, p.d_orb, p.d_orb_off, p.d_orb_len, cprec, x);
+    return cudaGetLastError();
+}
+template cudaError_t launch_precond<float>(const Plan &, int, const double *, float *, const float *, float *, float *,
+                                           float *, float *, double *, double *, cudaStream_t);
+template cudaError_t launch_precond<double>(const Plan &, int, const double *, double *, const double *, double *,
+                                            double *, double *, double *, double *, double *, cudaStream_t);
 
 // FP32/FP64 FMA throughput probe: independent FMA chains held in registers.
 template <class T>

@@ -38,12 +38,19 @@ struct OrbDev {
     int lr;
     int pad;
     long long psi;   // element offset of [psi_c | psi_f] in the psi/hpsi arrays
-    long long pot;   // element offset of this orbital's potential (ISF grid)
+    long long pot;   // element offset of this orbital's potential / density (ISF grid)
     long long sP;    // scratch element offsets: P (G3*F2*F1)
     long long sQ;    //   Q / Z1 (G3*I2*I1)
     long long sZ;    //   Z2 (G3*F2*F1)
     double c;        // shift of (T + c), preconditioner only
+    // optional absolute buffers (a batch that spans several owners' arrays);
+    // when set they replace base + offset
+    const void *in_ptr;
+    void *out_ptr;
+    const void *pot_ptr;
 };
+
+enum FusedMode { MODE_LOCHAM = 0, MODE_LOCDEN = 1, MODE_PRECOND = 2 };
 
 // Host view of an uploaded batch (plan) — owned by the context.
 struct Plan {
@@ -63,6 +70,26 @@ struct Plan {
     int n_work13 = 0, n_work2 = 0;
     int *d_part_slot13 = nullptr;  // slot of each plane CTA in the energy partials
     int *d_part_slot2 = nullptr;
+    // preconditioner: z-kernel items of the kinetic chain only
+    int4 *d_work2p = nullptr;
+    int *d_part_slot2p = nullptr;
+    int n_work2p = 0;
+    // density: z-kernel items {chunk, x0, y0, -} over groups of orbitals that
+    // share one density grid (same region, same pot_offset), split in chunks
+    int4 *d_workd = nullptr;
+    int n_workd = 0;
+    int nchunk = 0, ngroup = 0;
+    int *d_chunk_orb_start = nullptr;    // nchunk + 1 offsets into d_chunk_orbs
+    int *d_chunk_orbs = nullptr;
+    long long *d_chunk_part = nullptr;   // element offset of each chunk's partial density
+    long long part_den_elems = 0;
+    int *d_group_chunk_start = nullptr;  // ngroup + 1 chunk ranges
+    long long *d_group_rho = nullptr;    // density offset of each group
+    int *d_group_n = nullptr;            // ISF points of each group
+    int max_group_n = 0;
+    // per-orbital compressed vector offset / length (preconditioner vector ops)
+    long long *d_orb_off = nullptr;
+    int *d_orb_len = nullptr;
     int part_stride = 0;           // energy partial slots per orbital
     size_t smem13[2] = {0, 0};     // dynamic smem bytes (float, double)
     size_t smem2[2] = {0, 0};

@@ -219,6 +219,9 @@ extern "C" int wvlh_locham_noalloc(int precision, const int n[3], const int peri
     O.sQ = sP;
     O.sZ = sP + sQ;
     O.c = 0.0;
+    O.in_ptr = nullptr;
+    O.out_ptr = nullptr;
+    O.pot_ptr = nullptr;
     cudaError_t e = cudaSuccess;
 #define NA_CK(x)                                  \
     do {                                          \

@@ -67,7 +67,7 @@ WVLH_SYMBOLS = [
     "wvlh_batch_psi_size", "wvlh_batch_psi_offset", "wvlh_batch_scratch_bytes", "wvlh_locham_batched",
     "wvlh_locham_batched_host", "wvlh_locham_plain_batched", "wvlh_host_alloc", "wvlh_host_free",
     "wvlh_ctx_enable_timing", "wvlh_ctx_kernel_times", "wvlh_measure_fma_peak",
-    "wvlh_locham_noalloc", "wvlh_noalloc_capacity",
+    "wvlh_locham_noalloc", "wvlh_noalloc_capacity", "wvlh_locden_batched", "wvlh_precond_batched",
 ]
 
 
@@ -107,6 +107,8 @@ def lib():
     L.wvlh_locham_noalloc.argtypes = [C.c_int, ip, ip, dp, C.c_int, i32p, i32p, C.c_int, i32p, i32p,
                                       vp, vp, vp, vp, vp, vp]
     L.wvlh_noalloc_capacity.restype = C.c_size_t
+    L.wvlh_locden_batched.argtypes = [vp, C.c_int, vp, vp, vp]
+    L.wvlh_precond_batched.argtypes = [vp, C.c_int, C.c_int, vp, vp, vp, vp]
     L.wvlh_host_alloc.restype = vp
     L.wvlh_host_alloc.argtypes = [C.c_size_t]
     L.wvlh_host_free.argtypes = [vp]

@@ -125,6 +125,31 @@ class Batch:
                                             addr(epot))
         check(rc, "wvlh_locham_batched_host")
 
+    def locden(self, psi, hfac, rho):
+        """rho[pot_offset[o] + r] += hfac[o] |psi_o(r)|^2 (rho FP64 device tensor, accumulated)."""
+        torch = self.ctx.torch
+        prec = {torch.float32: 32, torch.float64: 64}[psi.dtype]
+        hf = torch.as_tensor(hfac, dtype=torch.float64, device=psi.device).contiguous()
+        if rho.dtype != torch.float64 or rho.numel() < self.pot_size:
+            raise WvlhError("rho must be a float64 tensor covering every density grid")
+        check(lib().wvlh_locden_batched(self.h, prec, _ptr(psi), _ptr(hf), _ptr(rho)), "wvlh_locden_batched")
+        self._keep_hf = hf
+        return rho
+
+    def precond(self, x, rhs, cprec, ncong, hist=None):
+        """ncong CG iterations of the preconditioner for every orbital; x is
+        overwritten with the result.  Returns x and the (ncong+1, norb)
+        squared residual norms."""
+        torch = self.ctx.torch
+        prec = {torch.float32: 32, torch.float64: 64}[x.dtype]
+        c = torch.as_tensor(cprec, dtype=torch.float64, device=x.device).contiguous()
+        if hist is None:
+            hist = torch.zeros(ncong + 1, self.norb, dtype=torch.float64, device=x.device)
+        check(lib().wvlh_precond_batched(self.h, prec, int(ncong), _ptr(c), _ptr(x), _ptr(rhs), _ptr(hist)),
+              "wvlh_precond_batched")
+        self._keep_c = c
+        return x, hist
+
     def locham_plain(self, psi, pot, hpsi=None, ekin=None, epot=None):
         """FP64, one kernel per 1D pass (the OpenCL backend's structure)."""
         torch = self.ctx.torch

@@ -253,6 +253,21 @@ int wvlh_locham_batched(wvlh_batch *batch, int precision, const void *psi, const
 /* same with HOST buffers: copies in, computes, copies out, synchronises */
 int wvlh_locham_batched_host(wvlh_batch *batch, int precision, const void *psi, const void *pot, void *hpsi,
                              double *ekin, double *epot);
+/* Density of all orbitals: rho[pot_offset[o] + r] += hfac[o] * |psi_o(r)|^2 on
+ * the ISF grid (local_partial_density, sumrho.f90:377-577; ocl_locden_generic,
+ * OpenCL/Density.c:37).  hfac: device array of norb doubles (kwgt*occ/vol);
+ * rho: device FP64, accumulated.  Orbitals sharing a density offset must share
+ * their region.  Fixed summation order: deterministic. */
+int wvlh_locden_batched(wvlh_batch *batch, int precision, const void *psi, const double *hfac, double *rho);
+/* Preconditioner of all orbitals: ncong CG iterations on
+ * D^-1/2 A (c_o + T) S D^-1/2 x = rhs, then x *= D^-1/2, per orbital, exactly the
+ * recurrence of ocl_preconditioner_generic (OpenCL/Preconditioner.c:130-195)
+ * with the shifts c_o = cprec[o] (device, norb doubles).  x (in: initial guess,
+ * out: result) and rhs are device arrays in the batch layout; hist (optional,
+ * device, (ncong+1)*norb doubles) receives the squared residual norms, entry 0
+ * the initial one.  Scalars stay on the device: no host synchronisation. */
+int wvlh_precond_batched(wvlh_batch *batch, int precision, int ncong, const double *cprec, void *x, const void *rhs,
+                         double *hist);
 /* FP64, one kernel per 1D pass (the OpenCL backend's structure) */
 int wvlh_locham_plain_batched(wvlh_batch *batch, const double *psi, const double *pot, double *hpsi,
                               double *ekin, double *epot);
