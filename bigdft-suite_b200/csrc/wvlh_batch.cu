@@ -48,7 +48,7 @@ struct DevBuf {
 struct wvlh_ctx {
     int device = 0;
     cudaStream_t stream = 0;
-    DevBuf cg_r, cg_d, cg_ad, cg_scal, den_part;
+    DevBuf cg_r, cg_d, cg_ad, cg_scal, den_part, ov_work;
     // optional per-kernel timing of the fused locham (K1, K2, K3, reduction)
     int timing = 0;
     cudaEvent_t ev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
@@ -111,6 +111,7 @@ extern "C" int wvlh_ctx_destroy(wvlh_ctx *ctx)
     ctx->cg_ad.release();
     ctx->cg_scal.release();
     ctx->den_part.release();
+    ctx->ov_work.release();
     for (auto &e : ctx->ev)
         if (e) cudaEventDestroy(e);
     delete ctx;
@@ -534,6 +535,31 @@ extern "C" int wvlh_precond_batched(wvlh_batch *b, int precision, int ncong, con
            : launch_precond<float>(p, ncong, cprec, (float *)x, (const float *)rhs, (float *)c->cg_r.p,
                                    (float *)c->cg_d.p, (float *)c->cg_ad.p, (float *)c->scratch.p,
                                    (double *)c->cg_scal.p, hist, c->stream);
+    CK(e);
+    return WVLH_OK;
+}
+
+namespace wvlh {
+size_t overlap_workspace_bytes(int norb, long long K, int nsm);
+template <class TI>
+cudaError_t launch_overlap(int norb, long long K, long long ld, const TI *psi, double *S, double *work, int nsm,
+                           cudaStream_t st);
+}  // namespace wvlh
+
+extern "C" int wvlh_overlap(wvlh_ctx *c, int precision, int norb, int64_t K, int64_t ld, const void *psi, double *S)
+{
+    if (!c || !psi || !S || norb <= 0 || K <= 0 || ld < K || (precision != 32 && precision != 64))
+        return fail(WVLH_ERR_ARG);
+    CK(cudaSetDevice(c->device));
+    int nsm = 0;
+    CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c->device));
+    int rc;
+    if ((rc = c->ov_work.ensure(overlap_workspace_bytes(norb, K, nsm)))) return fail(rc);
+    cudaError_t e = precision == 64
+                        ? launch_overlap<double>(norb, K, ld, (const double *)psi, S, (double *)c->ov_work.p, nsm,
+                                                 c->stream)
+                        : launch_overlap<float>(norb, K, ld, (const float *)psi, S, (double *)c->ov_work.p, nsm,
+                                                c->stream);
     CK(e);
     return WVLH_OK;
 }

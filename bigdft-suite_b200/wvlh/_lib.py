@@ -68,6 +68,7 @@ WVLH_SYMBOLS = [
     "wvlh_locham_batched_host", "wvlh_locham_plain_batched", "wvlh_host_alloc", "wvlh_host_free",
     "wvlh_ctx_enable_timing", "wvlh_ctx_kernel_times", "wvlh_measure_fma_peak",
     "wvlh_locham_noalloc", "wvlh_noalloc_capacity", "wvlh_locden_batched", "wvlh_precond_batched",
+    "wvlh_overlap",
 ]
 
 
@@ -109,6 +110,7 @@ def lib():
     L.wvlh_noalloc_capacity.restype = C.c_size_t
     L.wvlh_locden_batched.argtypes = [vp, C.c_int, vp, vp, vp]
     L.wvlh_precond_batched.argtypes = [vp, C.c_int, C.c_int, vp, vp, vp, vp]
+    L.wvlh_overlap.argtypes = [vp, C.c_int, C.c_int, C.c_int64, C.c_int64, vp, vp]
     L.wvlh_host_alloc.restype = vp
     L.wvlh_host_alloc.argtypes = [C.c_size_t]
     L.wvlh_host_free.argtypes = [vp]

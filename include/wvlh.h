@@ -268,6 +268,12 @@ int wvlh_locden_batched(wvlh_batch *batch, int precision, const void *psi, const
  * the initial one.  Scalars stay on the device: no host synchronisation. */
 int wvlh_precond_batched(wvlh_batch *batch, int precision, int ncong, const double *cprec, void *x, const void *rhs,
                          double *hist);
+/* Overlap S = Psi^T Psi (norb x norb, FP64, full symmetric, row-major) of
+ * norb coefficient rows of length K at row stride ld (device; precision 32:
+ * float rows widened to FP64, 64: double) on FP64 tensor cores; the
+ * reference's getOverlap syrk (wfn_opt/orthogonality.f90:2675) summed in a
+ * fixed order. */
+int wvlh_overlap(wvlh_ctx *ctx, int precision, int norb, int64_t K, int64_t ld, const void *psi, double *S);
 /* FP64, one kernel per 1D pass (the OpenCL backend's structure) */
 int wvlh_locham_plain_batched(wvlh_batch *batch, const double *psi, const double *pot, double *hpsi,
                               double *ekin, double *epot);
