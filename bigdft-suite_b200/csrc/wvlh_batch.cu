@@ -1,10 +1,15 @@
-// Batched ABI: contexts, batch plans (key validation and decoding, work
-// tables) and the batched local-Hamiltonian entry points.
+// Batched ABI: contexts, regions (validated and decoded keys of one
+// localisation region, resident on the device), batch plans (work tables) and
+// the batched local-Hamiltonian, density, preconditioner and overlap entry
+// points.
 #include <cuda_runtime.h>
 
 #include <algorithm>
 #include <cstdio>
 #include <cstring>
+#include <map>
+#include <type_traits>
+#include <utility>
 #include <vector>
 
 #include "../../include/wvlh.h"
@@ -18,6 +23,7 @@ cudaError_t launch_locham(const Plan &p, const TIO *psi, const TIO *pot, TIO *hp
                           double *part_kin, double *ekin, double *epot, int accumulate, cudaStream_t st,
                           cudaEvent_t *ev);
 cudaError_t fma_probe(int precision, int iters, float *ms, double *flops, cudaStream_t st);
+long long plane_tmp_elems(const Plan &p, int fp);
 void set_last_error(int code);
 }  // namespace wvlh
 
@@ -30,7 +36,11 @@ struct DevBuf {
     int ensure(size_t b)
     {
         if (b <= bytes) return WVLH_OK;
-        if (p) cudaFree(p);
+        if (p) {
+            // kernels queued earlier may still read the old buffer
+            cudaDeviceSynchronize();
+            cudaFree(p);
+        }
         p = nullptr;
         bytes = 0;
         if (cudaMalloc(&p, b) != cudaSuccess) return WVLH_ERR_NOMEM;
@@ -55,17 +65,35 @@ struct wvlh_ctx {
     double kernel_ms[4] = {0, 0, 0, 0};
     long long timed_calls = 0;
     DevBuf scratch, part_pot, part_kin, io_psi, io_pot, io_hpsi, io_e, plain[4], dotpart;
+    // tables of the orbital batches (wvlh_batch_create_orbitals): rewritten in
+    // stream order by each new batch, whose generation number it records
+    DevBuf arena;
+    unsigned long long arena_gen = 0;
+};
+
+// One localisation region: its box and its keys, validated once and kept on
+// the device in two forms: decoded {i0, i2, len, jj0} segments with per-plane
+// ranges (fused kernels) and the raw 1-based keys (one-pass-per-kernel path).
+struct wvlh_region {
+    int device = 0;
+    LrDev lr{};
+    const uint32_t *keyg_c = nullptr, *keyv_c = nullptr, *keyg_f = nullptr, *keyv_f = nullptr;
+    double hgrid[3] = {0, 0, 0};
+    void *mem = nullptr;  // one device block holding all of the above
 };
 
 struct wvlh_batch {
     wvlh_ctx *ctx = nullptr;
     Plan plan;
     std::vector<int64_t> pot_off;
-    bool density_ok = true;  // orbitals sharing a density grid share its region
-    // raw 1-based keys per region on the device (plain path)
-    std::vector<uint32_t *> d_keyg_c, d_keyv_c, d_keyg_f, d_keyv_f;
-    std::vector<int> nvc, nvf, nsc, nsf;
-    std::vector<double> hgrid;  // 3*nlr
+    bool density_ok = true;                  // orbitals sharing a density grid share its region
+    std::vector<const wvlh_region *> lr;     // region of each plan region index
+    std::vector<wvlh_region *> own_regions;  // regions made by wvlh_batch_create
+    // orbital batches: per-orbital device buffers, tables in the context arena
+    bool orbital_mode = false;
+    bool can_locham = true, can_locden = true;
+    unsigned long long arena_gen = 0;
+    void *mem = nullptr;  // owned table block (wvlh_batch_create)
 };
 
 static int fail(int code)
@@ -74,14 +102,36 @@ static int fail(int code)
     return code;
 }
 
-#define CK(x)                                                  \
-    do {                                                       \
-        cudaError_t e_ = (x);                                  \
-        if (e_ != cudaSuccess) {                               \
+#define CK(x)                                                      \
+    do {                                                           \
+        cudaError_t e_ = (x);                                      \
+        if (e_ != cudaSuccess) {                                   \
             fprintf(stderr, "wvlh: %s\n", cudaGetErrorString(e_)); \
-            return fail(WVLH_ERR_CUDA);                        \
-        }                                                      \
+            return fail(WVLH_ERR_CUDA);                            \
+        }                                                          \
     } while (0)
+
+// Host image of a set of device tables at 256-byte aligned offsets of one
+// device block; the pointers are set once the block's address is known.
+struct Packer {
+    std::vector<unsigned char> img;
+    std::vector<std::pair<void **, size_t>> fix;
+    template <class T, class P>
+    void add(const std::vector<T> &v, P **dst)
+    {
+        static_assert(sizeof(T) == sizeof(P), "table element type");
+        *dst = nullptr;
+        if (v.empty()) return;
+        const size_t off = (img.size() + 255) & ~size_t(255);
+        img.resize(off + v.size() * sizeof(T));
+        memcpy(img.data() + off, v.data(), v.size() * sizeof(T));
+        fix.emplace_back(reinterpret_cast<void **>(const_cast<std::remove_const_t<P> **>(dst)), off);
+    }
+    void place(void *base)
+    {
+        for (auto &f : fix) *f.first = static_cast<unsigned char *>(base) + f.second;
+    }
+};
 
 extern "C" int wvlh_ctx_create(int device, wvlh_ctx **ctx)
 {
@@ -97,21 +147,12 @@ extern "C" int wvlh_ctx_destroy(wvlh_ctx *ctx)
 {
     if (!ctx) return WVLH_OK;
     cudaSetDevice(ctx->device);
-    ctx->scratch.release();
-    ctx->part_pot.release();
-    ctx->part_kin.release();
-    ctx->io_psi.release();
-    ctx->io_pot.release();
-    ctx->io_hpsi.release();
-    ctx->io_e.release();
+    cudaStreamSynchronize(ctx->stream);
+    for (DevBuf *b : {&ctx->scratch, &ctx->part_pot, &ctx->part_kin, &ctx->io_psi, &ctx->io_pot, &ctx->io_hpsi,
+                      &ctx->io_e, &ctx->dotpart, &ctx->cg_r, &ctx->cg_d, &ctx->cg_ad, &ctx->cg_scal, &ctx->den_part,
+                      &ctx->ov_work, &ctx->arena})
+        b->release();
     for (auto &b : ctx->plain) b.release();
-    ctx->dotpart.release();
-    ctx->cg_r.release();
-    ctx->cg_d.release();
-    ctx->cg_ad.release();
-    ctx->cg_scal.release();
-    ctx->den_part.release();
-    ctx->ov_work.release();
     for (auto &e : ctx->ev)
         if (e) cudaEventDestroy(e);
     delete ctx;
@@ -138,6 +179,7 @@ static int decode_keys(const int *N, int nseg, const int32_t *keyg, const int32_
                        std::vector<int> &plane, int &nvctr)
 {
     const long long n12 = (long long)N[0] * N[1], ntot = n12 * N[2];
+    if (nseg > 0 && (!keyg || !keyv)) return WVLH_ERR_ARG;
     seg.resize(nseg);
     plane.assign(N[2] + 1, nseg);
     long long prev_end = 0;
@@ -164,89 +206,130 @@ static int decode_keys(const int *N, int nseg, const int32_t *keyg, const int32_
     return WVLH_OK;
 }
 
-template <class T>
-static int upload(Plan &p, const std::vector<T> &v, T **dst)
+static void region_free(wvlh_region *r)
 {
-    *dst = nullptr;
-    if (v.empty()) return WVLH_OK;
-    if (cudaMalloc(dst, v.size() * sizeof(T)) != cudaSuccess) return WVLH_ERR_NOMEM;
-    p.owned.push_back(*dst);
-    if (cudaMemcpy(*dst, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice) != cudaSuccess) return WVLH_ERR_CUDA;
+    if (!r) return;
+    if (r->mem) {
+        cudaSetDevice(r->device);
+        cudaFree(r->mem);
+    }
+    delete r;
+}
+
+// Validate, decode and upload the keys of one region (one device block).
+static int region_make(int device, const wvlh_locreg &L, wvlh_region **out)
+{
+    *out = nullptr;
+    for (int k = 0; k < 3; ++k) {
+        if (L.n[k] < 1 || L.n[k] > 1024) return WVLH_ERR_ARG;
+        // the periodic analysis/synthesis index arithmetic assumes at least 8 coarse cells
+        if (L.periodic[k] && L.n[k] < 8) return WVLH_ERR_ARG;
+    }
+    if (L.nseg_c < 0 || L.nseg_f < 0) return WVLH_ERR_ARG;
+    std::vector<int4> sc, sf;
+    std::vector<int> pc, pf;
+    int nvc = 0, nvf = 0, rc;
+    if ((rc = decode_keys(L.n, L.nseg_c, L.keyg_c, L.keyv_c, sc, pc, nvc))) return rc;
+    if ((rc = decode_keys(L.n, L.nseg_f, L.keyg_f, L.keyv_f, sf, pf, nvf))) return rc;
+    wvlh_region *r = new wvlh_region();
+    r->device = device;
+    LrDev &d = r->lr;
+    for (int k = 0; k < 3; ++k) {
+        d.N[k] = L.n[k];
+        d.per[k] = L.periodic[k] ? 1 : 0;
+        d.hgrid[k] = L.hgrid[k];
+        r->hgrid[k] = L.hgrid[k];
+    }
+    d.nseg_c = L.nseg_c;
+    d.nseg_f = L.nseg_f;
+    d.nvctr_c = nvc;
+    d.nvctr_f = nvf;
+    std::vector<uint32_t> kgc(L.keyg_c, L.keyg_c + 2 * (size_t)L.nseg_c), kvc(L.keyv_c, L.keyv_c + L.nseg_c);
+    std::vector<uint32_t> kgf(L.keyg_f, L.keyg_f + 2 * (size_t)L.nseg_f), kvf(L.keyv_f, L.keyv_f + L.nseg_f);
+    Packer pk;
+    pk.add(sc, &d.seg_c);
+    pk.add(sf, &d.seg_f);
+    pk.add(pc, &d.plane_c);
+    pk.add(pf, &d.plane_f);
+    pk.add(kgc, &r->keyg_c);
+    pk.add(kvc, &r->keyv_c);
+    pk.add(kgf, &r->keyg_f);
+    pk.add(kvf, &r->keyv_f);
+    if (cudaMalloc(&r->mem, pk.img.size()) != cudaSuccess) {
+        r->mem = nullptr;
+        region_free(r);
+        return WVLH_ERR_NOMEM;
+    }
+    if (cudaMemcpy(r->mem, pk.img.data(), pk.img.size(), cudaMemcpyHostToDevice) != cudaSuccess) {
+        region_free(r);
+        return WVLH_ERR_CUDA;
+    }
+    pk.place(r->mem);
+    *out = r;
     return WVLH_OK;
 }
 
-extern "C" int wvlh_batch_create(wvlh_ctx *ctx, int nlr, const wvlh_locreg *lrs, int norb, const int32_t *orb_lr,
-                                 const int64_t *pot_offset, wvlh_batch **out)
+extern "C" int wvlh_region_create(wvlh_ctx *ctx, const wvlh_locreg *lr, wvlh_region **out)
 {
-    if (!ctx || !lrs || nlr <= 0 || norb <= 0 || !orb_lr || !out) return fail(WVLH_ERR_ARG);
+    if (!ctx || !lr || !out) return fail(WVLH_ERR_ARG);
     CK(cudaSetDevice(ctx->device));
-    wvlh_batch *b = new wvlh_batch();
-    b->ctx = ctx;
+    const int rc = region_make(ctx->device, *lr, out);
+    return rc ? fail(rc) : WVLH_OK;
+}
+
+extern "C" int wvlh_region_destroy(wvlh_region *r)
+{
+    region_free(r);
+    return WVLH_OK;
+}
+
+extern "C" int64_t wvlh_region_psi_size(const wvlh_region *r)
+{
+    return r ? r->lr.nvctr_c + 7LL * r->lr.nvctr_f : -1;
+}
+
+extern "C" int64_t wvlh_region_grid_size(const wvlh_region *r)
+{
+    if (!r) return -1;
+    long long n = 1;
+    for (int k = 0; k < 3; ++k) n *= isf_len(r->lr.N[k], r->lr.per[k]);
+    return n;
+}
+
+// scratch elements of one orbital of a region in the fused kernels (P, Q, Z)
+static long long orbital_scratch(const LrDev &d)
+{
+    const int G3 = 2 * d.N[2];
+    const int F1 = fine_len(d.N[0], d.per[0]), F2 = fine_len(d.N[1], d.per[1]);
+    const int I1 = isf_len(d.N[0], d.per[0]), I2 = isf_len(d.N[1], d.per[1]);
+    return (long long)G3 * F2 * F1 * 2 + (long long)G3 * I2 * I1;
+}
+
+extern "C" int64_t wvlh_region_scratch_bytes(const wvlh_region *r, int precision)
+{
+    return r ? orbital_scratch(r->lr) * (precision == 32 ? 4 : 8) : -1;
+}
+
+// Lay out the orbitals of a batch over its regions (b->lr): scratch slices,
+// fused-kernel work lists, energy partial slots, density groups and chunks.
+// pot_key[o]: element offset of the orbital's potential (packed mode);
+// den_key[o]: identity of its density grid (offset, or address in orbital
+// mode); abs: per-orbital buffers (orbital mode) or null.
+static void layout(wvlh_batch *b, const std::vector<int> &orb_lr, const std::vector<long long> &pot_key,
+                   const std::vector<long long> &den_key, const wvlh_orbital *abs, Packer &pk)
+{
     Plan &p = b->plan;
+    const int nlr = (int)b->lr.size(), norb = (int)orb_lr.size();
     p.nlr = nlr;
     p.norb = norb;
     std::vector<LrDev> lrd(nlr);
-    b->hgrid.resize(3 * nlr);
-    int rc = WVLH_OK;
-    for (int l = 0; l < nlr && rc == WVLH_OK; ++l) {
-        const wvlh_locreg &L = lrs[l];
-        LrDev &d = lrd[l];
+    for (int l = 0; l < nlr; ++l) {
+        lrd[l] = b->lr[l]->lr;
         for (int k = 0; k < 3; ++k) {
-            if (L.n[k] < 1 || L.n[k] > 1024) rc = WVLH_ERR_ARG;
-            // the periodic analysis/synthesis index arithmetic assumes at least 8 coarse cells
-            if (L.periodic[k] && L.n[k] < 8) rc = WVLH_ERR_ARG;
-            d.N[k] = L.n[k];
-            d.per[k] = L.periodic[k] ? 1 : 0;
-            d.hgrid[k] = L.hgrid[k];
-            b->hgrid[3 * l + k] = L.hgrid[k];
-            p.lr_N.push_back(L.n[k]);
-            p.lr_per.push_back(d.per[k]);
+            p.lr_N.push_back(lrd[l].N[k]);
+            p.lr_per.push_back(lrd[l].per[k]);
         }
-        if (rc) break;
-        std::vector<int4> sc, sf;
-        std::vector<int> pc, pf;
-        int nvc = 0, nvf = 0;
-        if (L.nseg_c < 0 || L.nseg_f < 0) rc = WVLH_ERR_ARG;
-        if (!rc) rc = decode_keys(L.n, L.nseg_c, L.keyg_c, L.keyv_c, sc, pc, nvc);
-        if (!rc) rc = decode_keys(L.n, L.nseg_f, L.keyg_f, L.keyv_f, sf, pf, nvf);
-        if (rc) break;
-        d.nseg_c = L.nseg_c;
-        d.nseg_f = L.nseg_f;
-        d.nvctr_c = nvc;
-        d.nvctr_f = nvf;
-        int4 *dsc, *dsf;
-        int *dpc, *dpf;
-        if ((rc = upload(p, sc, &dsc)) || (rc = upload(p, sf, &dsf)) || (rc = upload(p, pc, &dpc)) ||
-            (rc = upload(p, pf, &dpf)))
-            break;
-        d.seg_c = dsc;
-        d.seg_f = dsf;
-        d.plane_c = dpc;
-        d.plane_f = dpf;
-        // raw keys for the plain path
-        std::vector<uint32_t> kgc(2 * (size_t)L.nseg_c), kvc(L.nseg_c), kgf(2 * (size_t)L.nseg_f), kvf(L.nseg_f);
-        for (int s = 0; s < 2 * L.nseg_c; ++s) kgc[s] = (uint32_t)L.keyg_c[s];
-        for (int s = 0; s < L.nseg_c; ++s) kvc[s] = (uint32_t)L.keyv_c[s];
-        for (int s = 0; s < 2 * L.nseg_f; ++s) kgf[s] = (uint32_t)L.keyg_f[s];
-        for (int s = 0; s < L.nseg_f; ++s) kvf[s] = (uint32_t)L.keyv_f[s];
-        uint32_t *a, *bb, *c, *dd;
-        if ((rc = upload(p, kgc, &a)) || (rc = upload(p, kvc, &bb)) || (rc = upload(p, kgf, &c)) ||
-            (rc = upload(p, kvf, &dd)))
-            break;
-        b->d_keyg_c.push_back(a);
-        b->d_keyv_c.push_back(bb);
-        b->d_keyg_f.push_back(c);
-        b->d_keyv_f.push_back(dd);
-        b->nvc.push_back(nvc);
-        b->nvf.push_back(nvf);
-        b->nsc.push_back(L.nseg_c);
-        b->nsf.push_back(L.nseg_f);
     }
-    if (rc) {
-        wvlh_batch_destroy(b);
-        return fail(rc);
-    }
-    // orbitals, scratch layout, work tables
     std::vector<OrbDev> od(norb);
     std::vector<int2> w13;
     std::vector<int> s13;
@@ -256,13 +339,9 @@ extern "C" int wvlh_batch_create(wvlh_ctx *ctx, int nlr, const wvlh_locreg *lrs,
     long long psi_off = 0, scr = 0;
     int stride = 0;
     size_t sm13_elems = 0, sm2_elems = 0;
-    b->pot_off.resize(norb);
+    b->pot_off.assign(pot_key.begin(), pot_key.end());
     for (int o = 0; o < norb; ++o) {
         const int l = orb_lr[o];
-        if (l < 0 || l >= nlr) {
-            wvlh_batch_destroy(b);
-            return fail(WVLH_ERR_ARG);
-        }
         const LrDev &d = lrd[l];
         const int N1 = d.N[0], N2 = d.N[1], N3 = d.N[2];
         const int G1 = 2 * N1, G2 = 2 * N2, G3 = 2 * N3;
@@ -270,9 +349,9 @@ extern "C" int wvlh_batch_create(wvlh_ctx *ctx, int nlr, const wvlh_locreg *lrs,
         const int I1 = isf_len(N1, d.per[0]), I2 = isf_len(N2, d.per[1]), I3 = isf_len(N3, d.per[2]);
         OrbDev &q = od[o];
         q.lr = l;
+        q.pad = 0;
         q.psi = psi_off;
-        q.pot = pot_offset ? pot_offset[o] : 0;
-        b->pot_off[o] = q.pot;
+        q.pot = pot_key[o];
         q.sP = scr;
         scr += (long long)G3 * F2 * F1;
         q.sQ = scr;
@@ -280,9 +359,15 @@ extern "C" int wvlh_batch_create(wvlh_ctx *ctx, int nlr, const wvlh_locreg *lrs,
         q.sZ = scr;
         scr += (long long)G3 * F2 * F1;
         q.c = 0.0;
+        q.in_ptr = abs ? abs[o].psi : nullptr;
+        q.out_ptr = abs ? abs[o].hpsi : nullptr;
+        q.pot_ptr = abs ? abs[o].pot : nullptr;
         p.orb_lr.push_back(l);
         p.orb_psi.push_back(psi_off);
-        psi_off += d.nvctr_c + 7LL * d.nvctr_f;
+        const int len = d.nvctr_c + 7 * d.nvctr_f;
+        orb_off.push_back(psi_off);
+        orb_len.push_back(len);
+        psi_off += len;
         const int ntx0 = (I1 + TX_ - 1) / TX_, nty0 = (I2 + TY_ - 1) / TY_;
         const int ntx1 = (F1 + TX_ - 1) / TX_, nty1 = (F2 + TY_ - 1) / TY_;
         for (int ty = 0; ty < nty0; ++ty)
@@ -297,8 +382,6 @@ extern "C" int wvlh_batch_create(wvlh_ctx *ctx, int nlr, const wvlh_locreg *lrs,
                 w2p.push_back(make_int4(o, 1, tx * TX_, ty * TY_));
                 s2p.push_back(ty * ntx1 + tx);
             }
-        orb_off.push_back(psi_off - (d.nvctr_c + 7LL * d.nvctr_f));
-        orb_len.push_back(d.nvctr_c + 7 * d.nvctr_f);
         for (int kz = 0; kz < G3; ++kz) {
             w13.push_back(make_int2(o, kz));
             s13.push_back(ntx1 * nty1 + kz);
@@ -315,6 +398,7 @@ extern "C" int wvlh_batch_create(wvlh_ctx *ctx, int nlr, const wvlh_locreg *lrs,
     for (int v : p.lr_per) p.all_periodic = p.all_periodic && v == 1;
     p.scratch_elems = scr;
     p.part_stride = stride;
+    p.plane_elems = (long long)(sm13_elems / 2);
     p.smem13[0] = sm13_elems * sizeof(float);
     p.smem13[1] = sm13_elems * sizeof(double);
     p.smem2[0] = sm2_elems * sizeof(float);
@@ -322,13 +406,13 @@ extern "C" int wvlh_batch_create(wvlh_ctx *ctx, int nlr, const wvlh_locreg *lrs,
     p.n_work13 = (int)w13.size();
     p.n_work2 = (int)w2.size();
     p.n_work2p = (int)w2p.size();
-    // density: group the orbitals by density grid (same region and offset),
+    // density: group the orbitals by density grid (same key, one region),
     // split each group in chunks of at most kDenChunk orbitals
     constexpr int kDenChunk = 32;
     std::vector<int> order(norb);
     for (int o = 0; o < norb; ++o) order[o] = o;
     std::stable_sort(order.begin(), order.end(), [&](int a, int c) {
-        return b->pot_off[a] != b->pot_off[c] ? b->pot_off[a] < b->pot_off[c] : orb_lr[a] < orb_lr[c];
+        return den_key[a] != den_key[c] ? den_key[a] < den_key[c] : orb_lr[a] < orb_lr[c];
     });
     std::vector<int> chunk_start, chunk_orbs, group_chunk_start, group_n;
     std::vector<long long> chunk_part, group_rho;
@@ -337,15 +421,17 @@ extern "C" int wvlh_batch_create(wvlh_ctx *ctx, int nlr, const wvlh_locreg *lrs,
     b->density_ok = true;
     for (int i = 0; i < norb;) {
         int j = i;
-        while (j < norb && b->pot_off[order[j]] == b->pot_off[order[i]]) {
+        while (j < norb && den_key[order[j]] == den_key[order[i]]) {
             if (orb_lr[order[j]] != orb_lr[order[i]]) b->density_ok = false;  // one grid, one region
             ++j;
         }
         const LrDev &d = lrd[orb_lr[order[i]]];
         const int I1 = isf_len(d.N[0], d.per[0]), I2 = isf_len(d.N[1], d.per[1]), I3 = isf_len(d.N[2], d.per[2]);
-        if (I3 * TX_ * TY_ > 32 * kZThreads) b->density_ok = false;   // accumulators of kd_density
+        // accumulators of kd_density: 32 per thread, 48 for the larger grids
+        if (I3 * TX_ * TY_ > 48 * kZThreads) b->density_ok = false;
+        if (I3 * TX_ * TY_ > 32 * kZThreads) p.den_acc = 48;
         group_chunk_start.push_back((int)chunk_start.size());
-        group_rho.push_back(b->pot_off[order[i]]);
+        group_rho.push_back(den_key[order[i]]);
         group_n.push_back(I1 * I2 * I3);
         p.max_group_n = std::max(p.max_group_n, I1 * I2 * I3);
         // a group of many orbitals is split in up to 8 chunks (one partial
@@ -371,17 +457,103 @@ extern "C" int wvlh_batch_create(wvlh_ctx *ctx, int nlr, const wvlh_locreg *lrs,
     p.ngroup = (int)group_rho.size();
     p.part_den_elems = den;
     p.n_workd = (int)wd.size();
-    if ((rc = upload(p, lrd, &p.d_lr)) || (rc = upload(p, od, &p.d_orb)) || (rc = upload(p, w13, &p.d_work13)) ||
-        (rc = upload(p, s13, &p.d_part_slot13)) || (rc = upload(p, w2, &p.d_work2)) ||
-        (rc = upload(p, s2, &p.d_part_slot2)) || (rc = upload(p, w2p, &p.d_work2p)) ||
-        (rc = upload(p, s2p, &p.d_part_slot2p)) || (rc = upload(p, wd, &p.d_workd)) ||
-        (rc = upload(p, chunk_start, &p.d_chunk_orb_start)) || (rc = upload(p, chunk_orbs, &p.d_chunk_orbs)) ||
-        (rc = upload(p, chunk_part, &p.d_chunk_part)) || (rc = upload(p, group_chunk_start, &p.d_group_chunk_start)) ||
-        (rc = upload(p, group_rho, &p.d_group_rho)) || (rc = upload(p, group_n, &p.d_group_n)) ||
-        (rc = upload(p, orb_off, &p.d_orb_off)) || (rc = upload(p, orb_len, &p.d_orb_len))) {
+    pk.add(lrd, &p.d_lr);
+    pk.add(od, &p.d_orb);
+    pk.add(w13, &p.d_work13);
+    pk.add(s13, &p.d_part_slot13);
+    pk.add(w2, &p.d_work2);
+    pk.add(s2, &p.d_part_slot2);
+    pk.add(w2p, &p.d_work2p);
+    pk.add(s2p, &p.d_part_slot2p);
+    pk.add(wd, &p.d_workd);
+    pk.add(chunk_start, &p.d_chunk_orb_start);
+    pk.add(chunk_orbs, &p.d_chunk_orbs);
+    pk.add(chunk_part, &p.d_chunk_part);
+    pk.add(group_chunk_start, &p.d_group_chunk_start);
+    pk.add(group_rho, &p.d_group_rho);
+    pk.add(group_n, &p.d_group_n);
+    pk.add(orb_off, &p.d_orb_off);
+    pk.add(orb_len, &p.d_orb_len);
+}
+
+extern "C" int wvlh_batch_create(wvlh_ctx *ctx, int nlr, const wvlh_locreg *lrs, int norb, const int32_t *orb_lr,
+                                 const int64_t *pot_offset, wvlh_batch **out)
+{
+    if (!ctx || !lrs || nlr <= 0 || norb <= 0 || !orb_lr || !out) return fail(WVLH_ERR_ARG);
+    for (int o = 0; o < norb; ++o)
+        if (orb_lr[o] < 0 || orb_lr[o] >= nlr) return fail(WVLH_ERR_ARG);
+    CK(cudaSetDevice(ctx->device));
+    wvlh_batch *b = new wvlh_batch();
+    b->ctx = ctx;
+    for (int l = 0; l < nlr; ++l) {
+        wvlh_region *r = nullptr;
+        const int rc = region_make(ctx->device, lrs[l], &r);
+        if (rc) {
+            wvlh_batch_destroy(b);
+            return fail(rc);
+        }
+        b->own_regions.push_back(r);
+        b->lr.push_back(r);
+    }
+    std::vector<int> ol(orb_lr, orb_lr + norb);
+    std::vector<long long> pk_pot(norb);
+    for (int o = 0; o < norb; ++o) pk_pot[o] = pot_offset ? pot_offset[o] : 0;
+    Packer pk;
+    layout(b, ol, pk_pot, pk_pot, nullptr, pk);
+    if (cudaMalloc(&b->mem, pk.img.size()) != cudaSuccess) {
+        b->mem = nullptr;
+        wvlh_batch_destroy(b);
+        return fail(WVLH_ERR_NOMEM);
+    }
+    if (cudaMemcpy(b->mem, pk.img.data(), pk.img.size(), cudaMemcpyHostToDevice) != cudaSuccess) {
+        wvlh_batch_destroy(b);
+        return fail(WVLH_ERR_CUDA);
+    }
+    pk.place(b->mem);
+    *out = b;
+    return WVLH_OK;
+}
+
+extern "C" int wvlh_batch_create_orbitals(wvlh_ctx *ctx, int norb, const wvlh_orbital *orbs, wvlh_batch **out)
+{
+    if (!ctx || norb <= 0 || !orbs || !out) return fail(WVLH_ERR_ARG);
+    std::map<const wvlh_region *, int> index;
+    std::vector<int> ol(norb);
+    std::vector<long long> pot(norb, 0), den(norb);
+    bool locham = true, locden = true;
+    for (int o = 0; o < norb; ++o) {
+        const wvlh_orbital &q = orbs[o];
+        if (!q.region || q.region->device != ctx->device || !q.psi) return fail(WVLH_ERR_ARG);
+        auto it = index.find(q.region);
+        ol[o] = it != index.end() ? it->second : (index[q.region] = (int)index.size());
+        den[o] = (long long)(uintptr_t)q.rho;
+        locham = locham && q.hpsi && q.pot;
+        locden = locden && q.rho;
+    }
+    CK(cudaSetDevice(ctx->device));
+    wvlh_batch *b = new wvlh_batch();
+    b->ctx = ctx;
+    b->orbital_mode = true;
+    b->lr.resize(index.size());
+    for (auto &kv : index) b->lr[kv.second] = kv.first;
+    Packer pk;
+    layout(b, ol, pot, den, orbs, pk);
+    b->can_locham = locham;
+    b->can_locden = locden && b->density_ok;
+    // the tables replace the previous batch's in the context arena, in stream
+    // order: launches queued before this call still read the old tables
+    int rc = ctx->arena.ensure(pk.img.size());
+    if (rc) {
         wvlh_batch_destroy(b);
         return fail(rc);
     }
+    if (cudaMemcpyAsync(ctx->arena.p, pk.img.data(), pk.img.size(), cudaMemcpyHostToDevice, ctx->stream) !=
+        cudaSuccess) {
+        wvlh_batch_destroy(b);
+        return fail(WVLH_ERR_CUDA);
+    }
+    pk.place(ctx->arena.p);
+    b->arena_gen = ++ctx->arena_gen;
     *out = b;
     return WVLH_OK;
 }
@@ -389,7 +561,11 @@ extern "C" int wvlh_batch_create(wvlh_ctx *ctx, int nlr, const wvlh_locreg *lrs,
 extern "C" int wvlh_batch_destroy(wvlh_batch *b)
 {
     if (!b) return WVLH_OK;
-    for (void *q : b->plan.owned) cudaFree(q);
+    if (b->mem) {
+        cudaSetDevice(b->ctx->device);
+        cudaFree(b->mem);
+    }
+    for (wvlh_region *r : b->own_regions) region_free(r);
     delete b;
     return WVLH_OK;
 }
@@ -404,6 +580,13 @@ extern "C" int64_t wvlh_batch_scratch_bytes(const wvlh_batch *b, int precision)
     return b ? b->plan.scratch_elems * (precision == 32 ? 4 : 8) : -1;
 }
 
+// an orbital batch's tables stay valid until the next orbital batch of its context
+static int batch_usable(const wvlh_batch *b)
+{
+    if (b->orbital_mode && b->arena_gen != b->ctx->arena_gen) return WVLH_ERR_STALE;
+    return WVLH_OK;
+}
+
 static size_t sm_limit()
 {
     int dev = 0, v = 0;
@@ -415,15 +598,18 @@ static size_t sm_limit()
 extern "C" int wvlh_locham_batched(wvlh_batch *b, int precision, const void *psi, const void *pot, void *hpsi,
                                    double *ekin, double *epot, int accumulate)
 {
-    if (!b || !psi || !pot || !hpsi || (precision != 32 && precision != 64)) return fail(WVLH_ERR_ARG);
+    if (!b || (precision != 32 && precision != 64)) return fail(WVLH_ERR_ARG);
+    // orbital batches carry their buffers per orbital; packed batches need the bases
+    if (b->orbital_mode ? !b->can_locham : (!psi || !pot || !hpsi)) return fail(WVLH_ERR_ARG);
+    int rc;
+    if ((rc = batch_usable(b))) return fail(rc);
     wvlh_ctx *c = b->ctx;
     CK(cudaSetDevice(c->device));
     const Plan &p = b->plan;
     const int fp = precision == 64;
     const size_t lim = sm_limit() - 1024;
-    if (p.smem13[fp] > lim || p.smem2[fp] > lim) return fail(WVLH_ERR_TOO_LARGE);
-    int rc;
-    if ((rc = c->scratch.ensure(p.scratch_elems * (fp ? 8 : 4))) ||
+    if (p.smem13[fp] / 2 > lim || p.smem2[fp] > lim) return fail(WVLH_ERR_TOO_LARGE);
+    if ((rc = c->scratch.ensure((p.scratch_elems + plane_tmp_elems(p, fp)) * (fp ? 8 : 4))) ||
         (rc = c->part_pot.ensure(sizeof(double) * (size_t)p.norb * p.part_stride)) ||
         (rc = c->part_kin.ensure(sizeof(double) * (size_t)p.norb * p.part_stride)))
         return fail(rc);
@@ -492,16 +678,19 @@ cudaError_t launch_precond(const Plan &p, int ncong, const double *cprec, T *x, 
 
 extern "C" int wvlh_locden_batched(wvlh_batch *b, int precision, const void *psi, const double *hfac, double *rho)
 {
-    if (!b || !psi || !hfac || !rho || (precision != 32 && precision != 64)) return fail(WVLH_ERR_ARG);
+    if (!b || !hfac || (precision != 32 && precision != 64)) return fail(WVLH_ERR_ARG);
+    if (b->orbital_mode ? !b->can_locden : (!psi || !rho)) return fail(WVLH_ERR_ARG);
     if (!b->density_ok) return fail(WVLH_ERR_UNSUPPORTED);
+    int rc;
+    if ((rc = batch_usable(b))) return fail(rc);
+    if (b->orbital_mode) rho = nullptr;  // the groups hold the density addresses
     wvlh_ctx *c = b->ctx;
     CK(cudaSetDevice(c->device));
     const Plan &p = b->plan;
     const int fp = precision == 64;
     const size_t lim = sm_limit() - 1024;
-    if (p.smem13[fp] > lim || p.smem2[fp] > lim) return fail(WVLH_ERR_TOO_LARGE);
-    int rc;
-    if ((rc = c->scratch.ensure(p.scratch_elems * (fp ? 8 : 4))) ||
+    if (p.smem13[fp] / 2 > lim || p.smem2[fp] > lim) return fail(WVLH_ERR_TOO_LARGE);
+    if ((rc = c->scratch.ensure((p.scratch_elems + plane_tmp_elems(p, fp)) * (fp ? 8 : 4))) ||
         (rc = c->den_part.ensure(sizeof(double) * (size_t)p.part_den_elems)))
         return fail(rc);
     cudaError_t e = fp ? launch_locden<double>(p, (const double *)psi, hfac, rho, (double *)c->scratch.p,
@@ -516,16 +705,17 @@ extern "C" int wvlh_precond_batched(wvlh_batch *b, int precision, int ncong, con
                                     const void *rhs, double *hist)
 {
     if (!b || !cprec || !x || !rhs || ncong < 0 || (precision != 32 && precision != 64)) return fail(WVLH_ERR_ARG);
+    if (b->orbital_mode) return fail(WVLH_ERR_UNSUPPORTED);  // CG vectors are packed
     wvlh_ctx *c = b->ctx;
     CK(cudaSetDevice(c->device));
     const Plan &p = b->plan;
     const int fp = precision == 64;
     const size_t lim = sm_limit() - 1024;
-    if (p.smem13[fp] > lim || p.smem2[fp] > lim) return fail(WVLH_ERR_TOO_LARGE);
+    if (p.smem13[fp] / 2 > lim || p.smem2[fp] > lim) return fail(WVLH_ERR_TOO_LARGE);
     const size_t es = fp ? 8 : 4;
     const size_t nv = (size_t)p.psi_total * es;
     int rc;
-    if ((rc = c->scratch.ensure(p.scratch_elems * es)) || (rc = c->cg_r.ensure(nv)) || (rc = c->cg_d.ensure(nv)) ||
+    if ((rc = c->scratch.ensure((p.scratch_elems + plane_tmp_elems(p, fp)) * es)) || (rc = c->cg_r.ensure(nv)) || (rc = c->cg_d.ensure(nv)) ||
         (rc = c->cg_ad.ensure(nv)) || (rc = c->cg_scal.ensure(sizeof(double) * (size_t)p.norb * (5 + 16))))
         return fail(rc);
     cudaError_t e =
@@ -580,6 +770,7 @@ extern "C" int wvlh_locham_batched_host(wvlh_batch *b, int precision, const void
                                         double *ekin, double *epot)
 {
     if (!b || !psi || !pot || !hpsi || (precision != 32 && precision != 64)) return fail(WVLH_ERR_ARG);
+    if (b->orbital_mode) return fail(WVLH_ERR_UNSUPPORTED);
     wvlh_ctx *c = b->ctx;
     CK(cudaSetDevice(c->device));
     const size_t es = precision == 32 ? 4 : 8;
@@ -657,6 +848,7 @@ extern "C" int wvlh_locham_plain_batched(wvlh_batch *b, const double *psi, const
                                          double *ekin, double *epot)
 {
     if (!b || !psi || !pot || !hpsi || !ekin || !epot) return fail(WVLH_ERR_ARG);
+    if (b->orbital_mode) return fail(WVLH_ERR_UNSUPPORTED);
     wvlh_ctx *c = b->ctx;
     CK(cudaSetDevice(c->device));
     cudaStream_t st = c->stream;
@@ -677,7 +869,8 @@ extern "C" int wvlh_locham_plain_batched(wvlh_batch *b, const double *psi, const
         const int F1 = fine_len(N1, q1), F2 = fine_len(N2, q2), F3 = fine_len(N3, q3);
         const int I1 = isf_len(N1, q1), I2 = isf_len(N2, q2), I3 = isf_len(N3, q3);
         const size_t ni = (size_t)I1 * I2 * I3;
-        const int nvc = b->nvc[l], nvf = b->nvf[l];
+        const wvlh_region &R = *b->lr[l];
+        const int nvc = R.lr.nvctr_c, nvf = R.lr.nvctr_f;
         const int ncomp = nvc + 7 * nvf;
         int rc;
         for (int k = 0; k < 4; ++k)
@@ -695,8 +888,8 @@ extern "C" int wvlh_locham_plain_batched(wvlh_batch *b, const double *psi, const
         k_gather_orbitals<<<dim3(64, nb), 256, 0, st>>>(psi, d_offs, ncomp, W3, 1);
         const int dims[3] = {N1, N2, N3};
         // uncompress (OpenCL/Uncompress.c:596-606): W3 -> W0
-        CK(plain_uncompress(0, dims, b->nsc[l], nvc, b->d_keyg_c[l], b->d_keyv_c[l], b->nsf[l], nvf,
-                            b->d_keyg_f[l], b->d_keyv_f[l], W3, W3 + nvc, W0, nullptr, nb, ncomp, ncomp, ni, st));
+        CK(plain_uncompress(0, dims, R.lr.nseg_c, nvc, R.keyg_c, R.keyv_c, R.lr.nseg_f, nvf, R.keyg_f,
+                            R.keyv_f, W3, W3 + nvc, W0, nullptr, nb, ncomp, ncomp, ni, st));
         // syn z, y, x (OpenCL/Wavelet.c:282-315): W0 -> W1 -> W0 -> W1 (X)
         CK(plain_syn1d(N3, 4 * N1 * N2, q3, W0, W1, nb, ni, ni, st));
         CK(plain_syn1d(N2, 2 * N1 * F3, q2, W1, W0, nb, ni, ni, st));
@@ -712,7 +905,7 @@ extern "C" int wvlh_locham_plain_batched(wvlh_batch *b, const double *psi, const
         CK(plain_mf1d(q2 ? 1 : 3, F2, I1 * F3, W2, W0, nb, ni, ni, st));
         CK(plain_mf1d(q1 ? 1 : 3, F1, F3 * F2, W0, W2, nb, ni, ni, st));
         // kinetic z, y, x (Kinetic.c:240-270): (x=W1, y=W2) -> (W0, W3) -> (W1, W2) -> (W0, W3)
-        const double h1 = 0.5 * b->hgrid[3 * l], h2 = 0.5 * b->hgrid[3 * l + 1], h3 = 0.5 * b->hgrid[3 * l + 2];
+        const double h1 = 0.5 * R.hgrid[0], h2 = 0.5 * R.hgrid[1], h3 = 0.5 * R.hgrid[2];
         CK(plain_kin1d(F3, F1 * F2, q3, -0.5 / (h3 * h3), W1, W0, W2, W3, nb, ni, ni, st));
         CK(plain_kin1d(F2, F1 * F3, q2, -0.5 / (h2 * h2), W0, W1, W3, W2, nb, ni, ni, st));
         CK(plain_kin1d(F1, F3 * F2, q1, -0.5 / (h1 * h1), W1, W0, W2, W3, nb, ni, ni, st));
@@ -723,8 +916,8 @@ extern "C" int wvlh_locham_plain_batched(wvlh_batch *b, const double *psi, const
         CK(plain_ana1d(N2, F1 * 2 * N3, q2, W1, W3, nb, ni, ni, st));
         CK(plain_ana1d(N1, 4 * N3 * N2, q1, W3, W1, nb, ni, ni, st));
         // compress (Uncompress.c:608-613): W1 -> W2 (compressed), scatter to hpsi
-        CK(plain_uncompress(1, dims, b->nsc[l], nvc, b->d_keyg_c[l], b->d_keyv_c[l], b->nsf[l], nvf,
-                            b->d_keyg_f[l], b->d_keyv_f[l], W2, W2 + nvc, W1, nullptr, nb, ncomp, ncomp, ni, st));
+        CK(plain_uncompress(1, dims, R.lr.nseg_c, nvc, R.keyg_c, R.keyv_c, R.lr.nseg_f, nvf, R.keyg_f,
+                            R.keyv_f, W2, W2 + nvc, W1, nullptr, nb, ncomp, ncomp, ni, st));
         k_gather_orbitals<<<dim3(64, nb), 256, 0, st>>>(hpsi, d_offs, ncomp, W2, 0);
         k_sum_rows<<<(nb + 127) / 128, 128, 0, st>>>(ppart, NPART, nb, d_oidx, epot, nullptr);
         k_sum_rows<<<(nb + 127) / 128, 128, 0, st>>>(kpart, NPART, nb, d_oidx, ekin, epot);

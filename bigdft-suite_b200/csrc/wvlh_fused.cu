@@ -189,43 +189,53 @@ __device__ __forceinline__ TO *out_ptr(const OrbDev &o, TO *base)
 // ---------------------------------------------------------------------------
 // K1: compressed psi -> P = S_x S_y psi (not in MODE_LOCDEN) and
 // Q = M_x M_y P (not in MODE_PRECOND) for one wavelet z-plane.
+//
+// Plane kernels (K1, K3) hold two plane buffers A and B in shared memory.
+// When two planes do not fit (FP64 boxes above about 60^3 periodic / 45^3
+// free), B lives in gtmp, a global slice of gstride elements per CTA, and the
+// grid is one CTA per SM looping over the work items (the slice is indexed by
+// blockIdx, so no two running CTAs share it).
 template <class T, class TI, bool ALLPER, int MODE>
 __global__ void __launch_bounds__(kPlaneThreads) k1_plane_forward(const LrDev *__restrict__ lrs,
                                                                   const OrbDev *__restrict__ orbs,
-                                                                  const int2 *__restrict__ work,
+                                                                  const int2 *__restrict__ work, int nwork,
                                                                   const TI *__restrict__ psi, T *__restrict__ scratch,
-                                                                  const double *__restrict__ cprec)
+                                                                  const double *__restrict__ cprec, T *gtmp,
+                                                                  long long gstride)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ T sc[8];
-    const int2 w = work[blockIdx.x];
-    const OrbDev o = orbs[w.x];
-    const LrDev L = lrs[o.lr];
-    const Dims d(L, ALLPER);
-    const int kz = w.y;
-    const int pitch = d.pitch();
-    T *A = reinterpret_cast<T *>(smem_raw);
-    T *B = A + d.rows() * pitch;
     constexpr int SEG = Seg<T>::v;
+    for (int it = blockIdx.x; it < nwork; it += gridDim.x) {
+        __syncthreads();  // the previous item is done with A, B and sc
+        const int2 w = work[it];
+        const OrbDev o = orbs[w.x];
+        const LrDev L = lrs[o.lr];
+        const Dims d(L, ALLPER);
+        const int kz = w.y;
+        const int pitch = d.pitch();
+        T *A = reinterpret_cast<T *>(smem_raw);
+        T *B = gtmp ? gtmp + (size_t)blockIdx.x * gstride : A + d.rows() * pitch;
 
-    if (MODE == MODE_PRECOND && threadIdx.x < 8) sc[threadIdx.x] = (T)prec_scal(L, cprec[w.x], threadIdx.x);
-    zero_region(A, d.G2, pitch);
-    __syncthreads();
-    gather_plane<T, TI>(A, pitch, L, kz, in_ptr(o, psi), MODE == MODE_PRECOND ? sc : nullptr);
-    __syncthreads();
-    pass_syn<T, SEG>(A, B, rows_geom(d.G2, pitch), d.N1, d.p1);   // S_x: G2 rows, G1 -> F1
-    __syncthreads();
-    pass_syn<T, SEG>(B, A, cols_geom(d.F1, pitch), d.N2, d.p2);   // S_y: F1 cols, G2 -> F2
-    __syncthreads();
-    if (MODE != MODE_LOCDEN) store_plane(A, pitch, d.F2, d.F1, scratch + o.sP + (size_t)kz * d.F2 * d.F1);
-    if (MODE == MODE_PRECOND) return;
-    if (d.p1) pass_mf<T, SEG, 0>(A, B, rows_geom(d.F2, pitch), d.F1, d.I1);
-    else pass_mf<T, SEG, 2>(A, B, rows_geom(d.F2, pitch), d.F1, d.I1);
-    __syncthreads();
-    if (d.p2) pass_mf<T, SEG, 0>(B, A, cols_geom(d.I1, pitch), d.F2, d.I2);
-    else pass_mf<T, SEG, 2>(B, A, cols_geom(d.I1, pitch), d.F2, d.I2);
-    __syncthreads();
-    store_plane(A, pitch, d.I2, d.I1, scratch + o.sQ + (size_t)kz * d.I2 * d.I1);
+        if (MODE == MODE_PRECOND && threadIdx.x < 8) sc[threadIdx.x] = (T)prec_scal(L, cprec[w.x], threadIdx.x);
+        zero_region(A, d.G2, pitch);
+        __syncthreads();
+        gather_plane<T, TI>(A, pitch, L, kz, in_ptr(o, psi), MODE == MODE_PRECOND ? sc : nullptr);
+        __syncthreads();
+        pass_syn<T, SEG>(A, B, rows_geom(d.G2, pitch), d.N1, d.p1);   // S_x: G2 rows, G1 -> F1
+        __syncthreads();
+        pass_syn<T, SEG>(B, A, cols_geom(d.F1, pitch), d.N2, d.p2);   // S_y: F1 cols, G2 -> F2
+        __syncthreads();
+        if (MODE != MODE_LOCDEN) store_plane(A, pitch, d.F2, d.F1, scratch + o.sP + (size_t)kz * d.F2 * d.F1);
+        if (MODE == MODE_PRECOND) continue;
+        if (d.p1) pass_mf<T, SEG, 0>(A, B, rows_geom(d.F2, pitch), d.F1, d.I1);
+        else pass_mf<T, SEG, 2>(A, B, rows_geom(d.F2, pitch), d.F1, d.I1);
+        __syncthreads();
+        if (d.p2) pass_mf<T, SEG, 0>(B, A, cols_geom(d.I1, pitch), d.F2, d.I2);
+        else pass_mf<T, SEG, 2>(B, A, cols_geom(d.I1, pitch), d.F2, d.I2);
+        __syncthreads();
+        store_plane(A, pitch, d.I2, d.I1, scratch + o.sQ + (size_t)kz * d.I2 * d.I1);
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -317,66 +327,70 @@ __global__ void __launch_bounds__(kZThreads) k2_zpencil(const LrDev *__restrict_
 template <class T, class TO, bool ALLPER, int MODE>
 __global__ void __launch_bounds__(kPlaneThreads) k3_plane_backward(const LrDev *__restrict__ lrs,
                                                                    const OrbDev *__restrict__ orbs,
-                                                                   const int2 *__restrict__ work,
+                                                                   const int2 *__restrict__ work, int nwork,
                                                                    const int *__restrict__ slots,
                                                                    const T *__restrict__ scratch, TO *__restrict__ hpsi,
                                                                    double *__restrict__ part_kin, int part_stride,
-                                                                   int accumulate, const double *__restrict__ cprec)
+                                                                   int accumulate, const double *__restrict__ cprec,
+                                                                   T *gtmp, long long gstride)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ double red[32];
     __shared__ T sc[8];
-    const int2 w = work[blockIdx.x];
-    const OrbDev o = orbs[w.x];
-    const LrDev L = lrs[o.lr];
-    const Dims d(L, ALLPER);
-    const int kz = w.y;
-    const int pitch = d.pitch();
-    T *A = reinterpret_cast<T *>(smem_raw);
-    T *B = A + d.rows() * pitch;
     constexpr int SEG = Seg<T>::v;
+    for (int it = blockIdx.x; it < nwork; it += gridDim.x) {
+        __syncthreads();  // the previous item is done with A, B, sc and red
+        const int2 w = work[it];
+        const OrbDev o = orbs[w.x];
+        const LrDev L = lrs[o.lr];
+        const Dims d(L, ALLPER);
+        const int kz = w.y;
+        const int pitch = d.pitch();
+        T *A = reinterpret_cast<T *>(smem_raw);
+        T *B = gtmp ? gtmp + (size_t)blockIdx.x * gstride : A + d.rows() * pitch;
 
-    T cshift = T(0);
-    if (MODE == MODE_PRECOND) {
-        cshift = (T)cprec[w.x];
-        if (threadIdx.x < 8) sc[threadIdx.x] = (T)prec_scal(L, cprec[w.x], threadIdx.x);
-    } else {
-        load_plane(A, pitch, d.I2, d.I1, scratch + o.sQ + (size_t)kz * d.I2 * d.I1);
-        __syncthreads();
-        if (d.p1) pass_mf<T, SEG, 1>(A, B, rows_geom(d.I2, pitch), d.I1, d.F1);   // Mt_x
-        else pass_mf<T, SEG, 3>(A, B, rows_geom(d.I2, pitch), d.I1, d.F1);
-        __syncthreads();
-        if (d.p2) pass_mf<T, SEG, 1>(B, A, cols_geom(d.F1, pitch), d.I2, d.F2);   // Mt_y
-        else pass_mf<T, SEG, 3>(B, A, cols_geom(d.F1, pitch), d.I2, d.F2);
-        __syncthreads();
-    }
-    {
-        const T *z2 = scratch + o.sZ + (size_t)kz * d.F2 * d.F1;
-        const T *p = scratch + o.sP + (size_t)kz * d.F2 * d.F1;
-        for (int i = threadIdx.x; i < d.F2 * d.F1; i += blockDim.x) {
-            const int r = i / d.F1, c = i - r * d.F1;
-            const T pv = p[i];
-            if (MODE == MODE_PRECOND) A[r * pitch + c] = fma(cshift, pv, z2[i]);
-            else A[r * pitch + c] += z2[i];
-            B[r * pitch + c] = pv;
+        T cshift = T(0);
+        if (MODE == MODE_PRECOND) {
+            cshift = (T)cprec[w.x];
+            if (threadIdx.x < 8) sc[threadIdx.x] = (T)prec_scal(L, cprec[w.x], threadIdx.x);
+        } else {
+            load_plane(A, pitch, d.I2, d.I1, scratch + o.sQ + (size_t)kz * d.I2 * d.I1);
+            __syncthreads();
+            if (d.p1) pass_mf<T, SEG, 1>(A, B, rows_geom(d.I2, pitch), d.I1, d.F1);   // Mt_x
+            else pass_mf<T, SEG, 3>(A, B, rows_geom(d.I2, pitch), d.I1, d.F1);
+            __syncthreads();
+            if (d.p2) pass_mf<T, SEG, 1>(B, A, cols_geom(d.F1, pitch), d.I2, d.F2);   // Mt_y
+            else pass_mf<T, SEG, 3>(B, A, cols_geom(d.F1, pitch), d.I2, d.F2);
+            __syncthreads();
         }
+        {
+            const T *z2 = scratch + o.sZ + (size_t)kz * d.F2 * d.F1;
+            const T *p = scratch + o.sP + (size_t)kz * d.F2 * d.F1;
+            for (int i = threadIdx.x; i < d.F2 * d.F1; i += blockDim.x) {
+                const int r = i / d.F1, c = i - r * d.F1;
+                const T pv = p[i];
+                if (MODE == MODE_PRECOND) A[r * pitch + c] = fma(cshift, pv, z2[i]);
+                else A[r * pitch + c] += z2[i];
+                B[r * pitch + c] = pv;
+            }
+        }
+        __syncthreads();
+        double e = 0.0;
+        const double sx = -0.5 / ((0.5 * L.hgrid[0]) * (0.5 * L.hgrid[0]));
+        const double sy = -0.5 / ((0.5 * L.hgrid[1]) * (0.5 * L.hgrid[1]));
+        pass_kin<T, SEG, true>(B, A, rows_geom(d.F2, pitch), d.F1, d.p1, sx, T(0), &e);   // += K_x P
+        __syncthreads();
+        pass_kin<T, SEG, true>(B, A, cols_geom(d.F1, pitch), d.F2, d.p2, sy, T(0), &e);   // += K_y P
+        __syncthreads();
+        pass_ana<T, SEG>(A, B, rows_geom(d.F2, pitch), d.N1, d.p1);   // A_x: F1 -> G1
+        __syncthreads();
+        pass_ana<T, SEG>(B, A, cols_geom(d.G1, pitch), d.N2, d.p2);   // A_y: F2 -> G2
+        __syncthreads();
+        scatter_plane<T, TO>(A, pitch, L, kz, out_ptr(o, hpsi), accumulate != 0,
+                             MODE == MODE_PRECOND ? sc : nullptr);
+        const double s = block_sum(e, red);
+        if (threadIdx.x == 0 && part_kin) part_kin[(size_t)w.x * part_stride + slots[it]] = s;
     }
-    __syncthreads();
-    double e = 0.0;
-    const double sx = -0.5 / ((0.5 * L.hgrid[0]) * (0.5 * L.hgrid[0]));
-    const double sy = -0.5 / ((0.5 * L.hgrid[1]) * (0.5 * L.hgrid[1]));
-    pass_kin<T, SEG, true>(B, A, rows_geom(d.F2, pitch), d.F1, d.p1, sx, T(0), &e);   // += K_x P
-    __syncthreads();
-    pass_kin<T, SEG, true>(B, A, cols_geom(d.F1, pitch), d.F2, d.p2, sy, T(0), &e);   // += K_y P
-    __syncthreads();
-    pass_ana<T, SEG>(A, B, rows_geom(d.F2, pitch), d.N1, d.p1);   // A_x: F1 -> G1
-    __syncthreads();
-    pass_ana<T, SEG>(B, A, cols_geom(d.G1, pitch), d.N2, d.p2);   // A_y: F2 -> G2
-    __syncthreads();
-    scatter_plane<T, TO>(A, pitch, L, kz, out_ptr(o, hpsi), accumulate != 0,
-                         MODE == MODE_PRECOND ? sc : nullptr);
-    const double s = block_sum(e, red);
-    if (threadIdx.x == 0 && part_kin) part_kin[(size_t)w.x * part_stride + slots[blockIdx.x]] = s;
 }
 
 // fixed-order per-orbital sum of the energy partial slots
@@ -403,7 +417,7 @@ __global__ void k_reduce_energies(const double *__restrict__ part_pot, const dou
 // ---------------------------------------------------------------------------
 // Density z-kernel: for a tile of ISF columns, loop over the orbitals of one
 // chunk: R = M_z S_z Q, acc += hfac R^2 (FP64), then write the chunk partial.
-template <class T, bool ALLPER>
+template <class T, bool ALLPER, int MAXP>
 __global__ void __launch_bounds__(kZThreads) kd_density(const LrDev *__restrict__ lrs,
                                                         const OrbDev *__restrict__ orbs,
                                                         const int4 *__restrict__ work,
@@ -414,7 +428,7 @@ __global__ void __launch_bounds__(kZThreads) kd_density(const LrDev *__restrict_
                                                         double *__restrict__ part)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    constexpr int MAXP = 32;   // accumulators per thread (I3 * TC / kZThreads <= MAXP)
+    // MAXP accumulators per thread: I3 * TC <= MAXP * kZThreads
     const int4 w = work[blockIdx.x];
     const int chunk = w.x, x0 = w.y, y0 = w.z;
     const int ob = chunk_orb_start[chunk], oe = chunk_orb_start[chunk + 1];
@@ -477,7 +491,8 @@ __global__ void k_density_reduce(const int *__restrict__ group_chunk_start, cons
     const int g = blockIdx.y;
     const int n = group_n[g];
     const int cb = group_chunk_start[g], ce = group_chunk_start[g + 1];
-    double *r = rho + group_rho[g];
+    // packed batches: offsets into rho; orbital batches: addresses (rho null)
+    double *r = rho ? rho + group_rho[g] : reinterpret_cast<double *>(group_rho[g]);
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         double s = r[i];
         for (int c = cb; c < ce; ++c) s += part[chunk_part[c] + i];
@@ -587,13 +602,47 @@ __global__ void k_cg_scale(const LrDev *__restrict__ lrs, const OrbDev *__restri
 
 // ---------------------------------------------------------------------------
 // host launchers
+
+// Launch shape of the plane kernels: two shared-memory planes when they fit,
+// else one shared plane + a global slice per CTA after the batch scratch.
+struct PlaneCfg {
+    size_t smem = 0;
+    int grid = 0;
+    long long gstride = 0;
+    bool global_b = false;
+};
+
+static PlaneCfg plane_cfg(const Plan &p, int fp, int nwork)
+{
+    int dev = 0, lim = 0, nsm = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&lim, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    PlaneCfg c;
+    c.global_b = p.smem13[fp] > (size_t)lim - 1024;
+    c.smem = c.global_b ? p.smem13[fp] / 2 : p.smem13[fp];
+    c.grid = c.global_b ? (nwork < nsm ? nwork : nsm) : nwork;
+    c.gstride = c.global_b ? p.plane_elems : 0;
+    return c;
+}
+
+long long plane_tmp_elems(const Plan &p, int fp)
+{
+    int dev = 0, lim = 0, nsm = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&lim, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    return p.smem13[fp] > (size_t)lim - 1024 ? (long long)nsm * p.plane_elems : 0;
+}
 template <class T, class TIO, bool ALLPER>
 static cudaError_t launch_locham_bc(const Plan &p, const TIO *psi, const TIO *pot, TIO *hpsi, T *scratch,
                                     double *part_pot, double *part_kin, double *ekin, double *epot, int accumulate,
                                     cudaStream_t st, cudaEvent_t *ev)
 {
     const int fp = sizeof(T) == 8 ? 1 : 0;
-    const size_t sm13 = p.smem13[fp], sm2 = p.smem2[fp];
+    const PlaneCfg pc = plane_cfg(p, fp, p.n_work13);
+    const size_t sm13 = pc.smem, sm2 = p.smem2[fp];
+    T *gtmp = pc.global_b ? scratch + p.scratch_elems : nullptr;
     cudaError_t err;
     auto k1 = k1_plane_forward<T, TIO, ALLPER, MODE_LOCHAM>;
     auto k2 = k2_zpencil<T, TIO, ALLPER>;
@@ -605,13 +654,14 @@ static cudaError_t launch_locham_bc(const Plan &p, const TIO *psi, const TIO *po
     cudaMemsetAsync(part_kin, 0, sizeof(double) * (size_t)p.norb * p.part_stride, st);
     // optional per-kernel timing: ev[0..4] bracket K1, K2, K3 and the reduction
     if (ev) cudaEventRecord(ev[0], st);
-    k1<<<p.n_work13, kPlaneThreads, sm13, st>>>(p.d_lr, p.d_orb, p.d_work13, psi, scratch, nullptr);
+    k1<<<pc.grid, kPlaneThreads, sm13, st>>>(p.d_lr, p.d_orb, p.d_work13, p.n_work13, psi, scratch, nullptr, gtmp,
+                                             pc.gstride);
     if (ev) cudaEventRecord(ev[1], st);
     k2<<<p.n_work2, kZThreads, sm2, st>>>(p.d_lr, p.d_orb, p.d_work2, p.d_part_slot2, pot, scratch, part_pot,
                                           part_kin, p.part_stride);
     if (ev) cudaEventRecord(ev[2], st);
-    k3<<<p.n_work13, kPlaneThreads, sm13, st>>>(p.d_lr, p.d_orb, p.d_work13, p.d_part_slot13, scratch, hpsi,
-                                                part_kin, p.part_stride, accumulate, nullptr);
+    k3<<<pc.grid, kPlaneThreads, sm13, st>>>(p.d_lr, p.d_orb, p.d_work13, p.n_work13, p.d_part_slot13, scratch,
+                                             hpsi, part_kin, p.part_stride, accumulate, nullptr, gtmp, pc.gstride);
     if (ev) cudaEventRecord(ev[3], st);
     k_reduce_energies<<<p.norb, 128, 0, st>>>(part_pot, part_kin, p.part_stride, p.norb, ekin, epot);
     if (ev) cudaEventRecord(ev[4], st);
@@ -642,13 +692,16 @@ static cudaError_t launch_locden_bc(const Plan &p, const T *psi, const double *h
                                     double *part, cudaStream_t st)
 {
     const int fp = sizeof(T) == 8 ? 1 : 0;
-    const size_t sm13 = p.smem13[fp], sm2 = p.smem2[fp];
+    const PlaneCfg pc = plane_cfg(p, fp, p.n_work13);
+    const size_t sm13 = pc.smem, sm2 = p.smem2[fp];
+    T *gtmp = pc.global_b ? scratch + p.scratch_elems : nullptr;
     cudaError_t err;
     auto k1 = k1_plane_forward<T, T, ALLPER, MODE_LOCDEN>;
-    auto kd = kd_density<T, ALLPER>;
+    auto kd = p.den_acc > 32 ? kd_density<T, ALLPER, 48> : kd_density<T, ALLPER, 32>;
     if ((err = cudaFuncSetAttribute(k1, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm13))) return err;
     if ((err = cudaFuncSetAttribute(kd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm2))) return err;
-    k1<<<p.n_work13, kPlaneThreads, sm13, st>>>(p.d_lr, p.d_orb, p.d_work13, psi, scratch, nullptr);
+    k1<<<pc.grid, kPlaneThreads, sm13, st>>>(p.d_lr, p.d_orb, p.d_work13, p.n_work13, psi, scratch, nullptr, gtmp,
+                                             pc.gstride);
     kd<<<p.n_workd, kZThreads, sm2, st>>>(p.d_lr, p.d_orb, p.d_workd, p.d_chunk_orb_start, p.d_chunk_orbs,
                                           p.d_chunk_part, scratch, hfac, part);
     dim3 g((p.max_group_n + 255) / 256 < 4096 ? (p.max_group_n + 255) / 256 : 4096, p.ngroup);
@@ -675,7 +728,9 @@ static cudaError_t launch_prec_apply_bc(const Plan &p, const T *x, T *y, const d
                                         cudaStream_t st)
 {
     const int fp = sizeof(T) == 8 ? 1 : 0;
-    const size_t sm13 = p.smem13[fp], sm2 = p.smem2[fp];
+    const PlaneCfg pc = plane_cfg(p, fp, p.n_work13);
+    const size_t sm13 = pc.smem, sm2 = p.smem2[fp];
+    T *gtmp = pc.global_b ? scratch + p.scratch_elems : nullptr;
     cudaError_t err;
     auto k1 = k1_plane_forward<T, T, ALLPER, MODE_PRECOND>;
     auto k2 = k2_zpencil<T, T, ALLPER>;
@@ -683,11 +738,12 @@ static cudaError_t launch_prec_apply_bc(const Plan &p, const T *x, T *y, const d
     if ((err = cudaFuncSetAttribute(k1, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm13))) return err;
     if ((err = cudaFuncSetAttribute(k2, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm2))) return err;
     if ((err = cudaFuncSetAttribute(k3, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm13))) return err;
-    k1<<<p.n_work13, kPlaneThreads, sm13, st>>>(p.d_lr, p.d_orb, p.d_work13, x, scratch, cprec);
+    k1<<<pc.grid, kPlaneThreads, sm13, st>>>(p.d_lr, p.d_orb, p.d_work13, p.n_work13, x, scratch, cprec, gtmp,
+                                             pc.gstride);
     k2<<<p.n_work2p, kZThreads, sm2, st>>>(p.d_lr, p.d_orb, p.d_work2p, p.d_part_slot2p, (const T *)nullptr,
                                            scratch, nullptr, nullptr, 0);
-    k3<<<p.n_work13, kPlaneThreads, sm13, st>>>(p.d_lr, p.d_orb, p.d_work13, p.d_part_slot13, scratch, y, nullptr, 0,
-                                                0, cprec);
+    k3<<<pc.grid, kPlaneThreads, sm13, st>>>(p.d_lr, p.d_orb, p.d_work13, p.n_work13, p.d_part_slot13, scratch, y,
+                                             nullptr, 0, 0, cprec, gtmp, pc.gstride);
     return cudaGetLastError();
 }
 

@@ -84,14 +84,16 @@ struct Plan {
     long long *d_chunk_part = nullptr;   // element offset of each chunk's partial density
     long long part_den_elems = 0;
     int *d_group_chunk_start = nullptr;  // ngroup + 1 chunk ranges
-    long long *d_group_rho = nullptr;    // density offset of each group
+    long long *d_group_rho = nullptr;    // density offset (or address) of each group
     int *d_group_n = nullptr;            // ISF points of each group
     int max_group_n = 0;
+    int den_acc = 32;                    // FP64 accumulators per thread of kd_density (32 or 48)
     // per-orbital compressed vector offset / length (preconditioner vector ops)
     long long *d_orb_off = nullptr;
     int *d_orb_len = nullptr;
     int part_stride = 0;           // energy partial slots per orbital
-    size_t smem13[2] = {0, 0};     // dynamic smem bytes (float, double)
+    size_t smem13[2] = {0, 0};     // dynamic smem bytes (float, double) of two planes
+    long long plane_elems = 0;     // elements of one plane buffer (rows x pitch)
     size_t smem2[2] = {0, 0};
     int pitch_max = 0, rows_max = 0, zlen_max = 0;
     std::vector<void *> owned;     // device allocations to free

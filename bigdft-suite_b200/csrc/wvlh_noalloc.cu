@@ -266,6 +266,8 @@ extern "C" int wvlh_locham_noalloc(int precision, const int n[3], const int peri
     p.n_work13 = G[2];
     p.n_work2 = nw2;
     p.part_stride = stride;
+    p.plane_elems = (long long)(rows * pitch);
+    p.scratch_elems = 2 * sP + sQ;
     p.smem13[0] = 2 * rows * pitch * 4;
     p.smem13[1] = 2 * rows * pitch * 8;
     p.smem2[0] = 2 * zl * TX_ * TY_ * 4;

@@ -57,6 +57,7 @@ extern "C" const char *wvlh_error_string(int code)
     case WVLH_ERR_NOMEM: return "device allocation failed";
     case WVLH_ERR_UNSUPPORTED: return "unsupported (k-points / spinors)";
     case WVLH_ERR_TOO_LARGE: return "box too large for this path";
+    case WVLH_ERR_STALE: return "batch tables replaced by a newer orbital batch";
     default: return "unknown error";
     }
 }

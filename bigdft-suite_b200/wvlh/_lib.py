@@ -16,7 +16,8 @@ class WvlhError(RuntimeError):
 
 
 ERRORS = {1: "CUDA runtime error", 2: "invalid argument", 3: "invalid segment keys",
-          4: "device allocation failed", 5: "unsupported (k-points / spinors)", 6: "box too large for this path"}
+          4: "device allocation failed", 5: "unsupported (k-points / spinors)", 6: "box too large for this path",
+          7: "batch tables replaced by a newer orbital batch"}
 
 
 def build(force=False):
@@ -41,6 +42,11 @@ class LocregDesc(C.Structure):
                 ("nseg_c", C.c_int), ("nseg_f", C.c_int),
                 ("keyg_c", C.POINTER(C.c_int32)), ("keyv_c", C.POINTER(C.c_int32)),
                 ("keyg_f", C.POINTER(C.c_int32)), ("keyv_f", C.POINTER(C.c_int32))]
+
+
+class OrbitalDesc(C.Structure):
+    _fields_ = [("region", C.c_void_p), ("psi", C.c_void_p), ("hpsi", C.c_void_p), ("pot", C.c_void_p),
+                ("rho", C.c_void_p)]
 
 
 # every extern "C" symbol declared in include/wvlh.h
@@ -68,7 +74,8 @@ WVLH_SYMBOLS = [
     "wvlh_locham_batched_host", "wvlh_locham_plain_batched", "wvlh_host_alloc", "wvlh_host_free",
     "wvlh_ctx_enable_timing", "wvlh_ctx_kernel_times", "wvlh_measure_fma_peak",
     "wvlh_locham_noalloc", "wvlh_noalloc_capacity", "wvlh_locden_batched", "wvlh_precond_batched",
-    "wvlh_overlap",
+    "wvlh_overlap", "wvlh_region_create", "wvlh_region_destroy", "wvlh_region_psi_size",
+    "wvlh_region_grid_size", "wvlh_region_scratch_bytes", "wvlh_batch_create_orbitals",
 ]
 
 
@@ -111,6 +118,14 @@ def lib():
     L.wvlh_locden_batched.argtypes = [vp, C.c_int, vp, vp, vp]
     L.wvlh_precond_batched.argtypes = [vp, C.c_int, C.c_int, vp, vp, vp, vp]
     L.wvlh_overlap.argtypes = [vp, C.c_int, C.c_int, C.c_int64, C.c_int64, vp, vp]
+    L.wvlh_region_create.argtypes = [vp, C.POINTER(LocregDesc), C.POINTER(vp)]
+    L.wvlh_region_destroy.argtypes = [vp]
+    for nm in ("wvlh_region_psi_size", "wvlh_region_grid_size"):
+        getattr(L, nm).restype = C.c_int64
+        getattr(L, nm).argtypes = [vp]
+    L.wvlh_region_scratch_bytes.restype = C.c_int64
+    L.wvlh_region_scratch_bytes.argtypes = [vp, C.c_int]
+    L.wvlh_batch_create_orbitals.argtypes = [vp, C.c_int, C.POINTER(OrbitalDesc), C.POINTER(vp)]
     L.wvlh_host_alloc.restype = vp
     L.wvlh_host_alloc.argtypes = [C.c_size_t]
     L.wvlh_host_free.argtypes = [vp]

@@ -13,11 +13,23 @@ import ctypes as C
 
 import numpy as np
 
-from ._lib import LocregDesc, WvlhError, check, lib, require_cuda
+from ._lib import LocregDesc, OrbitalDesc, WvlhError, check, lib, require_cuda
 
 
 def _ptr(t):
     return C.c_void_p(t.data_ptr()) if t is not None else None
+
+
+def _fill_desc(d, L, keep):
+    """wvlh_locreg of a Locreg; the key arrays are appended to keep."""
+    d.n[:] = list(L.n)
+    d.periodic[:] = list(L.periodic)
+    d.hgrid[:] = list(L.hgrid)
+    d.nseg_c, d.nseg_f = len(L.keyv_c), len(L.keyv_f)
+    for nm in ("keyg_c", "keyv_c", "keyg_f", "keyv_f"):
+        arr = np.ascontiguousarray(getattr(L, nm), np.int32)
+        keep.append(arr)
+        setattr(d, nm, arr.ctypes.data_as(C.POINTER(C.c_int32)))
 
 
 class Context:
@@ -61,15 +73,7 @@ class Batch:
         descs = (LocregDesc * len(self.locregs))()
         self._keep = []
         for i, L in enumerate(self.locregs):
-            d = descs[i]
-            d.n[:] = list(L.n)
-            d.periodic[:] = list(L.periodic)
-            d.hgrid[:] = list(L.hgrid)
-            d.nseg_c, d.nseg_f = len(L.keyv_c), len(L.keyv_f)
-            for nm in ("keyg_c", "keyv_c", "keyg_f", "keyv_f"):
-                arr = np.ascontiguousarray(getattr(L, nm), np.int32)
-                self._keep.append(arr)
-                setattr(d, nm, arr.ctypes.data_as(C.POINTER(C.c_int32)))
+            _fill_desc(descs[i], L, self._keep)
         if pot_offset is None:
             po = None
             self.pot_offset = np.zeros(self.norb, np.int64)
@@ -164,6 +168,94 @@ class Batch:
         rc = lib().wvlh_locham_plain_batched(self.h, _ptr(psi), _ptr(pot), _ptr(hpsi), _ptr(ekin), _ptr(epot))
         check(rc, "wvlh_locham_plain_batched")
         return hpsi, ekin, epot
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().wvlh_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Region:
+    """A localisation region resident on the device: keys validated, decoded
+    and uploaded once (wvlh_region_create), shared by every batch that
+    names it."""
+
+    def __init__(self, ctx, locreg):
+        self.ctx = ctx
+        self.locreg = locreg
+        d = LocregDesc()
+        keep = []
+        _fill_desc(d, locreg, keep)
+        h = C.c_void_p()
+        check(lib().wvlh_region_create(ctx.h, C.byref(d), C.byref(h)), "wvlh_region_create")
+        self.h = h
+        self.psi_size = int(lib().wvlh_region_psi_size(h))
+        self.grid_size = int(lib().wvlh_region_grid_size(h))
+
+    def scratch_bytes(self, precision):
+        """Fused-kernel scratch of one orbital of this region."""
+        return int(lib().wvlh_region_scratch_bytes(self.h, precision))
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().wvlh_region_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class OrbitalBatch:
+    """One launch over orbitals of any regions, each with its own device
+    buffers (wvlh_batch_create_orbitals).  orbitals: sequence of
+    (region, psi, hpsi, pot, rho) with tensors or None; the tables go to the
+    context's arena, so launch before the next OrbitalBatch of the context."""
+
+    def __init__(self, ctx, orbitals):
+        self.ctx = ctx
+        self.norb = len(orbitals)
+        descs = (OrbitalDesc * self.norb)()
+        self._keep = []
+        dtype = None
+        for i, (reg, psi, hpsi, pot, rho) in enumerate(orbitals):
+            d = descs[i]
+            d.region = reg.h.value
+            for nm, t in (("psi", psi), ("hpsi", hpsi), ("pot", pot), ("rho", rho)):
+                if t is not None:
+                    self._keep.append(t)
+                    setattr(d, nm, t.data_ptr())
+            if psi is not None:
+                if dtype is not None and psi.dtype != dtype:
+                    raise WvlhError("all orbitals of a batch share one precision")
+                dtype = psi.dtype
+        self.dtype = dtype
+        h = C.c_void_p()
+        check(lib().wvlh_batch_create_orbitals(ctx.h, self.norb, descs, C.byref(h)), "wvlh_batch_create_orbitals")
+        self.h = h
+
+    @property
+    def precision(self):
+        torch = self.ctx.torch
+        return {torch.float32: 32, torch.float64: 64}[self.dtype]
+
+    def locham(self, ekin, epot, accumulate=False):
+        """Hpsi of every orbital into its own hpsi; ekin/epot: device float64 (norb,)."""
+        rc = lib().wvlh_locham_batched(self.h, self.precision, None, None, None, _ptr(ekin), _ptr(epot),
+                                       int(bool(accumulate)))
+        check(rc, "wvlh_locham_batched")
+
+    def locden(self, hfac):
+        """rho_o += hfac[o] |psi_o|^2 into each orbital's own rho; hfac device float64 (norb,)."""
+        check(lib().wvlh_locden_batched(self.h, self.precision, None, _ptr(hfac), None), "wvlh_locden_batched")
 
     def close(self):
         if getattr(self, "h", None):

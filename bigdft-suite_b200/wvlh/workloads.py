@@ -85,3 +85,32 @@ def free_regions(nlr=1024, nmin=20, nmax=40, seed=2, hgrid=0.45):
         psis.append(random_psi(lr, 1, rng, normalize=True)[0])
         pots.append(gaussian_potential(lr, rng))
     return lrs, psis, pots
+
+
+def serving_clients(nclient=64, nmin=16, nmax=64, omin=4, omax=128, p_periodic=0.5, seed=4, hgrid=0.45):
+    """Clients of the serving benchmark: each an independent SCF run with its
+    own box (coarse cells per dimension uniform in [nmin, nmax]), periodic
+    (every cell fine) or free (fine ellipsoid) with probability p_periodic,
+    and uniform [omin, omax] orbitals.  Returns (locreg, norb, seed) per
+    client; coefficients and potentials are drawn from the per-client seed
+    where they are needed (on the device, see wvlh.serve)."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(nclient):
+        N = tuple(int(v) for v in rng.integers(nmin, nmax + 1, 3))
+        periodic = rng.uniform() < p_periodic
+        lr = full_periodic(N, hgrid) if periodic else free_sphere(N, hgrid)
+        norb = int(rng.integers(omin, omax + 1))
+        out.append((lr, norb, int(rng.integers(1 << 30))))
+    return out
+
+
+def poisson_arrivals(rate, nreq, nclient, seed=5, p_density=0.5):
+    """nreq requests at Poisson times of mean rate `rate` (1/s), each from a
+    uniform client, a density request with probability p_density (else H psi).
+    Returns a list of (t, client, kind) sorted by t, kind in {"H", "rho"}."""
+    rng = np.random.default_rng(seed)
+    t = np.cumsum(rng.exponential(1.0 / rate, nreq))
+    cl = rng.integers(0, nclient, nreq)
+    kind = rng.uniform(size=nreq) < p_density
+    return [(float(t[i]), int(cl[i]), "rho" if kind[i] else "H") for i in range(nreq)]

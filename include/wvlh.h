@@ -45,7 +45,8 @@ enum {
     WVLH_ERR_KEYS = 3,
     WVLH_ERR_NOMEM = 4,
     WVLH_ERR_UNSUPPORTED = 5,
-    WVLH_ERR_TOO_LARGE = 6
+    WVLH_ERR_TOO_LARGE = 6,
+    WVLH_ERR_STALE = 7
 };
 
 /* --------------------------------------------------------------------- */
@@ -242,6 +243,39 @@ int wvlh_batch_destroy(wvlh_batch *batch);
 int64_t wvlh_batch_psi_size(const wvlh_batch *batch);    /* total coefficient count */
 int64_t wvlh_batch_psi_offset(const wvlh_batch *batch, int orb);
 int64_t wvlh_batch_scratch_bytes(const wvlh_batch *batch, int precision);
+
+/* Resident regions and per-launch orbital batches (serving: many independent
+ * clients, each with its own box, buffers and density; no counterpart in the
+ * reference, whose host owns one set of buffers per process).
+ *
+ * A region is one client's localisation region with its keys validated,
+ * decoded and uploaded once; it must outlive the batches that use it. */
+typedef struct wvlh_region wvlh_region;
+int wvlh_region_create(wvlh_ctx *ctx, const wvlh_locreg *lr, wvlh_region **region);
+int wvlh_region_destroy(wvlh_region *region);
+int64_t wvlh_region_psi_size(const wvlh_region *region);   /* nvctr_c + 7 nvctr_f */
+int64_t wvlh_region_grid_size(const wvlh_region *region);  /* ISF (potential / density) points */
+int64_t wvlh_region_scratch_bytes(const wvlh_region *region, int precision);  /* per orbital */
+
+/* One orbital of an orbital batch: its region and its own DEVICE buffers
+ * (precision of the launch): psi [psi_c | psi_f], hpsi and the region's ISF
+ * potential for wvlh_locham_batched; rho (FP64 ISF grid, accumulated) for
+ * wvlh_locden_batched.  Unused buffers may be NULL. */
+typedef struct {
+    const wvlh_region *region;
+    const void *psi;
+    void *hpsi;
+    const void *pot;
+    double *rho;
+} wvlh_orbital;
+/* Build a batch over orbitals of any regions.  Its tables go to a grow-only
+ * arena of the context, written by a copy queued on the context's stream, so
+ * that a new batch costs no device allocation once the arena is large enough;
+ * launches of a batch must be queued before the next orbital batch of the
+ * same context is created (later launches return WVLH_ERR_STALE).  Launch
+ * with NULL psi/pot/hpsi (locham) or psi/rho (locden): each orbital's own
+ * buffers are used.  Orbitals that share rho must share their region. */
+int wvlh_batch_create_orbitals(wvlh_ctx *ctx, int norb, const wvlh_orbital *orbs, wvlh_batch **batch);
 
 /* Hpsi for all orbitals of the batch.  precision 32: psi/pot/hpsi are float,
  * 64: double.  Device pointers.  ekin/epot: device arrays of norb doubles

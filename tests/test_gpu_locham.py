@@ -153,3 +153,22 @@ def test_full_size_properties_fp32_vs_fp64(torch_cuda, wctx):
     # linearity: H(a x + y) = a Hx + Hy
     hx, _, _ = b.locham((2.5 * P[0:1] + P[1:2]).repeat(16, 1).ravel().contiguous(), v64)
     assert ((hx.view(16, -1)[0] - (2.5 * H[0] + H[1])).norm() / H[0].norm()).item() < 1e-13
+
+
+# FP64 planes too large for two shared-memory buffers (2 x rows x pitch x 8 B
+# above the 227 KB per block): the second buffer is a global slice per CTA.
+LARGE = [((48, 46, 6), (0, 0, 0), 0.5), ((64, 64, 8), (1, 1, 1), 1.0), ((60, 62, 9), (0, 0, 0), 0.4)]
+
+
+@pytest.mark.parametrize("N,per,dens", LARGE)
+def test_fp64_large_planes_match_oracle(oracle, torch_cuda, wctx, N, per, dens):
+    lr, psi, pot = case(N, per, dens, seed=5)
+    psi /= np.linalg.norm(psi)
+    ref, ek, ep = oracle_locham(oracle, lr, psi, pot)
+    out, gek, gep = run_batch(wctx, torch_cuda, [lr, lr], [psi, psi], [pot, pot], torch_cuda.float64)
+    for o in range(2):
+        assert rel(out[o], ref) < 1e-13
+        assert abs(gek[o] - ek) <= 1e-12 * abs(ek) and abs(gep[o] - ep) <= 1e-12 * abs(ep)
+    # the FP32 form of the same boxes keeps two shared planes
+    out, gek, gep = run_batch(wctx, torch_cuda, [lr], [psi], [pot], torch_cuda.float32)
+    assert rel(out[0], ref) < 1e-5 and abs(gek[0] - ek) < 1e-6 and abs(gep[0] - ep) < 1e-6
