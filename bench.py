@@ -45,7 +45,7 @@ def parse():
     ap.add_argument("--impl", default="wvlh", choices=["wvlh", "reference"])
     ap.add_argument("--n", type=int, default=48)
     ap.add_argument("--norb", type=int, default=256)
-    ap.add_argument("--no-extras", action="store_true", help="skip comparator / e2e / cpu legs")
+    ap.add_argument("--no-extras", action="store_true", help="skip comparator / e2e / cpu / other-row legs")
     return ap.parse_args()
 
 
@@ -173,6 +173,164 @@ def run_reference(args, ws, rank):
                              "sample": "2 orbitals of %d^3 per step" % n},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
+
+
+def _timed(torch, fn, reps, stream=None):
+    """Mean ms of fn over reps launches, CUDA events on the current stream, after one warm call."""
+    fn()
+    torch.cuda.synchronize()
+    st = stream or torch.cuda.current_stream()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(st)
+    for _ in range(reps):
+        fn()
+    b.record(st)
+    torch.cuda.synchronize()
+    return a.elapsed_time(b) / reps
+
+
+def leg_free_regions(torch, ctx, dev, nlr=1024, seed=2):
+    """Free-BC support functions of uneven size: nlr regions with coarse boxes
+    uniform 20..40 per dimension (all cells coarse), fine ellipsoid of radius
+    0.4 x the box, one normalised orbital and one Gaussian potential each, all
+    in one fused launch sequence.  FP32 fused vs FP64 fused vs FP64 plain."""
+    import numpy as np
+    from wvlh import workloads as W
+    from wvlh.batch import Batch
+    rng = np.random.default_rng(seed)
+    lrs = [W.free_sphere(tuple(int(v) for v in rng.integers(20, 41, 3)), 0.45) for _ in range(nlr)]
+    off = np.cumsum([0] + [lr.nisf for lr in lrs[:-1]])
+    b = Batch(ctx, lrs, np.arange(nlr, dtype=np.int32), off)
+    g = torch.Generator(device=dev)
+    g.manual_seed(seed)
+    psi64 = torch.rand(b.psi_size, generator=g, device=dev, dtype=torch.float64) * 2 - 1
+    lens = torch.tensor([lr.ncoeff for lr in lrs], device=dev)
+    idx = torch.repeat_interleave(torch.arange(nlr, device=dev), lens)
+    nrm = torch.zeros(nlr, dtype=torch.float64, device=dev).index_add_(0, idx, psi64 * psi64)
+    psi64 /= nrm.sqrt()[idx]
+    del idx
+    pot64 = torch.cat([W.gaussian_potential_device(lr, rng, dev) for lr in lrs])
+    psi32, pot32 = psi64.float(), pot64.float()
+    cells = sum(lr.coarse_cells for lr in lrs)
+    h32, h64 = torch.empty_like(psi32), torch.empty_like(psi64)
+    e = torch.empty(4, nlr, dtype=torch.float64, device=dev)
+    ms32 = _timed(torch, lambda: b.locham(psi32, pot32, h32, e[0], e[1]), 5)
+    ms64 = _timed(torch, lambda: b.locham(psi64, pot64, h64, e[2], e[3]), 3)
+    de = max((e[0] - e[2]).abs().max().item(), (e[1] - e[3]).abs().max().item())
+    ms_plain = _timed(torch, lambda: b.locham_plain(psi64, pot64, h64, e[2], e[3]), 1)
+    out = {"workload": "%d free-BC regions, coarse 20..40 per dim, fine ellipsoid 0.4, 1 orbital each" % nlr,
+           "coarse_cells": int(cells), "fp32_fused": {"value": cells / (ms32 * 1e-3), "ms": ms32},
+           "fp64_fused": {"value": cells / (ms64 * 1e-3), "ms": ms64},
+           "fp64_plain": {"value": cells / (ms_plain * 1e-3), "ms": ms_plain},
+           "speedup_fp32_vs_fp64_plain": ms_plain / ms32, "energy_err_ha_fp32_vs_fp64": de}
+    b.close()
+    return out
+
+
+def leg_precond(torch, ctx, dev, n=40, norb=512, ncong=5, seed=3):
+    """Preconditioner batch: norb orbitals on an n^3 periodic grid, ncong CG
+    iterations of (T - eps_i + c) x = r_i (c = 0.5, eps_i uniform(-1, -0.1)),
+    from x0 = b = r (seeded uniform); FP32 convolutions / FP64 dot products vs
+    FP64, with the squared residual norms of both."""
+    import numpy as np
+    from wvlh import workloads as W
+    from wvlh.batch import Batch
+    lr = W.full_periodic(n, 0.45)
+    b = Batch(ctx, [lr], np.zeros(norb, np.int32))
+    rng = np.random.default_rng(seed)
+    cprec = 0.5 - rng.uniform(-1.0, -0.1, norb)
+    g = torch.Generator(device=dev)
+    g.manual_seed(seed)
+    r64 = torch.rand(b.psi_size, generator=g, device=dev, dtype=torch.float64) * 2 - 1
+    r32 = r64.float()
+    x64, x32 = torch.empty_like(r64), torch.empty_like(r32)
+    res = {}
+
+    def run(x, r):
+        x.copy_(r)
+        return b.precond(x, r, cprec, ncong)
+
+    for nm, x, r in (("fp32", x32, r32), ("fp64", x64, r64)):
+        ms = _timed(torch, lambda: run(x, r), 3)
+        _, hist = run(x, r)
+        torch.cuda.synchronize()
+        res[nm] = {"ms": ms, "value": norb * lr.coarse_cells / (ms * 1e-3), "hist": hist.cpu().numpy()}
+    h32, h64 = res["fp32"].pop("hist"), res["fp64"].pop("hist")
+    rel = np.abs(h32 - h64) / np.abs(h64)
+    out = {"workload": "%d orbitals, %d^3 periodic, %d CG iterations" % (norb, n, ncong),
+           "fp32": res["fp32"], "fp64": res["fp64"],
+           "residual_norm2_mean_per_iter_fp64": [float(v) for v in h64.mean(axis=1)],
+           "residual_norm2_max_rel_err_fp32_vs_fp64": float(rel.max()),
+           "x_rel_l2_fp32_vs_fp64": float((x32.double() - x64).norm() / x64.norm())}
+    b.close()
+    return out
+
+
+def leg_density(torch, batch, psi32, psi64, lr, norb, dev):
+    """Density of the batched workload: rho(r) = sum_o 2/vol |psi_o(r)|^2 on the ISF grid."""
+    vol = (0.5 * lr.hgrid[0]) * (0.5 * lr.hgrid[1]) * (0.5 * lr.hgrid[2])
+    hf = torch.full((norb,), 2.0 / vol, dtype=torch.float64, device=dev)
+    r32 = torch.zeros(lr.nisf, dtype=torch.float64, device=dev)
+    r64 = torch.zeros_like(r32)
+
+    def go(psi, rho):
+        rho.zero_()
+        batch.locden(psi, hf, rho)
+
+    ms32 = _timed(torch, lambda: go(psi32, r32), 5)
+    ms64 = _timed(torch, lambda: go(psi64, r64), 3)
+    cells = norb * lr.coarse_cells
+    q32, q64 = r32.sum().item() * vol, r64.sum().item() * vol
+    return {"fp32": {"ms": ms32, "value": cells / (ms32 * 1e-3)}, "fp64": {"ms": ms64, "value": cells / (ms64 * 1e-3)},
+            "rho_rel_l2_fp32_vs_fp64": ((r32 - r64).norm() / r64.norm()).item(), "charge_fp64": q64,
+            "charge_err_fp32": abs(q32 - q64)}
+
+
+def leg_overlap(torch, ctx, psi64, norb):
+    """S = Psi Psi^T (norb x norb, FP64) on FP64 tensor cores vs cuBLAS DGEMM (torch.mm)."""
+    from wvlh.ortho import overlap
+    P = psi64.view(norb, -1)
+    K = P.shape[1]
+    S = torch.empty(norb, norb, dtype=torch.float64, device=P.device)
+    ms = _timed(torch, lambda: overlap(ctx, P, S=S), 5)
+    ms_cublas = _timed(torch, lambda: torch.mm(P, P.T), 5)
+    ref = torch.mm(P, P.T)
+    fl = norb * (norb + 1) * K
+    return {"ms": ms, "tflops": fl / (ms * 1e-3) / 1e12, "cublas_dgemm_ms": ms_cublas,
+            "max_abs_vs_cublas": (S - ref).abs().max().item(), "flops_count": "norb(norb+1)K (SYRK)"}
+
+
+def leg_serve(torch, dev, precision, nreq=300, load=0.7):
+    """Serving loop: 64 clients (coarse 16..64 per dim, periodic or free, 4..128
+    orbitals), requests 50/50 Hpsi and density; capacity from a burst of one
+    request of each kind per client, then Poisson arrivals at load x capacity."""
+    from wvlh import workloads as W
+    from wvlh.serve import Server, latency_stats
+    specs = W.serving_clients()
+    srv = Server(device=dev.index or 0, precision=precision, hbm_budget=150e9, n_slots=2, scratch_per_slot=16e9)
+    cl = [srv.register(lr, n, seed=s) for lr, n, s in specs]
+    cells = {c.id: c.coarse_cells for c in cl}
+    for _ in range(2):
+        t = time.perf_counter()
+        reqs = [srv.submit(c, k) for c in cl for k in ("H", "rho")]
+        srv.drain()
+        dt = time.perf_counter() - t
+    cap = len(reqs) / dt
+    cap_cells = sum(cells[r.client.id] for r in reqs) / dt
+    n0, k0 = srv.launches, srv.kernel_launches
+    t = time.perf_counter()
+    reqs = srv.replay(W.poisson_arrivals(load * cap, nreq, len(cl), seed=11))
+    dt = time.perf_counter() - t
+    st = latency_stats(reqs)
+    out = {"clients": len(cl), "resident_gb": srv.resident / 1e9, "capacity_req_s": cap,
+           "capacity_cells_s": cap_cells, "offered_req_s": load * cap, "served_req_s": len(reqs) / dt,
+           "served_cells_s": sum(cells[r.client.id] for r in reqs) / dt,
+           "p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"], "mean_ms": st["mean_ms"],
+           "launches": srv.launches - n0, "kernel_launches": srv.kernel_launches - k0, "requests": len(reqs)}
+    srv.close()
+    del srv, cl
+    torch.cuda.empty_cache()
+    return out
 
 
 def main():
@@ -321,6 +479,16 @@ def main():
         dt = (time.perf_counter() - t0) / reps
         extras["e2e"] = {"value": pts_step / dt, "unit": UNIT, "h2d_bytes_per_step": hp.numel() * 4 + hv.numel() * 4,
                          "d2h_bytes_per_step": hh.numel() * 4 + 2 * 8 * norb, "ms_per_step": dt * 1e3}
+        # the other rows of the path on this GPU
+        extras["density"] = leg_density(torch, batch, psi32, psi64, lr, norb, dev)
+        extras["overlap"] = leg_overlap(torch, ctx, psi64, norb)
+        del hp, hv, hh
+        extras["free_bc"] = leg_free_regions(torch, ctx, dev)
+        extras["precond"] = leg_precond(torch, ctx, dev)
+        serve = {}
+        for prec in (32, 64):
+            serve["fp%d" % prec] = leg_serve(torch, dev, prec)
+        extras["serve"] = serve
         if ws == 1:
             r, cores, sample = cpu_oracle_rate(n)
             extras["cpu_baseline"] = {"value": r, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample}

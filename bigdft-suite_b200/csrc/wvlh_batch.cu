@@ -331,10 +331,7 @@ static void layout(wvlh_batch *b, const std::vector<int> &orb_lr, const std::vec
         }
     }
     std::vector<OrbDev> od(norb);
-    std::vector<int2> w13;
-    std::vector<int> s13;
-    std::vector<int4> w2, w2p;
-    std::vector<int> s2, s2p, orb_len;
+    std::vector<int> pre13(1, 0), pre2(1, 0), pre2p(1, 0), orb_len;
     std::vector<long long> orb_off;
     long long psi_off = 0, scr = 0;
     int stride = 0;
@@ -370,22 +367,9 @@ static void layout(wvlh_batch *b, const std::vector<int> &orb_lr, const std::vec
         psi_off += len;
         const int ntx0 = (I1 + TX_ - 1) / TX_, nty0 = (I2 + TY_ - 1) / TY_;
         const int ntx1 = (F1 + TX_ - 1) / TX_, nty1 = (F2 + TY_ - 1) / TY_;
-        for (int ty = 0; ty < nty0; ++ty)
-            for (int tx = 0; tx < ntx0; ++tx) {
-                w2.push_back(make_int4(o, 0, tx * TX_, ty * TY_));
-                s2.push_back(ty * ntx0 + tx);
-            }
-        for (int ty = 0; ty < nty1; ++ty)
-            for (int tx = 0; tx < ntx1; ++tx) {
-                w2.push_back(make_int4(o, 1, tx * TX_, ty * TY_));
-                s2.push_back(ty * ntx1 + tx);
-                w2p.push_back(make_int4(o, 1, tx * TX_, ty * TY_));
-                s2p.push_back(ty * ntx1 + tx);
-            }
-        for (int kz = 0; kz < G3; ++kz) {
-            w13.push_back(make_int2(o, kz));
-            s13.push_back(ntx1 * nty1 + kz);
-        }
+        pre13.push_back(pre13.back() + G3);
+        pre2.push_back(pre2.back() + ntx0 * nty0 + ntx1 * nty1);
+        pre2p.push_back(pre2p.back() + ntx1 * nty1);
         stride = std::max(stride, std::max(ntx0 * nty0, ntx1 * nty1 + G3));
         const int pitch = std::max(G1, std::max(F1, I1)) | 1;
         const int rows = std::max(G2, std::max(F2, I2));
@@ -403,9 +387,9 @@ static void layout(wvlh_batch *b, const std::vector<int> &orb_lr, const std::vec
     p.smem13[1] = sm13_elems * sizeof(double);
     p.smem2[0] = sm2_elems * sizeof(float);
     p.smem2[1] = sm2_elems * sizeof(double);
-    p.n_work13 = (int)w13.size();
-    p.n_work2 = (int)w2.size();
-    p.n_work2p = (int)w2p.size();
+    p.n_work13 = pre13.back();
+    p.n_work2 = pre2.back();
+    p.n_work2p = pre2p.back();
     // density: group the orbitals by density grid (same key, one region),
     // split each group in chunks of at most kDenChunk orbitals
     constexpr int kDenChunk = 32;
@@ -416,7 +400,7 @@ static void layout(wvlh_batch *b, const std::vector<int> &orb_lr, const std::vec
     });
     std::vector<int> chunk_start, chunk_orbs, group_chunk_start, group_n;
     std::vector<long long> chunk_part, group_rho;
-    std::vector<int4> wd;
+    std::vector<int> pred(1, 0);
     long long den = 0;
     b->density_ok = true;
     for (int i = 0; i < norb;) {
@@ -440,14 +424,11 @@ static void layout(wvlh_batch *b, const std::vector<int> &orb_lr, const std::vec
         const int nch = std::min(n, std::max(8, (n + kDenChunk - 1) / kDenChunk));
         const int per_chunk = (n + nch - 1) / nch;
         for (int k = i; k < j; k += per_chunk) {
-            const int c = (int)chunk_start.size();
             chunk_start.push_back((int)chunk_orbs.size());
             for (int m = k; m < std::min(j, k + per_chunk); ++m) chunk_orbs.push_back(order[m]);
             chunk_part.push_back(den);
             den += (long long)I1 * I2 * I3;
-            const int ntx = (I1 + TX_ - 1) / TX_, nty = (I2 + TY_ - 1) / TY_;
-            for (int ty = 0; ty < nty; ++ty)
-                for (int tx = 0; tx < ntx; ++tx) wd.push_back(make_int4(c, tx * TX_, ty * TY_, 0));
+            pred.push_back(pred.back() + ((I1 + TX_ - 1) / TX_) * ((I2 + TY_ - 1) / TY_));
         }
         i = j;
     }
@@ -456,16 +437,13 @@ static void layout(wvlh_batch *b, const std::vector<int> &orb_lr, const std::vec
     p.nchunk = (int)chunk_part.size();
     p.ngroup = (int)group_rho.size();
     p.part_den_elems = den;
-    p.n_workd = (int)wd.size();
+    p.n_workd = pred.back();
     pk.add(lrd, &p.d_lr);
     pk.add(od, &p.d_orb);
-    pk.add(w13, &p.d_work13);
-    pk.add(s13, &p.d_part_slot13);
-    pk.add(w2, &p.d_work2);
-    pk.add(s2, &p.d_part_slot2);
-    pk.add(w2p, &p.d_work2p);
-    pk.add(s2p, &p.d_part_slot2p);
-    pk.add(wd, &p.d_workd);
+    pk.add(pre13, &p.d_pre13);
+    pk.add(pre2, &p.d_pre2);
+    pk.add(pre2p, &p.d_pre2p);
+    pk.add(pred, &p.d_pred);
     pk.add(chunk_start, &p.d_chunk_orb_start);
     pk.add(chunk_orbs, &p.d_chunk_orbs);
     pk.add(chunk_part, &p.d_chunk_part);

@@ -175,6 +175,27 @@ __device__ __forceinline__ void load_plane(T *A, int pitch, int rows, int cols, 
     }
 }
 
+// Owner of work item `it` when the items are laid out in runs, one run per
+// orbital (or density chunk): prefix[0..n] ascending, prefix[0] = 0,
+// prefix[n] = total.  Returns the o with prefix[o] <= it < prefix[o+1] by a
+// 32-way search, each lane probing one point per round (the table is small
+// and read by every CTA, so the probes hit L1).  All 32 lanes of the warp
+// must call it.
+__device__ __forceinline__ int find_owner(const int *__restrict__ prefix, int n, int it)
+{
+    const int lane = threadIdx.x & 31;
+    int lo = 0, hi = n;
+    while (hi - lo > 1) {
+        const int step = (hi - lo + 31) >> 5;
+        const int idx = lo + lane * step;
+        const bool le = idx < hi && __ldg(prefix + idx) <= it;
+        const unsigned m = __ballot_sync(0xffffffffu, le);
+        lo += (31 - __clz(m)) * step;
+        hi = min(hi, lo + step);
+    }
+    return lo;
+}
+
 template <class TI>
 __device__ __forceinline__ const TI *in_ptr(const OrbDev &o, const TI *base)
 {
@@ -193,31 +214,28 @@ __device__ __forceinline__ TO *out_ptr(const OrbDev &o, TO *base)
 // Plane kernels (K1, K3) hold two plane buffers A and B in shared memory.
 // When two planes do not fit (FP64 boxes above about 60^3 periodic / 45^3
 // free), B lives in gtmp, a global slice of gstride elements per CTA, and the
-// grid is one CTA per SM looping over the work items (the slice is indexed by
-// blockIdx, so no two running CTAs share it).
+// grid is one CTA per SM looping over the work items (PERSIST; the slice is
+// indexed by blockIdx, so no two running CTAs share it).  Otherwise every CTA
+// runs one item.
 template <class T, class TI, bool ALLPER, int MODE>
-__global__ void __launch_bounds__(kPlaneThreads) k1_plane_forward(const LrDev *__restrict__ lrs,
-                                                                  const OrbDev *__restrict__ orbs,
-                                                                  const int2 *__restrict__ work, int nwork,
-                                                                  const TI *__restrict__ psi, T *__restrict__ scratch,
-                                                                  const double *__restrict__ cprec, T *gtmp,
-                                                                  long long gstride)
+__device__ __forceinline__ void k1_item(const LrDev *__restrict__ lrs, const OrbDev *__restrict__ orbs,
+                                        const int *__restrict__ pre, int norb, const TI *__restrict__ psi,
+                                        T *__restrict__ scratch, const double *__restrict__ cprec, int it, T *sc,
+                                        T *bslice)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    __shared__ T sc[8];
     constexpr int SEG = Seg<T>::v;
-    for (int it = blockIdx.x; it < nwork; it += gridDim.x) {
-        __syncthreads();  // the previous item is done with A, B and sc
-        const int2 w = work[it];
-        const OrbDev o = orbs[w.x];
+    {
+        const int oi = find_owner(pre, norb, it);   // item = (orbital, wavelet plane kz)
+        const int kz = it - pre[oi];
+        const OrbDev o = orbs[oi];
         const LrDev L = lrs[o.lr];
         const Dims d(L, ALLPER);
-        const int kz = w.y;
         const int pitch = d.pitch();
         T *A = reinterpret_cast<T *>(smem_raw);
-        T *B = gtmp ? gtmp + (size_t)blockIdx.x * gstride : A + d.rows() * pitch;
+        T *B = bslice ? bslice : A + d.rows() * pitch;
 
-        if (MODE == MODE_PRECOND && threadIdx.x < 8) sc[threadIdx.x] = (T)prec_scal(L, cprec[w.x], threadIdx.x);
+        if (MODE == MODE_PRECOND && threadIdx.x < 8) sc[threadIdx.x] = (T)prec_scal(L, cprec[oi], threadIdx.x);
         zero_region(A, d.G2, pitch);
         __syncthreads();
         gather_plane<T, TI>(A, pitch, L, kz, in_ptr(o, psi), MODE == MODE_PRECOND ? sc : nullptr);
@@ -227,7 +245,7 @@ __global__ void __launch_bounds__(kPlaneThreads) k1_plane_forward(const LrDev *_
         pass_syn<T, SEG>(B, A, cols_geom(d.F1, pitch), d.N2, d.p2);   // S_y: F1 cols, G2 -> F2
         __syncthreads();
         if (MODE != MODE_LOCDEN) store_plane(A, pitch, d.F2, d.F1, scratch + o.sP + (size_t)kz * d.F2 * d.F1);
-        if (MODE == MODE_PRECOND) continue;
+        if (MODE == MODE_PRECOND) return;
         if (d.p1) pass_mf<T, SEG, 0>(A, B, rows_geom(d.F2, pitch), d.F1, d.I1);
         else pass_mf<T, SEG, 2>(A, B, rows_geom(d.F2, pitch), d.F1, d.I1);
         __syncthreads();
@@ -238,23 +256,52 @@ __global__ void __launch_bounds__(kPlaneThreads) k1_plane_forward(const LrDev *_
     }
 }
 
+template <class T, class TI, bool ALLPER, int MODE, bool PERSIST>
+__global__ void __launch_bounds__(kPlaneThreads) k1_plane_forward(const LrDev *__restrict__ lrs,
+                                                                  const OrbDev *__restrict__ orbs,
+                                                                  const int *__restrict__ pre, int norb,
+                                                                  const TI *__restrict__ psi, T *__restrict__ scratch,
+                                                                  const double *__restrict__ cprec, T *gtmp,
+                                                                  long long gstride)
+{
+    __shared__ T sc[8];
+    if (!PERSIST) {
+        k1_item<T, TI, ALLPER, MODE>(lrs, orbs, pre, norb, psi, scratch, cprec, blockIdx.x, sc, nullptr);
+        return;
+    }
+    const int nwork = pre[norb];
+    for (int it = blockIdx.x; it < nwork; it += gridDim.x) {
+        __syncthreads();  // the previous item is done with A, B and sc
+        k1_item<T, TI, ALLPER, MODE>(lrs, orbs, pre, norb, psi, scratch, cprec, it, sc,
+                                     gtmp + (size_t)blockIdx.x * gstride);
+    }
+}
+
 // ---------------------------------------------------------------------------
 // K2: z-pencil tiles.  chain 0: Z1 = A_z Mt_z (V . M_z S_z Q) in place of Q,
 // E_pot partial.  chain 1: Z2 = A_z K_z S_z P, E_kin(z) partial.
 template <class T, class TV, bool ALLPER>
 __global__ void __launch_bounds__(kZThreads) k2_zpencil(const LrDev *__restrict__ lrs, const OrbDev *__restrict__ orbs,
-                                                        const int4 *__restrict__ work, const int *__restrict__ slots,
+                                                        const int *__restrict__ pre, int norb, int kin_only,
                                                         const TV *__restrict__ pot, T *__restrict__ scratch,
                                                         double *__restrict__ part_pot, double *__restrict__ part_kin,
                                                         int part_stride)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ double red[32];
-    const int4 w = work[blockIdx.x];
-    const OrbDev o = orbs[w.x];
+    // item = (orbital, chain, tile): chain 0 tiles the I1 x I2 plane of Q,
+    // chain 1 the F1 x F2 plane of P (only chain 1 when kin_only), row-major
+    const int oi = find_owner(pre, norb, blockIdx.x);
+    const int j = blockIdx.x - pre[oi];
+    const OrbDev o = orbs[oi];
     const LrDev L = lrs[o.lr];
     const Dims d(L, ALLPER);
-    const int chain = w.y, x0 = w.z, y0 = w.w;
+    const int ntx0 = (d.I1 + TX - 1) / TX, nty0 = (d.I2 + TY - 1) / TY, ntx1 = (d.F1 + TX - 1) / TX;
+    const int chain = (!kin_only && j < ntx0 * nty0) ? 0 : 1;
+    const int jj = chain == 0 ? j : (kin_only ? j : j - ntx0 * nty0);
+    const int ntx = chain == 0 ? ntx0 : ntx1;
+    const int ty = jj / ntx, tx = jj - ty * ntx;   // jj is also the energy slot
+    const int x0 = tx * TX, y0 = ty * TY;
     const int zl = max(d.G3, max(d.F3, d.I3));
     T *A = reinterpret_cast<T *>(smem_raw);
     T *B = A + zl * TC;
@@ -318,41 +365,35 @@ __global__ void __launch_bounds__(kZThreads) k2_zpencil(const LrDev *__restrict_
     }
     const double s = block_sum(e, red);
     if (threadIdx.x == 0 && part_kin)
-        (chain == 0 ? part_pot : part_kin)[(size_t)w.x * part_stride + slots[blockIdx.x]] = s;
+        (chain == 0 ? part_pot : part_kin)[(size_t)oi * part_stride + jj] = s;
 }
 
 // ---------------------------------------------------------------------------
 // K3 (MODE_LOCHAM): Hpsi plane kz = A_x A_y [Mt_x Mt_y Z1 + Z2 + (K_x + K_y) P]
 // K3 (MODE_PRECOND): D^-1/2 A_x A_y [Z2 + c P + (K_x + K_y) P]
 template <class T, class TO, bool ALLPER, int MODE>
-__global__ void __launch_bounds__(kPlaneThreads) k3_plane_backward(const LrDev *__restrict__ lrs,
-                                                                   const OrbDev *__restrict__ orbs,
-                                                                   const int2 *__restrict__ work, int nwork,
-                                                                   const int *__restrict__ slots,
-                                                                   const T *__restrict__ scratch, TO *__restrict__ hpsi,
-                                                                   double *__restrict__ part_kin, int part_stride,
-                                                                   int accumulate, const double *__restrict__ cprec,
-                                                                   T *gtmp, long long gstride)
+__device__ __forceinline__ void k3_item(const LrDev *__restrict__ lrs, const OrbDev *__restrict__ orbs,
+                                        const int *__restrict__ pre, int norb, const T *__restrict__ scratch,
+                                        TO *__restrict__ hpsi, double *__restrict__ part_kin, int part_stride,
+                                        int accumulate, const double *__restrict__ cprec, int it, T *sc,
+                                        double *red, T *bslice)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    __shared__ double red[32];
-    __shared__ T sc[8];
     constexpr int SEG = Seg<T>::v;
-    for (int it = blockIdx.x; it < nwork; it += gridDim.x) {
-        __syncthreads();  // the previous item is done with A, B, sc and red
-        const int2 w = work[it];
-        const OrbDev o = orbs[w.x];
+    {
+        const int oi = find_owner(pre, norb, it);   // item = (orbital, wavelet plane kz)
+        const int kz = it - pre[oi];
+        const OrbDev o = orbs[oi];
         const LrDev L = lrs[o.lr];
         const Dims d(L, ALLPER);
-        const int kz = w.y;
         const int pitch = d.pitch();
         T *A = reinterpret_cast<T *>(smem_raw);
-        T *B = gtmp ? gtmp + (size_t)blockIdx.x * gstride : A + d.rows() * pitch;
+        T *B = bslice ? bslice : A + d.rows() * pitch;
 
         T cshift = T(0);
         if (MODE == MODE_PRECOND) {
-            cshift = (T)cprec[w.x];
-            if (threadIdx.x < 8) sc[threadIdx.x] = (T)prec_scal(L, cprec[w.x], threadIdx.x);
+            cshift = (T)cprec[oi];
+            if (threadIdx.x < 8) sc[threadIdx.x] = (T)prec_scal(L, cprec[oi], threadIdx.x);
         } else {
             load_plane(A, pitch, d.I2, d.I1, scratch + o.sQ + (size_t)kz * d.I2 * d.I1);
             __syncthreads();
@@ -389,7 +430,33 @@ __global__ void __launch_bounds__(kPlaneThreads) k3_plane_backward(const LrDev *
         scatter_plane<T, TO>(A, pitch, L, kz, out_ptr(o, hpsi), accumulate != 0,
                              MODE == MODE_PRECOND ? sc : nullptr);
         const double s = block_sum(e, red);
-        if (threadIdx.x == 0 && part_kin) part_kin[(size_t)w.x * part_stride + slots[it]] = s;
+        // slots 0 .. ntx1*nty1-1 belong to the z kernel's chain-1 tiles
+        const int slot = ((d.F1 + TX - 1) / TX) * ((d.F2 + TY - 1) / TY) + kz;
+        if (threadIdx.x == 0 && part_kin) part_kin[(size_t)oi * part_stride + slot] = s;
+    }
+}
+
+template <class T, class TO, bool ALLPER, int MODE, bool PERSIST>
+__global__ void __launch_bounds__(kPlaneThreads) k3_plane_backward(const LrDev *__restrict__ lrs,
+                                                                   const OrbDev *__restrict__ orbs,
+                                                                   const int *__restrict__ pre, int norb,
+                                                                   const T *__restrict__ scratch, TO *__restrict__ hpsi,
+                                                                   double *__restrict__ part_kin, int part_stride,
+                                                                   int accumulate, const double *__restrict__ cprec,
+                                                                   T *gtmp, long long gstride)
+{
+    __shared__ double red[32];
+    __shared__ T sc[8];
+    if (!PERSIST) {
+        k3_item<T, TO, ALLPER, MODE>(lrs, orbs, pre, norb, scratch, hpsi, part_kin, part_stride, accumulate, cprec,
+                                     blockIdx.x, sc, red, nullptr);
+        return;
+    }
+    const int nwork = pre[norb];
+    for (int it = blockIdx.x; it < nwork; it += gridDim.x) {
+        __syncthreads();  // the previous item is done with A, B, sc and red
+        k3_item<T, TO, ALLPER, MODE>(lrs, orbs, pre, norb, scratch, hpsi, part_kin, part_stride, accumulate, cprec,
+                                     it, sc, red, gtmp + (size_t)blockIdx.x * gstride);
     }
 }
 
@@ -420,7 +487,7 @@ __global__ void k_reduce_energies(const double *__restrict__ part_pot, const dou
 template <class T, bool ALLPER, int MAXP>
 __global__ void __launch_bounds__(kZThreads) kd_density(const LrDev *__restrict__ lrs,
                                                         const OrbDev *__restrict__ orbs,
-                                                        const int4 *__restrict__ work,
+                                                        const int *__restrict__ pre, int nchunk,
                                                         const int *__restrict__ chunk_orb_start,
                                                         const int *__restrict__ chunk_orbs,
                                                         const long long *__restrict__ chunk_part,
@@ -429,12 +496,15 @@ __global__ void __launch_bounds__(kZThreads) kd_density(const LrDev *__restrict_
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     // MAXP accumulators per thread: I3 * TC <= MAXP * kZThreads
-    const int4 w = work[blockIdx.x];
-    const int chunk = w.x, x0 = w.y, y0 = w.z;
+    // item = (chunk, tile of the I1 x I2 plane, row-major)
+    const int chunk = find_owner(pre, nchunk, blockIdx.x);
+    const int j = blockIdx.x - pre[chunk];
     const int ob = chunk_orb_start[chunk], oe = chunk_orb_start[chunk + 1];
     const OrbDev o0 = orbs[chunk_orbs[ob]];
     const LrDev L = lrs[o0.lr];
     const Dims d(L, ALLPER);
+    const int ntx = (d.I1 + TX - 1) / TX;
+    const int x0 = (j % ntx) * TX, y0 = (j / ntx) * TY;
     const int zl = max(d.G3, max(d.F3, d.I3));
     T *A = reinterpret_cast<T *>(smem_raw);
     T *B = A + zl * TC;
@@ -644,9 +714,9 @@ static cudaError_t launch_locham_bc(const Plan &p, const TIO *psi, const TIO *po
     const size_t sm13 = pc.smem, sm2 = p.smem2[fp];
     T *gtmp = pc.global_b ? scratch + p.scratch_elems : nullptr;
     cudaError_t err;
-    auto k1 = k1_plane_forward<T, TIO, ALLPER, MODE_LOCHAM>;
+    auto k1 = pc.global_b ? k1_plane_forward<T, TIO, ALLPER, MODE_LOCHAM, true> : k1_plane_forward<T, TIO, ALLPER, MODE_LOCHAM, false>;
     auto k2 = k2_zpencil<T, TIO, ALLPER>;
-    auto k3 = k3_plane_backward<T, TIO, ALLPER, MODE_LOCHAM>;
+    auto k3 = pc.global_b ? k3_plane_backward<T, TIO, ALLPER, MODE_LOCHAM, true> : k3_plane_backward<T, TIO, ALLPER, MODE_LOCHAM, false>;
     if ((err = cudaFuncSetAttribute(k1, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm13))) return err;
     if ((err = cudaFuncSetAttribute(k2, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm2))) return err;
     if ((err = cudaFuncSetAttribute(k3, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm13))) return err;
@@ -654,14 +724,14 @@ static cudaError_t launch_locham_bc(const Plan &p, const TIO *psi, const TIO *po
     cudaMemsetAsync(part_kin, 0, sizeof(double) * (size_t)p.norb * p.part_stride, st);
     // optional per-kernel timing: ev[0..4] bracket K1, K2, K3 and the reduction
     if (ev) cudaEventRecord(ev[0], st);
-    k1<<<pc.grid, kPlaneThreads, sm13, st>>>(p.d_lr, p.d_orb, p.d_work13, p.n_work13, psi, scratch, nullptr, gtmp,
+    k1<<<pc.grid, kPlaneThreads, sm13, st>>>(p.d_lr, p.d_orb, p.d_pre13, p.norb, psi, scratch, nullptr, gtmp,
                                              pc.gstride);
     if (ev) cudaEventRecord(ev[1], st);
-    k2<<<p.n_work2, kZThreads, sm2, st>>>(p.d_lr, p.d_orb, p.d_work2, p.d_part_slot2, pot, scratch, part_pot,
-                                          part_kin, p.part_stride);
+    k2<<<p.n_work2, kZThreads, sm2, st>>>(p.d_lr, p.d_orb, p.d_pre2, p.norb, 0, pot, scratch, part_pot, part_kin,
+                                          p.part_stride);
     if (ev) cudaEventRecord(ev[2], st);
-    k3<<<pc.grid, kPlaneThreads, sm13, st>>>(p.d_lr, p.d_orb, p.d_work13, p.n_work13, p.d_part_slot13, scratch,
-                                             hpsi, part_kin, p.part_stride, accumulate, nullptr, gtmp, pc.gstride);
+    k3<<<pc.grid, kPlaneThreads, sm13, st>>>(p.d_lr, p.d_orb, p.d_pre13, p.norb, scratch, hpsi, part_kin,
+                                             p.part_stride, accumulate, nullptr, gtmp, pc.gstride);
     if (ev) cudaEventRecord(ev[3], st);
     k_reduce_energies<<<p.norb, 128, 0, st>>>(part_pot, part_kin, p.part_stride, p.norb, ekin, epot);
     if (ev) cudaEventRecord(ev[4], st);
@@ -696,13 +766,13 @@ static cudaError_t launch_locden_bc(const Plan &p, const T *psi, const double *h
     const size_t sm13 = pc.smem, sm2 = p.smem2[fp];
     T *gtmp = pc.global_b ? scratch + p.scratch_elems : nullptr;
     cudaError_t err;
-    auto k1 = k1_plane_forward<T, T, ALLPER, MODE_LOCDEN>;
+    auto k1 = pc.global_b ? k1_plane_forward<T, T, ALLPER, MODE_LOCDEN, true> : k1_plane_forward<T, T, ALLPER, MODE_LOCDEN, false>;
     auto kd = p.den_acc > 32 ? kd_density<T, ALLPER, 48> : kd_density<T, ALLPER, 32>;
     if ((err = cudaFuncSetAttribute(k1, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm13))) return err;
     if ((err = cudaFuncSetAttribute(kd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm2))) return err;
-    k1<<<pc.grid, kPlaneThreads, sm13, st>>>(p.d_lr, p.d_orb, p.d_work13, p.n_work13, psi, scratch, nullptr, gtmp,
+    k1<<<pc.grid, kPlaneThreads, sm13, st>>>(p.d_lr, p.d_orb, p.d_pre13, p.norb, psi, scratch, nullptr, gtmp,
                                              pc.gstride);
-    kd<<<p.n_workd, kZThreads, sm2, st>>>(p.d_lr, p.d_orb, p.d_workd, p.d_chunk_orb_start, p.d_chunk_orbs,
+    kd<<<p.n_workd, kZThreads, sm2, st>>>(p.d_lr, p.d_orb, p.d_pred, p.nchunk, p.d_chunk_orb_start, p.d_chunk_orbs,
                                           p.d_chunk_part, scratch, hfac, part);
     dim3 g((p.max_group_n + 255) / 256 < 4096 ? (p.max_group_n + 255) / 256 : 4096, p.ngroup);
     k_density_reduce<<<g, 256, 0, st>>>(p.d_group_chunk_start, p.d_group_rho, p.d_group_n, p.d_chunk_part, part,
@@ -732,18 +802,18 @@ static cudaError_t launch_prec_apply_bc(const Plan &p, const T *x, T *y, const d
     const size_t sm13 = pc.smem, sm2 = p.smem2[fp];
     T *gtmp = pc.global_b ? scratch + p.scratch_elems : nullptr;
     cudaError_t err;
-    auto k1 = k1_plane_forward<T, T, ALLPER, MODE_PRECOND>;
+    auto k1 = pc.global_b ? k1_plane_forward<T, T, ALLPER, MODE_PRECOND, true> : k1_plane_forward<T, T, ALLPER, MODE_PRECOND, false>;
     auto k2 = k2_zpencil<T, T, ALLPER>;
-    auto k3 = k3_plane_backward<T, T, ALLPER, MODE_PRECOND>;
+    auto k3 = pc.global_b ? k3_plane_backward<T, T, ALLPER, MODE_PRECOND, true> : k3_plane_backward<T, T, ALLPER, MODE_PRECOND, false>;
     if ((err = cudaFuncSetAttribute(k1, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm13))) return err;
     if ((err = cudaFuncSetAttribute(k2, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm2))) return err;
     if ((err = cudaFuncSetAttribute(k3, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm13))) return err;
-    k1<<<pc.grid, kPlaneThreads, sm13, st>>>(p.d_lr, p.d_orb, p.d_work13, p.n_work13, x, scratch, cprec, gtmp,
+    k1<<<pc.grid, kPlaneThreads, sm13, st>>>(p.d_lr, p.d_orb, p.d_pre13, p.norb, x, scratch, cprec, gtmp,
                                              pc.gstride);
-    k2<<<p.n_work2p, kZThreads, sm2, st>>>(p.d_lr, p.d_orb, p.d_work2p, p.d_part_slot2p, (const T *)nullptr,
-                                           scratch, nullptr, nullptr, 0);
-    k3<<<pc.grid, kPlaneThreads, sm13, st>>>(p.d_lr, p.d_orb, p.d_work13, p.n_work13, p.d_part_slot13, scratch, y,
-                                             nullptr, 0, 0, cprec, gtmp, pc.gstride);
+    k2<<<p.n_work2p, kZThreads, sm2, st>>>(p.d_lr, p.d_orb, p.d_pre2p, p.norb, 1, (const T *)nullptr, scratch,
+                                           nullptr, nullptr, 0);
+    k3<<<pc.grid, kPlaneThreads, sm13, st>>>(p.d_lr, p.d_orb, p.d_pre13, p.norb, scratch, y, nullptr, 0, 0, cprec,
+                                             gtmp, pc.gstride);
     return cudaGetLastError();
 }
 

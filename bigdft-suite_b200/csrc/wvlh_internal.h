@@ -65,18 +65,18 @@ struct Plan {
     // device tables
     LrDev *d_lr = nullptr;
     OrbDev *d_orb = nullptr;
-    int2 *d_work13 = nullptr;  // (orb, kz) for the plane kernels
-    int4 *d_work2 = nullptr;   // (orb, chain, x0, y0) for the z kernel
-    int n_work13 = 0, n_work2 = 0;
-    int *d_part_slot13 = nullptr;  // slot of each plane CTA in the energy partials
-    int *d_part_slot2 = nullptr;
-    // preconditioner: z-kernel items of the kinetic chain only
-    int4 *d_work2p = nullptr;
-    int *d_part_slot2p = nullptr;
-    int n_work2p = 0;
-    // density: z-kernel items {chunk, x0, y0, -} over groups of orbitals that
-    // share one density grid (same region, same pot_offset), split in chunks
-    int4 *d_workd = nullptr;
+    // work items in runs of one orbital: prefix sums over the orbitals (norb+1
+    // entries) of the plane kernels' items (G3 wavelet planes each), of the z
+    // kernel's tiles (chain 0 over I1 x I2 then chain 1 over F1 x F2, 32 x 2
+    // columns each) and of the chain-1 tiles alone (preconditioner)
+    int *d_pre13 = nullptr;
+    int *d_pre2 = nullptr;
+    int *d_pre2p = nullptr;
+    int n_work13 = 0, n_work2 = 0, n_work2p = 0;
+    // density: z-kernel tiles of the I1 x I2 plane, in runs of one chunk
+    // (prefix over the chunks) of orbitals that share one density grid (same
+    // region, same density key)
+    int *d_pred = nullptr;
     int n_workd = 0;
     int nchunk = 0, ngroup = 0;
     int *d_chunk_orb_start = nullptr;    // nchunk + 1 offsets into d_chunk_orbs

@@ -66,22 +66,14 @@ __global__ void k_plane_ranges(int n12, int n3, int nseg, const int32_t *__restr
     plane[i3] = lo;
 }
 
-// work lists of one orbital: plane kernels (kz) and z-pencil tiles
-__global__ void k_work_lists(int G3, int ntx0, int nty0, int ntx1, int nty1, int2 *w13, int *s13, int4 *w2, int *s2)
+// work tables of one orbital: {0, G3} plane-kernel items, {0, n2} z-kernel tiles
+__global__ void k_work_lists(int G3, int n2, int *pre13, int *pre2)
 {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    const int n0 = ntx0 * nty0, n1 = ntx1 * nty1;
-    if (i < G3) {
-        w13[i] = make_int2(0, i);
-        s13[i] = n1 + i;
-    }
-    if (i < n0) {
-        w2[i] = make_int4(0, 0, (i % ntx0) * TX_, (i / ntx0) * TY_);
-        s2[i] = i;
-    } else if (i < n0 + n1) {
-        const int k = i - n0;
-        w2[i] = make_int4(0, 1, (k % ntx1) * TX_, (k / ntx1) * TY_);
-        s2[i] = k;
+    if (threadIdx.x == 0) {
+        pre13[0] = 0;
+        pre13[1] = G3;
+        pre2[0] = 0;
+        pre2[1] = n2;
     }
 }
 
@@ -154,10 +146,8 @@ extern "C" int wvlh_locham_noalloc(int precision, const int n[3], const int peri
     const size_t o_sf = off; off = up256(off + 16 * (size_t)nseg_f);
     const size_t o_pc = off; off = up256(off + 4 * (size_t)(N[2] + 1));
     const size_t o_pf = off; off = up256(off + 4 * (size_t)(N[2] + 1));
-    const size_t o_w13 = off; off = up256(off + 8 * (size_t)G[2]);
-    const size_t o_s13 = off; off = up256(off + 4 * (size_t)G[2]);
-    const size_t o_w2 = off; off = up256(off + 16 * (size_t)nw2);
-    const size_t o_s2 = off; off = up256(off + 4 * (size_t)nw2);
+    const size_t o_w13 = off; off = up256(off + 2 * sizeof(int));
+    const size_t o_w2 = off; off = up256(off + 2 * sizeof(int));
     const size_t o_pp = off; off = up256(off + 8 * (size_t)stride);
     const size_t o_pk = off; off = up256(off + 8 * (size_t)stride);
     const size_t o_scr = off; off = up256(off + es * (size_t)(2 * sP + sQ));
@@ -247,10 +237,7 @@ extern "C" int wvlh_locham_noalloc(int precision, const int n[3], const int peri
     }
     k_plane_ranges<<<(N[2] + 256) / 256, 256, 0, st>>>(N[0] * N[1], N[2], nseg_c, dkc, (int *)(base + o_pc));
     k_plane_ranges<<<(N[2] + 256) / 256, 256, 0, st>>>(N[0] * N[1], N[2], nseg_f, dkf, (int *)(base + o_pf));
-    const int nl = G[2] > nw2 ? G[2] : nw2;
-    k_work_lists<<<(nl + 255) / 256, 256, 0, st>>>(G[2], ntx0, nty0, ntx1, nty1, (int2 *)(base + o_w13),
-                                                   (int *)(base + o_s13), (int4 *)(base + o_w2),
-                                                   (int *)(base + o_s2));
+    k_work_lists<<<1, 32, 0, st>>>(G[2], nw2, (int *)(base + o_w13), (int *)(base + o_w2));
     NA_CK(cudaGetLastError());
     // the launch plan lives on the host stack; its device tables point into the static array
     Plan p;
@@ -259,10 +246,8 @@ extern "C" int wvlh_locham_noalloc(int precision, const int n[3], const int peri
     p.all_periodic = per[0] && per[1] && per[2];
     p.d_lr = (LrDev *)(base + o_lr);
     p.d_orb = (OrbDev *)(base + o_orb);
-    p.d_work13 = (int2 *)(base + o_w13);
-    p.d_part_slot13 = (int *)(base + o_s13);
-    p.d_work2 = (int4 *)(base + o_w2);
-    p.d_part_slot2 = (int *)(base + o_s2);
+    p.d_pre13 = (int *)(base + o_w13);
+    p.d_pre2 = (int *)(base + o_w2);
     p.n_work13 = G[2];
     p.n_work2 = nw2;
     p.part_stride = stride;

@@ -34,8 +34,8 @@ def free_sphere(N, hgrid=0.45, radius_frac=0.4):
     return Locreg.from_masks(mask_c, mask_f, (0, 0, 0), (hgrid,) * 3)
 
 
-def gaussian_potential(lr, rng, ngauss=4):
-    """V on the ISF grid of lr, flattened x-fastest (float64)."""
+def _gaussian_factors(lr, rng, ngauss):
+    """Depth and the three 1D factors of each Gaussian of the potential."""
     hf = [0.5 * h for h in lr.hgrid]
     I = lr.isf
     coords = []
@@ -43,7 +43,7 @@ def gaussian_potential(lr, rng, ngauss=4):
         off = 0 if lr.periodic[d] else -14       # ISF index r <-> fine position r-14 (free)
         coords.append((np.arange(I[d]) + off) * hf[d])
     L = [lr.n[d] * lr.hgrid[d] for d in range(3)]
-    V = np.zeros((I[2], I[1], I[0]))
+    out = []
     for _ in range(ngauss):
         cen = [rng.uniform(0, L[d]) for d in range(3)]
         w = rng.uniform(1.0, 3.0)
@@ -54,8 +54,28 @@ def gaussian_potential(lr, rng, ngauss=4):
             if lr.periodic[d]:
                 dx = dx - L[d] * np.round(dx / L[d])
             e.append(np.exp(-dx ** 2 / (2 * w * w)))
+        out.append((dep, e))
+    return out
+
+
+def gaussian_potential(lr, rng, ngauss=4):
+    """V on the ISF grid of lr, flattened x-fastest (float64)."""
+    I = lr.isf
+    V = np.zeros((I[2], I[1], I[0]))
+    for dep, e in _gaussian_factors(lr, rng, ngauss):
         V += dep * e[2][:, None, None] * e[1][None, :, None] * e[0][None, None, :]
     return V.ravel()
+
+
+def gaussian_potential_device(lr, rng, device, ngauss=4):
+    """The same potential (same draws from rng) evaluated on the device (torch float64)."""
+    import torch
+    I = lr.isf
+    V = torch.zeros(I[2], I[1], I[0], dtype=torch.float64, device=device)
+    for dep, e in _gaussian_factors(lr, rng, ngauss):
+        ex, ey, ez = (torch.tensor(v, device=device) for v in e)
+        V += dep * ez[:, None, None] * ey[None, :, None] * ex[None, None, :]
+    return V.reshape(-1)
 
 
 def random_psi(lr, norb, rng, normalize=False):
