@@ -1,0 +1,100 @@
+"""Orbital sharding over GPUs (one process per GPU) and the two exchanges the
+path has: energies and densities.
+
+The reference distributes orbitals over MPI ranks (``orbs%norbp`` /
+``orbs%isorb``, the per-rank loop of ``LocalHamiltonianApplication``,
+``bigdft/src/hpsiortho.f90:934-958``); H psi of an orbital needs nothing from
+other ranks.  The exchanges are:
+
+* energies: a sum over ranks of a few doubles (``fmpi_allreduce`` of the
+  energy terms, ``hpsiortho.f90:1572``) -> :func:`allreduce_energies`;
+* density: each rank's partial rho of its orbitals, summed over ranks and
+  either replicated (all-reduce) or left distributed in z-slabs
+  (``MPI_REDUCE_SCATTER`` in ``communicate_density``, ``sumrho.f90:219``)
+  -> :func:`reduce_density`.
+
+These functions take torch tensors and a ``torch.distributed`` process group:
+NCCL on GPUs, gloo for the CPU tests of this logic.
+"""
+import numpy as np
+
+
+def orbital_cost(locreg):
+    """Relative cost of one orbital of a region: coarse cells plus the fine
+    cells weighted by the seven wavelet components they carry."""
+    return locreg.nvctr_c + 7 * locreg.nvctr_f
+
+
+def shard_orbitals(costs, world_size):
+    """Split orbitals (in order) into world_size contiguous ranges of nearly
+    equal total cost, like the reference's contiguous orbs%isorb ranges.
+    Returns the (start, stop) range of each rank."""
+    costs = np.asarray(costs, np.float64)
+    n = len(costs)
+    if world_size <= 0:
+        raise ValueError("world_size must be positive")
+    cum = np.concatenate([[0.0], np.cumsum(costs)])
+    total = cum[-1]
+    bounds = [0]
+    for r in range(1, world_size):
+        # first index whose prefix reaches r/world of the total, kept monotone
+        b = int(np.searchsorted(cum, total * r / world_size, side="left"))
+        b = min(max(b, bounds[-1]), n)
+        bounds.append(b)
+    bounds.append(n)
+    return [(bounds[r], bounds[r + 1]) for r in range(world_size)]
+
+
+def allreduce_energies(ekin, epot, occ, group=None):
+    """Global E_kin and E_pot: occupation-weighted sums of this rank's
+    per-orbital energies, summed over ranks (FP64).  ekin/epot/occ: tensors
+    of this rank's orbitals (on the process group's device)."""
+    import torch
+    import torch.distributed as dist
+    e = torch.stack([(occ * ekin).sum(), (occ * epot).sum()]).to(torch.float64)
+    if dist.is_initialized() and dist.get_world_size(group) > 1:
+        dist.all_reduce(e, group=group)
+    return float(e[0]), float(e[1])
+
+
+def z_slabs(n3, world_size):
+    """z-planes [start, stop) of each rank's slab of an n3-plane grid (the
+    first n3 % world_size ranks take one plane more)."""
+    base, extra = divmod(n3, world_size)
+    out, s = [], 0
+    for r in range(world_size):
+        k = base + (1 if r < extra else 0)
+        out.append((s, s + k))
+        s += k
+    return out
+
+
+def reduce_density(rho, grid, group=None, scatter=False):
+    """Sum the ranks' partial densities rho (FP64, ISF grid `grid` = (I1, I2,
+    I3), x fastest).  scatter=False: every rank gets the full sum (in place).
+    scatter=True: returns this rank's z-slab (planes of z_slabs) of the sum."""
+    import torch
+    import torch.distributed as dist
+    I1, I2, I3 = grid
+    if rho.numel() != I1 * I2 * I3 or rho.dtype != torch.float64:
+        raise ValueError("rho must be the float64 ISF grid")
+    ws = dist.get_world_size(group) if dist.is_initialized() else 1
+    if not scatter:
+        if ws > 1:
+            dist.all_reduce(rho, group=group)
+        return rho
+    slabs = z_slabs(I3, ws)
+    rank = dist.get_rank(group) if ws > 1 else 0
+    plane = I1 * I2
+    if ws == 1:
+        return rho.view(I3, plane)[slabs[0][0]:slabs[0][1]].reshape(-1)
+    # reduce-scatter wants equal chunks: pad every slab to the largest
+    m = max(b - a for a, b in slabs)
+    src = torch.zeros(ws, m * plane, dtype=rho.dtype, device=rho.device)
+    v = rho.view(I3, plane)
+    for r, (a, b) in enumerate(slabs):
+        src[r, :(b - a) * plane] = v[a:b].reshape(-1)
+    out = torch.empty(m * plane, dtype=rho.dtype, device=rho.device)
+    dist.reduce_scatter_tensor(out, src.reshape(-1), group=group)
+    a, b = slabs[rank]
+    return out[:(b - a) * plane]
