@@ -436,8 +436,10 @@ __device__ __forceinline__ void k3_item(const LrDev *__restrict__ lrs, const Orb
     }
 }
 
+// FP32: 3 CTAs per SM (56 registers), which the 75 KB of shared memory of a
+// 96^2 plane pair allows; FP64 planes leave room for one CTA anyway
 template <class T, class TO, bool ALLPER, int MODE, bool PERSIST>
-__global__ void __launch_bounds__(kPlaneThreads) k3_plane_backward(const LrDev *__restrict__ lrs,
+__global__ void __launch_bounds__(kPlaneThreads, (sizeof(T) == 4 && !PERSIST) ? 3 : 1) k3_plane_backward(const LrDev *__restrict__ lrs,
                                                                    const OrbDev *__restrict__ orbs,
                                                                    const int *__restrict__ pre, int norb,
                                                                    const T *__restrict__ scratch, TO *__restrict__ hpsi,
