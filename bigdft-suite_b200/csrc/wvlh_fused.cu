@@ -196,6 +196,32 @@ __device__ __forceinline__ int find_owner(const int *__restrict__ prefix, int n,
     return lo;
 }
 
+// Asynchronous element copy global -> shared (cp.async, 4 or 8 bytes) with
+// zero fill: every thread queues all its copies of a tile before waiting once,
+// instead of one dependent load/store pair per element.  When !valid nothing
+// is read and the element is set to zero (src is still a valid address).
+template <class T>
+__device__ __forceinline__ void cp_async_elem(T *dst, const T *src, bool valid)
+{
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    const int n = valid ? (int)sizeof(T) : 0;
+    if constexpr (sizeof(T) == 4)
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(d), "l"(src), "r"(n) : "memory");
+    else
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(d), "l"(src), "r"(n) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
+// load_plane through cp.async (A in shared memory); the caller waits
+template <class T>
+__device__ __forceinline__ void load_plane_async(T *A, int pitch, int rows, int cols, const T *g)
+{
+    for (int i = threadIdx.x; i < rows * cols; i += blockDim.x) {
+        const int r = i / cols, c = i - r * cols;
+        cp_async_elem(A + r * pitch + c, g + i, true);
+    }
+}
+
 template <class TI>
 __device__ __forceinline__ const TI *in_ptr(const OrbDev &o, const TI *base)
 {
@@ -316,8 +342,10 @@ __global__ void __launch_bounds__(kZThreads) k2_zpencil(const LrDev *__restrict_
     for (int i = threadIdx.x; i < d.G3 * TC; i += blockDim.x) {
         const int z = i / TC, c = i - z * TC;
         const int x = x0 + (c % TX), y = y0 + (c / TX);
-        A[i] = (x < W && y < H) ? g[(size_t)z * plane + (size_t)y * W + x] : T(0);
+        const bool ok = x < W && y < H;
+        cp_async_elem(A + i, ok ? g + (size_t)z * plane + (size_t)y * W + x : g, ok);
     }
+    cp_async_wait_all();
     __syncthreads();
     const LineGeom zg{TC, 1, TC, 1, TC};
     double e = 0.0;
@@ -331,16 +359,28 @@ __global__ void __launch_bounds__(kZThreads) k2_zpencil(const LrDev *__restrict_
         // per-thread partial sum in T, one FP64 conversion per thread
         const TV *V = o.pot_ptr ? (const TV *)o.pot_ptr : pot + o.pot;
         T ep = T(0);
-        for (int i = threadIdx.x; i < d.I3 * TC; i += blockDim.x) {
-            const int z = i / TC, c = i - z * TC;
-            const int x = x0 + (c % TX), y = y0 + (c / TX);
-            if (x < W && y < H) {
-                const T r = A[i];
-                const T wv = (T)V[((size_t)z * d.I2 + y) * d.I1 + x] * r;
-                ep = fma(wv, r, ep);
-                A[i] = wv;
-            } else {
-                A[i] = T(0);
+        constexpr int U = 4;   // potential loads in flight per thread
+        const int nv = d.I3 * TC;
+        for (int i0 = threadIdx.x; i0 < nv; i0 += U * blockDim.x) {
+            T v[U];
+            bool ok[U];
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                const int i = i0 + u * blockDim.x;
+                const int z = i / TC, c = i - z * TC;
+                const int x = x0 + (c % TX), y = y0 + (c / TX);
+                ok[u] = i < nv && x < W && y < H;
+                v[u] = ok[u] ? (T)V[((size_t)z * d.I2 + y) * d.I1 + x] : T(0);
+            }
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                const int i = i0 + u * blockDim.x;
+                if (i < nv) {
+                    const T r = A[i];
+                    const T wv = v[u] * r;
+                    if (ok[u]) ep = fma(wv, r, ep);
+                    A[i] = ok[u] ? wv : T(0);
+                }
             }
         }
         e += (double)ep;
@@ -395,7 +435,8 @@ __device__ __forceinline__ void k3_item(const LrDev *__restrict__ lrs, const Orb
             cshift = (T)cprec[oi];
             if (threadIdx.x < 8) sc[threadIdx.x] = (T)prec_scal(L, cprec[oi], threadIdx.x);
         } else {
-            load_plane(A, pitch, d.I2, d.I1, scratch + o.sQ + (size_t)kz * d.I2 * d.I1);
+            load_plane_async(A, pitch, d.I2, d.I1, scratch + o.sQ + (size_t)kz * d.I2 * d.I1);
+            cp_async_wait_all();
             __syncthreads();
             if (d.p1) pass_mf<T, SEG, 1>(A, B, rows_geom(d.I2, pitch), d.I1, d.F1);   // Mt_x
             else pass_mf<T, SEG, 3>(A, B, rows_geom(d.I2, pitch), d.I1, d.F1);
@@ -407,12 +448,36 @@ __device__ __forceinline__ void k3_item(const LrDev *__restrict__ lrs, const Orb
         {
             const T *z2 = scratch + o.sZ + (size_t)kz * d.F2 * d.F1;
             const T *p = scratch + o.sP + (size_t)kz * d.F2 * d.F1;
-            for (int i = threadIdx.x; i < d.F2 * d.F1; i += blockDim.x) {
-                const int r = i / d.F1, c = i - r * d.F1;
-                const T pv = p[i];
-                if (MODE == MODE_PRECOND) A[r * pitch + c] = fma(cshift, pv, z2[i]);
-                else A[r * pitch + c] += z2[i];
-                B[r * pitch + c] = pv;
+            const int nf = d.F2 * d.F1;
+            if (MODE != MODE_PRECOND && !bslice) {
+                // P -> B asynchronously while Z2 is added into A, 4 loads in flight
+                load_plane_async(B, pitch, d.F2, d.F1, p);
+                constexpr int U = 4;
+                for (int i0 = threadIdx.x; i0 < nf; i0 += U * blockDim.x) {
+                    T v[U];
+#pragma unroll
+                    for (int u = 0; u < U; ++u) {
+                        const int i = i0 + u * blockDim.x;
+                        v[u] = i < nf ? z2[i] : T(0);
+                    }
+#pragma unroll
+                    for (int u = 0; u < U; ++u) {
+                        const int i = i0 + u * blockDim.x;
+                        if (i < nf) {
+                            const int r = i / d.F1, c = i - r * d.F1;
+                            A[r * pitch + c] += v[u];
+                        }
+                    }
+                }
+                cp_async_wait_all();
+            } else {
+                for (int i = threadIdx.x; i < nf; i += blockDim.x) {
+                    const int r = i / d.F1, c = i - r * d.F1;
+                    const T pv = p[i];
+                    if (MODE == MODE_PRECOND) A[r * pitch + c] = fma(cshift, pv, z2[i]);
+                    else A[r * pitch + c] += z2[i];
+                    B[r * pitch + c] = pv;
+                }
             }
         }
         __syncthreads();
