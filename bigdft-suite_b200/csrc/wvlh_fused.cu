@@ -25,6 +25,8 @@
 // kinetic chain of K2 and K3 (Z2 + c P + (K_x+K_y) P, scaled scatter).
 #include <cuda_runtime.h>
 
+#include <type_traits>
+
 #include "wvlh_common.cuh"
 #include "wvlh_internal.h"
 
@@ -222,6 +224,37 @@ __device__ __forceinline__ void load_plane_async(T *A, int pitch, int rows, int 
     }
 }
 
+// gather_plane through cp.async (no scaling, same element type); the caller
+// waits.  Each coefficient is one queued copy to its slot of the plane.
+template <class T>
+__device__ void gather_plane_async(T *A, int pitch, const LrDev &L, int kz, const T *psi)
+{
+    const int N1 = L.N[0], N2 = L.N[1], N3 = L.N[2];
+    const int s3 = kz >= N3;
+    const int i3 = kz - s3 * N3;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    if (!s3) {
+        const int a = L.plane_c[i3], b = L.plane_c[i3 + 1];
+        for (int sg = a + warp; sg < b; sg += nw) {
+            const int4 d = L.seg_c[sg];
+            for (int t = lane; t < d.z; t += 32) cp_async_elem(A + d.y * pitch + d.x + t, psi + d.w + t, true);
+        }
+    }
+    const T *pf = psi + L.nvctr_c;
+    const int a = L.plane_f[i3], b = L.plane_f[i3 + 1];
+    for (int sg = a + warp; sg < b; sg += nw) {
+        const int4 d = L.seg_f[sg];
+        for (int t = lane; t < d.z; t += 32) {
+            const T *src = pf + 7 * (size_t)(d.w + t);
+#pragma unroll
+            for (int c = 1; c <= 7; ++c) {
+                if (fs3(c) != s3) continue;
+                cp_async_elem(A + (fs2(c) * N2 + d.y) * pitch + fs1(c) * N1 + d.x + t, src + c - 1, true);
+            }
+        }
+    }
+}
+
 template <class TI>
 __device__ __forceinline__ const TI *in_ptr(const OrbDev &o, const TI *base)
 {
@@ -264,7 +297,12 @@ __device__ __forceinline__ void k1_item(const LrDev *__restrict__ lrs, const Orb
         if (MODE == MODE_PRECOND && threadIdx.x < 8) sc[threadIdx.x] = (T)prec_scal(L, cprec[oi], threadIdx.x);
         zero_region(A, d.G2, pitch);
         __syncthreads();
-        gather_plane<T, TI>(A, pitch, L, kz, in_ptr(o, psi), MODE == MODE_PRECOND ? sc : nullptr);
+        if constexpr (MODE != MODE_PRECOND && std::is_same<T, TI>::value) {
+            gather_plane_async<T>(A, pitch, L, kz, in_ptr(o, psi));
+            cp_async_wait_all();
+        } else {
+            gather_plane<T, TI>(A, pitch, L, kz, in_ptr(o, psi), MODE == MODE_PRECOND ? sc : nullptr);
+        }
         __syncthreads();
         pass_syn<T, SEG>(A, B, rows_geom(d.G2, pitch), d.N1, d.p1);   // S_x: G2 rows, G1 -> F1
         __syncthreads();
