@@ -368,7 +368,7 @@ static void layout(wvlh_batch *b, const std::vector<int> &orb_lr, const std::vec
         const int ntx0 = (I1 + TX_ - 1) / TX_, nty0 = (I2 + TY_ - 1) / TY_;
         const int ntx1 = (F1 + TX_ - 1) / TX_, nty1 = (F2 + TY_ - 1) / TY_;
         pre13.push_back(pre13.back() + G3);
-        pre2.push_back(pre2.back() + ntx0 * nty0 + ntx1 * nty1);
+        pre2.push_back(pre2.back() + ntx0 * nty0);
         pre2p.push_back(pre2p.back() + ntx1 * nty1);
         stride = std::max(stride, std::max(ntx0 * nty0, ntx1 * nty1 + G3));
         const int pitch = std::max(G1, std::max(F1, I1)) | 1;

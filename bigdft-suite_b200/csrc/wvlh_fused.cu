@@ -342,29 +342,29 @@ __global__ void __launch_bounds__(kPlaneThreads) k1_plane_forward(const LrDev *_
 }
 
 // ---------------------------------------------------------------------------
-// K2: z-pencil tiles.  chain 0: Z1 = A_z Mt_z (V . M_z S_z Q) in place of Q,
-// E_pot partial.  chain 1: Z2 = A_z K_z S_z P, E_kin(z) partial.
-template <class T, class TV, bool ALLPER>
+// K2: z-pencil tiles, one kernel instance per chain (each half the code of a
+// two-chain kernel, which eases instruction fetch).  CHAIN 0:
+// Z1 = A_z Mt_z (V . M_z S_z Q) in place of Q, E_pot partial.  CHAIN 1:
+// Z2 = A_z K_z S_z P, E_kin(z) partial.
+template <class T, class TV, bool ALLPER, int CHAIN>
 __global__ void __launch_bounds__(kZThreads) k2_zpencil(const LrDev *__restrict__ lrs, const OrbDev *__restrict__ orbs,
-                                                        const int *__restrict__ pre, int norb, int kin_only,
+                                                        const int *__restrict__ pre, int norb,
                                                         const TV *__restrict__ pot, T *__restrict__ scratch,
                                                         double *__restrict__ part_pot, double *__restrict__ part_kin,
                                                         int part_stride)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ double red[32];
-    // item = (orbital, chain, tile): chain 0 tiles the I1 x I2 plane of Q,
-    // chain 1 the F1 x F2 plane of P (only chain 1 when kin_only), row-major
+    // item = (orbital, tile): chain 0 tiles the I1 x I2 plane of Q, chain 1
+    // the F1 x F2 plane of P, row-major; pre is the chain's own prefix table
+    constexpr int chain = CHAIN;
     const int oi = find_owner(pre, norb, blockIdx.x);
-    const int j = blockIdx.x - pre[oi];
+    const int jj = blockIdx.x - pre[oi];   // tile index, also the energy slot
     const OrbDev o = orbs[oi];
     const LrDev L = lrs[o.lr];
     const Dims d(L, ALLPER);
-    const int ntx0 = (d.I1 + TX - 1) / TX, nty0 = (d.I2 + TY - 1) / TY, ntx1 = (d.F1 + TX - 1) / TX;
-    const int chain = (!kin_only && j < ntx0 * nty0) ? 0 : 1;
-    const int jj = chain == 0 ? j : (kin_only ? j : j - ntx0 * nty0);
-    const int ntx = chain == 0 ? ntx0 : ntx1;
-    const int ty = jj / ntx, tx = jj - ty * ntx;   // jj is also the energy slot
+    const int ntx = chain == 0 ? (d.I1 + TX - 1) / TX : (d.F1 + TX - 1) / TX;
+    const int ty = jj / ntx, tx = jj - ty * ntx;
     const int x0 = tx * TX, y0 = ty * TY;
     const int zl = max(d.G3, max(d.F3, d.I3));
     T *A = reinterpret_cast<T *>(smem_raw);
@@ -389,7 +389,7 @@ __global__ void __launch_bounds__(kZThreads) k2_zpencil(const LrDev *__restrict_
     double e = 0.0;
     pass_syn<T, SEG>(A, B, zg, d.N3, d.p3);                      // S_z: G3 -> F3
     __syncthreads();
-    if (chain == 0) {
+    if constexpr (chain == 0) {
         if (d.p3) pass_mf<T, SEG, 0>(B, A, zg, d.F3, d.I3);       // M_z: F3 -> I3
         else pass_mf<T, SEG, 2>(B, A, zg, d.F3, d.I3);
         __syncthreads();
@@ -820,10 +820,12 @@ static cudaError_t launch_locham_bc(const Plan &p, const TIO *psi, const TIO *po
     T *gtmp = pc.global_b ? scratch + p.scratch_elems : nullptr;
     cudaError_t err;
     auto k1 = pc.global_b ? k1_plane_forward<T, TIO, ALLPER, MODE_LOCHAM, true> : k1_plane_forward<T, TIO, ALLPER, MODE_LOCHAM, false>;
-    auto k2 = k2_zpencil<T, TIO, ALLPER>;
+    auto k2 = k2_zpencil<T, TIO, ALLPER, 0>;
+    auto k2k = k2_zpencil<T, TIO, ALLPER, 1>;
     auto k3 = pc.global_b ? k3_plane_backward<T, TIO, ALLPER, MODE_LOCHAM, true> : k3_plane_backward<T, TIO, ALLPER, MODE_LOCHAM, false>;
     if ((err = cudaFuncSetAttribute(k1, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm13))) return err;
     if ((err = cudaFuncSetAttribute(k2, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm2))) return err;
+    if ((err = cudaFuncSetAttribute(k2k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm2))) return err;
     if ((err = cudaFuncSetAttribute(k3, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm13))) return err;
     cudaMemsetAsync(part_pot, 0, sizeof(double) * (size_t)p.norb * p.part_stride, st);
     cudaMemsetAsync(part_kin, 0, sizeof(double) * (size_t)p.norb * p.part_stride, st);
@@ -832,8 +834,10 @@ static cudaError_t launch_locham_bc(const Plan &p, const TIO *psi, const TIO *po
     k1<<<pc.grid, kPlaneThreads, sm13, st>>>(p.d_lr, p.d_orb, p.d_pre13, p.norb, psi, scratch, nullptr, gtmp,
                                              pc.gstride);
     if (ev) cudaEventRecord(ev[1], st);
-    k2<<<p.n_work2, kZThreads, sm2, st>>>(p.d_lr, p.d_orb, p.d_pre2, p.norb, 0, pot, scratch, part_pot, part_kin,
+    k2<<<p.n_work2, kZThreads, sm2, st>>>(p.d_lr, p.d_orb, p.d_pre2, p.norb, pot, scratch, part_pot, part_kin,
                                           p.part_stride);
+    k2k<<<p.n_work2p, kZThreads, sm2, st>>>(p.d_lr, p.d_orb, p.d_pre2p, p.norb, pot, scratch, part_pot, part_kin,
+                                            p.part_stride);
     if (ev) cudaEventRecord(ev[2], st);
     k3<<<pc.grid, kPlaneThreads, sm13, st>>>(p.d_lr, p.d_orb, p.d_pre13, p.norb, scratch, hpsi, part_kin,
                                              p.part_stride, accumulate, nullptr, gtmp, pc.gstride);
@@ -908,14 +912,14 @@ static cudaError_t launch_prec_apply_bc(const Plan &p, const T *x, T *y, const d
     T *gtmp = pc.global_b ? scratch + p.scratch_elems : nullptr;
     cudaError_t err;
     auto k1 = pc.global_b ? k1_plane_forward<T, T, ALLPER, MODE_PRECOND, true> : k1_plane_forward<T, T, ALLPER, MODE_PRECOND, false>;
-    auto k2 = k2_zpencil<T, T, ALLPER>;
+    auto k2 = k2_zpencil<T, T, ALLPER, 1>;
     auto k3 = pc.global_b ? k3_plane_backward<T, T, ALLPER, MODE_PRECOND, true> : k3_plane_backward<T, T, ALLPER, MODE_PRECOND, false>;
     if ((err = cudaFuncSetAttribute(k1, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm13))) return err;
     if ((err = cudaFuncSetAttribute(k2, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm2))) return err;
     if ((err = cudaFuncSetAttribute(k3, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm13))) return err;
     k1<<<pc.grid, kPlaneThreads, sm13, st>>>(p.d_lr, p.d_orb, p.d_pre13, p.norb, x, scratch, cprec, gtmp,
                                              pc.gstride);
-    k2<<<p.n_work2p, kZThreads, sm2, st>>>(p.d_lr, p.d_orb, p.d_pre2p, p.norb, 1, (const T *)nullptr, scratch,
+    k2<<<p.n_work2p, kZThreads, sm2, st>>>(p.d_lr, p.d_orb, p.d_pre2p, p.norb, (const T *)nullptr, scratch,
                                            nullptr, nullptr, 0);
     k3<<<pc.grid, kPlaneThreads, sm13, st>>>(p.d_lr, p.d_orb, p.d_pre13, p.norb, scratch, y, nullptr, 0, 0, cprec,
                                              gtmp, pc.gstride);

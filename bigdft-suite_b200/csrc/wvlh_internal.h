@@ -66,9 +66,9 @@ struct Plan {
     LrDev *d_lr = nullptr;
     OrbDev *d_orb = nullptr;
     // work items in runs of one orbital: prefix sums over the orbitals (norb+1
-    // entries) of the plane kernels' items (G3 wavelet planes each), of the z
-    // kernel's tiles (chain 0 over I1 x I2 then chain 1 over F1 x F2, 32 x 2
-    // columns each) and of the chain-1 tiles alone (preconditioner)
+    // entries) of the plane kernels' items (G3 wavelet planes each) and of the
+    // z kernels' 32 x 2-column tiles: chain 0 over I1 x I2 (d_pre2), chain 1
+    // over F1 x F2 (d_pre2p)
     int *d_pre13 = nullptr;
     int *d_pre2 = nullptr;
     int *d_pre2p = nullptr;

@@ -66,14 +66,17 @@ __global__ void k_plane_ranges(int n12, int n3, int nseg, const int32_t *__restr
     plane[i3] = lo;
 }
 
-// work tables of one orbital: {0, G3} plane-kernel items, {0, n2} z-kernel tiles
-__global__ void k_work_lists(int G3, int n2, int *pre13, int *pre2)
+// work tables of one orbital: {0, G3} plane-kernel items, {0, n2} and {0, n2p}
+// z-kernel tiles of the potential and kinetic chains
+__global__ void k_work_lists(int G3, int n2, int n2p, int *pre13, int *pre2, int *pre2p)
 {
     if (threadIdx.x == 0) {
         pre13[0] = 0;
         pre13[1] = G3;
         pre2[0] = 0;
         pre2[1] = n2;
+        pre2p[0] = 0;
+        pre2p[1] = n2p;
     }
 }
 
@@ -133,7 +136,6 @@ extern "C" int wvlh_locham_noalloc(int precision, const int n[3], const int peri
     const size_t es = precision == 32 ? 4 : 8;
     const int ntx0 = (I[0] + TX_ - 1) / TX_, nty0 = (I[1] + TY_ - 1) / TY_;
     const int ntx1 = (F[0] + TX_ - 1) / TX_, nty1 = (F[1] + TY_ - 1) / TY_;
-    const int nw2 = ntx0 * nty0 + ntx1 * nty1;
     const int stride = (ntx0 * nty0 > ntx1 * nty1 + G[2]) ? ntx0 * nty0 : ntx1 * nty1 + G[2];
     const long long sP = (long long)G[2] * F[1] * F[0], sQ = (long long)G[2] * I[1] * I[0];
     // layout of the static array
@@ -148,6 +150,7 @@ extern "C" int wvlh_locham_noalloc(int precision, const int n[3], const int peri
     const size_t o_pf = off; off = up256(off + 4 * (size_t)(N[2] + 1));
     const size_t o_w13 = off; off = up256(off + 2 * sizeof(int));
     const size_t o_w2 = off; off = up256(off + 2 * sizeof(int));
+    const size_t o_w2p = off; off = up256(off + 2 * sizeof(int));
     const size_t o_pp = off; off = up256(off + 8 * (size_t)stride);
     const size_t o_pk = off; off = up256(off + 8 * (size_t)stride);
     const size_t o_scr = off; off = up256(off + es * (size_t)(2 * sP + sQ));
@@ -237,7 +240,8 @@ extern "C" int wvlh_locham_noalloc(int precision, const int n[3], const int peri
     }
     k_plane_ranges<<<(N[2] + 256) / 256, 256, 0, st>>>(N[0] * N[1], N[2], nseg_c, dkc, (int *)(base + o_pc));
     k_plane_ranges<<<(N[2] + 256) / 256, 256, 0, st>>>(N[0] * N[1], N[2], nseg_f, dkf, (int *)(base + o_pf));
-    k_work_lists<<<1, 32, 0, st>>>(G[2], nw2, (int *)(base + o_w13), (int *)(base + o_w2));
+    k_work_lists<<<1, 32, 0, st>>>(G[2], ntx0 * nty0, ntx1 * nty1, (int *)(base + o_w13), (int *)(base + o_w2),
+                                   (int *)(base + o_w2p));
     NA_CK(cudaGetLastError());
     // the launch plan lives on the host stack; its device tables point into the static array
     Plan p;
@@ -248,8 +252,10 @@ extern "C" int wvlh_locham_noalloc(int precision, const int n[3], const int peri
     p.d_orb = (OrbDev *)(base + o_orb);
     p.d_pre13 = (int *)(base + o_w13);
     p.d_pre2 = (int *)(base + o_w2);
+    p.d_pre2p = (int *)(base + o_w2p);
     p.n_work13 = G[2];
-    p.n_work2 = nw2;
+    p.n_work2 = ntx0 * nty0;
+    p.n_work2p = ntx1 * nty1;
     p.part_stride = stride;
     p.plane_elems = (long long)(rows * pitch);
     p.scratch_elems = 2 * sP + sQ;
