@@ -69,6 +69,7 @@ struct wvlh_ctx {
     // stream order by each new batch, whose generation number it records
     DevBuf arena;
     unsigned long long arena_gen = 0;
+    DevBuf wp_runs;  // compressed scalar products: one run per b segment
 };
 
 // One localisation region: its box and its keys, validated once and kept on
@@ -150,7 +151,7 @@ extern "C" int wvlh_ctx_destroy(wvlh_ctx *ctx)
     cudaStreamSynchronize(ctx->stream);
     for (DevBuf *b : {&ctx->scratch, &ctx->part_pot, &ctx->part_kin, &ctx->io_psi, &ctx->io_pot, &ctx->io_hpsi,
                       &ctx->io_e, &ctx->dotpart, &ctx->cg_r, &ctx->cg_d, &ctx->cg_ad, &ctx->cg_scal, &ctx->den_part,
-                      &ctx->ov_work, &ctx->arena})
+                      &ctx->ov_work, &ctx->arena, &ctx->wp_runs})
         b->release();
     for (auto &b : ctx->plain) b.release();
     for (auto &e : ctx->ev)
@@ -913,4 +914,42 @@ extern "C" void *wvlh_host_alloc(size_t bytes)
 extern "C" void wvlh_host_free(void *p)
 {
     if (p) cudaFreeHost(p);
+}
+
+namespace wvlh {
+template <class T>
+cudaError_t launch_wpdot(int nseg_ac, const uint32_t *kg_ac, const uint32_t *kv_ac, int nseg_af,
+                         const uint32_t *kg_af, const uint32_t *kv_af, int nvc_a, int nseg_bc, const uint32_t *kg_bc,
+                         const uint32_t *kv_bc, int nseg_bf, const uint32_t *kg_bf, const uint32_t *kv_bf, int nvc_b,
+                         int na, const T *a, long long lda, int nb, const T *b, long long ldb, double *out,
+                         int4 *runs, cudaStream_t st);
+}  // namespace wvlh
+
+extern "C" int wvlh_wpdot(wvlh_ctx *c, int precision, const wvlh_region *ra, int na, const void *a, int64_t lda,
+                          const wvlh_region *rb, int nb, const void *b, int64_t ldb, double *out)
+{
+    if (!c || !ra || !rb || !a || !b || !out || na <= 0 || nb <= 0 || (precision != 32 && precision != 64))
+        return fail(WVLH_ERR_ARG);
+    if (ra->device != c->device || rb->device != c->device) return fail(WVLH_ERR_ARG);
+    for (int k = 0; k < 3; ++k)
+        if (ra->lr.N[k] != rb->lr.N[k]) return fail(WVLH_ERR_ARG);  // keys of one box
+    if (lda < wvlh_region_psi_size(ra) || ldb < wvlh_region_psi_size(rb) || na > 65535) return fail(WVLH_ERR_ARG);
+    CK(cudaSetDevice(c->device));
+    const int nrun = rb->lr.nseg_c + rb->lr.nseg_f;
+    int rc;
+    if ((rc = c->wp_runs.ensure(sizeof(int4) * (size_t)(nrun > 0 ? nrun : 1)))) return fail(rc);
+    int4 *runs = (int4 *)c->wp_runs.p;
+    cudaError_t e;
+    if (precision == 64)
+        e = launch_wpdot<double>(ra->lr.nseg_c, ra->keyg_c, ra->keyv_c, ra->lr.nseg_f, ra->keyg_f, ra->keyv_f,
+                                 ra->lr.nvctr_c, rb->lr.nseg_c, rb->keyg_c, rb->keyv_c, rb->lr.nseg_f, rb->keyg_f,
+                                 rb->keyv_f, rb->lr.nvctr_c, na, (const double *)a, lda, nb, (const double *)b, ldb,
+                                 out, runs, c->stream);
+    else
+        e = launch_wpdot<float>(ra->lr.nseg_c, ra->keyg_c, ra->keyv_c, ra->lr.nseg_f, ra->keyg_f, ra->keyv_f,
+                                ra->lr.nvctr_c, rb->lr.nseg_c, rb->keyg_c, rb->keyv_c, rb->lr.nseg_f, rb->keyg_f,
+                                rb->keyv_f, rb->lr.nvctr_c, na, (const float *)a, lda, nb, (const float *)b, ldb, out,
+                                runs, c->stream);
+    CK(e);
+    return WVLH_OK;
 }

@@ -75,7 +75,7 @@ WVLH_SYMBOLS = [
     "wvlh_ctx_enable_timing", "wvlh_ctx_kernel_times", "wvlh_measure_fma_peak",
     "wvlh_locham_noalloc", "wvlh_noalloc_capacity", "wvlh_locden_batched", "wvlh_precond_batched",
     "wvlh_overlap", "wvlh_region_create", "wvlh_region_destroy", "wvlh_region_psi_size",
-    "wvlh_region_grid_size", "wvlh_region_scratch_bytes", "wvlh_batch_create_orbitals",
+    "wvlh_region_grid_size", "wvlh_region_scratch_bytes", "wvlh_batch_create_orbitals", "wvlh_wpdot",
 ]
 
 
@@ -126,6 +126,7 @@ def lib():
     L.wvlh_region_scratch_bytes.restype = C.c_int64
     L.wvlh_region_scratch_bytes.argtypes = [vp, C.c_int]
     L.wvlh_batch_create_orbitals.argtypes = [vp, C.c_int, C.POINTER(OrbitalDesc), C.POINTER(vp)]
+    L.wvlh_wpdot.argtypes = [vp, C.c_int, vp, C.c_int, vp, C.c_int64, vp, C.c_int, vp, C.c_int64, vp]
     L.wvlh_host_alloc.restype = vp
     L.wvlh_host_alloc.argtypes = [C.c_size_t]
     L.wvlh_host_free.argtypes = [vp]

@@ -267,3 +267,22 @@ class OrbitalBatch:
             self.close()
         except Exception:
             pass
+
+
+def scalar_products(ctx, ra, a, rb, b, out=None):
+    """<a_i|b_j> (FP64, (na, nb)) between the rows of a on region ra's keys and
+    the rows of b on region rb's keys, regions of the same box: the
+    reference's wpdot (wavelib/scalprod.f90:3222) on the device.  a, b: 2D
+    device tensors (float32 or float64, same dtype, unit column stride)."""
+    torch = ctx.torch
+    prec = {torch.float32: 32, torch.float64: 64}.get(a.dtype)
+    if prec is None or b.dtype != a.dtype or a.dim() != 2 or b.dim() != 2:
+        raise WvlhError("a and b must be 2D float32 or float64 tensors of one dtype")
+    if a.stride(1) != 1 or b.stride(1) != 1:
+        raise WvlhError("rows must be contiguous")
+    na, nb = a.shape[0], b.shape[0]
+    if out is None:
+        out = torch.empty(na, nb, dtype=torch.float64, device=a.device)
+    check(lib().wvlh_wpdot(ctx.h, prec, ra.h, na, _ptr(a), a.stride(0), rb.h, nb, _ptr(b), b.stride(0),
+                           _ptr(out)), "wvlh_wpdot")
+    return out

@@ -308,6 +308,17 @@ int wvlh_precond_batched(wvlh_batch *batch, int precision, int ncong, const doub
  * reference's getOverlap syrk (wfn_opt/orthogonality.f90:2675) summed in a
  * fixed order. */
 int wvlh_overlap(wvlh_ctx *ctx, int precision, int norb, int64_t K, int64_t ld, const void *psi, double *S);
+/* Compressed scalar products out[i*nb + j] = <a_i|b_j> (FP64) between na
+ * vectors on the keys of region ra (row stride lda) and nb vectors on the
+ * keys of region rb (row stride ldb), both regions with the same box (keys
+ * are linear indices of one grid): the reference's wpdot
+ * (wavelib/scalprod.f90:3222), coarse and 7 fine components, with its
+ * pairing of segments — each b segment takes its overlap with the first a
+ * segment it meets (the whole common part whenever each b segment meets at
+ * most one a segment, as for projectors inside a wavefunction's region).
+ * precision 32: float vectors, FP64 sums; 64: double.  Device pointers. */
+int wvlh_wpdot(wvlh_ctx *ctx, int precision, const wvlh_region *ra, int na, const void *a, int64_t lda,
+               const wvlh_region *rb, int nb, const void *b, int64_t ldb, double *out);
 /* FP64, one kernel per 1D pass (the OpenCL backend's structure) */
 int wvlh_locham_plain_batched(wvlh_batch *batch, const double *psi, const double *pot, double *hpsi,
                               double *ekin, double *epot);

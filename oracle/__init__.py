@@ -76,6 +76,8 @@ def lib():
         L.wo_overlap.argtypes = [C.c_int, C.c_int, f64p, f64p]
         L.wo_cholesky.argtypes = [C.c_int, f64p]
         L.wo_cholesky.restype = C.c_int
+        L.wo_wpdot.argtypes = [C.c_int, i32p, i32p, C.c_int, i32p, i32p, f64p, f64p] * 2
+        L.wo_wpdot.restype = C.c_double
         L.wo_apply_potential.argtypes = [C.c_size_t, f64p, f64p]
         L.wo_apply_potential.restype = C.c_double
         _lib = L
@@ -305,6 +307,20 @@ def cholesky_lower(S):
     if info:
         raise np.linalg.LinAlgError("not positive definite at %d" % info)
     return A.T.copy()
+
+
+def wpdot(ka, a, kb, b):
+    """<a|b> of two compressed vectors on different keys of one box, as the
+    reference's wpdot (wavelib/scalprod.f90:3222) computes it with one thread.
+    ka, kb: (keyg_c, keyv_c, keyg_f, keyv_f) 1-based; a, b: [c | f] vectors."""
+    def parts(k, v):
+        kgc, kvc, kgf, kvf = (np.ascontiguousarray(x, np.int32).ravel() for x in k)
+        nvc = int(sum(kgc[1::2] - kgc[0::2] + 1)) if len(kvc) else 0
+        v = np.ascontiguousarray(v, np.float64)
+        fine = v[nvc:] if len(v) > nvc else np.zeros(7)
+        return [len(kvc), _k(kgc), _k(kvc), len(kvf), _k(kgf), _k(kvf),
+                v[:nvc] if nvc else np.zeros(1), np.ascontiguousarray(fine)]
+    return lib().wo_wpdot(*parts(ka, a), *parts(kb, b))
 
 
 # ---------------------------------------------------------------- reference pin

@@ -783,3 +783,79 @@ int wo_cholesky(int n, double *S)
     }
     return 0;
 }
+
+/* ------------------------------------------------------------------ wpdot
+ * Scalar product of two compressed vectors a and b with different keys of the
+ * same box (wpdot, wavelib/scalprod.f90:3222-3420), as the reference runs it
+ * with one OpenMP thread.  For each b segment [kbs, kbe] (in order):
+ *   jb0 = max(kbs, first a start); the a segment s holding jb0 is found by
+ *   hunt_inline (:3427-3501: the last s with start(s) <= jb0);
+ *   if s reaches jb0 the overlap [jb0, min(kbe, end(s))] is summed, else the
+ *   next a segment, if it starts before kbe, contributes its overlap (:3300-3322);
+ *   only one a segment counts per b segment (the loop exits at the first
+ *   overlap, :3313);
+ *   once a b segment starting after the last a start has been handled with s
+ *   the last a segment, the search index runs past the end and every later b
+ *   segment is skipped (:3323 with hunt_inline's "jlo > n" return, :3439).
+ * Coarse products go to one FP64 sum and each of the 7 fine components to its
+ * own, added at the end (:3404).  Keys are 1-based, keyv the 1-based offset. */
+static int wp_hunt(const int32_t *keyg, int n, int x, int jlo)
+{
+    /* hunt_inline: the last 1-based s with start(s) <= x, 0 when x is below
+     * start(1), the input unchanged when it is past the end (disabled) */
+    if (jlo > n) return jlo;
+    if (x < keyg[0]) return 0;
+    int lo = 0, hi = n - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) / 2;
+        if (keyg[2 * mid] <= x) lo = mid; else hi = mid - 1;
+    }
+    return lo + 1;
+}
+
+static void wp_part(int nseg_a, const int32_t *keyg_a, const int32_t *keyv_a, const double *pa,
+                    int nseg_b, const int32_t *keyg_b, const int32_t *keyv_b, const double *pb,
+                    int ncomp, double *sums)
+{
+    int iaseg0 = 1;
+    if (nseg_a <= 0) return;
+    const int first_a = keyg_a[0], last_a = keyg_a[2 * (nseg_a - 1)];
+    for (int ib = 0; ib < nseg_b; ++ib) {
+        const int kbs = keyg_b[2 * ib], jb1 = keyg_b[2 * ib + 1];
+        int jbj = keyv_b[ib];
+        int jb0 = kbs > first_a ? kbs : first_a;
+        const int iboff = jb0 - kbs > 0 ? jb0 - kbs : 0;
+        iaseg0 = wp_hunt(keyg_a, nseg_a, jb0, iaseg0);
+        if (iaseg0 == 0) { iaseg0 = 1; continue; }
+        while (iaseg0 <= nseg_a) {
+            const int ja0 = keyg_a[2 * (iaseg0 - 1)];
+            const int ea = keyg_a[2 * (iaseg0 - 1) + 1];
+            const int ja1 = jb1 < ea ? jb1 : ea;
+            const int length = ja1 - jb0;
+            const int iaoff = jb0 - ja0 > 0 ? jb0 - ja0 : 0;
+            const int jaj = keyv_a[iaseg0 - 1];
+            for (int i = 0; i <= length; ++i)
+                for (int k = 0; k < ncomp; ++k)
+                    sums[k] += pa[(size_t)(jaj + iaoff + i - 1) * ncomp + k] *
+                               pb[(size_t)(jbj + i + iboff - 1) * ncomp + k];
+            if ((ja1 <= jb1 && length >= 0) || iaseg0 == nseg_a) break;
+            iaseg0 += 1;
+            const int sa = keyg_a[2 * (iaseg0 - 1)];
+            jb0 = kbs > sa ? kbs : sa;
+            if (sa > jb1) break;
+            jbj += jb0 - kbs > 0 ? jb0 - kbs : 0;
+        }
+        if (iaseg0 == nseg_a && kbs > last_a) iaseg0 += 1;
+    }
+}
+
+double wo_wpdot(int nseg_ac, const int32_t *keyg_ac, const int32_t *keyv_ac, int nseg_af, const int32_t *keyg_af,
+                const int32_t *keyv_af, const double *a_c, const double *a_f,
+                int nseg_bc, const int32_t *keyg_bc, const int32_t *keyv_bc, int nseg_bf, const int32_t *keyg_bf,
+                const int32_t *keyv_bf, const double *b_c, const double *b_f)
+{
+    double s[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    wp_part(nseg_ac, keyg_ac, keyv_ac, a_c, nseg_bc, keyg_bc, keyv_bc, b_c, 1, s);
+    wp_part(nseg_af, keyg_af, keyv_af, a_f, nseg_bf, keyg_bf, keyv_bf, b_f, 7, s + 1);
+    return s[0] + s[1] + s[2] + s[3] + s[4] + s[5] + s[6] + s[7];
+}
