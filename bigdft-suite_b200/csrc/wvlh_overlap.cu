@@ -7,26 +7,60 @@
 // S is computed as lower-triangular 64x64 tiles, split over K so that every
 // SM has work; each split writes an FP64 partial tile and a second kernel sums
 // the splits in a fixed order (deterministic) and mirrors the tile into the
-// upper triangle.  The contraction uses mma.sync m8n8k4 with FP64 operands
-// (the FP64 tensor-core instruction of sm_100a; the tcgen05 family has no
-// FP64 kind).  FP32 inputs are widened to FP64 when staged in shared memory.
+// upper triangle.
+//
+// Main loop: a 3-stage cp.async ring stages 64 x 32 slices of the two orbital
+// panels in their storage type (16-byte copies when rows are 16-byte aligned),
+// so the loads of slice s+2 overlap the MMAs of slice s.  The contraction uses
+// mma.sync m16n8k16 with FP64 operands (the largest FP64 tensor-core shape of
+// sm_90+/sm_100a; the tcgen05 family has no FP64 kind): 4 warps, each a 32 x 32
+// sub-tile = 2 x 4 MMA tiles; FP32 rows are widened when fragments are read.
 #include <cuda_runtime.h>
 
 #include <cstdint>
 
 namespace wvlh {
 
-constexpr int OV_BM = 64;      // tile edge (rows = orbitals i, cols = orbitals j)
-constexpr int OV_BK = 32;      // K slice staged per iteration
-constexpr int OV_LD = OV_BK + 2;
+constexpr int OV_BM = 64;       // tile edge (rows = orbitals i, cols = orbitals j)
+constexpr int OV_BK = 32;       // K slice per pipeline stage
+constexpr int OV_STAGES = 3;
 constexpr int OV_THREADS = 128;
 
-__device__ __forceinline__ void dmma_8x8x4(double (&c)[2], double a, double b)
+template <class TI> struct OvLd;   // padded smem row (elements): 16-byte multiple, 2-way bank spread
+template <> struct OvLd<double> { static constexpr int v = 36; };
+template <> struct OvLd<float> { static constexpr int v = 36; };
+
+__host__ __device__ constexpr size_t overlap_smem_bytes(size_t elem)
 {
-    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
-                 : "+d"(c[0]), "+d"(c[1])
-                 : "d"(a), "d"(b));
+    return (size_t)2 * OV_STAGES * OV_BM * 36 * elem;
 }
+
+// D = A(16x16) B(16x8) + D, FP64.  Fragments (lane = 4 g + t):
+// a[i] = A[g + 8 (i & 1)][t + 4 (i >> 1)], b[i] = B[t + 4 i][g],
+// c = {D[g][2t], D[g][2t+1], D[g+8][2t], D[g+8][2t+1]}
+__device__ __forceinline__ void dmma_16x8x16(double (&c)[4], const double (&a)[8], const double (&b)[4])
+{
+    asm volatile(
+        "mma.sync.aligned.m16n8k16.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5,%6,%7,%8,%9,%10,%11}, "
+        "{%12,%13,%14,%15}, {%0,%1,%2,%3};\n"
+        : "+d"(c[0]), "+d"(c[1]), "+d"(c[2]), "+d"(c[3])
+        : "d"(a[0]), "d"(a[1]), "d"(a[2]), "d"(a[3]), "d"(a[4]), "d"(a[5]), "d"(a[6]), "d"(a[7]), "d"(b[0]),
+          "d"(b[1]), "d"(b[2]), "d"(b[3]));
+}
+
+__device__ __forceinline__ void ov_cp_async(void *dst, const void *src, int bytes, int src_bytes)
+{
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    if (bytes == 16)
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(d), "l"(src), "r"(src_bytes) : "memory");
+    else if (bytes == 8)
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(d), "l"(src), "r"(src_bytes) : "memory");
+    else
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(d), "l"(src), "r"(src_bytes) : "memory");
+}
+__device__ __forceinline__ void ov_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void ov_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
 
 // tile t of the lower triangle -> (ti, tj), ti >= tj
 __device__ __forceinline__ void tri_tile(int t, int &ti, int &tj)
@@ -38,13 +72,36 @@ __device__ __forceinline__ void tri_tile(int t, int &ti, int &tj)
     tj = t - i * (i + 1) / 2;
 }
 
-template <class TI>
+// Stage rows r0.. of a 64 x 32 slice starting at column k0 (zero past ke or norb).
+// VEC: bytes per copy (16 when psi rows are 16-byte aligned, else the element size).
+template <class TI, int VEC>
+__device__ __forceinline__ void ov_stage(TI *dst, const TI *__restrict__ psi, long long ld, int row0, int norb,
+                                         long long k0, long long ke)
+{
+    constexpr int LD = OvLd<TI>::v;
+    constexpr int EPV = VEC / (int)sizeof(TI);        // elements per copy
+    constexpr int CPR = OV_BK / EPV;                  // copies per row
+    for (int e = threadIdx.x; e < OV_BM * CPR; e += OV_THREADS) {
+        const int r = e / CPR, c = (e - r * CPR) * EPV;
+        const long long k = k0 + c;
+        const int row = row0 + r;
+        long long nvalid = ke - k;
+        nvalid = nvalid < 0 ? 0 : (nvalid > EPV ? EPV : nvalid);
+        if (row >= norb) nvalid = 0;
+        const TI *src = nvalid ? psi + (size_t)row * ld + k : psi;
+        ov_cp_async(dst + r * LD + c, src, VEC, (int)(nvalid * sizeof(TI)));
+    }
+}
+
+template <class TI, int VEC>
 __global__ void __launch_bounds__(OV_THREADS) k_overlap_partial(int norb, long long K, long long ld,
                                                                 const TI *__restrict__ psi, int nsplit,
                                                                 long long kchunk, double *__restrict__ part)
 {
-    __shared__ double As[OV_BM * OV_LD];
-    __shared__ double Bs[OV_BM * OV_LD];
+    extern __shared__ __align__(16) unsigned char ov_smem[];
+    constexpr int LD = OvLd<TI>::v;
+    TI *As = reinterpret_cast<TI *>(ov_smem);
+    TI *Bs = As + OV_STAGES * OV_BM * LD;
     const int tile = blockIdx.x / nsplit, split = blockIdx.x % nsplit;
     int ti, tj;
     tri_tile(tile, ti, tj);
@@ -52,50 +109,80 @@ __global__ void __launch_bounds__(OV_THREADS) k_overlap_partial(int norb, long l
     const bool diag = ti == tj;
     const long long kb = split * kchunk;
     const long long ke = kb + kchunk < K ? kb + kchunk : K;
+    const int nk = ke > kb ? (int)((ke - kb + OV_BK - 1) / OV_BK) : 0;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int g = lane >> 2, t = lane & 3;
     const int wr = (warp >> 1) * 32, wc = (warp & 1) * 32;   // warp sub-tile origin
-    double acc[4][4][2];
+    // on a diagonal tile the strictly upper 32 x 32 block is not needed
+    const bool idle = diag && wc > wr;
+    double acc[2][4][4];
 #pragma unroll
-    for (int a = 0; a < 4; ++a)
+    for (int a = 0; a < 2; ++a)
 #pragma unroll
-        for (int b = 0; b < 4; ++b) acc[a][b][0] = acc[a][b][1] = 0.0;
+        for (int b = 0; b < 4; ++b)
+#pragma unroll
+            for (int q = 0; q < 4; ++q) acc[a][b][q] = 0.0;
 
-    for (long long k0 = kb; k0 < ke; k0 += OV_BK) {
-        // stage A (rows i0..i0+63) and B (rows j0..), zero outside
-        for (int e = threadIdx.x; e < OV_BM * OV_BK; e += OV_THREADS) {
-            const int r = e / OV_BK, c = e - r * OV_BK;
-            const long long k = k0 + c;
-            const int ia = i0 + r, jb = j0 + r;
-            As[r * OV_LD + c] = (ia < norb && k < ke) ? (double)psi[ia * ld + k] : 0.0;
-            if (!diag) Bs[r * OV_LD + c] = (jb < norb && k < ke) ? (double)psi[jb * ld + k] : 0.0;
+#pragma unroll
+    for (int s = 0; s < OV_STAGES - 1; ++s) {
+        if (s < nk) {
+            ov_stage<TI, VEC>(As + s * OV_BM * LD, psi, ld, i0, norb, kb + (long long)s * OV_BK, ke);
+            if (!diag) ov_stage<TI, VEC>(Bs + s * OV_BM * LD, psi, ld, j0, norb, kb + (long long)s * OV_BK, ke);
         }
-        __syncthreads();
-        const double *Bsrc = diag ? As : Bs;
-#pragma unroll
-        for (int kk = 0; kk < OV_BK; kk += 4) {
-            double fa[4], fb[4];
-#pragma unroll
-            for (int a = 0; a < 4; ++a) fa[a] = As[(wr + 8 * a + (lane >> 2)) * OV_LD + kk + (lane & 3)];
-#pragma unroll
-            for (int b = 0; b < 4; ++b) fb[b] = Bsrc[(wc + 8 * b + (lane >> 2)) * OV_LD + kk + (lane & 3)];
-#pragma unroll
-            for (int a = 0; a < 4; ++a)
-#pragma unroll
-                for (int b = 0; b < 4; ++b) dmma_8x8x4(acc[a][b], fa[a], fb[b]);
-        }
-        __syncthreads();
+        ov_commit();
     }
-    // partial tile, row-major 64x64
-    double *out = part + ((size_t)tile * nsplit + split) * OV_BM * OV_BM;
-#pragma unroll
-    for (int a = 0; a < 4; ++a)
-#pragma unroll
-        for (int b = 0; b < 4; ++b) {
-            const int r = wr + 8 * a + (lane >> 2);
-            const int c = wc + 8 * b + 2 * (lane & 3);
-            out[r * OV_BM + c] = acc[a][b][0];
-            out[r * OV_BM + c + 1] = acc[a][b][1];
+    for (int it = 0; it < nk; ++it) {
+        ov_wait<OV_STAGES - 2>();
+        __syncthreads();   // slice it is visible; slot (it-1) % STAGES is free
+        {
+            const int s = it + OV_STAGES - 1;
+            if (s < nk) {
+                const int slot = s % OV_STAGES;
+                ov_stage<TI, VEC>(As + slot * OV_BM * LD, psi, ld, i0, norb, kb + (long long)s * OV_BK, ke);
+                if (!diag)
+                    ov_stage<TI, VEC>(Bs + slot * OV_BM * LD, psi, ld, j0, norb, kb + (long long)s * OV_BK, ke);
+            }
+            ov_commit();
         }
+        const int slot = it % OV_STAGES;
+        const TI *Ar = As + slot * OV_BM * LD;
+        const TI *Br = (diag ? As : Bs) + slot * OV_BM * LD;
+        if (!idle) {
+#pragma unroll
+            for (int kk = 0; kk < OV_BK; kk += 16) {
+                double fa[2][8], fb[4][4];
+#pragma unroll
+                for (int a = 0; a < 2; ++a)
+#pragma unroll
+                    for (int i = 0; i < 8; ++i)
+                        fa[a][i] = (double)Ar[(wr + 16 * a + g + 8 * (i & 1)) * LD + kk + t + 4 * (i >> 1)];
+#pragma unroll
+                for (int b = 0; b < 4; ++b)
+#pragma unroll
+                    for (int i = 0; i < 4; ++i) fb[b][i] = (double)Br[(wc + 8 * b + g) * LD + kk + t + 4 * i];
+#pragma unroll
+                for (int a = 0; a < 2; ++a)
+#pragma unroll
+                    for (int b = 0; b < 4; ++b) dmma_16x8x16(acc[a][b], fa[a], fb[b]);
+            }
+        }
+    }
+    ov_wait<0>();
+    // partial tile, row-major 64x64 (the idle block of a diagonal tile is never read)
+    double *out = part + ((size_t)tile * nsplit + split) * OV_BM * OV_BM;
+    if (!idle) {
+#pragma unroll
+        for (int a = 0; a < 2; ++a)
+#pragma unroll
+            for (int b = 0; b < 4; ++b) {
+                const int r = wr + 16 * a + g;
+                const int c = wc + 8 * b + 2 * t;
+                out[r * OV_BM + c] = acc[a][b][0];
+                out[r * OV_BM + c + 1] = acc[a][b][1];
+                out[(r + 8) * OV_BM + c] = acc[a][b][2];
+                out[(r + 8) * OV_BM + c + 1] = acc[a][b][3];
+            }
+    }
 }
 
 __global__ void k_overlap_reduce(int norb, int nsplit, const double *__restrict__ part, double *__restrict__ S)
@@ -114,11 +201,12 @@ __global__ void k_overlap_reduce(int norb, int nsplit, const double *__restrict_
     }
 }
 
+// splits over K: about two CTAs per SM (the 3-stage FP64 ring takes 110 KB)
 int overlap_split(int norb, long long K, int nsm)
 {
     const int nt = (norb + OV_BM - 1) / OV_BM;
     const int ntile = nt * (nt + 1) / 2;
-    int nsplit = (4 * nsm + ntile - 1) / ntile;
+    int nsplit = (2 * nsm + ntile - 1) / ntile;
     const long long maxs = (K + OV_BK - 1) / OV_BK;
     if (nsplit > maxs) nsplit = (int)maxs;
     return nsplit < 1 ? 1 : nsplit;
@@ -139,7 +227,19 @@ cudaError_t launch_overlap(int norb, long long K, long long ld, const TI *psi, d
     const int nsplit = overlap_split(norb, K, nsm);
     long long kchunk = (K + nsplit - 1) / nsplit;
     kchunk = (kchunk + OV_BK - 1) / OV_BK * OV_BK;
-    k_overlap_partial<TI><<<ntile * nsplit, OV_THREADS, 0, st>>>(norb, K, ld, psi, nsplit, kchunk, work);
+    const size_t smem = overlap_smem_bytes(sizeof(TI));
+    // 16-byte copies need every row start (and the base) on a 16-byte boundary
+    const bool vec16 = ((uintptr_t)psi % 16 == 0) && ((ld * (long long)sizeof(TI)) % 16 == 0);
+    cudaError_t e;
+    if (vec16) {
+        auto k = k_overlap_partial<TI, 16>;
+        if ((e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem))) return e;
+        k<<<ntile * nsplit, OV_THREADS, smem, st>>>(norb, K, ld, psi, nsplit, kchunk, work);
+    } else {
+        auto k = k_overlap_partial<TI, (int)sizeof(TI)>;
+        if ((e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem))) return e;
+        k<<<ntile * nsplit, OV_THREADS, smem, st>>>(norb, K, ld, psi, nsplit, kchunk, work);
+    }
     k_overlap_reduce<<<ntile, 256, 0, st>>>(norb, nsplit, work, S);
     return cudaGetLastError();
 }

@@ -51,3 +51,18 @@ def test_orthonormalize(oracle, torch_cuda, wctx, method):
         Lref = oracle.cholesky_lower(S.cpu().numpy())
         Lgpu = torch.linalg.cholesky(S).cpu().numpy()
         assert np.abs(Lgpu - Lref).max() / np.abs(Lref).max() < 1e-12
+
+
+@pytest.mark.parametrize("dtype_name,ld", [("float64", 3001), ("float32", 5001)])
+def test_overlap_unaligned_rows(oracle, torch_cuda, wctx, dtype_name, ld):
+    """Row strides that are not 16-byte multiples take the element-copy path."""
+    torch = torch_cuda
+    rng = np.random.default_rng(ld)
+    full = rng.uniform(-1, 1, (70, ld))
+    dt = getattr(torch, dtype_name)
+    t = torch.tensor(full, dtype=dt, device="cuda")
+    K = ld - 37
+    S = overlap(wctx, t[:, :K]).cpu().numpy()
+    src = full[:, :K].astype(np.float32).astype(np.float64) if dtype_name == "float32" else full[:, :K]
+    ref = oracle.overlap(np.ascontiguousarray(src))
+    assert np.abs(S - ref).max() / np.abs(ref).max() < 1e-13
