@@ -60,11 +60,15 @@ __host__ __device__ constexpr bool big_tap(double v, double thr) { return v > th
 __host__ __device__ __forceinline__ int fine_len(int N, int per) { return per ? 2 * N : 2 * N + 14; }
 __host__ __device__ __forceinline__ int isf_len(int N, int per) { return per ? 2 * N : 2 * N + 29; }
 
-__device__ __forceinline__ int wrapi(int p, int L)
+// Periodic index for -L <= p < 3L, without a division.  The fused passes only
+// see periodic lines of at least 8 coarse / 16 fine points, and their windows
+// reach at most 15 points below and SEG + 13 (<= 21) points above the line.
+__device__ __forceinline__ int wrap_near(int p, int L)
 {
-    if ((unsigned)p < (unsigned)L) return p;
-    p %= L;
-    return p < 0 ? p + L : p;
+    p += p < 0 ? L : 0;
+    p -= p >= L ? L : 0;
+    p -= p >= L ? L : 0;
+    return p;
 }
 
 // Load x[k] = line(p0 + k), k < W, with periodic wrap or zero padding; the
@@ -78,7 +82,7 @@ __device__ __forceinline__ void load_window(T (&x)[W], const T *in, int ps, int 
         for (int k = 0; k < W; ++k) x[k] = b[k * ps];
     } else if (per) {
 #pragma unroll
-        for (int k = 0; k < W; ++k) x[k] = in[wrapi(p0 + k, L) * ps];
+        for (int k = 0; k < W; ++k) x[k] = in[wrap_near(p0 + k, L) * ps];
     } else {
 #pragma unroll
         for (int k = 0; k < W; ++k) {
@@ -94,12 +98,43 @@ __device__ __forceinline__ void load_window(T (&x)[W], const T *in, int ps, int 
 template <class F>
 __device__ __forceinline__ void for_items(int nlines, int nseg, F &&f)
 {
+    // item it = s * nlines + line, stepped by blockDim with one division per pass
     const int items = nlines * nseg;
-    for (int it = threadIdx.x; it < items; it += blockDim.x) {
-        const int s = it / nlines;
-        f(it - s * nlines, s);
+    const int bd = blockDim.x;
+    int s = threadIdx.x / nlines, line = threadIdx.x - s * nlines;
+    const int ds = bd / nlines, dl = bd - ds * nlines;
+    for (int it = threadIdx.x; it < items; it += bd) {
+        f(line, s);
+        line += dl;
+        s += ds;
+        if (line >= nlines) {
+            line -= nlines;
+            ++s;
+        }
     }
 }
+
+// (row, col) of element i = row * cols + col for i = threadIdx.x + k * blockDim.x,
+// advanced without a division per element
+struct RowCol {
+    int r, c, dr, dc, cols;
+    __device__ __forceinline__ explicit RowCol(int cols_) : cols(cols_)
+    {
+        r = threadIdx.x / cols;
+        c = threadIdx.x - r * cols;
+        dr = blockDim.x / cols;
+        dc = blockDim.x - dr * cols;
+    }
+    __device__ __forceinline__ void next()
+    {
+        c += dc;
+        r += dr;
+        if (c >= cols) {
+            c -= cols;
+            ++r;
+        }
+    }
+};
 
 struct LineGeom {
     int nlines;

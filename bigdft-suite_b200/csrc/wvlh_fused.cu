@@ -162,19 +162,15 @@ __device__ __forceinline__ void zero_region(T *A, int rows, int pitch)
 template <class T>
 __device__ __forceinline__ void store_plane(const T *A, int pitch, int rows, int cols, T *g)
 {
-    for (int i = threadIdx.x; i < rows * cols; i += blockDim.x) {
-        const int r = i / cols, c = i - r * cols;
-        g[i] = A[r * pitch + c];
-    }
+    RowCol q(cols);
+    for (int i = threadIdx.x; i < rows * cols; i += blockDim.x, q.next()) g[i] = A[q.r * pitch + q.c];
 }
 
 template <class T>
 __device__ __forceinline__ void load_plane(T *A, int pitch, int rows, int cols, const T *g)
 {
-    for (int i = threadIdx.x; i < rows * cols; i += blockDim.x) {
-        const int r = i / cols, c = i - r * cols;
-        A[r * pitch + c] = g[i];
-    }
+    RowCol q(cols);
+    for (int i = threadIdx.x; i < rows * cols; i += blockDim.x, q.next()) A[q.r * pitch + q.c] = g[i];
 }
 
 // Owner of work item `it` when the items are laid out in runs, one run per
@@ -218,10 +214,9 @@ __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wai
 template <class T>
 __device__ __forceinline__ void load_plane_async(T *A, int pitch, int rows, int cols, const T *g)
 {
-    for (int i = threadIdx.x; i < rows * cols; i += blockDim.x) {
-        const int r = i / cols, c = i - r * cols;
-        cp_async_elem(A + r * pitch + c, g + i, true);
-    }
+    RowCol q(cols);
+    for (int i = threadIdx.x; i < rows * cols; i += blockDim.x, q.next())
+        cp_async_elem(A + q.r * pitch + q.c, g + i, true);
 }
 
 // gather_plane through cp.async (no scaling, same element type); the caller
@@ -321,7 +316,7 @@ __device__ __forceinline__ void k1_item(const LrDev *__restrict__ lrs, const Orb
 }
 
 template <class T, class TI, bool ALLPER, int MODE, bool PERSIST>
-__global__ void __launch_bounds__(kPlaneThreads) k1_plane_forward(const LrDev *__restrict__ lrs,
+__global__ void __launch_bounds__(kPlaneThreads, (sizeof(T) == 4 && !PERSIST) ? 3 : 1) k1_plane_forward(const LrDev *__restrict__ lrs,
                                                                   const OrbDev *__restrict__ orbs,
                                                                   const int *__restrict__ pre, int norb,
                                                                   const TI *__restrict__ psi, T *__restrict__ scratch,
@@ -491,6 +486,7 @@ __device__ __forceinline__ void k3_item(const LrDev *__restrict__ lrs, const Orb
                 // P -> B asynchronously while Z2 is added into A, 4 loads in flight
                 load_plane_async(B, pitch, d.F2, d.F1, p);
                 constexpr int U = 4;
+                RowCol q(d.F1);
                 for (int i0 = threadIdx.x; i0 < nf; i0 += U * blockDim.x) {
                     T v[U];
 #pragma unroll
@@ -500,21 +496,19 @@ __device__ __forceinline__ void k3_item(const LrDev *__restrict__ lrs, const Orb
                     }
 #pragma unroll
                     for (int u = 0; u < U; ++u) {
-                        const int i = i0 + u * blockDim.x;
-                        if (i < nf) {
-                            const int r = i / d.F1, c = i - r * d.F1;
-                            A[r * pitch + c] += v[u];
-                        }
+                        if (i0 + u * (int)blockDim.x < nf) A[q.r * pitch + q.c] += v[u];
+                        q.next();
                     }
                 }
                 cp_async_wait_all();
             } else {
-                for (int i = threadIdx.x; i < nf; i += blockDim.x) {
-                    const int r = i / d.F1, c = i - r * d.F1;
+                RowCol q(d.F1);
+                for (int i = threadIdx.x; i < nf; i += blockDim.x, q.next()) {
+                    const int e = q.r * pitch + q.c;
                     const T pv = p[i];
-                    if (MODE == MODE_PRECOND) A[r * pitch + c] = fma(cshift, pv, z2[i]);
-                    else A[r * pitch + c] += z2[i];
-                    B[r * pitch + c] = pv;
+                    if (MODE == MODE_PRECOND) A[e] = fma(cshift, pv, z2[i]);
+                    else A[e] += z2[i];
+                    B[e] = pv;
                 }
             }
         }
