@@ -145,7 +145,7 @@ struct LineGeom {
 // ---------------------------------------------------------------- synthesis
 // src line: [s(0..N-1) | w(0..N-1)], dst line: F = fine_len(N,per) values.
 template <class T, int SEG>
-__device__ void pass_syn(const T *src, T *dst, const LineGeom g, int N, int per)
+__device__ __forceinline__ void pass_syn(const T *src, T *dst, const LineGeom g, int N, int per)
 {
     static_assert(SEG % 2 == 0, "even segment");
     constexpr int W = SEG / 2 + 8;
@@ -192,7 +192,7 @@ __device__ void pass_syn(const T *src, T *dst, const LineGeom g, int N, int per)
 // ---------------------------------------------------------------- analysis
 // src line: F fine values; dst line: [c(0..N-1) | d(0..N-1)]
 template <class T, int SEG>
-__device__ void pass_ana(const T *src, T *dst, const LineGeom g, int N, int per)
+__device__ __forceinline__ void pass_ana(const T *src, T *dst, const LineGeom g, int N, int per)
 {
     static_assert(SEG % 2 == 0, "even segment");
     constexpr int H = SEG / 2;
@@ -226,7 +226,7 @@ __device__ void pass_ana(const T *src, T *dst, const LineGeom g, int N, int per)
 // ---------------------------------------------------------------- magic filter
 // MODE 0: mf periodic, 1: mft periodic, 2: mf grow (F -> F+15), 3: mft shrink (F+15 -> F)
 template <class T, int SEG, int MODE>
-__device__ void pass_mf(const T *src, T *dst, const LineGeom g, int Lin, int Lout)
+__device__ __forceinline__ void pass_mf(const T *src, T *dst, const LineGeom g, int Lin, int Lout)
 {
     constexpr int W = SEG + 15;
     constexpr int shift = MODE == 0 ? -8 : MODE == 1 ? -7 : MODE == 2 ? -15 : 0;
@@ -262,7 +262,7 @@ __device__ void pass_mf(const T *src, T *dst, const LineGeom g, int Lin, int Lou
 // with scale = -1/(2h^2) (cshift: the preconditioner's c of (T + c),
 // OpenCL/Preconditioner.c:108); ekin += src(q) * scale * conv in FP64.
 template <class T, int SEG, bool ACC>
-__device__ void pass_kin(const T *src, T *dst, const LineGeom g, int L, int per, double scale_d, T cshift,
+__device__ __forceinline__ void pass_kin(const T *src, T *dst, const LineGeom g, int L, int per, double scale_d, T cshift,
                          double *ekin)
 {
     constexpr int W = SEG + 28;

@@ -370,14 +370,16 @@ __global__ void __launch_bounds__(kZThreads) k2_zpencil(const LrDev *__restrict_
     T *g = scratch + (chain == 0 ? o.sQ : o.sP);
     T *gz = scratch + (chain == 0 ? o.sQ : o.sZ);
     const size_t plane = (size_t)W * H;
+    // element loops: thread t owns tile column c = t % TC at z = t / TC + k ZS
+    constexpr int ZS = kZThreads / TC;
+    const int col = threadIdx.x % TC, zs = threadIdx.x / TC;
+    const int xc = x0 + (col % TX), yc = y0 + (col / TX);
+    const bool inside = xc < W && yc < H;
+    const size_t colofs = (size_t)yc * W + xc;
 
     // load the tile: TC columns x G3 z' rows, zero outside the plane
-    for (int i = threadIdx.x; i < d.G3 * TC; i += blockDim.x) {
-        const int z = i / TC, c = i - z * TC;
-        const int x = x0 + (c % TX), y = y0 + (c / TX);
-        const bool ok = x < W && y < H;
-        cp_async_elem(A + i, ok ? g + (size_t)z * plane + (size_t)y * W + x : g, ok);
-    }
+    for (int z = zs; z < d.G3; z += ZS)
+        cp_async_elem(A + z * TC + col, inside ? g + (size_t)z * plane + colofs : g, inside);
     cp_async_wait_all();
     __syncthreads();
     const LineGeom zg{TC, 1, TC, 1, TC};
@@ -393,26 +395,22 @@ __global__ void __launch_bounds__(kZThreads) k2_zpencil(const LrDev *__restrict_
         const TV *V = o.pot_ptr ? (const TV *)o.pot_ptr : pot + o.pot;
         T ep = T(0);
         constexpr int U = 4;   // potential loads in flight per thread
-        const int nv = d.I3 * TC;
-        for (int i0 = threadIdx.x; i0 < nv; i0 += U * blockDim.x) {
+        const TV *vc = V + colofs;   // chain 0: W, H are I1, I2, the potential's plane
+        for (int z0 = zs; z0 < d.I3; z0 += U * ZS) {
             T v[U];
-            bool ok[U];
 #pragma unroll
             for (int u = 0; u < U; ++u) {
-                const int i = i0 + u * blockDim.x;
-                const int z = i / TC, c = i - z * TC;
-                const int x = x0 + (c % TX), y = y0 + (c / TX);
-                ok[u] = i < nv && x < W && y < H;
-                v[u] = ok[u] ? (T)V[((size_t)z * d.I2 + y) * d.I1 + x] : T(0);
+                const int z = z0 + u * ZS;
+                v[u] = (inside && z < d.I3) ? (T)vc[(size_t)z * plane] : T(0);
             }
 #pragma unroll
             for (int u = 0; u < U; ++u) {
-                const int i = i0 + u * blockDim.x;
-                if (i < nv) {
-                    const T r = A[i];
+                const int z = z0 + u * ZS;
+                if (z < d.I3) {
+                    const T r = A[z * TC + col];
                     const T wv = v[u] * r;
-                    if (ok[u]) ep = fma(wv, r, ep);
-                    A[i] = ok[u] ? wv : T(0);
+                    if (inside) ep = fma(wv, r, ep);
+                    A[z * TC + col] = inside ? wv : T(0);
                 }
             }
         }
@@ -431,11 +429,8 @@ __global__ void __launch_bounds__(kZThreads) k2_zpencil(const LrDev *__restrict_
         T *t = A; A = B; B = t;                                   // result in A
     }
     __syncthreads();
-    for (int i = threadIdx.x; i < d.G3 * TC; i += blockDim.x) {
-        const int z = i / TC, c = i - z * TC;
-        const int x = x0 + (c % TX), y = y0 + (c / TX);
-        if (x < W && y < H) gz[(size_t)z * plane + (size_t)y * W + x] = A[i];
-    }
+    if (inside)
+        for (int z = zs; z < d.G3; z += ZS) gz[(size_t)z * plane + colofs] = A[z * TC + col];
     const double s = block_sum(e, red);
     if (threadIdx.x == 0 && part_kin)
         (chain == 0 ? part_pot : part_kin)[(size_t)oi * part_stride + jj] = s;
@@ -611,6 +606,12 @@ __global__ void __launch_bounds__(kZThreads) kd_density(const LrDev *__restrict_
     const int W = d.I1, H = d.I2;
     const size_t plane = (size_t)W * H;
     const LineGeom zg{TC, 1, TC, 1, TC};
+    // thread t owns tile column c = t % TC at z = t / TC + k ZS
+    constexpr int ZS = kZThreads / TC;
+    const int col = threadIdx.x % TC, zs = threadIdx.x / TC;
+    const int xc = x0 + (col % TX), yc = y0 + (col / TX);
+    const bool inside = xc < W && yc < H;
+    const size_t colofs = (size_t)yc * W + xc;
     double acc[MAXP];
 #pragma unroll
     for (int k = 0; k < MAXP; ++k) acc[k] = 0.0;
@@ -619,11 +620,9 @@ __global__ void __launch_bounds__(kZThreads) kd_density(const LrDev *__restrict_
         const OrbDev o = orbs[orb];
         const T *g = scratch + o.sQ;
         __syncthreads();
-        for (int i = threadIdx.x; i < d.G3 * TC; i += blockDim.x) {
-            const int z = i / TC, c = i - z * TC;
-            const int x = x0 + (c % TX), y = y0 + (c / TX);
-            A[i] = (x < W && y < H) ? g[(size_t)z * plane + (size_t)y * W + x] : T(0);
-        }
+        for (int z = zs; z < d.G3; z += ZS)
+            cp_async_elem(A + z * TC + col, inside ? g + (size_t)z * plane + colofs : g, inside);
+        cp_async_wait_all();
         __syncthreads();
         pass_syn<T, SEG>(A, B, zg, d.N3, d.p3);                  // S_z
         __syncthreads();
