@@ -426,10 +426,11 @@ def main():
         tf32 = C.c_double()
         lib().wvlh_measure_fma_peak(32, 20000, C.byref(tf32))
         ach = kbytes[dom] / (kt[dom] * 1e-3) / 1e9
-        # DRAM traffic of the z kernels (both chains): dram__bytes_read.sum + dram__bytes_write.sum
-        # from an ncu capture of one call over 48 orbitals of this 48^3 FP32 workload (582.587 MB),
-        # scaled by the orbitals of this launch (the traffic grows in proportion to them)
-        traffic = 582.587392e6 / 48 * norb if (dom == 1 and n == 48) else None
+        # DRAM traffic of each kernel (dram__bytes_read.sum + dram__bytes_write.sum) from ncu
+        # captures of one call over 48 orbitals of this 48^3 FP32 workload, scaled by the orbitals
+        # of this launch (the traffic grows in proportion to them); z kernels: both chains
+        traffic48 = [453.238528e6, 581.659136e6, 657.60768e6]
+        traffic = traffic48[dom] / 48 * norb if (dom < 3 and n == 48) else None
         extras["roofline"] = {"bound": "hbm", "achieved": ach, "peak": hbm, "unit": "GB/s", "frac": ach / hbm,
                               "traffic": traffic, "kernel": names[dom], "peak_source": hbm_src,
                               "algorithmic_bytes_per_launch": kbytes[dom]}

@@ -342,7 +342,7 @@ __global__ void __launch_bounds__(kPlaneThreads, (sizeof(T) == 4 && !PERSIST) ? 
 // Z1 = A_z Mt_z (V . M_z S_z Q) in place of Q, E_pot partial.  CHAIN 1:
 // Z2 = A_z K_z S_z P, E_kin(z) partial.
 template <class T, class TV, bool ALLPER, int CHAIN>
-__global__ void __launch_bounds__(kZThreads) k2_zpencil(const LrDev *__restrict__ lrs, const OrbDev *__restrict__ orbs,
+__global__ void __launch_bounds__(kZThreads, sizeof(T) == 4 ? 4 : 1) k2_zpencil(const LrDev *__restrict__ lrs, const OrbDev *__restrict__ orbs,
                                                         const int *__restrict__ pre, int norb,
                                                         const TV *__restrict__ pot, T *__restrict__ scratch,
                                                         double *__restrict__ part_pot, double *__restrict__ part_kin,
