@@ -336,7 +336,7 @@ static void layout(wvlh_batch *b, const std::vector<int> &orb_lr, const std::vec
     std::vector<long long> orb_off;
     long long psi_off = 0, scr = 0;
     int stride = 0;
-    size_t sm13_elems = 0, sm2_elems = 0;
+    size_t planeA = 0, planeB = 0, sm2_elems = 0;
     b->pot_off.assign(pot_key.begin(), pot_key.end());
     for (int o = 0; o < norb; ++o) {
         const int l = orb_lr[o];
@@ -372,9 +372,13 @@ static void layout(wvlh_batch *b, const std::vector<int> &orb_lr, const std::vec
         pre2.push_back(pre2.back() + ntx0 * nty0);
         pre2p.push_back(pre2p.back() + ntx1 * nty1);
         stride = std::max(stride, std::max(ntx0 * nty0, ntx1 * nty1 + G3));
+        // plane buffer A: rows (y) x pitch (x); B also holds transposed planes:
+        // rowsT (x) x pitchT (y)
         const int pitch = std::max(G1, std::max(F1, I1)) | 1;
         const int rows = std::max(G2, std::max(F2, I2));
-        sm13_elems = std::max(sm13_elems, (size_t)2 * rows * pitch);
+        const int rowsT = std::max(G1, std::max(F1, I1)), pitchT = rows | 1;
+        planeA = std::max(planeA, (size_t)rows * pitch);
+        planeB = std::max(planeB, std::max((size_t)rows * pitch, (size_t)rowsT * pitchT));
         const int zl = std::max(G3, std::max(F3, I3));
         sm2_elems = std::max(sm2_elems, (size_t)2 * zl * TX_ * TY_);
     }
@@ -383,9 +387,10 @@ static void layout(wvlh_batch *b, const std::vector<int> &orb_lr, const std::vec
     for (int v : p.lr_per) p.all_periodic = p.all_periodic && v == 1;
     p.scratch_elems = scr;
     p.part_stride = stride;
-    p.plane_elems = (long long)(sm13_elems / 2);
-    p.smem13[0] = sm13_elems * sizeof(float);
-    p.smem13[1] = sm13_elems * sizeof(double);
+    p.plane_elems = (long long)planeA;
+    p.planeB_elems = (long long)planeB;
+    p.smem13[0] = (planeA + planeB) * sizeof(float);
+    p.smem13[1] = (planeA + planeB) * sizeof(double);
     p.smem2[0] = sm2_elems * sizeof(float);
     p.smem2[1] = sm2_elems * sizeof(double);
     p.n_work13 = pre13.back();
@@ -587,7 +592,7 @@ extern "C" int wvlh_locham_batched(wvlh_batch *b, int precision, const void *psi
     const Plan &p = b->plan;
     const int fp = precision == 64;
     const size_t lim = sm_limit() - 1024;
-    if (p.smem13[fp] / 2 > lim || p.smem2[fp] > lim) return fail(WVLH_ERR_TOO_LARGE);
+    if ((size_t)p.plane_elems * (fp ? 8 : 4) > lim || p.smem2[fp] > lim) return fail(WVLH_ERR_TOO_LARGE);
     if ((rc = c->scratch.ensure((p.scratch_elems + plane_tmp_elems(p, fp)) * (fp ? 8 : 4))) ||
         (rc = c->part_pot.ensure(sizeof(double) * (size_t)p.norb * p.part_stride)) ||
         (rc = c->part_kin.ensure(sizeof(double) * (size_t)p.norb * p.part_stride)))
@@ -668,7 +673,7 @@ extern "C" int wvlh_locden_batched(wvlh_batch *b, int precision, const void *psi
     const Plan &p = b->plan;
     const int fp = precision == 64;
     const size_t lim = sm_limit() - 1024;
-    if (p.smem13[fp] / 2 > lim || p.smem2[fp] > lim) return fail(WVLH_ERR_TOO_LARGE);
+    if ((size_t)p.plane_elems * (fp ? 8 : 4) > lim || p.smem2[fp] > lim) return fail(WVLH_ERR_TOO_LARGE);
     if ((rc = c->scratch.ensure((p.scratch_elems + plane_tmp_elems(p, fp)) * (fp ? 8 : 4))) ||
         (rc = c->den_part.ensure(sizeof(double) * (size_t)p.part_den_elems)))
         return fail(rc);
@@ -690,7 +695,7 @@ extern "C" int wvlh_precond_batched(wvlh_batch *b, int precision, int ncong, con
     const Plan &p = b->plan;
     const int fp = precision == 64;
     const size_t lim = sm_limit() - 1024;
-    if (p.smem13[fp] / 2 > lim || p.smem2[fp] > lim) return fail(WVLH_ERR_TOO_LARGE);
+    if ((size_t)p.plane_elems * (fp ? 8 : 4) > lim || p.smem2[fp] > lim) return fail(WVLH_ERR_TOO_LARGE);
     const size_t es = fp ? 8 : 4;
     const size_t nv = (size_t)p.psi_total * es;
     int rc;

@@ -55,8 +55,11 @@ struct Dims {
         F1 = fine_len(N1, p1); F2 = fine_len(N2, p2); F3 = fine_len(N3, p3);
         I1 = isf_len(N1, p1); I2 = isf_len(N2, p2); I3 = isf_len(N3, p3);
     }
+    // plane buffer A: rows() lines (y) of pitch() points (x); the second buffer
+    // B also holds transposed planes: rowsT() lines (x) of pitchT() points (y)
     __device__ __forceinline__ int pitch() const { return (max(G1, max(F1, I1))) | 1; }
     __device__ __forceinline__ int rows() const { return max(G2, max(F2, I2)); }
+    __device__ __forceinline__ int pitchT() const { return rows() | 1; }
 };
 
 __device__ __forceinline__ LineGeom rows_geom(int nrows, int pitch)
@@ -66,6 +69,12 @@ __device__ __forceinline__ LineGeom rows_geom(int nrows, int pitch)
 __device__ __forceinline__ LineGeom cols_geom(int ncols, int pitch)
 {
     return LineGeom{ncols, 1, pitch, 1, pitch};
+}
+// lines read with unit stride, output written transposed: point q of line l
+// goes to dst[q * dst_pitch + l], so the next pass again reads unit stride
+__device__ __forceinline__ LineGeom xpose_geom(int nlines, int src_pitch, int dst_pitch)
+{
+    return LineGeom{nlines, src_pitch, 1, 1, dst_pitch};
 }
 
 // fine component c=1..7 of psi_f -> (s1,s2,s3) bits (wavelib/un-compress.f90:930-936)
@@ -299,17 +308,18 @@ __device__ __forceinline__ void k1_item(const LrDev *__restrict__ lrs, const Orb
             gather_plane<T, TI>(A, pitch, L, kz, in_ptr(o, psi), MODE == MODE_PRECOND ? sc : nullptr);
         }
         __syncthreads();
-        pass_syn<T, SEG>(A, B, rows_geom(d.G2, pitch), d.N1, d.p1);   // S_x: G2 rows, G1 -> F1
+        const int pt = d.pitchT();
+        pass_syn<T, SEG>(A, B, xpose_geom(d.G2, pitch, pt), d.N1, d.p1);   // S_x: G2 rows, G1 -> F1, into B^T
         __syncthreads();
-        pass_syn<T, SEG>(B, A, cols_geom(d.F1, pitch), d.N2, d.p2);   // S_y: F1 cols, G2 -> F2
+        pass_syn<T, SEG>(B, A, xpose_geom(d.F1, pt, pitch), d.N2, d.p2);   // S_y: F1 lines, G2 -> F2, into A
         __syncthreads();
         if (MODE != MODE_LOCDEN) store_plane(A, pitch, d.F2, d.F1, scratch + o.sP + (size_t)kz * d.F2 * d.F1);
         if (MODE == MODE_PRECOND) return;
-        if (d.p1) pass_mf<T, SEG, 0>(A, B, rows_geom(d.F2, pitch), d.F1, d.I1);
-        else pass_mf<T, SEG, 2>(A, B, rows_geom(d.F2, pitch), d.F1, d.I1);
+        if (d.p1) pass_mf<T, SEG, 0>(A, B, xpose_geom(d.F2, pitch, pt), d.F1, d.I1);   // M_x into B^T
+        else pass_mf<T, SEG, 2>(A, B, xpose_geom(d.F2, pitch, pt), d.F1, d.I1);
         __syncthreads();
-        if (d.p2) pass_mf<T, SEG, 0>(B, A, cols_geom(d.I1, pitch), d.F2, d.I2);
-        else pass_mf<T, SEG, 2>(B, A, cols_geom(d.I1, pitch), d.F2, d.I2);
+        if (d.p2) pass_mf<T, SEG, 0>(B, A, xpose_geom(d.I1, pt, pitch), d.F2, d.I2);   // M_y into A
+        else pass_mf<T, SEG, 2>(B, A, xpose_geom(d.I1, pt, pitch), d.F2, d.I2);
         __syncthreads();
         store_plane(A, pitch, d.I2, d.I1, scratch + o.sQ + (size_t)kz * d.I2 * d.I1);
     }
@@ -466,11 +476,11 @@ __device__ __forceinline__ void k3_item(const LrDev *__restrict__ lrs, const Orb
             load_plane_async(A, pitch, d.I2, d.I1, scratch + o.sQ + (size_t)kz * d.I2 * d.I1);
             cp_async_wait_all();
             __syncthreads();
-            if (d.p1) pass_mf<T, SEG, 1>(A, B, rows_geom(d.I2, pitch), d.I1, d.F1);   // Mt_x
-            else pass_mf<T, SEG, 3>(A, B, rows_geom(d.I2, pitch), d.I1, d.F1);
+            if (d.p1) pass_mf<T, SEG, 1>(A, B, xpose_geom(d.I2, pitch, d.pitchT()), d.I1, d.F1);   // Mt_x into B^T
+            else pass_mf<T, SEG, 3>(A, B, xpose_geom(d.I2, pitch, d.pitchT()), d.I1, d.F1);
             __syncthreads();
-            if (d.p2) pass_mf<T, SEG, 1>(B, A, cols_geom(d.F1, pitch), d.I2, d.F2);   // Mt_y
-            else pass_mf<T, SEG, 3>(B, A, cols_geom(d.F1, pitch), d.I2, d.F2);
+            if (d.p2) pass_mf<T, SEG, 1>(B, A, xpose_geom(d.F1, d.pitchT(), pitch), d.I2, d.F2);   // Mt_y into A
+            else pass_mf<T, SEG, 3>(B, A, xpose_geom(d.F1, d.pitchT(), pitch), d.I2, d.F2);
             __syncthreads();
         }
         {
@@ -515,9 +525,9 @@ __device__ __forceinline__ void k3_item(const LrDev *__restrict__ lrs, const Orb
         __syncthreads();
         pass_kin<T, SEG, true>(B, A, cols_geom(d.F1, pitch), d.F2, d.p2, sy, T(0), &e);   // += K_y P
         __syncthreads();
-        pass_ana<T, SEG>(A, B, rows_geom(d.F2, pitch), d.N1, d.p1);   // A_x: F1 -> G1
+        pass_ana<T, SEG>(A, B, xpose_geom(d.F2, pitch, d.pitchT()), d.N1, d.p1);   // A_x: F1 -> G1, into B^T
         __syncthreads();
-        pass_ana<T, SEG>(B, A, cols_geom(d.G1, pitch), d.N2, d.p2);   // A_y: F2 -> G2
+        pass_ana<T, SEG>(B, A, xpose_geom(d.G1, d.pitchT(), pitch), d.N2, d.p2);   // A_y: F2 -> G2, into A
         __syncthreads();
         scatter_plane<T, TO>(A, pitch, L, kz, out_ptr(o, hpsi), accumulate != 0,
                              MODE == MODE_PRECOND ? sc : nullptr);
@@ -788,9 +798,9 @@ static PlaneCfg plane_cfg(const Plan &p, int fp, int nwork)
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
     PlaneCfg c;
     c.global_b = p.smem13[fp] > (size_t)lim - 1024;
-    c.smem = c.global_b ? p.smem13[fp] / 2 : p.smem13[fp];
+    c.smem = c.global_b ? (size_t)p.plane_elems * (fp ? 8 : 4) : p.smem13[fp];
     c.grid = c.global_b ? (nwork < nsm ? nwork : nsm) : nwork;
-    c.gstride = c.global_b ? p.plane_elems : 0;
+    c.gstride = c.global_b ? p.planeB_elems : 0;
     return c;
 }
 
@@ -800,7 +810,7 @@ long long plane_tmp_elems(const Plan &p, int fp)
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&lim, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-    return p.smem13[fp] > (size_t)lim - 1024 ? (long long)nsm * p.plane_elems : 0;
+    return p.smem13[fp] > (size_t)lim - 1024 ? (long long)nsm * p.planeB_elems : 0;
 }
 template <class T, class TIO, bool ALLPER>
 static cudaError_t launch_locham_bc(const Plan &p, const TIO *psi, const TIO *pot, TIO *hpsi, T *scratch,

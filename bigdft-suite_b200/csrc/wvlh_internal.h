@@ -92,8 +92,9 @@ struct Plan {
     long long *d_orb_off = nullptr;
     int *d_orb_len = nullptr;
     int part_stride = 0;           // energy partial slots per orbital
-    size_t smem13[2] = {0, 0};     // dynamic smem bytes (float, double) of two planes
-    long long plane_elems = 0;     // elements of one plane buffer (rows x pitch)
+    size_t smem13[2] = {0, 0};     // dynamic smem bytes (float, double) of the two plane buffers
+    long long plane_elems = 0;     // elements of plane buffer A (rows x pitch)
+    long long planeB_elems = 0;    // elements of buffer B (a plane or a transposed plane)
     size_t smem2[2] = {0, 0};
     int pitch_max = 0, rows_max = 0, zlen_max = 0;
     std::vector<void *> owned;     // device allocations to free

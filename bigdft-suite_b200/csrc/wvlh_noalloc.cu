@@ -161,13 +161,16 @@ extern "C" int wvlh_locham_noalloc(int precision, const int n[3], const int peri
     const size_t pitch = (size_t)((G[0] > F[0] ? (G[0] > I[0] ? G[0] : I[0]) : (F[0] > I[0] ? F[0] : I[0])) | 1);
     const size_t rows = (size_t)(G[1] > F[1] ? (G[1] > I[1] ? G[1] : I[1]) : (F[1] > I[1] ? F[1] : I[1]));
     const size_t zl = (size_t)(G[2] > F[2] ? (G[2] > I[2] ? G[2] : I[2]) : (F[2] > I[2] ? F[2] : I[2]));
+    // second plane buffer: a plane or a transposed plane (rowsT lines of pitchT points)
+    const size_t rowsT = (size_t)(G[0] > F[0] ? (G[0] > I[0] ? G[0] : I[0]) : (F[0] > I[0] ? F[0] : I[0]));
+    const size_t planeB = rows * pitch > rowsT * (rows | 1) ? rows * pitch : rowsT * (rows | 1);
     int dev = 0, smax = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) {
         set_last_error(WVLH_ERR_CUDA);
         return WVLH_ERR_CUDA;
     }
     cudaDeviceGetAttribute(&smax, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
-    if (2 * rows * pitch * es > (size_t)smax - 1024 || 2 * zl * TX_ * TY_ * es > (size_t)smax - 1024) {
+    if ((rows * pitch + planeB) * es > (size_t)smax - 1024 || 2 * zl * TX_ * TY_ * es > (size_t)smax - 1024) {
         set_last_error(WVLH_ERR_TOO_LARGE);
         return WVLH_ERR_TOO_LARGE;
     }
@@ -258,9 +261,10 @@ extern "C" int wvlh_locham_noalloc(int precision, const int n[3], const int peri
     p.n_work2p = ntx1 * nty1;
     p.part_stride = stride;
     p.plane_elems = (long long)(rows * pitch);
+    p.planeB_elems = (long long)planeB;
     p.scratch_elems = 2 * sP + sQ;
-    p.smem13[0] = 2 * rows * pitch * 4;
-    p.smem13[1] = 2 * rows * pitch * 8;
+    p.smem13[0] = (rows * pitch + planeB) * 4;
+    p.smem13[1] = (rows * pitch + planeB) * 8;
     p.smem2[0] = 2 * zl * TX_ * TY_ * 4;
     p.smem2[1] = 2 * zl * TX_ * TY_ * 8;
     // the energy partials are cleared by the launcher; P, Q/Z1, Z2 are fully
