@@ -70,6 +70,10 @@ struct wvlh_ctx {
     DevBuf arena;
     unsigned long long arena_gen = 0;
     DevBuf wp_runs;  // compressed scalar products: one run per b segment
+    // host-buffer path: a second stream and the buffers of its in-flight chunk
+    cudaStream_t aux = nullptr;
+    cudaEvent_t ev_a = nullptr, ev_b = nullptr;
+    DevBuf scratch2, part_pot2, part_kin2;
 };
 
 // One localisation region: its box and its keys, validated once and kept on
@@ -95,6 +99,9 @@ struct wvlh_batch {
     bool can_locham = true, can_locden = true;
     unsigned long long arena_gen = 0;
     void *mem = nullptr;  // owned table block (wvlh_batch_create)
+    // host-buffer path: sub-batches over consecutive orbital ranges (made on first use)
+    std::vector<wvlh_batch *> chunks;
+    std::vector<int> chunk_o0;
 };
 
 static int fail(int code)
@@ -151,11 +158,18 @@ extern "C" int wvlh_ctx_destroy(wvlh_ctx *ctx)
     cudaStreamSynchronize(ctx->stream);
     for (DevBuf *b : {&ctx->scratch, &ctx->part_pot, &ctx->part_kin, &ctx->io_psi, &ctx->io_pot, &ctx->io_hpsi,
                       &ctx->io_e, &ctx->dotpart, &ctx->cg_r, &ctx->cg_d, &ctx->cg_ad, &ctx->cg_scal, &ctx->den_part,
-                      &ctx->ov_work, &ctx->arena, &ctx->wp_runs})
+                      &ctx->ov_work, &ctx->arena, &ctx->wp_runs, &ctx->scratch2, &ctx->part_pot2,
+                      &ctx->part_kin2})
         b->release();
     for (auto &b : ctx->plain) b.release();
     for (auto &e : ctx->ev)
         if (e) cudaEventDestroy(e);
+    if (ctx->ev_a) cudaEventDestroy(ctx->ev_a);
+    if (ctx->ev_b) cudaEventDestroy(ctx->ev_b);
+    if (ctx->aux) {
+        cudaStreamSynchronize(ctx->aux);
+        cudaStreamDestroy(ctx->aux);
+    }
     delete ctx;
     return WVLH_OK;
 }
@@ -549,6 +563,7 @@ extern "C" int wvlh_batch_destroy(wvlh_batch *b)
         cudaSetDevice(b->ctx->device);
         cudaFree(b->mem);
     }
+    for (wvlh_batch *q : b->chunks) wvlh_batch_destroy(q);
     for (wvlh_region *r : b->own_regions) region_free(r);
     delete b;
     return WVLH_OK;
@@ -750,6 +765,34 @@ static long long pot_extent(const wvlh_batch *b)
     return m;
 }
 
+// Sub-batch of the orbitals [o0, o1) of a packed batch: same regions and
+// potential offsets, coefficients counted from the range's first orbital.
+static int make_chunk(const wvlh_batch *parent, int o0, int o1, wvlh_batch **out)
+{
+    wvlh_batch *q = new wvlh_batch();
+    q->ctx = parent->ctx;
+    q->lr = parent->lr;
+    std::vector<int> ol(parent->plan.orb_lr.begin() + o0, parent->plan.orb_lr.begin() + o1);
+    std::vector<long long> pot(parent->pot_off.begin() + o0, parent->pot_off.begin() + o1);
+    Packer pk;
+    layout(q, ol, pot, pot, nullptr, pk);
+    if (cudaMalloc(&q->mem, pk.img.size()) != cudaSuccess) {
+        q->mem = nullptr;
+        wvlh_batch_destroy(q);
+        return WVLH_ERR_NOMEM;
+    }
+    if (cudaMemcpy(q->mem, pk.img.data(), pk.img.size(), cudaMemcpyHostToDevice) != cudaSuccess) {
+        wvlh_batch_destroy(q);
+        return WVLH_ERR_CUDA;
+    }
+    pk.place(q->mem);
+    *out = q;
+    return WVLH_OK;
+}
+
+// Host buffers: the orbitals go through in chunks that alternate between the
+// context's stream and a second one, so that the upload of one chunk, the
+// kernels of the previous one and the download of the one before overlap.
 extern "C" int wvlh_locham_batched_host(wvlh_batch *b, int precision, const void *psi, const void *pot, void *hpsi,
                                         double *ekin, double *epot)
 {
@@ -757,22 +800,77 @@ extern "C" int wvlh_locham_batched_host(wvlh_batch *b, int precision, const void
     if (b->orbital_mode) return fail(WVLH_ERR_UNSUPPORTED);
     wvlh_ctx *c = b->ctx;
     CK(cudaSetDevice(c->device));
-    const size_t es = precision == 32 ? 4 : 8;
-    const size_t npsi = (size_t)b->plan.psi_total * es, npot = (size_t)pot_extent(b) * es;
-    const size_t ne = sizeof(double) * b->plan.norb;
+    const int fp = precision == 64;
+    const size_t es = fp ? 8 : 4;
+    const Plan &p = b->plan;
+    const size_t npsi = (size_t)p.psi_total * es, npot = (size_t)pot_extent(b) * es;
+    const size_t ne = sizeof(double) * p.norb;
+    const size_t lim = sm_limit() - 1024;
+    if ((size_t)p.plane_elems * es > lim || p.smem2[fp] > lim) return fail(WVLH_ERR_TOO_LARGE);
     int rc;
     if ((rc = c->io_psi.ensure(npsi)) || (rc = c->io_hpsi.ensure(npsi)) || (rc = c->io_pot.ensure(npot)) ||
         (rc = c->io_e.ensure(2 * ne)))
         return fail(rc);
-    CK(cudaMemcpyAsync(c->io_psi.p, psi, npsi, cudaMemcpyHostToDevice, c->stream));
-    CK(cudaMemcpyAsync(c->io_pot.p, pot, npot, cudaMemcpyHostToDevice, c->stream));
+    // chunks of about norb / 16 orbitals (one chunk for small batches): the first
+    // upload and the last download are the parts that nothing overlaps
+    if (b->chunks.empty()) {
+        const int nch = p.norb >= 8 ? std::min(p.norb, 16) : 1;
+        const int per = (p.norb + nch - 1) / nch;
+        for (int o0 = 0; o0 < p.norb; o0 += per) {
+            wvlh_batch *q = nullptr;
+            if ((rc = make_chunk(b, o0, std::min(p.norb, o0 + per), &q))) {
+                for (wvlh_batch *x : b->chunks) wvlh_batch_destroy(x);
+                b->chunks.clear();
+                b->chunk_o0.clear();
+                return fail(rc);
+            }
+            b->chunks.push_back(q);
+            b->chunk_o0.push_back(o0);
+        }
+    }
+    if (!c->aux) CK(cudaStreamCreateWithFlags(&c->aux, cudaStreamNonBlocking));
+    if (!c->ev_a) CK(cudaEventCreateWithFlags(&c->ev_a, cudaEventDisableTiming));
+    if (!c->ev_b) CK(cudaEventCreateWithFlags(&c->ev_b, cudaEventDisableTiming));
+    DevBuf *scr[2] = {&c->scratch, &c->scratch2}, *pp[2] = {&c->part_pot, &c->part_pot2},
+           *pk[2] = {&c->part_kin, &c->part_kin2};
+    for (size_t k = 0; k < b->chunks.size(); ++k) {
+        const Plan &q = b->chunks[k]->plan;
+        const int s = (int)(k & 1);
+        if ((rc = scr[s]->ensure((q.scratch_elems + plane_tmp_elems(q, fp)) * es)) ||
+            (rc = pp[s]->ensure(sizeof(double) * (size_t)q.norb * q.part_stride)) ||
+            (rc = pk[s]->ensure(sizeof(double) * (size_t)q.norb * q.part_stride)))
+            return fail(rc);
+    }
+    cudaStream_t st[2] = {c->stream, c->aux};
+    unsigned char *dpsi = (unsigned char *)c->io_psi.p, *dh = (unsigned char *)c->io_hpsi.p;
     double *de = (double *)c->io_e.p;
-    rc = wvlh_locham_batched(b, precision, c->io_psi.p, c->io_pot.p, c->io_hpsi.p, de, de + b->plan.norb, 0);
-    if (rc) return rc;
-    CK(cudaMemcpyAsync(hpsi, c->io_hpsi.p, npsi, cudaMemcpyDeviceToHost, c->stream));
-    if (ekin) CK(cudaMemcpyAsync(ekin, de, ne, cudaMemcpyDeviceToHost, c->stream));
-    if (epot) CK(cudaMemcpyAsync(epot, de + b->plan.norb, ne, cudaMemcpyDeviceToHost, c->stream));
-    CK(cudaStreamSynchronize(c->stream));
+    // the potential first; the second stream starts after it (and after earlier work)
+    CK(cudaMemcpyAsync(c->io_pot.p, pot, npot, cudaMemcpyHostToDevice, st[0]));
+    CK(cudaEventRecord(c->ev_a, st[0]));
+    CK(cudaStreamWaitEvent(st[1], c->ev_a, 0));
+    for (size_t k = 0; k < b->chunks.size(); ++k) {
+        const Plan &q = b->chunks[k]->plan;
+        const int s = (int)(k & 1);
+        const int o0 = b->chunk_o0[k];
+        const size_t off = (size_t)p.orb_psi[o0] * es, n = (size_t)q.psi_total * es;
+        CK(cudaMemcpyAsync(dpsi + off, (const unsigned char *)psi + off, n, cudaMemcpyHostToDevice, st[s]));
+        cudaError_t e;
+        if (fp)
+            e = launch_locham<double, double>(q, (const double *)(dpsi + off), (const double *)c->io_pot.p,
+                                              (double *)(dh + off), (double *)scr[s]->p, (double *)pp[s]->p,
+                                              (double *)pk[s]->p, de + o0, de + p.norb + o0, 0, st[s], nullptr);
+        else
+            e = launch_locham<float, float>(q, (const float *)(dpsi + off), (const float *)c->io_pot.p,
+                                            (float *)(dh + off), (float *)scr[s]->p, (double *)pp[s]->p,
+                                            (double *)pk[s]->p, de + o0, de + p.norb + o0, 0, st[s], nullptr);
+        CK(e);
+        CK(cudaMemcpyAsync((unsigned char *)hpsi + off, dh + off, n, cudaMemcpyDeviceToHost, st[s]));
+    }
+    CK(cudaEventRecord(c->ev_b, st[1]));
+    CK(cudaStreamWaitEvent(st[0], c->ev_b, 0));
+    if (ekin) CK(cudaMemcpyAsync(ekin, de, ne, cudaMemcpyDeviceToHost, st[0]));
+    if (epot) CK(cudaMemcpyAsync(epot, de + p.norb, ne, cudaMemcpyDeviceToHost, st[0]));
+    CK(cudaStreamSynchronize(st[0]));
     return WVLH_OK;
 }
 

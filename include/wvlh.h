@@ -284,7 +284,10 @@ int wvlh_batch_create_orbitals(wvlh_ctx *ctx, int norb, const wvlh_orbital *orbs
  * compress_and_accumulate_mixed; 0 overwrites like compress_d. */
 int wvlh_locham_batched(wvlh_batch *batch, int precision, const void *psi, const void *pot, void *hpsi,
                         double *ekin, double *epot, int accumulate);
-/* same with HOST buffers: copies in, computes, copies out, synchronises */
+/* same with HOST buffers (pinned for full speed): copies in, computes, copies
+ * out, synchronises.  Batches of 8 orbitals or more go through in chunks of
+ * consecutive orbitals alternating between the context's stream and a second
+ * stream of the context, so that uploads, kernels and downloads overlap. */
 int wvlh_locham_batched_host(wvlh_batch *batch, int precision, const void *psi, const void *pot, void *hpsi,
                              double *ekin, double *epot);
 /* Density of all orbitals: rho[pot_offset[o] + r] += hfac[o] * |psi_o(r)|^2 on

@@ -119,6 +119,29 @@ def test_accumulate_and_host_entry(oracle, torch_cuda, wctx):
     assert rel(hh, ref) < 1e-13 and abs(e1[0] - ek) <= 1e-12 * abs(ek)
 
 
+@pytest.mark.parametrize("dtype_name", ["float32", "float64"])
+def test_host_entry_in_chunks_matches_device_entry(torch_cuda, wctx, dtype_name):
+    """Batches of 8 orbitals or more go through the host-buffer entry point in
+    chunks on two streams: the same kernels per orbital, so the same bits."""
+    torch = torch_cuda
+    lrs = [case((10, 9, 12), (1, 1, 1), 0.6, seed=21)[0], case((9, 8, 7), (0, 0, 0), 0.5, seed=22)[0]]
+    orb_lr = np.array([0, 1, 0, 0, 1, 0, 1, 1, 0, 0, 1, 0, 0], np.int32)
+    off = np.cumsum([0] + [lr.nisf for lr in lrs])
+    b = Batch(wctx, lrs, orb_lr, off[orb_lr])
+    rng = np.random.default_rng(4)
+    dt = np.float32 if dtype_name == "float32" else np.float64
+    psi = rng.uniform(-1, 1, b.psi_size).astype(dt)
+    pot = rng.uniform(-1, 0, int(off[-1])).astype(dt)
+    hd, ekd, epd = b.locham(torch.tensor(psi, device="cuda"), torch.tensor(pot, device="cuda"))
+    torch.cuda.synchronize()
+    hh = np.zeros_like(psi)
+    e1, e2 = np.zeros(len(orb_lr)), np.zeros(len(orb_lr))
+    for _ in range(2):   # the second call reuses the chunks
+        b.locham_host(psi, pot, hh, e1, e2, 32 if dt == np.float32 else 64)
+        assert np.array_equal(hh, hd.cpu().numpy())
+        assert np.array_equal(e1, ekd.cpu().numpy()) and np.array_equal(e2, epd.cpu().numpy())
+
+
 def test_invalid_keys_rejected(torch_cuda, wctx):
     from wvlh._lib import WvlhError
     lr, _, _ = case((8, 8, 8), (1, 1, 1), 0.5, seed=3)
