@@ -46,6 +46,8 @@ def parse():
     ap.add_argument("--n", type=int, default=48)
     ap.add_argument("--norb", type=int, default=256)
     ap.add_argument("--no-extras", action="store_true", help="skip comparator / e2e / cpu / other-row legs")
+    ap.add_argument("--leg", default=None, choices=["free_bc", "precond", "serve32", "serve64"],
+                    help="run one extra leg alone (one GPU) and print its result as one JSON line")
     return ap.parse_args()
 
 
@@ -344,6 +346,20 @@ def main():
             dist.destroy_process_group()
         return
     import numpy as np
+
+    if args.leg:
+        from wvlh.batch import Context
+        dev = torch.device("cuda", local)
+        ctx = Context(local)
+        if args.leg == "free_bc":
+            res = leg_free_regions(torch, ctx, dev)
+        elif args.leg == "precond":
+            res = leg_precond(torch, ctx, dev)
+        else:
+            res = leg_serve(torch, dev, 32 if args.leg == "serve32" else 64)
+        print(json.dumps({"leg": args.leg, "result": res}), flush=True)
+        ctx.close()
+        return
 
     from wvlh import workloads as W
     from wvlh._lib import lib

@@ -301,9 +301,17 @@ __device__ __forceinline__ void k1_item(const LrDev *__restrict__ lrs, const Orb
         if (MODE == MODE_PRECOND && threadIdx.x < 8) sc[threadIdx.x] = (T)prec_scal(L, cprec[oi], threadIdx.x);
         zero_region(A, d.G2, pitch);
         __syncthreads();
-        if constexpr (MODE != MODE_PRECOND && std::is_same<T, TI>::value) {
+        if constexpr (std::is_same<T, TI>::value) {
             gather_plane_async<T>(A, pitch, L, kz, in_ptr(o, psi));
             cp_async_wait_all();
+            if constexpr (MODE == MODE_PRECOND) {
+                // D^-1/2 per component k = s1 + 2 s2 + 4 s3 of each plane position
+                __syncthreads();
+                const int s3 = kz >= d.N3 ? 4 : 0;
+                RowCol q(d.G1);
+                for (int i = threadIdx.x; i < d.G2 * d.G1; i += blockDim.x, q.next())
+                    A[q.r * pitch + q.c] *= sc[(q.c >= d.N1 ? 1 : 0) + (q.r >= d.N2 ? 2 : 0) + s3];
+            }
         } else {
             gather_plane<T, TI>(A, pitch, L, kz, in_ptr(o, psi), MODE == MODE_PRECOND ? sc : nullptr);
         }
@@ -506,6 +514,17 @@ __device__ __forceinline__ void k3_item(const LrDev *__restrict__ lrs, const Orb
                     }
                 }
                 cp_async_wait_all();
+            } else if (MODE == MODE_PRECOND && !bslice) {
+                // P -> B and Z2 -> A asynchronously, then A = c P + Z2
+                load_plane_async(B, pitch, d.F2, d.F1, p);
+                load_plane_async(A, pitch, d.F2, d.F1, z2);
+                cp_async_wait_all();
+                __syncthreads();
+                RowCol q(d.F1);
+                for (int i = threadIdx.x; i < nf; i += blockDim.x, q.next()) {
+                    const int e = q.r * pitch + q.c;
+                    A[e] = fma(cshift, B[e], A[e]);
+                }
             } else {
                 RowCol q(d.F1);
                 for (int i = threadIdx.x; i < nf; i += blockDim.x, q.next()) {
@@ -713,31 +732,46 @@ __global__ void k_cg_sum(int norb, const double *__restrict__ part, double *__re
 
 // r = b - Ax; d = r
 template <class T>
+// r = b - A x, d = r, and the chunk partials of <r|r> (the order of k_cg_dot)
 __global__ void k_cg_init(const long long *__restrict__ off, const int *__restrict__ len, const T *__restrict__ b,
-                          const T *__restrict__ ax, T *__restrict__ r, T *__restrict__ d)
+                          const T *__restrict__ ax, T *__restrict__ r, T *__restrict__ d, double *__restrict__ part)
 {
+    __shared__ double red[32];
     const int o = blockIdx.y;
     const long long base = off[o];
+    double s = 0.0;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < len[o]; i += gridDim.x * blockDim.x) {
         const T v = b[base + i] - ax[base + i];
         r[base + i] = v;
         d[base + i] = v;
+        s += (double)v * (double)v;
     }
+    const double t = block_sum(s, red);
+    if (threadIdx.x == 0) part[o * kCgChunks + blockIdx.x] = t;
 }
 
 // alpha = rr/dAd; x += alpha d; if (update_r) r -= alpha Ad
 template <class T>
+// x += alpha d, r -= alpha A d, and the chunk partials of the new <r|r>
+// (the order of k_cg_dot)
 __global__ void k_cg_step(const long long *__restrict__ off, const int *__restrict__ len,
                           const double *__restrict__ rr, const double *__restrict__ dad, T *__restrict__ x,
-                          const T *__restrict__ d, T *__restrict__ r, const T *__restrict__ ad, int update_r)
+                          const T *__restrict__ d, T *__restrict__ r, const T *__restrict__ ad,
+                          double *__restrict__ part)
 {
+    __shared__ double red[32];
     const int o = blockIdx.y;
     const long long base = off[o];
     const T alpha = (T)(rr[o] / dad[o]);
+    double s = 0.0;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < len[o]; i += gridDim.x * blockDim.x) {
         x[base + i] = fma(alpha, d[base + i], x[base + i]);
-        if (update_r) r[base + i] = fma(-alpha, ad[base + i], r[base + i]);
+        const T v = fma(-alpha, ad[base + i], r[base + i]);
+        r[base + i] = v;
+        s += (double)v * (double)v;
     }
+    const double t = block_sum(s, red);
+    if (threadIdx.x == 0) part[o * kCgChunks + blockIdx.x] = t;
 }
 
 // beta = rr_new/rr; d = beta d + r; rr = rr_new
@@ -945,15 +979,13 @@ cudaError_t launch_precond(const Plan &p, int ncong, const double *cprec, T *x, 
     };
     cudaError_t err;
     if ((err = apply(x, ad))) return err;
-    k_cg_init<T><<<vg, 256, 0, st>>>(p.d_orb_off, p.d_orb_len, b, ad, r, dvec);
-    k_cg_dot<T><<<vg, 256, 0, st>>>(p.d_orb_off, p.d_orb_len, r, r, part);
+    k_cg_init<T><<<vg, 256, 0, st>>>(p.d_orb_off, p.d_orb_len, b, ad, r, dvec, part);
     k_cg_sum<<<(p.norb + 127) / 128, 128, 0, st>>>(p.norb, part, rr, hist);
     for (int it = 0; it < ncong; ++it) {
         if ((err = apply(dvec, ad))) return err;
         k_cg_dot<T><<<vg, 256, 0, st>>>(p.d_orb_off, p.d_orb_len, dvec, ad, part);
         k_cg_sum<<<(p.norb + 127) / 128, 128, 0, st>>>(p.norb, part, dad, nullptr);
-        k_cg_step<T><<<vg, 256, 0, st>>>(p.d_orb_off, p.d_orb_len, rr, dad, x, dvec, r, ad, 1);
-        k_cg_dot<T><<<vg, 256, 0, st>>>(p.d_orb_off, p.d_orb_len, r, r, part);
+        k_cg_step<T><<<vg, 256, 0, st>>>(p.d_orb_off, p.d_orb_len, rr, dad, x, dvec, r, ad, part);
         k_cg_sum<<<(p.norb + 127) / 128, 128, 0, st>>>(p.norb, part, rrn,
                                                       hist ? hist + (size_t)(it + 1) * p.norb : nullptr);
         if (it != ncong - 1) {
