@@ -110,3 +110,24 @@ def test_preconditioner_matches_oracle(oracle, torch_cuda, wctx, dtype_name, tol
         assert rel(got, ref) < tol
         assert np.allclose(hist[:, o], rn, rtol=10 * tol, atol=0)
         assert hist[-1, o] < hist[0, o]      # the CG reduces the residual
+
+
+@pytest.mark.parametrize("dtype_name,tol", [("float64", 1e-13), ("float32", 1e-5)])
+def test_density_long_z_pencils(oracle, torch_cuda, wctx, dtype_name, tol):
+    """Free box with 52 coarse cells along z: ISF z-length 133 > 128 takes the
+    density kernel's 48-accumulator variant."""
+    torch = torch_cuda
+    lr = region((9, 8, 52), (0, 0, 0), 8, 0.4)
+    b = Batch(wctx, [lr], np.zeros(3, np.int32))
+    rng = np.random.default_rng(9)
+    rows = [rng.uniform(-1, 1, lr.ncoeff) for _ in range(3)]
+    hfac = rng.uniform(0.5, 2.0, 3)
+    dt = getattr(torch, dtype_name)
+    psi = torch.tensor(layout(b, [lr], [0, 0, 0], rows), dtype=dt, device="cuda")
+    rho = torch.zeros(lr.nisf, dtype=torch.float64, device="cuda")
+    b.locden(psi, hfac, rho)
+    torch.cuda.synchronize()
+    ref = np.zeros(lr.nisf)
+    for o in range(3):
+        ref = oracle.locden(desc(oracle, lr), rows[o][:lr.nvctr_c], rows[o][lr.nvctr_c:], hfac[o], ref)
+    assert rel(rho.cpu().numpy(), ref) < tol
