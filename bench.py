@@ -455,6 +455,18 @@ def main():
                                   "frac": fach / tf32.value, "kernel": names[dom],
                                   "peak_source": "measured (register FMA-chain probe)"}
         extras["kernels_ms"] = {nm: round(v, 4) for nm, v in zip(names, kt)}
+        # the same step replayed as one captured CUDA graph
+        graph = batch.locham_graph(psi32, pot32, hpsi32, ek, ep)
+        ga, gb = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        graph.launch()
+        torch.cuda.synchronize()
+        ga.record(st)
+        for _ in range(args.steps):
+            graph.launch()
+        gb.record(st)
+        torch.cuda.synchronize()
+        extras["graph"] = {"ms_per_step": ga.elapsed_time(gb) / args.steps, "launches_per_step": 1}
+        graph.close()
 
         # comparators on the same workload: FP64 plain per-pass and FP64 fused
         h64 = torch.empty_like(psi64)

@@ -1056,3 +1056,84 @@ extern "C" int wvlh_wpdot(wvlh_ctx *c, int precision, const wvlh_region *ra, int
     CK(e);
     return WVLH_OK;
 }
+
+// ---------------------------------------------------------------------------
+// CUDA graph of one packed-batch locham call (the same batch applied at every
+// SCF iteration): the memsets and kernels are captured once and replayed with
+// one launch.  The graph owns its scratch, so that later calls on the context
+// (which may grow the context's buffers) cannot move memory under it.
+struct wvlh_graph {
+    wvlh_ctx *ctx = nullptr;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    DevBuf scratch, part_pot, part_kin;
+};
+
+extern "C" int wvlh_graph_destroy(wvlh_graph *g)
+{
+    if (!g) return WVLH_OK;
+    cudaSetDevice(g->ctx->device);
+    if (g->exec) cudaGraphExecDestroy(g->exec);
+    if (g->graph) cudaGraphDestroy(g->graph);
+    cudaDeviceSynchronize();
+    g->scratch.release();
+    g->part_pot.release();
+    g->part_kin.release();
+    delete g;
+    return WVLH_OK;
+}
+
+extern "C" int wvlh_locham_graph_create(wvlh_batch *b, int precision, const void *psi, const void *pot, void *hpsi,
+                                        double *ekin, double *epot, int accumulate, wvlh_graph **out)
+{
+    if (!b || !out || !psi || !pot || !hpsi || (precision != 32 && precision != 64)) return fail(WVLH_ERR_ARG);
+    if (b->orbital_mode) return fail(WVLH_ERR_UNSUPPORTED);  // its tables live in a shared arena
+    wvlh_ctx *c = b->ctx;
+    CK(cudaSetDevice(c->device));
+    const Plan &p = b->plan;
+    const int fp = precision == 64;
+    const size_t lim = sm_limit() - 1024;
+    if ((size_t)p.plane_elems * (fp ? 8 : 4) > lim || p.smem2[fp] > lim) return fail(WVLH_ERR_TOO_LARGE);
+    wvlh_graph *g = new wvlh_graph();
+    g->ctx = c;
+    int rc;
+    if ((rc = g->scratch.ensure((p.scratch_elems + plane_tmp_elems(p, fp)) * (fp ? 8 : 4))) ||
+        (rc = g->part_pot.ensure(sizeof(double) * (size_t)p.norb * p.part_stride)) ||
+        (rc = g->part_kin.ensure(sizeof(double) * (size_t)p.norb * p.part_stride))) {
+        wvlh_graph_destroy(g);
+        return fail(rc);
+    }
+    cudaStream_t cs = nullptr;
+    cudaError_t e = cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
+    if (e == cudaSuccess) {
+        cudaError_t le;
+        if (fp)
+            le = launch_locham<double, double>(p, (const double *)psi, (const double *)pot, (double *)hpsi,
+                                               (double *)g->scratch.p, (double *)g->part_pot.p,
+                                               (double *)g->part_kin.p, ekin, epot, accumulate, cs, nullptr);
+        else
+            le = launch_locham<float, float>(p, (const float *)psi, (const float *)pot, (float *)hpsi,
+                                             (float *)g->scratch.p, (double *)g->part_pot.p,
+                                             (double *)g->part_kin.p, ekin, epot, accumulate, cs, nullptr);
+        e = cudaStreamEndCapture(cs, &g->graph);
+        if (le != cudaSuccess) e = le;
+    }
+    if (e == cudaSuccess) e = cudaGraphInstantiate(&g->exec, g->graph, 0);
+    if (cs) cudaStreamDestroy(cs);
+    if (e != cudaSuccess) {
+        fprintf(stderr, "wvlh: %s\n", cudaGetErrorString(e));
+        wvlh_graph_destroy(g);
+        return fail(WVLH_ERR_CUDA);
+    }
+    *out = g;
+    return WVLH_OK;
+}
+
+extern "C" int wvlh_graph_launch(wvlh_graph *g)
+{
+    if (!g) return fail(WVLH_ERR_ARG);
+    CK(cudaSetDevice(g->ctx->device));
+    CK(cudaGraphLaunch(g->exec, g->ctx->stream));
+    return WVLH_OK;
+}

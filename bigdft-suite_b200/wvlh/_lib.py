@@ -76,6 +76,7 @@ WVLH_SYMBOLS = [
     "wvlh_locham_noalloc", "wvlh_noalloc_capacity", "wvlh_locden_batched", "wvlh_precond_batched",
     "wvlh_overlap", "wvlh_region_create", "wvlh_region_destroy", "wvlh_region_psi_size",
     "wvlh_region_grid_size", "wvlh_region_scratch_bytes", "wvlh_batch_create_orbitals", "wvlh_wpdot",
+    "wvlh_locham_graph_create", "wvlh_graph_launch", "wvlh_graph_destroy",
 ]
 
 
@@ -127,6 +128,9 @@ def lib():
     L.wvlh_region_scratch_bytes.argtypes = [vp, C.c_int]
     L.wvlh_batch_create_orbitals.argtypes = [vp, C.c_int, C.POINTER(OrbitalDesc), C.POINTER(vp)]
     L.wvlh_wpdot.argtypes = [vp, C.c_int, vp, C.c_int, vp, C.c_int64, vp, C.c_int, vp, C.c_int64, vp]
+    L.wvlh_locham_graph_create.argtypes = [vp, C.c_int, vp, vp, vp, vp, vp, C.c_int, C.POINTER(vp)]
+    L.wvlh_graph_launch.argtypes = [vp]
+    L.wvlh_graph_destroy.argtypes = [vp]
     L.wvlh_host_alloc.restype = vp
     L.wvlh_host_alloc.argtypes = [C.c_size_t]
     L.wvlh_host_free.argtypes = [vp]

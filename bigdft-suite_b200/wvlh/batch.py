@@ -121,6 +121,11 @@ class Batch:
         check(rc, "wvlh_locham_batched")
         return hpsi, ekin, epot
 
+    def locham_graph(self, psi, pot, hpsi, ekin, epot, accumulate=False):
+        """Capture locham(psi, pot, hpsi, ekin, epot) into a CUDA graph; replay
+        it with .launch() (the tensors must stay alive and in place)."""
+        return LochamGraph(self, psi, pot, hpsi, ekin, epot, accumulate)
+
     def locham_host(self, psi, pot, hpsi, ekin, epot, precision):
         """Host buffers (numpy arrays or CPU tensors, ideally pinned)."""
         def addr(a):
@@ -172,6 +177,37 @@ class Batch:
     def close(self):
         if getattr(self, "h", None):
             lib().wvlh_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class LochamGraph:
+    """One packed-batch locham call captured as a CUDA graph (wvlh_locham_graph_create)."""
+
+    def __init__(self, batch, psi, pot, hpsi, ekin, epot, accumulate=False):
+        torch = batch.ctx.torch
+        prec = {torch.float32: 32, torch.float64: 64}.get(psi.dtype)
+        if prec is None or pot.dtype != psi.dtype or hpsi.dtype != psi.dtype:
+            raise WvlhError("psi, pot and hpsi must share float32 or float64")
+        self.batch = batch
+        self._keep = (psi, pot, hpsi, ekin, epot)
+        h = C.c_void_p()
+        check(lib().wvlh_locham_graph_create(batch.h, prec, _ptr(psi), _ptr(pot), _ptr(hpsi), _ptr(ekin),
+                                             _ptr(epot), int(bool(accumulate)), C.byref(h)),
+              "wvlh_locham_graph_create")
+        self.h = h
+
+    def launch(self):
+        check(lib().wvlh_graph_launch(self.h), "wvlh_graph_launch")
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().wvlh_graph_destroy(self.h)
             self.h = None
 
     def __del__(self):

@@ -326,6 +326,18 @@ int wvlh_wpdot(wvlh_ctx *ctx, int precision, const wvlh_region *ra, int na, cons
 int wvlh_locham_plain_batched(wvlh_batch *batch, const double *psi, const double *pot, double *hpsi,
                               double *ekin, double *epot);
 
+/* CUDA graph of one wvlh_locham_batched call with fixed arguments (a packed
+ * batch applied at every SCF iteration): the memsets and kernels are captured
+ * once (on a private stream) and replayed by wvlh_graph_launch on the
+ * context's stream with one launch.  The graph owns its scratch; the batch and
+ * the buffers named at capture must outlive it.  Orbital batches are refused
+ * (WVLH_ERR_UNSUPPORTED): their tables are replaced by the next batch. */
+typedef struct wvlh_graph wvlh_graph;
+int wvlh_locham_graph_create(wvlh_batch *batch, int precision, const void *psi, const void *pot, void *hpsi,
+                             double *ekin, double *epot, int accumulate, wvlh_graph **graph);
+int wvlh_graph_launch(wvlh_graph *graph);
+int wvlh_graph_destroy(wvlh_graph *graph);
+
 /* Optional per-kernel timing with CUDA events recorded on the context's
  * stream around the fused kernels (K1 plane-forward, K2 z-pencil, K3
  * plane-backward, energy reduction).  While on, each wvlh_locham_batched call

@@ -142,6 +142,34 @@ def test_host_entry_in_chunks_matches_device_entry(torch_cuda, wctx, dtype_name)
         assert np.array_equal(e1, ekd.cpu().numpy()) and np.array_equal(e2, epd.cpu().numpy())
 
 
+@pytest.mark.parametrize("dtype_name", ["float32", "float64"])
+def test_graph_replay_matches_direct_call(torch_cuda, wctx, dtype_name):
+    """A captured locham replays the same kernels: the same bits, and it reads
+    the buffers' current contents at every launch."""
+    torch = torch_cuda
+    lrs = [case((10, 9, 12), (1, 1, 1), 0.6, seed=31)[0], case((9, 8, 7), (0, 0, 0), 0.5, seed=32)[0]]
+    orb_lr = np.array([0, 1, 1, 0, 0], np.int32)
+    off = np.cumsum([0] + [lr.nisf for lr in lrs])
+    b = Batch(wctx, lrs, orb_lr, off[orb_lr])
+    dt = getattr(torch, dtype_name)
+    g = torch.Generator(device="cuda").manual_seed(5)
+    psi = torch.rand(b.psi_size, generator=g, device="cuda", dtype=torch.float64).to(dt) - 0.5
+    pot = -torch.rand(int(off[-1]), generator=g, device="cuda", dtype=torch.float64).to(dt)
+    h1, e1, p1 = b.locham(psi, pot)
+    h2, e2, p2 = torch.zeros_like(h1), torch.zeros_like(e1), torch.zeros_like(p1)
+    graph = b.locham_graph(psi, pot, h2, e2, p2)
+    for _ in range(2):
+        graph.launch()
+        torch.cuda.synchronize()
+        assert torch.equal(h1, h2) and torch.equal(e1, e2) and torch.equal(p1, p2)
+    psi.mul_(2)
+    h3, e3, p3 = b.locham(psi, pot)
+    graph.launch()
+    torch.cuda.synchronize()
+    assert torch.equal(h3, h2) and torch.equal(e3, e2)
+    graph.close()
+
+
 def test_invalid_keys_rejected(torch_cuda, wctx):
     from wvlh._lib import WvlhError
     lr, _, _ = case((8, 8, 8), (1, 1, 1), 0.5, seed=3)
