@@ -351,6 +351,7 @@ static void layout(wvlh_batch *b, const std::vector<int> &orb_lr, const std::vec
     long long psi_off = 0, scr = 0;
     int stride = 0;
     size_t planeA = 0, planeB = 0, sm2_elems = 0;
+    std::vector<PlaneShape> shapes32, shapes64;  // plane geometry per orbital (CTA-size choice)
     b->pot_off.assign(pot_key.begin(), pot_key.end());
     for (int o = 0; o < norb; ++o) {
         const int l = orb_lr[o];
@@ -392,6 +393,12 @@ static void layout(wvlh_batch *b, const std::vector<int> &orb_lr, const std::vec
         const int rows = std::max(G2, std::max(F2, I2));
         const int rowsT = std::max(G1, std::max(F1, I1)), pitchT = rows | 1;
         planeA = std::max(planeA, (size_t)rows * pitch);
+        {
+            const long long len = std::max(G1, std::max(F1, I1)), w = (long long)G3 * rows * pitch;
+            const long long ab = (long long)rows * pitch + std::max((long long)rows * pitch, (long long)rowsT * pitchT);
+            shapes32.push_back(PlaneShape{rows, len, ab * 4, w});
+            shapes64.push_back(PlaneShape{rows, len, ab * 8, w});
+        }
         planeB = std::max(planeB, std::max((size_t)rows * pitch, (size_t)rowsT * pitchT));
         const int zl = std::max(G3, std::max(F3, I3));
         sm2_elems = std::max(sm2_elems, (size_t)2 * zl * TX_ * TY_);
@@ -401,6 +408,8 @@ static void layout(wvlh_batch *b, const std::vector<int> &orb_lr, const std::vec
     for (int v : p.lr_per) p.all_periodic = p.all_periodic && v == 1;
     p.scratch_elems = scr;
     p.part_stride = stride;
+    p.plane_threads[0] = choose_plane_threads(shapes32, true);
+    p.plane_threads[1] = choose_plane_threads(shapes64, false);
     p.plane_elems = (long long)planeA;
     p.planeB_elems = (long long)planeB;
     p.smem13[0] = (planeA + planeB) * sizeof(float);

@@ -270,6 +270,15 @@ __device__ __forceinline__ TO *out_ptr(const OrbDev &o, TO *base)
     return o.out_ptr ? (TO *)o.out_ptr : base + o.psi;
 }
 
+// Resident CTAs per SM the plane kernels are compiled for: FP32 CTAs of 384,
+// 256 or 128 threads at 56 or 64 registers (3, 4 or 8 per SM); FP64 CTAs of
+// 256 or 128 threads at up to 128 registers (2 or 4 per SM); the 384-thread
+// FP64 and the persistent variants take what their registers need.
+__host__ __device__ constexpr int plane_min_blocks(bool fp32, bool persist, int nt)
+{
+    return persist ? 1 : (fp32 ? (nt >= 384 ? 3 : (nt >= 256 ? 4 : 8)) : (nt >= 384 ? 1 : (nt >= 256 ? 2 : 4)));
+}
+
 // ---------------------------------------------------------------------------
 // K1: compressed psi -> P = S_x S_y psi (not in MODE_LOCDEN) and
 // Q = M_x M_y P (not in MODE_PRECOND) for one wavelet z-plane.
@@ -333,8 +342,8 @@ __device__ __forceinline__ void k1_item(const LrDev *__restrict__ lrs, const Orb
     }
 }
 
-template <class T, class TI, bool ALLPER, int MODE, bool PERSIST>
-__global__ void __launch_bounds__(kPlaneThreads, (sizeof(T) == 4 && !PERSIST) ? 3 : 1) k1_plane_forward(const LrDev *__restrict__ lrs,
+template <class T, class TI, bool ALLPER, int MODE, bool PERSIST, int NT>
+__global__ void __launch_bounds__(NT, plane_min_blocks(sizeof(T) == 4, PERSIST, NT)) k1_plane_forward(const LrDev *__restrict__ lrs,
                                                                   const OrbDev *__restrict__ orbs,
                                                                   const int *__restrict__ pre, int norb,
                                                                   const TI *__restrict__ psi, T *__restrict__ scratch,
@@ -559,8 +568,8 @@ __device__ __forceinline__ void k3_item(const LrDev *__restrict__ lrs, const Orb
 
 // FP32: 3 CTAs per SM (56 registers), which the 75 KB of shared memory of a
 // 96^2 plane pair allows; FP64 planes leave room for one CTA anyway
-template <class T, class TO, bool ALLPER, int MODE, bool PERSIST>
-__global__ void __launch_bounds__(kPlaneThreads, (sizeof(T) == 4 && !PERSIST) ? 3 : 1) k3_plane_backward(const LrDev *__restrict__ lrs,
+template <class T, class TO, bool ALLPER, int MODE, bool PERSIST, int NT>
+__global__ void __launch_bounds__(NT, plane_min_blocks(sizeof(T) == 4, PERSIST, NT)) k3_plane_backward(const LrDev *__restrict__ lrs,
                                                                    const OrbDev *__restrict__ orbs,
                                                                    const int *__restrict__ pre, int norb,
                                                                    const T *__restrict__ scratch, TO *__restrict__ hpsi,
@@ -820,6 +829,7 @@ __global__ void k_cg_scale(const LrDev *__restrict__ lrs, const OrbDev *__restri
 struct PlaneCfg {
     size_t smem = 0;
     int grid = 0;
+    int threads = kPlaneThreads;
     long long gstride = 0;
     bool global_b = false;
 };
@@ -835,7 +845,26 @@ static PlaneCfg plane_cfg(const Plan &p, int fp, int nwork)
     c.smem = c.global_b ? (size_t)p.plane_elems * (fp ? 8 : 4) : p.smem13[fp];
     c.grid = c.global_b ? (nwork < nsm ? nwork : nsm) : nwork;
     c.gstride = c.global_b ? p.planeB_elems : 0;
+    c.threads = c.global_b ? kPlaneThreads : p.plane_threads[fp];
     return c;
+}
+
+template <class T, class TI, bool ALLPER, int MODE>
+static auto k1_for(const PlaneCfg &pc) -> decltype(&k1_plane_forward<T, TI, ALLPER, MODE, false, kPlaneThreads>)
+{
+    if (pc.global_b) return k1_plane_forward<T, TI, ALLPER, MODE, true, kPlaneThreads>;
+    if (pc.threads == 128) return k1_plane_forward<T, TI, ALLPER, MODE, false, 128>;
+    if (pc.threads == 256) return k1_plane_forward<T, TI, ALLPER, MODE, false, 256>;
+    return k1_plane_forward<T, TI, ALLPER, MODE, false, kPlaneThreads>;
+}
+
+template <class T, class TO, bool ALLPER, int MODE>
+static auto k3_for(const PlaneCfg &pc) -> decltype(&k3_plane_backward<T, TO, ALLPER, MODE, false, kPlaneThreads>)
+{
+    if (pc.global_b) return k3_plane_backward<T, TO, ALLPER, MODE, true, kPlaneThreads>;
+    if (pc.threads == 128) return k3_plane_backward<T, TO, ALLPER, MODE, false, 128>;
+    if (pc.threads == 256) return k3_plane_backward<T, TO, ALLPER, MODE, false, 256>;
+    return k3_plane_backward<T, TO, ALLPER, MODE, false, kPlaneThreads>;
 }
 
 long long plane_tmp_elems(const Plan &p, int fp)
@@ -856,10 +885,10 @@ static cudaError_t launch_locham_bc(const Plan &p, const TIO *psi, const TIO *po
     const size_t sm13 = pc.smem, sm2 = p.smem2[fp];
     T *gtmp = pc.global_b ? scratch + p.scratch_elems : nullptr;
     cudaError_t err;
-    auto k1 = pc.global_b ? k1_plane_forward<T, TIO, ALLPER, MODE_LOCHAM, true> : k1_plane_forward<T, TIO, ALLPER, MODE_LOCHAM, false>;
+    auto k1 = k1_for<T, TIO, ALLPER, MODE_LOCHAM>(pc);
     auto k2 = k2_zpencil<T, TIO, ALLPER, 0>;
     auto k2k = k2_zpencil<T, TIO, ALLPER, 1>;
-    auto k3 = pc.global_b ? k3_plane_backward<T, TIO, ALLPER, MODE_LOCHAM, true> : k3_plane_backward<T, TIO, ALLPER, MODE_LOCHAM, false>;
+    auto k3 = k3_for<T, TIO, ALLPER, MODE_LOCHAM>(pc);
     if ((err = cudaFuncSetAttribute(k1, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm13))) return err;
     if ((err = cudaFuncSetAttribute(k2, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm2))) return err;
     if ((err = cudaFuncSetAttribute(k2k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm2))) return err;
@@ -868,7 +897,7 @@ static cudaError_t launch_locham_bc(const Plan &p, const TIO *psi, const TIO *po
     cudaMemsetAsync(part_kin, 0, sizeof(double) * (size_t)p.norb * p.part_stride, st);
     // optional per-kernel timing: ev[0..4] bracket K1, K2, K3 and the reduction
     if (ev) cudaEventRecord(ev[0], st);
-    k1<<<pc.grid, kPlaneThreads, sm13, st>>>(p.d_lr, p.d_orb, p.d_pre13, p.norb, psi, scratch, nullptr, gtmp,
+    k1<<<pc.grid, pc.threads, sm13, st>>>(p.d_lr, p.d_orb, p.d_pre13, p.norb, psi, scratch, nullptr, gtmp,
                                              pc.gstride);
     if (ev) cudaEventRecord(ev[1], st);
     k2<<<p.n_work2, kZThreads, sm2, st>>>(p.d_lr, p.d_orb, p.d_pre2, p.norb, pot, scratch, part_pot, part_kin,
@@ -876,7 +905,7 @@ static cudaError_t launch_locham_bc(const Plan &p, const TIO *psi, const TIO *po
     k2k<<<p.n_work2p, kZThreads, sm2, st>>>(p.d_lr, p.d_orb, p.d_pre2p, p.norb, pot, scratch, part_pot, part_kin,
                                             p.part_stride);
     if (ev) cudaEventRecord(ev[2], st);
-    k3<<<pc.grid, kPlaneThreads, sm13, st>>>(p.d_lr, p.d_orb, p.d_pre13, p.norb, scratch, hpsi, part_kin,
+    k3<<<pc.grid, pc.threads, sm13, st>>>(p.d_lr, p.d_orb, p.d_pre13, p.norb, scratch, hpsi, part_kin,
                                              p.part_stride, accumulate, nullptr, gtmp, pc.gstride);
     if (ev) cudaEventRecord(ev[3], st);
     k_reduce_energies<<<p.norb, 128, 0, st>>>(part_pot, part_kin, p.part_stride, p.norb, ekin, epot);
@@ -912,11 +941,11 @@ static cudaError_t launch_locden_bc(const Plan &p, const T *psi, const double *h
     const size_t sm13 = pc.smem, sm2 = p.smem2[fp];
     T *gtmp = pc.global_b ? scratch + p.scratch_elems : nullptr;
     cudaError_t err;
-    auto k1 = pc.global_b ? k1_plane_forward<T, T, ALLPER, MODE_LOCDEN, true> : k1_plane_forward<T, T, ALLPER, MODE_LOCDEN, false>;
+    auto k1 = k1_for<T, T, ALLPER, MODE_LOCDEN>(pc);
     auto kd = p.den_acc > 32 ? kd_density<T, ALLPER, 48> : kd_density<T, ALLPER, 32>;
     if ((err = cudaFuncSetAttribute(k1, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm13))) return err;
     if ((err = cudaFuncSetAttribute(kd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm2))) return err;
-    k1<<<pc.grid, kPlaneThreads, sm13, st>>>(p.d_lr, p.d_orb, p.d_pre13, p.norb, psi, scratch, nullptr, gtmp,
+    k1<<<pc.grid, pc.threads, sm13, st>>>(p.d_lr, p.d_orb, p.d_pre13, p.norb, psi, scratch, nullptr, gtmp,
                                              pc.gstride);
     kd<<<p.n_workd, kZThreads, sm2, st>>>(p.d_lr, p.d_orb, p.d_pred, p.nchunk, p.d_chunk_orb_start, p.d_chunk_orbs,
                                           p.d_chunk_part, scratch, hfac, part);
@@ -948,17 +977,17 @@ static cudaError_t launch_prec_apply_bc(const Plan &p, const T *x, T *y, const d
     const size_t sm13 = pc.smem, sm2 = p.smem2[fp];
     T *gtmp = pc.global_b ? scratch + p.scratch_elems : nullptr;
     cudaError_t err;
-    auto k1 = pc.global_b ? k1_plane_forward<T, T, ALLPER, MODE_PRECOND, true> : k1_plane_forward<T, T, ALLPER, MODE_PRECOND, false>;
+    auto k1 = k1_for<T, T, ALLPER, MODE_PRECOND>(pc);
     auto k2 = k2_zpencil<T, T, ALLPER, 1>;
-    auto k3 = pc.global_b ? k3_plane_backward<T, T, ALLPER, MODE_PRECOND, true> : k3_plane_backward<T, T, ALLPER, MODE_PRECOND, false>;
+    auto k3 = k3_for<T, T, ALLPER, MODE_PRECOND>(pc);
     if ((err = cudaFuncSetAttribute(k1, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm13))) return err;
     if ((err = cudaFuncSetAttribute(k2, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm2))) return err;
     if ((err = cudaFuncSetAttribute(k3, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm13))) return err;
-    k1<<<pc.grid, kPlaneThreads, sm13, st>>>(p.d_lr, p.d_orb, p.d_pre13, p.norb, x, scratch, cprec, gtmp,
+    k1<<<pc.grid, pc.threads, sm13, st>>>(p.d_lr, p.d_orb, p.d_pre13, p.norb, x, scratch, cprec, gtmp,
                                              pc.gstride);
     k2<<<p.n_work2p, kZThreads, sm2, st>>>(p.d_lr, p.d_orb, p.d_pre2p, p.norb, (const T *)nullptr, scratch,
                                            nullptr, nullptr, 0);
-    k3<<<pc.grid, kPlaneThreads, sm13, st>>>(p.d_lr, p.d_orb, p.d_pre13, p.norb, scratch, y, nullptr, 0, 0, cprec,
+    k3<<<pc.grid, pc.threads, sm13, st>>>(p.d_lr, p.d_orb, p.d_pre13, p.norb, scratch, y, nullptr, 0, 0, cprec,
                                              gtmp, pc.gstride);
     return cudaGetLastError();
 }

@@ -14,6 +14,45 @@ constexpr int TY_ = 2;
 // block sizes of the plane kernels (K1, K3) and of the z-pencil kernel (K2);
 // 384 threads give 3 line-segment items per thread on 96-point planes
 constexpr int kPlaneThreads = 384;
+
+// CTA size of the plane kernels (128, 256 or 384 threads), chosen per batch by
+// a small occupancy model: a pass has `rows` lines of up to `len` points cut
+// into segments of SEG outputs; with nt threads it takes ceil(items / nt)
+// rounds, so the busy fraction is items / (rounds nt); the SM holds as many
+// CTAs as registers (the compiled minimum per SM), shared memory and threads
+// allow.  The expected rate is busy x resident threads; each orbital's planes
+// weigh by their work, and the size with the least total cost wins.
+struct PlaneShape {
+    long long rows, len, smem_bytes, weight;
+};
+inline int choose_plane_threads(const std::vector<PlaneShape> &shapes, bool fp32)
+{
+    const int cand[3] = {kPlaneThreads, 256, 128};   // on a tie the larger CTA stays
+    const int seg = fp32 ? 8 : 4;
+    double best = 0.0;
+    int pick = 0;
+    for (int nt : cand) {
+        double cost = 0.0;
+        for (const PlaneShape &s : shapes) {
+            const long long items = s.rows * ((s.len + seg - 1) / seg);
+            const long long rounds = (items + nt - 1) / nt;
+            const double busy = (double)items / (double)(rounds * nt);
+            // FP32: compiled for 3 / 4 / 8 CTAs per SM; FP64: about 128 registers a thread
+            const long long by_regs = fp32 ? (nt >= 384 ? 3 : (nt >= 256 ? 4 : 8)) : 65536 / (128LL * nt);
+            const long long by_smem = (227LL * 1024) / (s.smem_bytes + 1024);
+            const long long by_threads = 2048 / nt;
+            long long ctas = by_regs < by_smem ? by_regs : by_smem;
+            ctas = ctas < by_threads ? ctas : by_threads;
+            const double rate = busy * (double)(ctas > 0 ? ctas : 1) * nt;
+            cost += (double)s.weight / rate;
+        }
+        if (pick == 0 || cost < best * 0.999) {
+            best = cost;
+            pick = nt;
+        }
+    }
+    return pick;
+}
 constexpr int kZThreads = 256;
 
 // One localisation region (box + compressed-key tables) as seen by kernels.
@@ -95,6 +134,7 @@ struct Plan {
     size_t smem13[2] = {0, 0};     // dynamic smem bytes (float, double) of the two plane buffers
     long long plane_elems = 0;     // elements of plane buffer A (rows x pitch)
     long long planeB_elems = 0;    // elements of buffer B (a plane or a transposed plane)
+    int plane_threads[2] = {kPlaneThreads, kPlaneThreads};   // plane-kernel CTA size (float, double)
     size_t smem2[2] = {0, 0};
     int pitch_max = 0, rows_max = 0, zlen_max = 0;
     std::vector<void *> owned;     // device allocations to free

@@ -261,6 +261,11 @@ extern "C" int wvlh_locham_noalloc(int precision, const int n[3], const int peri
     p.n_work2p = ntx1 * nty1;
     p.part_stride = stride;
     p.plane_elems = (long long)(rows * pitch);
+    {
+        const long long len = (long long)rowsT, ab = (long long)(rows * pitch + planeB);
+        p.plane_threads[0] = choose_plane_threads({PlaneShape{(long long)rows, len, ab * 4, 1}}, true);
+        p.plane_threads[1] = choose_plane_threads({PlaneShape{(long long)rows, len, ab * 8, 1}}, false);
+    }
     p.planeB_elems = (long long)planeB;
     p.scratch_elems = 2 * sP + sQ;
     p.smem13[0] = (rows * pitch + planeB) * 4;
