@@ -270,13 +270,14 @@ __device__ __forceinline__ TO *out_ptr(const OrbDev &o, TO *base)
     return o.out_ptr ? (TO *)o.out_ptr : base + o.psi;
 }
 
-// Resident CTAs per SM the plane kernels are compiled for: FP32 CTAs of 384,
-// 256 or 128 threads at 56 or 64 registers (3, 4 or 8 per SM); FP64 CTAs of
-// 256 or 128 threads at up to 128 registers (2 or 4 per SM); the 384-thread
-// FP64 and the persistent variants take what their registers need.
+// Resident CTAs per SM the plane kernels are compiled for (plane_ctas_per_sm
+// in wvlh_internal.h): FP32 CTAs of 1024, 512, 384, 256 or 128 threads at 64,
+// 64, 56, 64, 64 registers; FP64 CTAs of 512, 256 or 128 threads at up to 128
+// registers; the 384-thread FP64 and the persistent variants take what their
+// registers need.
 __host__ __device__ constexpr int plane_min_blocks(bool fp32, bool persist, int nt)
 {
-    return persist ? 1 : (fp32 ? (nt >= 384 ? 3 : (nt >= 256 ? 4 : 8)) : (nt >= 384 ? 1 : (nt >= 256 ? 2 : 4)));
+    return persist ? 1 : plane_ctas_per_sm(fp32, nt);
 }
 
 // ---------------------------------------------------------------------------
@@ -853,6 +854,9 @@ template <class T, class TI, bool ALLPER, int MODE>
 static auto k1_for(const PlaneCfg &pc) -> decltype(&k1_plane_forward<T, TI, ALLPER, MODE, false, kPlaneThreads>)
 {
     if (pc.global_b) return k1_plane_forward<T, TI, ALLPER, MODE, true, kPlaneThreads>;
+    if constexpr (sizeof(T) == 4)
+        if (pc.threads == 1024) return k1_plane_forward<T, TI, ALLPER, MODE, false, 1024>;
+    if (pc.threads == 512) return k1_plane_forward<T, TI, ALLPER, MODE, false, 512>;
     if (pc.threads == 128) return k1_plane_forward<T, TI, ALLPER, MODE, false, 128>;
     if (pc.threads == 256) return k1_plane_forward<T, TI, ALLPER, MODE, false, 256>;
     return k1_plane_forward<T, TI, ALLPER, MODE, false, kPlaneThreads>;
@@ -862,6 +866,9 @@ template <class T, class TO, bool ALLPER, int MODE>
 static auto k3_for(const PlaneCfg &pc) -> decltype(&k3_plane_backward<T, TO, ALLPER, MODE, false, kPlaneThreads>)
 {
     if (pc.global_b) return k3_plane_backward<T, TO, ALLPER, MODE, true, kPlaneThreads>;
+    if constexpr (sizeof(T) == 4)
+        if (pc.threads == 1024) return k3_plane_backward<T, TO, ALLPER, MODE, false, 1024>;
+    if (pc.threads == 512) return k3_plane_backward<T, TO, ALLPER, MODE, false, 512>;
     if (pc.threads == 128) return k3_plane_backward<T, TO, ALLPER, MODE, false, 128>;
     if (pc.threads == 256) return k3_plane_backward<T, TO, ALLPER, MODE, false, 256>;
     return k3_plane_backward<T, TO, ALLPER, MODE, false, kPlaneThreads>;

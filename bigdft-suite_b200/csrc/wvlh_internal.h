@@ -15,35 +15,50 @@ constexpr int TY_ = 2;
 // 384 threads give 3 line-segment items per thread on 96-point planes
 constexpr int kPlaneThreads = 384;
 
-// CTA size of the plane kernels (128, 256 or 384 threads), chosen per batch by
-// a small occupancy model: a pass has `rows` lines of up to `len` points cut
-// into segments of SEG outputs; with nt threads it takes ceil(items / nt)
-// rounds, so the busy fraction is items / (rounds nt); the SM holds as many
-// CTAs as registers (the compiled minimum per SM), shared memory and threads
-// allow.  The expected rate is busy x resident threads; each orbital's planes
-// weigh by their work, and the size with the least total cost wins.
+// CTAs per SM the plane kernels are compiled for (register budget): FP32
+// 1024 / 512 / 384 / 256 / 128 threads -> 1 / 2 / 3 / 4 / 8; FP64 (no 1024)
+// 512 / 384 / 256 / 128 -> 1 / 1 / 2 / 4.
+__host__ __device__ constexpr int plane_ctas_per_sm(bool fp32, int nt)
+{
+    return fp32 ? (nt >= 1024 ? 1 : nt >= 512 ? 2 : nt >= 384 ? 3 : nt >= 256 ? 4 : 8)
+                : (nt >= 384 ? 1 : nt >= 256 ? 2 : 4);
+}
+
+// CTA size of the plane kernels, chosen per batch by a small occupancy model:
+// a pass has `rows` lines of up to `len` points cut into segments of SEG
+// outputs; with nt threads it takes ceil(items / nt) rounds, so the busy
+// fraction is items / (rounds nt); the SM holds as many CTAs as registers (the
+// compiled count above), shared memory and threads allow.  The expected rate
+// is busy x resident threads x ctas / (ctas + 1/2) — the last factor because
+// a CTA's barrier waits are covered only by the other resident CTAs; each
+// orbital's planes weigh by their work, and the size with the least total cost
+// wins (a larger CTA on a tie).
 struct PlaneShape {
     long long rows, len, smem_bytes, weight;
 };
 inline int choose_plane_threads(const std::vector<PlaneShape> &shapes, bool fp32)
 {
-    const int cand[3] = {kPlaneThreads, 256, 128};   // on a tie the larger CTA stays
+    const int cand32[5] = {1024, 512, kPlaneThreads, 256, 128};
+    const int cand64[4] = {512, kPlaneThreads, 256, 128};
+    const int *cand = fp32 ? cand32 : cand64;
+    const int ncand = fp32 ? 5 : 4;
     const int seg = fp32 ? 8 : 4;
     double best = 0.0;
     int pick = 0;
-    for (int nt : cand) {
+    for (int k = 0; k < ncand; ++k) {
+        const int nt = cand[k];
         double cost = 0.0;
         for (const PlaneShape &s : shapes) {
             const long long items = s.rows * ((s.len + seg - 1) / seg);
             const long long rounds = (items + nt - 1) / nt;
             const double busy = (double)items / (double)(rounds * nt);
-            // FP32: compiled for 3 / 4 / 8 CTAs per SM; FP64: about 128 registers a thread
-            const long long by_regs = fp32 ? (nt >= 384 ? 3 : (nt >= 256 ? 4 : 8)) : 65536 / (128LL * nt);
+            const long long by_regs = plane_ctas_per_sm(fp32, nt);
             const long long by_smem = (227LL * 1024) / (s.smem_bytes + 1024);
             const long long by_threads = 2048 / nt;
             long long ctas = by_regs < by_smem ? by_regs : by_smem;
             ctas = ctas < by_threads ? ctas : by_threads;
-            const double rate = busy * (double)(ctas > 0 ? ctas : 1) * nt;
+            if (ctas < 1) ctas = 1;
+            const double rate = busy * (double)ctas * nt * ((double)ctas / ((double)ctas + 0.5));
             cost += (double)s.weight / rate;
         }
         if (pick == 0 || cost < best * 0.999) {
