@@ -46,7 +46,7 @@ def parse():
     ap.add_argument("--n", type=int, default=48)
     ap.add_argument("--norb", type=int, default=256)
     ap.add_argument("--no-extras", action="store_true", help="skip comparator / e2e / cpu / other-row legs")
-    ap.add_argument("--leg", default=None, choices=["free_bc", "precond", "serve32", "serve64"],
+    ap.add_argument("--leg", default=None, choices=["free_bc", "precond", "overlap", "serve32", "serve64"],
                     help="run one extra leg alone (one GPU) and print its result as one JSON line")
     return ap.parse_args()
 
@@ -355,6 +355,13 @@ def main():
             res = leg_free_regions(torch, ctx, dev)
         elif args.leg == "precond":
             res = leg_precond(torch, ctx, dev)
+        elif args.leg == "overlap":
+            from wvlh import workloads as W
+            lr = W.full_periodic(args.n, 0.45)
+            g = torch.Generator(device=dev)
+            g.manual_seed(1000)
+            psi = torch.rand(args.norb * lr.ncoeff, generator=g, device=dev, dtype=torch.float64) * 2 - 1
+            res = leg_overlap(torch, ctx, psi, args.norb)
         else:
             res = leg_serve(torch, dev, 32 if args.leg == "serve32" else 64)
         print(json.dumps({"leg": args.leg, "result": res}), flush=True)

@@ -9,9 +9,10 @@
 // the splits in a fixed order (deterministic) and mirrors the tile into the
 // upper triangle.
 //
-// Main loop: a 3-stage cp.async ring stages 64 x 32 slices of the two orbital
+// Main loop: a 2-stage cp.async ring stages 64 x 32 slices of the two orbital
 // panels in their storage type (16-byte copies when rows are 16-byte aligned),
-// so the loads of slice s+2 overlap the MMAs of slice s.  The contraction uses
+// so the loads of slice s+1 overlap the MMAs of slice s; at 74 KB (FP64) three
+// CTAs fit an SM.  The contraction uses
 // mma.sync m16n8k16 with FP64 operands (the largest FP64 tensor-core shape of
 // sm_90+/sm_100a; the tcgen05 family has no FP64 kind): 4 warps, each a 32 x 32
 // sub-tile = 2 x 4 MMA tiles; FP32 rows are widened when fragments are read.
@@ -23,7 +24,7 @@ namespace wvlh {
 
 constexpr int OV_BM = 64;       // tile edge (rows = orbitals i, cols = orbitals j)
 constexpr int OV_BK = 32;       // K slice per pipeline stage
-constexpr int OV_STAGES = 3;
+constexpr int OV_STAGES = 2;
 constexpr int OV_THREADS = 128;
 
 template <class TI> struct OvLd;   // padded smem row (elements): 16-byte multiple, 2-way bank spread
@@ -185,28 +186,30 @@ __global__ void __launch_bounds__(OV_THREADS) k_overlap_partial(int norb, long l
     }
 }
 
+// one thread per tile element (grid.x tiles, grid.y element blocks): the
+// splits are summed in order, so the result does not depend on the grid
 __global__ void k_overlap_reduce(int norb, int nsplit, const double *__restrict__ part, double *__restrict__ S)
 {
     const int tile = blockIdx.x;
     int ti, tj;
     tri_tile(tile, ti, tj);
-    for (int e = threadIdx.x; e < OV_BM * OV_BM; e += blockDim.x) {
-        const int r = e / OV_BM, c = e - r * OV_BM;
-        const int i = ti * OV_BM + r, j = tj * OV_BM + c;
-        if (i >= norb || j >= norb || j > i) continue;
-        double s = 0.0;
-        for (int k = 0; k < nsplit; ++k) s += part[((size_t)tile * nsplit + k) * OV_BM * OV_BM + e];
-        S[(size_t)i * norb + j] = s;
-        S[(size_t)j * norb + i] = s;
-    }
+    const int e = blockIdx.y * blockDim.x + threadIdx.x;
+    if (e >= OV_BM * OV_BM) return;
+    const int r = e / OV_BM, c = e - r * OV_BM;
+    const int i = ti * OV_BM + r, j = tj * OV_BM + c;
+    if (i >= norb || j >= norb || j > i) return;
+    double s = 0.0;
+    for (int k = 0; k < nsplit; ++k) s += part[((size_t)tile * nsplit + k) * OV_BM * OV_BM + e];
+    S[(size_t)i * norb + j] = s;
+    S[(size_t)j * norb + i] = s;
 }
 
-// splits over K: about two CTAs per SM (the 3-stage FP64 ring takes 110 KB)
+// splits over K: about three CTAs per SM (the 2-stage FP64 ring takes 74 KB)
 int overlap_split(int norb, long long K, int nsm)
 {
     const int nt = (norb + OV_BM - 1) / OV_BM;
     const int ntile = nt * (nt + 1) / 2;
-    int nsplit = (2 * nsm + ntile - 1) / ntile;
+    int nsplit = (3 * nsm + ntile - 1) / ntile;
     const long long maxs = (K + OV_BK - 1) / OV_BK;
     if (nsplit > maxs) nsplit = (int)maxs;
     return nsplit < 1 ? 1 : nsplit;
@@ -240,7 +243,7 @@ cudaError_t launch_overlap(int norb, long long K, long long ld, const TI *psi, d
         if ((e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem))) return e;
         k<<<ntile * nsplit, OV_THREADS, smem, st>>>(norb, K, ld, psi, nsplit, kchunk, work);
     }
-    k_overlap_reduce<<<ntile, 256, 0, st>>>(norb, nsplit, work, S);
+    k_overlap_reduce<<<dim3(ntile, OV_BM * OV_BM / 256), 256, 0, st>>>(norb, nsplit, work, S);
     return cudaGetLastError();
 }
 template cudaError_t launch_overlap<double>(int, long long, long long, const double *, double *, double *, int,
