@@ -34,6 +34,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <type_traits>
+
 #include "wvl_filters.h"
 
 namespace wvlh {
@@ -136,6 +138,18 @@ struct RowCol {
     }
 };
 
+// for_items over a pass body instantiated twice: FULL = true for segments
+// whose outputs all fall inside the line (no per-output bounds test), false
+// for the clipped ones; full(line, s) tells which.
+template <class Full, class Body>
+__device__ __forceinline__ void for_items2(int nlines, int nseg, Full &&full, Body &&body)
+{
+    for_items(nlines, nseg, [&](int line, int s) {
+        if (full(s)) body(line, s, std::true_type{});
+        else body(line, s, std::false_type{});
+    });
+}
+
 struct LineGeom {
     int nlines;
     int src_ls, src_ps;
@@ -153,7 +167,12 @@ __device__ __forceinline__ void pass_syn(const T *src, T *dst, const LineGeom g,
     const int off = per ? 0 : 7;      // storage index q = f + off
     const int fstart = per ? 0 : -8;  // even start in Fortran fine coordinates
     const int nseg = (F + off - fstart + SEG - 1) / SEG;
-    for_items(g.nlines, nseg, [&](int line, int s) {
+    auto full = [&](int s) {
+        const int q0 = fstart + s * SEG + off;
+        return q0 >= 0 && q0 + SEG <= F;
+    };
+    for_items2(g.nlines, nseg, full, [&](int line, int s, auto full_t) {
+        constexpr bool FULL = decltype(full_t)::value;
         const T *in = src + line * g.src_ls;
         T *out = dst + line * g.dst_ls;
         const int f0 = fstart + s * SEG;
@@ -184,7 +203,7 @@ __device__ __forceinline__ void pass_syn(const T *src, T *dst, const LineGeom g,
                 acc = fma(Filt<T>::ch(m + 7), xs[ic - l], acc);
                 acc = fma(Filt<T>::cg(m + 7), xw[ic - l], acc);
             }
-            if ((unsigned)q < (unsigned)F) out[q * g.dst_ps] = acc;
+            if (FULL || (unsigned)q < (unsigned)F) out[q * g.dst_ps] = acc;
         }
     });
 }
@@ -200,7 +219,9 @@ __device__ __forceinline__ void pass_ana(const T *src, T *dst, const LineGeom g,
     const int F = fine_len(N, per);
     const int off = per ? 0 : 7;
     const int nseg = (N + H - 1) / H;
-    for_items(g.nlines, nseg, [&](int line, int s) {
+    auto full = [&](int s) { return s * H + H <= N; };
+    for_items2(g.nlines, nseg, full, [&](int line, int s, auto full_t) {
+        constexpr bool FULL = decltype(full_t)::value;
         const T *in = src + line * g.src_ls;
         T *out = dst + line * g.dst_ls;
         const int i0 = s * H;
@@ -215,7 +236,7 @@ __device__ __forceinline__ void pass_ana(const T *src, T *dst, const LineGeom g,
                 di = fma(Filt<T>::cg(l), x[2 * t + l], di);
             }
             const int i = i0 + t;
-            if (i < N) {
+            if (FULL || i < N) {
                 out[i * g.dst_ps] = ci;
                 out[(i + N) * g.dst_ps] = di;
             }
@@ -233,7 +254,9 @@ __device__ __forceinline__ void pass_mf(const T *src, T *dst, const LineGeom g, 
     constexpr bool rev = (MODE == 1 || MODE == 3);
     constexpr int per = (MODE <= 1);
     const int nseg = (Lout + SEG - 1) / SEG;
-    for_items(g.nlines, nseg, [&](int line, int s) {
+    auto full = [&](int s) { return s * SEG + SEG <= Lout; };
+    for_items2(g.nlines, nseg, full, [&](int line, int s, auto full_t) {
+        constexpr bool FULL = decltype(full_t)::value;
         const T *in = src + line * g.src_ls;
         T *out = dst + line * g.dst_ls;
         const int q0 = s * SEG;
@@ -252,7 +275,7 @@ __device__ __forceinline__ void pass_mf(const T *src, T *dst, const LineGeom g, 
 #pragma unroll
             for (int k = 0; k < 16; ++k) acc = fma(Filt<T>::mf(rev ? 15 - k : k), x[t + k], acc);
             const int q = q0 + t;
-            if (q < Lout) out[q * g.dst_ps] = acc;
+            if (FULL || q < Lout) out[q * g.dst_ps] = acc;
         }
     });
 }
@@ -269,7 +292,9 @@ __device__ __forceinline__ void pass_kin(const T *src, T *dst, const LineGeom g,
     const T scale = (T)scale_d;
     const int nseg = (L + SEG - 1) / SEG;
     double e = 0.0;
-    for_items(g.nlines, nseg, [&](int line, int s) {
+    auto full = [&](int s) { return s * SEG + SEG <= L; };
+    for_items2(g.nlines, nseg, full, [&](int line, int s, auto full_t) {
+        constexpr bool FULL = decltype(full_t)::value;
         const T *in = src + line * g.src_ls;
         T *out = dst + line * g.dst_ls;
         const int q0 = s * SEG;
@@ -292,7 +317,7 @@ __device__ __forceinline__ void pass_kin(const T *src, T *dst, const LineGeom g,
                 }
             }
             const int q = q0 + t;
-            if (q < L) {
+            if (FULL || q < L) {
                 es = fma(x[t + 14], conv, es);
                 if constexpr (sizeof(T) == 4) el = fma(x[t + 14], lo, el);
                 const T base = ACC ? out[q * g.dst_ps] : cshift * x[t + 14];

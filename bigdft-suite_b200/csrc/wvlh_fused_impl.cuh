@@ -23,6 +23,12 @@
 // MODE_PRECOND the preconditioner operator D^-1/2 A (c + T) S D^-1/2 of
 // OpenCL/Preconditioner.c:98-128 through K1 (scaled gather, P only), the
 // kinetic chain of K2 and K3 (Z2 + c P + (K_x+K_y) P, scaled scatter).
+//
+// This file is the implementation shared by the translation units
+// wvlh_fused_f32.cu and wvlh_fused_f64.cu, which instantiate the launchers of
+// one precision each (the two compile in parallel); the common out-of-line
+// helpers are compiled in the FP64 unit (WVLH_FUSED_COMMON).
+#pragma once
 #include <cuda_runtime.h>
 
 #include <type_traits>
@@ -594,7 +600,7 @@ __global__ void __launch_bounds__(NT, plane_min_blocks(sizeof(T) == 4, PERSIST, 
 }
 
 // fixed-order per-orbital sum of the energy partial slots
-__global__ void k_reduce_energies(const double *__restrict__ part_pot, const double *__restrict__ part_kin,
+static __global__ void k_reduce_energies(const double *__restrict__ part_pot, const double *__restrict__ part_kin,
                                   int part_stride, int norb, double *__restrict__ ekin, double *__restrict__ epot)
 {
     __shared__ double red[32];
@@ -691,7 +697,7 @@ __global__ void __launch_bounds__(kZThreads) kd_density(const LrDev *__restrict_
 }
 
 // rho[group] += sum of the group's chunk partials, in chunk order
-__global__ void k_density_reduce(const int *__restrict__ group_chunk_start, const long long *__restrict__ group_rho,
+static __global__ void k_density_reduce(const int *__restrict__ group_chunk_start, const long long *__restrict__ group_rho,
                                  const int *__restrict__ group_n, const long long *__restrict__ chunk_part,
                                  const double *__restrict__ part, double *__restrict__ rho)
 {
@@ -729,7 +735,7 @@ __global__ void k_cg_dot(const long long *__restrict__ off, const int *__restric
 }
 
 // out[o] = sum of its chunk partials (fixed order); optionally copy into hist
-__global__ void k_cg_sum(int norb, const double *__restrict__ part, double *__restrict__ out,
+static __global__ void k_cg_sum(int norb, const double *__restrict__ part, double *__restrict__ out,
                          double *__restrict__ hist)
 {
     const int o = blockIdx.x * blockDim.x + threadIdx.x;
@@ -796,7 +802,7 @@ __global__ void k_cg_dir(const long long *__restrict__ off, const int *__restric
         d[base + i] = fma(beta, d[base + i], r[base + i]);
 }
 
-__global__ void k_copy_scalars(int n, const double *__restrict__ a, double *__restrict__ b)
+static __global__ void k_copy_scalars(int n, const double *__restrict__ a, double *__restrict__ b)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) b[i] = a[i];
@@ -874,6 +880,7 @@ static auto k3_for(const PlaneCfg &pc) -> decltype(&k3_plane_backward<T, TO, ALL
     return k3_plane_backward<T, TO, ALLPER, MODE, false, kPlaneThreads>;
 }
 
+#ifdef WVLH_FUSED_COMMON
 long long plane_tmp_elems(const Plan &p, int fp)
 {
     int dev = 0, lim = 0, nsm = 0;
@@ -882,6 +889,7 @@ long long plane_tmp_elems(const Plan &p, int fp)
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
     return p.smem13[fp] > (size_t)lim - 1024 ? (long long)nsm * p.planeB_elems : 0;
 }
+#endif
 template <class T, class TIO, bool ALLPER>
 static cudaError_t launch_locham_bc(const Plan &p, const TIO *psi, const TIO *pot, TIO *hpsi, T *scratch,
                                     double *part_pot, double *part_kin, double *ekin, double *epot, int accumulate,
@@ -932,12 +940,16 @@ cudaError_t launch_locham(const Plan &p, const TIO *psi, const TIO *pot, TIO *hp
                                            st, ev);
 }
 
+#ifdef WVLH_FUSED_F32
 template cudaError_t launch_locham<float, float>(const Plan &, const float *, const float *, float *, float *,
                                                  double *, double *, double *, double *, int, cudaStream_t,
                                                  cudaEvent_t *);
+#endif
+#ifdef WVLH_FUSED_F64
 template cudaError_t launch_locham<double, double>(const Plan &, const double *, const double *, double *, double *,
                                                    double *, double *, double *, double *, int, cudaStream_t,
                                                    cudaEvent_t *);
+#endif
 
 template <class T, bool ALLPER>
 static cudaError_t launch_locden_bc(const Plan &p, const T *psi, const double *hfac, double *rho, T *scratch,
@@ -969,10 +981,14 @@ cudaError_t launch_locden(const Plan &p, const T *psi, const double *hfac, doubl
     if (p.all_periodic) return launch_locden_bc<T, true>(p, psi, hfac, rho, scratch, part, st);
     return launch_locden_bc<T, false>(p, psi, hfac, rho, scratch, part, st);
 }
+#ifdef WVLH_FUSED_F32
 template cudaError_t launch_locden<float>(const Plan &, const float *, const double *, double *, float *, double *,
                                           cudaStream_t);
+#endif
+#ifdef WVLH_FUSED_F64
 template cudaError_t launch_locden<double>(const Plan &, const double *, const double *, double *, double *,
                                            double *, cudaStream_t);
+#endif
 
 // preconditioner operator y = D^-1/2 A (c + T) S D^-1/2 x for every orbital
 template <class T, bool ALLPER>
@@ -1032,11 +1048,16 @@ cudaError_t launch_precond(const Plan &p, int ncong, const double *cprec, T *x, 
     k_cg_scale<T><<<vg, 256, 0, st>>>(p.d_lr, p.d_orb, p.d_orb_off, p.d_orb_len, cprec, x);
     return cudaGetLastError();
 }
+#ifdef WVLH_FUSED_F32
 template cudaError_t launch_precond<float>(const Plan &, int, const double *, float *, const float *, float *, float *,
                                            float *, float *, double *, double *, cudaStream_t);
+#endif
+#ifdef WVLH_FUSED_F64
 template cudaError_t launch_precond<double>(const Plan &, int, const double *, double *, const double *, double *,
                                             double *, double *, double *, double *, double *, cudaStream_t);
+#endif
 
+#ifdef WVLH_FUSED_COMMON
 // FP32/FP64 FMA throughput probe: independent FMA chains held in registers.
 template <class T>
 __global__ void __launch_bounds__(256) k_fma_probe(T *out, int iters, T a, T b)
@@ -1080,5 +1101,7 @@ cudaError_t fma_probe(int precision, int iters, float *ms, double *flops, cudaSt
     cudaFree(buf);
     return cudaGetLastError();
 }
+
+#endif
 
 }  // namespace wvlh

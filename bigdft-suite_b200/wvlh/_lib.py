@@ -23,7 +23,7 @@ ERRORS = {1: "CUDA runtime error", 2: "invalid argument", 3: "invalid segment ke
 def build(force=False):
     """Compile libwvlh.so for sm_100a (nvcc cross-compiles without a GPU)."""
     if force or not LIB_PATH.exists():
-        subprocess.run(["make", "-s", "-C", str(CSRC)], check=True)
+        subprocess.run(["make", "-s", "-j4", "-C", str(CSRC)], check=True)
 
 
 def check(rc, what=""):
