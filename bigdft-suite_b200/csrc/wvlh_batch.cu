@@ -388,10 +388,12 @@ static void layout(wvlh_batch *b, const std::vector<int> &orb_lr, const std::vec
         pre2p.push_back(pre2p.back() + ntx1 * nty1);
         stride = std::max(stride, std::max(ntx0 * nty0, ntx1 * nty1 + G3));
         // plane buffer A: rows (y) x pitch (x); B also holds transposed planes:
-        // rowsT (x) x pitchT (y)
-        const int pitch = std::max(G1, std::max(F1, I1)) | 1;
-        const int rows = std::max(G2, std::max(F2, I2));
-        const int rowsT = std::max(G1, std::max(F1, I1)), pitchT = rows | 1;
+        // rowsT (x) x pitchT (y).  Coarse lines are stored with the wavelet
+        // half at an even offset (coarse_width), pitches are vec_pitch.
+        const int W1 = coarse_width(N1), W2 = coarse_width(N2);
+        const int pitch = vec_pitch(std::max(W1, std::max(F1, I1)));
+        const int rows = std::max(W2, std::max(F2, I2));
+        const int rowsT = std::max(W1, std::max(F1, I1)), pitchT = vec_pitch(rows);
         planeA = std::max(planeA, (size_t)rows * pitch);
         {
             const long long len = std::max(G1, std::max(F1, I1)), w = (long long)G3 * rows * pitch;
@@ -406,7 +408,7 @@ static void layout(wvlh_batch *b, const std::vector<int> &orb_lr, const std::vec
     p.psi_total = psi_off;
     p.all_periodic = true;
     for (int v : p.lr_per) p.all_periodic = p.all_periodic && v == 1;
-    p.scratch_elems = scr;
+    p.scratch_elems = (scr + 1) & ~1LL;  // even: the global plane slices after it start on a point pair
     p.part_stride = stride;
     p.plane_threads[0] = choose_plane_threads(shapes32, true);
     p.plane_threads[1] = choose_plane_threads(shapes64, false);

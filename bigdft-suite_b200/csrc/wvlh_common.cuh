@@ -73,6 +73,21 @@ __device__ __forceinline__ int wrap_near(int p, int L)
     return p;
 }
 
+// Plane layout of the fused kernels' shared-memory buffers.  A coarse line is
+// [s(0..N-1) | w(0..N-1)] with the wavelet half at the even offset
+// half_off(N), so both halves start on a point pair.  Buffers whose lines run
+// along rows use a row pitch with pitch % 4 == 2: every row starts on a point
+// pair (8 bytes FP32, 16 bytes FP64), which lets the unit-stride passes load
+// two points per instruction, and lanes that take consecutive rows still hit
+// distinct banks (half-warp phases for 8-byte, quarter-warp for 16-byte).
+__host__ __device__ constexpr int half_off(int N) { return (N + 1) & ~1; }
+__host__ __device__ constexpr int coarse_width(int N) { return half_off(N) + N; }
+__host__ __device__ constexpr int vec_pitch(int m) { return ((m + 1) & ~1) + ((((m + 1) & ~1) & 3) == 0 ? 2 : 0); }
+
+template <class T> struct Pair;
+template <> struct Pair<float> { using type = float2; };
+template <> struct Pair<double> { using type = double2; };
+
 // Load x[k] = line(p0 + k), k < W, with periodic wrap or zero padding; the
 // common interior case takes a single base address and constant strides.
 template <class T, int W>
@@ -92,6 +107,60 @@ __device__ __forceinline__ void load_window(T (&x)[W], const T *in, int ps, int 
             x[k] = ((unsigned)p < (unsigned)L) ? in[p * ps] : T(0);
         }
     }
+}
+
+// Window load for a unit-stride line that starts on a point pair, q0 even:
+// x[k] = line(q0 + SHIFT + k).  The window is read as W/2 + 1 point pairs from
+// the pair boundary below q0 + SHIFT (never past the pair holding the line's
+// last point, so reads stay inside the row); periodic wrap and zero padding
+// then act on whole pairs when L is even.  Odd L (free-BC ISF lines) takes the
+// scalar path at the line ends.
+template <class T, int W, int SHIFT>
+__device__ __forceinline__ void load_window_u(T (&x)[W], const T *in, int q0, int L, int per)
+{
+    using V = typename Pair<T>::type;
+    constexpr int R = SHIFT & 1;
+    constexpr int A0 = SHIFT - R;
+    constexpr int NV = (W + R + 1) / 2;
+    const int a = q0 + A0;
+    T y[2 * NV];
+    if (a >= 0 && q0 + SHIFT + W <= L) {
+        const V *b = reinterpret_cast<const V *>(in + a);
+#pragma unroll
+        for (int c = 0; c < NV; ++c) {
+            const V v = b[c];
+            y[2 * c] = v.x;
+            y[2 * c + 1] = v.y;
+        }
+    } else if (!(L & 1)) {
+#pragma unroll
+        for (int c = 0; c < NV; ++c) {
+            const int p = a + 2 * c;
+            V v;
+            if (per) {
+                v = *reinterpret_cast<const V *>(in + wrap_near(p, L));
+            } else {
+                v.x = T(0);
+                v.y = T(0);
+                if ((unsigned)p < (unsigned)L) v = *reinterpret_cast<const V *>(in + p);
+            }
+            y[2 * c] = v.x;
+            y[2 * c + 1] = v.y;
+        }
+    } else {
+        load_window<T, W>(x, in, 1, q0 + SHIFT, L, per);
+        return;
+    }
+#pragma unroll
+    for (int k = 0; k < W; ++k) x[k] = y[k + R];
+}
+
+// UNIT passes read lines with unit stride from rows that start on a point pair
+template <class T, int W, int SHIFT, bool UNIT>
+__device__ __forceinline__ void load_window_g(T (&x)[W], const T *in, int ps, int q0, int L, int per)
+{
+    if constexpr (UNIT) load_window_u<T, W, SHIFT>(x, in, q0, L, per);
+    else load_window<T, W>(x, in, ps, q0 + SHIFT, L, per);
 }
 
 // Distribute (line, segment) work items over the block: consecutive threads
@@ -157,9 +226,10 @@ struct LineGeom {
 };
 
 // ---------------------------------------------------------------- synthesis
-// src line: [s(0..N-1) | w(0..N-1)], dst line: F = fine_len(N,per) values.
-template <class T, int SEG>
-__device__ __forceinline__ void pass_syn(const T *src, T *dst, const LineGeom g, int N, int per)
+// src line: [s(0..N-1) | w(0..N-1)], the wavelet half at offset H (N, or
+// half_off(N) in the fused planes); dst line: F = fine_len(N,per) values.
+template <class T, int SEG, bool UNIT = false>
+__device__ __forceinline__ void pass_syn(const T *src, T *dst, const LineGeom g, int N, int H, int per)
 {
     static_assert(SEG % 2 == 0, "even segment");
     constexpr int W = SEG / 2 + 8;
@@ -176,10 +246,10 @@ __device__ __forceinline__ void pass_syn(const T *src, T *dst, const LineGeom g,
         const T *in = src + line * g.src_ls;
         T *out = dst + line * g.dst_ls;
         const int f0 = fstart + s * SEG;
-        const int ib = f0 / 2 - 4;  // f0 is even, so f0/2 is exact
+        const int c0 = f0 / 2;  // f0 is even, so f0/2 is exact (and even)
         T xs[W], xw[W];
-        load_window<T, W>(xs, in, g.src_ps, ib, N, per);
-        load_window<T, W>(xw, in + N * g.src_ps, g.src_ps, ib, N, per);
+        load_window_g<T, W, -4, UNIT>(xs, in, g.src_ps, c0, N, per);
+        load_window_g<T, W, -4, UNIT>(xw, in + H * g.src_ps, g.src_ps, c0, N, per);
 #pragma unroll
         for (int t = 0; t < SEG; ++t) {
             const int q = f0 + t + off;
@@ -209,26 +279,26 @@ __device__ __forceinline__ void pass_syn(const T *src, T *dst, const LineGeom g,
 }
 
 // ---------------------------------------------------------------- analysis
-// src line: F fine values; dst line: [c(0..N-1) | d(0..N-1)]
-template <class T, int SEG>
-__device__ __forceinline__ void pass_ana(const T *src, T *dst, const LineGeom g, int N, int per)
+// src line: F fine values; dst line: [c(0..N-1) | d(0..N-1)], d at offset H
+template <class T, int SEG, bool UNIT = false>
+__device__ __forceinline__ void pass_ana(const T *src, T *dst, const LineGeom g, int N, int H, int per)
 {
     static_assert(SEG % 2 == 0, "even segment");
-    constexpr int H = SEG / 2;
+    constexpr int HS = SEG / 2;
     constexpr int W = SEG + 14;
     const int F = fine_len(N, per);
-    const int off = per ? 0 : 7;
-    const int nseg = (N + H - 1) / H;
-    auto full = [&](int s) { return s * H + H <= N; };
+    const int nseg = (N + HS - 1) / HS;
+    auto full = [&](int s) { return s * HS + HS <= N; };
     for_items2(g.nlines, nseg, full, [&](int line, int s, auto full_t) {
         constexpr bool FULL = decltype(full_t)::value;
         const T *in = src + line * g.src_ls;
         T *out = dst + line * g.dst_ls;
-        const int i0 = s * H;
+        const int i0 = s * HS;
         T x[W];
-        load_window<T, W>(x, in, g.src_ps, 2 * i0 - 7 + off, F, per);
+        if (per) load_window_g<T, W, -7, UNIT>(x, in, g.src_ps, 2 * i0, F, 1);
+        else load_window_g<T, W, 0, UNIT>(x, in, g.src_ps, 2 * i0, F, 0);
 #pragma unroll
-        for (int t = 0; t < H; ++t) {
+        for (int t = 0; t < HS; ++t) {
             T ci = T(0), di = T(0);
 #pragma unroll
             for (int l = 0; l < 16; ++l) {
@@ -238,7 +308,7 @@ __device__ __forceinline__ void pass_ana(const T *src, T *dst, const LineGeom g,
             const int i = i0 + t;
             if (FULL || i < N) {
                 out[i * g.dst_ps] = ci;
-                out[(i + N) * g.dst_ps] = di;
+                out[(i + H) * g.dst_ps] = di;
             }
         }
     });
@@ -246,7 +316,7 @@ __device__ __forceinline__ void pass_ana(const T *src, T *dst, const LineGeom g,
 
 // ---------------------------------------------------------------- magic filter
 // MODE 0: mf periodic, 1: mft periodic, 2: mf grow (F -> F+15), 3: mft shrink (F+15 -> F)
-template <class T, int SEG, int MODE>
+template <class T, int SEG, int MODE, bool UNIT = false>
 __device__ __forceinline__ void pass_mf(const T *src, T *dst, const LineGeom g, int Lin, int Lout)
 {
     constexpr int W = SEG + 15;
@@ -261,7 +331,7 @@ __device__ __forceinline__ void pass_mf(const T *src, T *dst, const LineGeom g, 
         T *out = dst + line * g.dst_ls;
         const int q0 = s * SEG;
         T x[W];
-        load_window<T, W>(x, in, g.src_ps, q0 + shift, Lin, per);
+        load_window_g<T, W, shift, UNIT>(x, in, g.src_ps, q0, Lin, per);
 #pragma unroll
         for (int t = 0; t < SEG; ++t) {
             T acc = T(0);
@@ -284,7 +354,9 @@ __device__ __forceinline__ void pass_mf(const T *src, T *dst, const LineGeom g, 
 // dst(q) = (ACC ? dst(q) : cshift * src(q)) + scale * sum_l a(|l|) src(q+l)
 // with scale = -1/(2h^2) (cshift: the preconditioner's c of (T + c),
 // OpenCL/Preconditioner.c:108); ekin += src(q) * scale * conv in FP64.
-template <class T, int SEG, bool ACC>
+// UNIT: source and destination lines are unit-stride rows starting on a point
+// pair (window and full output segments move as point pairs).
+template <class T, int SEG, bool ACC, bool UNIT = false>
 __device__ __forceinline__ void pass_kin(const T *src, T *dst, const LineGeom g, int L, int per, double scale_d, T cshift,
                          double *ekin)
 {
@@ -299,10 +371,11 @@ __device__ __forceinline__ void pass_kin(const T *src, T *dst, const LineGeom g,
         T *out = dst + line * g.dst_ls;
         const int q0 = s * SEG;
         T x[W];
-        load_window<T, W>(x, in, g.src_ps, q0 - 14, L, per);
+        load_window_g<T, W, -14, UNIT>(x, in, g.src_ps, q0, L, per);
         // per-segment partial sums of x.conv (and of x.lo in FP32), converted
         // to FP64 once per segment; the rounding of these short sums is unbiased
         T es = T(0), el = T(0);
+        T prev = T(0);
 #pragma unroll
         for (int t = 0; t < SEG; ++t) {
             T conv = Filt<T>::kin(0) * x[t + 14];
@@ -320,8 +393,27 @@ __device__ __forceinline__ void pass_kin(const T *src, T *dst, const LineGeom g,
             if (FULL || q < L) {
                 es = fma(x[t + 14], conv, es);
                 if constexpr (sizeof(T) == 4) el = fma(x[t + 14], lo, el);
-                const T base = ACC ? out[q * g.dst_ps] : cshift * x[t + 14];
-                out[q * g.dst_ps] = fma(scale, conv, base);
+                if constexpr (UNIT && FULL) {
+                    // full unit-stride segment: store each point pair once both are formed
+                    if (t & 1) {
+                        using V = typename Pair<T>::type;
+                        V *o = reinterpret_cast<V *>(out + q - 1);
+                        V v;
+                        if (ACC) v = *o;
+                        else {
+                            v.x = cshift * x[t + 13];
+                            v.y = cshift * x[t + 14];
+                        }
+                        v.x = fma(scale, prev, v.x);
+                        v.y = fma(scale, conv, v.y);
+                        *o = v;
+                    } else {
+                        prev = conv;
+                    }
+                } else {
+                    const T base = ACC ? out[q * g.dst_ps] : cshift * x[t + 14];
+                    out[q * g.dst_ps] = fma(scale, conv, base);
+                }
             }
         }
         e += ((double)es + (double)el) * scale_d;

@@ -48,6 +48,7 @@ template <> struct Seg<double> { static constexpr int v = 4; };
 
 struct Dims {
     int N1, N2, N3, p1, p2, p3;
+    int H1, H2;  // offsets of the wavelet halves of the coarse x and y lines
     int G1, G2, G3, F1, F2, F3, I1, I2, I3;
     // allper: the batch is known to be periodic in every direction, which lets
     // the compiler drop the free-boundary variants from the kernel
@@ -57,15 +58,16 @@ struct Dims {
         p1 = allper ? 1 : L.per[0];
         p2 = allper ? 1 : L.per[1];
         p3 = allper ? 1 : L.per[2];
-        G1 = 2 * N1; G2 = 2 * N2; G3 = 2 * N3;
+        H1 = half_off(N1); H2 = half_off(N2);
+        G1 = coarse_width(N1); G2 = coarse_width(N2); G3 = 2 * N3;
         F1 = fine_len(N1, p1); F2 = fine_len(N2, p2); F3 = fine_len(N3, p3);
         I1 = isf_len(N1, p1); I2 = isf_len(N2, p2); I3 = isf_len(N3, p3);
     }
     // plane buffer A: rows() lines (y) of pitch() points (x); the second buffer
     // B also holds transposed planes: rowsT() lines (x) of pitchT() points (y)
-    __device__ __forceinline__ int pitch() const { return (max(G1, max(F1, I1))) | 1; }
+    __device__ __forceinline__ int pitch() const { return vec_pitch(max(G1, max(F1, I1))); }
     __device__ __forceinline__ int rows() const { return max(G2, max(F2, I2)); }
-    __device__ __forceinline__ int pitchT() const { return rows() | 1; }
+    __device__ __forceinline__ int pitchT() const { return vec_pitch(rows()); }
 };
 
 __device__ __forceinline__ LineGeom rows_geom(int nrows, int pitch)
@@ -101,16 +103,15 @@ __device__ __forceinline__ double prec_scal(const LrDev &L, double c, int k)
 }
 
 // Scatter the compressed coefficients of wavelet-basis plane kz into the
-// (G2 x G1, pitch) buffer A, which must be zero.  psi points at [psi_c|psi_f];
-// sc (8 factors) scales each component when non-null.
-template <class T, class TI>
-__device__ void gather_plane(T *A, int pitch, const LrDev &L, int kz, const TI *psi, const T *sc)
+// (G2 x G1, pitch) buffer A, which must be zero.  Wavelet components sit at
+// x + half_off(N1) and y + half_off(N2).  psi points at [psi_c|psi_f]; sc (8
+// factors) scales each component when non-null.
+template <class T, class TI, int S3>
+__device__ __forceinline__ void gather_plane_s(T *A, int pitch, const LrDev &L, int i3, const TI *psi, const T *sc)
 {
-    const int N1 = L.N[0], N2 = L.N[1], N3 = L.N[2];
-    const int s3 = kz >= N3;
-    const int i3 = kz - s3 * N3;
+    const int H1 = half_off(L.N[0]), H2 = half_off(L.N[1]);
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-    if (!s3) {
+    if (!S3) {
         const T s0 = sc ? sc[0] : T(1);
         const int a = L.plane_c[i3], b = L.plane_c[i3 + 1];
         for (int sg = a + warp; sg < b; sg += nw) {
@@ -126,22 +127,30 @@ __device__ void gather_plane(T *A, int pitch, const LrDev &L, int kz, const TI *
             const TI *src = pf + 7 * (size_t)(d.w + t);
 #pragma unroll
             for (int c = 1; c <= 7; ++c) {
-                if (fs3(c) != s3) continue;
-                A[(fs2(c) * N2 + d.y) * pitch + fs1(c) * N1 + d.x + t] = (T)src[c - 1] * (sc ? sc[c] : T(1));
+                if (fs3(c) != S3) continue;
+                A[(fs2(c) * H2 + d.y) * pitch + fs1(c) * H1 + d.x + t] = (T)src[c - 1] * (sc ? sc[c] : T(1));
             }
         }
     }
 }
 
-// Inverse of gather_plane: write (or add into) the compressed output.
-template <class T, class TO>
-__device__ void scatter_plane(const T *A, int pitch, const LrDev &L, int kz, TO *out, bool accumulate, const T *sc)
+// the z component s3 of a plane is uniform over the CTA: one copy of the
+// component loop per s3, so no instruction is issued for the other half
+template <class T, class TI>
+__device__ void gather_plane(T *A, int pitch, const LrDev &L, int kz, const TI *psi, const T *sc)
 {
-    const int N1 = L.N[0], N2 = L.N[1], N3 = L.N[2];
-    const int s3 = kz >= N3;
-    const int i3 = kz - s3 * N3;
+    if (kz >= L.N[2]) gather_plane_s<T, TI, 1>(A, pitch, L, kz - L.N[2], psi, sc);
+    else gather_plane_s<T, TI, 0>(A, pitch, L, kz, psi, sc);
+}
+
+// Inverse of gather_plane: write (or add into) the compressed output.
+template <class T, class TO, int S3>
+__device__ __forceinline__ void scatter_plane_s(const T *A, int pitch, const LrDev &L, int i3, TO *out, bool accumulate,
+                                                const T *sc)
+{
+    const int H1 = half_off(L.N[0]), H2 = half_off(L.N[1]);
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-    if (!s3) {
+    if (!S3) {
         const T s0 = sc ? sc[0] : T(1);
         const int a = L.plane_c[i3], b = L.plane_c[i3 + 1];
         for (int sg = a + warp; sg < b; sg += nw) {
@@ -160,23 +169,62 @@ __device__ void scatter_plane(const T *A, int pitch, const LrDev &L, int kz, TO 
             TO *dst = pf + 7 * (size_t)(d.w + t);
 #pragma unroll
             for (int c = 1; c <= 7; ++c) {
-                if (fs3(c) != s3) continue;
-                const TO v = (TO)(A[(fs2(c) * N2 + d.y) * pitch + fs1(c) * N1 + d.x + t] * (sc ? sc[c] : T(1)));
+                if (fs3(c) != S3) continue;
+                const TO v = (TO)(A[(fs2(c) * H2 + d.y) * pitch + fs1(c) * H1 + d.x + t] * (sc ? sc[c] : T(1)));
                 dst[c - 1] = accumulate ? dst[c - 1] + v : v;
             }
         }
     }
 }
 
+template <class T, class TO>
+__device__ void scatter_plane(const T *A, int pitch, const LrDev &L, int kz, TO *out, bool accumulate, const T *sc)
+{
+    if (kz >= L.N[2]) scatter_plane_s<T, TO, 1>(A, pitch, L, kz - L.N[2], out, accumulate, sc);
+    else scatter_plane_s<T, TO, 0>(A, pitch, L, kz, out, accumulate, sc);
+}
+
+// Rows of `cols` points walked as point pairs: warp w takes rows w, w + nwarps,
+// ...; its lanes take consecutive pairs of the row.  f(r, c), c even.
+template <class F>
+__device__ __forceinline__ void for_row_pairs(int rows, int cols, F &&f)
+{
+    const int lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+    const int np = cols >> 1;
+    for (int r = threadIdx.x >> 5; r < rows; r += nw)
+        for (int j = lane; j < np; j += 32) f(r, 2 * j);
+}
+
+// a dense global plane of `cols`-point rows can move as point pairs when cols
+// is even and the plane starts on a pair (the scratch planes do)
+template <class T>
+__device__ __forceinline__ bool pair_rows(int cols, const T *g)
+{
+    return !(cols & 1) && !(reinterpret_cast<uintptr_t>(g) & (2 * sizeof(T) - 1));
+}
+
 template <class T>
 __device__ __forceinline__ void zero_region(T *A, int rows, int pitch)
 {
-    for (int i = threadIdx.x; i < rows * pitch; i += blockDim.x) A[i] = T(0);
+    // rows * pitch is even and A starts on a pair
+    using V = typename Pair<T>::type;
+    V *a = reinterpret_cast<V *>(A);
+    V z;
+    z.x = T(0);
+    z.y = T(0);
+    for (int i = threadIdx.x; i < (rows * pitch) >> 1; i += blockDim.x) a[i] = z;
 }
 
 template <class T>
 __device__ __forceinline__ void store_plane(const T *A, int pitch, int rows, int cols, T *g)
 {
+    if (pair_rows(cols, g)) {
+        using V = typename Pair<T>::type;
+        for_row_pairs(rows, cols, [&](int r, int c) {
+            *reinterpret_cast<V *>(g + (size_t)r * cols + c) = *reinterpret_cast<const V *>(A + r * pitch + c);
+        });
+        return;
+    }
     RowCol q(cols);
     for (int i = threadIdx.x; i < rows * cols; i += blockDim.x, q.next()) g[i] = A[q.r * pitch + q.c];
 }
@@ -225,10 +273,25 @@ __device__ __forceinline__ void cp_async_elem(T *dst, const T *src, bool valid)
 }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
 
+// point-pair copy global -> shared (8 bytes FP32, 16 bytes FP64), both addresses on a pair
+template <class T>
+__device__ __forceinline__ void cp_async_pair(T *dst, const T *src)
+{
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    if constexpr (sizeof(T) == 4)
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(src) : "memory");
+    else
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(src) : "memory");
+}
+
 // load_plane through cp.async (A in shared memory); the caller waits
 template <class T>
 __device__ __forceinline__ void load_plane_async(T *A, int pitch, int rows, int cols, const T *g)
 {
+    if (pair_rows(cols, g)) {
+        for_row_pairs(rows, cols, [&](int r, int c) { cp_async_pair(A + r * pitch + c, g + (size_t)r * cols + c); });
+        return;
+    }
     RowCol q(cols);
     for (int i = threadIdx.x; i < rows * cols; i += blockDim.x, q.next())
         cp_async_elem(A + q.r * pitch + q.c, g + i, true);
@@ -236,14 +299,12 @@ __device__ __forceinline__ void load_plane_async(T *A, int pitch, int rows, int 
 
 // gather_plane through cp.async (no scaling, same element type); the caller
 // waits.  Each coefficient is one queued copy to its slot of the plane.
-template <class T>
-__device__ void gather_plane_async(T *A, int pitch, const LrDev &L, int kz, const T *psi)
+template <class T, int S3>
+__device__ __forceinline__ void gather_plane_async_s(T *A, int pitch, const LrDev &L, int i3, const T *psi)
 {
-    const int N1 = L.N[0], N2 = L.N[1], N3 = L.N[2];
-    const int s3 = kz >= N3;
-    const int i3 = kz - s3 * N3;
+    const int H1 = half_off(L.N[0]), H2 = half_off(L.N[1]);
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-    if (!s3) {
+    if (!S3) {
         const int a = L.plane_c[i3], b = L.plane_c[i3 + 1];
         for (int sg = a + warp; sg < b; sg += nw) {
             const int4 d = L.seg_c[sg];
@@ -258,11 +319,18 @@ __device__ void gather_plane_async(T *A, int pitch, const LrDev &L, int kz, cons
             const T *src = pf + 7 * (size_t)(d.w + t);
 #pragma unroll
             for (int c = 1; c <= 7; ++c) {
-                if (fs3(c) != s3) continue;
-                cp_async_elem(A + (fs2(c) * N2 + d.y) * pitch + fs1(c) * N1 + d.x + t, src + c - 1, true);
+                if (fs3(c) != S3) continue;
+                cp_async_elem(A + (fs2(c) * H2 + d.y) * pitch + fs1(c) * H1 + d.x + t, src + c - 1, true);
             }
         }
     }
+}
+
+template <class T>
+__device__ void gather_plane_async(T *A, int pitch, const LrDev &L, int kz, const T *psi)
+{
+    if (kz >= L.N[2]) gather_plane_async_s<T, 1>(A, pitch, L, kz - L.N[2], psi);
+    else gather_plane_async_s<T, 0>(A, pitch, L, kz, psi);
 }
 
 template <class TI>
@@ -326,24 +394,24 @@ __device__ __forceinline__ void k1_item(const LrDev *__restrict__ lrs, const Orb
                 const int s3 = kz >= d.N3 ? 4 : 0;
                 RowCol q(d.G1);
                 for (int i = threadIdx.x; i < d.G2 * d.G1; i += blockDim.x, q.next())
-                    A[q.r * pitch + q.c] *= sc[(q.c >= d.N1 ? 1 : 0) + (q.r >= d.N2 ? 2 : 0) + s3];
+                    A[q.r * pitch + q.c] *= sc[(q.c >= d.H1 ? 1 : 0) + (q.r >= d.H2 ? 2 : 0) + s3];
             }
         } else {
             gather_plane<T, TI>(A, pitch, L, kz, in_ptr(o, psi), MODE == MODE_PRECOND ? sc : nullptr);
         }
         __syncthreads();
         const int pt = d.pitchT();
-        pass_syn<T, SEG>(A, B, xpose_geom(d.G2, pitch, pt), d.N1, d.p1);   // S_x: G2 rows, G1 -> F1, into B^T
+        pass_syn<T, SEG, true>(A, B, xpose_geom(d.G2, pitch, pt), d.N1, d.H1, d.p1);   // S_x: G2 rows, G1 -> F1, into B^T
         __syncthreads();
-        pass_syn<T, SEG>(B, A, xpose_geom(d.F1, pt, pitch), d.N2, d.p2);   // S_y: F1 lines, G2 -> F2, into A
+        pass_syn<T, SEG, true>(B, A, xpose_geom(d.F1, pt, pitch), d.N2, d.H2, d.p2);   // S_y: F1 lines, G2 -> F2, into A
         __syncthreads();
         if (MODE != MODE_LOCDEN) store_plane(A, pitch, d.F2, d.F1, scratch + o.sP + (size_t)kz * d.F2 * d.F1);
         if (MODE == MODE_PRECOND) return;
-        if (d.p1) pass_mf<T, SEG, 0>(A, B, xpose_geom(d.F2, pitch, pt), d.F1, d.I1);   // M_x into B^T
-        else pass_mf<T, SEG, 2>(A, B, xpose_geom(d.F2, pitch, pt), d.F1, d.I1);
+        if (d.p1) pass_mf<T, SEG, 0, true>(A, B, xpose_geom(d.F2, pitch, pt), d.F1, d.I1);   // M_x into B^T
+        else pass_mf<T, SEG, 2, true>(A, B, xpose_geom(d.F2, pitch, pt), d.F1, d.I1);
         __syncthreads();
-        if (d.p2) pass_mf<T, SEG, 0>(B, A, xpose_geom(d.I1, pt, pitch), d.F2, d.I2);   // M_y into A
-        else pass_mf<T, SEG, 2>(B, A, xpose_geom(d.I1, pt, pitch), d.F2, d.I2);
+        if (d.p2) pass_mf<T, SEG, 0, true>(B, A, xpose_geom(d.I1, pt, pitch), d.F2, d.I2);   // M_y into A
+        else pass_mf<T, SEG, 2, true>(B, A, xpose_geom(d.I1, pt, pitch), d.F2, d.I2);
         __syncthreads();
         store_plane(A, pitch, d.I2, d.I1, scratch + o.sQ + (size_t)kz * d.I2 * d.I1);
     }
@@ -418,7 +486,7 @@ __global__ void __launch_bounds__(kZThreads, sizeof(T) == 4 ? 4 : 1) k2_zpencil(
     __syncthreads();
     const LineGeom zg{TC, 1, TC, 1, TC};
     double e = 0.0;
-    pass_syn<T, SEG>(A, B, zg, d.N3, d.p3);                      // S_z: G3 -> F3
+    pass_syn<T, SEG>(A, B, zg, d.N3, d.N3, d.p3);                      // S_z: G3 -> F3
     __syncthreads();
     if constexpr (chain == 0) {
         if (d.p3) pass_mf<T, SEG, 0>(B, A, zg, d.F3, d.I3);       // M_z: F3 -> I3
@@ -453,12 +521,12 @@ __global__ void __launch_bounds__(kZThreads, sizeof(T) == 4 ? 4 : 1) k2_zpencil(
         if (d.p3) pass_mf<T, SEG, 1>(A, B, zg, d.I3, d.F3);       // Mt_z: I3 -> F3
         else pass_mf<T, SEG, 3>(A, B, zg, d.I3, d.F3);
         __syncthreads();
-        pass_ana<T, SEG>(B, A, zg, d.N3, d.p3);                  // A_z: F3 -> G3
+        pass_ana<T, SEG>(B, A, zg, d.N3, d.N3, d.p3);                  // A_z: F3 -> G3
     } else {
         const double scale = -0.5 / ((0.5 * L.hgrid[2]) * (0.5 * L.hgrid[2]));
         pass_kin<T, SEG, false>(B, A, zg, d.F3, d.p3, scale, T(0), &e);   // K_z X
         __syncthreads();
-        pass_ana<T, SEG>(A, B, zg, d.N3, d.p3);                  // A_z: F3 -> G3
+        pass_ana<T, SEG>(A, B, zg, d.N3, d.N3, d.p3);                  // A_z: F3 -> G3
         __syncthreads();
         T *t = A; A = B; B = t;                                   // result in A
     }
@@ -500,11 +568,11 @@ __device__ __forceinline__ void k3_item(const LrDev *__restrict__ lrs, const Orb
             load_plane_async(A, pitch, d.I2, d.I1, scratch + o.sQ + (size_t)kz * d.I2 * d.I1);
             cp_async_wait_all();
             __syncthreads();
-            if (d.p1) pass_mf<T, SEG, 1>(A, B, xpose_geom(d.I2, pitch, d.pitchT()), d.I1, d.F1);   // Mt_x into B^T
-            else pass_mf<T, SEG, 3>(A, B, xpose_geom(d.I2, pitch, d.pitchT()), d.I1, d.F1);
+            if (d.p1) pass_mf<T, SEG, 1, true>(A, B, xpose_geom(d.I2, pitch, d.pitchT()), d.I1, d.F1);   // Mt_x into B^T
+            else pass_mf<T, SEG, 3, true>(A, B, xpose_geom(d.I2, pitch, d.pitchT()), d.I1, d.F1);
             __syncthreads();
-            if (d.p2) pass_mf<T, SEG, 1>(B, A, xpose_geom(d.F1, d.pitchT(), pitch), d.I2, d.F2);   // Mt_y into A
-            else pass_mf<T, SEG, 3>(B, A, xpose_geom(d.F1, d.pitchT(), pitch), d.I2, d.F2);
+            if (d.p2) pass_mf<T, SEG, 1, true>(B, A, xpose_geom(d.F1, d.pitchT(), pitch), d.I2, d.F2);   // Mt_y into A
+            else pass_mf<T, SEG, 3, true>(B, A, xpose_geom(d.F1, d.pitchT(), pitch), d.I2, d.F2);
             __syncthreads();
         }
         {
@@ -515,18 +583,46 @@ __device__ __forceinline__ void k3_item(const LrDev *__restrict__ lrs, const Orb
                 // P -> B asynchronously while Z2 is added into A, 4 loads in flight
                 load_plane_async(B, pitch, d.F2, d.F1, p);
                 constexpr int U = 4;
-                RowCol q(d.F1);
-                for (int i0 = threadIdx.x; i0 < nf; i0 += U * blockDim.x) {
-                    T v[U];
+                if (pair_rows(d.F1, z2)) {
+                    // point pairs: pair i = (row q.r, column 2 q.c) of the dense Z2 plane
+                    using V = typename Pair<T>::type;
+                    const int npair = nf >> 1;
+                    RowCol q(d.F1 >> 1);
+                    for (int i0 = threadIdx.x; i0 < npair; i0 += U * blockDim.x) {
+                        V v[U];
 #pragma unroll
-                    for (int u = 0; u < U; ++u) {
-                        const int i = i0 + u * blockDim.x;
-                        v[u] = i < nf ? z2[i] : T(0);
+                        for (int u = 0; u < U; ++u) {
+                            const int i = i0 + u * blockDim.x;
+                            v[u].x = T(0);
+                            v[u].y = T(0);
+                            if (i < npair) v[u] = *reinterpret_cast<const V *>(z2 + 2 * i);
+                        }
+#pragma unroll
+                        for (int u = 0; u < U; ++u) {
+                            if (i0 + u * (int)blockDim.x < npair) {
+                                V *a = reinterpret_cast<V *>(A + q.r * pitch + 2 * q.c);
+                                V w = *a;
+                                w.x += v[u].x;
+                                w.y += v[u].y;
+                                *a = w;
+                            }
+                            q.next();
+                        }
                     }
+                } else {
+                    RowCol q(d.F1);
+                    for (int i0 = threadIdx.x; i0 < nf; i0 += U * blockDim.x) {
+                        T v[U];
 #pragma unroll
-                    for (int u = 0; u < U; ++u) {
-                        if (i0 + u * (int)blockDim.x < nf) A[q.r * pitch + q.c] += v[u];
-                        q.next();
+                        for (int u = 0; u < U; ++u) {
+                            const int i = i0 + u * blockDim.x;
+                            v[u] = i < nf ? z2[i] : T(0);
+                        }
+#pragma unroll
+                        for (int u = 0; u < U; ++u) {
+                            if (i0 + u * (int)blockDim.x < nf) A[q.r * pitch + q.c] += v[u];
+                            q.next();
+                        }
                     }
                 }
                 cp_async_wait_all();
@@ -536,10 +632,22 @@ __device__ __forceinline__ void k3_item(const LrDev *__restrict__ lrs, const Orb
                 load_plane_async(A, pitch, d.F2, d.F1, z2);
                 cp_async_wait_all();
                 __syncthreads();
-                RowCol q(d.F1);
-                for (int i = threadIdx.x; i < nf; i += blockDim.x, q.next()) {
-                    const int e = q.r * pitch + q.c;
-                    A[e] = fma(cshift, B[e], A[e]);
+                if (!(d.F1 & 1)) {
+                    using V = typename Pair<T>::type;
+                    for_row_pairs(d.F2, d.F1, [&](int r, int c) {
+                        V *a = reinterpret_cast<V *>(A + r * pitch + c);
+                        const V b = *reinterpret_cast<const V *>(B + r * pitch + c);
+                        V w = *a;
+                        w.x = fma(cshift, b.x, w.x);
+                        w.y = fma(cshift, b.y, w.y);
+                        *a = w;
+                    });
+                } else {
+                    RowCol q(d.F1);
+                    for (int i = threadIdx.x; i < nf; i += blockDim.x, q.next()) {
+                        const int e = q.r * pitch + q.c;
+                        A[e] = fma(cshift, B[e], A[e]);
+                    }
                 }
             } else {
                 RowCol q(d.F1);
@@ -556,13 +664,13 @@ __device__ __forceinline__ void k3_item(const LrDev *__restrict__ lrs, const Orb
         double e = 0.0;
         const double sx = -0.5 / ((0.5 * L.hgrid[0]) * (0.5 * L.hgrid[0]));
         const double sy = -0.5 / ((0.5 * L.hgrid[1]) * (0.5 * L.hgrid[1]));
-        pass_kin<T, SEG, true>(B, A, rows_geom(d.F2, pitch), d.F1, d.p1, sx, T(0), &e);   // += K_x P
+        pass_kin<T, SEG, true, true>(B, A, rows_geom(d.F2, pitch), d.F1, d.p1, sx, T(0), &e);   // += K_x P
         __syncthreads();
         pass_kin<T, SEG, true>(B, A, cols_geom(d.F1, pitch), d.F2, d.p2, sy, T(0), &e);   // += K_y P
         __syncthreads();
-        pass_ana<T, SEG>(A, B, xpose_geom(d.F2, pitch, d.pitchT()), d.N1, d.p1);   // A_x: F1 -> G1, into B^T
+        pass_ana<T, SEG, true>(A, B, xpose_geom(d.F2, pitch, d.pitchT()), d.N1, d.H1, d.p1);   // A_x: F1 -> G1, into B^T
         __syncthreads();
-        pass_ana<T, SEG>(B, A, xpose_geom(d.G1, d.pitchT(), pitch), d.N2, d.p2);   // A_y: F2 -> G2, into A
+        pass_ana<T, SEG, true>(B, A, xpose_geom(d.G1, d.pitchT(), pitch), d.N2, d.H2, d.p2);   // A_y: F2 -> G2, into A
         __syncthreads();
         scatter_plane<T, TO>(A, pitch, L, kz, out_ptr(o, hpsi), accumulate != 0,
                              MODE == MODE_PRECOND ? sc : nullptr);
@@ -669,7 +777,7 @@ __global__ void __launch_bounds__(kZThreads) kd_density(const LrDev *__restrict_
             cp_async_elem(A + z * TC + col, inside ? g + (size_t)z * plane + colofs : g, inside);
         cp_async_wait_all();
         __syncthreads();
-        pass_syn<T, SEG>(A, B, zg, d.N3, d.p3);                  // S_z
+        pass_syn<T, SEG>(A, B, zg, d.N3, d.N3, d.p3);                  // S_z
         __syncthreads();
         if (d.p3) pass_mf<T, SEG, 0>(B, A, zg, d.F3, d.I3);       // M_z
         else pass_mf<T, SEG, 2>(B, A, zg, d.F3, d.I3);

@@ -158,12 +158,15 @@ extern "C" int wvlh_locham_noalloc(int precision, const int n[3], const int peri
         set_last_error(WVLH_ERR_TOO_LARGE);
         return WVLH_ERR_TOO_LARGE;
     }
-    const size_t pitch = (size_t)((G[0] > F[0] ? (G[0] > I[0] ? G[0] : I[0]) : (F[0] > I[0] ? F[0] : I[0])) | 1);
-    const size_t rows = (size_t)(G[1] > F[1] ? (G[1] > I[1] ? G[1] : I[1]) : (F[1] > I[1] ? F[1] : I[1]));
+    // plane buffers as the fused kernels lay them out (coarse_width, vec_pitch)
+    const int W1 = coarse_width(N[0]), W2 = coarse_width(N[1]);
+    const size_t rowsT = (size_t)(W1 > F[0] ? (W1 > I[0] ? W1 : I[0]) : (F[0] > I[0] ? F[0] : I[0]));
+    const size_t pitch = (size_t)vec_pitch((int)rowsT);
+    const size_t rows = (size_t)(W2 > F[1] ? (W2 > I[1] ? W2 : I[1]) : (F[1] > I[1] ? F[1] : I[1]));
     const size_t zl = (size_t)(G[2] > F[2] ? (G[2] > I[2] ? G[2] : I[2]) : (F[2] > I[2] ? F[2] : I[2]));
     // second plane buffer: a plane or a transposed plane (rowsT lines of pitchT points)
-    const size_t rowsT = (size_t)(G[0] > F[0] ? (G[0] > I[0] ? G[0] : I[0]) : (F[0] > I[0] ? F[0] : I[0]));
-    const size_t planeB = rows * pitch > rowsT * (rows | 1) ? rows * pitch : rowsT * (rows | 1);
+    const size_t pitchT = (size_t)vec_pitch((int)rows);
+    const size_t planeB = rows * pitch > rowsT * pitchT ? rows * pitch : rowsT * pitchT;
     int dev = 0, smax = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) {
         set_last_error(WVLH_ERR_CUDA);

@@ -49,8 +49,8 @@ __global__ void __launch_bounds__(256) k_pass1d(int n, int ndat, int per, double
     __syncthreads();
     const LineGeom g{JT, 1, JT + 1, Lp, 1};
     double e = 0.0;
-    if (KIND == P_SYN) pass_syn<double, 4>(S, D, g, n, per);
-    else if (KIND == P_ANA) pass_ana<double, 4>(S, D, g, n, per);
+    if (KIND == P_SYN) pass_syn<double, 4>(S, D, g, n, n, per);
+    else if (KIND == P_ANA) pass_ana<double, 4>(S, D, g, n, n, per);
     else if (KIND == P_MF) pass_mf<double, 4, 0>(S, D, g, Lin, Lout);
     else if (KIND == P_MFT) pass_mf<double, 4, 1>(S, D, g, Lin, Lout);
     else if (KIND == P_MFG) pass_mf<double, 4, 2>(S, D, g, Lin, Lout);
