@@ -387,21 +387,24 @@ static void layout(wvlh_batch *b, const std::vector<int> &orb_lr, const std::vec
         pre2.push_back(pre2.back() + ntx0 * nty0);
         pre2p.push_back(pre2p.back() + ntx1 * nty1);
         stride = std::max(stride, std::max(ntx0 * nty0, ntx1 * nty1 + G3));
-        // plane buffer A: rows (y) x pitch (x); B also holds transposed planes:
-        // rowsT (x) x pitchT (y).  Coarse lines are stored with the wavelet
-        // half at an even offset (coarse_width), pitches are vec_pitch.
+        // plane buffer A: rows (y) x pitch (x); B holds P (F2 rows x pitch)
+        // or a transposed plane (lines along x, each at the vec_pitch of its
+        // y length).  Coarse lines are stored with the wavelet half at an
+        // even offset (coarse_width).
         const int W1 = coarse_width(N1), W2 = coarse_width(N2);
         const int pitch = vec_pitch(std::max(W1, std::max(F1, I1)));
         const int rows = std::max(W2, std::max(F2, I2));
-        const int rowsT = std::max(W1, std::max(F1, I1)), pitchT = vec_pitch(rows);
+        const long long bT = std::max(std::max((long long)F1 * vec_pitch(W2), (long long)I1 * vec_pitch(F2)),
+                                      std::max((long long)F1 * vec_pitch(I2), (long long)W1 * vec_pitch(F2)));
+        const long long bsz = std::max((long long)F2 * pitch, bT);
         planeA = std::max(planeA, (size_t)rows * pitch);
         {
-            const long long len = std::max(G1, std::max(F1, I1)), w = (long long)G3 * rows * pitch;
-            const long long ab = (long long)rows * pitch + std::max((long long)rows * pitch, (long long)rowsT * pitchT);
+            const long long len = std::max(W1, std::max(F1, I1)), w = (long long)G3 * rows * pitch;
+            const long long ab = (long long)rows * pitch + bsz;
             shapes32.push_back(PlaneShape{rows, len, ab * 4, w});
             shapes64.push_back(PlaneShape{rows, len, ab * 8, w});
         }
-        planeB = std::max(planeB, std::max((size_t)rows * pitch, (size_t)rowsT * pitchT));
+        planeB = std::max(planeB, (size_t)bsz);
         const int zl = std::max(G3, std::max(F3, I3));
         sm2_elems = std::max(sm2_elems, (size_t)2 * zl * TX_ * TY_);
     }

@@ -111,10 +111,12 @@ __device__ __forceinline__ void load_window(T (&x)[W], const T *in, int ps, int 
 
 // Window load for a unit-stride line that starts on a point pair, q0 even:
 // x[k] = line(q0 + SHIFT + k).  The window is read as W/2 + 1 point pairs from
-// the pair boundary below q0 + SHIFT (never past the pair holding the line's
-// last point, so reads stay inside the row); periodic wrap and zero padding
-// then act on whole pairs when L is even.  Odd L (free-BC ISF lines) takes the
-// scalar path at the line ends.
+// the pair boundary below q0 + SHIFT, never past the pair holding the line's
+// last point: the rows hold at least L + 1 points when L is odd, so reads stay
+// inside the row.  Zero padding (free lines) masks whole pairs and the point
+// after an odd line's end; periodic wrap moves whole pairs when L is even.
+// Periodic lines of odd length (coarse lines of an odd box) take the scalar
+// path at the line ends.
 template <class T, int W, int SHIFT>
 __device__ __forceinline__ void load_window_u(T (&x)[W], const T *in, int q0, int L, int per)
 {
@@ -132,18 +134,21 @@ __device__ __forceinline__ void load_window_u(T (&x)[W], const T *in, int q0, in
             y[2 * c] = v.x;
             y[2 * c + 1] = v.y;
         }
-    } else if (!(L & 1)) {
+    } else if (!per) {
 #pragma unroll
         for (int c = 0; c < NV; ++c) {
             const int p = a + 2 * c;
             V v;
-            if (per) {
-                v = *reinterpret_cast<const V *>(in + wrap_near(p, L));
-            } else {
-                v.x = T(0);
-                v.y = T(0);
-                if ((unsigned)p < (unsigned)L) v = *reinterpret_cast<const V *>(in + p);
-            }
+            v.x = T(0);
+            v.y = T(0);
+            if ((unsigned)p < (unsigned)L) v = *reinterpret_cast<const V *>(in + p);
+            y[2 * c] = v.x;
+            y[2 * c + 1] = p + 1 < L ? v.y : T(0);
+        }
+    } else if (!(L & 1)) {
+#pragma unroll
+        for (int c = 0; c < NV; ++c) {
+            const V v = *reinterpret_cast<const V *>(in + wrap_near(a + 2 * c, L));
             y[2 * c] = v.x;
             y[2 * c + 1] = v.y;
         }
@@ -393,8 +398,11 @@ __device__ __forceinline__ void pass_kin(const T *src, T *dst, const LineGeom g,
             if (FULL || q < L) {
                 es = fma(x[t + 14], conv, es);
                 if constexpr (sizeof(T) == 4) el = fma(x[t + 14], lo, el);
-                if constexpr (UNIT && FULL) {
-                    // full unit-stride segment: store each point pair once both are formed
+            }
+            // unit-stride rows store each point pair once both are formed (a
+            // clipped segment of an even line ends on a whole pair)
+            if (UNIT && (FULL || !(L & 1))) {
+                if (FULL || q < L) {
                     if (t & 1) {
                         using V = typename Pair<T>::type;
                         V *o = reinterpret_cast<V *>(out + q - 1);
@@ -410,10 +418,10 @@ __device__ __forceinline__ void pass_kin(const T *src, T *dst, const LineGeom g,
                     } else {
                         prev = conv;
                     }
-                } else {
-                    const T base = ACC ? out[q * g.dst_ps] : cshift * x[t + 14];
-                    out[q * g.dst_ps] = fma(scale, conv, base);
                 }
+            } else if (FULL || q < L) {
+                const T base = ACC ? out[q * g.dst_ps] : cshift * x[t + 14];
+                out[q * g.dst_ps] = fma(scale, conv, base);
             }
         }
         e += ((double)es + (double)el) * scale_d;

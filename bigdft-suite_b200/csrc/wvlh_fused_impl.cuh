@@ -63,11 +63,13 @@ struct Dims {
         F1 = fine_len(N1, p1); F2 = fine_len(N2, p2); F3 = fine_len(N3, p3);
         I1 = isf_len(N1, p1); I2 = isf_len(N2, p2); I3 = isf_len(N3, p3);
     }
-    // plane buffer A: rows() lines (y) of pitch() points (x); the second buffer
-    // B also holds transposed planes: rowsT() lines (x) of pitchT() points (y)
+    // plane buffer A: rows() lines (y) of pitch() points (x).  The second
+    // buffer B holds P (F2 rows of pitch()) or a transposed plane: the lines
+    // along x of a pass, each of the y length `len` of its plane, at pitch
+    // pitchT(len) — sized per pass, so B is no larger than its largest use.
     __device__ __forceinline__ int pitch() const { return vec_pitch(max(G1, max(F1, I1))); }
     __device__ __forceinline__ int rows() const { return max(G2, max(F2, I2)); }
-    __device__ __forceinline__ int pitchT() const { return vec_pitch(rows()); }
+    __device__ __forceinline__ static int pitchT(int len) { return vec_pitch(len); }
 };
 
 __device__ __forceinline__ LineGeom rows_geom(int nrows, int pitch)
@@ -400,18 +402,18 @@ __device__ __forceinline__ void k1_item(const LrDev *__restrict__ lrs, const Orb
             gather_plane<T, TI>(A, pitch, L, kz, in_ptr(o, psi), MODE == MODE_PRECOND ? sc : nullptr);
         }
         __syncthreads();
-        const int pt = d.pitchT();
+        const int pt = d.pitchT(d.G2), ptf = d.pitchT(d.F2);
         pass_syn<T, SEG, true>(A, B, xpose_geom(d.G2, pitch, pt), d.N1, d.H1, d.p1);   // S_x: G2 rows, G1 -> F1, into B^T
         __syncthreads();
         pass_syn<T, SEG, true>(B, A, xpose_geom(d.F1, pt, pitch), d.N2, d.H2, d.p2);   // S_y: F1 lines, G2 -> F2, into A
         __syncthreads();
         if (MODE != MODE_LOCDEN) store_plane(A, pitch, d.F2, d.F1, scratch + o.sP + (size_t)kz * d.F2 * d.F1);
         if (MODE == MODE_PRECOND) return;
-        if (d.p1) pass_mf<T, SEG, 0, true>(A, B, xpose_geom(d.F2, pitch, pt), d.F1, d.I1);   // M_x into B^T
-        else pass_mf<T, SEG, 2, true>(A, B, xpose_geom(d.F2, pitch, pt), d.F1, d.I1);
+        if (d.p1) pass_mf<T, SEG, 0, true>(A, B, xpose_geom(d.F2, pitch, ptf), d.F1, d.I1);   // M_x into B^T
+        else pass_mf<T, SEG, 2, true>(A, B, xpose_geom(d.F2, pitch, ptf), d.F1, d.I1);
         __syncthreads();
-        if (d.p2) pass_mf<T, SEG, 0, true>(B, A, xpose_geom(d.I1, pt, pitch), d.F2, d.I2);   // M_y into A
-        else pass_mf<T, SEG, 2, true>(B, A, xpose_geom(d.I1, pt, pitch), d.F2, d.I2);
+        if (d.p2) pass_mf<T, SEG, 0, true>(B, A, xpose_geom(d.I1, ptf, pitch), d.F2, d.I2);   // M_y into A
+        else pass_mf<T, SEG, 2, true>(B, A, xpose_geom(d.I1, ptf, pitch), d.F2, d.I2);
         __syncthreads();
         store_plane(A, pitch, d.I2, d.I1, scratch + o.sQ + (size_t)kz * d.I2 * d.I1);
     }
@@ -568,11 +570,11 @@ __device__ __forceinline__ void k3_item(const LrDev *__restrict__ lrs, const Orb
             load_plane_async(A, pitch, d.I2, d.I1, scratch + o.sQ + (size_t)kz * d.I2 * d.I1);
             cp_async_wait_all();
             __syncthreads();
-            if (d.p1) pass_mf<T, SEG, 1, true>(A, B, xpose_geom(d.I2, pitch, d.pitchT()), d.I1, d.F1);   // Mt_x into B^T
-            else pass_mf<T, SEG, 3, true>(A, B, xpose_geom(d.I2, pitch, d.pitchT()), d.I1, d.F1);
+            if (d.p1) pass_mf<T, SEG, 1, true>(A, B, xpose_geom(d.I2, pitch, d.pitchT(d.I2)), d.I1, d.F1);   // Mt_x into B^T
+            else pass_mf<T, SEG, 3, true>(A, B, xpose_geom(d.I2, pitch, d.pitchT(d.I2)), d.I1, d.F1);
             __syncthreads();
-            if (d.p2) pass_mf<T, SEG, 1, true>(B, A, xpose_geom(d.F1, d.pitchT(), pitch), d.I2, d.F2);   // Mt_y into A
-            else pass_mf<T, SEG, 3, true>(B, A, xpose_geom(d.F1, d.pitchT(), pitch), d.I2, d.F2);
+            if (d.p2) pass_mf<T, SEG, 1, true>(B, A, xpose_geom(d.F1, d.pitchT(d.I2), pitch), d.I2, d.F2);   // Mt_y into A
+            else pass_mf<T, SEG, 3, true>(B, A, xpose_geom(d.F1, d.pitchT(d.I2), pitch), d.I2, d.F2);
             __syncthreads();
         }
         {
@@ -668,9 +670,9 @@ __device__ __forceinline__ void k3_item(const LrDev *__restrict__ lrs, const Orb
         __syncthreads();
         pass_kin<T, SEG, true>(B, A, cols_geom(d.F1, pitch), d.F2, d.p2, sy, T(0), &e);   // += K_y P
         __syncthreads();
-        pass_ana<T, SEG, true>(A, B, xpose_geom(d.F2, pitch, d.pitchT()), d.N1, d.H1, d.p1);   // A_x: F1 -> G1, into B^T
+        pass_ana<T, SEG, true>(A, B, xpose_geom(d.F2, pitch, d.pitchT(d.F2)), d.N1, d.H1, d.p1);   // A_x: F1 -> G1, into B^T
         __syncthreads();
-        pass_ana<T, SEG, true>(B, A, xpose_geom(d.G1, d.pitchT(), pitch), d.N2, d.H2, d.p2);   // A_y: F2 -> G2, into A
+        pass_ana<T, SEG, true>(B, A, xpose_geom(d.G1, d.pitchT(d.F2), pitch), d.N2, d.H2, d.p2);   // A_y: F2 -> G2, into A
         __syncthreads();
         scatter_plane<T, TO>(A, pitch, L, kz, out_ptr(o, hpsi), accumulate != 0,
                              MODE == MODE_PRECOND ? sc : nullptr);

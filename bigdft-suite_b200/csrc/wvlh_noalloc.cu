@@ -160,13 +160,16 @@ extern "C" int wvlh_locham_noalloc(int precision, const int n[3], const int peri
     }
     // plane buffers as the fused kernels lay them out (coarse_width, vec_pitch)
     const int W1 = coarse_width(N[0]), W2 = coarse_width(N[1]);
-    const size_t rowsT = (size_t)(W1 > F[0] ? (W1 > I[0] ? W1 : I[0]) : (F[0] > I[0] ? F[0] : I[0]));
-    const size_t pitch = (size_t)vec_pitch((int)rowsT);
+    const size_t width = (size_t)(W1 > F[0] ? (W1 > I[0] ? W1 : I[0]) : (F[0] > I[0] ? F[0] : I[0]));
+    const size_t pitch = (size_t)vec_pitch((int)width);
     const size_t rows = (size_t)(W2 > F[1] ? (W2 > I[1] ? W2 : I[1]) : (F[1] > I[1] ? F[1] : I[1]));
     const size_t zl = (size_t)(G[2] > F[2] ? (G[2] > I[2] ? G[2] : I[2]) : (F[2] > I[2] ? F[2] : I[2]));
-    // second plane buffer: a plane or a transposed plane (rowsT lines of pitchT points)
-    const size_t pitchT = (size_t)vec_pitch((int)rows);
-    const size_t planeB = rows * pitch > rowsT * pitchT ? rows * pitch : rowsT * pitchT;
+    // second plane buffer: P (F2 rows x pitch) or a transposed plane, each
+    // pass's lines along x at the vec_pitch of its y length
+    size_t planeB = (size_t)F[1] * pitch;
+    const size_t uses[4] = {(size_t)F[0] * vec_pitch(W2), (size_t)I[0] * vec_pitch(F[1]),
+                            (size_t)F[0] * vec_pitch(I[1]), (size_t)W1 * vec_pitch(F[1])};
+    for (size_t u : uses) planeB = u > planeB ? u : planeB;
     int dev = 0, smax = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) {
         set_last_error(WVLH_ERR_CUDA);
@@ -265,7 +268,7 @@ extern "C" int wvlh_locham_noalloc(int precision, const int n[3], const int peri
     p.part_stride = stride;
     p.plane_elems = (long long)(rows * pitch);
     {
-        const long long len = (long long)rowsT, ab = (long long)(rows * pitch + planeB);
+        const long long len = (long long)width, ab = (long long)(rows * pitch + planeB);
         p.plane_threads[0] = choose_plane_threads({PlaneShape{(long long)rows, len, ab * 4, 1}}, true);
         p.plane_threads[1] = choose_plane_threads({PlaneShape{(long long)rows, len, ab * 8, 1}}, false);
     }
