@@ -70,10 +70,11 @@ struct wvlh_ctx {
     DevBuf arena;
     unsigned long long arena_gen = 0;
     DevBuf wp_runs;  // compressed scalar products: one run per b segment
-    // host-buffer path: a second stream and the buffers of its in-flight chunk
-    cudaStream_t aux = nullptr;
-    cudaEvent_t ev_a = nullptr, ev_b = nullptr;
-    DevBuf scratch2, part_pot2, part_kin2;
+    // host-buffer path: an upload stream and a download stream around the
+    // context's stream, with per-chunk events (uploaded, computed)
+    cudaStream_t aux = nullptr, aux2 = nullptr;
+    cudaEvent_t ev_a = nullptr;
+    std::vector<cudaEvent_t> ev_in, ev_cmp;
 };
 
 // One localisation region: its box and its keys, validated once and kept on
@@ -158,18 +159,19 @@ extern "C" int wvlh_ctx_destroy(wvlh_ctx *ctx)
     cudaStreamSynchronize(ctx->stream);
     for (DevBuf *b : {&ctx->scratch, &ctx->part_pot, &ctx->part_kin, &ctx->io_psi, &ctx->io_pot, &ctx->io_hpsi,
                       &ctx->io_e, &ctx->dotpart, &ctx->cg_r, &ctx->cg_d, &ctx->cg_ad, &ctx->cg_scal, &ctx->den_part,
-                      &ctx->ov_work, &ctx->arena, &ctx->wp_runs, &ctx->scratch2, &ctx->part_pot2,
-                      &ctx->part_kin2})
+                      &ctx->ov_work, &ctx->arena, &ctx->wp_runs})
         b->release();
     for (auto &b : ctx->plain) b.release();
     for (auto &e : ctx->ev)
         if (e) cudaEventDestroy(e);
     if (ctx->ev_a) cudaEventDestroy(ctx->ev_a);
-    if (ctx->ev_b) cudaEventDestroy(ctx->ev_b);
-    if (ctx->aux) {
-        cudaStreamSynchronize(ctx->aux);
-        cudaStreamDestroy(ctx->aux);
-    }
+    for (cudaEvent_t e : ctx->ev_in) cudaEventDestroy(e);
+    for (cudaEvent_t e : ctx->ev_cmp) cudaEventDestroy(e);
+    for (cudaStream_t st : {ctx->aux, ctx->aux2})
+        if (st) {
+            cudaStreamSynchronize(st);
+            cudaStreamDestroy(st);
+        }
     delete ctx;
     return WVLH_OK;
 }
@@ -825,10 +827,10 @@ extern "C" int wvlh_locham_batched_host(wvlh_batch *b, int precision, const void
     if ((rc = c->io_psi.ensure(npsi)) || (rc = c->io_hpsi.ensure(npsi)) || (rc = c->io_pot.ensure(npot)) ||
         (rc = c->io_e.ensure(2 * ne)))
         return fail(rc);
-    // chunks of about norb / 16 orbitals (one chunk for small batches): the first
-    // upload and the last download are the parts that nothing overlaps
+    // chunks of at least 8 orbitals, up to 32 (one chunk for small batches): the
+    // first upload and the last download are the parts that nothing overlaps
     if (b->chunks.empty()) {
-        const int nch = p.norb >= 8 ? std::min(p.norb, 16) : 1;
+        const int nch = p.norb >= 16 ? std::min(32, p.norb / 8) : 1;
         const int per = (p.norb + nch - 1) / nch;
         for (int o0 = 0; o0 < p.norb; o0 += per) {
             wvlh_batch *q = nullptr;
@@ -842,49 +844,66 @@ extern "C" int wvlh_locham_batched_host(wvlh_batch *b, int precision, const void
             b->chunk_o0.push_back(o0);
         }
     }
+    const size_t nch = b->chunks.size();
     if (!c->aux) CK(cudaStreamCreateWithFlags(&c->aux, cudaStreamNonBlocking));
+    if (!c->aux2) CK(cudaStreamCreateWithFlags(&c->aux2, cudaStreamNonBlocking));
     if (!c->ev_a) CK(cudaEventCreateWithFlags(&c->ev_a, cudaEventDisableTiming));
-    if (!c->ev_b) CK(cudaEventCreateWithFlags(&c->ev_b, cudaEventDisableTiming));
-    DevBuf *scr[2] = {&c->scratch, &c->scratch2}, *pp[2] = {&c->part_pot, &c->part_pot2},
-           *pk[2] = {&c->part_kin, &c->part_kin2};
-    for (size_t k = 0; k < b->chunks.size(); ++k) {
+    while (c->ev_in.size() < nch) {
+        cudaEvent_t e1, e2;
+        CK(cudaEventCreateWithFlags(&e1, cudaEventDisableTiming));
+        c->ev_in.push_back(e1);
+        CK(cudaEventCreateWithFlags(&e2, cudaEventDisableTiming));
+        c->ev_cmp.push_back(e2);
+    }
+    // the chunks run one after another on the context's stream and share its scratch
+    for (size_t k = 0; k < nch; ++k) {
         const Plan &q = b->chunks[k]->plan;
-        const int s = (int)(k & 1);
-        if ((rc = scr[s]->ensure((q.scratch_elems + plane_tmp_elems(q, fp)) * es)) ||
-            (rc = pp[s]->ensure(sizeof(double) * (size_t)q.norb * q.part_stride)) ||
-            (rc = pk[s]->ensure(sizeof(double) * (size_t)q.norb * q.part_stride)))
+        if ((rc = c->scratch.ensure((q.scratch_elems + plane_tmp_elems(q, fp)) * es)) ||
+            (rc = c->part_pot.ensure(sizeof(double) * (size_t)q.norb * q.part_stride)) ||
+            (rc = c->part_kin.ensure(sizeof(double) * (size_t)q.norb * q.part_stride)))
             return fail(rc);
     }
-    cudaStream_t st[2] = {c->stream, c->aux};
+    // three queues: uploads (aux) back to back, the chunk computations (the
+    // context's stream) as their inputs arrive, downloads (aux2) as each chunk
+    // is computed; both copy directions stay busy for the whole call
+    cudaStream_t cs = c->stream, up = c->aux, down = c->aux2;
     unsigned char *dpsi = (unsigned char *)c->io_psi.p, *dh = (unsigned char *)c->io_hpsi.p;
     double *de = (double *)c->io_e.p;
-    // the potential first; the second stream starts after it (and after earlier work)
-    CK(cudaMemcpyAsync(c->io_pot.p, pot, npot, cudaMemcpyHostToDevice, st[0]));
-    CK(cudaEventRecord(c->ev_a, st[0]));
-    CK(cudaStreamWaitEvent(st[1], c->ev_a, 0));
-    for (size_t k = 0; k < b->chunks.size(); ++k) {
+    CK(cudaEventRecord(c->ev_a, cs));   // after earlier work on the context's stream
+    CK(cudaStreamWaitEvent(up, c->ev_a, 0));
+    CK(cudaStreamWaitEvent(down, c->ev_a, 0));
+    CK(cudaMemcpyAsync(c->io_pot.p, pot, npot, cudaMemcpyHostToDevice, up));
+    for (size_t k = 0; k < nch; ++k) {
+        const size_t off = (size_t)p.orb_psi[b->chunk_o0[k]] * es, n = (size_t)b->chunks[k]->plan.psi_total * es;
+        CK(cudaMemcpyAsync(dpsi + off, (const unsigned char *)psi + off, n, cudaMemcpyHostToDevice, up));
+        CK(cudaEventRecord(c->ev_in[k], up));
+    }
+    for (size_t k = 0; k < nch; ++k) {
         const Plan &q = b->chunks[k]->plan;
-        const int s = (int)(k & 1);
         const int o0 = b->chunk_o0[k];
-        const size_t off = (size_t)p.orb_psi[o0] * es, n = (size_t)q.psi_total * es;
-        CK(cudaMemcpyAsync(dpsi + off, (const unsigned char *)psi + off, n, cudaMemcpyHostToDevice, st[s]));
+        const size_t off = (size_t)p.orb_psi[o0] * es;
+        CK(cudaStreamWaitEvent(cs, c->ev_in[k], 0));
         cudaError_t e;
         if (fp)
             e = launch_locham<double, double>(q, (const double *)(dpsi + off), (const double *)c->io_pot.p,
-                                              (double *)(dh + off), (double *)scr[s]->p, (double *)pp[s]->p,
-                                              (double *)pk[s]->p, de + o0, de + p.norb + o0, 0, st[s], nullptr);
+                                              (double *)(dh + off), (double *)c->scratch.p, (double *)c->part_pot.p,
+                                              (double *)c->part_kin.p, de + o0, de + p.norb + o0, 0, cs, nullptr);
         else
             e = launch_locham<float, float>(q, (const float *)(dpsi + off), (const float *)c->io_pot.p,
-                                            (float *)(dh + off), (float *)scr[s]->p, (double *)pp[s]->p,
-                                            (double *)pk[s]->p, de + o0, de + p.norb + o0, 0, st[s], nullptr);
+                                            (float *)(dh + off), (float *)c->scratch.p, (double *)c->part_pot.p,
+                                            (double *)c->part_kin.p, de + o0, de + p.norb + o0, 0, cs, nullptr);
         CK(e);
-        CK(cudaMemcpyAsync((unsigned char *)hpsi + off, dh + off, n, cudaMemcpyDeviceToHost, st[s]));
+        CK(cudaEventRecord(c->ev_cmp[k], cs));
     }
-    CK(cudaEventRecord(c->ev_b, st[1]));
-    CK(cudaStreamWaitEvent(st[0], c->ev_b, 0));
-    if (ekin) CK(cudaMemcpyAsync(ekin, de, ne, cudaMemcpyDeviceToHost, st[0]));
-    if (epot) CK(cudaMemcpyAsync(epot, de + p.norb, ne, cudaMemcpyDeviceToHost, st[0]));
-    CK(cudaStreamSynchronize(st[0]));
+    for (size_t k = 0; k < nch; ++k) {
+        const size_t off = (size_t)p.orb_psi[b->chunk_o0[k]] * es, n = (size_t)b->chunks[k]->plan.psi_total * es;
+        CK(cudaStreamWaitEvent(down, c->ev_cmp[k], 0));
+        CK(cudaMemcpyAsync((unsigned char *)hpsi + off, dh + off, n, cudaMemcpyDeviceToHost, down));
+    }
+    if (ekin) CK(cudaMemcpyAsync(ekin, de, ne, cudaMemcpyDeviceToHost, down));
+    if (epot) CK(cudaMemcpyAsync(epot, de + p.norb, ne, cudaMemcpyDeviceToHost, down));
+    // the download queue waited for every computation, which waited for every upload
+    CK(cudaStreamSynchronize(down));
     return WVLH_OK;
 }
 

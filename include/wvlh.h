@@ -285,9 +285,12 @@ int wvlh_batch_create_orbitals(wvlh_ctx *ctx, int norb, const wvlh_orbital *orbs
 int wvlh_locham_batched(wvlh_batch *batch, int precision, const void *psi, const void *pot, void *hpsi,
                         double *ekin, double *epot, int accumulate);
 /* same with HOST buffers (pinned for full speed): copies in, computes, copies
- * out, synchronises.  Batches of 8 orbitals or more go through in chunks of
- * consecutive orbitals alternating between the context's stream and a second
- * stream of the context, so that uploads, kernels and downloads overlap. */
+ * out, synchronises.  Batches of 16 orbitals or more go through in chunks of
+ * consecutive orbitals (8 or more each, up to 32 chunks): all uploads queue
+ * back to back on one stream of the context, each chunk's kernels run on the
+ * context's stream once its input has arrived, and each chunk's download
+ * queues on a third stream once it is computed, so both copy directions and
+ * the kernels overlap. */
 int wvlh_locham_batched_host(wvlh_batch *batch, int precision, const void *psi, const void *pot, void *hpsi,
                              double *ekin, double *epot);
 /* Density of all orbitals: rho[pot_offset[o] + r] += hfac[o] * |psi_o(r)|^2 on
