@@ -302,10 +302,12 @@ def leg_overlap(torch, ctx, psi64, norb):
             "max_abs_vs_cublas": (S - ref).abs().max().item(), "flops_count": "norb(norb+1)K (SYRK)"}
 
 
-def leg_serve(torch, dev, precision, nreq=300, load=0.7):
+def leg_serve(torch, dev, precision, nreq=300, loads=(0.3, 0.5, 0.7)):
     """Serving loop: 64 clients (coarse 16..64 per dim, periodic or free, 4..128
     orbitals), requests 50/50 Hpsi and density; capacity from a burst of one
-    request of each kind per client, then Poisson arrivals at load x capacity."""
+    request of each kind per client, then Poisson arrivals swept over loads x
+    capacity.  The headline p50/p99 are those of the highest load whose
+    served rate kept up with the offered rate (within 5 %)."""
     from wvlh import workloads as W
     from wvlh.serve import Server, latency_stats
     specs = W.serving_clients()
@@ -319,16 +321,24 @@ def leg_serve(torch, dev, precision, nreq=300, load=0.7):
         dt = time.perf_counter() - t
     cap = len(reqs) / dt
     cap_cells = sum(cells[r.client.id] for r in reqs) / dt
+    sweep = []
     n0, k0 = srv.launches, srv.kernel_launches
-    t = time.perf_counter()
-    reqs = srv.replay(W.poisson_arrivals(load * cap, nreq, len(cl), seed=11))
-    dt = time.perf_counter() - t
-    st = latency_stats(reqs)
+    for i, load in enumerate(loads):
+        t = time.perf_counter()
+        reqs = srv.replay(W.poisson_arrivals(load * cap, nreq, len(cl), seed=11 + i))
+        dt = time.perf_counter() - t
+        st = latency_stats(reqs)
+        sweep.append({"load": load, "offered_req_s": load * cap, "served_req_s": len(reqs) / dt,
+                      "served_cells_s": sum(cells[r.client.id] for r in reqs) / dt,
+                      "p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"], "mean_ms": st["mean_ms"]})
+    kept = [w for w in sweep if w["served_req_s"] >= 0.95 * w["offered_req_s"]]
+    head = kept[-1] if kept else sweep[0]
     out = {"clients": len(cl), "resident_gb": srv.resident / 1e9, "capacity_req_s": cap,
-           "capacity_cells_s": cap_cells, "offered_req_s": load * cap, "served_req_s": len(reqs) / dt,
-           "served_cells_s": sum(cells[r.client.id] for r in reqs) / dt,
-           "p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"], "mean_ms": st["mean_ms"],
-           "launches": srv.launches - n0, "kernel_launches": srv.kernel_launches - k0, "requests": len(reqs)}
+           "capacity_cells_s": cap_cells, "sustained_load": head["load"], "offered_req_s": head["offered_req_s"],
+           "served_req_s": head["served_req_s"], "served_cells_s": head["served_cells_s"],
+           "p50_ms": head["p50_ms"], "p99_ms": head["p99_ms"], "mean_ms": head["mean_ms"], "sweep": sweep,
+           "launches": srv.launches - n0, "kernel_launches": srv.kernel_launches - k0,
+           "requests": nreq * len(loads)}
     srv.close()
     del srv, cl
     torch.cuda.empty_cache()
