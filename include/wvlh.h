@@ -325,6 +325,32 @@ int wvlh_overlap(wvlh_ctx *ctx, int precision, int norb, int64_t K, int64_t ld, 
  * precision 32: float vectors, FP64 sums; 64: double.  Device pointers. */
 int wvlh_wpdot(wvlh_ctx *ctx, int precision, const wvlh_region *ra, int na, const void *a, int64_t lda,
                const wvlh_region *rb, int nb, const void *b, int64_t ldb, double *out);
+/* Nonlocal pseudopotential projectors (NonLocalHamiltonianApplication,
+ * hpsiortho.f90:1044-1125, through DFT_PSP_projectors_iter_apply,
+ * modules/psp_projectors.f90:585-712): for every orbital psi on the keys of
+ * psi_region and every atom a, with p_1..p_m the atom's m = nproj[a]
+ * projectors on the keys of proj_regions[a] (same box as psi_region) and h its
+ * m x m coefficient matrix,
+ *     c_i = <p_i|psi>  (pr_dot_psi, locregs/compression.f90:505),
+ *     hc  = h c        (apply_hij_coeff, orbitals/pseudopotentials.f90:1208),
+ *     eproj += c . hc  (cproj_dot, compression.f90:540),
+ *     hpsi += sum_i hc_i p_i on the common points (cproj_pr_p_psi, :562).
+ * The common points are the reference's masks between the wavefunction's and
+ * the projector's segments (count_wblas_segs / fill_wblas_segs,
+ * locregs/scalar_product.f90:1012-1187: each projector segment meets the first
+ * wavefunction segment it overlaps), coarse and 7 fine components.  Atoms are
+ * applied in order, each orbital's sums in a fixed order (deterministic).
+ * proj: DEVICE doubles, per atom its m vectors of wvlh_region_psi_size(
+ * proj_regions[a]) values one after another, atoms one after another; copied
+ * at creation.  hij: HOST doubles, per atom m x m row-major, atoms one after
+ * another; copied.  m <= 32 per atom.  Regions must outlive the object. */
+typedef struct wvlh_nlpsp wvlh_nlpsp;
+int wvlh_nlpsp_create(wvlh_ctx *ctx, const wvlh_region *psi_region, int natoms, const wvlh_region *const *proj_regions,
+                      const int *nproj, const double *proj, const double *hij, wvlh_nlpsp **nl);
+/* norb orbitals on psi_region (row stride ld >= its psi size), DEVICE FP64:
+ * hpsi += V_nl psi, eproj[o] = sum over atoms of c . hc (written). */
+int wvlh_nlpsp_apply(wvlh_nlpsp *nl, int norb, const double *psi, int64_t ld, double *hpsi, double *eproj);
+int wvlh_nlpsp_destroy(wvlh_nlpsp *nl);
 /* FP64, one kernel per 1D pass (the OpenCL backend's structure) */
 int wvlh_locham_plain_batched(wvlh_batch *batch, const double *psi, const double *pot, double *hpsi,
                               double *ekin, double *epot);

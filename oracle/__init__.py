@@ -78,6 +78,7 @@ def lib():
         L.wo_cholesky.restype = C.c_int
         L.wo_wpdot.argtypes = [C.c_int, i32p, i32p, C.c_int, i32p, i32p, f64p, f64p] * 2
         L.wo_wpdot.restype = C.c_double
+        L.wo_mask_axpy.argtypes = [C.c_int, i32p, i32p, C.c_int, i32p, i32p, f64p, f64p] * 2 + [C.c_double]
         L.wo_apply_potential.argtypes = [C.c_size_t, f64p, f64p]
         L.wo_apply_potential.restype = C.c_double
         _lib = L
@@ -321,6 +322,50 @@ def wpdot(ka, a, kb, b):
         return [len(kvc), _k(kgc), _k(kvc), len(kvf), _k(kgf), _k(kvf),
                 v[:nvc] if nvc else np.zeros(1), np.ascontiguousarray(fine)]
     return lib().wo_wpdot(*parts(ka, a), *parts(kb, b))
+
+
+def _parts(k, v):
+    kgc, kvc, kgf, kvf = (np.ascontiguousarray(x, np.int32).ravel() for x in k)
+    nvc = int(sum(kgc[1::2] - kgc[0::2] + 1)) if len(kvc) else 0
+    return kgc, kvc, kgf, kvf, nvc
+
+
+def mask_axpy(ka, a, kb, b, s):
+    """a += s b on the points common to a's keys and b's keys, with the
+    reference's pairing of segments (waxpy_mask_unpack over the masks of
+    fill_wblas_segs, locregs/scalar_product.f90:953,1095).  a is updated in
+    place (a contiguous float64 [c | f] vector)."""
+    kgc, kvc, kgf, kvf, nva = _parts(ka, a)
+    lgc, lvc, lgf, lvf, nvb = _parts(kb, b)
+    b = np.ascontiguousarray(b, np.float64)
+    ac = a[:nva] if nva else np.zeros(1)
+    af = a[nva:] if len(a) > nva else np.zeros(7)
+    bc = b[:nvb] if nvb else np.zeros(1)
+    bf = np.ascontiguousarray(b[nvb:]) if len(b) > nvb else np.zeros(7)
+    lib().wo_mask_axpy(len(kvc), _k(kgc), _k(kvc), len(kvf), _k(kgf), _k(kvf), ac, af,
+                       len(lvc), _k(lgc), _k(lvc), len(lvf), _k(lgf), _k(lvf), bc, bf, float(s))
+
+
+def nlpsp_apply(kw, psi, atoms):
+    """Nonlocal projector application for the rows of psi on keys kw
+    (NonLocalHamiltonianApplication, hpsiortho.f90:1044-1125): per atom
+    (kp, proj, h) with proj (m, projector size) on keys kp and h (m, m),
+    c_i = <p_i|psi> (wpdot pairing), hc = h c, eproj += c.hc and
+    hpsi += sum_i hc_i p_i.  Returns (the added hpsi rows, eproj)."""
+    psi = np.atleast_2d(np.asarray(psi, np.float64))
+    out = np.zeros_like(psi)
+    eproj = np.zeros(psi.shape[0])
+    for o in range(psi.shape[0]):
+        row = np.ascontiguousarray(out[o])
+        for kp, proj, h in atoms:
+            proj = np.atleast_2d(np.asarray(proj, np.float64))
+            c = np.array([wpdot(kw, psi[o], kp, proj[i]) for i in range(proj.shape[0])])
+            hc = np.asarray(h, np.float64) @ c
+            eproj[o] += float(c @ hc)
+            for i in range(proj.shape[0]):
+                mask_axpy(kw, row, kp, proj[i], hc[i])
+        out[o] = row
+    return out, eproj
 
 
 # ---------------------------------------------------------------- reference pin

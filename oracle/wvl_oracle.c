@@ -849,6 +849,56 @@ static void wp_part(int nseg_a, const int32_t *keyg_a, const int32_t *keyv_a, co
     }
 }
 
+/* Update through the same pairing of segments: a[jaj..] += s * b[jbj..] on
+ * every common run (waxpy_mask_unpack, locregs/scalar_product.f90:953-1008,
+ * over the masks of fill_wblas_segs, :1095-1187, which walk the loop above). */
+static void wp_axpy_part(int nseg_a, const int32_t *keyg_a, const int32_t *keyv_a, double *pa,
+                         int nseg_b, const int32_t *keyg_b, const int32_t *keyv_b, const double *pb,
+                         int ncomp, double scal)
+{
+    int iaseg0 = 1;
+    if (nseg_a <= 0) return;
+    const int first_a = keyg_a[0], last_a = keyg_a[2 * (nseg_a - 1)];
+    for (int ib = 0; ib < nseg_b; ++ib) {
+        const int kbs = keyg_b[2 * ib], jb1 = keyg_b[2 * ib + 1];
+        int jbj = keyv_b[ib];
+        int jb0 = kbs > first_a ? kbs : first_a;
+        const int iboff = jb0 - kbs > 0 ? jb0 - kbs : 0;
+        iaseg0 = wp_hunt(keyg_a, nseg_a, jb0, iaseg0);
+        if (iaseg0 == 0) { iaseg0 = 1; continue; }
+        while (iaseg0 <= nseg_a) {
+            const int ja0 = keyg_a[2 * (iaseg0 - 1)];
+            const int ea = keyg_a[2 * (iaseg0 - 1) + 1];
+            const int ja1 = jb1 < ea ? jb1 : ea;
+            const int length = ja1 - jb0;
+            const int iaoff = jb0 - ja0 > 0 ? jb0 - ja0 : 0;
+            const int jaj = keyv_a[iaseg0 - 1];
+            for (int i = 0; i <= length; ++i)
+                for (int k = 0; k < ncomp; ++k)
+                    pa[(size_t)(jaj + iaoff + i - 1) * ncomp + k] += scal * pb[(size_t)(jbj + i + iboff - 1) * ncomp + k];
+            if ((ja1 <= jb1 && length >= 0) || iaseg0 == nseg_a) break;
+            iaseg0 += 1;
+            const int sa = keyg_a[2 * (iaseg0 - 1)];
+            jb0 = kbs > sa ? kbs : sa;
+            if (sa > jb1) break;
+            jbj += jb0 - kbs > 0 ? jb0 - kbs : 0;
+        }
+        if (iaseg0 == nseg_a && kbs > last_a) iaseg0 += 1;
+    }
+}
+
+/* a += s * b on the common points of a's keys and b's keys (coarse, then the
+ * 7 fine components): the projector update of cproj_pr_p_psi
+ * (locregs/compression.f90:562-589) for one projector vector b. */
+void wo_mask_axpy(int nseg_ac, const int32_t *keyg_ac, const int32_t *keyv_ac, int nseg_af, const int32_t *keyg_af,
+                  const int32_t *keyv_af, double *a_c, double *a_f,
+                  int nseg_bc, const int32_t *keyg_bc, const int32_t *keyv_bc, int nseg_bf, const int32_t *keyg_bf,
+                  const int32_t *keyv_bf, const double *b_c, const double *b_f, double s)
+{
+    wp_axpy_part(nseg_ac, keyg_ac, keyv_ac, a_c, nseg_bc, keyg_bc, keyv_bc, b_c, 1, s);
+    wp_axpy_part(nseg_af, keyg_af, keyv_af, a_f, nseg_bf, keyg_bf, keyv_bf, b_f, 7, s);
+}
+
 double wo_wpdot(int nseg_ac, const int32_t *keyg_ac, const int32_t *keyv_ac, int nseg_af, const int32_t *keyg_af,
                 const int32_t *keyv_af, const double *a_c, const double *a_f,
                 int nseg_bc, const int32_t *keyg_bc, const int32_t *keyv_bc, int nseg_bf, const int32_t *keyg_bf,
