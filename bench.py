@@ -46,7 +46,7 @@ def parse():
     ap.add_argument("--n", type=int, default=48)
     ap.add_argument("--norb", type=int, default=256)
     ap.add_argument("--no-extras", action="store_true", help="skip comparator / e2e / cpu / other-row legs")
-    ap.add_argument("--leg", default=None, choices=["free_bc", "precond", "overlap", "serve32", "serve64"],
+    ap.add_argument("--leg", default=None, choices=["free_bc", "precond", "overlap", "nlpsp", "serve32", "serve64"],
                     help="run one extra leg alone (one GPU) and print its result as one JSON line")
     return ap.parse_args()
 
@@ -302,6 +302,51 @@ def leg_overlap(torch, ctx, psi64, norb):
             "max_abs_vs_cublas": (S - ref).abs().max().item(), "flops_count": "norb(norb+1)K (SYRK)"}
 
 
+def leg_nlpsp(torch, ctx, psi64, lr, norb, natoms=64, seed=21):
+    """Nonlocal projectors on the batched workload's orbitals: natoms atoms at
+    seeded positions, each with 4 projectors (one s, three p: the shape of an
+    HGH pseudopotential with one radial function per l) on a coarse ball of
+    radius 10 cells with a fine ball of radius 5 cells, symmetric seeded h.
+    FP64, hpsi += V_nl psi and eproj per orbital; the oracle on a 2-orbital,
+    8-atom sample is the CPU figure."""
+    import numpy as np
+    from wvlh.batch import Region
+    from wvlh.keys import Locreg
+    from wvlh.nlpsp import Projectors
+    rng = np.random.default_rng(seed)
+    N = tuple(lr.n)
+    ax = [np.arange(n) for n in N[::-1]]
+    z, y, x = np.meshgrid(*ax, indexing="ij")
+    atoms = []
+    for _ in range(natoms):
+        c = rng.uniform(11, np.array(N) - 11)
+        d2 = (x - c[0]) ** 2 + (y - c[1]) ** 2 + (z - c[2]) ** 2
+        plr = Locreg.from_masks(d2 <= 100.0, d2 <= 25.0, (0, 0, 0), (0.45, 0.45, 0.45))
+        h = rng.uniform(-1, 1, (4, 4))
+        atoms.append((plr, rng.uniform(-1, 1, (4, plr.ncoeff)), h + h.T))
+    nl = Projectors(ctx, Region(ctx, lr), atoms)
+    P = psi64.view(norb, -1)
+    H = torch.zeros_like(P)
+    ms = _timed(torch, lambda: nl.apply(P, H), 5)
+    ncoef = sum(a[1].size for a in atoms)
+    out = {"workload": "%d orbitals of 48^3, %d atoms x 4 projectors (ball radius 10 coarse / 5 fine)" % (norb, natoms),
+           "ms": ms, "projector_values": int(ncoef),
+           "orbital_atom_pairs_per_s": norb * natoms / (ms * 1e-3)}
+    try:
+        from oracle import nlpsp_apply
+        sub = [((a[0].keyg_c, a[0].keyv_c, a[0].keyg_f, a[0].keyv_f), a[1], a[2]) for a in atoms[:8]]
+        kw = (lr.keyg_c, lr.keyv_c, lr.keyg_f, lr.keyv_f)
+        p2 = P[:2].cpu().numpy()
+        t = time.perf_counter()
+        nlpsp_apply(kw, p2, sub)
+        dt = time.perf_counter() - t
+        out["cpu_oracle_orbital_atom_pairs_per_s"] = 16 / dt
+    except Exception as e:  # the oracle is optional on the bench box
+        out["cpu_oracle"] = "unavailable: %s" % e
+    nl.close()
+    return out
+
+
 def leg_serve(torch, dev, precision, nreq=300, loads=(0.3, 0.5, 0.7)):
     """Serving loop: 64 clients (coarse 16..64 per dim, periodic or free, 4..128
     orbitals), requests 50/50 Hpsi and density; capacity from a burst of one
@@ -365,6 +410,13 @@ def main():
             res = leg_free_regions(torch, ctx, dev)
         elif args.leg == "precond":
             res = leg_precond(torch, ctx, dev)
+        elif args.leg == "nlpsp":
+            from wvlh import workloads as W
+            lr = W.full_periodic(args.n, 0.45)
+            g = torch.Generator(device=dev)
+            g.manual_seed(1000)
+            psi = torch.rand(args.norb * lr.ncoeff, generator=g, device=dev, dtype=torch.float64) * 2 - 1
+            res = leg_nlpsp(torch, ctx, psi, lr, args.norb)
         elif args.leg == "overlap":
             from wvlh import workloads as W
             lr = W.full_periodic(args.n, 0.45)
@@ -532,6 +584,7 @@ def main():
         # the other rows of the path on this GPU
         extras["density"] = leg_density(torch, batch, psi32, psi64, lr, norb, dev)
         extras["overlap"] = leg_overlap(torch, ctx, psi64, norb)
+        extras["nlpsp"] = leg_nlpsp(torch, ctx, psi64, lr, norb)
         del hp, hv, hh
         extras["free_bc"] = leg_free_regions(torch, ctx, dev)
         extras["precond"] = leg_precond(torch, ctx, dev)
