@@ -687,13 +687,15 @@ extern "C" int wvlh_precond_batched(wvlh_batch *b, int precision, int ncong, con
 }
 
 namespace wvlh {
-size_t overlap_workspace_bytes(int norb, long long K, int nsm);
+size_t overlap_workspace_bytes(int norb, long long K, int nsm, bool two);
 template <class TI>
-cudaError_t launch_overlap(int norb, long long K, long long ld, const TI *psi, double *S, double *work, int nsm,
-                           cudaStream_t st);
+cudaError_t launch_overlap(int norb, long long K, long long ld, const TI *psi, const TI *psib, double *S,
+                           double *work, int nsm, cudaStream_t st);
 }  // namespace wvlh
 
-extern "C" int wvlh_overlap(wvlh_ctx *c, int precision, int norb, int64_t K, int64_t ld, const void *psi, double *S)
+// S = psi psi^T, or L = psi hpsi^T when hpsi is given
+static int overlap_entry(wvlh_ctx *c, int precision, int norb, int64_t K, int64_t ld, const void *psi,
+                         const void *hpsi, double *S)
 {
     if (!c || !psi || !S || norb <= 0 || K <= 0 || ld < K || (precision != 32 && precision != 64))
         return fail(WVLH_ERR_ARG);
@@ -701,14 +703,26 @@ extern "C" int wvlh_overlap(wvlh_ctx *c, int precision, int norb, int64_t K, int
     int nsm = 0;
     CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c->device));
     int rc;
-    if ((rc = c->ov_work.ensure(overlap_workspace_bytes(norb, K, nsm)))) return fail(rc);
+    if ((rc = c->ov_work.ensure(overlap_workspace_bytes(norb, K, nsm, hpsi != nullptr)))) return fail(rc);
     cudaError_t e = precision == 64
-                        ? launch_overlap<double>(norb, K, ld, (const double *)psi, S, (double *)c->ov_work.p, nsm,
-                                                 c->stream)
-                        : launch_overlap<float>(norb, K, ld, (const float *)psi, S, (double *)c->ov_work.p, nsm,
-                                                c->stream);
+                        ? launch_overlap<double>(norb, K, ld, (const double *)psi, (const double *)hpsi, S,
+                                                 (double *)c->ov_work.p, nsm, c->stream)
+                        : launch_overlap<float>(norb, K, ld, (const float *)psi, (const float *)hpsi, S,
+                                                (double *)c->ov_work.p, nsm, c->stream);
     CK(e);
     return WVLH_OK;
+}
+
+extern "C" int wvlh_overlap(wvlh_ctx *c, int precision, int norb, int64_t K, int64_t ld, const void *psi, double *S)
+{
+    return overlap_entry(c, precision, norb, K, ld, psi, nullptr, S);
+}
+
+extern "C" int wvlh_subspace_matrix(wvlh_ctx *c, int precision, int norb, int64_t K, int64_t ld, const void *psi,
+                                    const void *hpsi, double *L)
+{
+    if (!hpsi) return fail(WVLH_ERR_ARG);
+    return overlap_entry(c, precision, norb, K, ld, psi, hpsi, L);
 }
 
 static long long pot_extent(const wvlh_batch *b)

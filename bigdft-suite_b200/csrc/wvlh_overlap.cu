@@ -9,6 +9,11 @@
 // the splits in a fixed order (deterministic) and mirrors the tile into the
 // upper triangle.
 //
+// The same kernel forms the subspace matrix L = Psi (H Psi)^T of two panels
+// (TWO: every tile of the square, B rows from the second panel, no mirror):
+// the Lagrange multipliers of orthoconstraint (orthogonality.f90:375-625,
+// subspace_matrix :196-224, gemm('T','N')).
+//
 // Main loop: a 2-stage cp.async ring stages 64 x 32 slices of the two orbital
 // panels in their storage type (16-byte copies when rows are 16-byte aligned),
 // so the loads of slice s+1 overlap the MMAs of slice s; at 74 KB (FP64) three
@@ -94,9 +99,10 @@ __device__ __forceinline__ void ov_stage(TI *dst, const TI *__restrict__ psi, lo
     }
 }
 
-template <class TI, int VEC>
+template <class TI, int VEC, bool TWO>
 __global__ void __launch_bounds__(OV_THREADS) k_overlap_partial(int norb, long long K, long long ld,
-                                                                const TI *__restrict__ psi, int nsplit,
+                                                                const TI *__restrict__ psi,
+                                                                const TI *__restrict__ psib, int nsplit,
                                                                 long long kchunk, double *__restrict__ part)
 {
     extern __shared__ __align__(16) unsigned char ov_smem[];
@@ -105,9 +111,16 @@ __global__ void __launch_bounds__(OV_THREADS) k_overlap_partial(int norb, long l
     TI *Bs = As + OV_STAGES * OV_BM * LD;
     const int tile = blockIdx.x / nsplit, split = blockIdx.x % nsplit;
     int ti, tj;
-    tri_tile(tile, ti, tj);
+    if (TWO) {
+        const int nt = (norb + OV_BM - 1) / OV_BM;
+        ti = tile / nt;
+        tj = tile - ti * nt;
+    } else {
+        tri_tile(tile, ti, tj);
+    }
+    const TI *pb = TWO ? psib : psi;
     const int i0 = ti * OV_BM, j0 = tj * OV_BM;
-    const bool diag = ti == tj;
+    const bool diag = !TWO && ti == tj;
     const long long kb = split * kchunk;
     const long long ke = kb + kchunk < K ? kb + kchunk : K;
     const int nk = ke > kb ? (int)((ke - kb + OV_BK - 1) / OV_BK) : 0;
@@ -128,7 +141,7 @@ __global__ void __launch_bounds__(OV_THREADS) k_overlap_partial(int norb, long l
     for (int s = 0; s < OV_STAGES - 1; ++s) {
         if (s < nk) {
             ov_stage<TI, VEC>(As + s * OV_BM * LD, psi, ld, i0, norb, kb + (long long)s * OV_BK, ke);
-            if (!diag) ov_stage<TI, VEC>(Bs + s * OV_BM * LD, psi, ld, j0, norb, kb + (long long)s * OV_BK, ke);
+            if (!diag) ov_stage<TI, VEC>(Bs + s * OV_BM * LD, pb, ld, j0, norb, kb + (long long)s * OV_BK, ke);
         }
         ov_commit();
     }
@@ -141,7 +154,7 @@ __global__ void __launch_bounds__(OV_THREADS) k_overlap_partial(int norb, long l
                 const int slot = s % OV_STAGES;
                 ov_stage<TI, VEC>(As + slot * OV_BM * LD, psi, ld, i0, norb, kb + (long long)s * OV_BK, ke);
                 if (!diag)
-                    ov_stage<TI, VEC>(Bs + slot * OV_BM * LD, psi, ld, j0, norb, kb + (long long)s * OV_BK, ke);
+                    ov_stage<TI, VEC>(Bs + slot * OV_BM * LD, pb, ld, j0, norb, kb + (long long)s * OV_BK, ke);
             }
             ov_commit();
         }
@@ -188,67 +201,81 @@ __global__ void __launch_bounds__(OV_THREADS) k_overlap_partial(int norb, long l
 
 // one thread per tile element (grid.x tiles, grid.y element blocks): the
 // splits are summed in order, so the result does not depend on the grid
+template <bool TWO>
 __global__ void k_overlap_reduce(int norb, int nsplit, const double *__restrict__ part, double *__restrict__ S)
 {
     const int tile = blockIdx.x;
     int ti, tj;
-    tri_tile(tile, ti, tj);
+    if (TWO) {
+        const int nt = (norb + OV_BM - 1) / OV_BM;
+        ti = tile / nt;
+        tj = tile - ti * nt;
+    } else {
+        tri_tile(tile, ti, tj);
+    }
     const int e = blockIdx.y * blockDim.x + threadIdx.x;
     if (e >= OV_BM * OV_BM) return;
     const int r = e / OV_BM, c = e - r * OV_BM;
     const int i = ti * OV_BM + r, j = tj * OV_BM + c;
-    if (i >= norb || j >= norb || j > i) return;
+    if (i >= norb || j >= norb || (!TWO && j > i)) return;
     double s = 0.0;
     for (int k = 0; k < nsplit; ++k) s += part[((size_t)tile * nsplit + k) * OV_BM * OV_BM + e];
     S[(size_t)i * norb + j] = s;
-    S[(size_t)j * norb + i] = s;
+    if (!TWO) S[(size_t)j * norb + i] = s;
 }
 
 // splits over K: about three CTAs per SM (the 2-stage FP64 ring takes 74 KB)
-int overlap_split(int norb, long long K, int nsm)
+static int overlap_tiles(int norb, bool two)
 {
     const int nt = (norb + OV_BM - 1) / OV_BM;
-    const int ntile = nt * (nt + 1) / 2;
+    return two ? nt * nt : nt * (nt + 1) / 2;
+}
+
+int overlap_split(int norb, long long K, int nsm, bool two)
+{
+    const int ntile = overlap_tiles(norb, two);
     int nsplit = (3 * nsm + ntile - 1) / ntile;
     const long long maxs = (K + OV_BK - 1) / OV_BK;
     if (nsplit > maxs) nsplit = (int)maxs;
     return nsplit < 1 ? 1 : nsplit;
 }
 
-size_t overlap_workspace_bytes(int norb, long long K, int nsm)
+size_t overlap_workspace_bytes(int norb, long long K, int nsm, bool two)
 {
-    const int nt = (norb + OV_BM - 1) / OV_BM;
-    return sizeof(double) * (size_t)(nt * (nt + 1) / 2) * overlap_split(norb, K, nsm) * OV_BM * OV_BM;
+    return sizeof(double) * (size_t)overlap_tiles(norb, two) * overlap_split(norb, K, nsm, two) * OV_BM * OV_BM;
 }
 
+// S = psi psi^T (psib null: lower tiles, mirrored) or psi psib^T (every tile)
 template <class TI>
-cudaError_t launch_overlap(int norb, long long K, long long ld, const TI *psi, double *S, double *work, int nsm,
-                           cudaStream_t st)
+cudaError_t launch_overlap(int norb, long long K, long long ld, const TI *psi, const TI *psib, double *S,
+                           double *work, int nsm, cudaStream_t st)
 {
-    const int nt = (norb + OV_BM - 1) / OV_BM;
-    const int ntile = nt * (nt + 1) / 2;
-    const int nsplit = overlap_split(norb, K, nsm);
+    const bool two = psib != nullptr;
+    const int ntile = overlap_tiles(norb, two);
+    const int nsplit = overlap_split(norb, K, nsm, two);
     long long kchunk = (K + nsplit - 1) / nsplit;
     kchunk = (kchunk + OV_BK - 1) / OV_BK * OV_BK;
     const size_t smem = overlap_smem_bytes(sizeof(TI));
-    // 16-byte copies need every row start (and the base) on a 16-byte boundary
-    const bool vec16 = ((uintptr_t)psi % 16 == 0) && ((ld * (long long)sizeof(TI)) % 16 == 0);
+    // 16-byte copies need every row start (and the bases) on a 16-byte boundary
+    const bool vec16 = ((uintptr_t)psi % 16 == 0) && (!two || (uintptr_t)psib % 16 == 0) &&
+                       ((ld * (long long)sizeof(TI)) % 16 == 0);
     cudaError_t e;
-    if (vec16) {
-        auto k = k_overlap_partial<TI, 16>;
-        if ((e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem))) return e;
-        k<<<ntile * nsplit, OV_THREADS, smem, st>>>(norb, K, ld, psi, nsplit, kchunk, work);
-    } else {
-        auto k = k_overlap_partial<TI, (int)sizeof(TI)>;
-        if ((e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem))) return e;
-        k<<<ntile * nsplit, OV_THREADS, smem, st>>>(norb, K, ld, psi, nsplit, kchunk, work);
-    }
-    k_overlap_reduce<<<dim3(ntile, OV_BM * OV_BM / 256), 256, 0, st>>>(norb, nsplit, work, S);
+    auto go = [&](auto k) -> cudaError_t {
+        cudaError_t r;
+        if ((r = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem))) return r;
+        k<<<ntile * nsplit, OV_THREADS, smem, st>>>(norb, K, ld, psi, psib, nsplit, kchunk, work);
+        return cudaGetLastError();
+    };
+    if (two) e = vec16 ? go(k_overlap_partial<TI, 16, true>) : go(k_overlap_partial<TI, (int)sizeof(TI), true>);
+    else e = vec16 ? go(k_overlap_partial<TI, 16, false>) : go(k_overlap_partial<TI, (int)sizeof(TI), false>);
+    if (e) return e;
+    if (two) k_overlap_reduce<true><<<dim3(ntile, OV_BM * OV_BM / 256), 256, 0, st>>>(norb, nsplit, work, S);
+    else k_overlap_reduce<false><<<dim3(ntile, OV_BM * OV_BM / 256), 256, 0, st>>>(norb, nsplit, work, S);
     return cudaGetLastError();
 }
-template cudaError_t launch_overlap<double>(int, long long, long long, const double *, double *, double *, int,
-                                            cudaStream_t);
-template cudaError_t launch_overlap<float>(int, long long, long long, const float *, double *, double *, int,
-                                           cudaStream_t);
+template cudaError_t launch_overlap<double>(int, long long, long long, const double *, const double *, double *,
+                                            double *, int, cudaStream_t);
+template cudaError_t launch_overlap<float>(int, long long, long long, const float *, const float *, double *,
+                                           double *, int, cudaStream_t);
 
 }  // namespace wvlh

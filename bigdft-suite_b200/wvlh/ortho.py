@@ -6,6 +6,11 @@
 :2297-2430: S = L L^T, Psi <- L^-1 Psi) or the Loewdin scheme (``loewdin``,
 :2431-2500: Psi <- S^-1/2 Psi), in FP64 on the device; the small dense
 factorisations (norb x norb) use torch.linalg (cuSOLVER).
+``orthoconstraint`` is the gradient step that follows the Hamiltonian
+(:375-625): Lagrange multipliers L = <psi_i|hpsi_j> on the same tensor-core
+kernel, symmetrised and corrected for unequal occupations
+(``lagrange_multiplier``, :293-369), then hpsi <- hpsi - L^T psi
+(``subspace_update``, :254-271; a plain DGEMM).
 """
 import ctypes as C
 
@@ -45,3 +50,67 @@ def orthonormalize(ctx, psi, method="cholesky"):
     else:
         raise WvlhError("method must be 'cholesky' or 'loewdin'")
     return psi, S
+
+
+def subspace_matrix(ctx, psi, hpsi, L=None):
+    """L[i, j] = <psi_i | hpsi_j> (FP64, norb x norb) of two (norb, K) device
+    tensors with one dtype and row stride."""
+    torch = ctx.torch
+    if psi.dim() != 2 or hpsi.shape != psi.shape or psi.dtype != hpsi.dtype or psi.stride() != hpsi.stride():
+        raise WvlhError("psi, hpsi: 2D tensors of one shape, dtype and layout")
+    if psi.stride(1) != 1:
+        raise WvlhError("rows must be contiguous")
+    prec = {torch.float32: 32, torch.float64: 64}.get(psi.dtype)
+    if prec is None:
+        raise WvlhError("psi must be float32 or float64")
+    norb, K = psi.shape
+    if L is None:
+        L = torch.empty(norb, norb, dtype=torch.float64, device=psi.device)
+    check(lib().wvlh_subspace_matrix(ctx.h, prec, int(norb), int(K), int(psi.stride(0)),
+                                     C.c_void_p(psi.data_ptr()), C.c_void_p(hpsi.data_ptr()),
+                                     C.c_void_p(L.data_ptr())), "wvlh_subspace_matrix")
+    return L
+
+
+def lagrange_multiplier(L, occup, symm=True, correction=True):
+    """In place on the (norb, norb) FP64 matrix L[i, j] = <psi_i|hpsi_j>, as the
+    reference's lagrange_multiplier (orthogonality.f90:293-369) with real
+    coefficients: its row loop symmetrises each pair (i < j) before either
+    element is scaled, so the result is the symmetrised matrix followed by the
+    occupation correction L[i, j] *= (f_i - f_j) / (2 f_i) (1/2 when |f_i| <=
+    0.5) wherever f_i != f_j.  Returns (trace, asymm, mix): the trace, the
+    largest (L_ij - L_ji)^2 and the largest squared coupling between states of
+    different occupation."""
+    import torch as _t
+    f = _t.as_tensor(occup, dtype=_t.float64, device=L.device)
+    trace = L.diagonal().sum()
+    iu = _t.triu_indices(L.shape[0], L.shape[0], 1, device=L.device)
+    d = L[iu[0], iu[1]] - L[iu[1], iu[0]]
+    asymm = (d * d).max() if d.numel() else _t.zeros((), dtype=_t.float64, device=L.device)
+    if symm:
+        u = 0.5 * (L[iu[0], iu[1]] + L[iu[1], iu[0]])
+        L[iu[0], iu[1]] = u
+        L[iu[1], iu[0]] = u
+    diff = f[:, None] != f[None, :]
+    mix = (L * L)[diff].max() if bool(diff.any()) else _t.zeros((), dtype=_t.float64, device=L.device)
+    if correction:
+        fac = _t.where(f.abs()[:, None] > 0.5, 0.5 * (f[:, None] - f[None, :]) / f[:, None],
+                       _t.full_like(L, 0.5))
+        L.copy_(_t.where(diff, fac * L, L))
+    return float(trace), float(asymm), float(mix)
+
+
+def orthoconstraint(ctx, psi, hpsi, occup=None, symm=True, tr_min=False):
+    """The orthogonality constraint on the gradient (orthoconstraint,
+    orthogonality.f90:375-625) for real orbitals of one spin and k-point:
+    L = <psi|hpsi>, lagrange_multiplier, hpsi -= L^T psi.  In place on hpsi;
+    returns (L, trace, asymm, mix) (scprsum = occ x trace, occ = kwgt (3 -
+    nspin) for the caller)."""
+    torch = ctx.torch
+    norb = psi.shape[0]
+    if occup is None:
+        occup = [2.0] * norb
+    L = subspace_matrix(ctx, psi, hpsi)
+    trace, asymm, mix = lagrange_multiplier(L, occup, symm=symm, correction=not tr_min)
+    hpsi.sub_(L.T.to(hpsi.dtype) @ psi)
+    return L, trace, asymm, mix

@@ -314,6 +314,13 @@ int wvlh_precond_batched(wvlh_batch *batch, int precision, int ncong, const doub
  * reference's getOverlap syrk (wfn_opt/orthogonality.f90:2675) summed in a
  * fixed order. */
 int wvlh_overlap(wvlh_ctx *ctx, int precision, int norb, int64_t K, int64_t ld, const void *psi, double *S);
+/* Subspace matrix L[i][j] = <psi_i | hpsi_j> (norb x norb, FP64, row-major:
+ * row i, column j) of two panels with the same layout: the Lagrange
+ * multipliers of orthoconstraint (wfn_opt/orthogonality.f90:375-625,
+ * subspace_matrix :196-224, gemm('T','N')), on the same FP64 tensor-core
+ * kernel, every tile of the square, splits summed in a fixed order. */
+int wvlh_subspace_matrix(wvlh_ctx *ctx, int precision, int norb, int64_t K, int64_t ld, const void *psi,
+                         const void *hpsi, double *L);
 /* Compressed scalar products out[i*nb + j] = <a_i|b_j> (FP64) between na
  * vectors on the keys of region ra (row stride lda) and nb vectors on the
  * keys of region rb (row stride ldb), both regions with the same box (keys

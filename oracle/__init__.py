@@ -368,6 +368,45 @@ def nlpsp_apply(kw, psi, atoms):
     return out, eproj
 
 
+def lagrange_multiplier(lam, occup, symm=True, correction=True):
+    """The reference's lagrange_multiplier (wfn_opt/orthogonality.f90:293-369)
+    for real coefficients, loop for loop: lam is the Fortran lambda(i, j) =
+    <psi_i|hpsi_j> as a numpy (norb, norb) array indexed [i, j]; modified in
+    place.  Returns (trace, asymm, mix)."""
+    norb = lam.shape[0]
+    tol = 0.5
+    asymm = mix = trace = 0.0
+    for i in range(norb):
+        trace += lam[i, i]
+        for j in range(i + 1, norb):
+            lij, lji = lam[i, j], lam[j, i]
+            asymm = max(asymm, (lij - lji) ** 2)
+            if symm:
+                lij = lij + lji
+                lam[i, j] = 0.5 * lij
+                lam[j, i] = 0.5 * lij
+        fi = occup[i]
+        for j in range(norb):
+            fj = occup[j]
+            if fi != fj:
+                mix = max(mix, lam[i, j] ** 2)
+                if correction:
+                    fac = 0.5 * ((fi - fj) / fi) if abs(fi) > tol else 0.5
+                    lam[i, j] = fac * lam[i, j]
+    return trace, asymm, mix
+
+
+def orthoconstraint(psi, hpsi, occup, symm=True, tr_min=False):
+    """orthoconstraint (orthogonality.f90:375-625) for real orbitals of one spin
+    and k-point, rows of psi/hpsi the orbitals: lambda = psi hpsi^T
+    (subspace_matrix, gemm('T','N')), lagrange_multiplier, then
+    hpsi_j -= sum_i lambda(i, j) psi_i (subspace_update, gemm('N','N', -1)).
+    Returns (new hpsi, lambda, trace, asymm, mix)."""
+    lam = np.asarray(psi, np.float64) @ np.asarray(hpsi, np.float64).T
+    tr, asy, mix = lagrange_multiplier(lam, occup, symm, not tr_min)
+    return hpsi - lam.T @ psi, lam, tr, asy, mix
+
+
 # ---------------------------------------------------------------- reference pin
 def ref_magicfilter():
     """ctypes handle to the reference's own C magic filter, or None."""

@@ -66,3 +66,36 @@ def test_overlap_unaligned_rows(oracle, torch_cuda, wctx, dtype_name, ld):
     src = full[:, :K].astype(np.float32).astype(np.float64) if dtype_name == "float32" else full[:, :K]
     ref = oracle.overlap(np.ascontiguousarray(src))
     assert np.abs(S - ref).max() / np.abs(ref).max() < 1e-13
+
+
+@pytest.mark.parametrize("norb,K,dtype_name", [(7, 1000, "float64"), (100, 12345, "float64"), (130, 9001, "float32")])
+def test_subspace_matrix_matches_gemm(torch_cuda, wctx, norb, K, dtype_name):
+    """L = <psi_i|hpsi_j> on every tile of the square (subspace_matrix,
+    orthogonality.f90:196-224), non-symmetric, FP32 rows widened."""
+    from wvlh.ortho import subspace_matrix
+    torch = torch_cuda
+    rng = np.random.default_rng(norb)
+    a, b = rng.uniform(-1, 1, (norb, K)), rng.uniform(-1, 1, (norb, K))
+    if dtype_name == "float32":
+        a, b = a.astype(np.float32).astype(np.float64), b.astype(np.float32).astype(np.float64)
+    dt = getattr(torch, dtype_name)
+    L = subspace_matrix(wctx, torch.tensor(a, dtype=dt, device="cuda"), torch.tensor(b, dtype=dt, device="cuda"))
+    ref = a @ b.T
+    assert np.abs(L.cpu().numpy() - ref).max() / np.abs(ref).max() < 1e-13
+
+
+@pytest.mark.parametrize("occ", ["equal", "mixed"])
+def test_orthoconstraint_matches_oracle(oracle, torch_cuda, wctx, occ):
+    from wvlh.ortho import orthoconstraint
+    torch = torch_cuda
+    rng = np.random.default_rng(5)
+    norb, K = 40, 20000
+    psi = rng.uniform(-1, 1, (norb, K))
+    hpsi = rng.uniform(-1, 1, (norb, K))
+    f = np.full(norb, 2.0) if occ == "equal" else rng.choice([2.0, 1.0, 0.0], norb)
+    g_ref, lam, tr, asy, mix = oracle.orthoconstraint(psi, hpsi, f)
+    tp, th = torch.tensor(psi, device="cuda"), torch.tensor(hpsi, device="cuda")
+    L, tr2, asy2, mix2 = orthoconstraint(wctx, tp, th, occup=f)
+    assert np.abs(L.cpu().numpy() - lam).max() / np.abs(lam).max() < 1e-13
+    assert np.abs(th.cpu().numpy() - g_ref).max() / np.abs(g_ref).max() < 1e-13
+    assert abs(tr2 - tr) <= 1e-12 * abs(tr) and abs(asy2 - asy) <= 1e-12 * asy and abs(mix2 - mix) <= 1e-12 * max(mix, 1e-300)
