@@ -236,6 +236,34 @@ class Server:
             self.resident -= c.resident_bytes
         self._admit()
 
+    def evict(self, c, radical, binary=True):
+        """Move a client's orbitals out of device memory into the reference's
+        restart files (wvlh.restart, one file per orbital: <radical>-k001-NR...)
+        and release its device state; its potential stays in host memory.
+        Restore it with restore()."""
+        from .restart import write_waves
+        if not c.admitted:
+            raise WvlhError("client %d is not resident" % c.id)
+        if any(k[0] == c.id for k in self.busy) or any(r.client is c for r in self.queue):
+            raise WvlhError("client %d still has requests" % c.id)
+        write_waves(radical, c.psi.double().cpu().numpy(), c.locreg, binary=binary)
+        pot = c.pot.cpu().numpy()
+        self.release(c)
+        c._evicted = (radical, binary, pot)
+
+    def restore(self, c):
+        """Read an evicted client's orbitals back and queue it for admission
+        (admitted now if the budget allows)."""
+        from .restart import read_waves
+        radical, binary, pot = getattr(c, "_evicted", (None, None, None))
+        if radical is None:
+            raise WvlhError("client %d was not evicted" % c.id)
+        psi = read_waves(radical, c.norb, c.locreg, binary=binary)
+        c._init = (0, psi, pot)
+        c._evicted = None
+        self.pending.append(c)
+        self._admit()
+
     # ----------------------------------------------------------------- requests
     def submit(self, c, kind, t_arrival=None):
         if kind not in ("H", "rho"):

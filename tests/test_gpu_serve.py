@@ -191,3 +191,28 @@ def test_poisson_replay_completes(torch_cuda):
     assert st["n"] == 60 and 0 < st["p50_ms"] <= st["p99_ms"]
     assert srv.launches < 60   # requests were batched
     srv.close()
+
+
+@pytest.mark.parametrize("precision,binary", [(64, True), (32, False)])
+def test_evict_to_restart_files_and_restore(torch_cuda, tmp_path, precision, binary):
+    """A client's orbitals leave the device as the reference's restart files
+    and come back: the same H psi and energies afterwards (bit for bit with
+    the binary form; FP32 values also survive the plain form's 12/10 digits)."""
+    torch = torch_cuda
+    specs = small_clients()[:2]
+    srv = Server(precision=precision, hbm_budget=8e9, n_slots=1, scratch_per_slot=2e9)
+    data = [client_data(lr, n, 300 + i) for i, (lr, n) in enumerate(specs)]
+    cl = [srv.register(lr, n, psi=psi, pot=pot) for (lr, n), (psi, pot) in zip(specs, data)]
+    r = srv.submit(cl[0], "H")
+    srv.drain()
+    before = (cl[0].hpsi.clone(), r.ekin, r.epot, cl[0].psi.clone())
+    srv.evict(cl[0], str(tmp_path / "wavefunction"), binary=binary)
+    assert not cl[0].admitted and cl[0].psi is None
+    assert (tmp_path / ("wavefunction-k001-NR.%sb000001" % ("bin." if binary else ""))).exists()
+    srv.restore(cl[0])
+    assert cl[0].admitted and torch.equal(cl[0].psi, before[3])
+    r = srv.submit(cl[0], "H")
+    srv.drain()
+    torch.cuda.synchronize()
+    assert torch.equal(cl[0].hpsi, before[0]) and r.ekin == before[1] and r.epot == before[2]
+    srv.close()
