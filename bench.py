@@ -514,7 +514,7 @@ def main():
         # DRAM traffic of each kernel (dram__bytes_read.sum + dram__bytes_write.sum) from ncu
         # captures of one call over 48 orbitals of this 48^3 FP32 workload, scaled by the orbitals
         # of this launch (the traffic grows in proportion to them); z kernels: both chains
-        traffic48 = [460.233984e6, 582.137856e6, 656.146944e6]
+        traffic48 = [452.768000e6, 580.762624e6, 655.957504e6]
         traffic = traffic48[dom] / 48 * norb if (dom < 3 and n == 48) else None
         extras["roofline"] = {"bound": "hbm", "achieved": ach, "peak": hbm, "unit": "GB/s", "frac": ach / hbm,
                               "traffic": traffic, "kernel": names[dom], "peak_source": hbm_src,
