@@ -46,7 +46,7 @@ def parse():
     ap.add_argument("--n", type=int, default=48)
     ap.add_argument("--norb", type=int, default=256)
     ap.add_argument("--no-extras", action="store_true", help="skip comparator / e2e / cpu / other-row legs")
-    ap.add_argument("--leg", default=None, choices=["free_bc", "precond", "overlap", "nlpsp", "serve32", "serve64"],
+    ap.add_argument("--leg", default=None, choices=["free_bc", "precond", "overlap", "nlpsp", "psolver", "serve32", "serve64"],
                     help="run one extra leg alone (one GPU) and print its result as one JSON line")
     return ap.parse_args()
 
@@ -347,6 +347,29 @@ def leg_nlpsp(torch, ctx, psi64, lr, norb, natoms=64, seed=21):
     return out
 
 
+def leg_psolver(torch, ctx, dev, n=96, h=0.225):
+    """Hartree potential of a seeded density on the periodic 96^3 ISF grid of
+    the batched workload (the potential step that follows the density):
+    wvlh_psolver_periodic (cuFFT and the ISF kernel multiply, FP64) against
+    the oracle's numpy restatement on the host."""
+    import numpy as np
+    from wvlh.psolver import hartree_periodic
+    rng = np.random.default_rng(5)
+    rho_h = rng.uniform(-1, 1, (n, n, n))
+    rho = torch.tensor(rho_h, device=dev)
+    pot = torch.empty_like(rho)
+    ms = _timed(torch, lambda: hartree_periodic(ctx, rho, (h, h, h), pot=pot), 10)
+    out = {"workload": "%d^3 periodic grid, h %.3f bohr, FP64" % (n, h), "ms": ms}
+    try:
+        from oracle import psolver_periodic
+        t = time.perf_counter()
+        psolver_periodic(rho_h, (h, h, h))
+        out["cpu_oracle_ms"] = (time.perf_counter() - t) * 1e3
+    except Exception as e:  # the oracle is optional on the bench box
+        out["cpu_oracle"] = "unavailable: %s" % e
+    return out
+
+
 def leg_serve(torch, dev, precision, nreq=300, loads=(0.3, 0.5, 0.7)):
     """Serving loop: 64 clients (coarse 16..64 per dim, periodic or free, 4..128
     orbitals), requests 50/50 Hpsi and density; capacity from a burst of one
@@ -410,6 +433,8 @@ def main():
             res = leg_free_regions(torch, ctx, dev)
         elif args.leg == "precond":
             res = leg_precond(torch, ctx, dev)
+        elif args.leg == "psolver":
+            res = leg_psolver(torch, ctx, dev)
         elif args.leg == "nlpsp":
             from wvlh import workloads as W
             lr = W.full_periodic(args.n, 0.45)
@@ -585,6 +610,7 @@ def main():
         extras["density"] = leg_density(torch, batch, psi32, psi64, lr, norb, dev)
         extras["overlap"] = leg_overlap(torch, ctx, psi64, norb)
         extras["nlpsp"] = leg_nlpsp(torch, ctx, psi64, lr, norb)
+        extras["psolver"] = leg_psolver(torch, ctx, dev)
         del hp, hv, hh
         extras["free_bc"] = leg_free_regions(torch, ctx, dev)
         extras["precond"] = leg_precond(torch, ctx, dev)

@@ -78,6 +78,7 @@ WVLH_SYMBOLS = [
     "wvlh_region_grid_size", "wvlh_region_scratch_bytes", "wvlh_batch_create_orbitals", "wvlh_wpdot",
     "wvlh_locham_graph_create", "wvlh_graph_launch", "wvlh_graph_destroy",
     "wvlh_nlpsp_create", "wvlh_nlpsp_apply", "wvlh_nlpsp_destroy", "wvlh_subspace_matrix",
+    "wvlh_psolver_periodic",
 ]
 
 
@@ -137,6 +138,7 @@ def lib():
     L.wvlh_nlpsp_apply.argtypes = [vp, C.c_int, vp, C.c_int64, vp, vp]
     L.wvlh_nlpsp_destroy.argtypes = [vp]
     L.wvlh_subspace_matrix.argtypes = [vp, C.c_int, C.c_int, C.c_int64, C.c_int64, vp, vp, vp]
+    L.wvlh_psolver_periodic.argtypes = [vp, C.POINTER(C.c_int), C.POINTER(C.c_double), vp, vp, C.c_double, vp]
     L.wvlh_host_alloc.restype = vp
     L.wvlh_host_alloc.argtypes = [C.c_size_t]
     L.wvlh_host_free.argtypes = [vp]

@@ -358,6 +358,18 @@ int wvlh_nlpsp_create(wvlh_ctx *ctx, const wvlh_region *psi_region, int natoms, 
  * hpsi += V_nl psi, eproj[o] = sum over atoms of c . hc (written). */
 int wvlh_nlpsp_apply(wvlh_nlpsp *nl, int norb, const double *psi, int64_t ld, double *hpsi, double *eproj);
 int wvlh_nlpsp_destroy(wvlh_nlpsp *nl);
+/* Hartree potential of a density on a periodic real-space (ISF) grid, the
+ * reference's PSolver for periodic boundary conditions (Periodic_Kernel and
+ * fourtrans_isf, psolver/src/Build_Kernel.f90:16-262; P_multkernel_NO,
+ * PSolver_Base_new.f90:2515-2640; scal 1/(n1 n2 n3), createKernel.f90:299):
+ * V^(k) = rho^(k) phi^_x phi^_y phi^_z / (pi g^2) with the order-16 ISF
+ * Fourier factors, the k = 0 term set to offset / h^3.  n: grid points per
+ * dimension (x fastest; even, >= 16), h: spacings (bohr), rho/pot: DEVICE FP64
+ * arrays of n1 n2 n3 values (pot may be rho when eh is NULL).  eh (DEVICE, one
+ * double, or NULL): the Hartree energy 0.5 sum(rho V) h1 h2 h3
+ * (PSolver_Main.f90:403).  FFTs by cuFFT, plans kept per context and grid. */
+int wvlh_psolver_periodic(wvlh_ctx *ctx, const int n[3], const double h[3], const double *rho, double *pot,
+                          double offset, double *eh);
 /* FP64, one kernel per 1D pass (the OpenCL backend's structure) */
 int wvlh_locham_plain_batched(wvlh_batch *batch, const double *psi, const double *pot, double *hpsi,
                               double *ekin, double *epot);

@@ -407,6 +407,72 @@ def orthoconstraint(psi, hpsi, occup, symm=True, tr_min=False):
     return hpsi - lam.T @ psi, lam, tr, asy, mix
 
 
+def isf_fourier(n):
+    """The order-16 ISF's Fourier transform at p = i 2 pi / (2 n), i = 0..n, as
+    fourtrans_isf computes it (psolver/src/Build_Kernel.f90:202-262): odd i by
+    the product of two-scale symbols H(p/2^j) until H is 1 to 1e-16, even i
+    from i/2 by one more symbol.  H(p) = 1/2 + sum over odd m <= 15 of
+    w_m cos(m p), w_m the 16-point Lagrange weights at the midpoint of the odd
+    offsets (the lazy_16 filter)."""
+    from fractions import Fraction
+    odd = list(range(-15, 16, 2))
+    w = {}
+    for m in range(1, 16, 2):
+        r = Fraction(1)
+        for i in odd:
+            if i != m:
+                r *= Fraction(-i, m - i)
+        w[m] = float(r)
+
+    def H(p):
+        return 0.5 + sum(w[m] * np.cos(m * p) for m in range(15, 0, -2))
+    f = np.zeros(n + 1)
+    f[0] = 1.0
+    for i in range(1, n + 1):
+        if i % 2 == 0:
+            continue
+        p = i * 2.0 * np.pi / (2.0 * n)
+        v, q = 1.0, p
+        while True:
+            q *= 0.5
+            hv = H(q)
+            if abs(hv - 1.0) <= 1e-16:
+                break
+            v *= hv
+        f[i] = v
+        j, q = i, p
+        while True:
+            j *= 2
+            if j > n:
+                break
+            f[j] = H(q) * f[j // 2]
+            q *= 2.0
+    return f
+
+
+def psolver_periodic(rho, h, offset=0.0):
+    """Hartree potential and energy of rho (n3, n2, n1; x fastest) on a
+    periodic grid of spacings h, the reference's periodic PSolver restated
+    with numpy FFTs (Periodic_Kernel, Build_Kernel.f90:16-197; P_multkernel_NO,
+    PSolver_Base_new.f90:2515-2640: V^ = rho^ phi^x phi^y phi^z / (pi g^2),
+    V^(0) = offset / h^3; scal = 1/N, createKernel.f90:299; energy
+    0.5 sum(rho V) h^3, PSolver_Main.f90:403)."""
+    rho = np.asarray(rho, np.float64)
+    n3, n2, n1 = rho.shape
+    L = (n1 * h[0], n2 * h[1], n3 * h[2])
+    fx, fy, fz = isf_fourier(n1 // 2), isf_fourier(n2 // 2), isf_fourier(n3 // 2)
+    k1 = np.arange(n1 // 2 + 1)
+    p2 = np.minimum(np.arange(n2), n2 - np.arange(n2))
+    p3 = np.minimum(np.arange(n3), n3 - np.arange(n3))
+    g = ((k1 / L[0])[None, None, :] ** 2 + (p2 / L[1])[None, :, None] ** 2 + (p3 / L[2])[:, None, None] ** 2)
+    fac = fx[None, None, k1] * fy[None, p2, None] * fz[p3, None, None]
+    g[0, 0, 0] = 1.0
+    z = np.fft.rfftn(rho) * fac / (np.pi * g)
+    z[0, 0, 0] = offset / (h[0] * h[1] * h[2])
+    V = np.fft.irfftn(z, s=rho.shape, axes=(0, 1, 2))
+    return V, 0.5 * float((rho * V).sum()) * h[0] * h[1] * h[2]
+
+
 # ---------------------------------------------------------------- reference pin
 def ref_magicfilter():
     """ctypes handle to the reference's own C magic filter, or None."""
