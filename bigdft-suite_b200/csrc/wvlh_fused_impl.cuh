@@ -286,6 +286,19 @@ __device__ __forceinline__ void cp_async_pair(T *dst, const T *src)
         asm volatile("cp.async.ca.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(src) : "memory");
 }
 
+// point-pair copy with zero fill: when !valid nothing is read (src must still be
+// a valid address) and the pair is set to zero
+template <class T>
+__device__ __forceinline__ void cp_async_pair_z(T *dst, const T *src, bool valid)
+{
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    const int n = valid ? 2 * (int)sizeof(T) : 0;
+    if constexpr (sizeof(T) == 4)
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(d), "l"(src), "r"(n) : "memory");
+    else
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 16, %2;\n" ::"r"(d), "l"(src), "r"(n) : "memory");
+}
+
 // load_plane through cp.async (A in shared memory); the caller waits
 template <class T>
 __device__ __forceinline__ void load_plane_async(T *A, int pitch, int rows, int cols, const T *g)
@@ -481,9 +494,22 @@ __global__ void __launch_bounds__(kZThreads, sizeof(T) == 4 ? 4 : 1) k2_zpencil(
     const bool inside = xc < W && yc < H;
     const size_t colofs = (size_t)yc * W + xc;
 
+    // column pairs (x, x + 1) of one tile row move as point pairs when the
+    // plane rows have even length (the scratch planes start on a pair)
+    const bool pairs = pair_rows(W, g);
+    constexpr int TP = TC / 2, ZP = kZThreads / TP;
+    const int pc = 2 * (threadIdx.x % TP), zp = threadIdx.x / TP;
+    const int xp = x0 + (pc % TX), yp = y0 + (pc / TX);
+    const bool pin = xp < W && yp < H;   // W even: x + 1 is inside too
+    const size_t pofs = (size_t)yp * W + xp;
+
     // load the tile: TC columns x G3 z' rows, zero outside the plane
-    for (int z = zs; z < d.G3; z += ZS)
-        cp_async_elem(A + z * TC + col, inside ? g + (size_t)z * plane + colofs : g, inside);
+    if (pairs) {
+        for (int z = zp; z < d.G3; z += ZP) cp_async_pair_z(A + z * TC + pc, pin ? g + (size_t)z * plane + pofs : g, pin);
+    } else {
+        for (int z = zs; z < d.G3; z += ZS)
+            cp_async_elem(A + z * TC + col, inside ? g + (size_t)z * plane + colofs : g, inside);
+    }
     cp_async_wait_all();
     __syncthreads();
     const LineGeom zg{TC, 1, TC, 1, TC};
@@ -533,8 +559,14 @@ __global__ void __launch_bounds__(kZThreads, sizeof(T) == 4 ? 4 : 1) k2_zpencil(
         T *t = A; A = B; B = t;                                   // result in A
     }
     __syncthreads();
-    if (inside)
+    if (pairs) {
+        using V = typename Pair<T>::type;
+        if (pin)
+            for (int z = zp; z < d.G3; z += ZP)
+                *reinterpret_cast<V *>(gz + (size_t)z * plane + pofs) = *reinterpret_cast<const V *>(A + z * TC + pc);
+    } else if (inside) {
         for (int z = zs; z < d.G3; z += ZS) gz[(size_t)z * plane + colofs] = A[z * TC + col];
+    }
     const double s = block_sum(e, red);
     if (threadIdx.x == 0 && part_kin)
         (chain == 0 ? part_pot : part_kin)[(size_t)oi * part_stride + jj] = s;
