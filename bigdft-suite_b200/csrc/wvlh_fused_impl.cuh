@@ -525,22 +525,44 @@ __global__ void __launch_bounds__(kZThreads, sizeof(T) == 4 ? 4 : 1) k2_zpencil(
         const TV *V = o.pot_ptr ? (const TV *)o.pot_ptr : pot + o.pot;
         T ep = T(0);
         constexpr int U = 4;   // potential loads in flight per thread
-        const TV *vc = V + colofs;   // chain 0: W, H are I1, I2, the potential's plane
-        for (int z0 = zs; z0 < d.I3; z0 += U * ZS) {
-            T v[U];
+        // thread t takes the column pair (x, x + 1) of pair index t % (TC/2) at
+        // z = t / (TC/2) + k ZP; the potential comes as a point pair when the
+        // rows are even and the buffer starts on a pair, else point by point.
+        // The arithmetic, and so the energy's summation order, is the same
+        // either way (it does not depend on where the potential lives).
+        using VV = typename Pair<TV>::type;
+        using P2 = typename Pair<T>::type;
+        const bool vpair = pairs && pair_rows(W, V);
+        const bool in0 = xp < W && yp < H, in1 = xp + 1 < W && yp < H;
+        const TV *vp = V + pofs;
+        for (int z0 = zp; z0 < d.I3; z0 += U * ZP) {
+            VV v[U];
 #pragma unroll
             for (int u = 0; u < U; ++u) {
-                const int z = z0 + u * ZS;
-                v[u] = (inside && z < d.I3) ? (T)vc[(size_t)z * plane] : T(0);
+                const int z = z0 + u * ZP;
+                v[u].x = TV(0);
+                v[u].y = TV(0);
+                if (z < d.I3) {
+                    if (vpair) {
+                        if (in0) v[u] = *reinterpret_cast<const VV *>(vp + (size_t)z * plane);
+                    } else {
+                        if (in0) v[u].x = vp[(size_t)z * plane];
+                        if (in1) v[u].y = vp[(size_t)z * plane + 1];
+                    }
+                }
             }
 #pragma unroll
             for (int u = 0; u < U; ++u) {
-                const int z = z0 + u * ZS;
+                const int z = z0 + u * ZP;
                 if (z < d.I3) {
-                    const T r = A[z * TC + col];
-                    const T wv = v[u] * r;
-                    if (inside) ep = fma(wv, r, ep);
-                    A[z * TC + col] = inside ? wv : T(0);
+                    P2 *a = reinterpret_cast<P2 *>(A + z * TC + pc);
+                    P2 r = *a;
+                    const T w0 = (T)v[u].x * r.x, w1 = (T)v[u].y * r.y;
+                    if (in0) ep = fma(w0, r.x, ep);
+                    if (in1) ep = fma(w1, r.y, ep);
+                    r.x = in0 ? w0 : T(0);
+                    r.y = in1 ? w1 : T(0);
+                    *a = r;
                 }
             }
         }
@@ -807,8 +829,19 @@ __global__ void __launch_bounds__(kZThreads) kd_density(const LrDev *__restrict_
         const OrbDev o = orbs[orb];
         const T *g = scratch + o.sQ;
         __syncthreads();
-        for (int z = zs; z < d.G3; z += ZS)
-            cp_async_elem(A + z * TC + col, inside ? g + (size_t)z * plane + colofs : g, inside);
+        if (pair_rows(W, g)) {
+            // column pairs as point pairs (even plane rows)
+            constexpr int TP = TC / 2, ZP = kZThreads / TP;
+            const int pc = 2 * (threadIdx.x % TP), zp = threadIdx.x / TP;
+            const int xp = x0 + (pc % TX), yp = y0 + (pc / TX);
+            const bool pin = xp < W && yp < H;
+            const size_t pofs = (size_t)yp * W + xp;
+            for (int z = zp; z < d.G3; z += ZP)
+                cp_async_pair_z(A + z * TC + pc, pin ? g + (size_t)z * plane + pofs : g, pin);
+        } else {
+            for (int z = zs; z < d.G3; z += ZS)
+                cp_async_elem(A + z * TC + col, inside ? g + (size_t)z * plane + colofs : g, inside);
+        }
         cp_async_wait_all();
         __syncthreads();
         pass_syn<T, SEG>(A, B, zg, d.N3, d.N3, d.p3);                  // S_z
