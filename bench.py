@@ -46,7 +46,7 @@ def parse():
     ap.add_argument("--n", type=int, default=48)
     ap.add_argument("--norb", type=int, default=256)
     ap.add_argument("--no-extras", action="store_true", help="skip comparator / e2e / cpu / other-row legs")
-    ap.add_argument("--leg", default=None, choices=["free_bc", "precond", "overlap", "nlpsp", "psolver", "serve32", "serve64"],
+    ap.add_argument("--leg", default=None, choices=["free_bc", "precond", "overlap", "nlpsp", "psolver", "conv_check", "serve32", "serve64"],
                     help="run one extra leg alone (one GPU) and print its result as one JSON line")
     return ap.parse_args()
 
@@ -370,6 +370,70 @@ def leg_psolver(torch, ctx, dev, n=96, h=0.225):
     return out
 
 
+# the reference's OpenCL conv_check run (bigdft/tests/libs/OpenCL/OpenCL.ref.yaml, fort.1 =
+# "76 92 130 2", FP64): its published CPU / GPU milliseconds per operation, unnamed hardware
+CONV_CHECK_REF = {
+    "magicfilter1d 76 x 11960": (17.09, 3.82), "magicfilter1d_t 76 x 11960": (17.04, 3.80),
+    "kinetic1d 76 x 11960": (151.47, 12.00), "ana1d 76 x 11960": (21.02, 4.48),
+    "syn1d 76 x 11960": (21.99, 4.59), "magic_filter_3d 76x92x130": (48.25, 11.19),
+    "magic_filter_t_3d 76x92x130": (50.33, 11.37), "potential_3d 76x92x130": (106.31, 23.76),
+    "kinetic_3d 76x92x130": (149.56, 28.18), "ana_3d 76x92x130": (66.95, 13.50),
+    "syn_3d 76x92x130": (67.50, 12.73),
+}
+
+
+def leg_conv_check(torch, reps=20):
+    """The drop-in per-operation kernels (ocl_* ABI, FP64) on the sizes of the
+    reference's conv_check benchmark, beside its published numbers."""
+    import ctypes as C
+    import numpy as np
+    from wvlh import ocl
+    q = ocl.OclQueue(0)
+    n1, n2, n3 = 76, 92, 130
+    npt = n1 * n2 * n3
+    rng = np.random.default_rng(3)
+    bufs = [q.buffer(8 * npt) for _ in range(6)]
+    for b in bufs[:2]:
+        q.write(b, rng.uniform(-1, 1, npt))
+    a, b, t1, t2, w1, w2 = bufs
+    dims = (ocl.u32 * 3)(n1 // 2, n2 // 2, n3 // 2)
+    per = (ocl.u32 * 3)(1, 1, 1)
+    h = (C.c_double * 3)(0.2, 0.2, 0.2)
+    e = (C.c_double * 2)()
+    c0 = C.c_double(0.0)
+    h1 = C.c_double(0.2)
+    ops = {
+        "magicfilter1d 76 x 11960": ("magicfilter1d_d_", (ocl._u(n1), ocl._u(n2 * n3), a.ref, b.ref)),
+        "magicfilter1d_t 76 x 11960": ("magicfilter1d_t_d_", (ocl._u(n1), ocl._u(n2 * n3), a.ref, b.ref)),
+        "kinetic1d 76 x 11960": ("kinetic1d_d_", (ocl._u(n1), ocl._u(n2 * n3), C.byref(h1), C.byref(c0), a.ref,
+                                                  b.ref, w1.ref, w2.ref, e)),
+        "ana1d 76 x 11960": ("ana1d_d_", (ocl._u(n1 // 2), ocl._u(n2 * n3), a.ref, b.ref)),
+        "syn1d 76 x 11960": ("syn1d_d_", (ocl._u(n1 // 2), ocl._u(n2 * n3), a.ref, b.ref)),
+        "magic_filter_3d 76x92x130": ("magic_filter_3d_generic_", (dims, per, t1.ref, t2.ref, a.ref, b.ref)),
+        "magic_filter_t_3d 76x92x130": ("magic_filter_t_3d_generic_", (dims, per, t1.ref, t2.ref, a.ref, b.ref)),
+        "potential_3d 76x92x130": ("potential_application_d_generic_", (dims, per, t1.ref, t2.ref, a.ref, b.ref,
+                                                                         w1.ref, e)),
+        "kinetic_3d 76x92x130": ("kinetic_d_generic_", (dims, per, h, a.ref, b.ref, w1.ref, w2.ref)),
+        "ana_3d 76x92x130": ("ana_self_d_generic_", (dims, per, a.ref, b.ref)),
+        "syn_3d 76x92x130": ("syn_self_d_generic_", (dims, per, a.ref, b.ref)),
+    }
+    out = {}
+    for name, (fn, args) in ops.items():
+        for _ in range(3):
+            q.call(fn, *args)
+        q.finish()
+        t = time.perf_counter()
+        for _ in range(reps):
+            q.call(fn, *args)
+        q.finish()
+        ms = (time.perf_counter() - t) * 1e3 / reps
+        cpu, gpu = CONV_CHECK_REF[name]
+        out[name] = {"ms": ms, "ref_cpu_ms": cpu, "ref_gpu_ms": gpu}
+    q.close()
+    return {"workload": "conv_check sizes, FP64, wall time per call over %d calls (launch included)" % reps,
+            "ops": out}
+
+
 def leg_serve(torch, dev, precision, nreq=300, loads=(0.3, 0.5, 0.7)):
     """Serving loop: 64 clients (coarse 16..64 per dim, periodic or free, 4..128
     orbitals), requests 50/50 Hpsi and density; capacity from a burst of one
@@ -433,6 +497,8 @@ def main():
             res = leg_free_regions(torch, ctx, dev)
         elif args.leg == "precond":
             res = leg_precond(torch, ctx, dev)
+        elif args.leg == "conv_check":
+            res = leg_conv_check(torch)
         elif args.leg == "psolver":
             res = leg_psolver(torch, ctx, dev)
         elif args.leg == "nlpsp":
@@ -611,6 +677,7 @@ def main():
         extras["overlap"] = leg_overlap(torch, ctx, psi64, norb)
         extras["nlpsp"] = leg_nlpsp(torch, ctx, psi64, lr, norb)
         extras["psolver"] = leg_psolver(torch, ctx, dev)
+        extras["conv_check"] = leg_conv_check(torch)
         del hp, hv, hh
         extras["free_bc"] = leg_free_regions(torch, ctx, dev)
         extras["precond"] = leg_precond(torch, ctx, dev)
