@@ -348,23 +348,36 @@ def leg_nlpsp(torch, ctx, psi64, lr, norb, natoms=64, seed=21):
 
 
 def leg_psolver(torch, ctx, dev, n=96, h=0.225):
-    """Hartree potential of a seeded density on the periodic 96^3 ISF grid of
-    the batched workload (the potential step that follows the density):
-    wvlh_psolver_periodic (cuFFT and the ISF kernel multiply, FP64) against
-    the oracle's numpy restatement on the host."""
+    """The potential step that follows the density, on the periodic 96^3 ISF
+    grid of the batched workload (seeded positive density, FP64): the Hartree
+    potential (wvlh_psolver_periodic: cuFFT and the ISF kernel multiply), the
+    Kohn-Sham potential V_H + V_ext + V_xc with its three energies
+    (wvlh_ks_potential_periodic) and the LDA alone (wvlh_xc_lda, 16 bytes a
+    point), against the oracle's numpy restatement on the host."""
     import numpy as np
-    from wvlh.psolver import hartree_periodic
+    from wvlh.psolver import hartree_periodic, ks_potential_periodic, xc_lda
     rng = np.random.default_rng(5)
-    rho_h = rng.uniform(-1, 1, (n, n, n))
+    rho_h = rng.uniform(1e-3, 1, (n, n, n))
+    vext_h = rng.uniform(-1, 1, (n, n, n))
     rho = torch.tensor(rho_h, device=dev)
+    vext = torch.tensor(vext_h, device=dev)
     pot = torch.empty_like(rho)
-    ms = _timed(torch, lambda: hartree_periodic(ctx, rho, (h, h, h), pot=pot), 10)
-    out = {"workload": "%d^3 periodic grid, h %.3f bohr, FP64" % (n, h), "ms": ms}
+    hh = (h, h, h)
+    ms = _timed(torch, lambda: hartree_periodic(ctx, rho, hh, pot=pot), 10)
+    ks_ms = _timed(torch, lambda: ks_potential_periodic(ctx, rho, hh, vext=vext, pot=pot), 10)
+    xc_ms = _timed(torch, lambda: xc_lda(ctx, rho, vxc=pot, dvol=h ** 3), 10)
+    out = {"workload": "%d^3 periodic grid, h %.3f bohr, FP64" % (n, h), "ms": ms,
+           "ks_potential_ms": ks_ms, "xc_lda_ms": xc_ms,
+           "xc_lda_gbs": 16.0 * n ** 3 / (xc_ms * 1e-3) / 1e9}
     try:
+        from oracle import ks_potential_periodic as ks_cpu
         from oracle import psolver_periodic
         t = time.perf_counter()
-        psolver_periodic(rho_h, (h, h, h))
+        psolver_periodic(rho_h, hh)
         out["cpu_oracle_ms"] = (time.perf_counter() - t) * 1e3
+        t = time.perf_counter()
+        ks_cpu(rho_h, hh, vext_h)
+        out["cpu_oracle_ks_ms"] = (time.perf_counter() - t) * 1e3
     except Exception as e:  # the oracle is optional on the bench box
         out["cpu_oracle"] = "unavailable: %s" % e
     return out

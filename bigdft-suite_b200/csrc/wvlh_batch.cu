@@ -114,6 +114,7 @@ extern "C" int wvlh_ctx_destroy(wvlh_ctx *ctx)
             cudaStreamSynchronize(st);
             cudaStreamDestroy(st);
         }
+    psolver_release(ctx);
     delete ctx;
     return WVLH_OK;
 }

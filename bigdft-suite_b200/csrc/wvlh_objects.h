@@ -39,6 +39,12 @@ struct DevBuf {
 
 }  // namespace wvlh
 
+struct wvlh_ctx;
+namespace wvlh {
+// frees the Poisson solver's plans and buffers of a context (wvlh_psolver.cu)
+void psolver_release(const wvlh_ctx *ctx);
+}  // namespace wvlh
+
 // the C ABI's opaque handles (global names, as include/wvlh.h declares them)
 struct wvlh_ctx {
     int device = 0;

@@ -19,6 +19,13 @@
 // FFTs are cuFFT (D2Z / Z2D, plans cached per grid); the kernel multiply, with
 // the folded frequencies and the three 1D ISF factors, and the deterministic
 // energy reduction are this file's kernels.
+//
+// The exchange-correlation part of the Kohn-Sham potential is the reference's
+// default LDA (ixc = 1: the Goedecker-Teter-Hutter Pade fit of the
+// Ceperley-Alder data, Phys. Rev. B 54, 1703 (1996); ABINIT's xcspol,
+// libABINIT/src/abi_xc_lowlevel/abi_xcspol.F90:105-250), spin-unpolarised,
+// evaluated point by point in the same pass that adds V_H, V_ext and V_xc
+// (updatePotential, bigdft/src/modules/rhopotential.f90:29-125).
 #include <cuda_runtime.h>
 #include <cufft.h>
 
@@ -137,6 +144,98 @@ __global__ void k_ps_sum(int n, const double *__restrict__ part, double scale, d
     if (threadIdx.x == 0) *out = t * scale;
 }
 
+// Teter 1993 paramagnetic parameters (abi_xcspol.F90:105-112) and
+// rs = (3 / (4 pi rho))^(1/3) = rsfac rho^(-1/3) (abi_drivexc.F90:134, 213-224)
+struct Teter93 {
+    static constexpr double a0 = 0.4581652932831429, a1 = 2.217058676663745, a2 = 0.7405551735357053,
+                            a3 = 0.01968227878617998;
+    static constexpr double b1 = 1.0, b2 = 4.504130959426697, b3 = 1.110667363742916, b4 = 0.02359291751427506;
+    static constexpr double rsfac = 0.6203504908994000;
+};
+
+// eps_xc and v_xc = d(rho eps_xc)/d rho of the total density rho (xcspol,
+// nspden = 1, order 1: :229-250); rs keeps the sign of rho as abi_invcb does
+__device__ __forceinline__ void teter_lda(double rho, double &eps, double &v)
+{
+    using T = Teter93;
+    const double rs = T::rsfac * copysign(rcbrt(fabs(rho)), rho);
+    const double n1 = T::a0 + rs * (T::a1 + rs * (T::a2 + rs * T::a3));
+    const double d1 = rs * (T::b1 + rs * (T::b2 + rs * (T::b3 + rs * T::b4)));
+    const double d1m1 = 1.0 / d1;
+    eps = -n1 * d1m1;
+    const double dn1 = T::a1 + rs * (2.0 * T::a2 + rs * (3.0 * T::a3));
+    const double dd1 = T::b1 + rs * (2.0 * T::b2 + rs * (3.0 * T::b3 + rs * (4.0 * T::b4)));
+    const double deps = -(dn1 + eps * dd1) * d1m1;
+    v = eps - (1.0 / 3.0) * rs * deps;
+}
+
+// V_xc of every point (written, or added when ACC), per-block partial sums of
+// eps rho and v rho (xc_energy_new, orbitals/xc.f90:888-917) in part[2 b + 0/1]
+template <bool ACC>
+__global__ void k_xc_lda(long long n, const double *__restrict__ rho, double *__restrict__ vxc,
+                         double *__restrict__ part)
+{
+    __shared__ double red[32];
+    double se = 0.0, sv = 0.0;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        const double r = rho[i];
+        double e, v;
+        teter_lda(r, e, v);
+        se = fma(e, r, se);
+        sv = fma(v, r, sv);
+        vxc[i] = ACC ? vxc[i] + v : v;
+    }
+    const double te = block_sum(se, red);
+    const double tv = block_sum(sv, red);
+    if (threadIdx.x == 0) {
+        part[2 * blockIdx.x] = te;
+        part[2 * blockIdx.x + 1] = tv;
+    }
+}
+
+// the Kohn-Sham potential from V_H (in pot): pot = (V_H + V_ext) + V_xc, the
+// order of H_potential's sum with pot_ion then updatePotential's axpy of V_XC;
+// per-block partials of rho V_H, eps rho, v rho in part[3 b + 0/1/2]
+__global__ void k_ks_combine(long long n, const double *__restrict__ rho, const double *__restrict__ vext,
+                             double *__restrict__ pot, double *__restrict__ part)
+{
+    __shared__ double red[32];
+    double sh = 0.0, se = 0.0, sv = 0.0;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        const double r = rho[i], vh = pot[i];
+        double e, v;
+        teter_lda(r, e, v);
+        sh = fma(vh, r, sh);
+        se = fma(e, r, se);
+        sv = fma(v, r, sv);
+        pot[i] = (vext ? vh + vext[i] : vh) + v;
+    }
+    const double th = block_sum(sh, red);
+    const double te = block_sum(se, red);
+    const double tv = block_sum(sv, red);
+    if (threadIdx.x == 0) {
+        part[3 * blockIdx.x] = th;
+        part[3 * blockIdx.x + 1] = te;
+        part[3 * blockIdx.x + 2] = tv;
+    }
+}
+
+// out[k] = scale[k] * sum over blocks of part[K b + k], blocks in a fixed order
+template <int K>
+__global__ void k_ps_sum_k(int nblk, const double *__restrict__ part, double s0, double s1, double s2,
+                           double *__restrict__ out)
+{
+    __shared__ double red[32];
+    const double sc[3] = {s0, s1, s2};
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+        double s = 0.0;
+        for (int i = threadIdx.x; i < nblk; i += blockDim.x) s += part[K * i + k];
+        const double t = block_sum(s, red);
+        if (threadIdx.x == 0) out[k] = t * sc[k];
+    }
+}
+
 struct PsPlan {
     cufftHandle fwd = 0, inv = 0;
     DevBuf spec, fac, part;
@@ -151,25 +250,45 @@ using namespace wvlh;
 static std::mutex g_ps_mutex;
 static std::map<std::tuple<const void *, int, int, int, int>, PsPlan *> g_ps_plans;
 
-extern "C" int wvlh_psolver_periodic(wvlh_ctx *ctx, const int n[3], const double h[3], const double *rho,
-                                     double *pot, double offset, double *eh)
+namespace wvlh {
+// the plans and buffers of a context, at its destruction (its stream is idle)
+void psolver_release(const wvlh_ctx *ctx)
 {
-    // the energy needs rho after the potential is written: no aliasing then
-    if (!ctx || !n || !h || !rho || !pot || (eh && pot == rho)) {
-        set_last_error(WVLH_ERR_ARG);
-        return WVLH_ERR_ARG;
-    }
-    for (int k = 0; k < 3; ++k)
-        if (n[k] < 16 || n[k] % 2 || !(h[k] > 0.0)) {   // the ISF needs 16 points, the kernel even sizes
-            set_last_error(WVLH_ERR_ARG);
-            return WVLH_ERR_ARG;
+    std::lock_guard<std::mutex> lock(g_ps_mutex);
+    for (auto it = g_ps_plans.begin(); it != g_ps_plans.end();) {
+        if (std::get<0>(it->first) != (const void *)ctx) {
+            ++it;
+            continue;
         }
-    if (cudaSetDevice(ctx->device) != cudaSuccess) {
-        set_last_error(WVLH_ERR_CUDA);
-        return WVLH_ERR_CUDA;
+        PsPlan *pl = it->second;
+        if (pl->fwd) cufftDestroy(pl->fwd);
+        if (pl->inv) cufftDestroy(pl->inv);
+        pl->spec.release();
+        pl->fac.release();
+        pl->part.release();
+        delete pl;
+        it = g_ps_plans.erase(it);
     }
+}
+}  // namespace wvlh
+
+static const int kPsBlocks = 1184;   // 8 per SM on 148 SMs
+
+static bool ps_args_ok(const int n[3], const double h[3])
+{
+    for (int k = 0; k < 3; ++k)
+        if (n[k] < 16 || n[k] % 2 || !(h[k] > 0.0)) return false;   // the ISF needs 16 points, the kernel even sizes
+    return true;
+}
+
+// V_H of rho into pot (D2Z, kernel multiply, Z2D on the context's stream);
+// returns the grid's plan (its part buffer holds kPsBlocks * 3 doubles)
+static int ps_hartree(wvlh_ctx *ctx, const int n[3], const double h[3], const double *rho, double *pot,
+                      double offset, PsPlan **out)
+{
+    if (cudaSetDevice(ctx->device) != cudaSuccess) return WVLH_ERR_CUDA;
     const int n1 = n[0], n2 = n[1], n3 = n[2];
-    const long long npt = (long long)n1 * n2 * n3, nc = (long long)n3 * n2 * (n1 / 2 + 1);
+    const long long nc = (long long)n3 * n2 * (n1 / 2 + 1);
     PsPlan *pl;
     {
         std::lock_guard<std::mutex> lock(g_ps_mutex);
@@ -178,13 +297,9 @@ extern "C" int wvlh_psolver_periodic(wvlh_ctx *ctx, const int n[3], const double
         if (it == g_ps_plans.end()) {
             // cuFFT's last dimension is the fastest: (n3, n2, n1) for x-fastest arrays
             cufftHandle f = 0, b = 0;
-            if (cufftPlan3d(&f, n3, n2, n1, CUFFT_D2Z) != CUFFT_SUCCESS) {
-                set_last_error(WVLH_ERR_CUDA);
-                return WVLH_ERR_CUDA;
-            }
+            if (cufftPlan3d(&f, n3, n2, n1, CUFFT_D2Z) != CUFFT_SUCCESS) return WVLH_ERR_CUDA;
             if (cufftPlan3d(&b, n3, n2, n1, CUFFT_Z2D) != CUFFT_SUCCESS) {
                 cufftDestroy(f);
-                set_last_error(WVLH_ERR_CUDA);
                 return WVLH_ERR_CUDA;
             }
             PsPlan *np = new PsPlan();
@@ -195,13 +310,10 @@ extern "C" int wvlh_psolver_periodic(wvlh_ctx *ctx, const int n[3], const double
         pl = it->second;
     }
     int rc;
-    const int nblk = 1184;   // 8 per SM on 148 SMs
     if ((rc = pl->spec.ensure(sizeof(cufftDoubleComplex) * (size_t)nc)) ||
         (rc = pl->fac.ensure(sizeof(double) * (size_t)(n1 / 2 + n2 / 2 + n3 / 2 + 3))) ||
-        (rc = pl->part.ensure(sizeof(double) * (size_t)(nblk + 1)))) {
-        set_last_error(rc);
+        (rc = pl->part.ensure(sizeof(double) * (size_t)(3 * kPsBlocks + 3))))
         return rc;
-    }
     std::vector<double> fx, fy, fz;
     fourtrans_isf(n1 / 2, fx);
     fourtrans_isf(n2 / 2, fy);
@@ -219,20 +331,84 @@ extern "C" int wvlh_psolver_periodic(wvlh_ctx *ctx, const int n[3], const double
     const double vol = h[0] * h[1] * h[2];
     const double scal = 1.0 / ((double)n1 * (double)n2 * (double)n3);
     if (ok) {
-        k_ps_multiply<<<nblk, 256, 0, st>>>(n1, n2, n3, n1 * h[0], n2 * h[1], n3 * h[2], d_fac, d_fac + fx.size(),
-                                            d_fac + fx.size() + fy.size(), scal, offset / vol * scal, z);
+        k_ps_multiply<<<kPsBlocks, 256, 0, st>>>(n1, n2, n3, n1 * h[0], n2 * h[1], n3 * h[2], d_fac,
+                                                 d_fac + fx.size(), d_fac + fx.size() + fy.size(), scal,
+                                                 offset / vol * scal, z);
         ok = cudaGetLastError() == cudaSuccess;
     }
     if (ok) ok = cufftExecZ2D(pl->inv, z, (cufftDoubleReal *)pot) == CUFFT_SUCCESS;
-    if (ok && eh) {
+    if (!ok) return WVLH_ERR_CUDA;
+    *out = pl;
+    return WVLH_OK;
+}
+
+static int ps_fail(int rc)
+{
+    set_last_error(rc);
+    return rc;
+}
+
+extern "C" int wvlh_psolver_periodic(wvlh_ctx *ctx, const int n[3], const double h[3], const double *rho,
+                                     double *pot, double offset, double *eh)
+{
+    // the energy needs rho after the potential is written: no aliasing then
+    if (!ctx || !n || !h || !rho || !pot || (eh && pot == rho) || !ps_args_ok(n, h)) return ps_fail(WVLH_ERR_ARG);
+    PsPlan *pl = nullptr;
+    int rc = ps_hartree(ctx, n, h, rho, pot, offset, &pl);
+    if (rc) return ps_fail(rc);
+    if (eh) {
+        const long long npt = (long long)n[0] * n[1] * n[2];
         double *part = (double *)pl->part.p;
-        k_ps_dot<<<nblk, 256, 0, st>>>(npt, rho, pot, part);
-        k_ps_sum<<<1, 1024, 0, st>>>(nblk, part, 0.5 * vol, eh);
-        ok = cudaGetLastError() == cudaSuccess;
+        k_ps_dot<<<kPsBlocks, 256, 0, ctx->stream>>>(npt, rho, pot, part);
+        k_ps_sum<<<1, 1024, 0, ctx->stream>>>(kPsBlocks, part, 0.5 * h[0] * h[1] * h[2], eh);
+        if (cudaGetLastError() != cudaSuccess) return ps_fail(WVLH_ERR_CUDA);
     }
-    if (!ok) {
-        set_last_error(WVLH_ERR_CUDA);
-        return WVLH_ERR_CUDA;
+    return WVLH_OK;
+}
+
+extern "C" int wvlh_xc_lda(wvlh_ctx *ctx, int64_t npts, const double *rho, double *vxc, int accumulate, double dvol,
+                           double *energies)
+{
+    // each point is read before its own V_xc is written: vxc may be rho
+    if (!ctx || npts < 0 || (npts > 0 && (!rho || !vxc))) return ps_fail(WVLH_ERR_ARG);
+    if (cudaSetDevice(ctx->device) != cudaSuccess) return ps_fail(WVLH_ERR_CUDA);
+    if (npts == 0 && !energies) return WVLH_OK;
+    // the partials live in the context's grid-independent entry, key (0, 0, 0)
+    PsPlan *pl;
+    {
+        std::lock_guard<std::mutex> lock(g_ps_mutex);
+        const auto key = std::make_tuple((const void *)ctx, ctx->device, 0, 0, 0);
+        auto it = g_ps_plans.find(key);
+        if (it == g_ps_plans.end()) it = g_ps_plans.emplace(key, new PsPlan()).first;
+        pl = it->second;
     }
+    int rc = pl->part.ensure(sizeof(double) * (size_t)(3 * kPsBlocks + 3));
+    if (rc) return ps_fail(rc);
+    double *part = (double *)pl->part.p;
+    cudaStream_t st = ctx->stream;
+    if (accumulate)
+        k_xc_lda<true><<<kPsBlocks, 256, 0, st>>>(npts, rho, vxc, part);
+    else
+        k_xc_lda<false><<<kPsBlocks, 256, 0, st>>>(npts, rho, vxc, part);
+    if (energies) k_ps_sum_k<2><<<1, 1024, 0, st>>>(kPsBlocks, part, dvol, dvol, 0.0, energies);
+    if (cudaGetLastError() != cudaSuccess) return ps_fail(WVLH_ERR_CUDA);
+    return WVLH_OK;
+}
+
+extern "C" int wvlh_ks_potential_periodic(wvlh_ctx *ctx, const int n[3], const double h[3], const double *rho,
+                                          const double *vext, double *pot, double *energies)
+{
+    // the combine pass reads rho and V_ext after V_H is written to pot
+    if (!ctx || !n || !h || !rho || !pot || pot == rho || (vext && vext == pot) || !ps_args_ok(n, h))
+        return ps_fail(WVLH_ERR_ARG);
+    PsPlan *pl = nullptr;
+    int rc = ps_hartree(ctx, n, h, rho, pot, 0.0, &pl);
+    if (rc) return ps_fail(rc);
+    const long long npt = (long long)n[0] * n[1] * n[2];
+    const double dvol = h[0] * h[1] * h[2];
+    double *part = (double *)pl->part.p;
+    k_ks_combine<<<kPsBlocks, 256, 0, ctx->stream>>>(npt, rho, vext, pot, part);
+    if (energies) k_ps_sum_k<3><<<1, 1024, 0, ctx->stream>>>(kPsBlocks, part, 0.5 * dvol, dvol, dvol, energies);
+    if (cudaGetLastError() != cudaSuccess) return ps_fail(WVLH_ERR_CUDA);
     return WVLH_OK;
 }

@@ -79,6 +79,8 @@ WVLH_SYMBOLS = [
     "wvlh_locham_graph_create", "wvlh_graph_launch", "wvlh_graph_destroy",
     "wvlh_nlpsp_create", "wvlh_nlpsp_apply", "wvlh_nlpsp_destroy", "wvlh_subspace_matrix",
     "wvlh_psolver_periodic",
+    "wvlh_xc_lda",
+    "wvlh_ks_potential_periodic",
 ]
 
 
@@ -139,6 +141,8 @@ def lib():
     L.wvlh_nlpsp_destroy.argtypes = [vp]
     L.wvlh_subspace_matrix.argtypes = [vp, C.c_int, C.c_int, C.c_int64, C.c_int64, vp, vp, vp]
     L.wvlh_psolver_periodic.argtypes = [vp, C.POINTER(C.c_int), C.POINTER(C.c_double), vp, vp, C.c_double, vp]
+    L.wvlh_xc_lda.argtypes = [vp, C.c_int64, vp, vp, C.c_int, C.c_double, vp]
+    L.wvlh_ks_potential_periodic.argtypes = [vp, C.POINTER(C.c_int), C.POINTER(C.c_double), vp, vp, vp, vp]
     L.wvlh_host_alloc.restype = vp
     L.wvlh_host_alloc.argtypes = [C.c_size_t]
     L.wvlh_host_free.argtypes = [vp]

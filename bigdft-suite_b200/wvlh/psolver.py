@@ -1,7 +1,10 @@
-"""Hartree potential on a periodic real-space grid (the reference's PSolver
-with periodic boundary conditions, order-16 interpolating scaling functions):
-wvlh_psolver_periodic on the device (cuFFT transforms, the library's kernel
-multiply and energy reduction)."""
+"""The potential from the density: the Hartree potential on a periodic
+real-space grid (the reference's PSolver with periodic boundary conditions,
+order-16 interpolating scaling functions; wvlh_psolver_periodic: cuFFT
+transforms, the library's kernel multiply and energy reduction), the
+exchange-correlation potential of the reference's default LDA (ixc = 1,
+wvlh_xc_lda) and their sum with an external potential, the Kohn-Sham potential
+of updatePotential (wvlh_ks_potential_periodic)."""
 import ctypes as C
 
 from ._lib import WvlhError, check, lib
@@ -26,3 +29,54 @@ def hartree_periodic(ctx, rho, h, offset=0.0, pot=None, energy=True):
                                       float(offset), C.c_void_p(eh.data_ptr()) if energy else None),
           "wvlh_psolver_periodic")
     return pot, eh
+
+
+def _check_rho(ctx, rho):
+    torch = ctx.torch
+    if rho.dtype != torch.float64 or not rho.is_contiguous() or not rho.is_cuda:
+        raise WvlhError("rho: contiguous float64 device tensor")
+
+
+def xc_lda(ctx, rho, vxc=None, accumulate=False, dvol=1.0, energy=True):
+    """V_xc of the total density rho (any shape) for the Teter 1993 LDA
+    (ixc = 1, spin-unpolarised): written into vxc (a new tensor unless given;
+    added to it when accumulate).  Returns (vxc, energies), energies a
+    (2,) device tensor (exc, evxc) = dvol * (sum eps rho, sum v_xc rho), or
+    None without energy."""
+    torch = ctx.torch
+    _check_rho(ctx, rho)
+    if vxc is None:
+        if accumulate:
+            raise WvlhError("accumulate needs vxc")
+        vxc = torch.empty_like(rho)
+    if vxc.shape != rho.shape or vxc.dtype != torch.float64 or not vxc.is_contiguous():
+        raise WvlhError("vxc: a tensor like rho")
+    en = torch.empty(2, dtype=torch.float64, device=rho.device) if energy else None
+    check(lib().wvlh_xc_lda(ctx.h, rho.numel(), C.c_void_p(rho.data_ptr()), C.c_void_p(vxc.data_ptr()),
+                            1 if accumulate else 0, float(dvol), C.c_void_p(en.data_ptr()) if energy else None),
+          "wvlh_xc_lda")
+    return vxc, en
+
+
+def ks_potential_periodic(ctx, rho, h, vext=None, pot=None, energy=True):
+    """pot = V_H[rho] + vext + V_xc[rho] on a periodic grid (rho: (n3, n2, n1)
+    float64 device tensor, x fastest; vext None or a tensor like rho).
+    Returns (pot, energies), energies a (3,) device tensor (eh, exc, evxc),
+    or None without energy."""
+    torch = ctx.torch
+    _check_rho(ctx, rho)
+    if rho.dim() != 3:
+        raise WvlhError("rho: (z, y, x) grid")
+    if pot is None:
+        pot = torch.empty_like(rho)
+    for name, t in (("pot", pot), ("vext", vext)):
+        if t is not None and (t.shape != rho.shape or t.dtype != torch.float64 or not t.is_contiguous()):
+            raise WvlhError("%s: a tensor like rho" % name)
+    n = (C.c_int * 3)(rho.shape[2], rho.shape[1], rho.shape[0])
+    hh = (C.c_double * 3)(*[float(v) for v in h])
+    en = torch.empty(3, dtype=torch.float64, device=rho.device) if energy else None
+    check(lib().wvlh_ks_potential_periodic(ctx.h, n, hh, C.c_void_p(rho.data_ptr()),
+                                           C.c_void_p(vext.data_ptr()) if vext is not None else None,
+                                           C.c_void_p(pot.data_ptr()), C.c_void_p(en.data_ptr()) if energy else None),
+          "wvlh_ks_potential_periodic")
+    return pot, en

@@ -370,6 +370,26 @@ int wvlh_nlpsp_destroy(wvlh_nlpsp *nl);
  * (PSolver_Main.f90:403).  FFTs by cuFFT, plans kept per context and grid. */
 int wvlh_psolver_periodic(wvlh_ctx *ctx, const int n[3], const double h[3], const double *rho, double *pot,
                           double offset, double *eh);
+/* Exchange-correlation potential of the reference's default functional
+ * (ixc = 1: the Goedecker-Teter-Hutter Pade LDA, ABINIT's xcspol,
+ * libABINIT/src/abi_xc_lowlevel/abi_xcspol.F90:105-250), spin-unpolarised,
+ * for npts points of the total density rho (DEVICE FP64, positive: the
+ * reference keeps it >= 1e-20): vxc[i] = v_xc(rho[i]), or vxc[i] += v_xc when
+ * accumulate (vxc may be rho).  energies (DEVICE double[2], or NULL):
+ * exc = dvol sum eps_xc rho, evxc = dvol sum v_xc rho (xc_energy_new,
+ * bigdft/src/orbitals/xc.f90:763-925).  Replaces XC_potential
+ * (xcPSolver/xcenergy.f90:428) for ixc = 1, nspin = 1, no core density. */
+int wvlh_xc_lda(wvlh_ctx *ctx, int64_t npts, const double *rho, double *vxc, int accumulate, double dvol,
+                double *energies);
+/* The Kohn-Sham potential of a periodic box from the total density (the
+ * reference's updatePotential, bigdft/src/modules/rhopotential.f90:29-125,
+ * nspin = 1, ixc = 1): pot = (V_H[rho] + vext) + V_xc[rho], V_H as
+ * wvlh_psolver_periodic with offset 0; vext may be NULL.  pot must not alias
+ * rho or vext.  energies (DEVICE double[3], or NULL): eh = 0.5 dvol sum rho
+ * V_H, exc, evxc.  One pass after the inverse FFT forms the sum and the three
+ * energies. */
+int wvlh_ks_potential_periodic(wvlh_ctx *ctx, const int n[3], const double h[3], const double *rho,
+                               const double *vext, double *pot, double *energies);
 /* FP64, one kernel per 1D pass (the OpenCL backend's structure) */
 int wvlh_locham_plain_batched(wvlh_batch *batch, const double *psi, const double *pot, double *hpsi,
                               double *ekin, double *epot);

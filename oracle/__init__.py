@@ -473,6 +473,50 @@ def psolver_periodic(rho, h, offset=0.0):
     return V, 0.5 * float((rho * V).sum()) * h[0] * h[1] * h[2]
 
 
+# Goedecker-Teter-Hutter Pade fit of the Ceperley-Alder LDA (Phys. Rev. B 54,
+# 1703 (1996), paramagnetic parameters; ixc = 1 of the reference, ABINIT's
+# xcspol, libABINIT/src/abi_xc_lowlevel/abi_xcspol.F90:105-112): eps_xc(rs) =
+# -(a0 + a1 rs + a2 rs^2 + a3 rs^3) / (b1 rs + b2 rs^2 + b3 rs^3 + b4 rs^4),
+# rs = (3 / (4 pi rho))^(1/3).
+TETER_A = (0.4581652932831429, 2.217058676663745, 0.7405551735357053, 0.01968227878617998)
+TETER_B = (1.0, 4.504130959426697, 1.110667363742916, 0.02359291751427506)
+RS_FAC = 0.6203504908994000     # (3 / (4 pi))^(1/3), abi_drivexc.F90:134
+
+
+def xc_lda(rho):
+    """(eps_xc, v_xc) of the total density rho (any shape), spin-unpolarised
+    (abi_xcspol nspden = 1, :229-250: exc = -n1/d1, vxc = exc - rs/3 d exc/d rs).
+    rs follows abi_drivexc (:213-224, rs = rsfac sign(|rho|^(-1/3), rho)); the
+    reference's abi_invcb reaches |rho|^(-1/3) by a Pade iteration stopped at a
+    relative residual of 1e-12, the oracle takes the cube root directly."""
+    rho = np.asarray(rho, np.float64)
+    a0, a1, a2, a3 = TETER_A
+    b1, b2, b3, b4 = TETER_B
+    rs = RS_FAC * np.sign(rho) * np.abs(rho) ** (-1.0 / 3.0)
+    n1 = a0 + rs * (a1 + rs * (a2 + rs * a3))
+    d1 = rs * (b1 + rs * (b2 + rs * (b3 + rs * b4)))
+    eps = -n1 / d1
+    dn1 = a1 + rs * (2.0 * a2 + rs * (3.0 * a3))
+    dd1 = b1 + rs * (2.0 * b2 + rs * (3.0 * b3 + rs * (4.0 * b4)))
+    deps = -(dn1 + eps * dd1) / d1
+    return eps, eps - rs / 3.0 * deps
+
+
+def ks_potential_periodic(rho, h, vext=None):
+    """The Kohn-Sham potential of a periodic box from the total density, as
+    updatePotential (bigdft/src/modules/rhopotential.f90:29-125) builds it for
+    nspin = 1 and ixc = 1: XC_potential (xcPSolver/xcenergy.f90:428; energies
+    xc_energy_new, orbitals/xc.f90:763-925: exc = dvol sum eps rho, evxc =
+    dvol sum v_xc rho), H_potential with V_ext summed in (offset 0), then
+    rhov += V_xc.  Returns (pot, (eh, exc, evxc))."""
+    rho = np.asarray(rho, np.float64)
+    vh, eh = psolver_periodic(rho, h)
+    eps, vxc = xc_lda(rho)
+    dvol = h[0] * h[1] * h[2]
+    pot = (vh if vext is None else vh + np.asarray(vext, np.float64)) + vxc   # H_potential's sum, then the axpy
+    return pot, (eh, float((eps * rho).sum()) * dvol, float((vxc * rho).sum()) * dvol)
+
+
 # ---------------------------------------------------------------- reference pin
 def ref_magicfilter():
     """ctypes handle to the reference's own C magic filter, or None."""

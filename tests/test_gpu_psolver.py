@@ -51,3 +51,72 @@ def test_rejects_odd_or_small_grids(torch_cuda, wctx):
     for shape in ((16, 16, 15), (8, 16, 16)):
         with pytest.raises(WvlhError):
             hartree_periodic(wctx, torch.zeros(shape, dtype=torch.float64, device="cuda"), (0.3, 0.3, 0.3))
+
+
+def test_reference_ps_check_periodic_golden(torch_cuda, wctx):
+    """The reference's own PS_Check periodic run (64^3, exp-cosine density):
+    the Hartree energy and the potential at (28, 28, 38) to its 13 printed
+    digits, the analytic potential to the reference's accuracy."""
+    from test_psolver_rule import PS_CHECK_EH, PS_CHECK_INF, PS_CHECK_V, ps_check_periodic
+    torch = torch_cuda
+    rho, V, h, off = ps_check_periodic()
+    pot, eh = hartree_periodic(wctx, torch.tensor(rho, device="cuda"), h, offset=off)
+    got = pot.cpu().numpy()
+    assert abs(eh.item() - PS_CHECK_EH) <= 5e-13 * PS_CHECK_EH
+    assert abs(got[37, 27, 27] - PS_CHECK_V) <= 5e-13 * abs(PS_CHECK_V)
+    assert np.abs(got - V).max() <= 2 * PS_CHECK_INF
+
+
+def test_xc_lda_matches_oracle_on_reference_test_density(oracle, torch_cuda, wctx):
+    from test_psolver_rule import xc_test_density
+    from wvlh.psolver import xc_lda
+    torch = torch_cuda
+    rho = 2.0 * xc_test_density()
+    eps, v = oracle.xc_lda(rho)
+    t = torch.tensor(rho, device="cuda")
+    vxc, en = xc_lda(wctx, t, dvol=1.0)
+    got = vxc.cpu().numpy()
+    assert np.abs(got - v).max() <= 1e-14 * np.abs(v).max()
+    e = en.cpu().numpy()
+    assert abs(e[0] - (eps * rho).sum()) <= 1e-13 * abs(e[0])
+    assert abs(e[1] - (v * rho).sum()) <= 1e-13 * abs(e[1])
+    # accumulate, and in place
+    acc = torch.full_like(t, 0.25)
+    xc_lda(wctx, t, vxc=acc, accumulate=True, energy=False)
+    assert np.abs(acc.cpu().numpy() - (0.25 + v)).max() <= 1e-14 * np.abs(v).max()
+    t2 = t.clone()
+    _, en2 = xc_lda(wctx, t2, vxc=t2)
+    assert torch.equal(t2, vxc) and torch.equal(en2, en)
+
+
+@pytest.mark.parametrize("n,h,ext", [((32, 32, 32), (0.3, 0.3, 0.3), True), ((48, 40, 36), (0.21, 0.25, 0.27), False),
+                                     ((96, 96, 96), (0.225, 0.225, 0.225), True)])
+def test_ks_potential_matches_oracle(oracle, torch_cuda, wctx, n, h, ext):
+    from wvlh.psolver import ks_potential_periodic
+    torch = torch_cuda
+    rng = np.random.default_rng(sum(n))
+    rho = rng.uniform(1e-4, 0.5, n[::-1])
+    vext = rng.uniform(-2, 2, n[::-1]) if ext else None
+    ref, (eh, exc, evxc) = oracle.ks_potential_periodic(rho, h, vext)
+    pot, en = ks_potential_periodic(wctx, torch.tensor(rho, device="cuda"), h,
+                                    vext=torch.tensor(vext, device="cuda") if ext else None)
+    got = pot.cpu().numpy()
+    assert np.abs(got - ref).max() <= 1e-13 * np.abs(ref).max()
+    e = en.cpu().numpy()
+    for a, b in zip(e, (eh, exc, evxc)):
+        assert abs(a - b) <= 1e-12 * abs(b)
+    # deterministic
+    pot2, en2 = ks_potential_periodic(wctx, torch.tensor(rho, device="cuda"), h,
+                                      vext=torch.tensor(vext, device="cuda") if ext else None)
+    assert torch.equal(pot, pot2) and torch.equal(en, en2)
+
+
+def test_ks_potential_rejects_aliasing(torch_cuda, wctx):
+    from wvlh.psolver import ks_potential_periodic
+    torch = torch_cuda
+    t = torch.full((16, 16, 16), 0.1, dtype=torch.float64, device="cuda")
+    with pytest.raises(WvlhError):
+        ks_potential_periodic(wctx, t, (0.3, 0.3, 0.3), pot=t)
+    v = torch.zeros_like(t)
+    with pytest.raises(WvlhError):
+        ks_potential_periodic(wctx, t, (0.3, 0.3, 0.3), vext=v, pot=v)

@@ -54,3 +54,100 @@ def test_uneven_grid_and_offset(oracle):
     # offset: the k = 0 term sets the mean of the potential to offset / volume
     got2, _ = oracle.psolver_periodic(rho, h, offset=3.0)
     assert abs(got2.mean() - 3.0 / np.prod(L)) <= 1e-12
+
+
+def ps_check_periodic():
+    """The periodic case of the reference's PS_Check test
+    (psolver/tests/PS_Check.f90:29-113, test_functions_new with f_exp_cosine of
+    frequency 2, psolver/tests/functions.f90:505-590, fill_functions_arrays
+    :411-434; atlab/src/f_functions.f90:435-455, 591-665): a 64^3 box of side
+    10 bohr, x = (i - 1) h - L/2, V = -4 pi f(x) f(y) f(z) with
+    f = exp(cos(2 pi x / L)), rho = lap(f(x) f(y) f(z)), offset = sum(V) h^3.
+    Arrays (z, y, x)."""
+    n, L = 64, 10.0
+    h = L / n
+    x = np.arange(n) * h - 0.5 * L
+    r = 2 * np.pi * x / L
+    f = np.exp(np.cos(r))
+    f2 = (2 * np.pi / L) ** 2 * (np.sin(r) ** 2 - np.cos(r)) * f
+    rho = (f2[None, None, :] * f[None, :, None] * f[:, None, None] + f[None, None, :] * f2[None, :, None] * f[:, None, None]
+           + f[None, None, :] * f[None, :, None] * f2[:, None, None])
+    V = -4 * np.pi * f[None, None, :] * f[None, :, None] * f[:, None, None]
+    return rho, V, (h, h, h), float(V.sum()) * h ** 3
+
+
+# psolver/tests/PS_Check.ref.yaml:224-233 (periodic, 64^3): the Hartree energy,
+# the largest difference from the analytic potential and the potential at
+# (28, 28, 38), 1-based (x, y, z)
+PS_CHECK_EH = 3.075484915324e04
+PS_CHECK_INF = 9.890754881781e-12
+PS_CHECK_V = -1.771130164828e02
+
+
+def test_reference_ps_check_periodic_golden(oracle):
+    rho, V, h, off = ps_check_periodic()
+    pot, eh = oracle.psolver_periodic(rho, h, offset=off)
+    assert abs(eh - PS_CHECK_EH) <= 5e-13 * PS_CHECK_EH      # all 13 printed digits
+    assert abs(pot[37, 27, 27] - PS_CHECK_V) <= 5e-13 * abs(PS_CHECK_V)
+    assert np.abs(pot - V).max() <= 2 * PS_CHECK_INF          # the same accuracy as the reference's run
+
+
+def xc_test_density(n=100000):
+    """The density of the reference's XC test (bigdft/tests/libs/xc/test_xc.f90:
+    gauss, :187-215, spin-unpolarised, ABINIT kind): 1e-20 everywhere
+    (xc_init_rho), a Gaussian over points 5..n-5, the 1e-20 floor
+    (xc_clean_rho), normalised by the sum of the first n values.  xc_getvxc
+    with nspden = 1 takes rho as the spin-up density: the total is 2 rho."""
+    rho = np.full(2 * n, 1e-20)
+    sigma = 1.0 / (n * 0.25)
+    j = np.arange(5, n - 5 + 1)
+    rho[j - 1] = np.exp(-((sigma * (n // 2 - j)) ** 2)) / n
+    rho[j - 1 + n] = rho[j - 1]
+    rho[rho < 1e-20] = 1e-20
+    return rho[:n] / rho[:n].sum()
+
+
+# bigdft/tests/libs/xc/xc.ref.yaml:2 (ixc 1, nosp): the sum of eps_xc over the test density
+XC_REF_IXC1_NOSP = -2766.214885143616
+
+
+def test_reference_xc_golden(oracle):
+    eps, _ = oracle.xc_lda(2.0 * xc_test_density())
+    assert abs(eps.sum() - XC_REF_IXC1_NOSP) <= 1e-12 * abs(XC_REF_IXC1_NOSP)
+
+
+def test_xc_potential_is_the_density_derivative(oracle):
+    """v_xc = d(rho eps_xc)/d rho (central differences, relative step 1e-5)."""
+    rho = np.geomspace(1e-8, 1e2, 61)
+    eps, v = oracle.xc_lda(rho)
+    d = 1e-5 * rho
+    ep, _ = oracle.xc_lda(rho + d)
+    em, _ = oracle.xc_lda(rho - d)
+    fd = ((rho + d) * ep - (rho - d) * em) / (2 * d)
+    assert np.abs(fd - v).max() <= 1e-8 * np.abs(v).max()
+    assert np.all(eps < 0) and np.all(v < eps)      # bound, and v_xc = eps + rho d eps/d rho < eps
+
+
+def test_xc_high_density_limit_is_slater_exchange(oracle):
+    """As rs -> 0 the fit tends to the exchange energy -(3/4)(3/(2 pi))^(2/3) / rs
+    (a0 of the fit) and v_xc to 4/3 of it."""
+    rs = 1e-6
+    rho = 3.0 / (4 * np.pi * rs ** 3)
+    eps, v = oracle.xc_lda(np.array([rho]))
+    ex = -0.75 * (3 / (2 * np.pi)) ** (2.0 / 3.0) / rs
+    assert abs(eps[0] / ex - 1) < 1e-5 and abs(v[0] / (4.0 / 3.0 * ex) - 1) < 1e-5
+
+
+def test_ks_potential_is_the_sum_of_its_parts(oracle):
+    rng = np.random.default_rng(3)
+    n = (32, 24, 20)
+    h = (0.3, 0.35, 0.4)
+    rho = rng.uniform(1e-3, 1.0, n)
+    vext = rng.uniform(-1, 1, n)
+    pot, (eh, exc, evxc) = oracle.ks_potential_periodic(rho, h, vext)
+    vh, eh0 = oracle.psolver_periodic(rho, h)
+    eps, vxc = oracle.xc_lda(rho)
+    assert np.array_equal(pot, (vh + vext) + vxc) and eh == eh0
+    dv = np.prod(h)
+    assert abs(exc - (eps * rho).sum() * dv) <= 1e-12 * abs(exc)
+    assert abs(evxc - (vxc * rho).sum() * dv) <= 1e-12 * abs(evxc)
