@@ -348,14 +348,16 @@ def leg_nlpsp(torch, ctx, psi64, lr, norb, natoms=64, seed=21):
 
 
 def leg_psolver(torch, ctx, dev, n=96, h=0.225):
-    """The potential step that follows the density, on the periodic 96^3 ISF
-    grid of the batched workload (seeded positive density, FP64): the Hartree
-    potential (wvlh_psolver_periodic: cuFFT and the ISF kernel multiply), the
-    Kohn-Sham potential V_H + V_ext + V_xc with its three energies
-    (wvlh_ks_potential_periodic) and the LDA alone (wvlh_xc_lda, 16 bytes a
-    point), against the oracle's numpy restatement on the host."""
+    """The potential step that follows the density, on the 96^3 ISF grid of
+    the batched workload (seeded positive density, FP64): the Hartree
+    potential, periodic (wvlh_psolver_periodic: cuFFT and the ISF kernel
+    multiply) and free (wvlh_psolver_free: the density padded to 192^3, the
+    kernel table built once and kept), the Kohn-Sham potential V_H + V_ext +
+    V_xc with its three energies (wvlh_ks_potential_periodic / _free) and the
+    LDA alone (wvlh_xc_lda, 16 bytes a point), against the oracle's numpy
+    restatement on the host."""
     import numpy as np
-    from wvlh.psolver import hartree_periodic, ks_potential_periodic, xc_lda
+    from wvlh.psolver import hartree_free, hartree_periodic, ks_potential_free, ks_potential_periodic, xc_lda
     rng = np.random.default_rng(5)
     rho_h = rng.uniform(1e-3, 1, (n, n, n))
     vext_h = rng.uniform(-1, 1, (n, n, n))
@@ -366,9 +368,13 @@ def leg_psolver(torch, ctx, dev, n=96, h=0.225):
     ms = _timed(torch, lambda: hartree_periodic(ctx, rho, hh, pot=pot), 10)
     ks_ms = _timed(torch, lambda: ks_potential_periodic(ctx, rho, hh, vext=vext, pot=pot), 10)
     xc_ms = _timed(torch, lambda: xc_lda(ctx, rho, vxc=pot, dvol=h ** 3), 10)
-    out = {"workload": "%d^3 periodic grid, h %.3f bohr, FP64" % (n, h), "ms": ms,
+    hartree_free(ctx, rho, hh, pot=pot)      # builds the free kernel and plans once
+    free_ms = _timed(torch, lambda: hartree_free(ctx, rho, hh, pot=pot), 10)
+    ks_free_ms = _timed(torch, lambda: ks_potential_free(ctx, rho, hh, vext=vext, pot=pot), 10)
+    out = {"workload": "%d^3 grid, h %.3f bohr, FP64" % (n, h), "ms": ms,
            "ks_potential_ms": ks_ms, "xc_lda_ms": xc_ms,
-           "xc_lda_gbs": 16.0 * n ** 3 / (xc_ms * 1e-3) / 1e9}
+           "xc_lda_gbs": 16.0 * n ** 3 / (xc_ms * 1e-3) / 1e9,
+           "free_ms": free_ms, "ks_potential_free_ms": ks_free_ms}
     try:
         from oracle import ks_potential_periodic as ks_cpu
         from oracle import psolver_periodic
@@ -378,6 +384,10 @@ def leg_psolver(torch, ctx, dev, n=96, h=0.225):
         t = time.perf_counter()
         ks_cpu(rho_h, hh, vext_h)
         out["cpu_oracle_ks_ms"] = (time.perf_counter() - t) * 1e3
+        from oracle import psolver_free
+        t = time.perf_counter()
+        psolver_free(rho_h, hh)
+        out["cpu_oracle_free_ms"] = (time.perf_counter() - t) * 1e3
     except Exception as e:  # the oracle is optional on the bench box
         out["cpu_oracle"] = "unavailable: %s" % e
     return out

@@ -15,6 +15,9 @@ the reference sources instead of being retyped:
   (``<psi|D2|psi>``): ``bigdft/src/orbitals/convolut_ib_optim.f90:987-1046``
   (``ConvolkineticT``); ``a`` equals the kinetic ``fil`` and ``b(i)=c(-i)``.
 * preconditioner diagonal ``A2``/``B2``: ``bigdft/src/OpenCL/Uncompress.c:377-378``.
+* the 89-term Gaussian expansion of 1/r that the free-boundary Poisson kernel
+  is built from (exponents ``p`` and weights ``w``, range [1e-9, 1]):
+  ``psolver/src/Build_Kernel.f90:1679-1873`` (``gequad``).
 
 Run ``python gen_filters.py /root/reference`` to rewrite the header; the
 generated header is committed so that the build never needs the reference.
@@ -83,18 +86,24 @@ def parse(ref_root):
     ewav = _indexed(ib, "e", 0, 14, ckt_line)
     a2 = re.search(r"#define\s+A2\s+(" + NUM + ")", unc).group(1)
     b2 = re.search(r"#define\s+B2\s+(" + NUM + ")", unc).group(1)
-    return dict(ch=ch, cg=cg, mf=mf, kin=kin, cwav=cwav, ewav=ewav, a2=a2, b2=b2)
+    bk = (Path(ref_root) / "psolver" / "src" / "Build_Kernel.f90").read_text()
+    gq_line = next(i for i, l in enumerate(bk.splitlines(), 1) if re.match(r"\s*subroutine gequad\(", l))
+    gq_p = _indexed(bk, "p", 1, 89, gq_line)
+    gq_w = _indexed(bk, "w", 1, 89, gq_line)
+    return dict(ch=ch, cg=cg, mf=mf, kin=kin, cwav=cwav, ewav=ewav, a2=a2, b2=b2, gq_p=gq_p, gq_w=gq_w)
 
 
 def render(f):
-    def arr(name, vals, comment):
+    def arr(name, vals, comment, at=True):
         body = ", \\\n".join("    %s" % v for v in vals)
-        # NAME_AT(i): the i-th tap as a constant expression (folds to an
-        # immediate when i is a compile-time constant)
-        at = "".join("(i) == %d ? (%s) : " % (k, v) for k, v in enumerate(vals)) + "0.0"
-        return ("/* %s */\n#define %s_INIT { \\\n%s}\nstatic const double %s[%d] = %s_INIT;\n"
-                "#define %s_AT(i) (%s)\n"
-                % (comment, name, body, name, len(vals), name, name, at))
+        out = ("/* %s */\n#define %s_INIT { \\\n%s}\nstatic const double %s[%d] = %s_INIT;\n"
+               % (comment, name, body, name, len(vals), name))
+        if at:
+            # NAME_AT(i): the i-th tap as a constant expression (folds to an
+            # immediate when i is a compile-time constant)
+            expr = "".join("(i) == %d ? (%s) : " % (k, v) for k, v in enumerate(vals)) + "0.0"
+            out += "#define %s_AT(i) (%s)\n" % (name, expr)
+        return out
 
     parts = [
         "/* Generated by gen_filters.py from the reference sources; do not edit. */",
@@ -109,6 +118,9 @@ def render(f):
         "/* preconditioner diagonal constants: OpenCL/Uncompress.c:377-378 */",
         "#define WVL_A2 %s" % f["a2"],
         "#define WVL_B2 %s" % f["b2"],
+        arr("WVL_GQ_P", f["gq_p"], "1/r = sum w(i) exp(-p(i) r^2), r in [1e-9, 1]: exponents p(1..89), "
+            "psolver/src/Build_Kernel.f90:1689-1777 (gequad)", at=False),
+        arr("WVL_GQ_W", f["gq_w"], "weights w(1..89): Build_Kernel.f90:1779-1867", at=False),
         "",
     ]
     return "\n".join(parts)

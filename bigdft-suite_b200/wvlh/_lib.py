@@ -81,6 +81,9 @@ WVLH_SYMBOLS = [
     "wvlh_psolver_periodic",
     "wvlh_xc_lda",
     "wvlh_ks_potential_periodic",
+    "wvlh_psolver_free",
+    "wvlh_ks_potential_free",
+    "wvlh_psolver_free_tables",
 ]
 
 
@@ -143,6 +146,11 @@ def lib():
     L.wvlh_psolver_periodic.argtypes = [vp, C.POINTER(C.c_int), C.POINTER(C.c_double), vp, vp, C.c_double, vp]
     L.wvlh_xc_lda.argtypes = [vp, C.c_int64, vp, vp, C.c_int, C.c_double, vp]
     L.wvlh_ks_potential_periodic.argtypes = [vp, C.POINTER(C.c_int), C.POINTER(C.c_double), vp, vp, vp, vp]
+    L.wvlh_psolver_free.argtypes = [vp, C.POINTER(C.c_int), C.POINTER(C.c_double), vp, vp, vp]
+    L.wvlh_ks_potential_free.argtypes = [vp, C.POINTER(C.c_int), C.POINTER(C.c_double), vp, vp, vp, vp]
+    L.wvlh_psolver_free_tables.argtypes = [C.POINTER(C.c_int), C.POINTER(C.c_double), C.POINTER(C.c_int), vp,
+                                           C.c_int64]
+    L.wvlh_psolver_free_tables.restype = C.c_int64
     L.wvlh_host_alloc.restype = vp
     L.wvlh_host_alloc.argtypes = [C.c_size_t]
     L.wvlh_host_free.argtypes = [vp]

@@ -10,6 +10,41 @@ import ctypes as C
 from ._lib import WvlhError, check, lib
 
 
+def free_kernel_tables(n, h):
+    """Host side of the free-BC kernel (no device work): (nf, rows, w) with
+    nf the padded FFT lengths (N1, N2, N3), rows (89, N1/2+N2/2+N3/2+3) the
+    1D cosine tables [C_x | C_y | C_z] per Gaussian and w the 89 weights."""
+    import numpy as np
+    nn = (C.c_int * 3)(*[int(v) for v in n])
+    hh = (C.c_double * 3)(*[float(v) for v in h])
+    nf = (C.c_int * 3)()
+    need = lib().wvlh_psolver_free_tables(nn, hh, nf, None, 0)
+    if need < 0:
+        check(int(need), "wvlh_psolver_free_tables")
+    tab = np.zeros(need)
+    check(min(0, int(lib().wvlh_psolver_free_tables(nn, hh, nf, tab.ctypes.data_as(C.c_void_p), need))),
+          "wvlh_psolver_free_tables")
+    return tuple(nf), tab[:-89].reshape(89, -1), tab[-89:]
+
+
+def hartree_free(ctx, rho, h, pot=None, energy=True):
+    """The Hartree potential with free (isolated) boundary conditions
+    (wvlh_psolver_free); arguments and results as hartree_periodic."""
+    torch = ctx.torch
+    if rho.dtype != torch.float64 or rho.dim() != 3 or not rho.is_contiguous():
+        raise WvlhError("rho: contiguous 3D float64 device tensor (z, y, x)")
+    if pot is None:
+        pot = torch.empty_like(rho)
+    if pot.shape != rho.shape or pot.dtype != torch.float64 or not pot.is_contiguous():
+        raise WvlhError("pot: a tensor like rho")
+    n = (C.c_int * 3)(rho.shape[2], rho.shape[1], rho.shape[0])
+    hh = (C.c_double * 3)(*[float(v) for v in h])
+    eh = torch.empty((), dtype=torch.float64, device=rho.device) if energy else None
+    check(lib().wvlh_psolver_free(ctx.h, n, hh, C.c_void_p(rho.data_ptr()), C.c_void_p(pot.data_ptr()),
+                                  C.c_void_p(eh.data_ptr()) if energy else None), "wvlh_psolver_free")
+    return pot, eh
+
+
 def hartree_periodic(ctx, rho, h, offset=0.0, pot=None, energy=True):
     """rho: (n3, n2, n1) float64 device tensor (x fastest), h: (hx, hy, hz).
     Returns (pot, eh): the potential (a new tensor unless pot is given; pot
@@ -58,11 +93,11 @@ def xc_lda(ctx, rho, vxc=None, accumulate=False, dvol=1.0, energy=True):
     return vxc, en
 
 
-def ks_potential_periodic(ctx, rho, h, vext=None, pot=None, energy=True):
-    """pot = V_H[rho] + vext + V_xc[rho] on a periodic grid (rho: (n3, n2, n1)
-    float64 device tensor, x fastest; vext None or a tensor like rho).
-    Returns (pot, energies), energies a (3,) device tensor (eh, exc, evxc),
-    or None without energy."""
+def ks_potential_periodic(ctx, rho, h, vext=None, pot=None, energy=True, free=False):
+    """pot = V_H[rho] + vext + V_xc[rho] on a periodic grid, or with free
+    boundary conditions when free (rho: (n3, n2, n1) float64 device tensor,
+    x fastest; vext None or a tensor like rho).  Returns (pot, energies),
+    energies a (3,) device tensor (eh, exc, evxc), or None without energy."""
     torch = ctx.torch
     _check_rho(ctx, rho)
     if rho.dim() != 3:
@@ -75,8 +110,13 @@ def ks_potential_periodic(ctx, rho, h, vext=None, pot=None, energy=True):
     n = (C.c_int * 3)(rho.shape[2], rho.shape[1], rho.shape[0])
     hh = (C.c_double * 3)(*[float(v) for v in h])
     en = torch.empty(3, dtype=torch.float64, device=rho.device) if energy else None
-    check(lib().wvlh_ks_potential_periodic(ctx.h, n, hh, C.c_void_p(rho.data_ptr()),
-                                           C.c_void_p(vext.data_ptr()) if vext is not None else None,
-                                           C.c_void_p(pot.data_ptr()), C.c_void_p(en.data_ptr()) if energy else None),
-          "wvlh_ks_potential_periodic")
+    fn = "wvlh_ks_potential_free" if free else "wvlh_ks_potential_periodic"
+    check(getattr(lib(), fn)(ctx.h, n, hh, C.c_void_p(rho.data_ptr()),
+                             C.c_void_p(vext.data_ptr()) if vext is not None else None,
+                             C.c_void_p(pot.data_ptr()), C.c_void_p(en.data_ptr()) if energy else None), fn)
     return pot, en
+
+
+def ks_potential_free(ctx, rho, h, vext=None, pot=None, energy=True):
+    """ks_potential_periodic with free boundary conditions."""
+    return ks_potential_periodic(ctx, rho, h, vext, pot, energy, free=True)

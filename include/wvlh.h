@@ -370,6 +370,23 @@ int wvlh_nlpsp_destroy(wvlh_nlpsp *nl);
  * (PSolver_Main.f90:403).  FFTs by cuFFT, plans kept per context and grid. */
 int wvlh_psolver_periodic(wvlh_ctx *ctx, const int n[3], const double h[3], const double *rho, double *pot,
                           double offset, double *eh);
+/* Hartree potential with free (isolated) boundary conditions, the reference's
+ * PSolver for geocode 'F' (Free_Kernel, psolver/src/Build_Kernel.f90:985-1175,
+ * from the 89-Gaussian expansion of 1/r, gequad :1679-1873, and the order-16
+ * ISF; scal h1 h2 h3 / (N1 N2 N3), createKernel.f90:439): rho zero-padded to
+ * at least twice each dimension, multiplied by the kernel's Fourier table,
+ * the first octant kept.  n: points per dimension (x fastest, 2..4096), h:
+ * spacings (bohr), rho/pot: DEVICE FP64 (pot may be rho when eh is NULL).
+ * eh (DEVICE, or NULL): 0.5 sum(rho V) h1 h2 h3.  The kernel table, FFT plans
+ * and padded buffers are built at the first call for a grid and kept. */
+int wvlh_psolver_free(wvlh_ctx *ctx, const int n[3], const double h[3], const double *rho, double *pot, double *eh);
+/* Host only (no device work): the padded FFT lengths nf and the free kernel's
+ * 1D tables that wvlh_psolver_free sums on the device: per Gaussian g = 0..88
+ * a row [C_x(0..N1/2) | C_y(0..N2/2) | C_z(0..N3/2)], then the 89 weights;
+ * K(k3, k2, k1) = sum_g C_x(k1) (C_z(k3) (C_y(k2) w_g)), g from 88 down to 0.
+ * With tab NULL returns the number of doubles; otherwise fills tab (cap
+ * doubles) and returns that number, or a negative error. */
+int64_t wvlh_psolver_free_tables(const int n[3], const double h[3], int nf[3], double *tab, int64_t cap);
 /* Exchange-correlation potential of the reference's default functional
  * (ixc = 1: the Goedecker-Teter-Hutter Pade LDA, ABINIT's xcspol,
  * libABINIT/src/abi_xc_lowlevel/abi_xcspol.F90:105-250), spin-unpolarised,
@@ -390,6 +407,10 @@ int wvlh_xc_lda(wvlh_ctx *ctx, int64_t npts, const double *rho, double *vxc, int
  * energies. */
 int wvlh_ks_potential_periodic(wvlh_ctx *ctx, const int n[3], const double h[3], const double *rho,
                                const double *vext, double *pot, double *energies);
+/* The same Kohn-Sham potential with free boundary conditions (V_H as
+ * wvlh_psolver_free). */
+int wvlh_ks_potential_free(wvlh_ctx *ctx, const int n[3], const double h[3], const double *rho, const double *vext,
+                           double *pot, double *energies);
 /* FP64, one kernel per 1D pass (the OpenCL backend's structure) */
 int wvlh_locham_plain_batched(wvlh_batch *batch, const double *psi, const double *pot, double *hpsi,
                               double *ekin, double *epot);

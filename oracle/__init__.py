@@ -407,13 +407,10 @@ def orthoconstraint(psi, hpsi, occup, symm=True, tr_min=False):
     return hpsi - lam.T @ psi, lam, tr, asy, mix
 
 
-def isf_fourier(n):
-    """The order-16 ISF's Fourier transform at p = i 2 pi / (2 n), i = 0..n, as
-    fourtrans_isf computes it (psolver/src/Build_Kernel.f90:202-262): odd i by
-    the product of two-scale symbols H(p/2^j) until H is 1 to 1e-16, even i
-    from i/2 by one more symbol.  H(p) = 1/2 + sum over odd m <= 15 of
-    w_m cos(m p), w_m the 16-point Lagrange weights at the midpoint of the odd
-    offsets (the lazy_16 filter)."""
+def isf_weights():
+    """{m: w_m} for odd m = 1..15: the 16-point Lagrange interpolation weights
+    at the midpoint of the odd offsets -15..15 (exact rationals), the odd taps
+    ch(+-m) of the order-16 ISF two-scale filter (lazy_16.inc, ch(0) = 1)."""
     from fractions import Fraction
     odd = list(range(-15, 16, 2))
     w = {}
@@ -423,6 +420,17 @@ def isf_fourier(n):
             if i != m:
                 r *= Fraction(-i, m - i)
         w[m] = float(r)
+    return w
+
+
+def isf_fourier(n):
+    """The order-16 ISF's Fourier transform at p = i 2 pi / (2 n), i = 0..n, as
+    fourtrans_isf computes it (psolver/src/Build_Kernel.f90:202-262): odd i by
+    the product of two-scale symbols H(p/2^j) until H is 1 to 1e-16, even i
+    from i/2 by one more symbol.  H(p) = 1/2 + sum over odd m <= 15 of
+    w_m cos(m p), w_m the 16-point Lagrange weights at the midpoint of the odd
+    offsets (the lazy_16 filter)."""
+    w = isf_weights()
 
     def H(p):
         return 0.5 + sum(w[m] * np.cos(m * p) for m in range(15, 0, -2))
@@ -473,6 +481,155 @@ def psolver_periodic(rho, h, offset=0.0):
     return V, 0.5 * float((rho * V).sum()) * h[0] * h[1] * h[2]
 
 
+def gequad():
+    """(p, w): the 89-term expansion 1/r = sum w exp(-p r^2) on [1e-9, 1] of
+    psolver/src/Build_Kernel.f90:1679-1873, from the generated filter header."""
+    import re
+    hdr = (HERE.parent / "bigdft-suite_b200" / "csrc" / "wvl_filters.h").read_text()
+    out = []
+    for name in ("WVL_GQ_P", "WVL_GQ_W"):
+        body = re.search(r"#define %s_INIT \{(.*?)\}" % name, hdr, re.S).group(1)
+        out.append(np.array([float(v) for v in body.replace("\\", " ").split(",")]))
+    return out[0], out[1]
+
+
+def isf_samples(itype=16, n_points=16):
+    """(x, y), 2 itype n_points + 1 points: the order-16 ISF on [-15, 17] at
+    spacing 1/16 by the cascade of scaling_function
+    (psolver/src/scaling_function.f90:12-110; back_trans_16 :1232-1266): a unit
+    value at x = 0 refined by doubling, even points kept, odd points the
+    midpoint interpolation sum_j ch(2j+1) x(i-j), periodic on the current
+    length (the support never reaches the wrap)."""
+    ni, nd = 2 * itype, 2 * itype * n_points
+    w = isf_weights()
+    ch = {0: 1.0}
+    for m, v in w.items():
+        ch[m] = ch[-m] = v
+    mm = itype + 2
+    x = np.zeros(nd + 1)
+    x[ni // 2 - 1] = 1.0
+    nt = ni
+    while True:
+        nt *= 2
+        half = nt // 2
+        prev = x[:half].copy()
+        y = np.zeros(nt)
+        y[0::2] = prev
+        for j in range(-mm // 2, mm // 2):
+            c = ch.get(2 * j + 1, 0.0)
+            if c:
+                y[1::2] += c * np.roll(prev, j)      # prev[(i - j) mod half]
+        x[:nt] = y
+        if nt == nd:
+            break
+    a = np.arange(nd + 1) * ni / nd - (0.5 * ni - 1.0)
+    return a, x
+
+
+def gauss_conv_isf(p, h, n_range, xs, ys, itype=16):
+    """k(i) = integral of phi(x - i) exp(-p h^2 x^2) dx (x in grid units), i =
+    -n_range..n_range (index i + n_range), as gauss_conv_scf
+    (psolver/src/Build_Kernel.f90:1597-1651): for a sharp Gaussian the
+    exponent is first divided by 4^n_iter (n_iter = nint(log4(p h^2))), the
+    Riemann sum over the ISF samples taken (terms past sqrt(634.7/p0)/h
+    skipped, stopping after the first value below 1e-18), then n_iter
+    two-scale steps k(i) <- 1/2 sum_j ch(j) k(2i - j) (scf_recursion_16,
+    scaling_function.f90:1324-1356) bring it back to p."""
+    dx = (2.0 * itype) / (len(xs) - 1)
+    p0_cell = 1.0 / (h * h)
+    n_iter = int(np.floor((np.log(p) - np.log(p0_cell)) / np.log(4.0) + 0.5))
+    if n_iter <= 0:
+        n_iter, p0 = 0, p
+    else:
+        p0 = p / 4.0 ** n_iter
+    x_limit = np.sqrt(634.71369555645470 / p0) / h
+    k = np.zeros(2 * n_range + 1)
+    for i in range(n_range + 1):
+        ab = xs - i
+        m = np.abs(ab) < x_limit
+        v = float(np.sum(ys[m] * np.exp(-p0 * (ab[m] * ab[m] * h ** 2))))
+        k[n_range + i] = k[n_range - i] = v * dx
+        if abs(v) < 1e-18:
+            break
+    w = isf_weights()
+    ch = {0: 1.0}
+    for mm, v in w.items():
+        ch[mm] = ch[-mm] = v
+    for _ in range(n_iter):
+        k1 = k.copy()
+        k[:] = 0.0
+        for i in range(n_range + 1):
+            tot = 0.0
+            for j in range(-(itype + 2), itype + 3):
+                ind = 2 * i - j
+                if -n_range <= ind <= n_range and j in ch:
+                    tot += ch[j] * k1[n_range + ind]
+            if tot == 0.0:
+                break
+            k[n_range + i] = k[n_range - i] = 0.5 * tot
+    return k
+
+
+def free_kernel(n0, h, nfft):
+    """The free-boundary Poisson kernel in Fourier space, as Free_Kernel
+    (psolver/src/Build_Kernel.f90:985-1175) builds it: for each Gaussian of
+    gequad, scaled to the box diagonal a (p / a^2, w / a), the three 1D
+    ISF-Gaussian overlaps (gauss_conv_isf, n_range = max(n01, n02, n03, 32)
+    points) cosine-transformed on the padded lengths nfft (gauconv_ffts
+    :1184-1340: the symmetric sequence of min(n_range, n/2) values; the
+    reference's centred layout multiplies each transform by (-1)^k, which only
+    moves the origin of its convolution), summed from the last Gaussian to
+    the first as k_x (k_z (k_y w)).  n0 = (n01, n02, n03), nfft = (N1, N2, N3);
+    returns K of shape (N3/2+1, N2/2+1, N1/2+1), x fastest."""
+    pg, wg = gequad()
+    a = [h[d] * n0[d] for d in range(3)]
+    a2 = a[0] * a[0] + a[1] * a[1] + a[2] * a[2]
+    factor, factor2 = 1.0 / np.sqrt(a2), 1.0 / a2
+    n_range = max(max(n0), 32)
+    xs, ys = isf_samples()
+    K = np.zeros((nfft[2] // 2 + 1, nfft[1] // 2 + 1, nfft[0] // 2 + 1))
+    cosk = []
+    for d in range(3):
+        n = nfft[d]
+        J = min(n_range, n // 2)
+        kk = np.arange(n // 2 + 1)[:, None]
+        jj = np.arange(1, J)[None, :]
+        cosk.append((J, np.cos(2.0 * np.pi * ((kk * jj) % n) / n)))
+    for g in range(len(pg) - 1, -1, -1):
+        pgauss = pg[g] * factor2
+        C = []
+        for d in range(3):
+            k = gauss_conv_isf(pgauss, h[d], n_range, xs, ys)
+            J, cs = cosk[d]
+            f = k[n_range:n_range + J]
+            C.append(f[0] + 2.0 * (cs @ f[1:]))
+        w = wg[g] * factor
+        K += C[0][None, None, :] * (C[2][:, None, None] * (C[1][None, :, None] * w))
+    return K
+
+
+def psolver_free(rho, h, nfft=None):
+    """Hartree potential and energy of rho (n3, n2, n1; x fastest) with free
+    boundary conditions: rho zero-padded to nfft (default twice each
+    dimension), multiplied in Fourier space by free_kernel, scaled by
+    h1 h2 h3 / (N1 N2 N3) (createKernel.f90:439), the first n0 points kept;
+    energy 0.5 sum(rho V) h^3 (PSolver_Main.f90:403)."""
+    rho = np.asarray(rho, np.float64)
+    n3, n2, n1 = rho.shape
+    if nfft is None:
+        nfft = (2 * n1, 2 * n2, 2 * n3)
+    K = free_kernel((n1, n2, n3), h, nfft)
+    N1, N2, N3 = nfft
+    pad = np.zeros((N3, N2, N1))
+    pad[:n3, :n2, :n1] = rho
+    p2 = np.minimum(np.arange(N2), N2 - np.arange(N2))
+    p3 = np.minimum(np.arange(N3), N3 - np.arange(N3))
+    Kf = K[p3][:, p2]
+    vol = h[0] * h[1] * h[2]
+    V = np.fft.irfftn(np.fft.rfftn(pad) * Kf, s=pad.shape, axes=(0, 1, 2))[:n3, :n2, :n1] * vol
+    return V, 0.5 * float((rho * V).sum()) * vol
+
+
 # Goedecker-Teter-Hutter Pade fit of the Ceperley-Alder LDA (Phys. Rev. B 54,
 # 1703 (1996), paramagnetic parameters; ixc = 1 of the reference, ABINIT's
 # xcspol, libABINIT/src/abi_xc_lowlevel/abi_xcspol.F90:105-112): eps_xc(rs) =
@@ -502,7 +659,12 @@ def xc_lda(rho):
     return eps, eps - rs / 3.0 * deps
 
 
-def ks_potential_periodic(rho, h, vext=None):
+def ks_potential_free(rho, h, vext=None):
+    """ks_potential_periodic with the free-boundary Hartree potential."""
+    return ks_potential_periodic(rho, h, vext, free=True)
+
+
+def ks_potential_periodic(rho, h, vext=None, free=False):
     """The Kohn-Sham potential of a periodic box from the total density, as
     updatePotential (bigdft/src/modules/rhopotential.f90:29-125) builds it for
     nspin = 1 and ixc = 1: XC_potential (xcPSolver/xcenergy.f90:428; energies
@@ -510,7 +672,7 @@ def ks_potential_periodic(rho, h, vext=None):
     dvol sum v_xc rho), H_potential with V_ext summed in (offset 0), then
     rhov += V_xc.  Returns (pot, (eh, exc, evxc))."""
     rho = np.asarray(rho, np.float64)
-    vh, eh = psolver_periodic(rho, h)
+    vh, eh = psolver_free(rho, h) if free else psolver_periodic(rho, h)
     eps, vxc = xc_lda(rho)
     dvol = h[0] * h[1] * h[2]
     pot = (vh if vext is None else vh + np.asarray(vext, np.float64)) + vxc   # H_potential's sum, then the axpy

@@ -120,3 +120,55 @@ def test_ks_potential_rejects_aliasing(torch_cuda, wctx):
     v = torch.zeros_like(t)
     with pytest.raises(WvlhError):
         ks_potential_periodic(wctx, t, (0.3, 0.3, 0.3), vext=v, pot=v)
+
+
+def test_reference_ps_check_free_golden(torch_cuda, wctx):
+    """The reference's PS_Check free-BC run (57 x 48 x 63 unit Gaussian): the
+    Hartree energy and the potential at its largest-deviation point to the 13
+    printed digits, the same deviation from the analytic potential."""
+    from test_psolver_rule import PS_FREE_AT, PS_FREE_EH, PS_FREE_INF, PS_FREE_V, ps_check_free
+    from wvlh.psolver import hartree_free
+    torch = torch_cuda
+    rho, V, h = ps_check_free()
+    pot, eh = hartree_free(wctx, torch.tensor(rho, device="cuda"), h)
+    got = pot.cpu().numpy()
+    i1, i2, i3 = (v - 1 for v in PS_FREE_AT)
+    assert abs(eh.item() - PS_FREE_EH) <= 5e-13 * PS_FREE_EH
+    assert abs(got[i3, i2, i1] - PS_FREE_V) <= 5e-13 * PS_FREE_V
+    assert abs(np.abs(got - V).max() - PS_FREE_INF) <= 1e-3 * PS_FREE_INF
+
+
+@pytest.mark.parametrize("n,h", [((9, 10, 12), (0.3, 0.25, 0.2)), ((33, 40, 28), (0.35, 0.3, 0.4)),
+                                 ((64, 64, 64), (0.225, 0.225, 0.225))])
+def test_free_matches_oracle(oracle, torch_cuda, wctx, n, h):
+    from wvlh.psolver import hartree_free
+    torch = torch_cuda
+    rng = np.random.default_rng(sum(n))
+    rho = rng.uniform(-1, 1, n[::-1])
+    ref, eref = oracle.psolver_free(rho, h)
+    t = torch.tensor(rho, device="cuda")
+    pot, eh = hartree_free(wctx, t, h)
+    assert np.abs(pot.cpu().numpy() - ref).max() <= 1e-13 * np.abs(ref).max()
+    assert abs(eh.item() - eref) <= 1e-12 * abs(eref)
+    # deterministic; the padded buffer's zeros survive repeated solves
+    pot2, eh2 = hartree_free(wctx, t, h)
+    assert torch.equal(pot, pot2) and torch.equal(eh, eh2)
+    # in place without the energy; refused with it
+    with pytest.raises(WvlhError):
+        hartree_free(wctx, t, h, pot=t, energy=True)
+    hartree_free(wctx, t, h, pot=t, energy=False)
+    assert torch.equal(t, pot)
+
+
+def test_ks_potential_free_matches_oracle(oracle, torch_cuda, wctx):
+    from wvlh.psolver import ks_potential_free
+    torch = torch_cuda
+    n, h = (40, 36, 44), (0.3, 0.3, 0.3)
+    rng = np.random.default_rng(11)
+    rho = rng.uniform(1e-4, 0.5, n[::-1])
+    vext = rng.uniform(-2, 2, n[::-1])
+    ref, (eh, exc, evxc) = oracle.ks_potential_free(rho, h, vext)
+    pot, en = ks_potential_free(wctx, torch.tensor(rho, device="cuda"), h, vext=torch.tensor(vext, device="cuda"))
+    assert np.abs(pot.cpu().numpy() - ref).max() <= 1e-13 * np.abs(ref).max()
+    for a, b in zip(en.cpu().numpy(), (eh, exc, evxc)):
+        assert abs(a - b) <= 1e-12 * abs(b)

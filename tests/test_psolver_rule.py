@@ -151,3 +151,82 @@ def test_ks_potential_is_the_sum_of_its_parts(oracle):
     dv = np.prod(h)
     assert abs(exc - (eps * rho).sum() * dv) <= 1e-12 * abs(exc)
     assert abs(evxc - (vxc * rho).sum() * dv) <= 1e-12 * abs(evxc)
+
+
+def ps_check_free():
+    """The free-BC case of the reference's PS_Check test (psolver/tests/
+    PS_Check.f90:29-113; test_functions_new case 'F', functions.f90:552-563):
+    a 57 x 48 x 63 box of side 10 bohr per dimension, x = (i - 1) h - L/2, a
+    unit Gaussian rho = exp(-r^2) / pi^(3/2) (a_gauss = 1) and its analytic
+    potential erf(r) / r.  Arrays (z, y, x)."""
+    from math import erf
+    n = (57, 48, 63)
+    h = tuple(10.0 / m for m in n)
+    ax = [np.arange(n[d]) * h[d] - 0.5 * n[d] * h[d] for d in range(3)]
+    z, y, x = np.meshgrid(ax[2], ax[1], ax[0], indexing="ij")
+    r2 = x * x + y * y + z * z
+    r = np.sqrt(r2)
+    rho = np.exp(-r2) / (np.pi * np.sqrt(np.pi))
+    verf = np.vectorize(erf)
+    V = np.where(r > 1e-15, verf(r) / np.where(r > 0, r, 1.0), 2.0 / np.sqrt(np.pi))
+    return rho, V, h
+
+
+# psolver/tests/PS_Check.ref.yaml:46-56 (free BC, 57 x 48 x 63): the Hartree
+# energy, the largest difference from the analytic potential, where it lies
+# (1-based x, y, z) and the potential there
+PS_FREE_EH = 3.989422803962e-01
+PS_FREE_INF = 3.365174805481e-10
+PS_FREE_AT = (30, 25, 33)
+PS_FREE_V = 1.123137867733e00
+
+
+def test_isf_cascade_samples(oracle):
+    """The cascade reproduces the interpolating scaling function: phi(k) =
+    delta_k at the integers, phi(1/2) = w_1, unit integral, support [-15, 15]."""
+    x, y = oracle.isf_samples()
+    assert len(x) == 513 and x[0] == -15.0 and x[-1] == 17.0
+    ints = (x == np.round(x))
+    assert np.array_equal(y[ints], (x[ints] == 0).astype(float))
+    assert y[15 * 16 + 8] == oracle.isf_weights()[1]
+    assert abs(y.sum() / 16 - 1.0) < 1e-14
+    assert np.all(y[x > 15] == 0)
+
+
+def test_reference_ps_check_free_golden(oracle):
+    rho, V, h = ps_check_free()
+    pot, eh = oracle.psolver_free(rho, h)
+    assert abs(eh - PS_FREE_EH) <= 5e-13 * PS_FREE_EH                   # all 13 printed digits
+    i1, i2, i3 = (v - 1 for v in PS_FREE_AT)
+    assert abs(pot[i3, i2, i1] - PS_FREE_V) <= 5e-13 * PS_FREE_V
+    d = np.abs(pot - V)
+    assert abs(d.max() - PS_FREE_INF) <= 1e-3 * PS_FREE_INF            # the same deviation ...
+    assert np.unravel_index(d.argmax(), d.shape) == (i3, i2, i1)        # ... at the same point
+
+
+def test_free_solution_independent_of_padding(oracle):
+    """The zero-padded convolution is exact for any FFT length >= twice the
+    box: the reference's FFT sizes (fourier_dim) and the doubled box agree."""
+    rng = np.random.default_rng(7)
+    rho = rng.uniform(0, 1, (12, 10, 9))
+    h = (0.3, 0.25, 0.2)
+    a, ea = oracle.psolver_free(rho, h)
+    b, eb = oracle.psolver_free(rho, h, nfft=(24, 24, 30))
+    assert np.abs(a - b).max() <= 1e-13 * np.abs(a).max() and abs(ea - eb) <= 1e-13 * abs(ea)
+
+
+def test_free_kernel_host_tables_match_oracle(oracle):
+    """The library's host construction of the free kernel (no device work)
+    equals the oracle's Free_Kernel restatement."""
+    from wvlh.psolver import free_kernel_tables
+    n = (57, 48, 63)
+    h = tuple(10.0 / m for m in n)
+    nf, rows, w = free_kernel_tables(n, h)
+    assert all(v >= 2 * m and v % 2 == 0 for v, m in zip(nf, n))
+    l1, l2, l3 = nf[0] // 2 + 1, nf[1] // 2 + 1, nf[2] // 2 + 1
+    K = np.zeros((l3, l2, l1))
+    for g in range(88, -1, -1):
+        cx, cy, cz = rows[g, :l1], rows[g, l1:l1 + l2], rows[g, l1 + l2:]
+        K += cx[None, None, :] * (cz[:, None, None] * (cy[None, :, None] * w[g]))
+    ref = oracle.free_kernel(n, h, nf)
+    assert np.abs(K - ref).max() <= 1e-13 * np.abs(ref).max()
