@@ -15,11 +15,14 @@
 //                the atom's common values: c = <p|psi>, fixed-order
 //                reductions (deterministic);
 //   k_nl_coeff:  one CTA per orbital: hc = h c per atom, eproj = sum c.hc;
-//   k_nl_update: one warp per (grid row, orbital block).  A run lies in one
-//                grid row (keys are runs along x) and a row's psi values are
-//                contiguous, so rows partition psi: lanes take the row's
-//                values, add sum_i hc_i p_i of every atom reaching the value
-//                (atoms in order) and write each value once.
+//                hc is written block-transposed, the kUpdBlock orbitals of a
+//                block contiguous per coefficient;
+//   k_nl_update: one warp per (grid row, block of kUpdBlock orbitals).  A run
+//                lies in one grid row (keys are runs along x) and a row's psi
+//                values are contiguous, so rows partition psi: lanes take the
+//                row's values, add sum_i hc_i p_i of every atom reaching the
+//                value (atoms in order) and write each value once; the block's
+//                hc of one coefficient arrive as 16-byte broadcast loads.
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -39,7 +42,10 @@ void set_last_error(int code);
 
 constexpr int kMaxProj = 32;   // projectors per atom
 constexpr int kProjChunk = 4;  // projectors summed per pass over an atom's runs
-constexpr int kOrbBlock = 8;   // orbitals per CTA (dot) or warp (update)
+// orbital blocks: each projector value loaded serves a block's orbitals;
+// smaller blocks (more resident warps) measured slower
+constexpr int kOrbBlock = 8;   // orbitals per CTA (dot)
+constexpr int kUpdBlock = 16;  // orbitals per warp (update), hc block width
 
 struct NlAtom {
     int nproj;
@@ -75,8 +81,11 @@ __global__ void __launch_bounds__(256) k_nl_dot(const NlAtom *__restrict__ atoms
         for (int b = 0; b < kOrbBlock; ++b)
 #pragma unroll
             for (int k = 0; k < kProjChunk; ++k) s[b][k] = 0.0;
+        // the next value's offsets are loaded one iteration ahead
+        int2 qn = threadIdx.x < at.nval ? v0[threadIdx.x] : make_int2(0, 0);
         for (int i = threadIdx.x; i < at.nval; i += blockDim.x) {
-            const int2 q = v0[i];   // (psi value, projector value)
+            const int2 q = qn;   // (psi value, projector value)
+            if (i + (int)blockDim.x < at.nval) qn = v0[i + blockDim.x];
             double pv[kProjChunk];
 #pragma unroll
             for (int k = 0; k < kProjChunk; ++k) pv[k] = k < np ? pa[(size_t)(p0 + k) * at.ld_p + q.y] : 0.0;
@@ -112,7 +121,8 @@ __global__ void __launch_bounds__(256) k_nl_dot(const NlAtom *__restrict__ atoms
 }
 
 // hc = h c per atom; eproj = sum over atoms of c . hc (thread t takes atoms
-// t, t + 128, ...; the thread sums are added in thread order: deterministic)
+// t, t + 128, ...; the thread sums are added in thread order: deterministic).
+// hc[(o / kUpdBlock) ctot + c][o % kUpdBlock]: a block's orbitals contiguous
 __global__ void __launch_bounds__(128) k_nl_coeff(int natoms, const NlAtom *__restrict__ atoms,
                                                   const double *__restrict__ hmat, int ctot,
                                                   const double *__restrict__ cf, double *__restrict__ hc,
@@ -121,7 +131,7 @@ __global__ void __launch_bounds__(128) k_nl_coeff(int natoms, const NlAtom *__re
     __shared__ double ea[128];
     const int o = blockIdx.x;
     const double *c = cf + (size_t)o * ctot;
-    double *h = hc + (size_t)o * ctot;
+    double *h = hc + (size_t)(o / kUpdBlock) * ctot * kUpdBlock + o % kUpdBlock;
     double e = 0.0;   // thread t: atoms t, t + 128, ...
     for (int a = threadIdx.x; a < natoms; a += blockDim.x) {
         const NlAtom at = atoms[a];
@@ -130,7 +140,7 @@ __global__ void __launch_bounds__(128) k_nl_coeff(int natoms, const NlAtom *__re
             const double *hr = hmat + at.h0 + (size_t)i * at.nproj;
             double v = 0.0;
             for (int j = 0; j < at.nproj; ++j) v = fma(hr[j], c[at.c0 + j], v);
-            h[at.c0 + i] = v;
+            h[(size_t)(at.c0 + i) * kUpdBlock] = v;
             ep = fma(c[at.c0 + i], v, ep);
         }
         e += ep;
@@ -144,45 +154,97 @@ __global__ void __launch_bounds__(128) k_nl_coeff(int natoms, const NlAtom *__re
     }
 }
 
+// a run as the update reads it: projector base such that proj + pb + wv is
+// the value of the run's first projector at psi value wv; psi range [w, w+n);
+// the atom's projector count, projector stride and first coefficient
+struct NlRunMeta {
+    long long pb;
+    int w, n, np, ldp, cc, pad;
+};
+
+// runs c .. min(c + 32, e1) - 1 of a row into the warp's metadata slots
+__device__ __forceinline__ void nl_stage_runs(const NlRun *__restrict__ rrun, const NlAtom *__restrict__ atoms,
+                                              int c, int e1, int lane, NlRunMeta *mw)
+{
+    __syncwarp();
+    if (lane < e1 - c) {
+        const NlRun r = rrun[c + lane];
+        const NlAtom at = atoms[r.atom];
+        NlRunMeta m;
+        m.pb = at.proj + r.p - r.w;
+        m.w = r.w;
+        m.n = r.n;
+        m.np = at.nproj;
+        m.ldp = at.ld_p;
+        m.cc = at.c0;
+        m.pad = 0;
+        mw[lane] = m;
+    }
+    __syncwarp();
+}
+
 // one warp per (row group, orbital block): rows[g] .. rows[g+1] index the
 // row-sorted run list (atoms in order within a row); rowv[g] = the row's first
-// psi value and value count
-__global__ void __launch_bounds__(256) k_nl_update(int ngroups, const int *__restrict__ rows,
-                                                   const int2 *__restrict__ rowv, const NlRun *__restrict__ rrun,
-                                                   const NlAtom *__restrict__ atoms,
-                                                   const double *__restrict__ proj, int norb, int ctot,
-                                                   const double *__restrict__ hc, long long ld,
-                                                   double *__restrict__ hpsi)
+// psi value and value count.  The row's runs (32 at a time) are staged in
+// shared memory once per warp, so the value loop reads no run or atom record
+// from memory; each lane prefetches its value's hpsi before the sums.  hc is
+// block-transposed (k_nl_coeff), zero for the orbitals past norb in the last
+// block, so every FMA is unconditional
+__global__ void __launch_bounds__(256, 2) k_nl_update(int ngroups, const int *__restrict__ rows,
+                                                      const int2 *__restrict__ rowv, const NlRun *__restrict__ rrun,
+                                                      const NlAtom *__restrict__ atoms,
+                                                      const double *__restrict__ proj, int norb, int ctot,
+                                                      const double *__restrict__ hc, long long ld,
+                                                      double *__restrict__ hpsi)
 {
-    const int lane = threadIdx.x & 31;
-    const int g = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-    if (g >= ngroups) return;
-    const int o0 = blockIdx.y * kOrbBlock;
-    const int nob = min(kOrbBlock, norb - o0);
+    __shared__ NlRunMeta meta[8][32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int g = blockIdx.x * (blockDim.x >> 5) + warp;
+    if (g >= ngroups) return;   // whole warps leave together
+    const int o0 = blockIdx.y * kUpdBlock;
+    const int nob = min(kUpdBlock, norb - o0);
     const int2 rv = rowv[g];
     const int e0 = rows[g], e1 = rows[g + 1];
-    for (int u = lane; u < rv.y; u += 32) {
+    const double2 *hblk = reinterpret_cast<const double2 *>(hc + (size_t)blockIdx.y * ctot * kUpdBlock);
+    NlRunMeta *mw = meta[warp];
+    const bool one = e1 - e0 <= 32;
+    if (one) nl_stage_runs(rrun, atoms, e0, e1, lane, mw);
+    for (int ub = 0; ub < rv.y; ub += 32) {   // warp-uniform: every lane stages
+        const int u = ub + lane;
+        const bool act = u < rv.y;
         const int wv = rv.x + u;
-        double v[kOrbBlock];
+        double old[kUpdBlock], v[kUpdBlock];
 #pragma unroll
-        for (int b = 0; b < kOrbBlock; ++b) v[b] = 0.0;
-        for (int e = e0; e < e1; ++e) {
-            const NlRun r = rrun[e];
-            const int t = wv - r.w;
-            if (t < 0 || t >= r.n) continue;
-            const NlAtom at = atoms[r.atom];
-            const double *pa = proj + at.proj + r.p + t;
-            const double *hb = hc + (size_t)o0 * ctot + at.c0;
-            for (int i = 0; i < at.nproj; ++i) {
-                const double p = pa[(size_t)i * at.ld_p];
+        for (int b = 0; b < kUpdBlock; ++b) {
+            old[b] = (act && b < nob) ? hpsi[(size_t)(o0 + b) * ld + wv] : 0.0;
+            v[b] = 0.0;
+        }
+        for (int c = e0; c < e1; c += 32) {
+            if (!one) nl_stage_runs(rrun, atoms, c, e1, lane, mw);
+            const int cnt = min(32, e1 - c);
+            if (!act) continue;
+            for (int k = 0; k < cnt; ++k) {
+                const int t = wv - mw[k].w;
+                if (t < 0 || t >= mw[k].n) continue;
+                const NlRunMeta m = mw[k];
+                const double *pa = proj + m.pb + wv;
+                const double2 *hb = hblk + (size_t)m.cc * (kUpdBlock / 2);
+                for (int i = 0; i < m.np; ++i) {
+                    const double p = pa[(size_t)i * m.ldp];
 #pragma unroll
-                for (int b = 0; b < kOrbBlock; ++b)
-                    if (b < nob) v[b] = fma(hb[(size_t)b * ctot + i], p, v[b]);
+                    for (int q = 0; q < kUpdBlock / 2; ++q) {
+                        const double2 h = hb[(size_t)i * (kUpdBlock / 2) + q];
+                        v[2 * q] = fma(h.x, p, v[2 * q]);
+                        v[2 * q + 1] = fma(h.y, p, v[2 * q + 1]);
+                    }
+                }
             }
         }
+        if (act) {
 #pragma unroll
-        for (int b = 0; b < kOrbBlock; ++b)
-            if (b < nob) hpsi[(size_t)(o0 + b) * ld + wv] += v[b];
+            for (int b = 0; b < kUpdBlock; ++b)
+                if (b < nob) hpsi[(size_t)(o0 + b) * ld + wv] = old[b] + v[b];
+        }
     }
 }
 
@@ -200,7 +262,7 @@ struct wvlh_nlpsp {
     NlRun *d_rrun = nullptr;
     int *d_rows = nullptr;
     double *d_proj = nullptr, *d_h = nullptr;
-    DevBuf cf, hc;         // c and hc, one row of ctot per orbital
+    DevBuf cf, hc;         // c (a row of ctot per orbital) and hc (block-transposed)
 };
 
 static int nl_fail(int code)
@@ -395,15 +457,21 @@ extern "C" int wvlh_nlpsp_apply(wvlh_nlpsp *nl, int norb, const double *psi, int
         return WVLH_OK;
     }
     const size_t cb = sizeof(double) * (size_t)norb * nl->ctot;
+    const int nub = (norb + kUpdBlock - 1) / kUpdBlock;
+    const size_t hb = sizeof(double) * (size_t)nub * kUpdBlock * nl->ctot;
     int rc;
-    if ((rc = nl->cf.ensure(cb)) || (rc = nl->hc.ensure(cb))) return nl_fail(rc);
+    if ((rc = nl->cf.ensure(cb)) || (rc = nl->hc.ensure(hb))) return nl_fail(rc);
     double *cf = (double *)nl->cf.p, *hc = (double *)nl->hc.p;
+    // the last block's columns past norb stay zero
+    if (norb % kUpdBlock && cudaMemsetAsync(hc + (size_t)(nub - 1) * kUpdBlock * nl->ctot, 0,
+                                            sizeof(double) * kUpdBlock * nl->ctot, st) != cudaSuccess)
+        return nl_fail(WVLH_ERR_CUDA);
     k_nl_dot<<<dim3(nl->natoms, nblk), 256, 0, st>>>(nl->d_atoms, nl->d_vals, nl->d_proj, psi, ld, norb, nl->ctot, cf);
     k_nl_coeff<<<norb, 128, 0, st>>>(nl->natoms, nl->d_atoms, nl->d_h, nl->ctot, cf, hc, eproj);
     if (nl->ngroups > 0)
-        k_nl_update<<<dim3((nl->ngroups + 7) / 8, nblk), 256, 0, st>>>(nl->ngroups, nl->d_rows, nl->d_rowv, nl->d_rrun,
-                                                                      nl->d_atoms, nl->d_proj, norb, nl->ctot, hc, ld,
-                                                                      hpsi);
+        k_nl_update<<<dim3((nl->ngroups + 7) / 8, nub), 256, 0, st>>>(nl->ngroups, nl->d_rows, nl->d_rowv, nl->d_rrun,
+                                                                     nl->d_atoms, nl->d_proj, norb, nl->ctot, hc, ld,
+                                                                     hpsi);
     if (cudaGetLastError() != cudaSuccess) return nl_fail(WVLH_ERR_CUDA);
     return WVLH_OK;
 }
