@@ -11,7 +11,12 @@ other ranks.  The exchanges are:
 * density: each rank's partial rho of its orbitals, summed over ranks and
   either replicated (all-reduce) or left distributed in z-slabs
   (``MPI_REDUCE_SCATTER`` in ``communicate_density``, ``sumrho.f90:219``)
-  -> :func:`reduce_density`.
+  -> :func:`reduce_density`;
+* overlap S = Psi Psi^T of orbitals held by different ranks: the orbital ->
+  component transposition (``transpose_v``, ``communications.f90:2318``, an
+  all-to-all), the symmetric product over the rank's slice of components
+  (``getOverlap``, ``wfn_opt/orthogonality.f90:2624-2697``) and the sum of the
+  partial matrices over ranks (``:2695``) -> :func:`overlap_sharded`.
 
 These functions take torch tensors and a ``torch.distributed`` process group:
 NCCL on GPUs, gloo for the CPU tests of this logic.
@@ -98,3 +103,56 @@ def reduce_density(rho, grid, group=None, scatter=False):
     dist.reduce_scatter_tensor(out, src.reshape(-1), group=group)
     a, b = slabs[rank]
     return out[:(b - a) * plane]
+
+
+def component_slices(ncoeff, world_size):
+    """[start, stop) of each rank's slice of the coefficients in the component
+    distribution (the first ncoeff % world_size ranks take one more)."""
+    return z_slabs(ncoeff, world_size)
+
+
+def overlap_sharded(psi_local, group=None, gram=None, ctx=None):
+    """S = Psi Psi^T (FP64, norb x norb on every rank) for orbitals sharded
+    over the ranks in order (rank r holds the (norb_r, ncoeff) rows
+    psi_local, ranks in orbital order).  The rows are transposed to the
+    component distribution with one all-to-all (each rank then holds all
+    orbitals on its slice of components), the slice's Gram matrix is formed
+    locally and the partial matrices are summed with an all-reduce.  gram(X)
+    returns X X^T: by default the library's FP64 tensor-core overlap kernel
+    (wvlh_overlap, needs ctx) for device tensors; the CPU tests pass a
+    matrix product."""
+    import torch
+    import torch.distributed as dist
+    if psi_local.dim() != 2:
+        raise ValueError("psi_local must be (norb_local, ncoeff)")
+    if gram is None:
+        if ctx is None:
+            raise ValueError("the device overlap needs the context (ctx)")
+        from .ortho import overlap as _overlap
+
+        def gram(X):
+            return _overlap(ctx, X)
+    ws = dist.get_world_size(group) if dist.is_initialized() else 1
+    if ws == 1:
+        return gram(psi_local.contiguous())
+    rank = dist.get_rank(group)
+    nloc, K = psi_local.shape
+    counts = torch.zeros(ws, dtype=torch.int64, device=psi_local.device)
+    counts[rank] = nloc
+    dist.all_reduce(counts, group=group)
+    counts = [int(c) for c in counts.tolist()]
+    norb = sum(counts)
+    sl = component_slices(K, ws)
+    lens = [b - a for a, b in sl]
+    # orbital -> component distribution: rank s receives every rank's rows
+    # restricted to its slice s (packed contiguous per destination)
+    send = torch.cat([psi_local[:, a:b].reshape(-1) for a, b in sl]) if nloc else \
+        psi_local.new_empty(0)
+    recv = psi_local.new_empty(norb * lens[rank])
+    dist.all_to_all_single(recv, send, output_split_sizes=[c * lens[rank] for c in counts],
+                           input_split_sizes=[nloc * n for n in lens], group=group)
+    X = recv.view(norb, lens[rank])       # ranks in orbital order
+    S = gram(X) if lens[rank] else torch.zeros(norb, norb, dtype=torch.float64, device=psi_local.device)
+    S = S.to(torch.float64).contiguous()
+    dist.all_reduce(S, group=group)
+    return S

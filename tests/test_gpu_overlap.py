@@ -99,3 +99,15 @@ def test_orthoconstraint_matches_oracle(oracle, torch_cuda, wctx, occ):
     assert np.abs(L.cpu().numpy() - lam).max() / np.abs(lam).max() < 1e-13
     assert np.abs(th.cpu().numpy() - g_ref).max() / np.abs(g_ref).max() < 1e-13
     assert abs(tr2 - tr) <= 1e-12 * abs(tr) and abs(asy2 - asy) <= 1e-12 * asy and abs(mix2 - mix) <= 1e-12 * max(mix, 1e-300)
+
+
+def test_overlap_sharded_single_process_uses_the_device_kernel(torch_cuda, wctx):
+    """Without a process group the sharded overlap is the library's overlap of
+    the local rows (the multi-rank exchange is covered by the gloo tests)."""
+    from wvlh.shard import overlap_sharded
+    torch = torch_cuda
+    g = torch.Generator(device="cuda").manual_seed(3)
+    X = torch.rand(40, 3001, generator=g, dtype=torch.float64, device="cuda") * 2 - 1
+    S = overlap_sharded(X, ctx=wctx)
+    ref = (X.cpu().numpy() @ X.cpu().numpy().T)
+    assert np.abs(S.cpu().numpy() - ref).max() <= 1e-13 * np.abs(ref).max()

@@ -1,6 +1,7 @@
 """Multi-process host logic of the orbital sharding (no GPU): world_size-2
 gloo process groups on CPU run the same exchange code that NCCL runs on
-GPUs (energy all-reduce, density all-reduce and z-slab reduce-scatter)."""
+GPUs (energy all-reduce, density all-reduce and z-slab reduce-scatter, the
+overlap's orbital -> component transposition and all-reduce)."""
 import socket
 
 import numpy as np
@@ -9,7 +10,8 @@ import torch
 import torch.multiprocessing as mp
 
 from wvlh.keys import Locreg
-from wvlh.shard import orbital_cost, reduce_density, allreduce_energies, shard_orbitals, z_slabs
+from wvlh.shard import (allreduce_energies, component_slices, orbital_cost, overlap_sharded, reduce_density,
+                        shard_orbitals, z_slabs)
 
 GRID = (6, 5, 7)  # (I1, I2, I3) of a small ISF grid
 
@@ -82,3 +84,37 @@ def test_z_slabs_and_cost():
     f[1:3, 1:3, 1:3] = True
     lr = Locreg.from_masks(m, f, (0, 0, 0), (0.5, 0.5, 0.5))
     assert orbital_cost(lr) == 64 + 7 * 8
+
+
+OV_COUNTS = {2: [5, 3], 3: [4, 0, 6]}   # orbitals per rank (one rank may hold none)
+OV_K = 29                               # coefficients (not a multiple of the ranks)
+
+
+def _ov_psi(world):
+    g = torch.Generator().manual_seed(7)
+    return torch.rand(sum(OV_COUNTS[world]), OV_K, generator=g, dtype=torch.float64) * 2 - 1
+
+
+def _ov_worker(rank, world, port, out):
+    import torch.distributed as dist
+    dist.init_process_group("gloo", init_method="tcp://127.0.0.1:%d" % port, rank=rank, world_size=world)
+    try:
+        psi = _ov_psi(world)
+        c = OV_COUNTS[world]
+        mine = psi[sum(c[:rank]):sum(c[:rank + 1])].clone()
+        S = overlap_sharded(mine, gram=lambda X: X @ X.T)
+        out[rank] = S.numpy().copy()
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("world", [2, 3])
+def test_overlap_transposition_and_allreduce(world):
+    mgr = mp.Manager()
+    out = mgr.dict()
+    mp.spawn(_ov_worker, args=(world, _free_port(), out), nprocs=world, join=True)
+    psi = _ov_psi(world).numpy()
+    ref = psi @ psi.T
+    for r in range(world):
+        assert np.abs(out[r] - ref).max() <= 1e-13 * np.abs(ref).max()
+    assert component_slices(OV_K, world)[-1][1] == OV_K
