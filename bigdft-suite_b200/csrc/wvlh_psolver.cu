@@ -26,8 +26,9 @@
 // on the host (the 89-Gaussian expansion of 1/r, gequad :1679-1873, each
 // Gaussian's 1D ISF overlaps and their cosine transforms) and summed into the
 // (N3/2+1, N2/2+1, N1/2+1) Fourier table on the device; each solve pads rho
-// into a persistent zero buffer of twice the size, D2Z, multiplies by the
-// table, Z2D, and crops the first octant.
+// into a persistent zero buffer, transforms (the 2D (y, x) transforms only
+// over the occupied half of the z-planes), multiplies by the table,
+// transforms back and crops the first octant.
 //
 // The exchange-correlation part of the Kohn-Sham potential is the reference's
 // default LDA (ixc = 1: the Goedecker-Teter-Hutter Pade fit of the
@@ -251,7 +252,8 @@ struct PsPlan {
     // free boundary conditions: padded sizes, Fourier table, padded input
     // (zero outside the density's octant) and padded output
     int nf[3] = {0, 0, 0};
-    DevBuf ker, pad, work;
+    cufftHandle fz = 0;     // z transforms over all (y, kx) columns
+    DevBuf ker, pad, work, zin;
 };
 
 // ---------------------------------------------------------------- free BC kernel
@@ -478,7 +480,8 @@ static void free_plan(PsPlan *pl)
 {
     if (pl->fwd) cufftDestroy(pl->fwd);
     if (pl->inv) cufftDestroy(pl->inv);
-    for (DevBuf *b : {&pl->spec, &pl->fac, &pl->part, &pl->ker, &pl->pad, &pl->work}) b->release();
+    if (pl->fz) cufftDestroy(pl->fz);
+    for (DevBuf *b : {&pl->spec, &pl->fac, &pl->part, &pl->ker, &pl->pad, &pl->work, &pl->zin}) b->release();
     delete pl;
 }
 
@@ -647,9 +650,15 @@ extern "C" int wvlh_ks_potential_periodic(wvlh_ctx *ctx, const int n[3], const d
     return WVLH_OK;
 }
 
-// the free-BC plan of a grid: cuFFT plans on the padded sizes, the Fourier
-// table of the kernel and the padded buffers (the input's zero padding is set
-// once; each solve rewrites only the density's octant)
+// the free-BC plan of a grid: the Fourier table of the kernel, the padded
+// buffers and three cuFFT plans that skip the all-zero half of the padded
+// volume: a 2D (y, x) D2Z over the n3 occupied z-planes only, a 1D z transform
+// of every (y, kx) column (z slowest, one stride), and on the way back the
+// same z transform then a 2D Z2D of the n3 planes that are kept.  Buffers:
+// pad (n3, N2, N1) real, zero outside the density's (n2, n1) corner; zin
+// (N3, N2, N1/2+1) complex, planes z >= n3 zero; spec (same shape) and work
+// (n3, N2, N1) real.  The zero parts are written once; no transform writes
+// into them.
 static int ps_free_plan(wvlh_ctx *ctx, const int n[3], const double h[3], PsPlan **out)
 {
     std::lock_guard<std::mutex> lock(g_ps_mutex);
@@ -663,11 +672,15 @@ static int ps_free_plan(wvlh_ctx *ctx, const int n[3], const double h[3], PsPlan
     for (int d = 0; d < 3; ++d) pl->nf[d] = fft_length(2 * n[d]);
     const int N1 = pl->nf[0], N2 = pl->nf[1], N3 = pl->nf[2];
     const int l1 = N1 / 2 + 1, l2 = N2 / 2 + 1, l3 = N3 / 2 + 1;
-    const size_t npad = (size_t)N3 * N2 * N1, nspec = (size_t)N3 * N2 * l1;
+    const size_t npad = (size_t)n[2] * N2 * N1, nspec = (size_t)N3 * N2 * l1;
     int rc = WVLH_OK;
-    if (cufftPlan3d(&pl->fwd, N3, N2, N1, CUFFT_D2Z) != CUFFT_SUCCESS ||
-        cufftPlan3d(&pl->inv, N3, N2, N1, CUFFT_Z2D) != CUFFT_SUCCESS)
-        rc = WVLH_ERR_CUDA;
+    {
+        int n2d[2] = {N2, N1}, rin[2] = {N2, N1}, cin[2] = {N2, l1}, nz[1] = {N3};
+        if (cufftPlanMany(&pl->fwd, 2, n2d, rin, 1, N2 * N1, cin, 1, N2 * l1, CUFFT_D2Z, n[2]) != CUFFT_SUCCESS ||
+            cufftPlanMany(&pl->inv, 2, n2d, cin, 1, N2 * l1, rin, 1, N2 * N1, CUFFT_Z2D, n[2]) != CUFFT_SUCCESS ||
+            cufftPlanMany(&pl->fz, 1, nz, nz, N2 * l1, 1, nz, N2 * l1, 1, CUFFT_Z2Z, N2 * l1) != CUFFT_SUCCESS)
+            rc = WVLH_ERR_CUDA;
+    }
     std::vector<double> tab;
     if (!rc) {
         free_kernel_tables(n, h, pl->nf, tab);
@@ -675,6 +688,7 @@ static int ps_free_plan(wvlh_ctx *ctx, const int n[3], const double h[3], PsPlan
             (rc = pl->fac.ensure(sizeof(double) * tab.size())) ||
             (rc = pl->pad.ensure(sizeof(double) * npad)) || (rc = pl->work.ensure(sizeof(double) * npad)) ||
             (rc = pl->spec.ensure(sizeof(cufftDoubleComplex) * nspec)) ||
+            (rc = pl->zin.ensure(sizeof(cufftDoubleComplex) * nspec)) ||
             (rc = pl->part.ensure(sizeof(double) * (size_t)(3 * kPsBlocks + 3))))
             ;
     }
@@ -683,7 +697,8 @@ static int ps_free_plan(wvlh_ctx *ctx, const int n[3], const double h[3], PsPlan
         cudaStream_t st = ctx->stream;
         bool ok = cudaMemcpyAsync(pl->fac.p, tab.data(), sizeof(double) * tab.size(), cudaMemcpyHostToDevice, st) ==
                       cudaSuccess &&
-                  cudaMemsetAsync(pl->pad.p, 0, sizeof(double) * npad, st) == cudaSuccess;
+                  cudaMemsetAsync(pl->pad.p, 0, sizeof(double) * npad, st) == cudaSuccess &&
+                  cudaMemsetAsync(pl->zin.p, 0, sizeof(cufftDoubleComplex) * nspec, st) == cudaSuccess;
         if (ok) {
             k_free_kernel<<<kPsBlocks, 256, 0, st>>>(l1, l2, l3, 89, (const double *)pl->fac.p, (double *)pl->ker.p);
             ok = cudaGetLastError() == cudaSuccess && cudaStreamSynchronize(st) == cudaSuccess;
@@ -717,14 +732,17 @@ static int ps_free_hartree(wvlh_ctx *ctx, const int n[3], const double h[3], con
     const int N1 = pl->nf[0], N2 = pl->nf[1], N3 = pl->nf[2];
     cudaStream_t st = ctx->stream;
     double *pad = (double *)pl->pad.p, *work = (double *)pl->work.p;
-    cufftDoubleComplex *z = (cufftDoubleComplex *)pl->spec.p;
+    cufftDoubleComplex *z = (cufftDoubleComplex *)pl->spec.p, *zin = (cufftDoubleComplex *)pl->zin.p;
     k_free_pad<<<kPsBlocks, 256, 0, st>>>(n[0], n[1], n[2], N1, N2, rho, pad);
     bool ok = cudaGetLastError() == cudaSuccess && cufftSetStream(pl->fwd, st) == CUFFT_SUCCESS &&
-              cufftSetStream(pl->inv, st) == CUFFT_SUCCESS && cufftExecD2Z(pl->fwd, pad, z) == CUFFT_SUCCESS;
+              cufftSetStream(pl->inv, st) == CUFFT_SUCCESS && cufftSetStream(pl->fz, st) == CUFFT_SUCCESS &&
+              cufftExecD2Z(pl->fwd, pad, zin) == CUFFT_SUCCESS &&               // (y, x) of the n3 planes
+              cufftExecZ2Z(pl->fz, zin, z, CUFFT_FORWARD) == CUFFT_SUCCESS;     // z of every column
     if (ok) {
         const double scal = h[0] * h[1] * h[2] / ((double)N1 * (double)N2 * (double)N3);
         k_free_multiply<<<kPsBlocks, 256, 0, st>>>(N1, N2, N3, (const double *)pl->ker.p, scal, z);
-        ok = cudaGetLastError() == cudaSuccess && cufftExecZ2D(pl->inv, z, work) == CUFFT_SUCCESS;
+        ok = cudaGetLastError() == cudaSuccess && cufftExecZ2Z(pl->fz, z, z, CUFFT_INVERSE) == CUFFT_SUCCESS &&
+             cufftExecZ2D(pl->inv, z, work) == CUFFT_SUCCESS;                   // the n3 planes kept
     }
     if (ok) {
         k_free_crop<<<kPsBlocks, 256, 0, st>>>(n[0], n[1], n[2], N1, N2, work, rho, pot,
