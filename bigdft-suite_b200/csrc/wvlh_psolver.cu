@@ -103,55 +103,78 @@ static void fourtrans_isf(int n, std::vector<double> &f)
     }
 }
 
-// one thread per complex coefficient of the D2Z output (n3, n2, n1/2 + 1)
-__global__ void k_ps_multiply(int n1, int n2, int n3, double L1, double L2, double L3,
-                              const double *__restrict__ fx, const double *__restrict__ fy,
-                              const double *__restrict__ fz, double scal, double zero,
-                              cufftDoubleComplex *__restrict__ z)
+// the D2Z spectrum (N3, N2, N1/2+1) times scal K(|k3|, |k2|, k1), K a real
+// table (N3/2+1, N2/2+1, N1/2+1) of the kernel; one warp per spectrum row.
+// zero_term: the k = 0 coefficient is set to (zero, 0) instead (the periodic
+// solver's offset term)
+__global__ void k_table_multiply(int N1, int N2, int N3, const double *__restrict__ ker, double scal, int zero_term,
+                                 double zero, cufftDoubleComplex *__restrict__ z)
 {
-    const int nh = n1 / 2 + 1;
-    const long long tot = (long long)n3 * n2 * nh;
-    const double pi = 3.14159265358979323846;
-    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < tot;
-         e += (long long)gridDim.x * blockDim.x) {
-        const int k1 = (int)(e % nh);
-        const long long r = e / nh;
-        const int k2 = (int)(r % n2), k3 = (int)(r / n2);
-        const int p2 = k2 <= n2 / 2 ? k2 : n2 - k2, p3 = k3 <= n3 / 2 ? k3 : n3 - k3;   // |frequency|
-        cufftDoubleComplex v = z[e];
-        if (k1 == 0 && k2 == 0 && k3 == 0) {
-            v.x = zero;
-            v.y = 0.0;
-        } else {
-            const double g1 = k1 / L1, g2 = p2 / L2, g3 = p3 / L3;
-            const double g = g1 * g1 + g2 * g2 + g3 * g3;
-            const double f = fx[k1] * fy[p2] * fz[p3] / (pi * g) * scal;
+    const int nh = N1 / 2 + 1, l2 = N2 / 2 + 1;
+    const int lane = threadIdx.x & 31;
+    const int nrow = N3 * N2;
+    const int w0 = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5), nw = (int)((gridDim.x * blockDim.x) >> 5);
+    for (int r = w0; r < nrow; r += nw) {
+        const int k3 = r / N2, k2 = r - k3 * N2;
+        const int p2 = k2 <= N2 / 2 ? k2 : N2 - k2, p3 = k3 <= N3 / 2 ? k3 : N3 - k3;   // |frequency|
+        const double *kr = ker + ((size_t)p3 * l2 + p2) * nh;
+        cufftDoubleComplex *zr = z + (size_t)r * nh;
+        for (int k1 = lane; k1 < nh; k1 += 32) {
+            cufftDoubleComplex v = zr[k1];
+            const double f = kr[k1] * scal;
             v.x *= f;
             v.y *= f;
+            if (zero_term && r == 0 && k1 == 0) {
+                v.x = zero;
+                v.y = 0.0;
+            }
+            zr[k1] = v;
         }
-        z[e] = v;
     }
 }
 
-// fixed-order sum of rho * V: per-block partials, then one block over them
+// Each block writes its K partial sums v[k] (block_sum over the threads) to
+// part[K b + k]; the last block to arrive (counted in *cnt) sums the blocks'
+// partials in block order and writes out[k] = sc[k] * sum, then resets the
+// counter for the next launch.  The order of every sum is fixed by the grid:
+// deterministic.  Called by every thread of the block.
+template <int K>
+__device__ __forceinline__ void finish_partials(const double (&v)[K], double *__restrict__ part, unsigned int *cnt,
+                                                const double (&sc)[K], double *__restrict__ out, double *red)
+{
+    __shared__ bool last;
+    double t[K];
+#pragma unroll
+    for (int k = 0; k < K; ++k) t[k] = block_sum(v[k], red);
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int k = 0; k < K; ++k) part[K * blockIdx.x + k] = t[k];
+        __threadfence();
+        last = atomicAdd(cnt, 1u) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+        double s = 0.0;
+        for (int i = threadIdx.x; i < (int)gridDim.x; i += blockDim.x) s += __ldcg(part + K * i + k);
+        const double r = block_sum(s, red);
+        if (threadIdx.x == 0) out[k] = r * sc[k];
+    }
+    if (threadIdx.x == 0) *cnt = 0u;
+}
+
+// out = scale sum(a b) (the Hartree energy of the periodic solver)
 __global__ void k_ps_dot(long long n, const double *__restrict__ a, const double *__restrict__ b,
-                         double *__restrict__ part)
+                         double *__restrict__ part, unsigned int *cnt, double scale, double *__restrict__ out)
 {
     __shared__ double red[32];
     double s = 0.0;
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
         s = fma(a[i], b[i], s);
-    const double t = block_sum(s, red);
-    if (threadIdx.x == 0) part[blockIdx.x] = t;
-}
-
-__global__ void k_ps_sum(int n, const double *__restrict__ part, double scale, double *__restrict__ out)
-{
-    __shared__ double red[32];
-    double s = 0.0;
-    for (int i = threadIdx.x; i < n; i += blockDim.x) s += part[i];
-    const double t = block_sum(s, red);
-    if (threadIdx.x == 0) *out = t * scale;
+    const double v[1] = {s}, sc[1] = {scale};
+    finish_partials<1>(v, part, cnt, sc, out, red);
 }
 
 // Teter 1993 paramagnetic parameters (abi_xcspol.F90:105-112) and
@@ -179,11 +202,11 @@ __device__ __forceinline__ void teter_lda(double rho, double &eps, double &v)
     v = eps - (1.0 / 3.0) * rs * deps;
 }
 
-// V_xc of every point (written, or added when ACC), per-block partial sums of
-// eps rho and v rho (xc_energy_new, orbitals/xc.f90:888-917) in part[2 b + 0/1]
+// V_xc of every point (written, or added when ACC); with out, out[0..1] =
+// dvol (sum eps rho, sum v rho) (xc_energy_new, orbitals/xc.f90:888-917)
 template <bool ACC>
 __global__ void k_xc_lda(long long n, const double *__restrict__ rho, double *__restrict__ vxc,
-                         double *__restrict__ part)
+                         double *__restrict__ part, unsigned int *cnt, double dvol, double *__restrict__ out)
 {
     __shared__ double red[32];
     double se = 0.0, sv = 0.0;
@@ -195,19 +218,17 @@ __global__ void k_xc_lda(long long n, const double *__restrict__ rho, double *__
         sv = fma(v, r, sv);
         vxc[i] = ACC ? vxc[i] + v : v;
     }
-    const double te = block_sum(se, red);
-    const double tv = block_sum(sv, red);
-    if (threadIdx.x == 0) {
-        part[2 * blockIdx.x] = te;
-        part[2 * blockIdx.x + 1] = tv;
-    }
+    if (!out) return;
+    const double v[2] = {se, sv}, sc[2] = {dvol, dvol};
+    finish_partials<2>(v, part, cnt, sc, out, red);
 }
 
 // the Kohn-Sham potential from V_H (in pot): pot = (V_H + V_ext) + V_xc, the
 // order of H_potential's sum with pot_ion then updatePotential's axpy of V_XC;
-// per-block partials of rho V_H, eps rho, v rho in part[3 b + 0/1/2]
+// with out, out[0..2] = (0.5 dvol sum rho V_H, dvol sum eps rho, dvol sum v rho)
 __global__ void k_ks_combine(long long n, const double *__restrict__ rho, const double *__restrict__ vext,
-                             double *__restrict__ pot, double *__restrict__ part)
+                             double *__restrict__ pot, double *__restrict__ part, unsigned int *cnt, double dvol,
+                             double *__restrict__ out)
 {
     __shared__ double red[32];
     double sh = 0.0, se = 0.0, sv = 0.0;
@@ -220,35 +241,16 @@ __global__ void k_ks_combine(long long n, const double *__restrict__ rho, const 
         sv = fma(v, r, sv);
         pot[i] = (vext ? vh + vext[i] : vh) + v;
     }
-    const double th = block_sum(sh, red);
-    const double te = block_sum(se, red);
-    const double tv = block_sum(sv, red);
-    if (threadIdx.x == 0) {
-        part[3 * blockIdx.x] = th;
-        part[3 * blockIdx.x + 1] = te;
-        part[3 * blockIdx.x + 2] = tv;
-    }
-}
-
-// out[k] = scale[k] * sum over blocks of part[K b + k], blocks in a fixed order
-template <int K>
-__global__ void k_ps_sum_k(int nblk, const double *__restrict__ part, double s0, double s1, double s2,
-                           double *__restrict__ out)
-{
-    __shared__ double red[32];
-    const double sc[3] = {s0, s1, s2};
-#pragma unroll
-    for (int k = 0; k < K; ++k) {
-        double s = 0.0;
-        for (int i = threadIdx.x; i < nblk; i += blockDim.x) s += part[K * i + k];
-        const double t = block_sum(s, red);
-        if (threadIdx.x == 0) out[k] = t * sc[k];
-    }
+    if (!out) return;
+    const double v[3] = {sh, se, sv}, sc[3] = {0.5 * dvol, dvol, dvol};
+    finish_partials<3>(v, part, cnt, sc, out, red);
 }
 
 struct PsPlan {
     cufftHandle fwd = 0, inv = 0;
-    DevBuf spec, fac, part;
+    DevBuf spec, fac, part, cnt;          // cnt: the block-arrival counter of the energy sums
+    bool cnt_zeroed = false;
+    double tab_h[3] = {0.0, 0.0, 0.0};   // spacings the periodic kernel table in ker was built for
     // free boundary conditions: padded sizes, Fourier table, padded input
     // (zero outside the density's octant) and padded output
     int nf[3] = {0, 0, 0};
@@ -423,46 +425,30 @@ __global__ void k_free_pad(int n1, int n2, int n3, int N1, int N2, const double 
     }
 }
 
-// the D2Z spectrum (N3, N2, N1/2+1) times scal K(|k3|, |k2|, k1)
-__global__ void k_free_multiply(int N1, int N2, int N3, const double *__restrict__ ker, double scal,
-                                cufftDoubleComplex *__restrict__ z)
-{
-    const int nh = N1 / 2 + 1, l2 = N2 / 2 + 1;
-    const long long tot = (long long)N3 * N2 * nh;
-    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < tot;
-         e += (long long)gridDim.x * blockDim.x) {
-        const int k1 = (int)(e % nh);
-        const long long r = e / nh;
-        const int k2 = (int)(r % N2), k3 = (int)(r / N2);
-        const int p2 = k2 <= N2 / 2 ? k2 : N2 - k2, p3 = k3 <= N3 / 2 ? k3 : N3 - k3;
-        const double f = ker[((long long)p3 * l2 + p2) * nh + k1] * scal;
-        cufftDoubleComplex v = z[e];
-        v.x *= f;
-        v.y *= f;
-        z[e] = v;
-    }
-}
-
-// pot = the first octant of the padded result; per-block partials of rho pot
+// pot = the first octant of the padded result (rows (i3, i2) of the
+// (n3, N2, N1) output); with out, *out = scale sum(rho pot)
 __global__ void k_free_crop(int n1, int n2, int n3, int N1, int N2, const double *__restrict__ work,
-                            const double *__restrict__ rho, double *__restrict__ pot, double *__restrict__ part)
+                            const double *__restrict__ rho, double *__restrict__ pot, double *__restrict__ part,
+                            unsigned int *cnt, double scale, double *__restrict__ out)
 {
     __shared__ double red[32];
-    const long long tot = (long long)n3 * n2 * n1;
+    const int lane = threadIdx.x & 31;
+    const int nrow = n3 * n2;
+    const int w0 = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5), nw = (int)((gridDim.x * blockDim.x) >> 5);
     double s = 0.0;
-    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < tot;
-         e += (long long)gridDim.x * blockDim.x) {
-        const int i1 = (int)(e % n1);
-        const long long r = e / n1;
-        const int i2 = (int)(r % n2), i3 = (int)(r / n2);
-        const double v = work[((long long)i3 * N2 + i2) * N1 + i1];
-        if (part) s = fma(rho[e], v, s);
-        pot[e] = v;
+    for (int r = w0; r < nrow; r += nw) {
+        const int i3 = r / n2, i2 = r - i3 * n2;
+        const double *wr = work + ((size_t)i3 * N2 + i2) * N1;
+        const size_t o = (size_t)r * n1;
+        for (int i1 = lane; i1 < n1; i1 += 32) {
+            const double v = wr[i1];
+            if (out) s = fma(rho[o + i1], v, s);
+            pot[o + i1] = v;
+        }
     }
-    if (part) {
-        const double t = block_sum(s, red);
-        if (threadIdx.x == 0) part[blockIdx.x] = t;
-    }
+    if (!out) return;
+    const double v[1] = {s}, sc[1] = {scale};
+    finish_partials<1>(v, part, cnt, sc, out, red);
 }
 
 }  // namespace wvlh
@@ -481,7 +467,8 @@ static void free_plan(PsPlan *pl)
     if (pl->fwd) cufftDestroy(pl->fwd);
     if (pl->inv) cufftDestroy(pl->inv);
     if (pl->fz) cufftDestroy(pl->fz);
-    for (DevBuf *b : {&pl->spec, &pl->fac, &pl->part, &pl->ker, &pl->pad, &pl->work, &pl->zin}) b->release();
+    for (DevBuf *b : {&pl->spec, &pl->fac, &pl->part, &pl->cnt, &pl->ker, &pl->pad, &pl->work, &pl->zin})
+        b->release();
     delete pl;
 }
 
@@ -518,6 +505,19 @@ static bool ps_args_ok(const int n[3], const double h[3])
     return true;
 }
 
+// the energy partials (3 per block) and the zeroed block-arrival counter
+static int ps_energy_buffers(wvlh_ctx *ctx, PsPlan *pl)
+{
+    int rc;
+    if ((rc = pl->part.ensure(sizeof(double) * (size_t)(3 * kPsBlocks + 3))) || (rc = pl->cnt.ensure(256)))
+        return rc;
+    if (!pl->cnt_zeroed) {
+        if (cudaMemsetAsync(pl->cnt.p, 0, 256, ctx->stream) != cudaSuccess) return WVLH_ERR_CUDA;
+        pl->cnt_zeroed = true;
+    }
+    return WVLH_OK;
+}
+
 // V_H of rho into pot (D2Z, kernel multiply, Z2D on the context's stream);
 // returns the grid's plan (its part buffer holds kPsBlocks * 3 doubles)
 static int ps_hartree(wvlh_ctx *ctx, const int n[3], const double h[3], const double *rho, double *pot,
@@ -547,30 +547,42 @@ static int ps_hartree(wvlh_ctx *ctx, const int n[3], const double h[3], const do
         pl = it->second;
     }
     int rc;
+    const int l1 = n1 / 2 + 1, l2 = n2 / 2 + 1, l3 = n3 / 2 + 1;
     if ((rc = pl->spec.ensure(sizeof(cufftDoubleComplex) * (size_t)nc)) ||
-        (rc = pl->fac.ensure(sizeof(double) * (size_t)(n1 / 2 + n2 / 2 + n3 / 2 + 3))) ||
-        (rc = pl->part.ensure(sizeof(double) * (size_t)(3 * kPsBlocks + 3))))
+        (rc = pl->ker.ensure(sizeof(double) * (size_t)l3 * l2 * l1)) || (rc = ps_energy_buffers(ctx, pl)))
         return rc;
-    std::vector<double> fx, fy, fz;
-    fourtrans_isf(n1 / 2, fx);
-    fourtrans_isf(n2 / 2, fy);
-    fourtrans_isf(n3 / 2, fz);
-    std::vector<double> fac(fx);
-    fac.insert(fac.end(), fy.begin(), fy.end());
-    fac.insert(fac.end(), fz.begin(), fz.end());
     cudaStream_t st = ctx->stream;
-    double *d_fac = (double *)pl->fac.p;
+    if (pl->tab_h[0] != h[0] || pl->tab_h[1] != h[1] || pl->tab_h[2] != h[2]) {
+        // the kernel table of this grid and spacing, (l3, l2, l1), k = 0 unused:
+        // K = phi^_x phi^_y phi^_z / (pi g^2) at the folded frequencies
+        std::vector<double> fx, fy, fz;
+        fourtrans_isf(n1 / 2, fx);
+        fourtrans_isf(n2 / 2, fy);
+        fourtrans_isf(n3 / 2, fz);
+        const double pi = 3.14159265358979323846, L1 = n1 * h[0], L2 = n2 * h[1], L3 = n3 * h[2];
+        std::vector<double> tab((size_t)l3 * l2 * l1, 0.0);
+        for (int p3 = 0; p3 < l3; ++p3)
+            for (int p2 = 0; p2 < l2; ++p2)
+                for (int k1 = 0; k1 < l1; ++k1) {
+                    if (!k1 && !p2 && !p3) continue;
+                    const double g1 = k1 / L1, g2 = p2 / L2, g3 = p3 / L3;
+                    const double g = g1 * g1 + g2 * g2 + g3 * g3;
+                    tab[((size_t)p3 * l2 + p2) * l1 + k1] = fx[k1] * fy[p2] * fz[p3] / (pi * g);
+                }
+        if (cudaMemcpyAsync(pl->ker.p, tab.data(), sizeof(double) * tab.size(), cudaMemcpyHostToDevice, st) !=
+                cudaSuccess ||
+            cudaStreamSynchronize(st) != cudaSuccess)
+            return WVLH_ERR_CUDA;
+        for (int d = 0; d < 3; ++d) pl->tab_h[d] = h[d];
+    }
     cufftDoubleComplex *z = (cufftDoubleComplex *)pl->spec.p;
-    cudaError_t e = cudaMemcpyAsync(d_fac, fac.data(), sizeof(double) * fac.size(), cudaMemcpyHostToDevice, st);
-    bool ok = e == cudaSuccess && cufftSetStream(pl->fwd, st) == CUFFT_SUCCESS &&
-              cufftSetStream(pl->inv, st) == CUFFT_SUCCESS &&
+    bool ok = cufftSetStream(pl->fwd, st) == CUFFT_SUCCESS && cufftSetStream(pl->inv, st) == CUFFT_SUCCESS &&
               cufftExecD2Z(pl->fwd, (cufftDoubleReal *)rho, z) == CUFFT_SUCCESS;
     const double vol = h[0] * h[1] * h[2];
     const double scal = 1.0 / ((double)n1 * (double)n2 * (double)n3);
     if (ok) {
-        k_ps_multiply<<<kPsBlocks, 256, 0, st>>>(n1, n2, n3, n1 * h[0], n2 * h[1], n3 * h[2], d_fac,
-                                                 d_fac + fx.size(), d_fac + fx.size() + fy.size(), scal,
-                                                 offset / vol * scal, z);
+        k_table_multiply<<<kPsBlocks, 256, 0, st>>>(n1, n2, n3, (const double *)pl->ker.p, scal, 1,
+                                                    offset / vol * scal, z);
         ok = cudaGetLastError() == cudaSuccess;
     }
     if (ok) ok = cufftExecZ2D(pl->inv, z, (cufftDoubleReal *)pot) == CUFFT_SUCCESS;
@@ -595,9 +607,8 @@ extern "C" int wvlh_psolver_periodic(wvlh_ctx *ctx, const int n[3], const double
     if (rc) return ps_fail(rc);
     if (eh) {
         const long long npt = (long long)n[0] * n[1] * n[2];
-        double *part = (double *)pl->part.p;
-        k_ps_dot<<<kPsBlocks, 256, 0, ctx->stream>>>(npt, rho, pot, part);
-        k_ps_sum<<<1, 1024, 0, ctx->stream>>>(kPsBlocks, part, 0.5 * h[0] * h[1] * h[2], eh);
+        k_ps_dot<<<kPsBlocks, 256, 0, ctx->stream>>>(npt, rho, pot, (double *)pl->part.p, (unsigned int *)pl->cnt.p,
+                                                     0.5 * h[0] * h[1] * h[2], eh);
         if (cudaGetLastError() != cudaSuccess) return ps_fail(WVLH_ERR_CUDA);
     }
     return WVLH_OK;
@@ -619,15 +630,15 @@ extern "C" int wvlh_xc_lda(wvlh_ctx *ctx, int64_t npts, const double *rho, doubl
         if (it == g_ps_plans.end()) it = g_ps_plans.emplace(key, new PsPlan()).first;
         pl = it->second;
     }
-    int rc = pl->part.ensure(sizeof(double) * (size_t)(3 * kPsBlocks + 3));
+    int rc = ps_energy_buffers(ctx, pl);
     if (rc) return ps_fail(rc);
     double *part = (double *)pl->part.p;
+    unsigned int *cnt = (unsigned int *)pl->cnt.p;
     cudaStream_t st = ctx->stream;
     if (accumulate)
-        k_xc_lda<true><<<kPsBlocks, 256, 0, st>>>(npts, rho, vxc, part);
+        k_xc_lda<true><<<kPsBlocks, 256, 0, st>>>(npts, rho, vxc, part, cnt, dvol, energies);
     else
-        k_xc_lda<false><<<kPsBlocks, 256, 0, st>>>(npts, rho, vxc, part);
-    if (energies) k_ps_sum_k<2><<<1, 1024, 0, st>>>(kPsBlocks, part, dvol, dvol, 0.0, energies);
+        k_xc_lda<false><<<kPsBlocks, 256, 0, st>>>(npts, rho, vxc, part, cnt, dvol, energies);
     if (cudaGetLastError() != cudaSuccess) return ps_fail(WVLH_ERR_CUDA);
     return WVLH_OK;
 }
@@ -643,9 +654,8 @@ extern "C" int wvlh_ks_potential_periodic(wvlh_ctx *ctx, const int n[3], const d
     if (rc) return ps_fail(rc);
     const long long npt = (long long)n[0] * n[1] * n[2];
     const double dvol = h[0] * h[1] * h[2];
-    double *part = (double *)pl->part.p;
-    k_ks_combine<<<kPsBlocks, 256, 0, ctx->stream>>>(npt, rho, vext, pot, part);
-    if (energies) k_ps_sum_k<3><<<1, 1024, 0, ctx->stream>>>(kPsBlocks, part, 0.5 * dvol, dvol, dvol, energies);
+    k_ks_combine<<<kPsBlocks, 256, 0, ctx->stream>>>(npt, rho, vext, pot, (double *)pl->part.p,
+                                                     (unsigned int *)pl->cnt.p, dvol, energies);
     if (cudaGetLastError() != cudaSuccess) return ps_fail(WVLH_ERR_CUDA);
     return WVLH_OK;
 }
@@ -688,8 +698,7 @@ static int ps_free_plan(wvlh_ctx *ctx, const int n[3], const double h[3], PsPlan
             (rc = pl->fac.ensure(sizeof(double) * tab.size())) ||
             (rc = pl->pad.ensure(sizeof(double) * npad)) || (rc = pl->work.ensure(sizeof(double) * npad)) ||
             (rc = pl->spec.ensure(sizeof(cufftDoubleComplex) * nspec)) ||
-            (rc = pl->zin.ensure(sizeof(cufftDoubleComplex) * nspec)) ||
-            (rc = pl->part.ensure(sizeof(double) * (size_t)(3 * kPsBlocks + 3))))
+            (rc = pl->zin.ensure(sizeof(cufftDoubleComplex) * nspec)) || (rc = ps_energy_buffers(ctx, pl)))
             ;
     }
     if (!rc) {
@@ -721,9 +730,10 @@ static bool ps_free_args_ok(const int n[3], const double h[3])
     return true;
 }
 
-// V_H of rho with free boundary conditions into pot; eh partials when part
+// V_H of rho with free boundary conditions into pot; with eh, *eh = the
+// Hartree energy (reduced by the crop)
 static int ps_free_hartree(wvlh_ctx *ctx, const int n[3], const double h[3], const double *rho, double *pot,
-                           bool energy, PsPlan **out)
+                           double *eh, PsPlan **out)
 {
     if (cudaSetDevice(ctx->device) != cudaSuccess) return WVLH_ERR_CUDA;
     PsPlan *pl = nullptr;
@@ -740,13 +750,13 @@ static int ps_free_hartree(wvlh_ctx *ctx, const int n[3], const double h[3], con
               cufftExecZ2Z(pl->fz, zin, z, CUFFT_FORWARD) == CUFFT_SUCCESS;     // z of every column
     if (ok) {
         const double scal = h[0] * h[1] * h[2] / ((double)N1 * (double)N2 * (double)N3);
-        k_free_multiply<<<kPsBlocks, 256, 0, st>>>(N1, N2, N3, (const double *)pl->ker.p, scal, z);
+        k_table_multiply<<<kPsBlocks, 256, 0, st>>>(N1, N2, N3, (const double *)pl->ker.p, scal, 0, 0.0, z);
         ok = cudaGetLastError() == cudaSuccess && cufftExecZ2Z(pl->fz, z, z, CUFFT_INVERSE) == CUFFT_SUCCESS &&
              cufftExecZ2D(pl->inv, z, work) == CUFFT_SUCCESS;                   // the n3 planes kept
     }
     if (ok) {
-        k_free_crop<<<kPsBlocks, 256, 0, st>>>(n[0], n[1], n[2], N1, N2, work, rho, pot,
-                                               energy ? (double *)pl->part.p : nullptr);
+        k_free_crop<<<kPsBlocks, 256, 0, st>>>(n[0], n[1], n[2], N1, N2, work, rho, pot, (double *)pl->part.p,
+                                               (unsigned int *)pl->cnt.p, 0.5 * h[0] * h[1] * h[2], eh);
         ok = cudaGetLastError() == cudaSuccess;
     }
     if (!ok) return WVLH_ERR_CUDA;
@@ -762,12 +772,8 @@ extern "C" int wvlh_psolver_free(wvlh_ctx *ctx, const int n[3], const double h[3
     if (!ctx || !n || !h || !rho || !pot || (eh && pot == rho) || !ps_free_args_ok(n, h))
         return ps_fail(WVLH_ERR_ARG);
     PsPlan *pl = nullptr;
-    int rc = ps_free_hartree(ctx, n, h, rho, pot, eh != nullptr, &pl);
+    int rc = ps_free_hartree(ctx, n, h, rho, pot, eh, &pl);
     if (rc) return ps_fail(rc);
-    if (eh) {
-        k_ps_sum<<<1, 1024, 0, ctx->stream>>>(kPsBlocks, (const double *)pl->part.p, 0.5 * h[0] * h[1] * h[2], eh);
-        if (cudaGetLastError() != cudaSuccess) return ps_fail(WVLH_ERR_CUDA);
-    }
     return WVLH_OK;
 }
 
@@ -777,13 +783,12 @@ extern "C" int wvlh_ks_potential_free(wvlh_ctx *ctx, const int n[3], const doubl
     if (!ctx || !n || !h || !rho || !pot || pot == rho || (vext && vext == pot) || !ps_free_args_ok(n, h))
         return ps_fail(WVLH_ERR_ARG);
     PsPlan *pl = nullptr;
-    int rc = ps_free_hartree(ctx, n, h, rho, pot, false, &pl);
+    int rc = ps_free_hartree(ctx, n, h, rho, pot, nullptr, &pl);
     if (rc) return ps_fail(rc);
     const long long npt = (long long)n[0] * n[1] * n[2];
     const double dvol = h[0] * h[1] * h[2];
-    double *part = (double *)pl->part.p;
-    k_ks_combine<<<kPsBlocks, 256, 0, ctx->stream>>>(npt, rho, vext, pot, part);
-    if (energies) k_ps_sum_k<3><<<1, 1024, 0, ctx->stream>>>(kPsBlocks, part, 0.5 * dvol, dvol, dvol, energies);
+    k_ks_combine<<<kPsBlocks, 256, 0, ctx->stream>>>(npt, rho, vext, pot, (double *)pl->part.p,
+                                                     (unsigned int *)pl->cnt.p, dvol, energies);
     if (cudaGetLastError() != cudaSuccess) return ps_fail(WVLH_ERR_CUDA);
     return WVLH_OK;
 }
