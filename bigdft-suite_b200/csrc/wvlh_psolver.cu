@@ -246,6 +246,106 @@ __global__ void k_ks_combine(long long n, const double *__restrict__ rho, const 
     finish_partials<3>(v, part, cnt, sc, out, red);
 }
 
+// ferromagnetic - paramagnetic differences of the fit (abi_xcspol.F90:113-116)
+struct Teter93Spin {
+    static constexpr double da0 = 0.119086804055547, da1 = 0.6157402568883345, da2 = 0.1574201515892867,
+                            da3 = 0.003532336663397157;
+    static constexpr double db1 = 0.0, db2 = 0.2673612973836267, db3 = 0.2052004607777787,
+                            db4 = 0.004200005045691381;
+    static constexpr double alpha = 1.0 - 1.0e-6;
+};
+
+// eps_xc and v_xc of both spins (xcspol, nspden = 2, order 1, :355-395):
+// zeta = 2 up / rho - 1, the parameters interpolated with
+// f(zeta) = ((1 + a z)^(4/3) + (1 - a z)^(4/3) - 2) / (2^(4/3) - 2),
+// v_up/dn = v_para - (zeta -/+ 1) d eps / d zeta
+__device__ __forceinline__ void teter_lsda(double up, double dn, double &eps, double &vu, double &vd)
+{
+    using T = Teter93;
+    using S = Teter93Spin;
+    const double rho = up + dn;
+    const double zet = 2.0 * up / rho - 1.0;
+    const double rs = T::rsfac * copysign(rcbrt(fabs(rho)), rho);
+    const double fact = 1.0 / (2.5198420997897464 - 2.0);   // 2^(4/3) = 2.5198420997897464
+    const double zp = 1.0 + zet * S::alpha, zm = 1.0 - zet * S::alpha;
+    const double zp3 = cbrt(zp), zm3 = cbrt(zm);
+    const double fxc = (zp * zp3 + zm * zm3 - 2.0) * fact;
+    const double a0 = T::a0 + fxc * S::da0, a1 = T::a1 + fxc * S::da1, a2 = T::a2 + fxc * S::da2,
+                 a3 = T::a3 + fxc * S::da3;
+    const double b1 = T::b1 + fxc * S::db1, b2 = T::b2 + fxc * S::db2, b3 = T::b3 + fxc * S::db3,
+                 b4 = T::b4 + fxc * S::db4;
+    const double n1 = a0 + rs * (a1 + rs * (a2 + rs * a3));
+    const double d1 = rs * (b1 + rs * (b2 + rs * (b3 + rs * b4)));
+    const double d1m1 = 1.0 / d1;
+    eps = -n1 * d1m1;
+    const double dn1 = a1 + rs * (2.0 * a2 + rs * (3.0 * a3));
+    const double dd1 = b1 + rs * (2.0 * b2 + rs * (3.0 * b3 + rs * (4.0 * b4)));
+    const double vp = eps - (1.0 / 3.0) * rs * (-(dn1 + eps * dd1) * d1m1);
+    const double dfdz = (4.0 / 3.0) * S::alpha * (zp3 - zm3) * fact;
+    const double dn1df = S::da0 + rs * (S::da1 + rs * (S::da2 + rs * S::da3));
+    const double dd1df = rs * (S::db1 + rs * (S::db2 + rs * (S::db3 + rs * S::db4)));
+    const double dedz = dfdz * (-(dn1df + eps * dd1df) * d1m1);
+    vu = vp - (zet - 1.0) * dedz;
+    vd = vp - (zet + 1.0) * dedz;
+}
+
+// V_xc of both spins (written, or added when ACC); with out, out[0..1] =
+// dvol (sum eps rho, sum_sigma v_sigma rho_sigma) (xc_energy_new :888-917)
+template <bool ACC>
+__global__ void k_xc_lsda(long long n, const double *__restrict__ up, const double *__restrict__ dn,
+                          double *__restrict__ vu, double *__restrict__ vd, double *__restrict__ part,
+                          unsigned int *cnt, double dvol, double *__restrict__ out)
+{
+    __shared__ double red[32];
+    double se = 0.0, sv = 0.0;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        const double ru = up[i], rd = dn[i];
+        double e, a, b;
+        teter_lsda(ru, rd, e, a, b);
+        se = fma(e, ru + rd, se);
+        sv = fma(a, ru, fma(b, rd, sv));
+        vu[i] = ACC ? vu[i] + a : a;
+        vd[i] = ACC ? vd[i] + b : b;
+    }
+    if (!out) return;
+    const double v[2] = {se, sv}, sc[2] = {dvol, dvol};
+    finish_partials<2>(v, part, cnt, sc, out, red);
+}
+
+// the total density of the two spins (the Hartree solve's input)
+__global__ void k_spin_total(long long n, const double *__restrict__ up, const double *__restrict__ dn,
+                             double *__restrict__ tot)
+{
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        tot[i] = up[i] + dn[i];
+}
+
+// the spin-polarised Kohn-Sham potentials from V_H (in pu): p_sigma =
+// (V_H + V_ext) + V_xc,sigma (updatePotential with nspin = 2); with out,
+// out[0..2] = (0.5 dvol sum rho V_H, dvol sum eps rho, dvol sum_sigma v rho)
+__global__ void k_ks_combine_spin(long long n, const double *__restrict__ up, const double *__restrict__ dn,
+                                  const double *__restrict__ vext, double *__restrict__ pu, double *__restrict__ pd,
+                                  double *__restrict__ part, unsigned int *cnt, double dvol, double *__restrict__ out)
+{
+    __shared__ double red[32];
+    double sh = 0.0, se = 0.0, sv = 0.0;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        const double ru = up[i], rd = dn[i], vh = pu[i];
+        double e, a, b;
+        teter_lsda(ru, rd, e, a, b);
+        const double r = ru + rd;
+        sh = fma(vh, r, sh);
+        se = fma(e, r, se);
+        sv = fma(a, ru, fma(b, rd, sv));
+        const double base = vext ? vh + vext[i] : vh;
+        pu[i] = base + a;
+        pd[i] = base + b;
+    }
+    if (!out) return;
+    const double v[3] = {sh, se, sv}, sc[3] = {0.5 * dvol, dvol, dvol};
+    finish_partials<3>(v, part, cnt, sc, out, red);
+}
+
 struct PsPlan {
     cufftHandle fwd = 0, inv = 0;
     DevBuf spec, fac, part, cnt;          // cnt: the block-arrival counter of the energy sums
@@ -804,4 +904,59 @@ extern "C" int64_t wvlh_psolver_free_tables(const int n[3], const double h[3], i
     free_kernel_tables(n, h, nf, t);
     std::copy(t.begin(), t.end(), tab);
     return need;
+}
+
+extern "C" int wvlh_xc_lsda(wvlh_ctx *ctx, int64_t npts, const double *rho_up, const double *rho_dn, double *vxc_up,
+                            double *vxc_dn, int accumulate, double dvol, double *energies)
+{
+    // each point's two densities are read before its potentials are written
+    if (!ctx || npts < 0 || (npts > 0 && (!rho_up || !rho_dn || !vxc_up || !vxc_dn)) || vxc_up == vxc_dn)
+        return ps_fail(WVLH_ERR_ARG);
+    if (cudaSetDevice(ctx->device) != cudaSuccess) return ps_fail(WVLH_ERR_CUDA);
+    if (npts == 0 && !energies) return WVLH_OK;
+    PsPlan *pl;
+    {
+        std::lock_guard<std::mutex> lock(g_ps_mutex);
+        const auto key = std::make_tuple((const void *)ctx, ctx->device, 0, 0, 0);
+        auto it = g_ps_plans.find(key);
+        if (it == g_ps_plans.end()) it = g_ps_plans.emplace(key, new PsPlan()).first;
+        pl = it->second;
+    }
+    int rc = ps_energy_buffers(ctx, pl);
+    if (rc) return ps_fail(rc);
+    double *part = (double *)pl->part.p;
+    unsigned int *cnt = (unsigned int *)pl->cnt.p;
+    cudaStream_t st = ctx->stream;
+    if (accumulate)
+        k_xc_lsda<true><<<kPsBlocks, 256, 0, st>>>(npts, rho_up, rho_dn, vxc_up, vxc_dn, part, cnt, dvol, energies);
+    else
+        k_xc_lsda<false><<<kPsBlocks, 256, 0, st>>>(npts, rho_up, rho_dn, vxc_up, vxc_dn, part, cnt, dvol, energies);
+    if (cudaGetLastError() != cudaSuccess) return ps_fail(WVLH_ERR_CUDA);
+    return WVLH_OK;
+}
+
+extern "C" int wvlh_ks_potential_spin(wvlh_ctx *ctx, int free_bc, const int n[3], const double h[3],
+                                      const double *rho_up, const double *rho_dn, const double *vext, double *pot_up,
+                                      double *pot_dn, double *energies)
+{
+    // pot_dn holds the total density for the Hartree solve, pot_up takes V_H:
+    // neither may alias an input or the other
+    if (!ctx || !n || !h || !rho_up || !rho_dn || !pot_up || !pot_dn || pot_up == pot_dn)
+        return ps_fail(WVLH_ERR_ARG);
+    for (const double *q : {rho_up, rho_dn, vext})
+        if (q && (q == pot_up || q == pot_dn)) return ps_fail(WVLH_ERR_ARG);
+    if (free_bc ? !ps_free_args_ok(n, h) : !ps_args_ok(n, h)) return ps_fail(WVLH_ERR_ARG);
+    if (cudaSetDevice(ctx->device) != cudaSuccess) return ps_fail(WVLH_ERR_CUDA);
+    const long long npt = (long long)n[0] * n[1] * n[2];
+    k_spin_total<<<kPsBlocks, 256, 0, ctx->stream>>>(npt, rho_up, rho_dn, pot_dn);
+    if (cudaGetLastError() != cudaSuccess) return ps_fail(WVLH_ERR_CUDA);
+    PsPlan *pl = nullptr;
+    int rc = free_bc ? ps_free_hartree(ctx, n, h, pot_dn, pot_up, nullptr, &pl)
+                     : ps_hartree(ctx, n, h, pot_dn, pot_up, 0.0, &pl);
+    if (rc) return ps_fail(rc);
+    k_ks_combine_spin<<<kPsBlocks, 256, 0, ctx->stream>>>(npt, rho_up, rho_dn, vext, pot_up, pot_dn,
+                                                          (double *)pl->part.p, (unsigned int *)pl->cnt.p,
+                                                          h[0] * h[1] * h[2], energies);
+    if (cudaGetLastError() != cudaSuccess) return ps_fail(WVLH_ERR_CUDA);
+    return WVLH_OK;
 }

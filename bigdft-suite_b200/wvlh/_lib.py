@@ -84,6 +84,8 @@ WVLH_SYMBOLS = [
     "wvlh_psolver_free",
     "wvlh_ks_potential_free",
     "wvlh_psolver_free_tables",
+    "wvlh_xc_lsda",
+    "wvlh_ks_potential_spin",
 ]
 
 
@@ -151,6 +153,9 @@ def lib():
     L.wvlh_psolver_free_tables.argtypes = [C.POINTER(C.c_int), C.POINTER(C.c_double), C.POINTER(C.c_int), vp,
                                            C.c_int64]
     L.wvlh_psolver_free_tables.restype = C.c_int64
+    L.wvlh_xc_lsda.argtypes = [vp, C.c_int64, vp, vp, vp, vp, C.c_int, C.c_double, vp]
+    L.wvlh_ks_potential_spin.argtypes = [vp, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_double), vp, vp, vp, vp,
+                                         vp, vp]
     L.wvlh_host_alloc.restype = vp
     L.wvlh_host_alloc.argtypes = [C.c_size_t]
     L.wvlh_host_free.argtypes = [vp]

@@ -120,3 +120,51 @@ def ks_potential_periodic(ctx, rho, h, vext=None, pot=None, energy=True, free=Fa
 def ks_potential_free(ctx, rho, h, vext=None, pot=None, energy=True):
     """ks_potential_periodic with free boundary conditions."""
     return ks_potential_periodic(ctx, rho, h, vext, pot, energy, free=True)
+
+
+def xc_lsda(ctx, rho_up, rho_dn, vxc_up=None, vxc_dn=None, accumulate=False, dvol=1.0, energy=True):
+    """Spin-polarised LDA (ixc = 1, nspin = 2) of the spin densities (two
+    float64 device tensors of one shape): returns (vxc_up, vxc_dn, energies),
+    energies a (2,) device tensor (exc, evxc) or None without energy."""
+    torch = ctx.torch
+    _check_rho(ctx, rho_up)
+    _check_rho(ctx, rho_dn)
+    if rho_up.shape != rho_dn.shape:
+        raise WvlhError("rho_up and rho_dn must have one shape")
+    if accumulate and (vxc_up is None or vxc_dn is None):
+        raise WvlhError("accumulate needs vxc_up and vxc_dn")
+    vxc_up = torch.empty_like(rho_up) if vxc_up is None else vxc_up
+    vxc_dn = torch.empty_like(rho_dn) if vxc_dn is None else vxc_dn
+    for t in (vxc_up, vxc_dn):
+        if t.shape != rho_up.shape or t.dtype != torch.float64 or not t.is_contiguous():
+            raise WvlhError("vxc: tensors like rho")
+    en = torch.empty(2, dtype=torch.float64, device=rho_up.device) if energy else None
+    check(lib().wvlh_xc_lsda(ctx.h, rho_up.numel(), C.c_void_p(rho_up.data_ptr()), C.c_void_p(rho_dn.data_ptr()),
+                             C.c_void_p(vxc_up.data_ptr()), C.c_void_p(vxc_dn.data_ptr()), 1 if accumulate else 0,
+                             float(dvol), C.c_void_p(en.data_ptr()) if energy else None), "wvlh_xc_lsda")
+    return vxc_up, vxc_dn, en
+
+
+def ks_potential_spin(ctx, rho_up, rho_dn, h, vext=None, free=False, pot_up=None, pot_dn=None, energy=True):
+    """The two Kohn-Sham potentials (nspin = 2) on a periodic grid, or with
+    free boundary conditions when free: returns (pot_up, pot_dn, energies),
+    energies a (3,) device tensor (eh, exc, evxc) or None."""
+    torch = ctx.torch
+    for t in (rho_up, rho_dn):
+        _check_rho(ctx, t)
+    if rho_up.dim() != 3 or rho_dn.shape != rho_up.shape:
+        raise WvlhError("rho_up, rho_dn: (z, y, x) grids of one shape")
+    pot_up = torch.empty_like(rho_up) if pot_up is None else pot_up
+    pot_dn = torch.empty_like(rho_up) if pot_dn is None else pot_dn
+    for name, t in (("pot_up", pot_up), ("pot_dn", pot_dn), ("vext", vext)):
+        if t is not None and (t.shape != rho_up.shape or t.dtype != torch.float64 or not t.is_contiguous()):
+            raise WvlhError("%s: a tensor like rho" % name)
+    n = (C.c_int * 3)(rho_up.shape[2], rho_up.shape[1], rho_up.shape[0])
+    hh = (C.c_double * 3)(*[float(v) for v in h])
+    en = torch.empty(3, dtype=torch.float64, device=rho_up.device) if energy else None
+    check(lib().wvlh_ks_potential_spin(ctx.h, 1 if free else 0, n, hh, C.c_void_p(rho_up.data_ptr()),
+                                       C.c_void_p(rho_dn.data_ptr()),
+                                       C.c_void_p(vext.data_ptr()) if vext is not None else None,
+                                       C.c_void_p(pot_up.data_ptr()), C.c_void_p(pot_dn.data_ptr()),
+                                       C.c_void_p(en.data_ptr()) if energy else None), "wvlh_ks_potential_spin")
+    return pot_up, pot_dn, en

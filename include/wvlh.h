@@ -411,6 +411,22 @@ int wvlh_ks_potential_periodic(wvlh_ctx *ctx, const int n[3], const double h[3],
  * wvlh_psolver_free). */
 int wvlh_ks_potential_free(wvlh_ctx *ctx, const int n[3], const double h[3], const double *rho, const double *vext,
                            double *pot, double *energies);
+/* Spin-polarised LDA (ixc = 1, nspin = 2: xcspol's spin interpolation with the
+ * fit's ferromagnetic differences, abi_xcspol.F90:113-116, 355-395) for npts
+ * points of the spin densities (DEVICE FP64): vxc_up/dn[i] = v_xc,sigma (or
+ * added when accumulate; vxc_up may be rho_up, vxc_dn rho_dn).  energies
+ * (DEVICE double[2], or NULL): exc = dvol sum eps (up + dn), evxc = dvol
+ * sum_sigma v_sigma rho_sigma. */
+int wvlh_xc_lsda(wvlh_ctx *ctx, int64_t npts, const double *rho_up, const double *rho_dn, double *vxc_up,
+                 double *vxc_dn, int accumulate, double dvol, double *energies);
+/* The Kohn-Sham potentials of updatePotential with nspin = 2
+ * (rhopotential.f90:87-120): V_H of the total density (periodic, or free
+ * boundary conditions when free_bc), pot_sigma = (V_H + vext) + V_xc,sigma;
+ * energies as wvlh_ks_potential_periodic (evxc summed over both spins).
+ * pot_up and pot_dn are distinct and alias no input. */
+int wvlh_ks_potential_spin(wvlh_ctx *ctx, int free_bc, const int n[3], const double h[3], const double *rho_up,
+                           const double *rho_dn, const double *vext, double *pot_up, double *pot_dn,
+                           double *energies);
 /* FP64, one kernel per 1D pass (the OpenCL backend's structure) */
 int wvlh_locham_plain_batched(wvlh_batch *batch, const double *psi, const double *pot, double *hpsi,
                               double *ekin, double *epot);

@@ -659,6 +659,60 @@ def xc_lda(rho):
     return eps, eps - rs / 3.0 * deps
 
 
+# ferromagnetic - paramagnetic differences of the fit's parameters (same
+# paper; abi_xcspol.F90:113-116), the spin interpolation's alpha and
+# fact = 1 / (2^(4/3) - 2) (:107, :176)
+TETER_DA = (0.119086804055547, 0.6157402568883345, 0.1574201515892867, 0.003532336663397157)
+TETER_DB = (0.0, 0.2673612973836267, 0.2052004607777787, 0.004200005045691381)
+TETER_ALPHA = 1.0 - 1.0e-6
+
+
+def xc_lsda(rho_up, rho_dn):
+    """(eps_xc, v_up, v_dn) of a spin-polarised density (abi_xcspol
+    nspden = 2, order 1, :355-395): zeta = 2 rho_up / rho - 1 (abi_drivexc
+    :226-233), the parameters interpolated with f(zeta) = ((1 + a z)^(4/3) +
+    (1 - a z)^(4/3) - 2) / (2^(4/3) - 2), v_up/dn = v_para - (zeta -/+ 1)
+    d eps / d zeta."""
+    up = np.asarray(rho_up, np.float64)
+    dn = np.asarray(rho_dn, np.float64)
+    rho = up + dn
+    zet = 2.0 * up / rho - 1.0
+    rs = RS_FAC * np.sign(rho) * np.abs(rho) ** (-1.0 / 3.0)
+    fact = 1.0 / (2.0 ** (4.0 / 3.0) - 2.0)
+    zp, zm = 1.0 + zet * TETER_ALPHA, 1.0 - zet * TETER_ALPHA
+    zp3, zm3 = zp ** (1.0 / 3.0), zm ** (1.0 / 3.0)
+    fxc = (zp * zp3 + zm * zm3 - 2.0) * fact
+    a = [TETER_A[i] + fxc * TETER_DA[i] for i in range(4)]
+    b = [TETER_B[i] + fxc * TETER_DB[i] for i in range(4)]
+    n1 = a[0] + rs * (a[1] + rs * (a[2] + rs * a[3]))
+    d1 = rs * (b[0] + rs * (b[1] + rs * (b[2] + rs * b[3])))
+    eps = -n1 / d1
+    dn1 = a[1] + rs * (2.0 * a[2] + rs * (3.0 * a[3]))
+    dd1 = b[0] + rs * (2.0 * b[1] + rs * (3.0 * b[2] + rs * (4.0 * b[3])))
+    vp = eps - rs / 3.0 * (-(dn1 + eps * dd1) / d1)
+    dfdz = 4.0 / 3.0 * TETER_ALPHA * (zp3 - zm3) * fact
+    dn1df = TETER_DA[0] + rs * (TETER_DA[1] + rs * (TETER_DA[2] + rs * TETER_DA[3]))
+    dd1df = rs * (TETER_DB[0] + rs * (TETER_DB[1] + rs * (TETER_DB[2] + rs * TETER_DB[3])))
+    dedz = dfdz * (-(dn1df + eps * dd1df) / d1)
+    return eps, vp - (zet - 1.0) * dedz, vp - (zet + 1.0) * dedz
+
+
+def ks_potential_spin(rho_up, rho_dn, h, vext=None, free=False):
+    """updatePotential for nspin = 2 (bigdft/src/modules/rhopotential.f90:
+    87-120): V_H of the total density (XC_potential leaves the total in the
+    first half, xc_energy_new :902-908), pot_sigma = (V_H + V_ext) + V_xc,sigma.
+    Returns (pot_up, pot_dn, (eh, exc, evxc)), evxc = dvol sum_sigma v rho."""
+    up = np.asarray(rho_up, np.float64)
+    dn = np.asarray(rho_dn, np.float64)
+    tot = up + dn
+    vh, eh = psolver_free(tot, h) if free else psolver_periodic(tot, h)
+    eps, vu, vd = xc_lsda(up, dn)
+    base = vh if vext is None else vh + np.asarray(vext, np.float64)
+    dvol = h[0] * h[1] * h[2]
+    return (base + vu, base + vd,
+            (eh, float((eps * tot).sum()) * dvol, float((vu * up + vd * dn).sum()) * dvol))
+
+
 def ks_potential_free(rho, h, vext=None):
     """ks_potential_periodic with the free-boundary Hartree potential."""
     return ks_potential_periodic(rho, h, vext, free=True)

@@ -172,3 +172,44 @@ def test_ks_potential_free_matches_oracle(oracle, torch_cuda, wctx):
     assert np.abs(pot.cpu().numpy() - ref).max() <= 1e-13 * np.abs(ref).max()
     for a, b in zip(en.cpu().numpy(), (eh, exc, evxc)):
         assert abs(a - b) <= 1e-12 * abs(b)
+
+
+def test_xc_lsda_matches_oracle_on_reference_test_density(oracle, torch_cuda, wctx):
+    from test_psolver_rule import xc_test_density_spin
+    from wvlh.psolver import xc_lsda
+    torch = torch_cuda
+    up, dn = xc_test_density_spin()
+    eps, vu, vd = oracle.xc_lsda(up, dn)
+    tu, td = torch.tensor(up, device="cuda"), torch.tensor(dn, device="cuda")
+    gu, gd, en = xc_lsda(wctx, tu, td)
+    scale = max(np.abs(vu).max(), np.abs(vd).max())
+    assert np.abs(gu.cpu().numpy() - vu).max() <= 1e-14 * scale
+    assert np.abs(gd.cpu().numpy() - vd).max() <= 1e-14 * scale
+    e = en.cpu().numpy()
+    assert abs(e[0] - (eps * (up + dn)).sum()) <= 1e-13 * abs(e[0])
+    assert abs(e[1] - (vu * up + vd * dn).sum()) <= 1e-13 * abs(e[1])
+    # in place
+    xc_lsda(wctx, tu, td, vxc_up=tu, vxc_dn=td, energy=False)
+    assert torch.equal(tu, gu) and torch.equal(td, gd)
+
+
+@pytest.mark.parametrize("free", [False, True])
+def test_ks_potential_spin_matches_oracle(oracle, torch_cuda, wctx, free):
+    from wvlh.psolver import ks_potential_spin
+    torch = torch_cuda
+    n, h = (32, 28, 36), (0.3, 0.32, 0.28)
+    rng = np.random.default_rng(21 + free)
+    up = rng.uniform(1e-4, 0.4, n[::-1])
+    dn = rng.uniform(1e-4, 0.4, n[::-1])
+    vext = rng.uniform(-1, 1, n[::-1])
+    ru, rd, (eh, exc, evxc) = oracle.ks_potential_spin(up, dn, h, vext, free=free)
+    pu, pd, en = ks_potential_spin(wctx, torch.tensor(up, device="cuda"), torch.tensor(dn, device="cuda"), h,
+                                   vext=torch.tensor(vext, device="cuda"), free=free)
+    scale = max(np.abs(ru).max(), np.abs(rd).max())
+    assert np.abs(pu.cpu().numpy() - ru).max() <= 1e-13 * scale
+    assert np.abs(pd.cpu().numpy() - rd).max() <= 1e-13 * scale
+    for a, b in zip(en.cpu().numpy(), (eh, exc, evxc)):
+        assert abs(a - b) <= 1e-12 * abs(b)
+    t = torch.tensor(up, device="cuda")
+    with pytest.raises(WvlhError):
+        ks_potential_spin(wctx, t, t.clone(), h, pot_up=t)
