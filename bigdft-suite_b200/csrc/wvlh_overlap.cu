@@ -234,7 +234,11 @@ static int overlap_tiles(int norb, bool two)
 int overlap_split(int norb, long long K, int nsm, bool two)
 {
     const int ntile = overlap_tiles(norb, two);
-    int nsplit = (3 * nsm + ntile - 1) / ntile;
+    // three CTAs fit an SM (72 KB of shared memory each in FP64): as many
+    // splits as fill those slots without starting a second, nearly empty wave
+    // (rounding up put 450 CTAs on 444 slots at 256 orbitals: the last six ran
+    // alone and the tensor pipes idled a third of the time)
+    int nsplit = 3 * nsm / ntile;
     const long long maxs = (K + OV_BK - 1) / OV_BK;
     if (nsplit > maxs) nsplit = (int)maxs;
     return nsplit < 1 ? 1 : nsplit;
