@@ -352,12 +352,14 @@ def leg_psolver(torch, ctx, dev, n=96, h=0.225):
     the batched workload (seeded positive density, FP64): the Hartree
     potential, periodic (wvlh_psolver_periodic: cuFFT and the ISF kernel
     multiply) and free (wvlh_psolver_free: the density padded to 192^3, the
-    kernel table built once and kept), the Kohn-Sham potential V_H + V_ext +
+    kernel table built once and kept) and surface (x, z periodic, y free,
+    padded to 192 along y), the Kohn-Sham potential V_H + V_ext +
     V_xc with its three energies (wvlh_ks_potential_periodic / _free) and the
     LDA alone (wvlh_xc_lda, 16 bytes a point), against the oracle's numpy
     restatement on the host."""
     import numpy as np
-    from wvlh.psolver import hartree_free, hartree_periodic, ks_potential_free, ks_potential_periodic, xc_lda
+    from wvlh.psolver import (hartree_free, hartree_periodic, hartree_surface, ks_potential_free,
+                              ks_potential_periodic, xc_lda)
     rng = np.random.default_rng(5)
     rho_h = rng.uniform(1e-3, 1, (n, n, n))
     vext_h = rng.uniform(-1, 1, (n, n, n))
@@ -371,10 +373,16 @@ def leg_psolver(torch, ctx, dev, n=96, h=0.225):
     hartree_free(ctx, rho, hh, pot=pot)      # builds the free kernel and plans once
     free_ms = _timed(torch, lambda: hartree_free(ctx, rho, hh, pot=pot), 10)
     ks_free_ms = _timed(torch, lambda: ks_potential_free(ctx, rho, hh, vext=vext, pot=pot), 10)
+    t = time.perf_counter()
+    hartree_surface(ctx, rho, hh, pot=pot)   # builds the surface kernel table and plans once
+    torch.cuda.synchronize()
+    surf_setup_ms = (time.perf_counter() - t) * 1e3
+    surf_ms = _timed(torch, lambda: hartree_surface(ctx, rho, hh, pot=pot), 10)
     out = {"workload": "%d^3 grid, h %.3f bohr, FP64" % (n, h), "ms": ms,
            "ks_potential_ms": ks_ms, "xc_lda_ms": xc_ms,
            "xc_lda_gbs": 16.0 * n ** 3 / (xc_ms * 1e-3) / 1e9,
-           "free_ms": free_ms, "ks_potential_free_ms": ks_free_ms}
+           "free_ms": free_ms, "ks_potential_free_ms": ks_free_ms,
+           "surface_ms": surf_ms, "surface_setup_ms": surf_setup_ms}
     try:
         from oracle import ks_potential_periodic as ks_cpu
         from oracle import psolver_periodic

@@ -42,6 +42,7 @@
 #include <cmath>
 #include <map>
 #include <mutex>
+#include <thread>
 #include <tuple>
 #include <vector>
 
@@ -551,6 +552,198 @@ __global__ void k_free_crop(int n1, int n2, int n3, int N1, int N2, const double
     finish_partials<1>(v, part, cnt, sc, out, red);
 }
 
+
+// ---------------------------------------------------------------- surface BC kernel
+// (x and z periodic, y free: Surfaces_Kernel, Build_Kernel.f90:279-731)
+
+// closed 9-point Newton-Cotes weights, the order-8 composite rule of
+// calculates_green_opt (intorder 8, cpol(:, 8) times 8)
+static const double kNC9[9] = {989.0 * 4.0 / 14175.0,  5888.0 * 4.0 / 14175.0, -928.0 * 4.0 / 14175.0,
+                               10496.0 * 4.0 / 14175.0, -4540.0 * 4.0 / 14175.0, 10496.0 * 4.0 / 14175.0,
+                               -928.0 * 4.0 / 14175.0,  5888.0 * 4.0 / 14175.0, 989.0 * 4.0 / 14175.0};
+
+// the ISF at spacing 32 / nd on [-15, 17] (the cascade of isf_samples, to nd points)
+static void isf_samples_n(int nd, std::vector<double> &x, std::vector<double> &y)
+{
+    const int ni = 32, mh = 9;
+    y.assign(nd + 1, 0.0);
+    y[ni / 2 - 1] = 1.0;
+    std::vector<double> prev, out;
+    for (int nt = 2 * ni;; nt *= 2) {
+        const int half = nt / 2;
+        prev.assign(y.begin(), y.begin() + half);
+        out.assign(nt, 0.0);
+        for (int i = 0; i < half; ++i) {
+            out[2 * i] = prev[i];
+            double v = 0.0;
+            for (int j = -mh; j < mh; ++j) {
+                const int m = 2 * j + 1;
+                if (m < -15 || m > 15) continue;
+                v += isf_weight(m < 0 ? -m : m) * prev[((i - j) % half + half) % half];
+            }
+            out[2 * i + 1] = v;
+        }
+        std::copy(out.begin(), out.end(), y.begin());
+        if (nt == nd) break;
+    }
+    x.resize(nd + 1);
+    for (int i = 0; i <= nd; ++i) x[i] = (double)i * ni / nd - (0.5 * ni - 1.0);
+}
+
+// n_iter two-scale steps k(i) <- 1/2 sum_j ch(j) k(2i - j) on k(-nr..nr),
+// stopping at the first zero sum (scf_recursion_16)
+static void two_scale_steps(std::vector<double> &k, int nr, int n_iter, std::vector<double> &k1)
+{
+    double ch[37];
+    for (int j = -18; j <= 18; ++j)
+        ch[j + 18] = j == 0 ? 1.0 : ((j & 1) && j >= -15 && j <= 15 ? isf_weight(j < 0 ? -j : j) : 0.0);
+    for (int it = 0; it < n_iter; ++it) {
+        k1 = k;
+        std::fill(k.begin(), k.end(), 0.0);
+        for (int i = 0; i <= nr; ++i) {
+            double tot = 0.0;
+            for (int j = -18; j <= 18; ++j) {
+                const int ind = 2 * i - j;
+                if (ind >= -nr && ind <= nr) tot += ch[j + 18] * k1[nr + ind];
+            }
+            if (tot == 0.0) break;
+            k[nr + i] = k[nr - i] = 0.5 * tot;
+        }
+    }
+}
+
+struct IsfFine {
+    std::vector<double> x, y;
+    int n_scf = 0, izero = 0;
+    double hres = 0.0;
+    IsfFine()
+    {
+        isf_samples_n(2048, x, y);
+        n_scf = 2048;
+        hres = 32.0 / n_scf;
+        while (izero < n_scf && x[izero] < 0.0) ++izero;
+    }
+    // the right-half integral from x = 0 of y g (panels while 9 points and one
+    // more remain, then the leftover points with the first weights)
+    template <class G> double right(G g) const
+    {
+        double s = 0.0;
+        int iv = izero;
+        for (; iv < n_scf - 9; iv += 8)
+            for (int i = 0; i < 9; ++i) s += kNC9[i] * y[iv + i] * g(x[iv + i]);
+        for (int i = 0; iv + i < n_scf; ++i) s += kNC9[i] * y[iv + i] * g(x[iv + i]);
+        return s;
+    }
+    // the integral of y g over the unit segment [j-1, j] (j >= 1), 0 past the samples
+    template <class G> double segment(int j, G g) const
+    {
+        const int s0 = izero + 64 * (j - 1);
+        if (s0 >= n_scf) return 0.0;
+        double s = 0.0;
+        for (int p = 0; p < 8; ++p)
+            for (int i = 0; i < 9; ++i) s += kNC9[i] * y[s0 + 8 * p + i] * g(x[s0 + 8 * p + i]);
+        return s;
+    }
+};
+
+// g(j) = integral of phi(x - j) exp(-mu |x|), j = 0..n-1 (calculates_green_opt,
+// Build_Kernel.f90:734-864)
+static void green_surface(int n, double mu, const IsfFine &f, std::vector<double> &out, std::vector<double> &g,
+                          std::vector<double> &tmp)
+{
+    int n_iter = 0;
+    double mu0 = mu;
+    if (mu > 0.2) {
+        n_iter = 1;
+        while (mu / std::pow(2.0, n_iter) > 0.2) ++n_iter;
+        mu0 = mu / std::pow(2.0, n_iter);
+    }
+    int nrec = (1 << n_iter) * n;
+    g.assign(2 * nrec + 1, 0.0);
+    double gright = f.hres * f.right([mu0](double x) { return std::exp(-mu0 * x); });
+    double gleft = gright;
+    g[nrec] = gleft + gright;
+    const int nseg = (f.n_scf - f.izero) / 64;   // unit segments holding samples
+    const double em = std::exp(-mu0), ep = std::exp(mu0);
+    int nr = nrec;
+    for (int ik = 1; ik <= nrec; ++ik) {
+        const double lt = f.segment(ik, [mu0](double x) { return std::exp(mu0 * x); });
+        const double rt = f.segment(ik, [mu0](double x) { return std::exp(-mu0 * x); });
+        gleft = em * (gleft + f.hres * std::exp(-mu0 * (ik - 1)) * lt);
+        gright = ik < nseg ? ep * (gright - f.hres * std::exp(mu0 * (ik - 1)) * rt) : 0.0;
+        g[nrec + ik] = g[nrec - ik] = gleft + gright;
+        if (std::fabs(gleft + gright) <= 1e-20) {
+            nr = ik;
+            break;
+        }
+    }
+    std::vector<double> k(g.begin() + (nrec - nr), g.begin() + (nrec + nr + 1));
+    two_scale_steps(k, nr, n_iter, tmp);
+    out.assign(n, 0.0);
+    for (int j = 0; j < std::min(n, nr); ++j) out[j] = k[nr + j];
+}
+
+// g(j) = integral of phi(x) |x - j|, j = 0..n-1 (calculates_green_opt_muzero,
+// Build_Kernel.f90:867-953)
+static void green_surface_mu0(int n, const IsfFine &f, std::vector<double> &out)
+{
+    double gr1 = f.hres * f.right([](double x) { return x; });
+    double gl1 = -gr1, gl0 = 0.5, gr0 = 0.5;
+    out.assign(n, 0.0);
+    out[0] = 2.0 * gr1;
+    for (int ik = 1; ik < n; ++ik) {
+        const double c0 = f.hres * f.segment(ik, [](double) { return 1.0; });
+        const double c1 = f.hres * f.segment(ik, [](double x) { return x; });
+        gl0 += c0;
+        gl1 += c1;
+        gr0 -= c0;
+        gr1 -= c1;
+        out[ik] = ik * (gl0 - gr0) + gr1 - gl1;
+    }
+}
+
+// the (n3/2+1, N2/2+1, n1/2+1) table K(k3, ky, k1): for each in-plane
+// frequency mu = 2 pi h_y |g|, the Green's function along y (-h_y/(2 mu) g,
+// or h_y/2 g at mu = 0) on the n2 points, cosine-transformed on N2 (without the
+// reference's centring sign (-1)^k); rows of k3 computed on the host's threads
+static void surface_kernel_table(const int n[3], const double h[3], int N2, std::vector<double> &tab)
+{
+    static const IsfFine f;
+    const int n1 = n[0], n2 = n[1], n3 = n[2];
+    const int nr = std::max(n2, 32), l1 = n1 / 2 + 1, l2 = N2 / 2 + 1, l3 = n3 / 2 + 1, J = std::min(n2, N2 / 2);
+    std::vector<double> cs((size_t)l2 * J);
+    for (int q = 0; q < l2; ++q)
+        for (int j = 0; j < J; ++j)
+            cs[(size_t)q * J + j] = std::cos(6.28318530717958647688 * ((long long)q * j % N2) / N2);
+    tab.assign((size_t)l3 * l2 * l1, 0.0);
+    auto rows = [&](int r0, int r1) {
+        std::vector<double> v, g, tmp;
+        for (int k3 = r0; k3 < r1; ++k3)
+            for (int k1 = 0; k1 < l1; ++k1) {
+                const double g1 = k1 / (n1 * h[0]), g3 = k3 / (n3 * h[2]);
+                const double mu = h[1] * 6.28318530717958647688 * std::sqrt(g1 * g1 + g3 * g3);
+                double sc;
+                if (k1 == 0 && k3 == 0) {
+                    green_surface_mu0(nr, f, v);
+                    sc = 0.5 * h[1];
+                } else {
+                    green_surface(nr, mu, f, v, g, tmp);
+                    sc = -0.5 * h[1] / mu;
+                }
+                for (int q = 0; q < l2; ++q) {
+                    const double *c = cs.data() + (size_t)q * J;
+                    double s = 0.0;
+                    for (int j = 1; j < J; ++j) s += sc * v[j] * c[j];
+                    tab[((size_t)k3 * l2 + q) * l1 + k1] = sc * v[0] + 2.0 * s;
+                }
+            }
+    };
+    const int nt = std::max(1, std::min(l3, (int)std::thread::hardware_concurrency()));
+    std::vector<std::thread> th;
+    for (int t = 0; t < nt; ++t) th.emplace_back(rows, (int)((long long)l3 * t / nt), (int)((long long)l3 * (t + 1) / nt));
+    for (auto &x : th) x.join();
+}
+
 }  // namespace wvlh
 
 using namespace wvlh;
@@ -561,6 +754,8 @@ static std::mutex g_ps_mutex;
 static std::map<std::tuple<const void *, int, int, int, int>, PsPlan *> g_ps_plans;
 // free boundary conditions: per (context, device, grid, spacings)
 static std::map<std::tuple<const void *, int, int, int, int, double, double, double>, PsPlan *> g_ps_free;
+// surface boundary conditions: the same key
+static std::map<std::tuple<const void *, int, int, int, int, double, double, double>, PsPlan *> g_ps_surf;
 
 static void free_plan(PsPlan *pl)
 {
@@ -585,14 +780,15 @@ void psolver_release(const wvlh_ctx *ctx)
         free_plan(it->second);
         it = g_ps_plans.erase(it);
     }
-    for (auto it = g_ps_free.begin(); it != g_ps_free.end();) {
-        if (std::get<0>(it->first) != (const void *)ctx) {
-            ++it;
-            continue;
+    for (auto *m : {&g_ps_free, &g_ps_surf})
+        for (auto it = m->begin(); it != m->end();) {
+            if (std::get<0>(it->first) != (const void *)ctx) {
+                ++it;
+                continue;
+            }
+            free_plan(it->second);
+            it = m->erase(it);
         }
-        free_plan(it->second);
-        it = g_ps_free.erase(it);
-    }
 }
 }  // namespace wvlh
 
@@ -959,4 +1155,98 @@ extern "C" int wvlh_ks_potential_spin(wvlh_ctx *ctx, int free_bc, const int n[3]
                                                           h[0] * h[1] * h[2], energies);
     if (cudaGetLastError() != cudaSuccess) return ps_fail(WVLH_ERR_CUDA);
     return WVLH_OK;
+}
+
+// the surface-BC plan of a grid (x, z periodic, y free): y padded to N2,
+// cuFFT D2Z / Z2D over (n3, N2, n1), the kernel table (n3/2+1, N2/2+1,
+// n1/2+1) built on the host once, the padded input (zero for y >= n2, set once)
+static int ps_surface_plan(wvlh_ctx *ctx, const int n[3], const double h[3], PsPlan **out)
+{
+    std::lock_guard<std::mutex> lock(g_ps_mutex);
+    const auto key = std::make_tuple((const void *)ctx, ctx->device, n[0], n[1], n[2], h[0], h[1], h[2]);
+    auto it = g_ps_surf.find(key);
+    if (it != g_ps_surf.end()) {
+        *out = it->second;
+        return WVLH_OK;
+    }
+    PsPlan *pl = new PsPlan();
+    pl->nf[0] = n[0];
+    pl->nf[1] = fft_length(2 * n[1]);
+    pl->nf[2] = n[2];
+    const int N1 = pl->nf[0], N2 = pl->nf[1], N3 = pl->nf[2];
+    const size_t npad = (size_t)N3 * N2 * N1, nspec = (size_t)N3 * N2 * (N1 / 2 + 1);
+    int rc = WVLH_OK;
+    if (cufftPlan3d(&pl->fwd, N3, N2, N1, CUFFT_D2Z) != CUFFT_SUCCESS ||
+        cufftPlan3d(&pl->inv, N3, N2, N1, CUFFT_Z2D) != CUFFT_SUCCESS)
+        rc = WVLH_ERR_CUDA;
+    std::vector<double> tab;
+    if (!rc) {
+        surface_kernel_table(n, h, N2, tab);
+        if ((rc = pl->ker.ensure(sizeof(double) * tab.size())) || (rc = pl->pad.ensure(sizeof(double) * npad)) ||
+            (rc = pl->work.ensure(sizeof(double) * npad)) ||
+            (rc = pl->spec.ensure(sizeof(cufftDoubleComplex) * nspec)) || (rc = ps_energy_buffers(ctx, pl)))
+            ;
+    }
+    if (!rc) {
+        cudaStream_t st = ctx->stream;
+        const bool ok =
+            cudaMemcpyAsync(pl->ker.p, tab.data(), sizeof(double) * tab.size(), cudaMemcpyHostToDevice, st) ==
+                cudaSuccess &&
+            cudaMemsetAsync(pl->pad.p, 0, sizeof(double) * npad, st) == cudaSuccess &&
+            cudaStreamSynchronize(st) == cudaSuccess;
+        if (!ok) rc = WVLH_ERR_CUDA;
+    }
+    if (rc) {
+        free_plan(pl);
+        return rc;
+    }
+    g_ps_surf.emplace(key, pl);
+    *out = pl;
+    return WVLH_OK;
+}
+
+extern "C" int wvlh_psolver_surface(wvlh_ctx *ctx, const int n[3], const double h[3], const double *rho,
+                                    double *pot, double *eh)
+{
+    // rho is copied into the padded buffer before pot is written: pot may be
+    // rho, unless the energy (which reads rho after) is asked for
+    if (!ctx || !n || !h || !rho || !pot || (eh && pot == rho) || !ps_free_args_ok(n, h))
+        return ps_fail(WVLH_ERR_ARG);
+    if (cudaSetDevice(ctx->device) != cudaSuccess) return ps_fail(WVLH_ERR_CUDA);
+    PsPlan *pl = nullptr;
+    int rc = ps_surface_plan(ctx, n, h, &pl);
+    if (rc) return ps_fail(rc);
+    const int N1 = pl->nf[0], N2 = pl->nf[1], N3 = pl->nf[2];
+    cudaStream_t st = ctx->stream;
+    double *pad = (double *)pl->pad.p, *work = (double *)pl->work.p;
+    cufftDoubleComplex *z = (cufftDoubleComplex *)pl->spec.p;
+    k_free_pad<<<kPsBlocks, 256, 0, st>>>(n[0], n[1], n[2], N1, N2, rho, pad);
+    bool ok = cudaGetLastError() == cudaSuccess && cufftSetStream(pl->fwd, st) == CUFFT_SUCCESS &&
+              cufftSetStream(pl->inv, st) == CUFFT_SUCCESS && cufftExecD2Z(pl->fwd, pad, z) == CUFFT_SUCCESS;
+    if (ok) {
+        // -4 pi h_y / (N1 N2 N3), createKernel.f90:374
+        const double scal = -4.0 * 3.14159265358979323846 * h[1] / ((double)N1 * (double)N2 * (double)N3);
+        k_table_multiply<<<kPsBlocks, 256, 0, st>>>(N1, N2, N3, (const double *)pl->ker.p, scal, 0, 0.0, z);
+        ok = cudaGetLastError() == cudaSuccess && cufftExecZ2D(pl->inv, z, work) == CUFFT_SUCCESS;
+    }
+    if (ok) {
+        k_free_crop<<<kPsBlocks, 256, 0, st>>>(n[0], n[1], n[2], N1, N2, work, rho, pot, (double *)pl->part.p,
+                                               (unsigned int *)pl->cnt.p, 0.5 * h[0] * h[1] * h[2], eh);
+        ok = cudaGetLastError() == cudaSuccess;
+    }
+    if (!ok) return ps_fail(WVLH_ERR_CUDA);
+    return WVLH_OK;
+}
+
+extern "C" int64_t wvlh_psolver_surface_table(const int n[3], const double h[3], int *N2, double *tab, int64_t cap)
+{
+    if (!n || !h || !N2 || !ps_free_args_ok(n, h)) return ps_fail(WVLH_ERR_ARG);
+    *N2 = fft_length(2 * n[1]);
+    const int64_t need = (int64_t)(n[2] / 2 + 1) * (*N2 / 2 + 1) * (n[0] / 2 + 1);
+    if (!tab) return need;
+    if (cap < need) return ps_fail(WVLH_ERR_ARG);
+    std::vector<double> t;
+    surface_kernel_table(n, h, *N2, t);
+    std::copy(t.begin(), t.end(), tab);
+    return need;
 }

@@ -45,6 +45,40 @@ def hartree_free(ctx, rho, h, pot=None, energy=True):
     return pot, eh
 
 
+def surface_kernel_table(n, h):
+    """Host side of the surface-BC kernel (no device work): (N2, K), N2 the
+    padded y length and K the (n3/2+1, N2/2+1, n1/2+1) Fourier table."""
+    import numpy as np
+    nn = (C.c_int * 3)(*[int(v) for v in n])
+    hh = (C.c_double * 3)(*[float(v) for v in h])
+    N2 = C.c_int()
+    need = lib().wvlh_psolver_surface_table(nn, hh, C.byref(N2), None, 0)
+    if need < 0:
+        check(int(need), "wvlh_psolver_surface_table")
+    tab = np.zeros(need)
+    check(min(0, int(lib().wvlh_psolver_surface_table(nn, hh, C.byref(N2), tab.ctypes.data_as(C.c_void_p), need))),
+          "wvlh_psolver_surface_table")
+    return N2.value, tab.reshape(n[2] // 2 + 1, N2.value // 2 + 1, n[0] // 2 + 1)
+
+
+def hartree_surface(ctx, rho, h, pot=None, energy=True):
+    """The Hartree potential with surface boundary conditions (x, z periodic,
+    y free; wvlh_psolver_surface); arguments and results as hartree_periodic."""
+    torch = ctx.torch
+    if rho.dtype != torch.float64 or rho.dim() != 3 or not rho.is_contiguous():
+        raise WvlhError("rho: contiguous 3D float64 device tensor (z, y, x)")
+    if pot is None:
+        pot = torch.empty_like(rho)
+    if pot.shape != rho.shape or pot.dtype != torch.float64 or not pot.is_contiguous():
+        raise WvlhError("pot: a tensor like rho")
+    n = (C.c_int * 3)(rho.shape[2], rho.shape[1], rho.shape[0])
+    hh = (C.c_double * 3)(*[float(v) for v in h])
+    eh = torch.empty((), dtype=torch.float64, device=rho.device) if energy else None
+    check(lib().wvlh_psolver_surface(ctx.h, n, hh, C.c_void_p(rho.data_ptr()), C.c_void_p(pot.data_ptr()),
+                                     C.c_void_p(eh.data_ptr()) if energy else None), "wvlh_psolver_surface")
+    return pot, eh
+
+
 def hartree_periodic(ctx, rho, h, offset=0.0, pot=None, energy=True):
     """rho: (n3, n2, n1) float64 device tensor (x fastest), h: (hx, hy, hz).
     Returns (pot, eh): the potential (a new tensor unless pot is given; pot

@@ -387,6 +387,21 @@ int wvlh_psolver_free(wvlh_ctx *ctx, const int n[3], const double h[3], const do
  * With tab NULL returns the number of doubles; otherwise fills tab (cap
  * doubles) and returns that number, or a negative error. */
 int64_t wvlh_psolver_free_tables(const int n[3], const double h[3], int nf[3], double *tab, int64_t cap);
+/* Hartree potential with surface boundary conditions (x and z periodic, y
+ * free: the reference's PSolver for geocode 'S', Surfaces_Kernel,
+ * psolver/src/Build_Kernel.f90:279-864; scal -4 pi h_y / N, createKernel.f90:
+ * 374): for each in-plane frequency the 1D Green's function along y of the
+ * order-16 ISF (exp(-mu |y|) / mu, |y| at zero frequency), rho zero-padded
+ * along y to at least twice n2.  Arguments and results as wvlh_psolver_free;
+ * the kernel table (built once per grid on the host's threads), FFT plans and
+ * padded buffers are kept by the context. */
+int wvlh_psolver_surface(wvlh_ctx *ctx, const int n[3], const double h[3], const double *rho, double *pot,
+                         double *eh);
+/* Host only (no device work): the padded y length N2 and the surface kernel
+ * table K(k3, ky, k1), (n3/2+1, N2/2+1, n1/2+1) doubles, that
+ * wvlh_psolver_surface multiplies by.  With tab NULL returns the number of
+ * doubles; otherwise fills tab (cap doubles) and returns that number. */
+int64_t wvlh_psolver_surface_table(const int n[3], const double h[3], int *N2, double *tab, int64_t cap);
 /* Exchange-correlation potential of the reference's default functional
  * (ixc = 1: the Goedecker-Teter-Hutter Pade LDA, ABINIT's xcspol,
  * libABINIT/src/abi_xc_lowlevel/abi_xcspol.F90:105-250), spin-unpolarised,

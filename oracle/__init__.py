@@ -608,6 +608,196 @@ def free_kernel(n0, h, nfft):
     return K
 
 
+# closed 9-point Newton-Cotes weights (the composite rule of order 8 that
+# calculates_green_opt integrates with: intorder 8, cpol(:, 8) times 8,
+# psolver/src/Build_Kernel.f90:279-360, :734-864)
+NC9 = np.array([989.0, 5888.0, -928.0, 10496.0, -4540.0, 10496.0, -928.0, 5888.0, 989.0]) * 4.0 / 14175.0
+
+
+def _isf_fine():
+    """The order-16 ISF sampled at 1/64 on [-15, 17] (scaling_function with
+    2 * 16 * 64 intervals, as Surfaces_Kernel samples it)."""
+    global _ISF_FINE
+    try:
+        return _ISF_FINE
+    except NameError:
+        _ISF_FINE = isf_samples(16, 64)
+        return _ISF_FINE
+
+
+def _two_scale_recursion(k, nr, n_iter, itype=16):
+    """n_iter steps of k(i) <- 1/2 sum_j ch(j) k(2i - j) on k(-nr..nr) (index
+    i + nr), stopping at the first zero sum (scf_recursion_16,
+    scaling_function.f90:1324-1356)."""
+    w = isf_weights()
+    ch = {0: 1.0}
+    for mm, v in w.items():
+        ch[mm] = ch[-mm] = v
+    i = np.arange(nr + 1)
+    for _ in range(n_iter):
+        k1 = k.copy()
+        tot = np.zeros(nr + 1)
+        for j in range(-(itype + 2), itype + 3):
+            if j not in ch:
+                continue
+            ind = 2 * i - j
+            ok = (ind >= -nr) & (ind <= nr)
+            tot[ok] += ch[j] * k1[nr + ind[ok]]
+        zero = np.nonzero(tot == 0.0)[0]
+        if len(zero):
+            tot[zero[0]:] = 0.0
+        k[:] = 0.0
+        k[nr:] = 0.5 * tot
+        k[:nr + 1] = (0.5 * tot)[::-1]
+    return k
+
+
+def _segment_sums(xs, ys, izero, g, n_scf):
+    """The composite Newton-Cotes integral of g(x) y(x) over each unit segment
+    [j-1, j] from x = 0 (loop_integration of calculates_green_opt): returns a
+    list, one sum per segment until the samples end."""
+    out = []
+    s = izero
+    while s < n_scf:
+        tot = 0.0
+        for p in range(8):                       # 8 panels of 8 intervals at spacing 1/64
+            idx = s + 8 * p + np.arange(9)
+            tot += float(np.dot(NC9, ys[idx] * g(xs[idx])))
+        out.append(tot)
+        s += 64
+    return out
+
+
+def green_surface(n, mu, itype=16):
+    """g(j), j = 0..n-1: the integral of phi(x - j) exp(-mu |x|) (mu > 0), as
+    calculates_green_opt computes it (Build_Kernel.f90:734-864): mu divided by
+    2^n_iter until it is <= 0.2, the integrals from each side accumulated
+    segment by segment with exp(-+mu0) factors, then n_iter two-scale steps."""
+    xs, ys = _isf_fine()
+    n_scf = len(xs) - 1
+    hres = 32.0 / n_scf
+    n_iter, mu0 = 0, mu
+    if mu > 0.2:
+        n_iter = 1
+        while mu / 2.0 ** n_iter > 0.2:
+            n_iter += 1
+        mu0 = mu / 2.0 ** n_iter
+    nrec = 2 ** n_iter * n
+    izero = int(np.argmax(xs >= 0.0))
+    green = np.zeros(2 * nrec + 1)
+    # the right half from x = 0: panels while 9 points and one more remain, then
+    # the leftover points with the first weights (the tail is outside the support)
+    gr, iv = 0.0, izero
+    while iv < n_scf - 9:
+        idx = iv + np.arange(9)
+        gr += float(np.dot(NC9, ys[idx] * np.exp(-mu0 * xs[idx])))
+        iv += 8
+    idx = iv + np.arange(n_scf - iv)
+    gr += float(np.dot(NC9[:len(idx)], ys[idx] * np.exp(-mu0 * xs[idx])))
+    gright = hres * gr
+    gleft = gright
+    green[nrec] = gleft + gright
+    sl = _segment_sums(xs, ys, izero, lambda x: np.exp(mu0 * x), n_scf)
+    sr = _segment_sums(xs, ys, izero, lambda x: np.exp(-mu0 * x), n_scf)
+    em, ep = np.exp(-mu0), np.exp(mu0)
+    for ik in range(1, nrec + 1):
+        lt = sl[ik - 1] if ik - 1 < len(sl) else 0.0
+        rt = sr[ik - 1] if ik - 1 < len(sr) else 0.0
+        gleft = em * (gleft + hres * np.exp(-mu0 * (ik - 1)) * lt)
+        gright = ep * (gright - hres * np.exp(mu0 * (ik - 1)) * rt) if ik < len(sl) else 0.0
+        green[nrec + ik] = green[nrec - ik] = gleft + gright
+        if abs(gleft + gright) <= 1e-20:
+            nrec_eff = ik
+            break
+    else:
+        nrec_eff = nrec
+    # the recursion runs on green(-nrec_eff..nrec_eff)
+    k = green[nrec - nrec_eff:nrec + nrec_eff + 1].copy()
+    k = _two_scale_recursion(k, nrec_eff, n_iter)
+    out = np.zeros(n)
+    m = min(n, nrec_eff)
+    out[:m] = k[nrec_eff:nrec_eff + m]
+    return out
+
+
+def green_surface_mu0(n):
+    """g(j), j = 0..n-1: the integral of phi(x) |x - j| (the k = 0 term),
+    as calculates_green_opt_muzero (Build_Kernel.f90:867-953)."""
+    xs, ys = _isf_fine()
+    n_scf = len(xs) - 1
+    hres = 32.0 / n_scf
+    izero = int(np.argmax(xs >= 0.0))
+    gr, iv = 0.0, izero
+    while iv < n_scf - 9:
+        idx = iv + np.arange(9)
+        gr += float(np.dot(NC9, xs[idx] * ys[idx]))
+        iv += 8
+    idx = iv + np.arange(n_scf - iv)
+    gr += float(np.dot(NC9[:len(idx)], xs[idx] * ys[idx]))
+    gr1 = hres * gr
+    gl1, gl0, gr0 = -gr1, 0.5, 0.5
+    out = np.zeros(n)
+    out[0] = 2.0 * gr1
+    s0 = _segment_sums(xs, ys, izero, lambda x: np.ones_like(x), n_scf)
+    s1 = _segment_sums(xs, ys, izero, lambda x: x, n_scf)
+    for ik in range(1, n):
+        c0 = hres * (s0[ik - 1] if ik - 1 < len(s0) else 0.0)
+        c1 = hres * (s1[ik - 1] if ik - 1 < len(s1) else 0.0)
+        gl0 += c0
+        gl1 += c1
+        gr0 -= c0
+        gr1 -= c1
+        out[ik] = ik * (gl0 - gr0) + gr1 - gl1
+    return out
+
+
+def surface_kernel(n0, h, N2):
+    """The surface-BC kernel in Fourier space (x and z periodic, y free;
+    Surfaces_Kernel, Build_Kernel.f90:279-731): for each in-plane frequency
+    (k1, k3), mu = 2 pi h_y |g| and the 1D Green's function along y (-h_y /
+    (2 mu) green_surface, or h_y / 2 green_surface_mu0 at mu = 0) on the
+    box's n2 points, cosine-transformed on the padded length N2 (without the
+    reference's centring sign (-1)^k).  n0 = (n1, n2, n3); returns K of shape
+    (n3/2+1, N2/2+1, n1/2+1)."""
+    n1, n2, n3 = n0
+    nr = max(n2, 32)
+    l1, l2, l3 = n1 // 2 + 1, N2 // 2 + 1, n3 // 2 + 1
+    J = min(n2, N2 // 2)
+    kk = np.arange(l2)[:, None]
+    jj = np.arange(1, J)[None, :]
+    cs = np.cos(2.0 * np.pi * ((kk * jj) % N2) / N2)
+    K = np.zeros((l3, l2, l1))
+    for k3 in range(l3):
+        for k1 in range(l1):
+            g1, g3 = k1 / (n1 * h[0]), k3 / (n3 * h[2])
+            mu = h[1] * 2.0 * np.pi * np.sqrt(g1 * g1 + g3 * g3)
+            if k1 == 0 and k3 == 0:
+                v = 0.5 * h[1] * green_surface_mu0(nr)[:n2]
+            else:
+                v = -0.5 * h[1] / mu * green_surface(nr, mu)[:n2]
+            K[k3, :, k1] = v[0] + 2.0 * (cs @ v[1:J])
+    return K
+
+
+def psolver_surface(rho, h, N2=None):
+    """Hartree potential and energy of rho (n3, n2, n1; x fastest) with
+    surface boundary conditions (x, z periodic; y free): rho zero-padded
+    along y to N2 (default 2 n2), multiplied in Fourier space by
+    surface_kernel, scaled by -4 pi h_y / (n1 N2 n3) (createKernel.f90:374),
+    the first n2 planes of y kept; energy 0.5 sum(rho V) h^3."""
+    rho = np.asarray(rho, np.float64)
+    n3, n2, n1 = rho.shape
+    N2 = 2 * n2 if N2 is None else N2
+    K = surface_kernel((n1, n2, n3), h, N2)
+    pad = np.zeros((n3, N2, n1))
+    pad[:, :n2, :] = rho
+    p2 = np.minimum(np.arange(N2), N2 - np.arange(N2))
+    p3 = np.minimum(np.arange(n3), n3 - np.arange(n3))
+    Kf = K[p3][:, p2]
+    V = np.fft.irfftn(np.fft.rfftn(pad) * Kf, s=pad.shape, axes=(0, 1, 2))[:, :n2, :] * (-4.0 * np.pi * h[1])
+    return V, 0.5 * float((rho * V).sum()) * h[0] * h[1] * h[2]
+
+
 def psolver_free(rho, h, nfft=None):
     """Hartree potential and energy of rho (n3, n2, n1; x fastest) with free
     boundary conditions: rho zero-padded to nfft (default twice each

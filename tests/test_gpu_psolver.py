@@ -213,3 +213,38 @@ def test_ks_potential_spin_matches_oracle(oracle, torch_cuda, wctx, free):
     t = torch.tensor(up, device="cuda")
     with pytest.raises(WvlhError):
         ks_potential_spin(wctx, t, t.clone(), h, pot_up=t)
+
+
+def test_reference_ps_check_surface_golden(torch_cuda, wctx):
+    """The reference's PS_Check surface-BC run (32 x 64 x 48): the Hartree
+    energy to its 13 printed digits, the potential at the printed point, the
+    same deviation from the analytic potential."""
+    from test_psolver_rule import PS_SURF_AT, PS_SURF_EH, PS_SURF_INF, PS_SURF_V, ps_check_surface
+    from wvlh.psolver import hartree_surface
+    torch = torch_cuda
+    rho, V, h = ps_check_surface()
+    pot, eh = hartree_surface(wctx, torch.tensor(rho, device="cuda"), h)
+    got = pot.cpu().numpy()
+    i1, i2, i3 = (v - 1 for v in PS_SURF_AT)
+    assert abs(eh.item() - PS_SURF_EH) <= 5e-13 * PS_SURF_EH
+    assert abs(got[i3, i2, i1] - PS_SURF_V) <= 1e-14
+    assert abs(np.abs(got - V).max() - PS_SURF_INF) <= 1e-4 * PS_SURF_INF
+
+
+@pytest.mark.parametrize("n,h", [((12, 10, 8), (0.3, 0.25, 0.35)), ((32, 24, 40), (0.3, 0.35, 0.28))])
+def test_surface_matches_oracle(oracle, torch_cuda, wctx, n, h):
+    from wvlh.psolver import hartree_surface
+    torch = torch_cuda
+    rng = np.random.default_rng(sum(n) + 1)
+    rho = rng.uniform(-1, 1, n[::-1])
+    ref, eref = oracle.psolver_surface(rho, h)
+    t = torch.tensor(rho, device="cuda")
+    pot, eh = hartree_surface(wctx, t, h)
+    assert np.abs(pot.cpu().numpy() - ref).max() <= 1e-13 * np.abs(ref).max()
+    assert abs(eh.item() - eref) <= 1e-12 * abs(eref)
+    pot2, eh2 = hartree_surface(wctx, t, h)
+    assert torch.equal(pot, pot2) and torch.equal(eh, eh2)
+    with pytest.raises(WvlhError):
+        hartree_surface(wctx, t, h, pot=t, energy=True)
+    hartree_surface(wctx, t, h, pot=t, energy=False)
+    assert torch.equal(t, pot)

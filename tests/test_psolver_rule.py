@@ -306,3 +306,88 @@ def test_ks_potential_spin_is_the_sum_of_its_parts(oracle):
     assert np.array_equal(pu, (vh + vext) + vu) and np.array_equal(pd, (vh + vext) + vd) and eh == eh0
     dv = np.prod(h)
     assert abs(evxc - (vu * up + vd * dn).sum() * dv) <= 1e-12 * abs(evxc)
+
+
+def ps_check_surface():
+    """The surface-BC case of the reference's PS_Check test (x and z
+    periodic, y free; test_functions_new case 'S', functions.f90:541-546,
+    f_functions.f90:395-486): a 32 x 64 x 48 box of side 10 bohr per
+    dimension, x = (i - 1) h - L/2, f = exp(cos(2 pi x / L)) along x and z, the
+    shrunk Gaussian exp(-tan(pi y / L)^2) exp(-50 y^2 / L^2) along y,
+    V = -f(x) f(y) f(z) and rho = lap(f f f) / (4 pi).  Arrays (z, y, x)."""
+    n = (32, 64, 48)
+    h = tuple(10.0 / m for m in n)
+    ax = [np.arange(n[d]) * h[d] - 0.5 * n[d] * h[d] for d in range(3)]
+
+    def expcos(x, L):
+        r = 2 * np.pi * x / L
+        f = np.exp(np.cos(r))
+        return f, (2 * np.pi / L) ** 2 * (np.sin(r) ** 2 - np.cos(r)) * f
+
+    def shrunk(x, L):
+        r = np.pi * x / L
+        y = np.tan(r)
+        g = np.exp(-y ** 2)
+        g1 = -2 * np.pi * g * y / (L * np.cos(r) ** 2)
+        g2 = 2 * np.pi ** 2 * (2 * y ** 6 + y ** 4 - 2 * y ** 2 - 1) / L ** 2 * g
+        a = 50.0 / L ** 2
+        e = np.exp(-a * x * x)
+        return g * e, g2 * e + g * (-2 * a + 4 * a * a * x * x) * e + 2 * g1 * (-2 * a * x * e)
+    fx, fx2 = expcos(ax[0], 10.0)
+    fy, fy2 = shrunk(ax[1], 10.0)
+    fz, fz2 = expcos(ax[2], 10.0)
+
+    def prod(a, b, c):
+        return a[None, None, :] * b[None, :, None] * c[:, None, None]
+    rho = (prod(fx2, fy, fz) + prod(fx, fy2, fz) + prod(fx, fy, fz2)) / (4 * np.pi)
+    return rho, -prod(fx, fy, fz), h
+
+
+# psolver/tests/PS_Check.ref.yaml:398-406 (surface BC, 32 x 64 x 48): the
+# Hartree energy, the largest deviation from the analytic potential, where it
+# lies (1-based x, y, z) and the potential there
+PS_SURF_EH = 2.969431884210e01
+PS_SURF_INF = 5.449589889578e-10
+PS_SURF_AT = (17, 58, 25)
+PS_SURF_V = -1.455736584652e-06
+
+
+def test_reference_ps_check_surface_golden(oracle):
+    rho, V, h = ps_check_surface()
+    pot, eh = oracle.psolver_surface(rho, h)
+    assert abs(eh - PS_SURF_EH) <= 5e-13 * PS_SURF_EH                    # all 13 printed digits
+    i1, i2, i3 = (v - 1 for v in PS_SURF_AT)
+    assert abs(pot[i3, i2, i1] - PS_SURF_V) <= 1e-14                      # the potential is O(1)
+    d = np.abs(pot - V)
+    assert abs(d.max() - PS_SURF_INF) <= 1e-4 * PS_SURF_INF
+    # the deviation peaks at the reference's point or its mirror in y (the test is symmetric in y)
+    j3, j2, j1 = np.unravel_index(d.argmax(), d.shape)
+    assert (j3, j1) == (i3, i1) and j2 in (i2, rho.shape[1] - i2)
+
+
+def test_surface_green_functions(oracle):
+    """The 1D Green's functions tend to their continuum forms away from the
+    ISF support: exp(-mu j) * (integral of phi e^(mu x)) and |j|."""
+    g = oracle.green_surface(40, 0.3)
+    assert np.all(np.diff(g[20:]) < 0) and abs(g[30] / g[29] - np.exp(-0.3)) < 1e-12
+    g0 = oracle.green_surface_mu0(40)
+    assert np.abs(np.diff(g0[20:]) - 1.0).max() < 1e-12        # slope 1 outside the support
+
+
+def test_surface_solution_independent_of_padding(oracle):
+    rng = np.random.default_rng(9)
+    rho = rng.uniform(0, 1, (8, 10, 12))
+    h = (0.3, 0.25, 0.35)
+    a, ea = oracle.psolver_surface(rho, h)
+    b, eb = oracle.psolver_surface(rho, h, N2=26)
+    assert np.abs(a - b).max() <= 1e-13 * np.abs(a).max() and abs(ea - eb) <= 1e-13 * abs(ea)
+
+
+def test_surface_kernel_host_table_matches_oracle(oracle):
+    from wvlh.psolver import surface_kernel_table
+    n = (10, 12, 8)
+    h = (0.3, 0.35, 0.4)
+    N2, K = surface_kernel_table(n, h)
+    assert N2 >= 2 * n[1] and N2 % 2 == 0
+    ref = oracle.surface_kernel(n, h, N2)
+    assert np.abs(K - ref).max() <= 1e-13 * np.abs(ref).max()
