@@ -353,12 +353,13 @@ def leg_psolver(torch, ctx, dev, n=96, h=0.225):
     potential, periodic (wvlh_psolver_periodic: cuFFT and the ISF kernel
     multiply) and free (wvlh_psolver_free: the density padded to 192^3, the
     kernel table built once and kept) and surface (x, z periodic, y free,
-    padded to 192 along y), the Kohn-Sham potential V_H + V_ext +
+    padded to 192 along y) and wire (z periodic, x and y padded to 192), the
+    Kohn-Sham potential V_H + V_ext +
     V_xc with its three energies (wvlh_ks_potential_periodic / _free) and the
     LDA alone (wvlh_xc_lda, 16 bytes a point), against the oracle's numpy
     restatement on the host."""
     import numpy as np
-    from wvlh.psolver import (hartree_free, hartree_periodic, hartree_surface, ks_potential_free,
+    from wvlh.psolver import (hartree_free, hartree_periodic, hartree_surface, hartree_wire, ks_potential_free,
                               ks_potential_periodic, xc_lda)
     rng = np.random.default_rng(5)
     rho_h = rng.uniform(1e-3, 1, (n, n, n))
@@ -378,11 +379,17 @@ def leg_psolver(torch, ctx, dev, n=96, h=0.225):
     torch.cuda.synchronize()
     surf_setup_ms = (time.perf_counter() - t) * 1e3
     surf_ms = _timed(torch, lambda: hartree_surface(ctx, rho, hh, pot=pot), 10)
+    t = time.perf_counter()
+    hartree_wire(ctx, rho, hh, pot=pot)      # builds the wire kernel table and plans once
+    torch.cuda.synchronize()
+    wire_setup_ms = (time.perf_counter() - t) * 1e3
+    wire_ms = _timed(torch, lambda: hartree_wire(ctx, rho, hh, pot=pot), 10)
     out = {"workload": "%d^3 grid, h %.3f bohr, FP64" % (n, h), "ms": ms,
            "ks_potential_ms": ks_ms, "xc_lda_ms": xc_ms,
            "xc_lda_gbs": 16.0 * n ** 3 / (xc_ms * 1e-3) / 1e9,
            "free_ms": free_ms, "ks_potential_free_ms": ks_free_ms,
-           "surface_ms": surf_ms, "surface_setup_ms": surf_setup_ms}
+           "surface_ms": surf_ms, "surface_setup_ms": surf_setup_ms,
+           "wire_ms": wire_ms, "wire_setup_ms": wire_setup_ms}
     try:
         from oracle import ks_potential_periodic as ks_cpu
         from oracle import psolver_periodic

@@ -18,6 +18,9 @@ the reference sources instead of being retyped:
 * the 89-term Gaussian expansion of 1/r that the free-boundary Poisson kernel
   is built from (exponents ``p`` and weights ``w``, range [1e-9, 1]):
   ``psolver/src/Build_Kernel.f90:1679-1873`` (``gequad``).
+* the Gaussian fits of the wire-BC kernel (log r at zero frequency: ``p1``,
+  ``w1``; K0(r) otherwise: ``p2``, ``w2``; the first 144 of 150 are used):
+  ``psolver/src/gaussfit_wires.inc``.
 
 Run ``python gen_filters.py /root/reference`` to rewrite the header; the
 generated header is committed so that the build never needs the reference.
@@ -90,7 +93,16 @@ def parse(ref_root):
     gq_line = next(i for i, l in enumerate(bk.splitlines(), 1) if re.match(r"\s*subroutine gequad\(", l))
     gq_p = _indexed(bk, "p", 1, 89, gq_line)
     gq_w = _indexed(bk, "w", 1, 89, gq_line)
-    return dict(ch=ch, cg=cg, mf=mf, kin=kin, cwav=cwav, ewav=ewav, a2=a2, b2=b2, gq_p=gq_p, gq_w=gq_w)
+    gw = (Path(ref_root) / "psolver" / "src" / "gaussfit_wires.inc").read_text()
+    wires = {}
+    for name in ("p1", "w1", "p2", "w2"):
+        body = re.search(r"^\s*" + name + r"\s*=\s*\(/(.*?)/\)", gw, re.S | re.M).group(1)
+        vals = [v.replace("d", "e").replace("D", "e") for v in
+                re.findall(NUM, re.sub(r"_dp", "", body.replace("&", " ")))]
+        assert len(vals) == 150, (name, len(vals))
+        wires[name] = vals
+    return dict(ch=ch, cg=cg, mf=mf, kin=kin, cwav=cwav, ewav=ewav, a2=a2, b2=b2, gq_p=gq_p, gq_w=gq_w,
+                wires=wires)
 
 
 def render(f):
@@ -121,6 +133,12 @@ def render(f):
         arr("WVL_GQ_P", f["gq_p"], "1/r = sum w(i) exp(-p(i) r^2), r in [1e-9, 1]: exponents p(1..89), "
             "psolver/src/Build_Kernel.f90:1689-1777 (gequad)", at=False),
         arr("WVL_GQ_W", f["gq_w"], "weights w(1..89): Build_Kernel.f90:1779-1867", at=False),
+        arr("WVL_WIRE_P1", f["wires"]["p1"], "log r = sum w1 exp(-p1 r^2) (wire BC, zero frequency): exponents, "
+            "psolver/src/gaussfit_wires.inc (p1)", at=False),
+        arr("WVL_WIRE_W1", f["wires"]["w1"], "weights w1: gaussfit_wires.inc", at=False),
+        arr("WVL_WIRE_P2", f["wires"]["p2"], "K0(r) = sum w2 exp(-p2 r^2) (wire BC): exponents, gaussfit_wires.inc",
+            at=False),
+        arr("WVL_WIRE_W2", f["wires"]["w2"], "weights w2: gaussfit_wires.inc", at=False),
         "",
     ]
     return "\n".join(parts)

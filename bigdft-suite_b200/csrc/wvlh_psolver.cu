@@ -744,6 +744,76 @@ static void surface_kernel_table(const int n[3], const double h[3], int N2, std:
     for (auto &x : th) x.join();
 }
 
+
+// ---------------------------------------------------------------- wire BC kernel
+// (z periodic, x and y free: Wires_Kernel, Build_Kernel.f90:2244-2364)
+
+// K(kz, ky, kx), (n_z/2+1, Ny/2+1, Nx/2+1): per z frequency the plane's Green's
+// function as 144 separable Gaussians (log(mu0 r) at k_z = 0 with -log(mu0)
+// added at k = 0, -K0(mu r) otherwise), each through the ISF overlaps and
+// cosine transforms of the free kernel on the padded lengths; summed in the
+// reference's order (Gaussian 1 to 144, (w C_x) C_y); k_z rows on the host's threads
+static void wire_kernel_table(const int n[3], const double h[3], int Nx, int Ny, std::vector<double> &tab)
+{
+    const int nx = n[0], ny = n[1], nz = n[2];
+    const int nr = std::max(std::max(nx, ny), 32);
+    const int lx = Nx / 2 + 1, ly = Ny / 2 + 1, lz = nz / 2 + 1;
+    const int Jx = std::min(nr, Nx / 2), Jy = std::min(nr, Ny / 2);
+    std::vector<double> xs, ys;
+    isf_samples(xs, ys);
+    std::vector<double> csx((size_t)lx * Jx), csy((size_t)ly * Jy);
+    for (int q = 0; q < lx; ++q)
+        for (int j = 0; j < Jx; ++j) csx[(size_t)q * Jx + j] = std::cos(6.28318530717958647688 * ((long long)q * j % Nx) / Nx);
+    for (int q = 0; q < ly; ++q)
+        for (int j = 0; j < Jy; ++j) csy[(size_t)q * Jy + j] = std::cos(6.28318530717958647688 * ((long long)q * j % Ny) / Ny);
+    tab.assign((size_t)lz * ly * lx, 0.0);
+    auto rows = [&](int r0, int r1) {
+        std::vector<double> k, k1, cx(lx), cy(ly);
+        for (int kz = r0; kz < r1; ++kz) {
+            double mu;
+            const double *alpha, *wt;
+            double wsign;
+            if (kz == 0) {
+                mu = 1.0 / std::sqrt((h[0] * (nx + 32)) * (h[0] * (nx + 32)) + (h[1] * (ny + 32)) * (h[1] * (ny + 32)));
+                alpha = WVL_WIRE_P1;
+                wt = WVL_WIRE_W1;
+                wsign = 1.0;
+            } else {
+                mu = 6.28318530717958647688 / nz * kz / h[2];
+                alpha = WVL_WIRE_P2;
+                wt = WVL_WIRE_W2;
+                wsign = -1.0;   // -K0
+            }
+            double *out = tab.data() + (size_t)kz * ly * lx;
+            for (int g = 0; g < 144; ++g) {
+                const double p = alpha[g] * mu * mu;
+                gauss_conv_isf(p, h[0], nr, xs, ys, k, k1);
+                for (int q = 0; q < lx; ++q) {
+                    const double *c = csx.data() + (size_t)q * Jx;
+                    double s = 0.0;
+                    for (int j = 1; j < Jx; ++j) s += k[nr + j] * c[j];
+                    cx[q] = k[nr] + 2.0 * s;
+                }
+                gauss_conv_isf(p, h[1], nr, xs, ys, k, k1);
+                for (int q = 0; q < ly; ++q) {
+                    const double *c = csy.data() + (size_t)q * Jy;
+                    double s = 0.0;
+                    for (int j = 1; j < Jy; ++j) s += k[nr + j] * c[j];
+                    cy[q] = k[nr] + 2.0 * s;
+                }
+                const double w = wsign * wt[g];
+                for (int qy = 0; qy < ly; ++qy)
+                    for (int qx = 0; qx < lx; ++qx) out[(size_t)qy * lx + qx] += (w * cx[qx]) * cy[qy];
+            }
+            if (kz == 0) out[0] -= (double)Nx * (double)Ny * std::log(mu);
+        }
+    };
+    const int nt = std::max(1, std::min(lz, (int)std::thread::hardware_concurrency()));
+    std::vector<std::thread> th;
+    for (int t = 0; t < nt; ++t) th.emplace_back(rows, (int)((long long)lz * t / nt), (int)((long long)lz * (t + 1) / nt));
+    for (auto &x : th) x.join();
+}
+
 }  // namespace wvlh
 
 using namespace wvlh;
@@ -754,8 +824,9 @@ static std::mutex g_ps_mutex;
 static std::map<std::tuple<const void *, int, int, int, int>, PsPlan *> g_ps_plans;
 // free boundary conditions: per (context, device, grid, spacings)
 static std::map<std::tuple<const void *, int, int, int, int, double, double, double>, PsPlan *> g_ps_free;
-// surface boundary conditions: the same key
+// surface and wire boundary conditions: the same key
 static std::map<std::tuple<const void *, int, int, int, int, double, double, double>, PsPlan *> g_ps_surf;
+static std::map<std::tuple<const void *, int, int, int, int, double, double, double>, PsPlan *> g_ps_wire;
 
 static void free_plan(PsPlan *pl)
 {
@@ -780,7 +851,7 @@ void psolver_release(const wvlh_ctx *ctx)
         free_plan(it->second);
         it = g_ps_plans.erase(it);
     }
-    for (auto *m : {&g_ps_free, &g_ps_surf})
+    for (auto *m : {&g_ps_free, &g_ps_surf, &g_ps_wire})
         for (auto it = m->begin(); it != m->end();) {
             if (std::get<0>(it->first) != (const void *)ctx) {
                 ++it;
@@ -1247,6 +1318,99 @@ extern "C" int64_t wvlh_psolver_surface_table(const int n[3], const double h[3],
     if (cap < need) return ps_fail(WVLH_ERR_ARG);
     std::vector<double> t;
     surface_kernel_table(n, h, *N2, t);
+    std::copy(t.begin(), t.end(), tab);
+    return need;
+}
+
+// the wire-BC plan of a grid (z periodic, x and y free): x and y padded,
+// cuFFT D2Z / Z2D over (n_z, Ny, Nx), the kernel table built on the host once,
+// the padded input (zero outside the (n_y, n_x) corner, set once)
+static int ps_wire_plan(wvlh_ctx *ctx, const int n[3], const double h[3], PsPlan **out)
+{
+    std::lock_guard<std::mutex> lock(g_ps_mutex);
+    const auto key = std::make_tuple((const void *)ctx, ctx->device, n[0], n[1], n[2], h[0], h[1], h[2]);
+    auto it = g_ps_wire.find(key);
+    if (it != g_ps_wire.end()) {
+        *out = it->second;
+        return WVLH_OK;
+    }
+    PsPlan *pl = new PsPlan();
+    pl->nf[0] = fft_length(2 * n[0]);
+    pl->nf[1] = fft_length(2 * n[1]);
+    pl->nf[2] = n[2];
+    const int N1 = pl->nf[0], N2 = pl->nf[1], N3 = pl->nf[2];
+    const size_t npad = (size_t)N3 * N2 * N1, nspec = (size_t)N3 * N2 * (N1 / 2 + 1);
+    int rc = WVLH_OK;
+    if (cufftPlan3d(&pl->fwd, N3, N2, N1, CUFFT_D2Z) != CUFFT_SUCCESS ||
+        cufftPlan3d(&pl->inv, N3, N2, N1, CUFFT_Z2D) != CUFFT_SUCCESS)
+        rc = WVLH_ERR_CUDA;
+    std::vector<double> tab;
+    if (!rc) {
+        wire_kernel_table(n, h, N1, N2, tab);
+        if ((rc = pl->ker.ensure(sizeof(double) * tab.size())) || (rc = pl->pad.ensure(sizeof(double) * npad)) ||
+            (rc = pl->work.ensure(sizeof(double) * npad)) ||
+            (rc = pl->spec.ensure(sizeof(cufftDoubleComplex) * nspec)) || (rc = ps_energy_buffers(ctx, pl)))
+            ;
+    }
+    if (!rc) {
+        cudaStream_t st = ctx->stream;
+        const bool ok =
+            cudaMemcpyAsync(pl->ker.p, tab.data(), sizeof(double) * tab.size(), cudaMemcpyHostToDevice, st) ==
+                cudaSuccess &&
+            cudaMemsetAsync(pl->pad.p, 0, sizeof(double) * npad, st) == cudaSuccess &&
+            cudaStreamSynchronize(st) == cudaSuccess;
+        if (!ok) rc = WVLH_ERR_CUDA;
+    }
+    if (rc) {
+        free_plan(pl);
+        return rc;
+    }
+    g_ps_wire.emplace(key, pl);
+    *out = pl;
+    return WVLH_OK;
+}
+
+extern "C" int wvlh_psolver_wire(wvlh_ctx *ctx, const int n[3], const double h[3], const double *rho, double *pot,
+                                 double *eh)
+{
+    if (!ctx || !n || !h || !rho || !pot || (eh && pot == rho) || !ps_free_args_ok(n, h))
+        return ps_fail(WVLH_ERR_ARG);
+    if (cudaSetDevice(ctx->device) != cudaSuccess) return ps_fail(WVLH_ERR_CUDA);
+    PsPlan *pl = nullptr;
+    int rc = ps_wire_plan(ctx, n, h, &pl);
+    if (rc) return ps_fail(rc);
+    const int N1 = pl->nf[0], N2 = pl->nf[1], N3 = pl->nf[2];
+    cudaStream_t st = ctx->stream;
+    double *pad = (double *)pl->pad.p, *work = (double *)pl->work.p;
+    cufftDoubleComplex *z = (cufftDoubleComplex *)pl->spec.p;
+    k_free_pad<<<kPsBlocks, 256, 0, st>>>(n[0], n[1], n[2], N1, N2, rho, pad);
+    bool ok = cudaGetLastError() == cudaSuccess && cufftSetStream(pl->fwd, st) == CUFFT_SUCCESS &&
+              cufftSetStream(pl->inv, st) == CUFFT_SUCCESS && cufftExecD2Z(pl->fwd, pad, z) == CUFFT_SUCCESS;
+    if (ok) {
+        // -2 h_x h_y / (N1 N2 N3), createKernel.f90:502
+        const double scal = -2.0 * h[0] * h[1] / ((double)N1 * (double)N2 * (double)N3);
+        k_table_multiply<<<kPsBlocks, 256, 0, st>>>(N1, N2, N3, (const double *)pl->ker.p, scal, 0, 0.0, z);
+        ok = cudaGetLastError() == cudaSuccess && cufftExecZ2D(pl->inv, z, work) == CUFFT_SUCCESS;
+    }
+    if (ok) {
+        k_free_crop<<<kPsBlocks, 256, 0, st>>>(n[0], n[1], n[2], N1, N2, work, rho, pot, (double *)pl->part.p,
+                                               (unsigned int *)pl->cnt.p, 0.5 * h[0] * h[1] * h[2], eh);
+        ok = cudaGetLastError() == cudaSuccess;
+    }
+    if (!ok) return ps_fail(WVLH_ERR_CUDA);
+    return WVLH_OK;
+}
+
+extern "C" int64_t wvlh_psolver_wire_table(const int n[3], const double h[3], int nf[2], double *tab, int64_t cap)
+{
+    if (!n || !h || !nf || !ps_free_args_ok(n, h)) return ps_fail(WVLH_ERR_ARG);
+    nf[0] = fft_length(2 * n[0]);
+    nf[1] = fft_length(2 * n[1]);
+    const int64_t need = (int64_t)(n[2] / 2 + 1) * (nf[1] / 2 + 1) * (nf[0] / 2 + 1);
+    if (!tab) return need;
+    if (cap < need) return ps_fail(WVLH_ERR_ARG);
+    std::vector<double> t;
+    wire_kernel_table(n, h, nf[0], nf[1], t);
     std::copy(t.begin(), t.end(), tab);
     return need;
 }

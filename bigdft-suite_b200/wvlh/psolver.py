@@ -61,6 +61,44 @@ def surface_kernel_table(n, h):
     return N2.value, tab.reshape(n[2] // 2 + 1, N2.value // 2 + 1, n[0] // 2 + 1)
 
 
+def wire_kernel_table(n, h):
+    """Host side of the wire-BC kernel (no device work): ((Nx, Ny), K), the
+    padded x and y lengths and the (n3/2+1, Ny/2+1, Nx/2+1) Fourier table."""
+    import numpy as np
+    nn = (C.c_int * 3)(*[int(v) for v in n])
+    hh = (C.c_double * 3)(*[float(v) for v in h])
+    nf = (C.c_int * 2)()
+    need = lib().wvlh_psolver_wire_table(nn, hh, nf, None, 0)
+    if need < 0:
+        check(int(need), "wvlh_psolver_wire_table")
+    tab = np.zeros(need)
+    check(min(0, int(lib().wvlh_psolver_wire_table(nn, hh, nf, tab.ctypes.data_as(C.c_void_p), need))),
+          "wvlh_psolver_wire_table")
+    return (nf[0], nf[1]), tab.reshape(n[2] // 2 + 1, nf[1] // 2 + 1, nf[0] // 2 + 1)
+
+
+def _hartree_bc(ctx, fn, rho, h, pot, energy):
+    torch = ctx.torch
+    if rho.dtype != torch.float64 or rho.dim() != 3 or not rho.is_contiguous():
+        raise WvlhError("rho: contiguous 3D float64 device tensor (z, y, x)")
+    if pot is None:
+        pot = torch.empty_like(rho)
+    if pot.shape != rho.shape or pot.dtype != torch.float64 or not pot.is_contiguous():
+        raise WvlhError("pot: a tensor like rho")
+    n = (C.c_int * 3)(rho.shape[2], rho.shape[1], rho.shape[0])
+    hh = (C.c_double * 3)(*[float(v) for v in h])
+    eh = torch.empty((), dtype=torch.float64, device=rho.device) if energy else None
+    check(getattr(lib(), fn)(ctx.h, n, hh, C.c_void_p(rho.data_ptr()), C.c_void_p(pot.data_ptr()),
+                             C.c_void_p(eh.data_ptr()) if energy else None), fn)
+    return pot, eh
+
+
+def hartree_wire(ctx, rho, h, pot=None, energy=True):
+    """The Hartree potential with wire boundary conditions (z periodic, x and
+    y free; wvlh_psolver_wire); arguments and results as hartree_periodic."""
+    return _hartree_bc(ctx, "wvlh_psolver_wire", rho, h, pot, energy)
+
+
 def hartree_surface(ctx, rho, h, pot=None, energy=True):
     """The Hartree potential with surface boundary conditions (x, z periodic,
     y free; wvlh_psolver_surface); arguments and results as hartree_periodic."""

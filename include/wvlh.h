@@ -402,6 +402,18 @@ int wvlh_psolver_surface(wvlh_ctx *ctx, const int n[3], const double h[3], const
  * wvlh_psolver_surface multiplies by.  With tab NULL returns the number of
  * doubles; otherwise fills tab (cap doubles) and returns that number. */
 int64_t wvlh_psolver_surface_table(const int n[3], const double h[3], int *N2, double *tab, int64_t cap);
+/* Hartree potential with wire boundary conditions (z periodic, x and y
+ * free: the reference's PSolver for geocode 'W', Wires_Kernel,
+ * psolver/src/Build_Kernel.f90:2244-2364, from the Gaussian fits of log r
+ * and K0(r) in gaussfit_wires.inc; scal -2 h_x h_y / N, createKernel.f90:
+ * 502): rho zero-padded in x and y to at least twice each.  Arguments and
+ * results as wvlh_psolver_free; the kernel table (built once per grid on the
+ * host's threads), FFT plans and padded buffers are kept by the context. */
+int wvlh_psolver_wire(wvlh_ctx *ctx, const int n[3], const double h[3], const double *rho, double *pot, double *eh);
+/* Host only (no device work): the padded x and y lengths nf and the wire
+ * kernel table K(kz, ky, kx), (n3/2+1, nf[1]/2+1, nf[0]/2+1) doubles.  With
+ * tab NULL returns the number of doubles; otherwise fills tab (cap doubles). */
+int64_t wvlh_psolver_wire_table(const int n[3], const double h[3], int nf[2], double *tab, int64_t cap);
 /* Exchange-correlation potential of the reference's default functional
  * (ixc = 1: the Goedecker-Teter-Hutter Pade LDA, ABINIT's xcspol,
  * libABINIT/src/abi_xc_lowlevel/abi_xcspol.F90:105-250), spin-unpolarised,

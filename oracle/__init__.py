@@ -798,6 +798,76 @@ def psolver_surface(rho, h, N2=None):
     return V, 0.5 * float((rho * V).sum()) * h[0] * h[1] * h[2]
 
 
+def wire_fits():
+    """(p1, w1, p2, w2): the Gaussian fits of log r and K0(r) that the wire
+    kernel is built from (psolver/src/gaussfit_wires.inc; 144 terms used),
+    from the generated filter header."""
+    import re
+    hdr = (HERE.parent / "bigdft-suite_b200" / "csrc" / "wvl_filters.h").read_text()
+    out = []
+    for name in ("WVL_WIRE_P1", "WVL_WIRE_W1", "WVL_WIRE_P2", "WVL_WIRE_W2"):
+        body = re.search(r"#define %s_INIT \{(.*?)\}" % name, hdr, re.S).group(1)
+        out.append(np.array([float(v) for v in body.replace("\\", " ").split(",")])[:144])
+    return tuple(out)
+
+
+def wire_kernel(n0, h, Nx, Ny):
+    """The wire-BC kernel in Fourier space (z periodic, x and y free;
+    Wires_Kernel, Build_Kernel.f90:2244-2364): for each z frequency the 2D
+    Green's function of the plane as a sum of separable Gaussians, each
+    through the ISF overlaps and cosine transforms of the free kernel on the
+    padded lengths (Nx, Ny): at k_z = 0 log(mu0 r) (p1, w1, mu0 =
+    1/sqrt((h_x (n_x + 32))^2 + (h_y (n_y + 32))^2)) and -log(mu0) added at
+    k = 0; otherwise -K0(mu r), mu = 2 pi k_z / (n_z h_z) (p2, -w2).
+    n0 = (n_x, n_y, n_z); returns K of shape (n_z/2+1, Ny/2+1, Nx/2+1)."""
+    nx, ny, nz = n0
+    p1, w1, p2, w2 = wire_fits()
+    nr = max(nx, ny, 32)
+    xs, ys = isf_samples()
+    cos = []
+    for n in (Nx, Ny):
+        J = min(nr, n // 2)
+        kk = np.arange(n // 2 + 1)[:, None]
+        jj = np.arange(1, J)[None, :]
+        cos.append((J, np.cos(2.0 * np.pi * ((kk * jj) % n) / n)))
+    K = np.zeros((nz // 2 + 1, Ny // 2 + 1, Nx // 2 + 1))
+    for kz in range(nz // 2 + 1):
+        if kz == 0:
+            mu = 1.0 / np.sqrt((h[0] * (nx + 32)) ** 2 + (h[1] * (ny + 32)) ** 2)
+            alpha, w = p1, w1
+        else:
+            mu = 2.0 * np.pi / nz * kz / h[2]
+            alpha, w = p2, -w2
+        for k in range(144):
+            C = []
+            for d, (J, cs) in enumerate(cos):
+                f = gauss_conv_isf(alpha[k] * mu * mu, h[d], nr, xs, ys)[nr:nr + J]
+                C.append(f[0] + 2.0 * (cs @ f[1:]))
+            K[kz] += (w[k] * C[0])[None, :] * C[1][:, None]
+        if kz == 0:
+            K[0, 0, 0] -= Nx * Ny * np.log(mu)
+    return K
+
+
+def psolver_wire(rho, h, nfft=None):
+    """Hartree potential and energy of rho (n_z, n_y, n_x; x fastest) with
+    wire boundary conditions (z periodic, x and y free): rho zero-padded in
+    x and y to (Nx, Ny) (default twice), multiplied in Fourier space by
+    wire_kernel, scaled by -2 h_x h_y / (Nx Ny n_z) (createKernel.f90:502),
+    the first (n_y, n_x) kept; energy 0.5 sum(rho V) h^3."""
+    rho = np.asarray(rho, np.float64)
+    nz, ny, nx = rho.shape
+    Nx, Ny = (2 * nx, 2 * ny) if nfft is None else nfft
+    K = wire_kernel((nx, ny, nz), h, Nx, Ny)
+    pad = np.zeros((nz, Ny, Nx))
+    pad[:, :ny, :nx] = rho
+    py = np.minimum(np.arange(Ny), Ny - np.arange(Ny))
+    pz = np.minimum(np.arange(nz), nz - np.arange(nz))
+    Kf = K[pz][:, py]
+    V = np.fft.irfftn(np.fft.rfftn(pad) * Kf, s=pad.shape, axes=(0, 1, 2))[:, :ny, :nx] * (-2.0 * h[0] * h[1])
+    return V, 0.5 * float((rho * V).sum()) * h[0] * h[1] * h[2]
+
+
 def psolver_free(rho, h, nfft=None):
     """Hartree potential and energy of rho (n3, n2, n1; x fastest) with free
     boundary conditions: rho zero-padded to nfft (default twice each

@@ -248,3 +248,31 @@ def test_surface_matches_oracle(oracle, torch_cuda, wctx, n, h):
         hartree_surface(wctx, t, h, pot=t, energy=True)
     hartree_surface(wctx, t, h, pot=t, energy=False)
     assert torch.equal(t, pot)
+
+
+def test_reference_ps_check_wire_golden(torch_cuda, wctx):
+    """The reference's PS_Check wire-BC run (51 x 55 x 64): the Hartree
+    energy and the potential at the printed point to their 13 digits."""
+    from test_psolver_rule import PS_WIRE_AT, PS_WIRE_EH, PS_WIRE_V, ps_check_wire
+    from wvlh.psolver import hartree_wire
+    torch = torch_cuda
+    rho, h = ps_check_wire()
+    pot, eh = hartree_wire(wctx, torch.tensor(rho, device="cuda"), h)
+    i1, i2, i3 = (v - 1 for v in PS_WIRE_AT)
+    assert abs(eh.item() - PS_WIRE_EH) <= 5e-13 * PS_WIRE_EH
+    assert abs(pot.cpu().numpy()[i3, i2, i1] - PS_WIRE_V) <= 5e-13 * PS_WIRE_V
+
+
+def test_wire_matches_oracle(oracle, torch_cuda, wctx):
+    from wvlh.psolver import hartree_wire
+    torch = torch_cuda
+    n, h = (10, 12, 8), (0.3, 0.35, 0.4)
+    rng = np.random.default_rng(13)
+    rho = rng.uniform(-1, 1, n[::-1])
+    ref, eref = oracle.psolver_wire(rho, h)
+    t = torch.tensor(rho, device="cuda")
+    pot, eh = hartree_wire(wctx, t, h)
+    assert np.abs(pot.cpu().numpy() - ref).max() <= 1e-13 * np.abs(ref).max()
+    assert abs(eh.item() - eref) <= 1e-12 * abs(eref)
+    pot2, eh2 = hartree_wire(wctx, t, h)
+    assert torch.equal(pot, pot2) and torch.equal(eh, eh2)

@@ -391,3 +391,41 @@ def test_surface_kernel_host_table_matches_oracle(oracle):
     assert N2 >= 2 * n[1] and N2 % 2 == 0
     ref = oracle.surface_kernel(n, h, N2)
     assert np.abs(K - ref).max() <= 1e-13 * np.abs(ref).max()
+
+
+def ps_check_wire():
+    """The wire-BC case of the reference's PS_Check test (z periodic, x and
+    y free; fill_functions_arrays_wires, psolver/tests/functions.f90:437-467):
+    a 51 x 55 x 64 box of side 10 bohr per dimension, rho = exp(-2 (x^2 + y^2))
+    on centred coordinates.  Arrays (z, y, x)."""
+    n = (51, 55, 64)
+    h = tuple(10.0 / m for m in n)
+    x = np.arange(n[0]) * h[0] - 0.5 * n[0] * h[0]
+    y = np.arange(n[1]) * h[1] - 0.5 * n[1] * h[1]
+    r2 = x[None, None, :] ** 2 + y[None, :, None] ** 2
+    return np.broadcast_to(np.exp(-2.0 * r2), (n[2], n[1], n[0])).copy(), h
+
+
+# psolver/tests/PS_Check.ref.yaml:569-578 (wire BC, 51 x 55 x 64): the Hartree
+# energy and the potential at (26, 28, 1), 1-based (x, y, z)
+PS_WIRE_EH = 7.121112829810e00
+PS_WIRE_AT = (26, 28, 1)
+PS_WIRE_V = 1.939819652123e00
+
+
+def test_reference_ps_check_wire_golden(oracle):
+    rho, h = ps_check_wire()
+    pot, eh = oracle.psolver_wire(rho, h)
+    assert abs(eh - PS_WIRE_EH) <= 5e-13 * PS_WIRE_EH                    # all 13 printed digits
+    i1, i2, i3 = (v - 1 for v in PS_WIRE_AT)
+    assert abs(pot[i3, i2, i1] - PS_WIRE_V) <= 5e-13 * PS_WIRE_V
+
+
+def test_wire_kernel_host_table_matches_oracle(oracle):
+    from wvlh.psolver import wire_kernel_table
+    n = (10, 12, 8)
+    h = (0.3, 0.35, 0.4)
+    (Nx, Ny), K = wire_kernel_table(n, h)
+    assert Nx >= 2 * n[0] and Ny >= 2 * n[1]
+    ref = oracle.wire_kernel(n, h, Nx, Ny)
+    assert np.abs(K - ref).max() <= 1e-12 * np.abs(ref).max()
