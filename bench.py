@@ -40,7 +40,7 @@ UNIT = "coarse pts/s"
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=100)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="wvlh", choices=["wvlh", "reference"])
     ap.add_argument("--n", type=int, default=48)
@@ -60,8 +60,12 @@ def peaks():
 
 
 class ClockSampler:
-    """nvidia-smi clock / throttle sampling during the timed region."""
-    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+    """nvidia-smi clock / throttle sampling during the timed region: samples
+    every 50 ms with their timestamps; stop(window) keeps those taken between
+    the host clock readings around the timed loop (all of them if none fall
+    inside a very short region, which the result then says)."""
+    Q = ("timestamp,index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,"
          "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
          "clocks_event_reasons.sw_power_cap")
 
@@ -74,12 +78,13 @@ class ClockSampler:
         try:
             self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.idx), "--query-gpu=" + self.Q,
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                          "--format=csv,noheader,nounits", "-lms", "50"],
                                          stdout=self.f, stderr=subprocess.DEVNULL)
         except Exception:
             self.proc = None
 
-    def stop(self):
+    def stop(self, window=None):
+        import datetime
         if not self.proc:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
         self.proc.terminate()
@@ -90,22 +95,34 @@ class ClockSampler:
         self.f.flush()
         rows = [l.split(",") for l in Path(self.f.name).read_text().splitlines() if l.strip()]
         os.unlink(self.f.name)
+        rows = [[x.strip() for x in r] for r in rows]
+
+        def stamp(r):
+            try:
+                return datetime.datetime.strptime(r[0], "%Y/%m/%d %H:%M:%S.%f").timestamp()
+            except (ValueError, IndexError):
+                return None
+        scope = "timed region"
+        if window:
+            inside = [r for r in rows if stamp(r) is not None and window[0] - 0.05 <= stamp(r) <= window[1] + 0.05]
+            if inside:
+                rows = inside
+            else:
+                scope = "whole run (timed region shorter than the sampling interval)"
         sm, smax, reasons = [], None, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         for r in rows:
-            r = [x.strip() for x in r]
             try:
-                sm.append(float(r[1]))
-                smax = float(r[2])
+                sm.append(float(r[2]))
+                smax = float(r[3])
             except (ValueError, IndexError):
                 continue
             for k, nm in enumerate(names):
-                if len(r) > 5 + k and r[5 + k].lower().startswith("active"):
+                if len(r) > 6 + k and r[6 + k].lower().startswith("active"):
                     reasons.add(nm)
         sm.sort()
-        load = [s for s in sm if smax and s > 0.3 * smax] or sm
-        med = load[len(load) // 2] if load else None
-        return {"sm_mhz": med, "sm_max_mhz": smax, "reasons": sorted(reasons), "samples": len(sm)}
+        med = sm[len(sm) // 2] if sm else None
+        return {"sm_mhz": med, "sm_max_mhz": smax, "reasons": sorted(reasons), "samples": len(sm), "scope": scope}
 
 
 def dist_setup(args):
@@ -601,14 +618,16 @@ def main():
     torch.cuda.synchronize()
     st = torch.cuda.current_stream(dev)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    w0 = time.time()
     e0.record(st)
     for _ in range(args.steps):
         step()
     e1.record(st)
     torch.cuda.synchronize()
+    w1 = time.time()
     if ws > 1:
         torch.distributed.barrier()
-    clocks = sampler.stop()
+    clocks = sampler.stop((w0, w1))
     ms = e0.elapsed_time(e1)
     t = torch.tensor([ms], dtype=torch.float64, device=dev)
     if ws > 1:
