@@ -1162,11 +1162,11 @@ extern "C" int wvlh_ks_potential_free(wvlh_ctx *ctx, const int n[3], const doubl
 
 extern "C" int64_t wvlh_psolver_free_tables(const int n[3], const double h[3], int nf[3], double *tab, int64_t cap)
 {
-    if (!n || !h || !nf || !ps_free_args_ok(n, h)) return ps_fail(WVLH_ERR_ARG);
+    if (!n || !h || !nf || !ps_free_args_ok(n, h)) return -(int64_t)ps_fail(WVLH_ERR_ARG);
     for (int d = 0; d < 3; ++d) nf[d] = fft_length(2 * n[d]);
     const int64_t need = 89LL * (nf[0] / 2 + nf[1] / 2 + nf[2] / 2 + 3) + 89;
     if (!tab) return need;
-    if (cap < need) return ps_fail(WVLH_ERR_ARG);
+    if (cap < need) return -(int64_t)ps_fail(WVLH_ERR_ARG);
     std::vector<double> t;
     free_kernel_tables(n, h, nf, t);
     std::copy(t.begin(), t.end(), tab);
@@ -1311,11 +1311,11 @@ extern "C" int wvlh_psolver_surface(wvlh_ctx *ctx, const int n[3], const double 
 
 extern "C" int64_t wvlh_psolver_surface_table(const int n[3], const double h[3], int *N2, double *tab, int64_t cap)
 {
-    if (!n || !h || !N2 || !ps_free_args_ok(n, h)) return ps_fail(WVLH_ERR_ARG);
+    if (!n || !h || !N2 || !ps_free_args_ok(n, h)) return -(int64_t)ps_fail(WVLH_ERR_ARG);
     *N2 = fft_length(2 * n[1]);
     const int64_t need = (int64_t)(n[2] / 2 + 1) * (*N2 / 2 + 1) * (n[0] / 2 + 1);
     if (!tab) return need;
-    if (cap < need) return ps_fail(WVLH_ERR_ARG);
+    if (cap < need) return -(int64_t)ps_fail(WVLH_ERR_ARG);
     std::vector<double> t;
     surface_kernel_table(n, h, *N2, t);
     std::copy(t.begin(), t.end(), tab);
@@ -1403,12 +1403,12 @@ extern "C" int wvlh_psolver_wire(wvlh_ctx *ctx, const int n[3], const double h[3
 
 extern "C" int64_t wvlh_psolver_wire_table(const int n[3], const double h[3], int nf[2], double *tab, int64_t cap)
 {
-    if (!n || !h || !nf || !ps_free_args_ok(n, h)) return ps_fail(WVLH_ERR_ARG);
+    if (!n || !h || !nf || !ps_free_args_ok(n, h)) return -(int64_t)ps_fail(WVLH_ERR_ARG);
     nf[0] = fft_length(2 * n[0]);
     nf[1] = fft_length(2 * n[1]);
     const int64_t need = (int64_t)(n[2] / 2 + 1) * (nf[1] / 2 + 1) * (nf[0] / 2 + 1);
     if (!tab) return need;
-    if (cap < need) return ps_fail(WVLH_ERR_ARG);
+    if (cap < need) return -(int64_t)ps_fail(WVLH_ERR_ARG);
     std::vector<double> t;
     wire_kernel_table(n, h, nf[0], nf[1], t);
     std::copy(t.begin(), t.end(), tab);

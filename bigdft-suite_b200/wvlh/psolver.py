@@ -20,9 +20,9 @@ def free_kernel_tables(n, h):
     nf = (C.c_int * 3)()
     need = lib().wvlh_psolver_free_tables(nn, hh, nf, None, 0)
     if need < 0:
-        check(int(need), "wvlh_psolver_free_tables")
+        check(-int(need), "wvlh_psolver_free_tables")
     tab = np.zeros(need)
-    check(min(0, int(lib().wvlh_psolver_free_tables(nn, hh, nf, tab.ctypes.data_as(C.c_void_p), need))),
+    check(max(0, -int(lib().wvlh_psolver_free_tables(nn, hh, nf, tab.ctypes.data_as(C.c_void_p), need))),
           "wvlh_psolver_free_tables")
     return tuple(nf), tab[:-89].reshape(89, -1), tab[-89:]
 
@@ -54,9 +54,9 @@ def surface_kernel_table(n, h):
     N2 = C.c_int()
     need = lib().wvlh_psolver_surface_table(nn, hh, C.byref(N2), None, 0)
     if need < 0:
-        check(int(need), "wvlh_psolver_surface_table")
+        check(-int(need), "wvlh_psolver_surface_table")
     tab = np.zeros(need)
-    check(min(0, int(lib().wvlh_psolver_surface_table(nn, hh, C.byref(N2), tab.ctypes.data_as(C.c_void_p), need))),
+    check(max(0, -int(lib().wvlh_psolver_surface_table(nn, hh, C.byref(N2), tab.ctypes.data_as(C.c_void_p), need))),
           "wvlh_psolver_surface_table")
     return N2.value, tab.reshape(n[2] // 2 + 1, N2.value // 2 + 1, n[0] // 2 + 1)
 
@@ -70,9 +70,9 @@ def wire_kernel_table(n, h):
     nf = (C.c_int * 2)()
     need = lib().wvlh_psolver_wire_table(nn, hh, nf, None, 0)
     if need < 0:
-        check(int(need), "wvlh_psolver_wire_table")
+        check(-int(need), "wvlh_psolver_wire_table")
     tab = np.zeros(need)
-    check(min(0, int(lib().wvlh_psolver_wire_table(nn, hh, nf, tab.ctypes.data_as(C.c_void_p), need))),
+    check(max(0, -int(lib().wvlh_psolver_wire_table(nn, hh, nf, tab.ctypes.data_as(C.c_void_p), need))),
           "wvlh_psolver_wire_table")
     return (nf[0], nf[1]), tab.reshape(n[2] // 2 + 1, nf[1] // 2 + 1, nf[0] // 2 + 1)
 

@@ -385,7 +385,7 @@ int wvlh_psolver_free(wvlh_ctx *ctx, const int n[3], const double h[3], const do
  * a row [C_x(0..N1/2) | C_y(0..N2/2) | C_z(0..N3/2)], then the 89 weights;
  * K(k3, k2, k1) = sum_g C_x(k1) (C_z(k3) (C_y(k2) w_g)), g from 88 down to 0.
  * With tab NULL returns the number of doubles; otherwise fills tab (cap
- * doubles) and returns that number, or a negative error. */
+ * doubles) and returns that number; on an error, minus the error code. */
 int64_t wvlh_psolver_free_tables(const int n[3], const double h[3], int nf[3], double *tab, int64_t cap);
 /* Hartree potential with surface boundary conditions (x and z periodic, y
  * free: the reference's PSolver for geocode 'S', Surfaces_Kernel,
@@ -400,7 +400,8 @@ int wvlh_psolver_surface(wvlh_ctx *ctx, const int n[3], const double h[3], const
 /* Host only (no device work): the padded y length N2 and the surface kernel
  * table K(k3, ky, k1), (n3/2+1, N2/2+1, n1/2+1) doubles, that
  * wvlh_psolver_surface multiplies by.  With tab NULL returns the number of
- * doubles; otherwise fills tab (cap doubles) and returns that number. */
+ * doubles; otherwise fills tab (cap doubles) and returns that number; on an
+ * error, minus the error code. */
 int64_t wvlh_psolver_surface_table(const int n[3], const double h[3], int *N2, double *tab, int64_t cap);
 /* Hartree potential with wire boundary conditions (z periodic, x and y
  * free: the reference's PSolver for geocode 'W', Wires_Kernel,
@@ -412,7 +413,8 @@ int64_t wvlh_psolver_surface_table(const int n[3], const double h[3], int *N2, d
 int wvlh_psolver_wire(wvlh_ctx *ctx, const int n[3], const double h[3], const double *rho, double *pot, double *eh);
 /* Host only (no device work): the padded x and y lengths nf and the wire
  * kernel table K(kz, ky, kx), (n3/2+1, nf[1]/2+1, nf[0]/2+1) doubles.  With
- * tab NULL returns the number of doubles; otherwise fills tab (cap doubles). */
+ * tab NULL returns the number of doubles; otherwise fills tab (cap doubles)
+ * and returns that number; on an error, minus the error code. */
 int64_t wvlh_psolver_wire_table(const int n[3], const double h[3], int nf[2], double *tab, int64_t cap);
 /* Exchange-correlation potential of the reference's default functional
  * (ixc = 1: the Goedecker-Teter-Hutter Pade LDA, ABINIT's xcspol,

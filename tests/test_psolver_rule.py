@@ -429,3 +429,15 @@ def test_wire_kernel_host_table_matches_oracle(oracle):
     assert Nx >= 2 * n[0] and Ny >= 2 * n[1]
     ref = oracle.wire_kernel(n, h, Nx, Ny)
     assert np.abs(K - ref).max() <= 1e-12 * np.abs(ref).max()
+
+
+def test_kernel_table_entry_points_reject_bad_grids():
+    """The host-only table builders validate their arguments like the device
+    entry points: at least 2 points per dimension, positive spacings."""
+    from wvlh._lib import WvlhError
+    from wvlh.psolver import free_kernel_tables, surface_kernel_table, wire_kernel_table
+    for fn in (free_kernel_tables, surface_kernel_table, wire_kernel_table):
+        with pytest.raises(WvlhError):
+            fn((1, 8, 8), (0.3, 0.3, 0.3))
+        with pytest.raises(WvlhError):
+            fn((8, 8, 8), (0.3, 0.0, 0.3))
