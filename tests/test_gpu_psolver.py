@@ -276,3 +276,18 @@ def test_wire_matches_oracle(oracle, torch_cuda, wctx):
     assert abs(eh.item() - eref) <= 1e-12 * abs(eref)
     pot2, eh2 = hartree_wire(wctx, t, h)
     assert torch.equal(pot, pot2) and torch.equal(eh, eh2)
+
+
+@pytest.mark.parametrize("n", [(11, 10, 9), (9, 13, 7)])
+def test_surface_and_wire_odd_periodic_sizes(oracle, torch_cuda, wctx, n):
+    from wvlh.psolver import hartree_surface, hartree_wire
+    torch = torch_cuda
+    h = (0.31, 0.27, 0.35)
+    rng = np.random.default_rng(sum(n) + 7)
+    rho = rng.uniform(-1, 1, n[::-1])
+    t = torch.tensor(rho, device="cuda")
+    for fn, ref_fn in ((hartree_surface, oracle.psolver_surface), (hartree_wire, oracle.psolver_wire)):
+        ref, eref = ref_fn(rho, h)
+        pot, eh = fn(wctx, t, h)
+        assert np.abs(pot.cpu().numpy() - ref).max() <= 1e-13 * np.abs(ref).max()
+        assert abs(eh.item() - eref) <= 1e-12 * abs(eref)

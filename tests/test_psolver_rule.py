@@ -441,3 +441,17 @@ def test_kernel_table_entry_points_reject_bad_grids():
             fn((1, 8, 8), (0.3, 0.3, 0.3))
         with pytest.raises(WvlhError):
             fn((8, 8, 8), (0.3, 0.0, 0.3))
+
+
+@pytest.mark.parametrize("n", [(11, 10, 9), (9, 13, 7)])
+def test_odd_periodic_sizes_host_tables_match_oracle(oracle, n):
+    """Odd lengths along the periodic axes (x and z for surfaces, z for
+    wires): the half-spectrum and folded frequencies stay consistent."""
+    from wvlh.psolver import surface_kernel_table, wire_kernel_table
+    h = (0.31, 0.27, 0.35)
+    N2, K = surface_kernel_table(n, h)
+    ref = oracle.surface_kernel(n, h, N2)
+    assert np.abs(K - ref).max() <= 1e-13 * np.abs(ref).max()
+    (Nx, Ny), K = wire_kernel_table(n, h)
+    ref = oracle.wire_kernel(n, h, Nx, Ny)
+    assert np.abs(K - ref).max() <= 1e-12 * np.abs(ref).max()
