@@ -1202,6 +1202,39 @@ extern "C" int wvlh_xc_lsda(wvlh_ctx *ctx, int64_t npts, const double *rho_up, c
     return WVLH_OK;
 }
 
+static int ps_padded_hartree(wvlh_ctx *ctx, bool wire, const int n[3], const double h[3], const double *rho,
+                             double *pot, double *eh, PsPlan **out);
+
+// V_H into pot for boundary-condition code bc (0 periodic, offset 0; 1 free;
+// 2 surface; 3 wire), no energy; returns the grid's plan for the energy partials
+static int ps_hartree_bc(wvlh_ctx *ctx, int bc, const int n[3], const double h[3], const double *rho, double *pot,
+                         PsPlan **pl)
+{
+    switch (bc) {
+    case 0: return ps_hartree(ctx, n, h, rho, pot, 0.0, pl);
+    case 1: return ps_free_hartree(ctx, n, h, rho, pot, nullptr, pl);
+    case 2: return ps_padded_hartree(ctx, false, n, h, rho, pot, nullptr, pl);
+    default: return ps_padded_hartree(ctx, true, n, h, rho, pot, nullptr, pl);
+    }
+}
+
+extern "C" int wvlh_ks_potential_bc(wvlh_ctx *ctx, int bc, const int n[3], const double h[3], const double *rho,
+                                    const double *vext, double *pot, double *energies)
+{
+    // the combine pass reads rho and V_ext after V_H is written to pot
+    if (!ctx || !n || !h || !rho || !pot || pot == rho || (vext && vext == pot) || bc < 0 || bc > 3 ||
+        (bc ? !ps_free_args_ok(n, h) : !ps_args_ok(n, h)))
+        return ps_fail(WVLH_ERR_ARG);
+    PsPlan *pl = nullptr;
+    int rc = ps_hartree_bc(ctx, bc, n, h, rho, pot, &pl);
+    if (rc) return ps_fail(rc);
+    const long long npt = (long long)n[0] * n[1] * n[2];
+    k_ks_combine<<<kPsBlocks, 256, 0, ctx->stream>>>(npt, rho, vext, pot, (double *)pl->part.p,
+                                                     (unsigned int *)pl->cnt.p, h[0] * h[1] * h[2], energies);
+    if (cudaGetLastError() != cudaSuccess) return ps_fail(WVLH_ERR_CUDA);
+    return WVLH_OK;
+}
+
 extern "C" int wvlh_ks_potential_spin(wvlh_ctx *ctx, int free_bc, const int n[3], const double h[3],
                                       const double *rho_up, const double *rho_dn, const double *vext, double *pot_up,
                                       double *pot_dn, double *energies)
@@ -1212,14 +1245,14 @@ extern "C" int wvlh_ks_potential_spin(wvlh_ctx *ctx, int free_bc, const int n[3]
         return ps_fail(WVLH_ERR_ARG);
     for (const double *q : {rho_up, rho_dn, vext})
         if (q && (q == pot_up || q == pot_dn)) return ps_fail(WVLH_ERR_ARG);
-    if (free_bc ? !ps_free_args_ok(n, h) : !ps_args_ok(n, h)) return ps_fail(WVLH_ERR_ARG);
+    if (free_bc < 0 || free_bc > 3 || (free_bc ? !ps_free_args_ok(n, h) : !ps_args_ok(n, h)))
+        return ps_fail(WVLH_ERR_ARG);
     if (cudaSetDevice(ctx->device) != cudaSuccess) return ps_fail(WVLH_ERR_CUDA);
     const long long npt = (long long)n[0] * n[1] * n[2];
     k_spin_total<<<kPsBlocks, 256, 0, ctx->stream>>>(npt, rho_up, rho_dn, pot_dn);
     if (cudaGetLastError() != cudaSuccess) return ps_fail(WVLH_ERR_CUDA);
     PsPlan *pl = nullptr;
-    int rc = free_bc ? ps_free_hartree(ctx, n, h, pot_dn, pot_up, nullptr, &pl)
-                     : ps_hartree(ctx, n, h, pot_dn, pot_up, 0.0, &pl);
+    int rc = ps_hartree_bc(ctx, free_bc, n, h, pot_dn, pot_up, &pl);
     if (rc) return ps_fail(rc);
     k_ks_combine_spin<<<kPsBlocks, 256, 0, ctx->stream>>>(npt, rho_up, rho_dn, vext, pot_up, pot_dn,
                                                           (double *)pl->part.p, (unsigned int *)pl->cnt.p,
@@ -1276,17 +1309,17 @@ static int ps_surface_plan(wvlh_ctx *ctx, const int n[3], const double h[3], PsP
     return WVLH_OK;
 }
 
-extern "C" int wvlh_psolver_surface(wvlh_ctx *ctx, const int n[3], const double h[3], const double *rho,
-                                    double *pot, double *eh)
+static int ps_wire_plan(wvlh_ctx *ctx, const int n[3], const double h[3], PsPlan **out);
+
+// V_H of rho with surface (wire when wire) boundary conditions into pot; with
+// eh, *eh = the Hartree energy (reduced by the crop)
+static int ps_padded_hartree(wvlh_ctx *ctx, bool wire, const int n[3], const double h[3], const double *rho,
+                             double *pot, double *eh, PsPlan **out)
 {
-    // rho is copied into the padded buffer before pot is written: pot may be
-    // rho, unless the energy (which reads rho after) is asked for
-    if (!ctx || !n || !h || !rho || !pot || (eh && pot == rho) || !ps_free_args_ok(n, h))
-        return ps_fail(WVLH_ERR_ARG);
-    if (cudaSetDevice(ctx->device) != cudaSuccess) return ps_fail(WVLH_ERR_CUDA);
+    if (cudaSetDevice(ctx->device) != cudaSuccess) return WVLH_ERR_CUDA;
     PsPlan *pl = nullptr;
-    int rc = ps_surface_plan(ctx, n, h, &pl);
-    if (rc) return ps_fail(rc);
+    int rc = wire ? ps_wire_plan(ctx, n, h, &pl) : ps_surface_plan(ctx, n, h, &pl);
+    if (rc) return rc;
     const int N1 = pl->nf[0], N2 = pl->nf[1], N3 = pl->nf[2];
     cudaStream_t st = ctx->stream;
     double *pad = (double *)pl->pad.p, *work = (double *)pl->work.p;
@@ -1295,8 +1328,9 @@ extern "C" int wvlh_psolver_surface(wvlh_ctx *ctx, const int n[3], const double 
     bool ok = cudaGetLastError() == cudaSuccess && cufftSetStream(pl->fwd, st) == CUFFT_SUCCESS &&
               cufftSetStream(pl->inv, st) == CUFFT_SUCCESS && cufftExecD2Z(pl->fwd, pad, z) == CUFFT_SUCCESS;
     if (ok) {
-        // -4 pi h_y / (N1 N2 N3), createKernel.f90:374
-        const double scal = -4.0 * 3.14159265358979323846 * h[1] / ((double)N1 * (double)N2 * (double)N3);
+        // surface: -4 pi h_y / (N1 N2 N3), createKernel.f90:374; wire: -2 h_x h_y / (N1 N2 N3), :502
+        const double scal = (wire ? -2.0 * h[0] * h[1] : -4.0 * 3.14159265358979323846 * h[1]) /
+                            ((double)N1 * (double)N2 * (double)N3);
         k_table_multiply<<<kPsBlocks, 256, 0, st>>>(N1, N2, N3, (const double *)pl->ker.p, scal, 0, 0.0, z);
         ok = cudaGetLastError() == cudaSuccess && cufftExecZ2D(pl->inv, z, work) == CUFFT_SUCCESS;
     }
@@ -1305,8 +1339,21 @@ extern "C" int wvlh_psolver_surface(wvlh_ctx *ctx, const int n[3], const double 
                                                (unsigned int *)pl->cnt.p, 0.5 * h[0] * h[1] * h[2], eh);
         ok = cudaGetLastError() == cudaSuccess;
     }
-    if (!ok) return ps_fail(WVLH_ERR_CUDA);
+    if (!ok) return WVLH_ERR_CUDA;
+    *out = pl;
     return WVLH_OK;
+}
+
+extern "C" int wvlh_psolver_surface(wvlh_ctx *ctx, const int n[3], const double h[3], const double *rho,
+                                    double *pot, double *eh)
+{
+    // rho is copied into the padded buffer before pot is written: pot may be
+    // rho, unless the energy (which reads rho after) is asked for
+    if (!ctx || !n || !h || !rho || !pot || (eh && pot == rho) || !ps_free_args_ok(n, h))
+        return ps_fail(WVLH_ERR_ARG);
+    PsPlan *pl = nullptr;
+    const int rc = ps_padded_hartree(ctx, false, n, h, rho, pot, eh, &pl);
+    return rc ? ps_fail(rc) : WVLH_OK;
 }
 
 extern "C" int64_t wvlh_psolver_surface_table(const int n[3], const double h[3], int *N2, double *tab, int64_t cap)
@@ -1375,30 +1422,9 @@ extern "C" int wvlh_psolver_wire(wvlh_ctx *ctx, const int n[3], const double h[3
 {
     if (!ctx || !n || !h || !rho || !pot || (eh && pot == rho) || !ps_free_args_ok(n, h))
         return ps_fail(WVLH_ERR_ARG);
-    if (cudaSetDevice(ctx->device) != cudaSuccess) return ps_fail(WVLH_ERR_CUDA);
     PsPlan *pl = nullptr;
-    int rc = ps_wire_plan(ctx, n, h, &pl);
-    if (rc) return ps_fail(rc);
-    const int N1 = pl->nf[0], N2 = pl->nf[1], N3 = pl->nf[2];
-    cudaStream_t st = ctx->stream;
-    double *pad = (double *)pl->pad.p, *work = (double *)pl->work.p;
-    cufftDoubleComplex *z = (cufftDoubleComplex *)pl->spec.p;
-    k_free_pad<<<kPsBlocks, 256, 0, st>>>(n[0], n[1], n[2], N1, N2, rho, pad);
-    bool ok = cudaGetLastError() == cudaSuccess && cufftSetStream(pl->fwd, st) == CUFFT_SUCCESS &&
-              cufftSetStream(pl->inv, st) == CUFFT_SUCCESS && cufftExecD2Z(pl->fwd, pad, z) == CUFFT_SUCCESS;
-    if (ok) {
-        // -2 h_x h_y / (N1 N2 N3), createKernel.f90:502
-        const double scal = -2.0 * h[0] * h[1] / ((double)N1 * (double)N2 * (double)N3);
-        k_table_multiply<<<kPsBlocks, 256, 0, st>>>(N1, N2, N3, (const double *)pl->ker.p, scal, 0, 0.0, z);
-        ok = cudaGetLastError() == cudaSuccess && cufftExecZ2D(pl->inv, z, work) == CUFFT_SUCCESS;
-    }
-    if (ok) {
-        k_free_crop<<<kPsBlocks, 256, 0, st>>>(n[0], n[1], n[2], N1, N2, work, rho, pot, (double *)pl->part.p,
-                                               (unsigned int *)pl->cnt.p, 0.5 * h[0] * h[1] * h[2], eh);
-        ok = cudaGetLastError() == cudaSuccess;
-    }
-    if (!ok) return ps_fail(WVLH_ERR_CUDA);
-    return WVLH_OK;
+    const int rc = ps_padded_hartree(ctx, true, n, h, rho, pot, eh, &pl);
+    return rc ? ps_fail(rc) : WVLH_OK;
 }
 
 extern "C" int64_t wvlh_psolver_wire_table(const int n[3], const double h[3], int nf[2], double *tab, int64_t cap)

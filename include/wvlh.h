@@ -448,9 +448,17 @@ int wvlh_ks_potential_free(wvlh_ctx *ctx, const int n[3], const double h[3], con
  * sum_sigma v_sigma rho_sigma. */
 int wvlh_xc_lsda(wvlh_ctx *ctx, int64_t npts, const double *rho_up, const double *rho_dn, double *vxc_up,
                  double *vxc_dn, int accumulate, double dvol, double *energies);
+/* The Kohn-Sham potential of updatePotential for any of the reference's
+ * boundary conditions, bc = 0 periodic (offset 0), 1 free, 2 surface, 3 wire:
+ * pot = (V_H[rho] + vext) + V_xc[rho], V_H as wvlh_psolver_periodic / _free /
+ * _surface / _wire; arguments, aliasing rules and energies as
+ * wvlh_ks_potential_periodic. */
+int wvlh_ks_potential_bc(wvlh_ctx *ctx, int bc, const int n[3], const double h[3], const double *rho,
+                         const double *vext, double *pot, double *energies);
 /* The Kohn-Sham potentials of updatePotential with nspin = 2
- * (rhopotential.f90:87-120): V_H of the total density (periodic, or free
- * boundary conditions when free_bc), pot_sigma = (V_H + vext) + V_xc,sigma;
+ * (rhopotential.f90:87-120): V_H of the total density (free_bc: the
+ * boundary-condition code of wvlh_ks_potential_bc; 0 periodic, 1 free,
+ * 2 surface, 3 wire), pot_sigma = (V_H + vext) + V_xc,sigma;
  * energies as wvlh_ks_potential_periodic (evxc summed over both spins).
  * pot_up and pot_dn are distinct and alias no input. */
 int wvlh_ks_potential_spin(wvlh_ctx *ctx, int free_bc, const int n[3], const double h[3], const double *rho_up,

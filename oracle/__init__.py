@@ -965,12 +965,20 @@ def ks_potential_spin(rho_up, rho_dn, h, vext=None, free=False):
     up = np.asarray(rho_up, np.float64)
     dn = np.asarray(rho_dn, np.float64)
     tot = up + dn
-    vh, eh = psolver_free(tot, h) if free else psolver_periodic(tot, h)
+    vh, eh = _hartree_bc(tot, h, free)
     eps, vu, vd = xc_lsda(up, dn)
     base = vh if vext is None else vh + np.asarray(vext, np.float64)
     dvol = h[0] * h[1] * h[2]
     return (base + vu, base + vd,
             (eh, float((eps * tot).sum()) * dvol, float((vu * up + vd * dn).sum()) * dvol))
+
+
+def _hartree_bc(rho, h, bc):
+    """V_H for a boundary condition: False / "periodic", True / "free",
+    "surface" or "wire"."""
+    bc = {False: "periodic", True: "free"}.get(bc, bc)
+    return {"periodic": psolver_periodic, "free": psolver_free, "surface": psolver_surface,
+            "wire": psolver_wire}[bc](rho, h)
 
 
 def ks_potential_free(rho, h, vext=None):
@@ -986,7 +994,7 @@ def ks_potential_periodic(rho, h, vext=None, free=False):
     dvol sum v_xc rho), H_potential with V_ext summed in (offset 0), then
     rhov += V_xc.  Returns (pot, (eh, exc, evxc))."""
     rho = np.asarray(rho, np.float64)
-    vh, eh = psolver_free(rho, h) if free else psolver_periodic(rho, h)
+    vh, eh = _hartree_bc(rho, h, free)
     eps, vxc = xc_lda(rho)
     dvol = h[0] * h[1] * h[2]
     pot = (vh if vext is None else vh + np.asarray(vext, np.float64)) + vxc   # H_potential's sum, then the axpy

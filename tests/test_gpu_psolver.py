@@ -291,3 +291,29 @@ def test_surface_and_wire_odd_periodic_sizes(oracle, torch_cuda, wctx, n):
         pot, eh = fn(wctx, t, h)
         assert np.abs(pot.cpu().numpy() - ref).max() <= 1e-13 * np.abs(ref).max()
         assert abs(eh.item() - eref) <= 1e-12 * abs(eref)
+
+
+@pytest.mark.parametrize("bc", ["surface", "wire", "free", "periodic"])
+def test_ks_potential_every_boundary_condition(oracle, torch_cuda, wctx, bc):
+    """updatePotential's step for each of the reference's boundary
+    conditions, nspin = 1 and 2, against the oracle."""
+    from wvlh.psolver import ks_potential, ks_potential_spin
+    torch = torch_cuda
+    n, h = (16, 18, 20), (0.3, 0.32, 0.28)
+    rng = np.random.default_rng(len(bc))
+    up = rng.uniform(1e-4, 0.4, n[::-1])
+    dn = rng.uniform(1e-4, 0.4, n[::-1])
+    vext = rng.uniform(-1, 1, n[::-1])
+    tu, td, tv = (torch.tensor(a, device="cuda") for a in (up, dn, vext))
+    ref, (eh, exc, evxc) = oracle.ks_potential_periodic(up + dn, h, vext, free=bc)
+    pot, en = ks_potential(wctx, tu + td, h, bc=bc, vext=tv)
+    assert np.abs(pot.cpu().numpy() - ref).max() <= 1e-13 * np.abs(ref).max()
+    for a, b in zip(en.cpu().numpy(), (eh, exc, evxc)):
+        assert abs(a - b) <= 1e-12 * abs(b)
+    ru, rd, refs = oracle.ks_potential_spin(up, dn, h, vext, free=bc)
+    pu, pd, en2 = ks_potential_spin(wctx, tu, td, h, vext=tv, bc=bc)
+    scale = max(np.abs(ru).max(), np.abs(rd).max())
+    assert np.abs(pu.cpu().numpy() - ru).max() <= 1e-13 * scale
+    assert np.abs(pd.cpu().numpy() - rd).max() <= 1e-13 * scale
+    for a, b in zip(en2.cpu().numpy(), refs):
+        assert abs(a - b) <= 1e-12 * abs(b)
