@@ -229,16 +229,19 @@ __global__ void k_xc_lda(long long n, const double *__restrict__ rho, double *__
 // with out, out[0..2] = (0.5 dvol sum rho V_H, dvol sum eps rho, dvol sum v rho)
 __global__ void k_ks_combine(long long n, const double *__restrict__ rho, const double *__restrict__ vext,
                              double *__restrict__ pot, double *__restrict__ part, unsigned int *cnt, double dvol,
-                             double *__restrict__ out)
+                             double *__restrict__ out, const double *__restrict__ rhocore = nullptr)
 {
     __shared__ double red[32];
     double sh = 0.0, se = 0.0, sv = 0.0;
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
         const double r = rho[i], vh = pot[i];
+        // a core density joins the valence one for XC only (XC_potential adds it
+        // before the functional and takes its share out of int rho V_xc)
+        const double rx = rhocore ? r + rhocore[i] : r;
         double e, v;
-        teter_lda(r, e, v);
+        teter_lda(rx, e, v);
         sh = fma(vh, r, sh);
-        se = fma(e, r, se);
+        se = fma(e, rx, se);
         sv = fma(v, r, sv);
         pot[i] = (vext ? vh + vext[i] : vh) + v;
     }
@@ -326,17 +329,19 @@ __global__ void k_spin_total(long long n, const double *__restrict__ up, const d
 // out[0..2] = (0.5 dvol sum rho V_H, dvol sum eps rho, dvol sum_sigma v rho)
 __global__ void k_ks_combine_spin(long long n, const double *__restrict__ up, const double *__restrict__ dn,
                                   const double *__restrict__ vext, double *__restrict__ pu, double *__restrict__ pd,
-                                  double *__restrict__ part, unsigned int *cnt, double dvol, double *__restrict__ out)
+                                  double *__restrict__ part, unsigned int *cnt, double dvol, double *__restrict__ out,
+                                  const double *__restrict__ rhocore = nullptr)
 {
     __shared__ double red[32];
     double sh = 0.0, se = 0.0, sv = 0.0;
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
         const double ru = up[i], rd = dn[i], vh = pu[i];
+        const double hc = rhocore ? 0.5 * rhocore[i] : 0.0;   // half the core density on each spin
         double e, a, b;
-        teter_lsda(ru, rd, e, a, b);
+        teter_lsda(ru + hc, rd + hc, e, a, b);
         const double r = ru + rd;
         sh = fma(vh, r, sh);
-        se = fma(e, r, se);
+        se = fma(e, (ru + hc) + (rd + hc), se);
         sv = fma(a, ru, fma(b, rd, sv));
         const double base = vext ? vh + vext[i] : vh;
         pu[i] = base + a;
@@ -1219,10 +1224,11 @@ static int ps_hartree_bc(wvlh_ctx *ctx, int bc, const int n[3], const double h[3
 }
 
 extern "C" int wvlh_ks_potential_bc(wvlh_ctx *ctx, int bc, const int n[3], const double h[3], const double *rho,
-                                    const double *vext, double *pot, double *energies)
+                                    const double *rhocore, const double *vext, double *pot, double *energies)
 {
-    // the combine pass reads rho and V_ext after V_H is written to pot
-    if (!ctx || !n || !h || !rho || !pot || pot == rho || (vext && vext == pot) || bc < 0 || bc > 3 ||
+    // the combine pass reads rho, the core density and V_ext after V_H is written to pot
+    if (!ctx || !n || !h || !rho || !pot || pot == rho || (vext && vext == pot) || (rhocore && rhocore == pot) ||
+        bc < 0 || bc > 3 ||
         (bc ? !ps_free_args_ok(n, h) : !ps_args_ok(n, h)))
         return ps_fail(WVLH_ERR_ARG);
     PsPlan *pl = nullptr;
@@ -1230,20 +1236,20 @@ extern "C" int wvlh_ks_potential_bc(wvlh_ctx *ctx, int bc, const int n[3], const
     if (rc) return ps_fail(rc);
     const long long npt = (long long)n[0] * n[1] * n[2];
     k_ks_combine<<<kPsBlocks, 256, 0, ctx->stream>>>(npt, rho, vext, pot, (double *)pl->part.p,
-                                                     (unsigned int *)pl->cnt.p, h[0] * h[1] * h[2], energies);
+                                                     (unsigned int *)pl->cnt.p, h[0] * h[1] * h[2], energies, rhocore);
     if (cudaGetLastError() != cudaSuccess) return ps_fail(WVLH_ERR_CUDA);
     return WVLH_OK;
 }
 
 extern "C" int wvlh_ks_potential_spin(wvlh_ctx *ctx, int free_bc, const int n[3], const double h[3],
-                                      const double *rho_up, const double *rho_dn, const double *vext, double *pot_up,
-                                      double *pot_dn, double *energies)
+                                      const double *rho_up, const double *rho_dn, const double *rhocore,
+                                      const double *vext, double *pot_up, double *pot_dn, double *energies)
 {
     // pot_dn holds the total density for the Hartree solve, pot_up takes V_H:
     // neither may alias an input or the other
     if (!ctx || !n || !h || !rho_up || !rho_dn || !pot_up || !pot_dn || pot_up == pot_dn)
         return ps_fail(WVLH_ERR_ARG);
-    for (const double *q : {rho_up, rho_dn, vext})
+    for (const double *q : {rho_up, rho_dn, vext, rhocore})
         if (q && (q == pot_up || q == pot_dn)) return ps_fail(WVLH_ERR_ARG);
     if (free_bc < 0 || free_bc > 3 || (free_bc ? !ps_free_args_ok(n, h) : !ps_args_ok(n, h)))
         return ps_fail(WVLH_ERR_ARG);
@@ -1256,7 +1262,7 @@ extern "C" int wvlh_ks_potential_spin(wvlh_ctx *ctx, int free_bc, const int n[3]
     if (rc) return ps_fail(rc);
     k_ks_combine_spin<<<kPsBlocks, 256, 0, ctx->stream>>>(npt, rho_up, rho_dn, vext, pot_up, pot_dn,
                                                           (double *)pl->part.p, (unsigned int *)pl->cnt.p,
-                                                          h[0] * h[1] * h[2], energies);
+                                                          h[0] * h[1] * h[2], energies, rhocore);
     if (cudaGetLastError() != cudaSuccess) return ps_fail(WVLH_ERR_CUDA);
     return WVLH_OK;
 }

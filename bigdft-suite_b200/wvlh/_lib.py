@@ -166,10 +166,10 @@ def lib():
     L.wvlh_psolver_wire_table.argtypes = [C.POINTER(C.c_int), C.POINTER(C.c_double), C.POINTER(C.c_int), vp,
                                           C.c_int64]
     L.wvlh_psolver_wire_table.restype = C.c_int64
-    L.wvlh_ks_potential_bc.argtypes = [vp, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_double), vp, vp, vp, vp]
+    L.wvlh_ks_potential_bc.argtypes = [vp, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_double), vp, vp, vp, vp, vp]
     L.wvlh_xc_lsda.argtypes = [vp, C.c_int64, vp, vp, vp, vp, C.c_int, C.c_double, vp]
     L.wvlh_ks_potential_spin.argtypes = [vp, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_double), vp, vp, vp, vp,
-                                         vp, vp]
+                                         vp, vp, vp]
     L.wvlh_host_alloc.restype = vp
     L.wvlh_host_alloc.argtypes = [C.c_size_t]
     L.wvlh_host_free.argtypes = [vp]

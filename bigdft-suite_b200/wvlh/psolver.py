@@ -192,10 +192,11 @@ def ks_potential_periodic(ctx, rho, h, vext=None, pot=None, energy=True, free=Fa
 BC_CODES = {"periodic": 0, "free": 1, "surface": 2, "wire": 3}
 
 
-def ks_potential(ctx, rho, h, bc="periodic", vext=None, pot=None, energy=True):
+def ks_potential(ctx, rho, h, bc="periodic", vext=None, pot=None, energy=True, rhocore=None):
     """The Kohn-Sham potential V_H + vext + V_xc and (eh, exc, evxc) for the
     boundary conditions bc ("periodic", "free", "surface": y free, "wire":
-    x and y free), through wvlh_ks_potential_bc."""
+    x and y free), through wvlh_ks_potential_bc; rhocore: an optional core
+    density for the nonlinear core correction (XC only)."""
     torch = ctx.torch
     _check_rho(ctx, rho)
     if rho.dim() != 3:
@@ -203,13 +204,14 @@ def ks_potential(ctx, rho, h, bc="periodic", vext=None, pot=None, energy=True):
     if bc not in BC_CODES:
         raise WvlhError("bc: one of %s" % sorted(BC_CODES))
     pot = torch.empty_like(rho) if pot is None else pot
-    for name, t in (("pot", pot), ("vext", vext)):
+    for name, t in (("pot", pot), ("vext", vext), ("rhocore", rhocore)):
         if t is not None and (t.shape != rho.shape or t.dtype != torch.float64 or not t.is_contiguous()):
             raise WvlhError("%s: a tensor like rho" % name)
     n = (C.c_int * 3)(rho.shape[2], rho.shape[1], rho.shape[0])
     hh = (C.c_double * 3)(*[float(v) for v in h])
     en = torch.empty(3, dtype=torch.float64, device=rho.device) if energy else None
     check(lib().wvlh_ks_potential_bc(ctx.h, BC_CODES[bc], n, hh, C.c_void_p(rho.data_ptr()),
+                                     C.c_void_p(rhocore.data_ptr()) if rhocore is not None else None,
                                      C.c_void_p(vext.data_ptr()) if vext is not None else None,
                                      C.c_void_p(pot.data_ptr()), C.c_void_p(en.data_ptr()) if energy else None),
           "wvlh_ks_potential_bc")
@@ -245,7 +247,7 @@ def xc_lsda(ctx, rho_up, rho_dn, vxc_up=None, vxc_dn=None, accumulate=False, dvo
 
 
 def ks_potential_spin(ctx, rho_up, rho_dn, h, vext=None, free=False, pot_up=None, pot_dn=None, energy=True,
-                      bc=None):
+                      bc=None, rhocore=None):
     """The two Kohn-Sham potentials (nspin = 2) on a periodic grid, or with
     free boundary conditions when free (bc, one of BC_CODES, overrides free):
     returns (pot_up, pot_dn, energies), energies a (3,) device tensor (eh,
@@ -257,7 +259,7 @@ def ks_potential_spin(ctx, rho_up, rho_dn, h, vext=None, free=False, pot_up=None
         raise WvlhError("rho_up, rho_dn: (z, y, x) grids of one shape")
     pot_up = torch.empty_like(rho_up) if pot_up is None else pot_up
     pot_dn = torch.empty_like(rho_up) if pot_dn is None else pot_dn
-    for name, t in (("pot_up", pot_up), ("pot_dn", pot_dn), ("vext", vext)):
+    for name, t in (("pot_up", pot_up), ("pot_dn", pot_dn), ("vext", vext), ("rhocore", rhocore)):
         if t is not None and (t.shape != rho_up.shape or t.dtype != torch.float64 or not t.is_contiguous()):
             raise WvlhError("%s: a tensor like rho" % name)
     n = (C.c_int * 3)(rho_up.shape[2], rho_up.shape[1], rho_up.shape[0])
@@ -266,6 +268,7 @@ def ks_potential_spin(ctx, rho_up, rho_dn, h, vext=None, free=False, pot_up=None
     code = BC_CODES[bc] if bc is not None else (1 if free else 0)
     check(lib().wvlh_ks_potential_spin(ctx.h, code, n, hh, C.c_void_p(rho_up.data_ptr()),
                                        C.c_void_p(rho_dn.data_ptr()),
+                                       C.c_void_p(rhocore.data_ptr()) if rhocore is not None else None,
                                        C.c_void_p(vext.data_ptr()) if vext is not None else None,
                                        C.c_void_p(pot_up.data_ptr()), C.c_void_p(pot_dn.data_ptr()),
                                        C.c_void_p(en.data_ptr()) if energy else None), "wvlh_ks_potential_spin")

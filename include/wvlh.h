@@ -452,18 +452,22 @@ int wvlh_xc_lsda(wvlh_ctx *ctx, int64_t npts, const double *rho_up, const double
  * boundary conditions, bc = 0 periodic (offset 0), 1 free, 2 surface, 3 wire:
  * pot = (V_H[rho] + vext) + V_xc[rho], V_H as wvlh_psolver_periodic / _free /
  * _surface / _wire; arguments, aliasing rules and energies as
- * wvlh_ks_potential_periodic. */
+ * wvlh_ks_potential_periodic.  rhocore (DEVICE, or NULL): a core density for
+ * the nonlinear core correction, added to rho for V_xc and E_xc only, with
+ * evxc counting the valence density alone (XC_potential with rhocore,
+ * xcPSolver/xcenergy.f90:720-725, substract_from_vexcu :850-882). */
 int wvlh_ks_potential_bc(wvlh_ctx *ctx, int bc, const int n[3], const double h[3], const double *rho,
-                         const double *vext, double *pot, double *energies);
+                         const double *rhocore, const double *vext, double *pot, double *energies);
 /* The Kohn-Sham potentials of updatePotential with nspin = 2
  * (rhopotential.f90:87-120): V_H of the total density (free_bc: the
  * boundary-condition code of wvlh_ks_potential_bc; 0 periodic, 1 free,
  * 2 surface, 3 wire), pot_sigma = (V_H + vext) + V_xc,sigma;
- * energies as wvlh_ks_potential_periodic (evxc summed over both spins).
+ * energies as wvlh_ks_potential_periodic (evxc summed over both spins);
+ * rhocore as wvlh_ks_potential_bc, half of it on each spin.
  * pot_up and pot_dn are distinct and alias no input. */
 int wvlh_ks_potential_spin(wvlh_ctx *ctx, int free_bc, const int n[3], const double h[3], const double *rho_up,
-                           const double *rho_dn, const double *vext, double *pot_up, double *pot_dn,
-                           double *energies);
+                           const double *rho_dn, const double *rhocore, const double *vext, double *pot_up,
+                           double *pot_dn, double *energies);
 /* FP64, one kernel per 1D pass (the OpenCL backend's structure) */
 int wvlh_locham_plain_batched(wvlh_batch *batch, const double *psi, const double *pot, double *hpsi,
                               double *ekin, double *epot);

@@ -957,7 +957,7 @@ def xc_lsda(rho_up, rho_dn):
     return eps, vp - (zet - 1.0) * dedz, vp - (zet + 1.0) * dedz
 
 
-def ks_potential_spin(rho_up, rho_dn, h, vext=None, free=False):
+def ks_potential_spin(rho_up, rho_dn, h, vext=None, free=False, rhocore=None):
     """updatePotential for nspin = 2 (bigdft/src/modules/rhopotential.f90:
     87-120): V_H of the total density (XC_potential leaves the total in the
     first half, xc_energy_new :902-908), pot_sigma = (V_H + V_ext) + V_xc,sigma.
@@ -966,11 +966,12 @@ def ks_potential_spin(rho_up, rho_dn, h, vext=None, free=False):
     dn = np.asarray(rho_dn, np.float64)
     tot = up + dn
     vh, eh = _hartree_bc(tot, h, free)
-    eps, vu, vd = xc_lsda(up, dn)
+    hc = 0.0 if rhocore is None else 0.5 * np.asarray(rhocore, np.float64)   # half the core on each spin
+    eps, vu, vd = xc_lsda(up + hc, dn + hc)
     base = vh if vext is None else vh + np.asarray(vext, np.float64)
     dvol = h[0] * h[1] * h[2]
     return (base + vu, base + vd,
-            (eh, float((eps * tot).sum()) * dvol, float((vu * up + vd * dn).sum()) * dvol))
+            (eh, float((eps * ((up + hc) + (dn + hc))).sum()) * dvol, float((vu * up + vd * dn).sum()) * dvol))
 
 
 def _hartree_bc(rho, h, bc):
@@ -986,7 +987,7 @@ def ks_potential_free(rho, h, vext=None):
     return ks_potential_periodic(rho, h, vext, free=True)
 
 
-def ks_potential_periodic(rho, h, vext=None, free=False):
+def ks_potential_periodic(rho, h, vext=None, free=False, rhocore=None):
     """The Kohn-Sham potential of a periodic box from the total density, as
     updatePotential (bigdft/src/modules/rhopotential.f90:29-125) builds it for
     nspin = 1 and ixc = 1: XC_potential (xcPSolver/xcenergy.f90:428; energies
@@ -995,10 +996,13 @@ def ks_potential_periodic(rho, h, vext=None, free=False):
     rhov += V_xc.  Returns (pot, (eh, exc, evxc))."""
     rho = np.asarray(rho, np.float64)
     vh, eh = _hartree_bc(rho, h, free)
-    eps, vxc = xc_lda(rho)
+    # a core density joins the valence one for XC only; evxc keeps the valence
+    # part (substract_from_vexcu, xcPSolver/xcenergy.f90:850-882)
+    rx = rho if rhocore is None else rho + np.asarray(rhocore, np.float64)
+    eps, vxc = xc_lda(rx)
     dvol = h[0] * h[1] * h[2]
     pot = (vh if vext is None else vh + np.asarray(vext, np.float64)) + vxc   # H_potential's sum, then the axpy
-    return pot, (eh, float((eps * rho).sum()) * dvol, float((vxc * rho).sum()) * dvol)
+    return pot, (eh, float((eps * rx).sum()) * dvol, float((vxc * rho).sum()) * dvol)
 
 
 # ---------------------------------------------------------------- reference pin

@@ -317,3 +317,27 @@ def test_ks_potential_every_boundary_condition(oracle, torch_cuda, wctx, bc):
     assert np.abs(pd.cpu().numpy() - rd).max() <= 1e-13 * scale
     for a, b in zip(en2.cpu().numpy(), refs):
         assert abs(a - b) <= 1e-12 * abs(b)
+
+
+@pytest.mark.parametrize("bc", ["periodic", "free"])
+def test_ks_potential_with_core_density(oracle, torch_cuda, wctx, bc):
+    from wvlh.psolver import ks_potential, ks_potential_spin
+    torch = torch_cuda
+    n, h = (16, 18, 20), (0.3, 0.32, 0.28)
+    rng = np.random.default_rng(40 + len(bc))
+    up = rng.uniform(1e-4, 0.4, n[::-1])
+    dn = rng.uniform(1e-4, 0.4, n[::-1])
+    core = rng.uniform(0.0, 0.3, n[::-1])
+    tu, td, tc = (torch.tensor(a, device="cuda") for a in (up, dn, core))
+    ref, refs = oracle.ks_potential_periodic(up + dn, h, free=bc, rhocore=core)
+    pot, en = ks_potential(wctx, tu + td, h, bc=bc, rhocore=tc)
+    assert np.abs(pot.cpu().numpy() - ref).max() <= 1e-13 * np.abs(ref).max()
+    for a, b in zip(en.cpu().numpy(), refs):
+        assert abs(a - b) <= 1e-12 * abs(b)
+    ru, rd, refs2 = oracle.ks_potential_spin(up, dn, h, free=bc, rhocore=core)
+    pu, pd, en2 = ks_potential_spin(wctx, tu, td, h, bc=bc, rhocore=tc)
+    scale = max(np.abs(ru).max(), np.abs(rd).max())
+    assert np.abs(pu.cpu().numpy() - ru).max() <= 1e-13 * scale
+    assert np.abs(pd.cpu().numpy() - rd).max() <= 1e-13 * scale
+    for a, b in zip(en2.cpu().numpy(), refs2):
+        assert abs(a - b) <= 1e-12 * abs(b)

@@ -455,3 +455,24 @@ def test_odd_periodic_sizes_host_tables_match_oracle(oracle, n):
     (Nx, Ny), K = wire_kernel_table(n, h)
     ref = oracle.wire_kernel(n, h, Nx, Ny)
     assert np.abs(K - ref).max() <= 1e-12 * np.abs(ref).max()
+
+
+def test_core_density_enters_xc_only(oracle):
+    """The nonlinear core correction: V_xc and E_xc see rho + rho_core, V_H
+    and int rho V_xc the valence density alone (XC_potential with rhocore,
+    substract_from_vexcu)."""
+    rng = np.random.default_rng(6)
+    n, h = (20, 16, 18), (0.3, 0.35, 0.32)
+    rho = rng.uniform(1e-3, 0.5, n)
+    core = rng.uniform(0.0, 0.3, n)
+    pot, (eh, exc, evxc) = oracle.ks_potential_periodic(rho, h, rhocore=core)
+    vh, eh0 = oracle.psolver_periodic(rho, h)
+    eps, vxc = oracle.xc_lda(rho + core)
+    dv = np.prod(h)
+    assert np.array_equal(pot, vh + vxc) and eh == eh0
+    assert abs(exc - (eps * (rho + core)).sum() * dv) <= 1e-12 * abs(exc)
+    assert abs(evxc - (vxc * rho).sum() * dv) <= 1e-12 * abs(evxc)
+    # spin-unpolarised limit of the spin variant with the core split evenly
+    pu, pd, (eh2, exc2, evxc2) = oracle.ks_potential_spin(rho / 2, rho / 2, h, rhocore=core)
+    assert np.abs(pu - pot).max() <= 1e-13 * np.abs(pot).max() and np.array_equal(pu, pd)
+    assert abs(exc2 - exc) <= 1e-12 * abs(exc) and abs(evxc2 - evxc) <= 1e-12 * abs(evxc)
