@@ -184,3 +184,24 @@ def test_gaussian_kinetic_energy_known_answer(oracle):
     _, _, ekin, _ = oracle.locham(d, (h, h, h), pc, pf, np.zeros(int(np.prod(d.I))))
     norm = pc @ pc + pf @ pf
     assert abs(ekin / norm - 3 / (4 * s * s)) / (3 / (4 * s * s)) < 1e-6
+
+
+def test_isf_weights_match_reference_lazy16():
+    """The order-16 ISF two-scale filter the Poisson kernels use is computed
+    from the 16-point Lagrange formula; it equals the reference's table
+    (psolver/src/lazy_16.inc, ch(-18..18)) to its printed digits."""
+    src = REFERENCE / "psolver" / "src" / "lazy_16.inc"
+    if not src.exists():
+        pytest.skip("reference tree not present")
+    import re
+    import oracle
+    body = re.search(r"dimension\(-m:m\)\s*::\s*ch\s*=\s*\(/(.*?)/\)", src.read_text(), re.S).group(1)
+    vals = [float(v.replace("D", "e").replace("d", "e")) for v in re.findall(r"[-+]?(?:\d+\.\d*|\.\d+|\d+)(?:[dDeE][-+]?\d+)?",
+                                                                            body.replace("&", " "))]
+    assert len(vals) == 37
+    ch = dict(zip(range(-18, 19), vals))
+    w = oracle.isf_weights()
+    assert ch[0] == 1.0
+    for m in range(-18, 19):
+        want = 1.0 if m == 0 else (w[abs(m)] if m % 2 and abs(m) <= 15 else 0.0)
+        assert abs(ch[m] - want) <= 1e-17 + 1e-15 * abs(want)
