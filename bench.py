@@ -35,6 +35,16 @@ sys.path.insert(0, str(ROOT / "bigdft-suite_b200"))
 
 METRIC = "Hψ coarse pts/s FP32-batched vs FP64 plain (≤1e-6 Ha); serve p50/p99 ms"
 UNIT = "coarse pts/s"
+DATA = "synthetic (seeded uniform(-1,1) coefficients normalised per orbital, 4-Gaussian potential)"
+
+
+def workload_config(n, norb, ngpu):
+    """The workload both arms measure (the same dict in both lines)."""
+    return {"workload": "batched periodic locham: %d orbitals on one %d^3 coarse grid (%d^3 ISF), hgrid 0.45, "
+                        "4-Gaussian potential" % (norb, n, 2 * n),
+            "n_coarse": n, "norb": norb, "hgrid": 0.45, "parallelism": "orbital shards x%d" % ngpu,
+            "l2": "inputs larger than L2 (%.0f MB of FP32 psi read + written per step)" %
+                  (norb * 8 * n ** 3 * 4 * 2 / 1e6)}
 
 
 def parse():
@@ -141,12 +151,47 @@ def dist_setup(args):
     return ws, rank, local
 
 
+def host_cpu():
+    """Host CPU model, physical cores and usable hardware threads (from
+    /proc/cpuinfo, as lscpu reports them)."""
+    model, cores = None, set()
+    phys = core = None
+    try:
+        for line in open("/proc/cpuinfo"):
+            k, _, v = line.partition(":")
+            k, v = k.strip(), v.strip()
+            if k == "model name" and model is None:
+                model = v
+            elif k == "physical id":
+                phys = v
+            elif k == "core id":
+                core = v
+            elif not k and phys is not None:
+                cores.add((phys, core))
+                phys = core = None
+        if phys is not None:
+            cores.add((phys, core))
+    except OSError:
+        pass
+    threads = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else (os.cpu_count() or 1)
+    ncores = min(len(cores), threads) if cores else threads
+    return {"model": model, "physical_cores": ncores, "threads": threads}
+
+
+def omp_threads():
+    """OpenMP threads of the CPU legs: one per physical core (set before the
+    oracle's OpenMP runtime starts)."""
+    n = host_cpu()["physical_cores"]
+    os.environ.setdefault("OMP_NUM_THREADS", str(n))
+    return int(os.environ["OMP_NUM_THREADS"])
+
+
 def cpu_oracle_rate(n, budget_s=12.0, max_orb=32, seed=7):
     """Time the CPU oracle (the reference's Fortran chain restated in C, OpenMP
-    on all host threads) on a bounded sample of orbitals of the same workload."""
+    over one thread per physical core) on a bounded sample of orbitals of the
+    same workload."""
     import numpy as np
-    nthreads = os.cpu_count() or 1
-    os.environ["OMP_NUM_THREADS"] = str(nthreads)
+    nthreads = omp_threads()
     import oracle as O
     O.lib()
     from wvlh import workloads as W
@@ -176,20 +221,22 @@ def run_reference(args, ws, rank):
         cpu_oracle_rate(n, budget_s=0.0, max_orb=1)
     t0 = time.perf_counter()
     rates = []
+    cores = 1
     for _ in range(args.steps):
         r, cores, sample = cpu_oracle_rate(n, budget_s=0.0, max_orb=2)
         rates.append(r)
     dt = time.perf_counter() - t0
     value = sum(rates) / len(rates)
+    cpu = host_cpu()
     line = {"metric": METRIC, "value": value, "unit": UNIT, "impl": "reference", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * dt / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-            "data": "synthetic (seeded uniform coefficients, 4-Gaussian potential)",
-            "config": {"workload": "batched periodic locham, %d^3 coarse, %d orbitals (each step: a 2-orbital "
-                                   "sample scaled to coarse pts/s)" % (n, args.norb), "n_coarse": n,
-                       "norb": args.norb, "parallelism": "host OpenMP"},
-            "cpu_baseline": {"value": value, "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
-                             "sample": "2 orbitals of %d^3 per step" % n},
+            "data": DATA, "config": workload_config(n, args.norb, args.gpus),
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
+                             "cpu_model": cpu["model"], "physical_cores": cpu["physical_cores"],
+                             "sample": "each step: 2 orbitals of the %d-orbital %d^3 workload through the oracle "
+                                       "(FP64, OpenMP over %d threads), coarse pts/s of the sample" %
+                                       (args.norb, n, cores)},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -206,6 +253,24 @@ def _timed(torch, fn, reps, stream=None):
     b.record(st)
     torch.cuda.synchronize()
     return a.elapsed_time(b) / reps
+
+
+def oracle_errors(lr_list, psi_rows, pot_rows, hpsi_rows, ekin, epot):
+    """Error of sampled results against the CPU oracle (outside any timed
+    region): Hpsi relative L2 (largest over the sample), largest |dE_kin| and
+    |dE_pot| in Ha."""
+    import numpy as np
+    import oracle as O
+    worst = {"hpsi_rel_l2": 0.0, "ekin_abs_ha": 0.0, "epot_abs_ha": 0.0}
+    for lr, x, v, h, e1, e2 in zip(lr_list, psi_rows, pot_rows, hpsi_rows, ekin, epot):
+        d = O.Desc(lr.n, lr.periodic, lr.keyg_c, lr.keyv_c, lr.keyg_f, lr.keyv_f)
+        hc, hf, rk, rp = O.locham(d, lr.hgrid, x[:lr.nvctr_c], x[lr.nvctr_c:], v)
+        ref = np.concatenate([hc, hf])
+        worst["hpsi_rel_l2"] = max(worst["hpsi_rel_l2"], float(np.linalg.norm(h - ref) / np.linalg.norm(ref)))
+        worst["ekin_abs_ha"] = max(worst["ekin_abs_ha"], abs(float(e1) - rk))
+        worst["epot_abs_ha"] = max(worst["epot_abs_ha"], abs(float(e2) - rp))
+    worst["sample"] = len(psi_rows)
+    return worst
 
 
 def leg_free_regions(torch, ctx, dev, nlr=1024, seed=2):
@@ -237,7 +302,20 @@ def leg_free_regions(torch, ctx, dev, nlr=1024, seed=2):
     ms64 = _timed(torch, lambda: b.locham(psi64, pot64, h64, e[2], e[3]), 3)
     de = max((e[0] - e[2]).abs().max().item(), (e[1] - e[3]).abs().max().item())
     ms_plain = _timed(torch, lambda: b.locham_plain(psi64, pot64, h64, e[2], e[3]), 1)
+    # sampled regions against the oracle, both precisions
+    err = {}
+    sample = [0, nlr - 1]
+    poff = np.concatenate([[0], np.cumsum([lr.nisf for lr in lrs])])
+    rows = [psi64[b.psi_offset(o):b.psi_offset(o) + lrs[o].ncoeff].cpu().numpy() for o in sample]
+    vrows = [pot64[poff[o]:poff[o + 1]].cpu().numpy() for o in sample]
+    for nm, ps, pt, hh, k in (("fp32", psi32, pot32, h32, 0), ("fp64", psi64, pot64, h64, 2)):
+        b.locham(ps, pt, hh, e[k], e[k + 1])
+        torch.cuda.synchronize()
+        hr = [hh[b.psi_offset(o):b.psi_offset(o) + lrs[o].ncoeff].double().cpu().numpy() for o in sample]
+        err[nm] = oracle_errors([lrs[o] for o in sample], rows, vrows, hr, [e[k][o].item() for o in sample],
+                                [e[k + 1][o].item() for o in sample])
     out = {"workload": "%d free-BC regions, coarse 20..40 per dim, fine ellipsoid 0.4, 1 orbital each" % nlr,
+           "err_vs_oracle": err,
            "coarse_cells": int(cells), "fp32_fused": {"value": cells / (ms32 * 1e-3), "ms": ms32},
            "fp64_fused": {"value": cells / (ms64 * 1e-3), "ms": ms64},
            "fp64_plain": {"value": cells / (ms_plain * 1e-3), "ms": ms_plain},
@@ -276,11 +354,27 @@ def leg_precond(torch, ctx, dev, n=40, norb=512, ncong=5, seed=3):
         res[nm] = {"ms": ms, "value": norb * lr.coarse_cells / (ms * 1e-3), "hist": hist.cpu().numpy()}
     h32, h64 = res["fp32"].pop("hist"), res["fp64"].pop("hist")
     rel = np.abs(h32 - h64) / np.abs(h64)
+    # two orbitals through the oracle's CG (x0 = b = r): x relative L2 and the
+    # largest relative error of a squared residual norm, per precision
+    import oracle as O
+    d = O.Desc(lr.n, lr.periodic, lr.keyg_c, lr.keyv_c, lr.keyg_f, lr.keyv_f)
+    hf = [0.5 * h for h in lr.hgrid]
+    err = {"fp32": {"x_rel_l2": 0.0, "residual_norm2_rel": 0.0}, "fp64": {"x_rel_l2": 0.0, "residual_norm2_rel": 0.0}}
+    for o in (0, norb - 1):
+        sl = slice(b.psi_offset(o), b.psi_offset(o) + lr.ncoeff)
+        rr = r64[sl].cpu().numpy()
+        xr, rn = O.precond(d, hf, cprec[o], ncong, rr, rr)
+        for nm, x, hist in (("fp32", x32, h32), ("fp64", x64, h64)):
+            xo = x[sl].double().cpu().numpy()
+            err[nm]["x_rel_l2"] = max(err[nm]["x_rel_l2"], float(np.linalg.norm(xo - xr) / np.linalg.norm(xr)))
+            err[nm]["residual_norm2_rel"] = max(err[nm]["residual_norm2_rel"],
+                                                float(np.max(np.abs(hist[:, o] - rn) / np.abs(rn))))
     out = {"workload": "%d orbitals, %d^3 periodic, %d CG iterations" % (norb, n, ncong),
            "fp32": res["fp32"], "fp64": res["fp64"],
            "residual_norm2_mean_per_iter_fp64": [float(v) for v in h64.mean(axis=1)],
            "residual_norm2_max_rel_err_fp32_vs_fp64": float(rel.max()),
-           "x_rel_l2_fp32_vs_fp64": float((x32.double() - x64).norm() / x64.norm())}
+           "x_rel_l2_fp32_vs_fp64": float((x32.double() - x64).norm() / x64.norm()),
+           "err_vs_oracle": err}
     b.close()
     return out
 
@@ -300,7 +394,26 @@ def leg_density(torch, batch, psi32, psi64, lr, norb, dev):
     ms64 = _timed(torch, lambda: go(psi64, r64), 3)
     cells = norb * lr.coarse_cells
     q32, q64 = r32.sum().item() * vol, r64.sum().item() * vol
+    # a 4-orbital density against the oracle, both precisions
+    import numpy as np
+    import oracle as O
+    from wvlh.batch import Batch
+    d = O.Desc(lr.n, lr.periodic, lr.keyg_c, lr.keyv_c, lr.keyg_f, lr.keyv_f)
+    P64 = psi64.view(norb, -1)[:4]
+    ref = np.zeros(lr.nisf)
+    for o in range(4):
+        x = P64[o].cpu().numpy()
+        ref = O.locden(d, x[:lr.nvctr_c], x[lr.nvctr_c:], 2.0 / vol, ref)
+    b4 = Batch(batch.ctx, [lr], np.zeros(4, np.int32))
+    err = {}
+    for nm, P in (("fp32", psi32.view(norb, -1)[:4]), ("fp64", P64)):
+        r = torch.zeros(lr.nisf, dtype=torch.float64, device=dev)
+        b4.locden(P.reshape(-1), hf[:4], r)
+        torch.cuda.synchronize()
+        err[nm] = {"rho_rel_l2": float(np.linalg.norm(r.cpu().numpy() - ref) / np.linalg.norm(ref)), "sample": 4}
+    b4.close()
     return {"fp32": {"ms": ms32, "value": cells / (ms32 * 1e-3)}, "fp64": {"ms": ms64, "value": cells / (ms64 * 1e-3)},
+            "err_vs_oracle": err,
             "rho_rel_l2_fp32_vs_fp64": ((r32 - r64).norm() / r64.norm()).item(), "charge_fp64": q64,
             "charge_err_fp32": abs(q32 - q64)}
 
@@ -534,6 +647,7 @@ def leg_serve(torch, dev, precision, nreq=300, loads=(0.3, 0.5, 0.7)):
 
 def main():
     args = parse()
+    omp_threads()
     import torch
     ws, rank, local = dist_setup(args)
     if args.impl == "reference":
@@ -582,14 +696,7 @@ def main():
 
     dev = torch.device("cuda", local)
     n, norb = args.n, args.norb
-    lr = W.full_periodic(n, 0.45)
-    rng = np.random.default_rng(1234 + rank)
-    pot64 = torch.tensor(W.gaussian_potential(lr, rng), device=dev)
-    g = torch.Generator(device=dev)
-    g.manual_seed(1000 + rank)
-    psi64 = torch.rand(norb, lr.ncoeff, generator=g, device=dev, dtype=torch.float64) * 2 - 1
-    psi64 /= psi64.norm(dim=1, keepdim=True)
-    psi64 = psi64.reshape(-1).contiguous()
+    lr, psi64, pot64 = W.batched_periodic_device(torch, dev, n=n, norb=norb, seed=1000 + rank, pot_seed=1234 + rank)
     psi32 = psi64.float()
     pot32 = pot64.float()
     ctx = Context(local)
@@ -652,21 +759,31 @@ def main():
         names = ["k1_plane_forward", "k2_zpencil", "k3_plane_backward", "k_reduce_energies"]
         npt = 8 * lr.coarse_cells  # fine points per orbital (96^3)
         B = 4
-        kbytes = [3 * B * npt * norb, 4 * B * npt * norb + B * npt, 4 * B * npt * norb, 0]
+        # kernel I/O (what each kernel reads and writes, intermediates included)
+        kio = [3 * B * npt * norb, 4 * B * npt * norb + B * npt, 4 * B * npt * norb, 0]
         kflops = [128 * npt * norb, 252 * npt * norb, 254 * npt * norb, 0]
         dom = max(range(3), key=lambda i: kt[i])
+        # algorithmic bytes of the path per launch: 8 values in + 8 values out
+        # per coarse cell of each orbital (64 B in FP32) plus the potential once
+        alg = 64 * lr.coarse_cells * norb + 4 * npt
         hbm, hbm_src = peaks()
         tf32 = C.c_double()
         lib().wvlh_measure_fma_peak(32, 20000, C.byref(tf32))
-        ach = kbytes[dom] / (kt[dom] * 1e-3) / 1e9
+        ach = alg / (kt[dom] * 1e-3) / 1e9
         # DRAM traffic of each kernel (dram__bytes_read.sum + dram__bytes_write.sum) from ncu
         # captures of one call over 48 orbitals of this 48^3 FP32 workload, scaled by the orbitals
         # of this launch (the traffic grows in proportion to them); z kernels: both chains
         traffic48 = [452.768000e6, 580.762624e6, 655.957504e6]
         traffic = traffic48[dom] / 48 * norb if (dom < 3 and n == 48) else None
+        step_s = ms / args.steps * 1e-3
         extras["roofline"] = {"bound": "hbm", "achieved": ach, "peak": hbm, "unit": "GB/s", "frac": ach / hbm,
                               "traffic": traffic, "kernel": names[dom], "peak_source": hbm_src,
-                              "algorithmic_bytes_per_launch": kbytes[dom]}
+                              "algorithmic_bytes_per_launch": alg,
+                              "algorithmic_bytes_rule": "64 B per coarse cell of each orbital (FP32 psi in, "
+                                                        "Hpsi out) + the potential once",
+                              "kernel_io_bytes": kio[dom],
+                              "kernel_ms": kt[dom],
+                              "whole_step": {"achieved": alg / step_s / 1e9, "frac": alg / step_s / 1e9 / hbm}}
         fach = kflops[dom] / (kt[dom] * 1e-3) / 1e12
         extras["roofline_fma"] = {"bound": "fp32_fma", "achieved": fach, "peak": tf32.value, "unit": "TFLOP/s",
                                   "frac": fach / tf32.value, "kernel": names[dom],
@@ -710,8 +827,42 @@ def main():
         extras["fp64_plain"] = {"value": pts_step / (ms_plain * 1e-3), "ms_per_step": ms_plain}
         extras["fp64_fused"] = {"value": pts_step / (ms_f64 * 1e-3), "ms_per_step": ms_f64}
         extras["speedup_vs_fp64_plain"] = (pts_step / (ms / args.steps * 1e-3)) / (pts_step / (ms_plain * 1e-3))
+        extras["speedup_fp64_fused_vs_fp64_plain"] = ms_plain / ms_f64
         extras["energy_err_ha"] = {"fp32_vs_fp64_max_per_orbital": de, "plain_vs_fused_fp64": dplain}
+        # sampled orbitals of this step against the CPU oracle (FP64), both precisions
+        sample = [0, norb // 3, norb - 1]
+        P64 = psi64.view(norb, -1)
+        rows = [P64[o].cpu().numpy() for o in sample]
+        vh = pot64.cpu().numpy()
+        err = {}
+        batch.locham(psi64, pot64, h64, ek64, ep64)
+        for nm, H, e1, e2 in (("fp32", hpsi32, ek, ep), ("fp64", h64, ek64, ep64)):
+            torch.cuda.synchronize()
+            Hs = H.view(norb, -1)
+            err[nm] = oracle_errors([lr] * len(sample), rows, [vh] * len(sample),
+                                    [Hs[o].double().cpu().numpy() for o in sample],
+                                    [e1[o].item() for o in sample], [e2[o].item() for o in sample])
+        extras["err_vs_oracle"] = err
         del h64
+
+        # FP64 fused end to end (host buffers, same call as below)
+        hp64 = torch.empty(psi64.numel(), dtype=torch.float64, pin_memory=True)
+        hp64.copy_(psi64.cpu())
+        hv64 = torch.empty(pot64.numel(), dtype=torch.float64, pin_memory=True)
+        hv64.copy_(pot64.cpu())
+        hh64 = torch.empty_like(hp64).pin_memory()
+        hek = torch.empty(norb, dtype=torch.float64).pin_memory()
+        hep = torch.empty(norb, dtype=torch.float64).pin_memory()
+        batch.locham_host(hp64, hv64, hh64, hek, hep, 64)
+        t0 = time.perf_counter()
+        for _ in range(3):
+            batch.locham_host(hp64, hv64, hh64, hek, hep, 64)
+        dt64 = (time.perf_counter() - t0) / 3
+        e2e64 = {"value": pts_step / dt64, "ms_per_step": dt64 * 1e3,
+                 "h2d_bytes_per_step": hp64.numel() * 8 + hv64.numel() * 8,
+                 "d2h_bytes_per_step": hh64.numel() * 8 + 2 * 8 * norb}
+        extras["fp64_fused"]["e2e"] = e2e64
+        del hp64, hv64, hh64
 
         # end to end through the C ABI with pinned host buffers
         hp = torch.empty(psi32.numel(), dtype=torch.float32, pin_memory=True)
@@ -728,7 +879,17 @@ def main():
             batch.locham_host(hp, hv, hh, hek, hep, 32)
         dt = (time.perf_counter() - t0) / reps
         extras["e2e"] = {"value": pts_step / dt, "unit": UNIT, "h2d_bytes_per_step": hp.numel() * 4 + hv.numel() * 4,
-                         "d2h_bytes_per_step": hh.numel() * 4 + 2 * 8 * norb, "ms_per_step": dt * 1e3}
+                         "d2h_bytes_per_step": hh.numel() * 4 + 2 * 8 * norb, "ms_per_step": dt * 1e3,
+                         "fp64_fused": {"value": e2e64["value"], "ms_per_step": e2e64["ms_per_step"]}}
+        # the precision-matched comparators and the oracle errors, also inside
+        # the roofline record (FP64 fused and plain on this workload)
+        extras["roofline"]["same_workload"] = {
+            "fp32_fused_ms": ms / args.steps, "fp64_fused_ms": ms_f64, "fp64_plain_ms": ms_plain,
+            "fp64_fused_value": pts_step / (ms_f64 * 1e-3), "fp64_plain_value": pts_step / (ms_plain * 1e-3),
+            "speedup_fp32_vs_fp64_plain": extras["speedup_vs_fp64_plain"],
+            "speedup_fp64_fused_vs_fp64_plain": ms_plain / ms_f64,
+            "fp64_fused_frac": 2 * alg / (ms_f64 * 1e-3) / 1e9 / hbm,
+            "err_vs_oracle": err}
         # the other rows of the path on this GPU
         extras["density"] = leg_density(torch, batch, psi32, psi64, lr, norb, dev)
         extras["overlap"] = leg_overlap(torch, ctx, psi64, norb)
@@ -744,18 +905,15 @@ def main():
         extras["serve"] = serve
         if ws == 1:
             r, cores, sample = cpu_oracle_rate(n)
-            extras["cpu_baseline"] = {"value": r, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample}
+            cpu = host_cpu()
+            extras["cpu_baseline"] = {"value": r, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample,
+                                      "cpu_model": cpu["model"], "physical_cores": cpu["physical_cores"]}
 
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-                "data": "synthetic (seeded uniform(-1,1) coefficients normalised per orbital, 4-Gaussian potential)",
-                "config": {"workload": "batched periodic locham: %d orbitals on one %d^3 coarse grid (%d^3 ISF), "
-                                       "FP32 convolutions + FP64 energies" % (norb, n, 2 * n),
-                           "n_coarse": n, "norb": norb, "hgrid": 0.45, "parallelism": "orbital shards x%d" % ws,
-                           "l2": "inputs larger than L2 (%.0f MB of psi read + written per step)" %
-                                 (psi32.numel() * 8 / 1e6)},
+                "data": DATA, "config": workload_config(n, norb, ws),
                 "gpu_launches": launches, "clocks": clocks}
         line.update(extras)
         print(json.dumps(line), flush=True)

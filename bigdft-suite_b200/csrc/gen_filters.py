@@ -22,7 +22,7 @@ the reference sources instead of being retyped:
   ``w1``; K0(r) otherwise: ``p2``, ``w2``; the first 144 of 150 are used):
   ``psolver/src/gaussfit_wires.inc``.
 
-Run ``python gen_filters.py /root/reference`` to rewrite the header; the
+Run ``python gen_filters.py <reference source tree>`` to rewrite the header; the
 generated header is committed so that the build never needs the reference.
 """
 import re
@@ -145,7 +145,9 @@ def render(f):
 
 
 if __name__ == "__main__":
-    ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    if len(sys.argv) < 2:
+        sys.exit("usage: python gen_filters.py <reference source tree>")
+    ref = sys.argv[1]
     out = Path(__file__).with_name("wvl_filters.h")
     out.write_text(render(parse(ref)))
     print("wrote", out)

@@ -138,18 +138,15 @@ extern "C" int wvlh_ctx_synchronize(wvlh_ctx *ctx)
 static int decode_keys(const int *N, int nseg, const int32_t *keyg, const int32_t *keyv, std::vector<int4> &seg,
                        std::vector<int> &plane, int &nvctr)
 {
-    const long long n12 = (long long)N[0] * N[1], ntot = n12 * N[2];
+    const long long n12 = (long long)N[0] * N[1];
     if (nseg > 0 && (!keyg || !keyv)) return WVLH_ERR_ARG;
+    if (check_keys(N, nseg, keyg, keyv, nullptr)) return WVLH_ERR_KEYS;
     seg.resize(nseg);
     plane.assign(N[2] + 1, nseg);
-    long long prev_end = 0;
     long long cum = 0;
     int cur_plane = 0;
     for (int s = 0; s < nseg; ++s) {
         const long long j0 = keyg[2 * s], j1 = keyg[2 * s + 1];
-        if (j0 < 1 || j1 < j0 || j1 > ntot || j0 <= prev_end) return WVLH_ERR_KEYS;
-        if ((j0 - 1) / N[0] != (j1 - 1) / N[0]) return WVLH_ERR_KEYS;  // segments stay on one x-line
-        if ((long long)keyv[s] != cum + 1) return WVLH_ERR_KEYS;
         long long ii = j0 - 1;
         const int i3 = (int)(ii / n12);
         ii -= (long long)i3 * n12;
@@ -159,7 +156,6 @@ static int decode_keys(const int *N, int nseg, const int32_t *keyg, const int32_
         seg[s] = make_int4(i0, i2, len, (int)cum);
         while (cur_plane <= i3) plane[cur_plane++] = s;
         cum += len;
-        prev_end = j1;
     }
     while (cur_plane <= N[2]) plane[cur_plane++] = nseg;
     nvctr = (int)cum;

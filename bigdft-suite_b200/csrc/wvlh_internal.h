@@ -155,4 +155,25 @@ struct Plan {
     std::vector<void *> owned;     // device allocations to free
 };
 
+// Checks the reference's 1-based keys of one region (compression.f90:29-39):
+// keyg = (first, last) linear index of each segment in the N[0] x N[1] x N[2]
+// box, x fastest, strictly increasing, each segment on one x-line; keyv the
+// running 1-based offset of each segment in the compressed vector.  Returns
+// WVLH_OK or WVLH_ERR_KEYS; on success nvctr is the number of values.
+inline int check_keys(const int *N, int nseg, const int32_t *keyg, const int32_t *keyv, long long *nvctr)
+{
+    const long long n12 = (long long)N[0] * N[1], ntot = n12 * N[2];
+    long long prev_end = 0, cum = 0;
+    for (int s = 0; s < nseg; ++s) {
+        const long long j0 = keyg[2 * s], j1 = keyg[2 * s + 1];
+        if (j0 < 1 || j1 < j0 || j1 > ntot || j0 <= prev_end) return 3;          // WVLH_ERR_KEYS
+        if ((j0 - 1) / N[0] != (j1 - 1) / N[0]) return 3;                         // one x-line per segment
+        if ((long long)keyv[s] != cum + 1) return 3;
+        cum += j1 - j0 + 1;
+        prev_end = j1;
+    }
+    if (nvctr) *nvctr = cum;
+    return 0;
+}
+
 }  // namespace wvlh

@@ -2,9 +2,9 @@
 //
 // Some callers cannot call cudaMalloc at all: code running under a memory
 // manager that owns every device allocation (a host program whose allocator
-// hands out one fixed pool, or a runtime that forbids allocation once it has
-// started capturing work), and library layers that must not grow the device
-// footprint behind their host's back.  For them this file gives one entry
+// hands out one fixed pool and fails any allocation made around it), and
+// library layers that must not grow the device footprint behind their host's
+// back.  For them this file gives one entry
 // point that runs the same fused kernels as wvlh_locham_batched, with every
 // table and all of its scratch (the P, Q/Z1 and Z2 planes and the energy
 // partials) carved out of a file-scope static device array of fixed size.
@@ -82,22 +82,6 @@ __global__ void k_work_lists(int G3, int n2, int n2p, int *pre13, int *pre2, int
 
 inline size_t up256(size_t b) { return (b + 255) & ~size_t(255); }
 
-// host-side validation of the reference's keys, without allocating
-int check_keys(const int *N, int nseg, const int32_t *keyg, const int32_t *keyv)
-{
-    const long long n12 = (long long)N[0] * N[1], ntot = n12 * N[2];
-    long long prev = 0, cum = 0;
-    for (int s = 0; s < nseg; ++s) {
-        const long long j0 = keyg[2 * s], j1 = keyg[2 * s + 1];
-        if (j0 < 1 || j1 < j0 || j1 > ntot || j0 <= prev) return WVLH_ERR_KEYS;
-        if ((j0 - 1) / N[0] != (j1 - 1) / N[0]) return WVLH_ERR_KEYS;
-        if ((long long)keyv[s] != cum + 1) return WVLH_ERR_KEYS;
-        cum += j1 - j0 + 1;
-        prev = j1;
-    }
-    return WVLH_OK;
-}
-
 }  // namespace
 
 extern "C" size_t wvlh_noalloc_capacity(void) { return kNoAllocBytes; }
@@ -121,8 +105,10 @@ extern "C" int wvlh_locham_noalloc(int precision, const int n[3], const int peri
             return WVLH_ERR_ARG;
         }
     }
-    int rc = check_keys(N, nseg_c, keyg_c, keyv_c);
-    if (!rc) rc = check_keys(N, nseg_f, keyg_f, keyv_f);
+    // host-side validation of the keys (the same check as every other entry point)
+    long long nvc = 0, nvf = 0;
+    int rc = check_keys(N, nseg_c, keyg_c, keyv_c, &nvc);
+    if (!rc) rc = check_keys(N, nseg_f, keyg_f, keyv_f, &nvf);
     if (rc) {
         set_last_error(rc);
         return rc;
@@ -175,12 +161,17 @@ extern "C" int wvlh_locham_noalloc(int precision, const int n[3], const int peri
         set_last_error(WVLH_ERR_CUDA);
         return WVLH_ERR_CUDA;
     }
-    cudaDeviceGetAttribute(&smax, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    if (cudaDeviceGetAttribute(&smax, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess || smax <= 1024) {
+        set_last_error(WVLH_ERR_CUDA);
+        return WVLH_ERR_CUDA;
+    }
     if ((rows * pitch + planeB) * es > (size_t)smax - 1024 || 2 * zl * TX_ * TY_ * es > (size_t)smax - 1024) {
         set_last_error(WVLH_ERR_TOO_LARGE);
         return WVLH_ERR_TOO_LARGE;
     }
-    // one-time set-up on this device: the device address of the static array
+    // one-time set-up on this device: the device address of the static array,
+    // kept for the life of the process (the library does not support a reset
+    // of the device, which would reload its module, while it is loaded)
     unsigned char *base;
     {
         std::lock_guard<std::mutex> lock(g_setup_mutex);
@@ -203,9 +194,6 @@ extern "C" int wvlh_locham_noalloc(int precision, const int n[3], const int peri
     }
     L.nseg_c = nseg_c;
     L.nseg_f = nseg_f;
-    long long nvc = 0, nvf = 0;
-    for (int s = 0; s < nseg_c; ++s) nvc += keyg_c[2 * s + 1] - keyg_c[2 * s] + 1;
-    for (int s = 0; s < nseg_f; ++s) nvf += keyg_f[2 * s + 1] - keyg_f[2 * s] + 1;
     L.nvctr_c = (int)nvc;
     L.nvctr_f = (int)nvf;
     L.seg_c = (const int4 *)(base + o_sc);

@@ -10,6 +10,9 @@
 
 #include <cmath>
 #include <cstdio>
+#include <ctime>
+#include <algorithm>
+#include <map>
 #include <mutex>
 #include <vector>
 
@@ -17,9 +20,17 @@
 #include "wvlh_common.cuh"
 #include "wvlh_plain.h"
 
+// A cl_mem is device memory (cudaMalloc, host == nullptr) or host memory the
+// caller handed over (host != nullptr: the reference's CL_MEM_USE_HOST_PTR
+// buffers and pinned regions), page-locked so that copies from and to it run
+// as DMA without staging.  Under unified addressing the locked range is
+// addressable from kernels at its host address.  pages: keys of the
+// registered page ranges the handle holds a reference on.
 struct wvlh_mem {
     void *ptr;
     size_t size;
+    void *host = nullptr;
+    std::vector<uintptr_t> pages;
 };
 struct wvlh_ocl_context {
     int device;
@@ -33,6 +44,15 @@ struct wvlh_ocl_queue {
     std::vector<std::pair<double *, int>> pending;  // (host destination, slot) resolved at ocl_finish
     int error;
 };
+
+// page-locked host ranges (see pin_acquire)
+struct PinRange {
+    uintptr_t end;
+    int refs;
+};
+static std::mutex g_pin_mu;
+static std::map<uintptr_t, PinRange> g_pins;
+static std::vector<wvlh_ocl_queue *> g_queues;  // every live queue, for the wait before unlocking
 
 namespace wvlh {
 static int g_last_error = 0;
@@ -106,6 +126,15 @@ extern "C" void ocl_create_context_(bigdft_context *context, const char *platfor
     ocl_create_gpu_context_(context, device_number);
 }
 
+// real-time clock in nanoseconds since the epoch (OpenCL_wrappers.h:305-306),
+// the host's timer (memguess.f90:2164, MPIfake.f90:419)
+extern "C" void nanosec_(unsigned long long *t)
+{
+    timespec ts;
+    clock_gettime(CLOCK_REALTIME, &ts);
+    *t = (unsigned long long)ts.tv_sec * 1000000000ull + (unsigned long long)ts.tv_nsec;
+}
+
 extern "C" void ocl_build_programs_(bigdft_context *context) { (void)context; }
 extern "C" void init_event_list_(bigdft_context *context) { (void)context; }
 extern "C" void print_event_list_(bigdft_context *context) { (void)context; }
@@ -124,6 +153,10 @@ extern "C" void ocl_create_command_queue_id_(bigdft_command_queue *command_queue
     *command_queue = q;
     QCK(q, cudaSetDevice(dev));
     QCK(q, cudaStreamCreateWithFlags(&q->stream, cudaStreamNonBlocking));
+    {
+        std::lock_guard<std::mutex> lk(g_pin_mu);
+        g_queues.push_back(q);
+    }
     QCK(q, cudaMalloc(&q->d_work, sizeof(double) * (kDotParts + 64)));
     QCK(q, cudaMallocHost(&q->h_stage, sizeof(double) * 64));
 }
@@ -154,12 +187,177 @@ extern "C" void ocl_create_read_buffer_and_copy_(bigdft_context *, cl_uint *size
     if ((*b)->ptr && cudaMemcpy((*b)->ptr, host_ptr, *size, cudaMemcpyHostToDevice) != cudaSuccess)
         qerr(nullptr, WVLH_ERR_CUDA, "ocl_create_read_buffer_and_copy");
 }
+// Page-locked host ranges, process-wide (cudaHostRegister is): page-aligned
+// [begin, end) ranges that never overlap, each with the number of live handles
+// whose memory touches it.  A handle takes a reference on every range its
+// memory overlaps, registering the pages no range covers yet, so two handles
+// over neighbouring arrays that share a page never lock it twice.  Releasing a
+// handle drops its references; a range left without references stays locked
+// until the next ocl_finish, which waits for every queue (copies queued before
+// or after the release may still use the pages) and then unlocks it.
+
+static void pin_acquire(wvlh_mem *m)
+{
+    const uintptr_t pg = 4096;
+    const uintptr_t a = (uintptr_t)m->host & ~(pg - 1);
+    const uintptr_t b = ((uintptr_t)m->host + m->size + pg - 1) & ~(pg - 1);
+    std::lock_guard<std::mutex> lk(g_pin_mu);
+    // walk [a, b) in address order: lock each gap no range covers, then
+    // reference every range that overlaps
+    auto it = g_pins.upper_bound(a);
+    if (it != g_pins.begin() && std::prev(it)->second.end > a) --it;
+    uintptr_t x = a;
+    std::vector<std::pair<uintptr_t, uintptr_t>> gaps;
+    for (auto j = it; j != g_pins.end() && j->first < b; ++j) {
+        if (j->first > x) gaps.push_back({x, j->first});
+        x = std::max(x, j->second.end);
+    }
+    if (x < b) gaps.push_back({x, b});
+    for (auto &g : gaps) {
+        const cudaError_t e =
+            cudaHostRegister((void *)g.first, g.second - g.first, cudaHostRegisterMapped | cudaHostRegisterPortable);
+        if (e == cudaSuccess) g_pins[g.first] = PinRange{g.second, 0};
+        else cudaGetLastError();  // locked by someone else (e.g. cudaMallocHost) or not lockable: copies stage
+    }
+    it = g_pins.upper_bound(a);
+    if (it != g_pins.begin() && std::prev(it)->second.end > a) --it;
+    for (; it != g_pins.end() && it->first < b; ++it) {
+        ++it->second.refs;
+        m->pages.push_back(it->first);
+    }
+}
+
+static void pin_release(wvlh_mem *m)
+{
+    std::lock_guard<std::mutex> lk(g_pin_mu);
+    for (uintptr_t k : m->pages) {
+        auto it = g_pins.find(k);
+        if (it != g_pins.end()) --it->second.refs;
+    }
+    m->pages.clear();
+}
+
+// unlock the ranges no handle references, after every queue has drained
+static void pin_reap()
+{
+    std::unique_lock<std::mutex> lk(g_pin_mu);
+    bool idle = false;
+    for (auto &e : g_pins) idle |= e.second.refs == 0;
+    if (!idle) return;
+    for (wvlh_ocl_queue *q : g_queues) cudaStreamSynchronize(q->stream);
+    for (auto it = g_pins.begin(); it != g_pins.end();) {
+        if (it->second.refs == 0) {
+            cudaHostUnregister((void *)it->first);
+            it = g_pins.erase(it);
+        } else {
+            ++it;
+        }
+    }
+}
+
 extern "C" void ocl_release_mem_object_(cl_mem *buff_ptr)
 {
     if (!buff_ptr || !*buff_ptr) return;
-    if ((*buff_ptr)->ptr) cudaFree((*buff_ptr)->ptr);
-    delete *buff_ptr;
+    wvlh_mem *m = *buff_ptr;
+    if (!m->host) {
+        if (m->ptr) cudaFree(m->ptr);
+    } else {
+        pin_release(m);
+    }
+    delete m;
     *buff_ptr = nullptr;
+}
+
+// A buffer over caller host memory (CL_MEM_USE_HOST_PTR): the range is
+// page-locked, so queued copies between it and device buffers are DMA
+// transfers, and kernels may read it at its (unified) address.
+static void create_host_buffer(bigdft_context *context, cl_uint *size, void *host_ptr, cl_mem *buff_ptr)
+{
+    (void)context;
+    wvlh_mem *m = new wvlh_mem();
+    m->size = *size;
+    m->host = host_ptr;
+    m->ptr = host_ptr;
+    *buff_ptr = m;
+    if (host_ptr && m->size) pin_acquire(m);
+}
+extern "C" void ocl_create_read_buffer_host_(bigdft_context *context, cl_uint *size, void *host_ptr, cl_mem *b)
+{
+    create_host_buffer(context, size, host_ptr, b);
+}
+extern "C" void ocl_create_write_buffer_host_(bigdft_context *context, cl_uint *size, void *host_ptr, cl_mem *b)
+{
+    create_host_buffer(context, size, host_ptr, b);
+}
+extern "C" void ocl_create_read_write_buffer_host_(bigdft_context *context, cl_uint *size, void *host_ptr,
+                                                   cl_mem *b)
+{
+    create_host_buffer(context, size, host_ptr, b);
+}
+
+// Mapping a buffer makes its contents visible to the host once the commands
+// queued before it are done.  A host buffer is the host memory itself, so a
+// map orders nothing beyond the queue: the blocking forms wait for the queue,
+// the asynchronous ones are queue-ordered no-ops, as is unmapping.
+static void map_buffer(bigdft_command_queue *command_queue, bool blocking)
+{
+    bigdft_command_queue q = command_queue ? *command_queue : nullptr;
+    if (q && blocking) QCK(q, cudaStreamSynchronize(q->stream));
+}
+extern "C" void ocl_map_read_buffer_(bigdft_command_queue *q, cl_mem *, cl_uint *, cl_uint *) { map_buffer(q, true); }
+extern "C" void ocl_map_write_buffer_(bigdft_command_queue *q, cl_mem *, cl_uint *, cl_uint *) { map_buffer(q, true); }
+extern "C" void ocl_map_read_write_buffer_(bigdft_command_queue *q, cl_mem *, cl_uint *, cl_uint *)
+{
+    map_buffer(q, true);
+}
+extern "C" void ocl_map_read_buffer_async_(bigdft_command_queue *q, cl_mem *, cl_uint *, cl_uint *)
+{
+    map_buffer(q, false);
+}
+extern "C" void ocl_map_write_buffer_async_(bigdft_command_queue *q, cl_mem *, cl_uint *, cl_uint *)
+{
+    map_buffer(q, false);
+}
+extern "C" void ocl_map_read_write_buffer_async_(bigdft_command_queue *q, cl_mem *, cl_uint *, cl_uint *)
+{
+    map_buffer(q, false);
+}
+extern "C" void ocl_unmap_mem_object_(bigdft_command_queue *q, cl_mem *, void *) { map_buffer(q, false); }
+
+// pin = a host buffer over the range, then a map (OpenCL_wrappers.c:424-505)
+static void pin_buffer(bigdft_context *context, bigdft_command_queue *command_queue, cl_uint *size, void *host_ptr,
+                       cl_mem *buff_ptr, bool blocking)
+{
+    create_host_buffer(context, size, host_ptr, buff_ptr);
+    map_buffer(command_queue, blocking);
+}
+extern "C" void ocl_pin_read_write_buffer_(bigdft_context *c, bigdft_command_queue *q, cl_uint *size, void *h,
+                                           cl_mem *b)
+{
+    pin_buffer(c, q, size, h, b, true);
+}
+extern "C" void ocl_pin_write_buffer_(bigdft_context *c, bigdft_command_queue *q, cl_uint *size, void *h, cl_mem *b)
+{
+    pin_buffer(c, q, size, h, b, true);
+}
+extern "C" void ocl_pin_read_buffer_(bigdft_context *c, bigdft_command_queue *q, cl_uint *size, void *h, cl_mem *b)
+{
+    pin_buffer(c, q, size, h, b, true);
+}
+extern "C" void ocl_pin_read_write_buffer_async_(bigdft_context *c, bigdft_command_queue *q, cl_uint *size, void *h,
+                                                 cl_mem *b)
+{
+    pin_buffer(c, q, size, h, b, false);
+}
+extern "C" void ocl_pin_write_buffer_async_(bigdft_context *c, bigdft_command_queue *q, cl_uint *size, void *h,
+                                            cl_mem *b)
+{
+    pin_buffer(c, q, size, h, b, false);
+}
+extern "C" void ocl_pin_read_buffer_async_(bigdft_context *c, bigdft_command_queue *q, cl_uint *size, void *h,
+                                           cl_mem *b)
+{
+    pin_buffer(c, q, size, h, b, false);
 }
 
 static void resolve_pending(bigdft_command_queue q)
@@ -174,6 +372,7 @@ extern "C" void ocl_finish_(bigdft_command_queue *command_queue)
     bigdft_command_queue q = *command_queue;
     QCK(q, cudaStreamSynchronize(q->stream));
     resolve_pending(q);
+    pin_reap();
 }
 extern "C" void ocl_enqueue_barrier_(bigdft_command_queue *command_queue) { (void)command_queue; }
 
@@ -181,20 +380,20 @@ extern "C" void ocl_enqueue_write_buffer_(bigdft_command_queue *command_queue, c
                                           const void *host_ptr)
 {
     bigdft_command_queue q = *command_queue;
-    QCK(q, cudaMemcpyAsync((*buffer)->ptr, host_ptr, *size, cudaMemcpyHostToDevice, q->stream));
+    QCK(q, cudaMemcpyAsync((*buffer)->ptr, host_ptr, *size, cudaMemcpyDefault, q->stream));
     QCK(q, cudaStreamSynchronize(q->stream));
 }
 extern "C" void ocl_enqueue_write_buffer_async_(bigdft_command_queue *command_queue, cl_mem *buffer, cl_uint *size,
                                                 const void *host_ptr)
 {
     bigdft_command_queue q = *command_queue;
-    QCK(q, cudaMemcpyAsync((*buffer)->ptr, host_ptr, *size, cudaMemcpyHostToDevice, q->stream));
+    QCK(q, cudaMemcpyAsync((*buffer)->ptr, host_ptr, *size, cudaMemcpyDefault, q->stream));
 }
 extern "C" void ocl_enqueue_read_buffer_(bigdft_command_queue *command_queue, cl_mem *buffer, cl_uint *size,
                                          void *host_ptr)
 {
     bigdft_command_queue q = *command_queue;
-    QCK(q, cudaMemcpyAsync(host_ptr, (*buffer)->ptr, *size, cudaMemcpyDeviceToHost, q->stream));
+    QCK(q, cudaMemcpyAsync(host_ptr, (*buffer)->ptr, *size, cudaMemcpyDefault, q->stream));
     QCK(q, cudaStreamSynchronize(q->stream));
     resolve_pending(q);
 }
@@ -202,7 +401,7 @@ extern "C" void ocl_enqueue_read_buffer_async_(bigdft_command_queue *command_que
                                                void *host_ptr)
 {
     bigdft_command_queue q = *command_queue;
-    QCK(q, cudaMemcpyAsync(host_ptr, (*buffer)->ptr, *size, cudaMemcpyDeviceToHost, q->stream));
+    QCK(q, cudaMemcpyAsync(host_ptr, (*buffer)->ptr, *size, cudaMemcpyDefault, q->stream));
 }
 
 extern "C" void ocl_clean_command_queue_(bigdft_command_queue *command_queue)
@@ -211,6 +410,10 @@ extern "C" void ocl_clean_command_queue_(bigdft_command_queue *command_queue)
     if (!q) return;
     cudaStreamSynchronize(q->stream);
     resolve_pending(q);
+    {
+        std::lock_guard<std::mutex> lk(g_pin_mu);
+        g_queues.erase(std::remove(g_queues.begin(), g_queues.end(), q), g_queues.end());
+    }
     cudaFree(q->d_work);
     cudaFreeHost(q->h_stage);
     cudaStreamDestroy(q->stream);
@@ -220,6 +423,7 @@ extern "C" void ocl_clean_command_queue_(bigdft_command_queue *command_queue)
 extern "C" void ocl_clean_(bigdft_context *context)
 {
     if (context && *context) {
+        pin_reap();
         delete *context;
         *context = nullptr;
     }

@@ -56,7 +56,12 @@ OCL_SYMBOLS = [
     "ocl_create_read_write_buffer_", "ocl_create_read_buffer_and_copy_", "ocl_release_mem_object_",
     "ocl_enqueue_read_buffer_", "ocl_enqueue_write_buffer_", "ocl_enqueue_read_buffer_async_",
     "ocl_enqueue_write_buffer_async_", "ocl_finish_", "ocl_enqueue_barrier_", "ocl_clean_command_queue_",
-    "ocl_clean_", "init_event_list_", "print_event_list_",
+    "ocl_clean_", "init_event_list_", "print_event_list_", "nanosec_",
+    "ocl_create_read_buffer_host_", "ocl_create_write_buffer_host_", "ocl_create_read_write_buffer_host_",
+    "ocl_map_read_buffer_", "ocl_map_write_buffer_", "ocl_map_read_write_buffer_", "ocl_map_read_buffer_async_",
+    "ocl_map_write_buffer_async_", "ocl_map_read_write_buffer_async_", "ocl_unmap_mem_object_",
+    "ocl_pin_read_write_buffer_", "ocl_pin_write_buffer_", "ocl_pin_read_buffer_",
+    "ocl_pin_read_write_buffer_async_", "ocl_pin_write_buffer_async_", "ocl_pin_read_buffer_async_",
     "uncompress_d_", "compress_d_", "uncompress_scale_d_", "compress_scale_d_", "scale_psi_d_",
     "syn1d_d_", "syngrow1d_d_", "ana1d_d_", "anashrink1d_d_", "magicfilter1d_d_", "magicfiltergrow1d_d_",
     "magicfilter1d_t_d_", "magicfiltershrink1d_d_", "magicfilter1d_pot_d_", "kinetic1d_d_",

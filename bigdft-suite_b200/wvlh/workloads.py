@@ -94,6 +94,30 @@ def batched_periodic(n=48, norb=256, seed=1, hgrid=0.45):
     return lr, psi, pot
 
 
+def single_orbital(n=32, seed=0, hgrid=0.45):
+    """One orbital of uniform(-1, 1) coefficients on a periodic n^3 box with
+    the 4-Gaussian potential (the single-orbital plain FP64 workload)."""
+    rng = np.random.default_rng(seed)
+    lr = full_periodic(n, hgrid)
+    psi = random_psi(lr, 1, rng)[0]
+    pot = gaussian_potential(lr, rng)
+    return lr, psi, pot
+
+
+def batched_periodic_device(torch, device, n=48, norb=256, seed=1000, pot_seed=1234, hgrid=0.45):
+    """The batched workload generated on the device: norb orbitals of
+    uniform(-1, 1) coefficients from a torch generator seeded with `seed`,
+    each normalised, packed back to back (float64, flat), and the 4-Gaussian
+    potential drawn from numpy's generator seeded with `pot_seed`."""
+    lr = full_periodic(n, hgrid)
+    pot = torch.tensor(gaussian_potential(lr, np.random.default_rng(pot_seed)), device=device)
+    g = torch.Generator(device=device)
+    g.manual_seed(seed)
+    psi = torch.rand(norb, lr.ncoeff, generator=g, device=device, dtype=torch.float64) * 2 - 1
+    psi /= psi.norm(dim=1, keepdim=True)
+    return lr, psi.reshape(-1).contiguous(), pot
+
+
 def free_regions(nlr=1024, nmin=20, nmax=40, seed=2, hgrid=0.45):
     """nlr free-BC regions of uneven size, one support function each, one potential each."""
     rng = np.random.default_rng(seed)

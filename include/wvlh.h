@@ -67,6 +67,42 @@ void ocl_create_read_write_buffer_(bigdft_context *context, cl_uint *size, cl_me
 void ocl_create_read_buffer_and_copy_(bigdft_context *context, cl_uint *size, void *host_ptr,
                                       cl_mem *buff_ptr);                               /* :332 */
 void ocl_release_mem_object_(cl_mem *buff_ptr);                                         /* :340 */
+/* Buffers over caller host memory (CL_MEM_USE_HOST_PTR) and pinned regions,
+   OpenCL_wrappers.h:1238-1253 (bodies OpenCL_wrappers.c:345-505): the range is
+   page-locked (cudaHostRegister, mapped) so queued copies to and from it are
+   DMA transfers; releasing the handle unlocks the range once the copies queued
+   before the release are done.  A map makes the host memory current after the
+   commands queued before it (blocking forms wait for the queue; asynchronous
+   forms and unmap are queue-ordered and need no work). */
+void ocl_create_read_buffer_host_(bigdft_context *context, cl_uint *size, void *host_ptr, cl_mem *buff_ptr); /* :1238 */
+void ocl_create_write_buffer_host_(bigdft_context *context, cl_uint *size, void *host_ptr, cl_mem *buff_ptr); /* :1239 */
+void ocl_create_read_write_buffer_host_(bigdft_context *context, cl_uint *size, void *host_ptr,
+                                        cl_mem *buff_ptr);                             /* :1240 */
+void ocl_map_read_buffer_(bigdft_command_queue *command_queue, cl_mem *buff_ptr, cl_uint *offset,
+                          cl_uint *size);                                              /* :1241 */
+void ocl_map_write_buffer_(bigdft_command_queue *command_queue, cl_mem *buff_ptr, cl_uint *offset,
+                           cl_uint *size);                                             /* :1242 */
+void ocl_map_read_write_buffer_(bigdft_command_queue *command_queue, cl_mem *buff_ptr, cl_uint *offset,
+                                cl_uint *size);                                        /* :1243 */
+void ocl_map_read_buffer_async_(bigdft_command_queue *command_queue, cl_mem *buff_ptr, cl_uint *offset,
+                                cl_uint *size);                                        /* :1244 */
+void ocl_map_write_buffer_async_(bigdft_command_queue *command_queue, cl_mem *buff_ptr, cl_uint *offset,
+                                 cl_uint *size);                                       /* :1245 */
+void ocl_map_read_write_buffer_async_(bigdft_command_queue *command_queue, cl_mem *buff_ptr, cl_uint *offset,
+                                      cl_uint *size);                                  /* :1246 */
+void ocl_unmap_mem_object_(bigdft_command_queue *command_queue, cl_mem *buff_ptr, void *host_ptr); /* :1247 */
+void ocl_pin_read_write_buffer_(bigdft_context *context, bigdft_command_queue *command_queue, cl_uint *size,
+                                void *host_ptr, cl_mem *buff_ptr);                     /* :1248 */
+void ocl_pin_write_buffer_(bigdft_context *context, bigdft_command_queue *command_queue, cl_uint *size,
+                           void *host_ptr, cl_mem *buff_ptr);                          /* :1249 */
+void ocl_pin_read_buffer_(bigdft_context *context, bigdft_command_queue *command_queue, cl_uint *size,
+                          void *host_ptr, cl_mem *buff_ptr);                           /* :1250 */
+void ocl_pin_read_write_buffer_async_(bigdft_context *context, bigdft_command_queue *command_queue, cl_uint *size,
+                                      void *host_ptr, cl_mem *buff_ptr);               /* :1251 */
+void ocl_pin_write_buffer_async_(bigdft_context *context, bigdft_command_queue *command_queue, cl_uint *size,
+                                 void *host_ptr, cl_mem *buff_ptr);                    /* :1252 */
+void ocl_pin_read_buffer_async_(bigdft_context *context, bigdft_command_queue *command_queue, cl_uint *size,
+                                void *host_ptr, cl_mem *buff_ptr);                     /* :1253 */
 void ocl_enqueue_read_buffer_(bigdft_command_queue *command_queue, cl_mem *buffer, cl_uint *size,
                               void *host_ptr);                                         /* :347 */
 void ocl_enqueue_write_buffer_(bigdft_command_queue *command_queue, cl_mem *buffer, cl_uint *size,
@@ -79,6 +115,7 @@ void ocl_finish_(bigdft_command_queue *command_queue);                          
 void ocl_enqueue_barrier_(bigdft_command_queue *command_queue);                         /* :377 */
 void ocl_clean_command_queue_(bigdft_command_queue *command_queue);                     /* :379 */
 void ocl_clean_(bigdft_context *context);                                               /* :381 */
+void nanosec_(unsigned long long *t);   /* :306, real-time clock in ns since the epoch */
 void init_event_list_(bigdft_context *context);                                         /* :309 */
 void print_event_list_(bigdft_context *context);                                        /* :311 */
 
@@ -505,8 +542,10 @@ int wvlh_measure_fma_peak(int precision, int iters, double *tflops);
  * HOST arrays, 1-based as in the reference, read by copies queued on `stream`
  * (keep them unchanged until the stream reaches the call).  Boxes whose
  * scratch exceeds the capacity return WVLH_ERR_TOO_LARGE.  The first call on
- * a device looks up the device address of the static array (set-up): make
- * that first call before any stream capture.  Every call uses the same array,
+ * a device looks up the device address of the static array (set-up) and keeps
+ * it for the life of the process, so resetting the device while the library
+ * is loaded is not supported: make that first call before any stream capture.
+ * Every call uses the same array,
  * so calls that overlap on the GPU (other streams, other host threads) race:
  * serialise them. */
 int wvlh_locham_noalloc(int precision, const int n[3], const int periodic[3], const double hgrid[3], int nseg_c,

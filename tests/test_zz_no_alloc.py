@@ -46,7 +46,8 @@ def call_noalloc(torch, lr, psi, pot, prec, stream):
 
 
 @pytest.mark.parametrize("N,per,prec", [((12, 10, 11), (1, 1, 1), 64), ((9, 8, 10), (0, 0, 0), 64),
-                                        ((16, 16, 16), (1, 1, 1), 32)])
+                                        ((16, 16, 16), (1, 1, 1), 32), ((10, 8, 12), (1, 0, 1), 64),
+                                        ((11, 9, 8), (0, 0, 0), 32)])
 def test_noalloc_matches_batched_entry_two_calls(N, per, prec):
     import torch
     if not torch.cuda.is_available():
