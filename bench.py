@@ -186,7 +186,7 @@ def omp_threads():
     return int(os.environ["OMP_NUM_THREADS"])
 
 
-def cpu_oracle_rate(n, budget_s=12.0, max_orb=32, seed=7):
+def cpu_oracle_rate(n, budget_s=12.0, max_orb=512, seed=7):
     """Time the CPU oracle (the reference's Fortran chain restated in C, OpenMP
     over one thread per physical core) on a bounded sample of orbitals of the
     same workload."""

@@ -24,13 +24,12 @@
 // caller handed over (host != nullptr: the reference's CL_MEM_USE_HOST_PTR
 // buffers and pinned regions), page-locked so that copies from and to it run
 // as DMA without staging.  Under unified addressing the locked range is
-// addressable from kernels at its host address.  pages: keys of the
-// registered page ranges the handle holds a reference on.
+// addressable from kernels at its host address.
 struct wvlh_mem {
     void *ptr;
     size_t size;
     void *host = nullptr;
-    std::vector<uintptr_t> pages;
+    uintptr_t pin_lo = 0, pin_hi = 0;  // the page range this handle holds locked (0, 0: none)
 };
 struct wvlh_ocl_context {
     int device;
@@ -189,52 +188,68 @@ extern "C" void ocl_create_read_buffer_and_copy_(bigdft_context *, cl_uint *size
 }
 // Page-locked host ranges, process-wide (cudaHostRegister is): page-aligned
 // [begin, end) ranges that never overlap, each with the number of live handles
-// whose memory touches it.  A handle takes a reference on every range its
-// memory overlaps, registering the pages no range covers yet, so two handles
-// over neighbouring arrays that share a page never lock it twice.  Releasing a
-// handle drops its references; a range left without references stays locked
+// inside it.  A copy must stay inside one registration, so a handle's pages
+// always lie in exactly one range: a request inside a range takes a reference
+// on it, a request that overlaps none is registered as a new range, and a
+// request that straddles ranges (two arrays sharing a page, or one array
+// pinned piece by piece) merges them with it into one range after waiting for
+// every queue, since the old ranges must be unlocked first.  Releasing a
+// handle drops its reference; a range left without references stays locked
 // until the next ocl_finish, which waits for every queue (copies queued before
 // or after the release may still use the pages) and then unlocks it.
+static inline uintptr_t page_down(uintptr_t a) { return a & ~(uintptr_t)4095; }
+static inline uintptr_t page_up(uintptr_t a) { return (a + 4095) & ~(uintptr_t)4095; }
 
 static void pin_acquire(wvlh_mem *m)
 {
-    const uintptr_t pg = 4096;
-    const uintptr_t a = (uintptr_t)m->host & ~(pg - 1);
-    const uintptr_t b = ((uintptr_t)m->host + m->size + pg - 1) & ~(pg - 1);
+    const uintptr_t a = page_down((uintptr_t)m->host), b = page_up((uintptr_t)m->host + m->size);
+    m->pin_lo = a;
+    m->pin_hi = b;
     std::lock_guard<std::mutex> lk(g_pin_mu);
-    // walk [a, b) in address order: lock each gap no range covers, then
-    // reference every range that overlaps
-    auto it = g_pins.upper_bound(a);
-    if (it != g_pins.begin() && std::prev(it)->second.end > a) --it;
-    uintptr_t x = a;
-    std::vector<std::pair<uintptr_t, uintptr_t>> gaps;
-    for (auto j = it; j != g_pins.end() && j->first < b; ++j) {
-        if (j->first > x) gaps.push_back({x, j->first});
-        x = std::max(x, j->second.end);
+    auto first = g_pins.upper_bound(a);
+    if (first != g_pins.begin() && std::prev(first)->second.end > a) --first;
+    auto last = first;
+    int n = 0;
+    while (last != g_pins.end() && last->first < b) {
+        ++last;
+        ++n;
     }
-    if (x < b) gaps.push_back({x, b});
-    for (auto &g : gaps) {
-        const cudaError_t e =
-            cudaHostRegister((void *)g.first, g.second - g.first, cudaHostRegisterMapped | cudaHostRegisterPortable);
-        if (e == cudaSuccess) g_pins[g.first] = PinRange{g.second, 0};
-        else cudaGetLastError();  // locked by someone else (e.g. cudaMallocHost) or not lockable: copies stage
+    if (n == 1 && first->first <= a && first->second.end >= b) {
+        ++first->second.refs;  // inside one locked range
+        return;
     }
-    it = g_pins.upper_bound(a);
-    if (it != g_pins.begin() && std::prev(it)->second.end > a) --it;
-    for (; it != g_pins.end() && it->first < b; ++it) {
-        ++it->second.refs;
-        m->pages.push_back(it->first);
+    uintptr_t lo = a, hi = b;
+    int refs = 0;
+    if (n > 0) {
+        // straddles locked ranges: unlock them once no queue can be using them
+        lo = std::min(lo, first->first);
+        for (auto it = first; it != last; ++it) {
+            hi = std::max(hi, it->second.end);
+            refs += it->second.refs;
+        }
+        for (wvlh_ocl_queue *q : g_queues) cudaStreamSynchronize(q->stream);
+        for (auto it = first; it != last; ++it) cudaHostUnregister((void *)it->first);
+        g_pins.erase(first, last);
+    }
+    const cudaError_t e = cudaHostRegister((void *)lo, hi - lo, cudaHostRegisterMapped | cudaHostRegisterPortable);
+    if (e == cudaSuccess) {
+        g_pins[lo] = PinRange{hi, refs + 1};
+    } else {
+        cudaGetLastError();  // pages locked by someone else (e.g. cudaMallocHost) or not lockable: copies stage
+        m->pin_lo = m->pin_hi = 0;
     }
 }
 
 static void pin_release(wvlh_mem *m)
 {
+    if (m->pin_hi == 0) return;
     std::lock_guard<std::mutex> lk(g_pin_mu);
-    for (uintptr_t k : m->pages) {
-        auto it = g_pins.find(k);
-        if (it != g_pins.end()) --it->second.refs;
+    auto it = g_pins.upper_bound(m->pin_lo);
+    if (it != g_pins.begin()) {
+        --it;
+        if (it->first <= m->pin_lo && it->second.end >= m->pin_hi) --it->second.refs;
     }
-    m->pages.clear();
+    m->pin_lo = m->pin_hi = 0;
 }
 
 // unlock the ranges no handle references, after every queue has drained

@@ -76,8 +76,8 @@ def test_pinned_locham_matches_plain_and_oracle(oracle, torch_cuda):
             L.ocl_pin_read_buffer_async_(C.byref(ctx), C.byref(q), u(8 * n), addr, C.byref(ph))
             L.ocl_enqueue_write_buffer_async_(C.byref(q), C.byref(buf), u(8 * n), addr)
             L.ocl_release_mem_object_(C.byref(ph))
-        L.ocl_fulllocham_generic_k_(C.byref(q), dims, per, hg, kpt, u(lr.nseg_c), u(nc), C.byref(kb[0]), C.byref(kb[1]),
-                                    u(lr.nseg_f), u(nf), C.byref(kb[2]), C.byref(kb[3]), C.byref(psi_c),
+        L.ocl_fulllocham_generic_k_(C.byref(q), dims, per, hg, kpt, u(len(lr.keyv_c)), u(nc), C.byref(kb[0]), C.byref(kb[1]),
+                                    u(len(lr.keyv_f)), u(nf), C.byref(kb[2]), C.byref(kb[3]), C.byref(psi_c),
                                     C.byref(psi_f), C.byref(psi_c), C.byref(psi_f), C.byref(rhopot),
                                     C.byref(work[0]), C.byref(work[1]), C.byref(work[2]), C.byref(work[0]),
                                     C.byref(work[1]), C.byref(work[2]), C.byref(work[3]), C.byref(work[3]),
