@@ -428,8 +428,33 @@ def leg_overlap(torch, ctx, psi64, norb):
     ms_cublas = _timed(torch, lambda: torch.mm(P, P.T), 5)
     ref = torch.mm(P, P.T)
     fl = norb * (norb + 1) * K
-    return {"ms": ms, "tflops": fl / (ms * 1e-3) / 1e12, "cublas_dgemm_ms": ms_cublas,
-            "max_abs_vs_cublas": (S - ref).abs().max().item(), "flops_count": "norb(norb+1)K (SYRK)"}
+    out = {"ms": ms, "tflops": fl / (ms * 1e-3) / 1e12, "cublas_dgemm_ms": ms_cublas,
+           "max_abs_vs_cublas": (S - ref).abs().max().item(), "flops_count": "norb(norb+1)K (SYRK)"}
+    # the psi-sized products of the orthonormalisation on the panel apply,
+    # against the cuBLAS calls they replace: Loewdin / subspace update (dense
+    # M psi, 2 norb^2 K flop), Cholesky (L^-1 psi, triangular: norb^2 K flop;
+    # cuBLAS TRSM with L through torch.linalg.solve_triangular)
+    from wvlh.ortho import panel_apply
+    g = torch.Generator(device=P.device)
+    g.manual_seed(17)
+    Mf = torch.rand(norb, norb, generator=g, dtype=torch.float64, device=P.device) - 0.5
+    L = torch.linalg.cholesky(ref / K + torch.eye(norb, dtype=torch.float64, device=P.device))
+    Linv = torch.linalg.solve_triangular(L, torch.eye(norb, dtype=torch.float64, device=P.device), upper=False)
+    O = torch.empty_like(P)
+    ms_dense = _timed(lambda: panel_apply(ctx, Mf, P, out=O), 3)
+    ms_dense_cublas = _timed(lambda: torch.mm(Mf, P, out=O), 3)
+    err_dense = (panel_apply(ctx, Mf, P, out=O) - torch.mm(Mf, P)).abs().max().item()
+    ms_tri = _timed(lambda: panel_apply(ctx, Linv, P, out=O, lower=True), 3)
+    ms_trsm = _timed(lambda: torch.linalg.solve_triangular(L, P, upper=False), 2)
+    ms_sub = _timed(lambda: panel_apply(ctx, Mf, P, out=O, alpha=-1.0, beta=1.0), 3)
+    del O
+    fd = 2.0 * norb * norb * K
+    out["panel_apply"] = {"workload": "%d x %d FP64 matrix times the %d x %d orbital panel" % (norb, norb, norb, K),
+                          "dense_ms": ms_dense, "dense_tflops": fd / (ms_dense * 1e-3) / 1e12,
+                          "cublas_dgemm_ms": ms_dense_cublas, "max_abs_vs_cublas": err_dense,
+                          "cholesky_trmm_ms": ms_tri, "cublas_trsm_ms": ms_trsm,
+                          "subspace_update_ms": ms_sub}
+    return out
 
 
 def leg_nlpsp(torch, ctx, psi64, lr, norb, natoms=64, seed=21):

@@ -8,6 +8,8 @@
 #include <cstdio>
 #include <cstring>
 #include <map>
+#include <mutex>
+#include <string>
 #include <type_traits>
 #include <utility>
 #include <vector>
@@ -17,6 +19,9 @@
 #include "wvlh_internal.h"
 #include "wvlh_objects.h"
 #include "wvlh_plain.h"
+#include "wvlh_tma.cuh"
+
+#include <cudaTypedefs.h>
 
 namespace wvlh {
 template <class T, class TIO>
@@ -46,6 +51,8 @@ struct wvlh_batch {
     std::vector<wvlh_batch *> chunks;
     std::vector<int> chunk_o0;
 };
+
+static void apply_tuned(Plan &p);
 
 static int fail(int code)
 {
@@ -132,6 +139,39 @@ extern "C" int wvlh_ctx_synchronize(wvlh_ctx *ctx)
     CK(cudaStreamSynchronize(ctx->stream));
     return WVLH_OK;
 }
+
+namespace wvlh {
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no link
+// against the driver library)
+bool encode_tile_map(CUtensorMap *map, const void *base, int elem_bytes, long long W, long long H, long long Z,
+                     long long norb, long long orb_stride_elems)
+{
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    static bool looked = false;
+    if (!looked) {
+        looked = true;
+        void *f = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = (PFN_cuTensorMapEncodeTiled_v12000)f;
+        cudaGetLastError();
+    }
+    if (!fn || Z > 256 || Z < 1 || W < 1 || H < 1 || norb < 1) return false;
+    const long long rowb = W * elem_bytes, planeb = rowb * H, orbb = orb_stride_elems * elem_bytes;
+    // strides and the base address must be multiples of 16 bytes
+    if ((rowb % 16) || (planeb % 16) || (orbb % 16) || ((uintptr_t)base % 16)) return false;
+    const cuuint64_t dim[4] = {(cuuint64_t)W, (cuuint64_t)H, (cuuint64_t)Z, (cuuint64_t)norb};
+    const cuuint64_t stride[3] = {(cuuint64_t)rowb, (cuuint64_t)planeb, (cuuint64_t)orbb};
+    const cuuint32_t box[4] = {(cuuint32_t)TX_, (cuuint32_t)TY_, (cuuint32_t)Z, 1};
+    const cuuint32_t estr[4] = {1, 1, 1, 1};
+    const CUresult r = fn(map, elem_bytes == 4 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 4,
+                          const_cast<void *>(base), dim, stride, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                          CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                          CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS;
+}
+}  // namespace wvlh
 
 // Validate the reference's 1-based keys of one region and decode them into
 // {i0, i2, len, jj0} plus per-plane segment ranges (wavelib/un-compress.f90:896-905).
@@ -353,9 +393,23 @@ static void layout(wvlh_batch *b, const std::vector<int> &orb_lr, const std::vec
     p.all_periodic = true;
     for (int v : p.lr_per) p.all_periodic = p.all_periodic && v == 1;
     p.scratch_elems = (scr + 1) & ~1LL;  // even: the global plane slices after it start on a point pair
+    {
+        // one region for every orbital: regular (x, y, z, orbital) plane tensors
+        bool one = norb > 0;
+        for (int o = 1; o < norb && one; ++o) one = orb_lr[o] == orb_lr[0];
+        if (one) {
+            const LrDev &d = lrd[orb_lr[0]];
+            const long long G3 = 2LL * d.N[2], F1 = fine_len(d.N[0], d.per[0]), F2 = fine_len(d.N[1], d.per[1]),
+                            I1 = isf_len(d.N[0], d.per[0]), I2 = isf_len(d.N[1], d.per[1]);
+            p.orb_scratch = 2 * G3 * F2 * F1 + G3 * I2 * I1;
+            const long long dims[5] = {G3, F1, F2, I1, I2};
+            for (int k = 0; k < 5; ++k) p.tile_dims[k] = dims[k];
+        }
+    }
     p.part_stride = stride;
     p.plane_threads[0] = choose_plane_threads(shapes32, true);
     p.plane_threads[1] = choose_plane_threads(shapes64, false);
+    apply_tuned(p);   // a measured choice for this shape, when wvlh_batch_autotune made one
     p.plane_elems = (long long)planeA;
     p.planeB_elems = (long long)planeB;
     p.smem13[0] = (planeA + planeB) * sizeof(float);
@@ -720,6 +774,104 @@ extern "C" int wvlh_subspace_matrix(wvlh_ctx *c, int precision, int norb, int64_
 {
     if (!hpsi) return fail(WVLH_ERR_ARG);
     return overlap_entry(c, precision, norb, K, ld, psi, hpsi, L);
+}
+
+namespace wvlh {
+cudaError_t launch_panel_apply(int norb, long long K, long long ld, const double *M, int lower, double alpha,
+                               const double *psi, double beta, double *C, cudaStream_t st);
+}  // namespace wvlh
+
+extern "C" int wvlh_panel_apply(wvlh_ctx *c, int norb, int64_t K, int64_t ld, const double *M, int lower,
+                                double alpha, const double *psi, double beta, double *out)
+{
+    if (!c || !M || !psi || !out || norb <= 0 || K <= 0 || ld < K || psi == out) return fail(WVLH_ERR_ARG);
+    if (((uintptr_t)psi % 8) || ((uintptr_t)out % 8) || ((uintptr_t)M % 8)) return fail(WVLH_ERR_ARG);
+    CK(cudaSetDevice(c->device));
+    CK(launch_panel_apply(norb, K, ld, M, lower, alpha, psi, beta, out, c->stream));
+    return WVLH_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Measured choice of the plane kernels' block size.  The analytic model of
+// choose_plane_threads is a starting point; wvlh_batch_autotune times the
+// batch's own local Hamiltonian with every candidate block size and keeps the
+// fastest, both in the batch and in a process-wide table keyed by the batch's
+// shape (precision and every orbital's box), which later batches of the same
+// shape read at creation.
+static std::mutex g_tune_mu;
+static std::map<std::string, int> g_tuned;
+
+static std::string tune_key(const Plan &p, int fp)
+{
+    std::string k = fp ? "64" : "32";
+    for (int o = 0; o < p.norb; ++o) {
+        const int l = p.orb_lr[o];
+        char buf[64];
+        snprintf(buf, sizeof buf, "|%d,%d,%d,%d%d%d", p.lr_N[3 * l], p.lr_N[3 * l + 1], p.lr_N[3 * l + 2],
+                 p.lr_per[3 * l], p.lr_per[3 * l + 1], p.lr_per[3 * l + 2]);
+        k += buf;
+    }
+    return k;
+}
+
+// the block sizes the plane kernels are compiled for
+static const int kTune32[5] = {1024, 512, kPlaneThreads, 256, 128};
+static const int kTune64[4] = {512, kPlaneThreads, 256, 128};
+
+static void apply_tuned(Plan &p)
+{
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    for (int fp = 0; fp < 2; ++fp) {
+        auto it = g_tuned.find(tune_key(p, fp));
+        if (it != g_tuned.end()) p.plane_threads[fp] = it->second;
+    }
+}
+
+extern "C" int wvlh_batch_autotune(wvlh_batch *b, int precision, const void *psi, const void *pot, void *hpsi,
+                                   double *ekin, double *epot, int reps, int *chosen, int *cand, double *ms,
+                                   int *ncand)
+{
+    if (!b || (precision != 32 && precision != 64) || reps < 1) return fail(WVLH_ERR_ARG);
+    wvlh_ctx *c = b->ctx;
+    CK(cudaSetDevice(c->device));
+    const int fp = precision == 64;
+    const int n = fp ? 4 : 5;
+    const int *cs = fp ? kTune64 : kTune32;
+    cudaEvent_t a, z;
+    CK(cudaEventCreate(&a));
+    CK(cudaEventCreate(&z));
+    int best = b->plan.plane_threads[fp];
+    double best_ms = -1.0;
+    int rc = WVLH_OK;
+    for (int k = 0; k < n && rc == WVLH_OK; ++k) {
+        b->plan.plane_threads[fp] = cs[k];
+        rc = wvlh_locham_batched(b, precision, psi, pot, hpsi, ekin, epot, 0);   // warm-up
+        cudaEventRecord(a, c->stream);
+        for (int r = 0; r < reps && rc == WVLH_OK; ++r) rc = wvlh_locham_batched(b, precision, psi, pot, hpsi, ekin, epot, 0);
+        cudaEventRecord(z, c->stream);
+        if (rc) break;
+        cudaEventSynchronize(z);
+        float t = 0.f;
+        cudaEventElapsedTime(&t, a, z);
+        const double per = t / reps;
+        if (cand) cand[k] = cs[k];
+        if (ms) ms[k] = per;
+        if (best_ms < 0 || per < best_ms) {
+            best_ms = per;
+            best = cs[k];
+        }
+    }
+    cudaEventDestroy(a);
+    cudaEventDestroy(z);
+    b->plan.plane_threads[fp] = best;
+    if (rc) return fail(rc);
+    {
+        std::lock_guard<std::mutex> lk(g_tune_mu);
+        g_tuned[tune_key(b->plan, fp)] = best;
+    }
+    if (chosen) *chosen = best;
+    if (ncand) *ncand = n;
+    return WVLH_OK;
 }
 
 static long long pot_extent(const wvlh_batch *b)

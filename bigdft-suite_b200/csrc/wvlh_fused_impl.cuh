@@ -31,16 +31,24 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <cstring>
 #include <type_traits>
 
 #include "wvlh_common.cuh"
 #include "wvlh_internal.h"
+#include "wvlh_pairs.cuh"
+#include "wvlh_tma.cuh"
 
 namespace wvlh {
 
 constexpr int TX = TX_;
 constexpr int TY = TY_;
 constexpr int TC = TX * TY;
+// alignment of the z kernel's tile buffer (a TMA box destination), and the
+// bytes its launches add to the two tile buffers: the block-sum slots and
+// the TMA barrier
+constexpr int kZAlign = 128;
+constexpr int kZExtra = 32 * 8 + 16;
 
 template <class T> struct Seg;
 template <> struct Seg<float> { static constexpr int v = 8; };
@@ -454,6 +462,37 @@ __global__ void __launch_bounds__(NT, plane_min_blocks(sizeof(T) == 4, PERSIST, 
 }
 
 // ---------------------------------------------------------------------------
+// Passes along the z-pencils of a TC-column tile (columns side by side, z
+// points TC apart): FP32 as line pairs with packed FMAs (wvlh_pairs.cuh),
+// FP64 one line per thread (FP64 has no packed FMA, and its pairs would
+// double the registers a thread holds).
+template <class T>
+__device__ __forceinline__ void z_syn(const T *src, T *dst, int N, int per)
+{
+    if constexpr (sizeof(T) == 4) pass2_syn<kPairSeg>(src, dst, PairGeom{TC / 2, TC, TC}, N, N, per);
+    else pass_syn<T, Seg<T>::v>(src, dst, LineGeom{TC, 1, TC, 1, TC}, N, N, per);
+}
+template <class T>
+__device__ __forceinline__ void z_ana(const T *src, T *dst, int N, int per)
+{
+    if constexpr (sizeof(T) == 4) pass2_ana<kPairSeg>(src, dst, PairGeom{TC / 2, TC, TC}, N, N, per);
+    else pass_ana<T, Seg<T>::v>(src, dst, LineGeom{TC, 1, TC, 1, TC}, N, N, per);
+}
+template <class T, int MODE>
+__device__ __forceinline__ void z_mf(const T *src, T *dst, int Lin, int Lout)
+{
+    if constexpr (sizeof(T) == 4) pass2_mf<kPairSeg, MODE>(src, dst, PairGeom{TC / 2, TC, TC}, Lin, Lout);
+    else pass_mf<T, Seg<T>::v, MODE>(src, dst, LineGeom{TC, 1, TC, 1, TC}, Lin, Lout);
+}
+template <class T>
+__device__ __forceinline__ void z_kin(const T *src, T *dst, int L, int per, double scale, double *e)
+{
+    if constexpr (sizeof(T) == 4)
+        pass2_kin<kPairSeg, false>(src, dst, PairGeom{TC / 2, TC, TC}, L, per, scale, 0.f, e);
+    else pass_kin<T, Seg<T>::v, false>(src, dst, LineGeom{TC, 1, TC, 1, TC}, L, per, scale, T(0), e);
+}
+
+// ---------------------------------------------------------------------------
 // K2: z-pencil tiles, one kernel instance per chain (each half the code of a
 // two-chain kernel, which eases instruction fetch).  CHAIN 0:
 // Z1 = A_z Mt_z (V . M_z S_z Q) in place of Q, E_pot partial.  CHAIN 1:
@@ -463,10 +502,12 @@ __global__ void __launch_bounds__(kZThreads, sizeof(T) == 4 ? 4 : 1) k2_zpencil(
                                                         const int *__restrict__ pre, int norb,
                                                         const TV *__restrict__ pot, T *__restrict__ scratch,
                                                         double *__restrict__ part_pot, double *__restrict__ part_kin,
-                                                        int part_stride)
+                                                        int part_stride, const __grid_constant__ CUtensorMap tm_in,
+                                                        const __grid_constant__ CUtensorMap tm_out, int tma)
 {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    __shared__ double red[32];
+    // dynamic shared memory only (A, B, then the reduction slots and the TMA
+    // barrier), so that the tile buffer starts the block's shared window
+    extern __shared__ __align__(128) unsigned char smem_raw[];
     // item = (orbital, tile): chain 0 tiles the I1 x I2 plane of Q, chain 1
     // the F1 x F2 plane of P, row-major; pre is the chain's own prefix table
     constexpr int chain = CHAIN;
@@ -481,6 +522,10 @@ __global__ void __launch_bounds__(kZThreads, sizeof(T) == 4 ? 4 : 1) k2_zpencil(
     const int zl = max(d.G3, max(d.F3, d.I3));
     T *A = reinterpret_cast<T *>(smem_raw);
     T *B = A + zl * TC;
+    double *red = reinterpret_cast<double *>(B + zl * TC);
+    uint64_t *tma_bar = reinterpret_cast<uint64_t *>(red + 32);
+    // TMA writes the tile only into a kZAlign-aligned buffer
+    tma = tma && !(smem_addr(A) & (kZAlign - 1));
     constexpr int SEG = Seg<T>::v;
     const int W = chain == 0 ? d.I1 : d.F1;   // plane width/height of the data
     const int H = chain == 0 ? d.I2 : d.F2;
@@ -504,21 +549,39 @@ __global__ void __launch_bounds__(kZThreads, sizeof(T) == 4 ? 4 : 1) k2_zpencil(
     const size_t pofs = (size_t)yp * W + xp;
 
     // load the tile: TC columns x G3 z' rows, zero outside the plane
-    if (pairs) {
-        for (int z = zp; z < d.G3; z += ZP) cp_async_pair_z(A + z * TC + pc, pin ? g + (size_t)z * plane + pofs : g, pin);
+    if (tma) {
+        // one box {32, 2, G3} of the batch's (x, y, z, orbital) scratch tensor
+        if (threadIdx.x == 0) mbar_init(tma_bar, 1);
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            mbar_expect_tx(tma_bar, (unsigned)(TC * d.G3 * sizeof(T)));
+            tma_load_4d(A, &tm_in, x0, y0, 0, oi, tma_bar);
+        }
+        const bool ok = mbar_wait_bounded(tma_bar, 0);
+        if (!__syncthreads_and(ok)) {
+            // the copy did not complete in time: poison this tile's energy
+            // slot (the orbital's energies come out NaN) and leave the tile
+            if (threadIdx.x == 0 && part_kin)
+                (chain == 0 ? part_pot : part_kin)[(size_t)oi * part_stride + jj] = __longlong_as_double(-1LL);
+            return;
+        }
     } else {
-        for (int z = zs; z < d.G3; z += ZS)
-            cp_async_elem(A + z * TC + col, inside ? g + (size_t)z * plane + colofs : g, inside);
+        if (pairs) {
+            for (int z = zp; z < d.G3; z += ZP)
+                cp_async_pair_z(A + z * TC + pc, pin ? g + (size_t)z * plane + pofs : g, pin);
+        } else {
+            for (int z = zs; z < d.G3; z += ZS)
+                cp_async_elem(A + z * TC + col, inside ? g + (size_t)z * plane + colofs : g, inside);
+        }
+        cp_async_wait_all();
+        __syncthreads();
     }
-    cp_async_wait_all();
-    __syncthreads();
-    const LineGeom zg{TC, 1, TC, 1, TC};
     double e = 0.0;
-    pass_syn<T, SEG>(A, B, zg, d.N3, d.N3, d.p3);                      // S_z: G3 -> F3
+    z_syn<T>(A, B, d.N3, d.p3);                                   // S_z: G3 -> F3
     __syncthreads();
     if constexpr (chain == 0) {
-        if (d.p3) pass_mf<T, SEG, 0>(B, A, zg, d.F3, d.I3);       // M_z: F3 -> I3
-        else pass_mf<T, SEG, 2>(B, A, zg, d.F3, d.I3);
+        if (d.p3) z_mf<T, 0>(B, A, d.F3, d.I3);                   // M_z: F3 -> I3
+        else z_mf<T, 2>(B, A, d.F3, d.I3);
         __syncthreads();
         // psir <- V psir, epot += V psir^2 (orbitals/potential.f90:1011-1031);
         // per-thread partial sum in T, one FP64 conversion per thread
@@ -568,26 +631,38 @@ __global__ void __launch_bounds__(kZThreads, sizeof(T) == 4 ? 4 : 1) k2_zpencil(
         }
         e += (double)ep;
         __syncthreads();
-        if (d.p3) pass_mf<T, SEG, 1>(A, B, zg, d.I3, d.F3);       // Mt_z: I3 -> F3
-        else pass_mf<T, SEG, 3>(A, B, zg, d.I3, d.F3);
+        if (d.p3) z_mf<T, 1>(A, B, d.I3, d.F3);                   // Mt_z: I3 -> F3
+        else z_mf<T, 3>(A, B, d.I3, d.F3);
         __syncthreads();
-        pass_ana<T, SEG>(B, A, zg, d.N3, d.N3, d.p3);                  // A_z: F3 -> G3
+        z_ana<T>(B, A, d.N3, d.p3);                               // A_z: F3 -> G3
     } else {
         const double scale = -0.5 / ((0.5 * L.hgrid[2]) * (0.5 * L.hgrid[2]));
-        pass_kin<T, SEG, false>(B, A, zg, d.F3, d.p3, scale, T(0), &e);   // K_z X
+        z_kin<T>(B, A, d.F3, d.p3, scale, &e);                    // K_z X
         __syncthreads();
-        pass_ana<T, SEG>(A, B, zg, d.N3, d.N3, d.p3);                  // A_z: F3 -> G3
+        z_ana<T>(A, B, d.N3, d.p3);                               // A_z: F3 -> G3
         __syncthreads();
         T *t = A; A = B; B = t;                                   // result in A
     }
-    __syncthreads();
-    if (pairs) {
-        using V = typename Pair<T>::type;
-        if (pin)
-            for (int z = zp; z < d.G3; z += ZP)
-                *reinterpret_cast<V *>(gz + (size_t)z * plane + pofs) = *reinterpret_cast<const V *>(A + z * TC + pc);
-    } else if (inside) {
-        for (int z = zs; z < d.G3; z += ZS) gz[(size_t)z * plane + colofs] = A[z * TC + col];
+    if (tma) {
+        // the result tile goes back as one box (columns past the plane's
+        // edge are not written)
+        fence_async_smem();
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            tma_store_4d(&tm_out, x0, y0, 0, oi, A);
+            tma_store_drain();
+        }
+    } else {
+        __syncthreads();
+        if (pairs) {
+            using V = typename Pair<T>::type;
+            if (pin)
+                for (int z = zp; z < d.G3; z += ZP)
+                    *reinterpret_cast<V *>(gz + (size_t)z * plane + pofs) =
+                        *reinterpret_cast<const V *>(A + z * TC + pc);
+        } else if (inside) {
+            for (int z = zs; z < d.G3; z += ZS) gz[(size_t)z * plane + colofs] = A[z * TC + col];
+        }
     }
     const double s = block_sum(e, red);
     if (threadIdx.x == 0 && part_kin)
@@ -814,7 +889,6 @@ __global__ void __launch_bounds__(kZThreads) kd_density(const LrDev *__restrict_
     constexpr int SEG = Seg<T>::v;
     const int W = d.I1, H = d.I2;
     const size_t plane = (size_t)W * H;
-    const LineGeom zg{TC, 1, TC, 1, TC};
     // thread t owns tile column c = t % TC at z = t / TC + k ZS
     constexpr int ZS = kZThreads / TC;
     const int col = threadIdx.x % TC, zs = threadIdx.x / TC;
@@ -844,10 +918,10 @@ __global__ void __launch_bounds__(kZThreads) kd_density(const LrDev *__restrict_
         }
         cp_async_wait_all();
         __syncthreads();
-        pass_syn<T, SEG>(A, B, zg, d.N3, d.N3, d.p3);                  // S_z
+        z_syn<T>(A, B, d.N3, d.p3);                               // S_z
         __syncthreads();
-        if (d.p3) pass_mf<T, SEG, 0>(B, A, zg, d.F3, d.I3);       // M_z
-        else pass_mf<T, SEG, 2>(B, A, zg, d.F3, d.I3);
+        if (d.p3) z_mf<T, 0>(B, A, d.F3, d.I3);                   // M_z
+        else z_mf<T, 2>(B, A, d.F3, d.I3);
         __syncthreads();
         const double hf = hfac[orb];
 #pragma unroll
@@ -1055,6 +1129,53 @@ static auto k3_for(const PlaneCfg &pc) -> decltype(&k3_plane_backward<T, TO, ALL
     return k3_plane_backward<T, TO, ALLPER, MODE, false, kPlaneThreads>;
 }
 
+// TMA maps of the z kernel's tiles: when every orbital of the batch lies in
+// one region, the scratch planes of all orbitals form regular 4-D tensors
+// (x, y, z, orbital) for Q (chain 0, read and written in place), P (chain 1
+// input) and Z2 (chain 1 output); otherwise (several regions, or rows whose
+// byte length TMA cannot stride) the tiles move with cp.async.
+struct ZMaps {
+    CUtensorMap q, p, z;
+    int ok = 0;
+};
+template <class T>
+static void zmaps(const Plan &p, T *scratch, ZMaps &m)
+{
+    memset(&m, 0, sizeof(m));
+    if (p.orb_scratch <= 0) return;
+    const int es = (int)sizeof(T);
+    const long long G3 = p.tile_dims[0], F1 = p.tile_dims[1], F2 = p.tile_dims[2], I1 = p.tile_dims[3],
+                    I2 = p.tile_dims[4];
+    const long long sQ0 = G3 * F2 * F1, sZ0 = sQ0 + G3 * I2 * I1;
+    m.ok = encode_tile_map(&m.q, scratch + sQ0, es, I1, I2, G3, p.norb, p.orb_scratch) &&
+           encode_tile_map(&m.p, scratch, es, F1, F2, G3, p.norb, p.orb_scratch) &&
+           encode_tile_map(&m.z, scratch + sZ0, es, F1, F2, G3, p.norb, p.orb_scratch);
+}
+
+// K1 / K3 launch with the plane configuration of the batch
+template <class T, class TI, bool ALLPER, int MODE>
+static cudaError_t run_k1(const Plan &p, const PlaneCfg &pc, const TI *psi, T *scratch, const double *cprec, T *gtmp,
+                          cudaStream_t st)
+{
+    cudaError_t err;
+    auto k = k1_for<T, TI, ALLPER, MODE>(pc);
+    if ((err = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pc.smem))) return err;
+    k<<<pc.grid, pc.threads, pc.smem, st>>>(p.d_lr, p.d_orb, p.d_pre13, p.norb, psi, scratch, cprec, gtmp, pc.gstride);
+    return cudaSuccess;
+}
+
+template <class T, class TO, bool ALLPER, int MODE>
+static cudaError_t run_k3(const Plan &p, const PlaneCfg &pc, const T *scratch, TO *out, double *part_kin,
+                          int part_stride, int accumulate, const double *cprec, T *gtmp, cudaStream_t st)
+{
+    cudaError_t err;
+    auto k = k3_for<T, TO, ALLPER, MODE>(pc);
+    if ((err = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pc.smem))) return err;
+    k<<<pc.grid, pc.threads, pc.smem, st>>>(p.d_lr, p.d_orb, p.d_pre13, p.norb, scratch, out, part_kin, part_stride,
+                                            accumulate, cprec, gtmp, pc.gstride);
+    return cudaSuccess;
+}
+
 #ifdef WVLH_FUSED_COMMON
 long long plane_tmp_elems(const Plan &p, int fp)
 {
@@ -1072,31 +1193,29 @@ static cudaError_t launch_locham_bc(const Plan &p, const TIO *psi, const TIO *po
 {
     const int fp = sizeof(T) == 8 ? 1 : 0;
     const PlaneCfg pc = plane_cfg(p, fp, p.n_work13);
-    const size_t sm13 = pc.smem, sm2 = p.smem2[fp];
+    const size_t sm2 = p.smem2[fp] + kZExtra;
     T *gtmp = pc.global_b ? scratch + p.scratch_elems : nullptr;
     cudaError_t err;
-    auto k1 = k1_for<T, TIO, ALLPER, MODE_LOCHAM>(pc);
     auto k2 = k2_zpencil<T, TIO, ALLPER, 0>;
     auto k2k = k2_zpencil<T, TIO, ALLPER, 1>;
-    auto k3 = k3_for<T, TIO, ALLPER, MODE_LOCHAM>(pc);
-    if ((err = cudaFuncSetAttribute(k1, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm13))) return err;
     if ((err = cudaFuncSetAttribute(k2, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm2))) return err;
     if ((err = cudaFuncSetAttribute(k2k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm2))) return err;
-    if ((err = cudaFuncSetAttribute(k3, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm13))) return err;
     cudaMemsetAsync(part_pot, 0, sizeof(double) * (size_t)p.norb * p.part_stride, st);
     cudaMemsetAsync(part_kin, 0, sizeof(double) * (size_t)p.norb * p.part_stride, st);
+    ZMaps zm;
+    zmaps(p, scratch, zm);
     // optional per-kernel timing: ev[0..4] bracket K1, K2, K3 and the reduction
     if (ev) cudaEventRecord(ev[0], st);
-    k1<<<pc.grid, pc.threads, sm13, st>>>(p.d_lr, p.d_orb, p.d_pre13, p.norb, psi, scratch, nullptr, gtmp,
-                                             pc.gstride);
+    if ((err = run_k1<T, TIO, ALLPER, MODE_LOCHAM>(p, pc, psi, scratch, nullptr, gtmp, st))) return err;
     if (ev) cudaEventRecord(ev[1], st);
     k2<<<p.n_work2, kZThreads, sm2, st>>>(p.d_lr, p.d_orb, p.d_pre2, p.norb, pot, scratch, part_pot, part_kin,
-                                          p.part_stride);
+                                          p.part_stride, zm.q, zm.q, zm.ok);
     k2k<<<p.n_work2p, kZThreads, sm2, st>>>(p.d_lr, p.d_orb, p.d_pre2p, p.norb, pot, scratch, part_pot, part_kin,
-                                            p.part_stride);
+                                            p.part_stride, zm.p, zm.z, zm.ok);
     if (ev) cudaEventRecord(ev[2], st);
-    k3<<<pc.grid, pc.threads, sm13, st>>>(p.d_lr, p.d_orb, p.d_pre13, p.norb, scratch, hpsi, part_kin,
-                                             p.part_stride, accumulate, nullptr, gtmp, pc.gstride);
+    if ((err = run_k3<T, TIO, ALLPER, MODE_LOCHAM>(p, pc, scratch, hpsi, part_kin, p.part_stride, accumulate, nullptr,
+                                                   gtmp, st)))
+        return err;
     if (ev) cudaEventRecord(ev[3], st);
     k_reduce_energies<<<p.norb, 128, 0, st>>>(part_pot, part_kin, p.part_stride, p.norb, ekin, epot);
     if (ev) cudaEventRecord(ev[4], st);
@@ -1132,15 +1251,12 @@ static cudaError_t launch_locden_bc(const Plan &p, const T *psi, const double *h
 {
     const int fp = sizeof(T) == 8 ? 1 : 0;
     const PlaneCfg pc = plane_cfg(p, fp, p.n_work13);
-    const size_t sm13 = pc.smem, sm2 = p.smem2[fp];
+    const size_t sm2 = p.smem2[fp] + kZExtra;
     T *gtmp = pc.global_b ? scratch + p.scratch_elems : nullptr;
     cudaError_t err;
-    auto k1 = k1_for<T, T, ALLPER, MODE_LOCDEN>(pc);
     auto kd = p.den_acc > 32 ? kd_density<T, ALLPER, 48> : kd_density<T, ALLPER, 32>;
-    if ((err = cudaFuncSetAttribute(k1, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm13))) return err;
     if ((err = cudaFuncSetAttribute(kd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm2))) return err;
-    k1<<<pc.grid, pc.threads, sm13, st>>>(p.d_lr, p.d_orb, p.d_pre13, p.norb, psi, scratch, nullptr, gtmp,
-                                             pc.gstride);
+    if ((err = run_k1<T, T, ALLPER, MODE_LOCDEN>(p, pc, psi, scratch, nullptr, gtmp, st))) return err;
     kd<<<p.n_workd, kZThreads, sm2, st>>>(p.d_lr, p.d_orb, p.d_pred, p.nchunk, p.d_chunk_orb_start, p.d_chunk_orbs,
                                           p.d_chunk_part, scratch, hfac, part);
     dim3 g((p.max_group_n + 255) / 256 < 4096 ? (p.max_group_n + 255) / 256 : 4096, p.ngroup);
@@ -1172,21 +1288,17 @@ static cudaError_t launch_prec_apply_bc(const Plan &p, const T *x, T *y, const d
 {
     const int fp = sizeof(T) == 8 ? 1 : 0;
     const PlaneCfg pc = plane_cfg(p, fp, p.n_work13);
-    const size_t sm13 = pc.smem, sm2 = p.smem2[fp];
+    const size_t sm2 = p.smem2[fp] + kZExtra;
     T *gtmp = pc.global_b ? scratch + p.scratch_elems : nullptr;
     cudaError_t err;
-    auto k1 = k1_for<T, T, ALLPER, MODE_PRECOND>(pc);
     auto k2 = k2_zpencil<T, T, ALLPER, 1>;
-    auto k3 = k3_for<T, T, ALLPER, MODE_PRECOND>(pc);
-    if ((err = cudaFuncSetAttribute(k1, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm13))) return err;
     if ((err = cudaFuncSetAttribute(k2, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm2))) return err;
-    if ((err = cudaFuncSetAttribute(k3, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm13))) return err;
-    k1<<<pc.grid, pc.threads, sm13, st>>>(p.d_lr, p.d_orb, p.d_pre13, p.norb, x, scratch, cprec, gtmp,
-                                             pc.gstride);
+    if ((err = run_k1<T, T, ALLPER, MODE_PRECOND>(p, pc, x, scratch, cprec, gtmp, st))) return err;
+    ZMaps zm;
+    zmaps(p, scratch, zm);
     k2<<<p.n_work2p, kZThreads, sm2, st>>>(p.d_lr, p.d_orb, p.d_pre2p, p.norb, (const T *)nullptr, scratch,
-                                           nullptr, nullptr, 0);
-    k3<<<pc.grid, pc.threads, sm13, st>>>(p.d_lr, p.d_orb, p.d_pre13, p.norb, scratch, y, nullptr, 0, 0, cprec,
-                                             gtmp, pc.gstride);
+                                           nullptr, nullptr, 0, zm.p, zm.z, zm.ok);
+    if ((err = run_k3<T, T, ALLPER, MODE_PRECOND>(p, pc, scratch, y, nullptr, 0, 0, cprec, gtmp, st))) return err;
     return cudaGetLastError();
 }
 

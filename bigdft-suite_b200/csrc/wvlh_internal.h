@@ -152,6 +152,11 @@ struct Plan {
     int plane_threads[2] = {kPlaneThreads, kPlaneThreads};   // plane-kernel CTA size (float, double)
     size_t smem2[2] = {0, 0};
     int pitch_max = 0, rows_max = 0, zlen_max = 0;
+    // scratch elements per orbital when every orbital lies in one region (the
+    // planes then form regular (x, y, z, orbital) tensors: TMA tiles), else 0;
+    // tile_dims = {G3, F1, F2, I1, I2} of that region
+    long long orb_scratch = 0;
+    long long tile_dims[5] = {0, 0, 0, 0, 0};
     std::vector<void *> owned;     // device allocations to free
 };
 

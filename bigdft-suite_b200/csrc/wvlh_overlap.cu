@@ -279,6 +279,157 @@ cudaError_t launch_overlap(int norb, long long K, long long ld, const TI *psi, c
 }
 template cudaError_t launch_overlap<double>(int, long long, long long, const double *, const double *, double *,
                                             double *, int, cudaStream_t);
+
+// ---------------------------------------------------------------------------
+// Panel apply C = beta C + alpha M Psi (norb x K, FP64) with a small
+// norb x norb matrix M, the psi-sized step of the orthonormalisation and of
+// the Lagrange-multiplier update:
+//   Cholesky   Psi <- L^-1 Psi     (dpotrf, dtrtri, dtrmm; orthogonality.f90:2351-2366)
+//   Loewdin    Psi <- S^-1/2 Psi   (dsyev, then the product; :2486)
+//   subspace   HPsi <- HPsi - L^T Psi (subspace_update, :254-271)
+// Each CTA forms a 64 (i) x 64 (k) tile of C, contracting over j in slices
+// of 32 staged by a 2-stage cp.async ring (16-byte copies): M[i0.., j0..]
+// as 64 x 32 and Psi[j0.., k0..] as 32 x 64, on the same FP64 tensor-core
+// MMA as the overlap (4 warps, 32 x 32 each).  LOWER: M is lower triangular,
+// so the slices past the tile's last row are skipped (the TRMM of dtrmm).
+// The contraction over j runs in a fixed order: results do not depend on the
+// grid.  C must not alias Psi.
+constexpr int PA_LDB = 64 + 4;   // Psi slice row: 64 k + 4 (conflict-free fragment loads)
+
+// VEC: 16-byte copies (two doubles) when norb, ld and the bases allow,
+// else one double per copy
+template <int VEC>
+__device__ __forceinline__ void pa_stage(double *As, double *Bs, const double *__restrict__ M, int norb,
+                                         const double *__restrict__ psi, long long ld, long long K, int i0, int j0,
+                                         long long k0)
+{
+    constexpr int LD = OvLd<double>::v;
+    constexpr int E = VEC / 8;   // doubles per copy
+    // M slice: 64 rows x 32 columns
+    for (int e = threadIdx.x; e < OV_BM * (OV_BK / E); e += OV_THREADS) {
+        const int r = e / (OV_BK / E), c = (e - r * (OV_BK / E)) * E;
+        const int i = i0 + r, j = j0 + c;
+        const int nvalid = (i < norb) ? (norb - j >= E ? E : (norb - j > 0 ? norb - j : 0)) : 0;
+        const double *src = nvalid ? M + (size_t)i * norb + j : M;
+        ov_cp_async(As + r * LD + c, src, VEC, nvalid * 8);
+    }
+    // Psi slice: 32 rows x 64 columns
+    for (int e = threadIdx.x; e < OV_BK * (OV_BM / E); e += OV_THREADS) {
+        const int r = e / (OV_BM / E), c = (e - r * (OV_BM / E)) * E;
+        const int j = j0 + r;
+        const long long k = k0 + c;
+        long long nv = K - k;
+        nv = nv < 0 ? 0 : (nv > E ? E : nv);
+        if (j >= norb) nv = 0;
+        const double *src = nv ? psi + (size_t)j * ld + k : psi;
+        ov_cp_async(Bs + r * PA_LDB + c, src, VEC, (int)(nv * 8));
+    }
+}
+
+template <bool LOWER, int VEC>
+__global__ void __launch_bounds__(OV_THREADS) k_panel_apply(int norb, long long K, long long ld,
+                                                            const double *__restrict__ M,
+                                                            const double *__restrict__ psi, double alpha,
+                                                            double beta, double *__restrict__ C)
+{
+    extern __shared__ __align__(16) unsigned char pa_smem[];
+    constexpr int LD = OvLd<double>::v;
+    constexpr int ASZ = OV_BM * LD, BSZ = OV_BK * PA_LDB;
+    double *As = reinterpret_cast<double *>(pa_smem);
+    double *Bs = As + OV_STAGES * ASZ;
+    const long long k0 = (long long)blockIdx.x * OV_BM;
+    const int i0 = blockIdx.y * OV_BM;
+    // contraction range: all of j, or j <= the tile's last row (lower M)
+    const int jend = LOWER ? min(norb, i0 + OV_BM) : norb;
+    const int nj = (jend + OV_BK - 1) / OV_BK;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int g = lane >> 2, t = lane & 3;
+    const int wr = (warp >> 1) * 32, wc = (warp & 1) * 32;
+    double acc[2][4][4];
+#pragma unroll
+    for (int a = 0; a < 2; ++a)
+#pragma unroll
+        for (int b = 0; b < 4; ++b)
+#pragma unroll
+            for (int q = 0; q < 4; ++q) acc[a][b][q] = 0.0;
+    if (nj > 0) pa_stage<VEC>(As, Bs, M, norb, psi, ld, K, i0, 0, k0);
+    ov_commit();
+    for (int it = 0; it < nj; ++it) {
+        ov_wait<0>();
+        __syncthreads();   // slice it is visible; the other slot is free
+        if (it + 1 < nj) {
+            const int slot = (it + 1) % OV_STAGES;
+            pa_stage<VEC>(As + slot * ASZ, Bs + slot * BSZ, M, norb, psi, ld, K, i0, (it + 1) * OV_BK, k0);
+        }
+        ov_commit();
+        const int slot = it % OV_STAGES;
+        const double *Ar = As + slot * ASZ;
+        const double *Br = Bs + slot * BSZ;
+#pragma unroll
+        for (int kk = 0; kk < OV_BK; kk += 16) {
+            double fa[2][8], fb[4][4];
+#pragma unroll
+            for (int a = 0; a < 2; ++a)
+#pragma unroll
+                for (int i = 0; i < 8; ++i) fa[a][i] = Ar[(wr + 16 * a + g + 8 * (i & 1)) * LD + kk + t + 4 * (i >> 1)];
+#pragma unroll
+            for (int b = 0; b < 4; ++b)
+#pragma unroll
+                for (int i = 0; i < 4; ++i) fb[b][i] = Br[(kk + t + 4 * i) * PA_LDB + wc + 8 * b + g];
+#pragma unroll
+            for (int a = 0; a < 2; ++a)
+#pragma unroll
+                for (int b = 0; b < 4; ++b) dmma_16x8x16(acc[a][b], fa[a], fb[b]);
+        }
+    }
+    ov_wait<0>();
+    // C rows i, columns k: two neighbouring columns per fragment row
+#pragma unroll
+    for (int a = 0; a < 2; ++a)
+#pragma unroll
+        for (int b = 0; b < 4; ++b)
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const int i = i0 + wr + 16 * a + g + 8 * h;
+                const long long k = k0 + wc + 8 * b + 2 * t;
+                if (i >= norb) continue;
+                double *c = C + (size_t)i * ld + k;
+                const double v0 = alpha * acc[a][b][2 * h], v1 = alpha * acc[a][b][2 * h + 1];
+                if (VEC == 16 && k + 1 < K) {
+                    double2 o = make_double2(v0, v1);
+                    if (beta != 0.0) {
+                        const double2 old = *reinterpret_cast<const double2 *>(c);
+                        o.x = fma(beta, old.x, v0);
+                        o.y = fma(beta, old.y, v1);
+                    }
+                    *reinterpret_cast<double2 *>(c) = o;
+                } else {
+                    if (k < K) c[0] = beta != 0.0 ? fma(beta, c[0], v0) : v0;
+                    if (k + 1 < K) c[1] = beta != 0.0 ? fma(beta, c[1], v1) : v1;
+                }
+            }
+}
+
+size_t panel_apply_smem_bytes() { return sizeof(double) * OV_STAGES * (OV_BM * OvLd<double>::v + OV_BK * PA_LDB); }
+
+// C = beta C + alpha M psi; psi, C rows of K at row stride ld
+cudaError_t launch_panel_apply(int norb, long long K, long long ld, const double *M, int lower, double alpha,
+                               const double *psi, double beta, double *C, cudaStream_t st)
+{
+    const size_t smem = panel_apply_smem_bytes();
+    const dim3 grid((unsigned)((K + OV_BM - 1) / OV_BM), (unsigned)((norb + OV_BM - 1) / OV_BM));
+    auto go = [&](auto k) -> cudaError_t {
+        cudaError_t r;
+        if ((r = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem))) return r;
+        k<<<grid, OV_THREADS, smem, st>>>(norb, K, ld, M, psi, alpha, beta, C);
+        return cudaGetLastError();
+    };
+    // two doubles per copy and store when every row start is on 16 bytes
+    const bool v16 = !(norb % 2) && !(ld % 2) && !((uintptr_t)M % 16) && !((uintptr_t)psi % 16) &&
+                     !((uintptr_t)C % 16);
+    if (v16) return lower ? go(k_panel_apply<true, 16>) : go(k_panel_apply<false, 16>);
+    return lower ? go(k_panel_apply<true, 8>) : go(k_panel_apply<false, 8>);
+}
 template cudaError_t launch_overlap<float>(int, long long, long long, const float *, const float *, double *,
                                            double *, int, cudaStream_t);
 

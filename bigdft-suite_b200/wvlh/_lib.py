@@ -82,7 +82,8 @@ WVLH_SYMBOLS = [
     "wvlh_overlap", "wvlh_region_create", "wvlh_region_destroy", "wvlh_region_psi_size",
     "wvlh_region_grid_size", "wvlh_region_scratch_bytes", "wvlh_batch_create_orbitals", "wvlh_wpdot",
     "wvlh_locham_graph_create", "wvlh_graph_launch", "wvlh_graph_destroy",
-    "wvlh_nlpsp_create", "wvlh_nlpsp_apply", "wvlh_nlpsp_destroy", "wvlh_subspace_matrix",
+    "wvlh_nlpsp_create", "wvlh_nlpsp_apply", "wvlh_nlpsp_destroy", "wvlh_subspace_matrix", "wvlh_panel_apply",
+    "wvlh_batch_autotune",
     "wvlh_psolver_periodic",
     "wvlh_xc_lda",
     "wvlh_ks_potential_periodic",
@@ -155,6 +156,9 @@ def lib():
     L.wvlh_nlpsp_apply.argtypes = [vp, C.c_int, vp, C.c_int64, vp, vp]
     L.wvlh_nlpsp_destroy.argtypes = [vp]
     L.wvlh_subspace_matrix.argtypes = [vp, C.c_int, C.c_int, C.c_int64, C.c_int64, vp, vp, vp]
+    L.wvlh_batch_autotune.argtypes = [vp, C.c_int, vp, vp, vp, vp, vp, C.c_int, C.POINTER(C.c_int),
+                                      C.POINTER(C.c_int), C.POINTER(C.c_double), C.POINTER(C.c_int)]
+    L.wvlh_panel_apply.argtypes = [vp, C.c_int, C.c_int64, C.c_int64, vp, C.c_int, C.c_double, vp, C.c_double, vp]
     L.wvlh_psolver_periodic.argtypes = [vp, C.POINTER(C.c_int), C.POINTER(C.c_double), vp, vp, C.c_double, vp]
     L.wvlh_xc_lda.argtypes = [vp, C.c_int64, vp, vp, C.c_int, C.c_double, vp]
     L.wvlh_ks_potential_periodic.argtypes = [vp, C.POINTER(C.c_int), C.POINTER(C.c_double), vp, vp, vp, vp]

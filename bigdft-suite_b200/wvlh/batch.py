@@ -121,6 +121,26 @@ class Batch:
         check(rc, "wvlh_locham_batched")
         return hpsi, ekin, epot
 
+    def autotune(self, psi, pot, hpsi=None, ekin=None, epot=None, reps=2):
+        """Measure the plane kernels' block sizes on this batch's locham
+        (wvlh_batch_autotune) and keep the fastest; returns (chosen,
+        {block size: ms per call})."""
+        torch = self.ctx.torch
+        prec = {torch.float32: 32, torch.float64: 64}.get(psi.dtype)
+        if prec is None or pot.dtype != psi.dtype:
+            raise WvlhError("psi and pot must both be float32 or float64")
+        if hpsi is None:
+            hpsi = torch.empty_like(psi)
+        if ekin is None:
+            ekin = torch.empty(self.norb, dtype=torch.float64, device=psi.device)
+        if epot is None:
+            epot = torch.empty(self.norb, dtype=torch.float64, device=psi.device)
+        chosen, n = C.c_int(), C.c_int()
+        cand, ms = (C.c_int * 5)(), (C.c_double * 5)()
+        check(lib().wvlh_batch_autotune(self.h, prec, _ptr(psi), _ptr(pot), _ptr(hpsi), _ptr(ekin), _ptr(epot),
+                                        int(reps), C.byref(chosen), cand, ms, C.byref(n)), "wvlh_batch_autotune")
+        return chosen.value, {int(cand[k]): float(ms[k]) for k in range(n.value)}
+
     def locham_graph(self, psi, pot, hpsi, ekin, epot, accumulate=False):
         """Capture locham(psi, pot, hpsi, ekin, epot) into a CUDA graph; replay
         it with .launch() (the tensors must stay alive and in place)."""

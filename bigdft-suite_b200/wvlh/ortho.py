@@ -4,13 +4,14 @@
 (the reference's ``getOverlap``, ``wfn_opt/orthogonality.f90:2624-2697``).
 ``orthonormalize`` then applies either the Cholesky scheme (``cholesky``,
 :2297-2430: S = L L^T, Psi <- L^-1 Psi) or the Loewdin scheme (``loewdin``,
-:2431-2500: Psi <- S^-1/2 Psi), in FP64 on the device; the small dense
-factorisations (norb x norb) use torch.linalg (cuSOLVER).
+:2431-2500: Psi <- S^-1/2 Psi), in FP64 on the device: the psi-sized
+product on the library's tensor-core panel apply (``panel_apply``), the
+small dense factorisations (norb x norb) with torch.linalg (cuSOLVER).
 ``orthoconstraint`` is the gradient step that follows the Hamiltonian
 (:375-625): Lagrange multipliers L = <psi_i|hpsi_j> on the same tensor-core
 kernel, symmetrised and corrected for unequal occupations
 (``lagrange_multiplier``, :293-369), then hpsi <- hpsi - L^T psi
-(``subspace_update``, :254-271; a plain DGEMM).
+(``subspace_update``, :254-271) on the panel apply.
 """
 import ctypes as C
 
@@ -37,18 +38,51 @@ def overlap(ctx, psi, norb=None, K=None, ld=None, S=None):
     return S
 
 
-def orthonormalize(ctx, psi, method="cholesky"):
-    """In place on a (norb, K) float64 device tensor; returns (psi, S)."""
+def panel_apply(ctx, M, psi, out=None, alpha=1.0, beta=0.0, lower=False):
+    """out = beta out + alpha M psi on the FP64 tensor-core kernel
+    (wvlh_panel_apply): M (norb, norb) float64, psi and out (norb, K) float64
+    device tensors with one row stride; out must not alias psi."""
+    torch = ctx.torch
+    norb, K = psi.shape
+    if psi.dtype != torch.float64 or M.dtype != torch.float64 or M.shape != (norb, norb):
+        raise WvlhError("panel_apply: FP64 M (norb, norb) and psi (norb, K)")
+    if psi.stride(1) != 1:
+        raise WvlhError("rows must be contiguous")
+    M = M.contiguous()
+    if out is None:
+        out = torch.empty_like(psi)
+    if out.stride() != psi.stride():
+        raise WvlhError("out and psi must share one layout")
+    check(lib().wvlh_panel_apply(ctx.h, int(norb), int(K), int(psi.stride(0)), C.c_void_p(M.data_ptr()),
+                                 int(bool(lower)), float(alpha), C.c_void_p(psi.data_ptr()), float(beta),
+                                 C.c_void_p(out.data_ptr())), "wvlh_panel_apply")
+    return out
+
+
+def orthonormalize(ctx, psi, method="cholesky", work=None):
+    """In place on a (norb, K) float64 device tensor; returns (psi, S).
+
+    Cholesky (orthogonality.f90:2297-2430): S = L L^T (dpotrf), L^-1
+    (dtrtri) and psi <- L^-1 psi (dtrmm), the last on the library's
+    tensor-core panel apply with the triangle's empty slices skipped.
+    Loewdin (:2431-2500): S = U w U^T (dsyev), psi <- U w^-1/2 U^T psi on the
+    same kernel.  The norb x norb factorisations use torch.linalg (cuSOLVER);
+    work: an optional (norb, K) buffer for the product."""
     torch = ctx.torch
     S = overlap(ctx, psi)
     if method == "cholesky":
         L = torch.linalg.cholesky(S)
-        psi.copy_(torch.linalg.solve_triangular(L, psi, upper=False))
+        eye = torch.eye(L.shape[0], dtype=L.dtype, device=L.device)
+        M = torch.linalg.solve_triangular(L, eye, upper=False)
+        lower = True
     elif method == "loewdin":
         w, U = torch.linalg.eigh(S)
-        psi.copy_((U * w.rsqrt()) @ U.T @ psi)
+        M = (U * w.rsqrt()) @ U.T
+        lower = False
     else:
         raise WvlhError("method must be 'cholesky' or 'loewdin'")
+    out = panel_apply(ctx, M, psi, out=work, lower=lower)
+    psi.copy_(out)
     return psi, S
 
 
@@ -112,5 +146,8 @@ def orthoconstraint(ctx, psi, hpsi, occup=None, symm=True, tr_min=False):
         occup = [2.0] * norb
     L = subspace_matrix(ctx, psi, hpsi)
     trace, asymm, mix = lagrange_multiplier(L, occup, symm=symm, correction=not tr_min)
-    hpsi.sub_(L.T.to(hpsi.dtype) @ psi)
+    if psi.dtype == torch.float64 and hpsi.dtype == torch.float64 and psi.stride() == hpsi.stride():
+        panel_apply(ctx, L.T.contiguous(), psi, out=hpsi, alpha=-1.0, beta=1.0)   # subspace_update
+    else:
+        hpsi.sub_(L.T.to(hpsi.dtype) @ psi)
     return L, trace, asymm, mix

@@ -358,6 +358,17 @@ int wvlh_overlap(wvlh_ctx *ctx, int precision, int norb, int64_t K, int64_t ld, 
  * kernel, every tile of the square, splits summed in a fixed order. */
 int wvlh_subspace_matrix(wvlh_ctx *ctx, int precision, int norb, int64_t K, int64_t ld, const void *psi,
                          const void *hpsi, double *L);
+/* Panel apply out = beta out + alpha M psi (FP64, device): M is norb x norb
+ * row-major (lower != 0: lower triangular, the slices above the diagonal are
+ * skipped), psi and out are norb rows of K values at row stride ld (out
+ * must not alias psi).  The psi-sized
+ * products of the orthonormalisation (wfn_opt/orthogonality.f90): Cholesky
+ * psi <- L^-1 psi (dtrtri then dtrmm, :2351-2366), Loewdin psi <- S^-1/2 psi
+ * (:2486), and the Lagrange step hpsi <- hpsi - L^T psi (subspace_update,
+ * :254-271; M = L^T, alpha = -1, beta = 1), on FP64 tensor cores, the
+ * contraction in a fixed order. */
+int wvlh_panel_apply(wvlh_ctx *ctx, int norb, int64_t K, int64_t ld, const double *M, int lower, double alpha,
+                     const double *psi, double beta, double *out);
 /* Compressed scalar products out[i*nb + j] = <a_i|b_j> (FP64) between na
  * vectors on the keys of region ra (row stride lda) and nb vectors on the
  * keys of region rb (row stride ldb), both regions with the same box (keys
@@ -505,6 +516,17 @@ int wvlh_ks_potential_bc(wvlh_ctx *ctx, int bc, const int n[3], const double h[3
 int wvlh_ks_potential_spin(wvlh_ctx *ctx, int free_bc, const int n[3], const double h[3], const double *rho_up,
                            const double *rho_dn, const double *rhocore, const double *vext, double *pot_up,
                            double *pot_dn, double *energies);
+/* Measured block size of the plane kernels: times reps calls of
+ * wvlh_locham_batched (after one warm-up each) with every block size the
+ * kernels are compiled for (FP32 1024/512/384/256/128, FP64 512/384/256/128),
+ * keeps the fastest in the batch and in a process-wide table keyed by the
+ * batch's shape (precision and every orbital's box), which batches of the
+ * same shape created later start from.  Arguments as wvlh_locham_batched
+ * (hpsi, ekin, epot are overwritten); chosen: the pick; cand/ms (up to 5
+ * entries each, or NULL): the candidates and their ms per call; ncand: how
+ * many were timed. */
+int wvlh_batch_autotune(wvlh_batch *batch, int precision, const void *psi, const void *pot, void *hpsi,
+                        double *ekin, double *epot, int reps, int *chosen, int *cand, double *ms, int *ncand);
 /* FP64, one kernel per 1D pass (the OpenCL backend's structure) */
 int wvlh_locham_plain_batched(wvlh_batch *batch, const double *psi, const double *pot, double *hpsi,
                               double *ekin, double *epot);

@@ -29,6 +29,7 @@ import numpy as np
 HERE = Path(__file__).resolve().parent
 LIB = HERE / "_build" / "liboracle.so"
 REF_MF = HERE / "_ref" / "libref_magicfilter.so"
+REF_CONVIB = HERE / "_ref" / "libref_convib.so"
 
 _lib = None
 
@@ -1014,3 +1015,70 @@ def ref_magicfilter():
     for nm in ("magicfilter1d_naive_", "magicfilter1d_t_naive_", "magicfilter1d_sse_", "magicfilter1d_t_sse_"):
         getattr(L, nm).argtypes = [C.POINTER(C.c_uint), C.POINTER(C.c_uint), f64p, f64p]
     return L
+
+
+def ref_convib():
+    """ctypes handle to the reference's own SSE wavelet-basis kinetic
+    operator (bigdft/src/orbitals/convolut_ib_sse.c), or None."""
+    if not REF_CONVIB.exists():
+        return None
+    return C.CDLL(str(REF_CONVIB))
+
+
+_FINE_X = ("convolut_ib_sse_fx_wss_", "convolut_ib_sse_fx_sws_wws_", "convolut_ib_sse_fx_ssw_wsw_",
+           "convolut_ib_sse_fx_sww_www_")
+_FINE_YZ = ("convolut_ib_sse_fy_sws_", "convolut_ib_sse_fy_wss_wws_", "convolut_ib_sse_fy_ssw_sww_",
+            "convolut_ib_sse_fy_wsw_www_", "convolut_ib_sse_fz_ssw_", "convolut_ib_sse_fz_wss_wsw_",
+            "convolut_ib_sse_fz_sws_sww_", "convolut_ib_sse_fz_wws_www_")
+
+
+def ref_kinetic_sse(n, hgrid, cprecr, x_c, x_f, nfl, nfu, ibc, ibf):
+    """The reference's FP32 SSE kinetic operator (c + T) in the wavelet
+    basis, called as Convolkinetic_SSE does (convolut_ib_optim.f90:868-903):
+    coarse->coarse (convolut_ib_sse_cxyz_) and fine->fine (the _fx/_fy/_fz
+    functions, in that order), filters a, b, c, e (the tables of
+    ConvolkineticT, :962-1046) scaled by -1/(2 h^2) for an isotropic coarse
+    spacing h.  x_c: (n3+1, n2+1, n1+1) float32; x_f: (nfu3-nfl3+1,
+    nfu2-nfl2+1, nfu1-nfl1+1, 7) float32; ibc / ibf: make_bounds triples
+    (ibyz, ibxz, ibxy) as (.., .., 2) int32 arrays.  Returns (y_c, y_f)."""
+    L = ref_convib()
+    n1, n2, n3 = (int(v) for v in n)
+    sc = -0.5 / (hgrid * hgrid)
+    a = np.zeros(29)
+    e = np.zeros(29)
+    cc = np.zeros(29)
+    b = np.zeros(29)
+    for l in range(15):
+        a[14 + l] = a[14 - l] = _filter_table("WVL_KIN")[l]
+        e[14 + l] = e[14 - l] = _filter_table("WVL_KIN_E")[l]
+    kc = _filter_table("WVL_KIN_C")
+    for l in range(-14, 15):
+        cc[l + 14] = kc[l + 14]
+        b[l + 14] = kc[-l + 14]
+    fa, fb, fc, fe = (np.ascontiguousarray(v * sc, np.float32) for v in (a, b, cc, e))
+    x_c = np.ascontiguousarray(x_c, np.float32)
+    x_f = np.ascontiguousarray(x_f, np.float32)
+    y_c = np.zeros_like(x_c)
+    y_f = np.zeros_like(x_f)
+    ii = lambda v: C.byref(C.c_int(int(v)))
+    cp = C.byref(C.c_float(cprecr))
+    P = lambda arr: arr.ctypes.data_as(C.c_void_p)
+    ibc = [np.ascontiguousarray(v, np.int32) for v in ibc]
+    ibf = [np.ascontiguousarray(v, np.int32) for v in ibf]
+    L.convolut_ib_sse_cxyz_(ii(n1), ii(n2), ii(n3), P(ibc[0]), P(ibc[1]), P(ibc[2]), cp, P(x_c), P(y_c), P(fa))
+    lim = [ii(nfl[0]), ii(nfu[0]), ii(nfl[1]), ii(nfu[1]), ii(nfl[2]), ii(nfu[2])]
+    for nm in _FINE_X:
+        getattr(L, nm)(ii(n1), ii(n2), ii(n3), P(ibf[0]), cp, *lim, P(x_f), P(y_f), P(fa), P(fb), P(fc), P(fe))
+    for nm in _FINE_YZ:
+        ib = ibf[1] if "_fy_" in nm else ibf[2]
+        getattr(L, nm)(ii(n1), ii(n2), ii(n3), P(ib), *lim, P(x_f), P(y_f), P(fa), P(fb), P(fc), P(fe))
+    return y_c, y_f
+
+
+def _filter_table(name):
+    """A coefficient table of the generated filter header (parsed from the
+    reference sources at build time), as float64."""
+    import re
+    hdr = (HERE.parent / "bigdft-suite_b200" / "csrc" / "wvl_filters.h").read_text()
+    m = re.search(r"#define %s_AT\(i\) (.*)" % name, hdr)
+    return [float(v) for v in re.findall(r"\(([-+]?\d[\d.eE+-]*)\)", m.group(1))]

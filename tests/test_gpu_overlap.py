@@ -111,3 +111,45 @@ def test_overlap_sharded_single_process_uses_the_device_kernel(torch_cuda, wctx)
     S = overlap_sharded(X, ctx=wctx)
     ref = (X.cpu().numpy() @ X.cpu().numpy().T)
     assert np.abs(S.cpu().numpy() - ref).max() <= 1e-13 * np.abs(ref).max()
+
+
+@pytest.mark.parametrize("norb,K,lower,beta", [(64, 4096, False, 0.0), (37, 5003, True, 0.0), (100, 12345, False, 1.0),
+                                               (256, 30000, True, 0.0), (33, 777, False, 1.0)])
+def test_panel_apply_matches_fp64_product(torch_cuda, wctx, norb, K, lower, beta):
+    """out = beta out + alpha M psi on the tensor-core panel apply against the
+    FP64 product on the host (odd orbital counts and lengths take the
+    one-double copies; lower skips the slices above the diagonal)."""
+    from wvlh.ortho import panel_apply
+    torch = torch_cuda
+    rng = np.random.default_rng(norb * K)
+    M = rng.uniform(-1, 1, (norb, norb))
+    if lower:
+        M = np.tril(M)
+    psi = rng.uniform(-1, 1, (norb, K))
+    out0 = rng.uniform(-1, 1, (norb, K))
+    alpha = -0.75
+    tout = torch.tensor(out0, device="cuda")
+    panel_apply(wctx, torch.tensor(M, device="cuda"), torch.tensor(psi, device="cuda"), out=tout, alpha=alpha,
+                beta=beta, lower=lower)
+    ref = beta * out0 + alpha * (M @ psi)
+    assert np.abs(tout.cpu().numpy() - ref).max() / np.abs(ref).max() < 1e-13
+
+
+@pytest.mark.parametrize("method", ["cholesky", "loewdin"])
+def test_orthonormalize_matches_oracle_chain(oracle, torch_cuda, wctx, method):
+    """psi <- L^-1 psi (dpotrf, dtrtri, dtrmm) or S^-1/2 psi on the panel
+    apply against the same steps in FP64 on the host from the oracle's S."""
+    torch = torch_cuda
+    rng = np.random.default_rng(11)
+    norb, K = 48, 30011
+    psi = rng.uniform(-1, 1, (norb, K))
+    t = torch.tensor(psi, device="cuda")
+    orthonormalize(wctx, t, method)
+    S = oracle.overlap(psi)
+    if method == "cholesky":
+        M = np.linalg.inv(oracle.cholesky_lower(S))
+    else:
+        w, U = np.linalg.eigh(S)
+        M = (U / np.sqrt(w)) @ U.T
+    ref = M @ psi
+    assert np.abs(t.cpu().numpy() - ref).max() / np.abs(ref).max() < 1e-11

@@ -205,3 +205,62 @@ def test_isf_weights_match_reference_lazy16():
     for m in range(-18, 19):
         want = 1.0 if m == 0 else (w[abs(m)] if m % 2 and abs(m) <= 15 else 0.0)
         assert abs(ch[m] - want) <= 1e-17 + 1e-15 * abs(want)
+
+
+def _ellipsoid(N, frac, shift=(0.0, 0.0, 0.0)):
+    idx = np.meshgrid(*[np.arange(v) for v in N[::-1]], indexing="ij")
+    r2 = np.zeros(N[::-1])
+    for ax, n, s in zip(idx, N[::-1], shift[::-1]):
+        r2 += ((ax - (n - 1) / 2.0 - s) / (frac * n)) ** 2
+    return r2 <= 1.0
+
+
+@pytest.mark.parametrize("N,fc,ff,cprecr", [((12, 10, 14), 0.6, 0.35, 0.0), ((16, 13, 11), 0.55, 0.3, 0.7)])
+def test_wavelet_kinetic_matches_reference_sse(oracle, N, fc, ff, cprecr):
+    """The oracle's wavelet-basis kinetic operator (the a, b, c, e filters of
+    ConvolkineticT) against the reference's own SSE implementation of it,
+    convolut_ib_sse.c (compiled where it lies into oracle/_ref), on a free
+    region with irregular coarse and fine masks: coarse->coarse on a coarse
+    input, fine->fine on a fine input, (c + T) x.  The reference computes in
+    FP32: agreement to 2e-6 of the largest output."""
+    if oracle.ref_convib() is None:
+        pytest.skip("oracle/_ref not built (needs the reference tree)")
+    from wvlh.keys import Locreg, make_bounds
+    mc = _ellipsoid(N, fc)
+    mf = _ellipsoid(N, ff, (0.5, -0.5, 0.3)) & mc
+    lr = Locreg.from_masks(mc, mf, (0, 0, 0), (0.45, 0.45, 0.45))
+    d = oracle.Desc(lr.n, lr.periodic, lr.keyg_c, lr.keyv_c, lr.keyg_f, lr.keyv_f)
+    rng = np.random.default_rng(sum(N))
+    # FP32-representable inputs, so both sides see the same numbers
+    pc = rng.uniform(-1, 1, lr.nvctr_c).astype(np.float32).astype(np.float64)
+    pf = rng.uniform(-1, 1, 7 * lr.nvctr_f).astype(np.float32).astype(np.float64)
+    fz, fy, fx = np.nonzero(mf)
+    nfl, nfu = (fx.min(), fy.min(), fz.min()), (fx.max(), fy.max(), fz.max())
+
+    def ib(m):
+        return [np.stack([b.lo, b.hi], axis=-1) for b in make_bounds(m)]
+
+    def dense(c, f):
+        """coarse (n3+1, n2+1, n1+1) and fine (.., .., .., 7) arrays from compressed values"""
+        xc = np.zeros(N[::-1])
+        xc[mc] = c                      # keys run x fastest, like C order of (i3, i2, i1)
+        xf = np.zeros(N[::-1] + (7,))
+        xf[mf] = f.reshape(-1, 7)
+        return xc, xf[nfl[2]:nfu[2] + 1, nfl[1]:nfu[1] + 1, nfl[0]:nfu[0] + 1]
+
+    n = tuple(v - 1 for v in N)
+    h = lr.hgrid[0]
+    zc, zf = np.zeros_like(pc), np.zeros_like(pf)
+    for part in ("coarse", "fine"):
+        c, f = (pc, zf) if part == "coarse" else (zc, pf)
+        y, _ = oracle.kinetic_wavelet(d, lr.hgrid, oracle.uncompress(d, c, f))
+        yc, yf = oracle.compress(d, y)
+        xc, xf = dense(c, f)
+        rc, rf = oracle.ref_kinetic_sse(n, h, cprecr, xc, xf, nfl, nfu, ib(mc), ib(mf))
+        if part == "coarse":
+            got, want = rc[mc], yc + cprecr * c
+        else:
+            full = np.zeros(N[::-1] + (7,), np.float32)
+            full[nfl[2]:nfu[2] + 1, nfl[1]:nfu[1] + 1, nfl[0]:nfu[0] + 1] = rf
+            got, want = full[mf].ravel(), yf + cprecr * f
+        assert np.abs(got - want).max() <= 2e-6 * np.abs(want).max(), part
