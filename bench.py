@@ -273,6 +273,42 @@ def oracle_errors(lr_list, psi_rows, pot_rows, hpsi_rows, ekin, epot):
     return worst
 
 
+def leg_exchanges(torch, ctx, batch, psi32, psi64, lr, norb, ws, dev, reps=5):
+    """The two data-path exchanges of an SCF step on sharded orbitals, every
+    rank taking part (NCCL): the density of this rank's orbitals summed over
+    the ranks into z-slabs (reduce-scatter, communicate_density,
+    sumrho.f90:219), and the overlap S of all orbitals through the
+    orbital -> component all-to-all, the local FP64 tensor-core Gram matrix
+    and the all-reduce of S (orthogonality.f90:2695).  Timed on the device
+    with CUDA events, the max over ranks."""
+    import torch.distributed as dist
+    from wvlh.shard import overlap_sharded, reduce_density
+    vol = (0.5 * lr.hgrid[0]) * (0.5 * lr.hgrid[1]) * (0.5 * lr.hgrid[2])
+    hf = torch.full((norb,), 2.0 / vol, dtype=torch.float64, device=dev)
+    rho = torch.zeros(lr.nisf, dtype=torch.float64, device=dev)
+    P = psi64.view(norb, -1)
+    res = {}
+    for name, fn in (("density_reduce_scatter", lambda: (rho.zero_(), batch.locden(psi32, hf, rho),
+                                                         reduce_density(rho, lr.isf, scatter=True))),
+                     ("overlap_sharded", lambda: overlap_sharded(P, ctx=ctx))):
+        for _ in range(2):
+            fn()
+        torch.cuda.synchronize()
+        dist.barrier()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        for _ in range(reps):
+            fn()
+        b.record()
+        torch.cuda.synchronize()
+        t = torch.tensor([a.elapsed_time(b) / reps], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        res[name + "_ms"] = t.item()
+    res["orbitals_per_rank"] = norb
+    res["ranks"] = ws
+    return res
+
+
 def leg_free_regions(torch, ctx, dev, nlr=1024, seed=2):
     """Free-BC support functions of uneven size: nlr regions with coarse boxes
     uniform 20..40 per dimension (all cells coarse), fine ellipsoid of radius
@@ -298,6 +334,8 @@ def leg_free_regions(torch, ctx, dev, nlr=1024, seed=2):
     cells = sum(lr.coarse_cells for lr in lrs)
     h32, h64 = torch.empty_like(psi32), torch.empty_like(psi64)
     e = torch.empty(4, nlr, dtype=torch.float64, device=dev)
+    tuned = {nm: b.autotune(ps, pt, hh, e[0], e[1], reps=1)[0]
+             for nm, ps, pt, hh in (("fp32", psi32, pot32, h32), ("fp64", psi64, pot64, h64))}
     ms32 = _timed(torch, lambda: b.locham(psi32, pot32, h32, e[0], e[1]), 5)
     ms64 = _timed(torch, lambda: b.locham(psi64, pot64, h64, e[2], e[3]), 3)
     de = max((e[0] - e[2]).abs().max().item(), (e[1] - e[3]).abs().max().item())
@@ -315,7 +353,7 @@ def leg_free_regions(torch, ctx, dev, nlr=1024, seed=2):
         err[nm] = oracle_errors([lrs[o] for o in sample], rows, vrows, hr, [e[k][o].item() for o in sample],
                                 [e[k + 1][o].item() for o in sample])
     out = {"workload": "%d free-BC regions, coarse 20..40 per dim, fine ellipsoid 0.4, 1 orbital each" % nlr,
-           "err_vs_oracle": err,
+           "err_vs_oracle": err, "plane_threads_measured": tuned,
            "coarse_cells": int(cells), "fp32_fused": {"value": cells / (ms32 * 1e-3), "ms": ms32},
            "fp64_fused": {"value": cells / (ms64 * 1e-3), "ms": ms64},
            "fp64_plain": {"value": cells / (ms_plain * 1e-3), "ms": ms_plain},
@@ -732,6 +770,14 @@ def main():
     esum = torch.zeros(2, dtype=torch.float64, device=dev)
     pts_step = norb * lr.coarse_cells
 
+    # measured block size of the plane kernels for this batch (kept for the run)
+    tuned = {}
+    for nm, ps, pt in (("fp32", psi32, pot32), ("fp64", psi64, pot64)):
+        hh = torch.empty_like(ps)
+        pick, times = batch.autotune(ps, pt, hh, ek, ep, reps=2)
+        tuned[nm] = {"plane_threads": pick, "ms_by_block_size": times}
+        del hh
+
     def step():
         batch.locham(psi32, pot32, hpsi32, ek, ep)
         if ws > 1:
@@ -768,7 +814,9 @@ def main():
     value = ws * pts_step * args.steps / (ms * 1e-3)
     launches = 4 * args.steps
 
-    extras = {}
+    extras = {"autotune": tuned}
+    if ws > 1 and not args.no_extras:
+        extras["multi_gpu"] = leg_exchanges(torch, ctx, batch, psi32, psi64, lr, norb, ws, dev)
     if rank == 0 and not args.no_extras:
         # per-kernel CUDA-event times on the library stream
         import ctypes as C

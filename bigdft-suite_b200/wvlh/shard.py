@@ -156,3 +156,49 @@ def overlap_sharded(psi_local, group=None, gram=None, ctx=None):
     S = S.to(torch.float64).contiguous()
     dist.all_reduce(S, group=group)
     return S
+
+
+class RankFailure(RuntimeError):
+    """Raised on the surviving ranks when a peer did not reach a step."""
+
+    def __init__(self, step, missing):
+        super().__init__("step %d: rank(s) %s did not arrive" % (step, ", ".join(map(str, missing))))
+        self.step = step
+        self.missing = list(missing)
+
+
+class StepMonitor:
+    """Host-side failure detection between steps, before any collective of
+    the step is entered: each rank records in a key-value store (a
+    torch.distributed TCPStore) that it reached step k, then waits at most
+    `timeout` seconds for the others.  A rank that left between steps (an
+    exception, a crash) is found here and reported with RankFailure, so no
+    rank starts a collective (or a kernel that would wait for a peer) that
+    the missing rank will never join.  A collective already in flight when a
+    rank dies is ended by the process group's own timeout instead."""
+
+    def __init__(self, store, rank, world, prefix="wvlh/step"):
+        self.store, self.rank, self.world, self.prefix = store, rank, world, prefix
+
+    def _key(self, step, r):
+        return "%s/%d/%d" % (self.prefix, step, r)
+
+    def arrive(self, step):
+        self.store.set(self._key(step, self.rank), "1")
+
+    def missing(self, step, timeout=2.0, poll=0.02):
+        import time
+        keys = [self._key(step, r) for r in range(self.world)]
+        t0 = time.monotonic()
+        while True:
+            absent = [r for r, k in enumerate(keys) if not self.store.check([k])]
+            if not absent or time.monotonic() - t0 > timeout:
+                return absent
+            time.sleep(poll)
+
+    def barrier(self, step, timeout=2.0):
+        """arrive at step, then raise RankFailure if a peer does not"""
+        self.arrive(step)
+        absent = self.missing(step, timeout)
+        if absent:
+            raise RankFailure(step, absent)

@@ -223,3 +223,26 @@ def test_fp64_large_planes_match_oracle(oracle, torch_cuda, wctx, N, per, dens):
     # the FP32 form of the same boxes keeps two shared planes
     out, gek, gep = run_batch(wctx, torch_cuda, [lr], [psi], [pot], torch_cuda.float32)
     assert rel(out[0], ref) < 1e-5 and abs(gek[0] - ek) < 1e-6 and abs(gep[0] - ep) < 1e-6
+
+
+@pytest.mark.parametrize("dtype_name,tol", [("float64", 1e-13), ("float32", 1e-6)])
+def test_autotune_times_every_block_size_and_keeps_results(oracle, torch_cuda, wctx, dtype_name, tol):
+    """wvlh_batch_autotune times each compiled block size of the plane kernels
+    on the batch's own locham and keeps the fastest; the result does not
+    depend on the pick (beyond the energies' summation order)."""
+    torch = torch_cuda
+    lrs = [case((12, 10, 9), (0, 0, 0), 0.6, seed=1)[0], case((10, 11, 12), (1, 1, 1), 0.5, seed=2)[0]]
+    rng = np.random.default_rng(4)
+    b = Batch(wctx, lrs, [0, 1, 1], np.cumsum([0] + [lrs[0].nisf, lrs[1].nisf])[:3])
+    dt = getattr(torch, dtype_name)
+    psi = torch.tensor(rng.uniform(-1, 1, b.psi_size), dtype=dt, device="cuda")
+    pot = torch.tensor(rng.uniform(-1, 0, b.pot_size), dtype=dt, device="cuda")
+    h0, e0, p0 = b.locham(psi, pot)
+    h0, e0, p0 = h0.clone(), e0.clone(), p0.clone()
+    pick, times = b.autotune(psi, pot, reps=1)
+    assert pick in times and len(times) >= 4 and all(t > 0 for t in times.values())
+    h1, e1, p1 = b.locham(psi, pot)
+    torch.cuda.synchronize()
+    assert ((h1 - h0).norm() / h0.norm()).item() <= tol
+    assert ((e1 - e0).abs() / e0.abs()).max().item() <= 1e-12 and ((p1 - p0).abs() / p0.abs()).max().item() <= 1e-12
+    b.close()
