@@ -386,10 +386,13 @@ def leg_precond(torch, ctx, dev, n=40, norb=512, ncong=5, seed=3):
         return b.precond(x, r, cprec, ncong)
 
     for nm, x, r in (("fp32", x32, r32), ("fp64", x64, r64)):
+        # measured block size of the preconditioner's plane kernels (untimed)
+        pick, by_size = b.autotune_precond(x, r, cprec, ncong, reps=1)
         ms = _timed(torch, lambda: run(x, r), 3)
         _, hist = run(x, r)
         torch.cuda.synchronize()
-        res[nm] = {"ms": ms, "value": norb * lr.coarse_cells / (ms * 1e-3), "hist": hist.cpu().numpy()}
+        res[nm] = {"ms": ms, "value": norb * lr.coarse_cells / (ms * 1e-3), "hist": hist.cpu().numpy(),
+                   "plane_threads": pick, "ms_by_block_size": by_size}
     h32, h64 = res["fp32"].pop("hist"), res["fp64"].pop("hist")
     rel = np.abs(h32 - h64) / np.abs(h64)
     # two orbitals through the oracle's CG (x0 = b = r): x relative L2 and the
@@ -409,6 +412,7 @@ def leg_precond(torch, ctx, dev, n=40, norb=512, ncong=5, seed=3):
                                                 float(np.max(np.abs(hist[:, o] - rn) / np.abs(rn))))
     out = {"workload": "%d orbitals, %d^3 periodic, %d CG iterations" % (norb, n, ncong),
            "fp32": res["fp32"], "fp64": res["fp64"],
+           "speedup_fp32_vs_fp64": res["fp64"]["ms"] / res["fp32"]["ms"],
            "residual_norm2_mean_per_iter_fp64": [float(v) for v in h64.mean(axis=1)],
            "residual_norm2_max_rel_err_fp32_vs_fp64": float(rel.max()),
            "x_rel_l2_fp32_vs_fp64": float((x32.double() - x64).norm() / x64.norm()),
@@ -479,12 +483,12 @@ def leg_overlap(torch, ctx, psi64, norb):
     L = torch.linalg.cholesky(ref / K + torch.eye(norb, dtype=torch.float64, device=P.device))
     Linv = torch.linalg.solve_triangular(L, torch.eye(norb, dtype=torch.float64, device=P.device), upper=False)
     O = torch.empty_like(P)
-    ms_dense = _timed(lambda: panel_apply(ctx, Mf, P, out=O), 3)
-    ms_dense_cublas = _timed(lambda: torch.mm(Mf, P, out=O), 3)
+    ms_dense = _timed(torch, lambda: panel_apply(ctx, Mf, P, out=O), 3)
+    ms_dense_cublas = _timed(torch, lambda: torch.mm(Mf, P, out=O), 3)
     err_dense = (panel_apply(ctx, Mf, P, out=O) - torch.mm(Mf, P)).abs().max().item()
-    ms_tri = _timed(lambda: panel_apply(ctx, Linv, P, out=O, lower=True), 3)
-    ms_trsm = _timed(lambda: torch.linalg.solve_triangular(L, P, upper=False), 2)
-    ms_sub = _timed(lambda: panel_apply(ctx, Mf, P, out=O, alpha=-1.0, beta=1.0), 3)
+    ms_tri = _timed(torch, lambda: panel_apply(ctx, Linv, P, out=O, lower=True), 3)
+    ms_trsm = _timed(torch, lambda: torch.linalg.solve_triangular(L, P, upper=False), 2)
+    ms_sub = _timed(torch, lambda: panel_apply(ctx, Mf, P, out=O, alpha=-1.0, beta=1.0), 3)
     del O
     fd = 2.0 * norb * norb * K
     out["panel_apply"] = {"workload": "%d x %d FP64 matrix times the %d x %d orbital panel" % (norb, norb, norb, K),
@@ -693,13 +697,18 @@ def leg_serve(torch, dev, precision, nreq=300, loads=(0.3, 0.5, 0.7)):
         st = latency_stats(reqs)
         sweep.append({"load": load, "offered_req_s": load * cap, "served_req_s": len(reqs) / dt,
                       "served_cells_s": sum(cells[r.client.id] for r in reqs) / dt,
-                      "p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"], "mean_ms": st["mean_ms"]})
+                      "p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"], "mean_ms": st["mean_ms"],
+                      "queued_p50_ms": st["queued_p50_ms"], "queued_p99_ms": st["queued_p99_ms"],
+                      "launched_p50_ms": st["launched_p50_ms"], "launched_p99_ms": st["launched_p99_ms"],
+                      "tail": st["tail"]})
     kept = [w for w in sweep if w["served_req_s"] >= 0.95 * w["offered_req_s"]]
     head = kept[-1] if kept else sweep[0]
     out = {"clients": len(cl), "resident_gb": srv.resident / 1e9, "capacity_req_s": cap,
            "capacity_cells_s": cap_cells, "sustained_load": head["load"], "offered_req_s": head["offered_req_s"],
            "served_req_s": head["served_req_s"], "served_cells_s": head["served_cells_s"],
-           "p50_ms": head["p50_ms"], "p99_ms": head["p99_ms"], "mean_ms": head["mean_ms"], "sweep": sweep,
+           "p50_ms": head["p50_ms"], "p99_ms": head["p99_ms"], "mean_ms": head["mean_ms"],
+           "queued_p99_ms": head["queued_p99_ms"], "launched_p99_ms": head["launched_p99_ms"], "tail": head["tail"],
+           "sweep": sweep,
            "launches": srv.launches - n0, "kernel_launches": srv.kernel_launches - k0,
            "requests": nreq * len(loads)}
     srv.close()

@@ -338,7 +338,7 @@ static void layout(wvlh_batch *b, const std::vector<int> &orb_lr, const std::vec
         const int l = orb_lr[o];
         const LrDev &d = lrd[l];
         const int N1 = d.N[0], N2 = d.N[1], N3 = d.N[2];
-        const int G1 = 2 * N1, G2 = 2 * N2, G3 = 2 * N3;
+        const int G3 = 2 * N3;
         const int F1 = fine_len(N1, d.per[0]), F2 = fine_len(N2, d.per[1]), F3 = fine_len(N3, d.per[2]);
         const int I1 = isf_len(N1, d.per[0]), I2 = isf_len(N2, d.per[1]), I3 = isf_len(N3, d.per[2]);
         OrbDev &q = od[o];
@@ -409,6 +409,8 @@ static void layout(wvlh_batch *b, const std::vector<int> &orb_lr, const std::vec
     p.part_stride = stride;
     p.plane_threads[0] = choose_plane_threads(shapes32, true);
     p.plane_threads[1] = choose_plane_threads(shapes64, false);
+    p.plane_threads_pre[0] = p.plane_threads[0];
+    p.plane_threads_pre[1] = p.plane_threads[1];
     apply_tuned(p);   // a measured choice for this shape, when wvlh_batch_autotune made one
     p.plane_elems = (long long)planeA;
     p.planeB_elems = (long long)planeB;
@@ -724,7 +726,7 @@ extern "C" int wvlh_precond_batched(wvlh_batch *b, int precision, int ncong, con
     const size_t nv = (size_t)p.psi_total * es;
     int rc;
     if ((rc = c->scratch.ensure((p.scratch_elems + plane_tmp_elems(p, fp)) * es)) || (rc = c->cg_r.ensure(nv)) || (rc = c->cg_d.ensure(nv)) ||
-        (rc = c->cg_ad.ensure(nv)) || (rc = c->cg_scal.ensure(sizeof(double) * (size_t)p.norb * (5 + 16))))
+        (rc = c->cg_ad.ensure(nv)) || (rc = c->cg_scal.ensure(sizeof(double) * (size_t)p.norb * (5 + 16 + p.part_stride))))
         return fail(rc);
     cudaError_t e =
         fp ? launch_precond<double>(p, ncong, cprec, (double *)x, (const double *)rhs, (double *)c->cg_r.p,
@@ -796,14 +798,17 @@ extern "C" int wvlh_panel_apply(wvlh_ctx *c, int norb, int64_t K, int64_t ld, co
 // choose_plane_threads is a starting point; wvlh_batch_autotune times the
 // batch's own local Hamiltonian with every candidate block size and keeps the
 // fastest, both in the batch and in a process-wide table keyed by the batch's
-// shape (precision and every orbital's box), which later batches of the same
-// shape read at creation.
+// shape (operation, precision and every orbital's box), which later batches of
+// the same shape read at creation.  wvlh_batch_autotune_precond does the same
+// for the preconditioner operator, whose plane kernels run fewer passes per
+// plane and so may prefer another size.
 static std::mutex g_tune_mu;
 static std::map<std::string, int> g_tuned;
 
-static std::string tune_key(const Plan &p, int fp)
+// what: 0 plane kernels, 1 z kernel; pre: the preconditioner operator
+static std::string tune_key(const Plan &p, int fp, bool pre = false, int what = 0)
 {
-    std::string k = fp ? "64" : "32";
+    std::string k = std::string(what ? "z" : "") + (pre ? "p" : "") + (fp ? "64" : "32");
     for (int o = 0; o < p.norb; ++o) {
         const int l = p.orb_lr[o];
         char buf[64];
@@ -817,6 +822,8 @@ static std::string tune_key(const Plan &p, int fp)
 // the block sizes the plane kernels are compiled for
 static const int kTune32[5] = {1024, 512, kPlaneThreads, 256, 128};
 static const int kTune64[4] = {512, kPlaneThreads, 256, 128};
+// the block sizes the FP32 z kernel is compiled for
+static const int kTuneZ32[3] = {kZThreads, 320, 384};
 
 static void apply_tuned(Plan &p)
 {
@@ -824,30 +831,32 @@ static void apply_tuned(Plan &p)
     for (int fp = 0; fp < 2; ++fp) {
         auto it = g_tuned.find(tune_key(p, fp));
         if (it != g_tuned.end()) p.plane_threads[fp] = it->second;
+        it = g_tuned.find(tune_key(p, fp, true));
+        if (it != g_tuned.end()) p.plane_threads_pre[fp] = it->second;
+        it = g_tuned.find(tune_key(p, fp, false, 1));
+        if (it != g_tuned.end()) p.z_threads[fp] = it->second;
+        it = g_tuned.find(tune_key(p, fp, true, 1));
+        if (it != g_tuned.end()) p.z_threads_pre[fp] = it->second;
     }
 }
 
-extern "C" int wvlh_batch_autotune(wvlh_batch *b, int precision, const void *psi, const void *pot, void *hpsi,
-                                   double *ekin, double *epot, int reps, int *chosen, int *cand, double *ms,
-                                   int *ncand)
+// Times fn() (reps calls after one warm-up) with each candidate block size
+// written into *slot; leaves the fastest in *slot and returns it in *chosen.
+template <class F>
+static int time_candidates(wvlh_ctx *c, int *slot, const int *cs, int n, int reps, F &&fn, int *chosen, int *cand,
+                           double *ms, int *ncand)
 {
-    if (!b || (precision != 32 && precision != 64) || reps < 1) return fail(WVLH_ERR_ARG);
-    wvlh_ctx *c = b->ctx;
-    CK(cudaSetDevice(c->device));
-    const int fp = precision == 64;
-    const int n = fp ? 4 : 5;
-    const int *cs = fp ? kTune64 : kTune32;
     cudaEvent_t a, z;
     CK(cudaEventCreate(&a));
     CK(cudaEventCreate(&z));
-    int best = b->plan.plane_threads[fp];
+    int best = *slot;
     double best_ms = -1.0;
     int rc = WVLH_OK;
     for (int k = 0; k < n && rc == WVLH_OK; ++k) {
-        b->plan.plane_threads[fp] = cs[k];
-        rc = wvlh_locham_batched(b, precision, psi, pot, hpsi, ekin, epot, 0);   // warm-up
+        *slot = cs[k];
+        rc = fn();   // warm-up
         cudaEventRecord(a, c->stream);
-        for (int r = 0; r < reps && rc == WVLH_OK; ++r) rc = wvlh_locham_batched(b, precision, psi, pot, hpsi, ekin, epot, 0);
+        for (int r = 0; r < reps && rc == WVLH_OK; ++r) rc = fn();
         cudaEventRecord(z, c->stream);
         if (rc) break;
         cudaEventSynchronize(z);
@@ -863,14 +872,59 @@ extern "C" int wvlh_batch_autotune(wvlh_batch *b, int precision, const void *psi
     }
     cudaEventDestroy(a);
     cudaEventDestroy(z);
-    b->plan.plane_threads[fp] = best;
-    if (rc) return fail(rc);
-    {
-        std::lock_guard<std::mutex> lk(g_tune_mu);
-        g_tuned[tune_key(b->plan, fp)] = best;
-    }
+    *slot = best;
+    if (rc) return rc;
     if (chosen) *chosen = best;
     if (ncand) *ncand = n;
+    return WVLH_OK;
+}
+
+extern "C" int wvlh_batch_autotune(wvlh_batch *b, int precision, const void *psi, const void *pot, void *hpsi,
+                                   double *ekin, double *epot, int reps, int *chosen, int *cand, double *ms,
+                                   int *ncand)
+{
+    if (!b || (precision != 32 && precision != 64) || reps < 1) return fail(WVLH_ERR_ARG);
+    wvlh_ctx *c = b->ctx;
+    CK(cudaSetDevice(c->device));
+    const int fp = precision == 64;
+    auto call = [&] { return wvlh_locham_batched(b, precision, psi, pot, hpsi, ekin, epot, 0); };
+    int rc = time_candidates(c, &b->plan.plane_threads[fp], fp ? kTune64 : kTune32, fp ? 4 : 5, reps, call, chosen,
+                             cand, ms, ncand);
+    // then the z kernel's block size (FP32), with the plane kernels' pick
+    if (!rc && !fp) rc = time_candidates(c, &b->plan.z_threads[0], kTuneZ32, 3, reps, call, nullptr, nullptr, nullptr, nullptr);
+    if (rc) return fail(rc);
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    g_tuned[tune_key(b->plan, fp)] = b->plan.plane_threads[fp];
+    g_tuned[tune_key(b->plan, fp, false, 1)] = b->plan.z_threads[fp];
+    return WVLH_OK;
+}
+
+extern "C" int wvlh_batch_block_sizes(const wvlh_batch *b, int *sizes)
+{
+    if (!b || !sizes) return fail(WVLH_ERR_ARG);
+    const Plan &p = b->plan;
+    const int v[8] = {p.plane_threads[0], p.plane_threads[1], p.z_threads[0], p.z_threads[1],
+                      p.plane_threads_pre[0], p.plane_threads_pre[1], p.z_threads_pre[0], p.z_threads_pre[1]};
+    for (int k = 0; k < 8; ++k) sizes[k] = v[k];
+    return WVLH_OK;
+}
+
+extern "C" int wvlh_batch_autotune_precond(wvlh_batch *b, int precision, int ncong, const double *cprec, void *x,
+                                           const void *rhs, int reps, int *chosen, int *cand, double *ms, int *ncand)
+{
+    if (!b || (precision != 32 && precision != 64) || reps < 1 || ncong < 0) return fail(WVLH_ERR_ARG);
+    wvlh_ctx *c = b->ctx;
+    CK(cudaSetDevice(c->device));
+    const int fp = precision == 64;
+    auto call = [&] { return wvlh_precond_batched(b, precision, ncong, cprec, x, rhs, nullptr); };
+    int rc = time_candidates(c, &b->plan.plane_threads_pre[fp], fp ? kTune64 : kTune32, fp ? 4 : 5, reps, call,
+                             chosen, cand, ms, ncand);
+    if (!rc && !fp)
+        rc = time_candidates(c, &b->plan.z_threads_pre[0], kTuneZ32, 3, reps, call, nullptr, nullptr, nullptr, nullptr);
+    if (rc) return fail(rc);
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    g_tuned[tune_key(b->plan, fp, true)] = b->plan.plane_threads_pre[fp];
+    g_tuned[tune_key(b->plan, fp, true, 1)] = b->plan.z_threads_pre[fp];
     return WVLH_OK;
 }
 

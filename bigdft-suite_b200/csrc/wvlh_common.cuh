@@ -384,7 +384,7 @@ __device__ __forceinline__ void pass_kin(const T *src, T *dst, const LineGeom g,
 #pragma unroll
         for (int t = 0; t < SEG; ++t) {
             T conv = Filt<T>::kin(0) * x[t + 14];
-            T lo = T(0);
+            [[maybe_unused]] T lo = T(0);
             if constexpr (sizeof(T) == 4) lo = Filt<T>::kin_lo(0) * x[t + 14];
 #pragma unroll
             for (int l = 1; l <= 14; ++l) {

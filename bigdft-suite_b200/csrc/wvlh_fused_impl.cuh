@@ -154,12 +154,13 @@ __device__ void gather_plane(T *A, int pitch, const LrDev &L, int kz, const TI *
 }
 
 // Inverse of gather_plane: write (or add into) the compressed output.
-template <class T, class TO, int S3>
+template <class T, class TO, int S3, bool DOT = false>
 __device__ __forceinline__ void scatter_plane_s(const T *A, int pitch, const LrDev &L, int i3, TO *out, bool accumulate,
-                                                const T *sc)
+                                                const T *sc, const TO *dotv, double &dot)
 {
     const int H1 = half_off(L.N[0]), H2 = half_off(L.N[1]);
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    // dotv (optional): dot += <dotv | written values> over this plane's values
     if (!S3) {
         const T s0 = sc ? sc[0] : T(1);
         const int a = L.plane_c[i3], b = L.plane_c[i3 + 1];
@@ -168,30 +169,35 @@ __device__ __forceinline__ void scatter_plane_s(const T *A, int pitch, const LrD
             for (int t = lane; t < d.z; t += 32) {
                 const TO v = (TO)(A[d.y * pitch + d.x + t] * s0);
                 out[d.w + t] = accumulate ? out[d.w + t] + v : v;
+                if (DOT && dotv) dot += (double)v * (double)dotv[d.w + t];
             }
         }
     }
     TO *pf = out + L.nvctr_c;
+    const TO *df = DOT && dotv ? dotv + L.nvctr_c : nullptr;
     const int a = L.plane_f[i3], b = L.plane_f[i3 + 1];
     for (int sg = a + warp; sg < b; sg += nw) {
         const int4 d = L.seg_f[sg];
         for (int t = lane; t < d.z; t += 32) {
-            TO *dst = pf + 7 * (size_t)(d.w + t);
+            const size_t i = 7 * (size_t)(d.w + t);
+            TO *dst = pf + i;
 #pragma unroll
             for (int c = 1; c <= 7; ++c) {
                 if (fs3(c) != S3) continue;
                 const TO v = (TO)(A[(fs2(c) * H2 + d.y) * pitch + fs1(c) * H1 + d.x + t] * (sc ? sc[c] : T(1)));
                 dst[c - 1] = accumulate ? dst[c - 1] + v : v;
+                if (DOT && df) dot += (double)v * (double)df[i + c - 1];
             }
         }
     }
 }
 
-template <class T, class TO>
-__device__ void scatter_plane(const T *A, int pitch, const LrDev &L, int kz, TO *out, bool accumulate, const T *sc)
+template <class T, class TO, bool DOT = false>
+__device__ void scatter_plane(const T *A, int pitch, const LrDev &L, int kz, TO *out, bool accumulate, const T *sc,
+                              const TO *dotv, double &dot)
 {
-    if (kz >= L.N[2]) scatter_plane_s<T, TO, 1>(A, pitch, L, kz - L.N[2], out, accumulate, sc);
-    else scatter_plane_s<T, TO, 0>(A, pitch, L, kz, out, accumulate, sc);
+    if (kz >= L.N[2]) scatter_plane_s<T, TO, 1, DOT>(A, pitch, L, kz - L.N[2], out, accumulate, sc, dotv, dot);
+    else scatter_plane_s<T, TO, 0, DOT>(A, pitch, L, kz, out, accumulate, sc, dotv, dot);
 }
 
 // Rows of `cols` points walked as point pairs: warp w takes rows w, w + nwarps,
@@ -378,6 +384,54 @@ __host__ __device__ constexpr int plane_min_blocks(bool fp32, bool persist, int 
 }
 
 // ---------------------------------------------------------------------------
+// CG vectors the preconditioner's plane kernels fold in (MODE_PRECOND): K1
+// forms the search direction while it gathers it (dir 1: d = r, the first
+// iteration; dir 2: d = beta d + r with beta = rrn / rr, in T), and
+// writes d back; K3 accumulates <d | A d> over the values it scatters, into
+// one partial per plane.  dir 0 / d null: plain gather / scatter.
+template <class T> struct CgIo {
+    T *d;
+    const T *r;
+    const double *rr, *rrn;
+    int dir;
+};
+
+// gather_plane_s with the direction update: every coefficient of the plane
+// is read from d and r once, updated, written back to d and stored scaled
+template <class T, int S3>
+__device__ __forceinline__ void gather_plane_dir_s(T *A, int pitch, const LrDev &L, int i3, T *d, const T *r,
+                                                   T beta, bool first, const T *sc)
+{
+    const int H1 = half_off(L.N[0]), H2 = half_off(L.N[1]);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    auto upd = [&](size_t i) {
+        const T v = first ? r[i] : fma(beta, d[i], r[i]);
+        d[i] = v;
+        return v;
+    };
+    if (!S3) {
+        const int a = L.plane_c[i3], b = L.plane_c[i3 + 1];
+        for (int sg = a + warp; sg < b; sg += nw) {
+            const int4 q = L.seg_c[sg];
+            for (int t = lane; t < q.z; t += 32) A[q.y * pitch + q.x + t] = upd(q.w + t) * sc[0];
+        }
+    }
+    const size_t f0 = L.nvctr_c;
+    const int a = L.plane_f[i3], b = L.plane_f[i3 + 1];
+    for (int sg = a + warp; sg < b; sg += nw) {
+        const int4 q = L.seg_f[sg];
+        for (int t = lane; t < q.z; t += 32) {
+            const size_t i = f0 + 7 * (size_t)(q.w + t);
+#pragma unroll
+            for (int c = 1; c <= 7; ++c) {
+                if (fs3(c) != S3) continue;
+                A[(fs2(c) * H2 + q.y) * pitch + fs1(c) * H1 + q.x + t] = upd(i + c - 1) * sc[c];
+            }
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
 // K1: compressed psi -> P = S_x S_y psi (not in MODE_LOCDEN) and
 // Q = M_x M_y P (not in MODE_PRECOND) for one wavelet z-plane.
 //
@@ -391,9 +445,9 @@ template <class T, class TI, bool ALLPER, int MODE>
 __device__ __forceinline__ void k1_item(const LrDev *__restrict__ lrs, const OrbDev *__restrict__ orbs,
                                         const int *__restrict__ pre, int norb, const TI *__restrict__ psi,
                                         T *__restrict__ scratch, const double *__restrict__ cprec, int it, T *sc,
-                                        T *bslice)
+                                        T *bslice, const CgIo<T> &cg)
 {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
+    extern __shared__ __align__(128) unsigned char smem_raw[];
     constexpr int SEG = Seg<T>::v;
     {
         const int oi = find_owner(pre, norb, it);   // item = (orbital, wavelet plane kz)
@@ -408,7 +462,14 @@ __device__ __forceinline__ void k1_item(const LrDev *__restrict__ lrs, const Orb
         if (MODE == MODE_PRECOND && threadIdx.x < 8) sc[threadIdx.x] = (T)prec_scal(L, cprec[oi], threadIdx.x);
         zero_region(A, d.G2, pitch);
         __syncthreads();
-        if constexpr (std::is_same<T, TI>::value) {
+        if (MODE == MODE_PRECOND && cg.dir) {
+            // the CG direction, updated and scaled on the way in
+            T *dv = cg.d + o.psi;
+            const T *rv = cg.r + o.psi;
+            const T beta = cg.dir == 1 ? T(0) : (T)(cg.rrn[oi] / cg.rr[oi]);
+            if (kz >= d.N3) gather_plane_dir_s<T, 1>(A, pitch, L, kz - d.N3, dv, rv, beta, cg.dir == 1, sc);
+            else gather_plane_dir_s<T, 0>(A, pitch, L, kz, dv, rv, beta, cg.dir == 1, sc);
+        } else if constexpr (std::is_same<T, TI>::value) {
             gather_plane_async<T>(A, pitch, L, kz, in_ptr(o, psi));
             cp_async_wait_all();
             if constexpr (MODE == MODE_PRECOND) {
@@ -446,18 +507,18 @@ __global__ void __launch_bounds__(NT, plane_min_blocks(sizeof(T) == 4, PERSIST, 
                                                                   const int *__restrict__ pre, int norb,
                                                                   const TI *__restrict__ psi, T *__restrict__ scratch,
                                                                   const double *__restrict__ cprec, T *gtmp,
-                                                                  long long gstride)
+                                                                  long long gstride, const CgIo<T> cg)
 {
     __shared__ T sc[8];
     if (!PERSIST) {
-        k1_item<T, TI, ALLPER, MODE>(lrs, orbs, pre, norb, psi, scratch, cprec, blockIdx.x, sc, nullptr);
+        k1_item<T, TI, ALLPER, MODE>(lrs, orbs, pre, norb, psi, scratch, cprec, blockIdx.x, sc, nullptr, cg);
         return;
     }
     const int nwork = pre[norb];
     for (int it = blockIdx.x; it < nwork; it += gridDim.x) {
         __syncthreads();  // the previous item is done with A, B and sc
         k1_item<T, TI, ALLPER, MODE>(lrs, orbs, pre, norb, psi, scratch, cprec, it, sc,
-                                     gtmp + (size_t)blockIdx.x * gstride);
+                                     gtmp + (size_t)blockIdx.x * gstride, cg);
     }
 }
 
@@ -497,8 +558,13 @@ __device__ __forceinline__ void z_kin(const T *src, T *dst, int L, int per, doub
 // two-chain kernel, which eases instruction fetch).  CHAIN 0:
 // Z1 = A_z Mt_z (V . M_z S_z Q) in place of Q, E_pot partial.  CHAIN 1:
 // Z2 = A_z K_z S_z P, E_kin(z) partial.
-template <class T, class TV, bool ALLPER, int CHAIN>
-__global__ void __launch_bounds__(kZThreads, sizeof(T) == 4 ? 4 : 1) k2_zpencil(const LrDev *__restrict__ lrs, const OrbDev *__restrict__ orbs,
+// NT threads per CTA: 256, or for FP32 320 / 384, which give the passes over
+// 80- and 96-point z lines (32 line pairs x 10 or 12 eight-point segments)
+// one item per thread; resident CTAs per SM at 64 registers a thread.
+__host__ __device__ constexpr int z_min_blocks(bool fp32, int nt) { return fp32 ? 65536 / (64 * nt) : 1; }
+
+template <class T, class TV, bool ALLPER, int CHAIN, int NT = kZThreads>
+__global__ void __launch_bounds__(NT, z_min_blocks(sizeof(T) == 4, NT)) k2_zpencil(const LrDev *__restrict__ lrs, const OrbDev *__restrict__ orbs,
                                                         const int *__restrict__ pre, int norb,
                                                         const TV *__restrict__ pot, T *__restrict__ scratch,
                                                         double *__restrict__ part_pot, double *__restrict__ part_kin,
@@ -526,14 +592,13 @@ __global__ void __launch_bounds__(kZThreads, sizeof(T) == 4 ? 4 : 1) k2_zpencil(
     uint64_t *tma_bar = reinterpret_cast<uint64_t *>(red + 32);
     // TMA writes the tile only into a kZAlign-aligned buffer
     tma = tma && !(smem_addr(A) & (kZAlign - 1));
-    constexpr int SEG = Seg<T>::v;
     const int W = chain == 0 ? d.I1 : d.F1;   // plane width/height of the data
     const int H = chain == 0 ? d.I2 : d.F2;
     T *g = scratch + (chain == 0 ? o.sQ : o.sP);
     T *gz = scratch + (chain == 0 ? o.sQ : o.sZ);
     const size_t plane = (size_t)W * H;
     // element loops: thread t owns tile column c = t % TC at z = t / TC + k ZS
-    constexpr int ZS = kZThreads / TC;
+    constexpr int ZS = NT / TC;
     const int col = threadIdx.x % TC, zs = threadIdx.x / TC;
     const int xc = x0 + (col % TX), yc = y0 + (col / TX);
     const bool inside = xc < W && yc < H;
@@ -542,7 +607,7 @@ __global__ void __launch_bounds__(kZThreads, sizeof(T) == 4 ? 4 : 1) k2_zpencil(
     // column pairs (x, x + 1) of one tile row move as point pairs when the
     // plane rows have even length (the scratch planes start on a pair)
     const bool pairs = pair_rows(W, g);
-    constexpr int TP = TC / 2, ZP = kZThreads / TP;
+    constexpr int TP = TC / 2, ZP = NT / TP;
     const int pc = 2 * (threadIdx.x % TP), zp = threadIdx.x / TP;
     const int xp = x0 + (pc % TX), yp = y0 + (pc / TX);
     const bool pin = xp < W && yp < H;   // W even: x + 1 is inside too
@@ -560,9 +625,13 @@ __global__ void __launch_bounds__(kZThreads, sizeof(T) == 4 ? 4 : 1) k2_zpencil(
         const bool ok = mbar_wait_bounded(tma_bar, 0);
         if (!__syncthreads_and(ok)) {
             // the copy did not complete in time: poison this tile's energy
-            // slot (the orbital's energies come out NaN) and leave the tile
-            if (threadIdx.x == 0 && part_kin)
-                (chain == 0 ? part_pot : part_kin)[(size_t)oi * part_stride + jj] = __longlong_as_double(-1LL);
+            // slot (the orbital's energies come out NaN), give the copy in
+            // flight one more bounded wait and leave the tile
+            if (threadIdx.x == 0) {
+                if (part_kin)
+                    (chain == 0 ? part_pot : part_kin)[(size_t)oi * part_stride + jj] = __longlong_as_double(-1LL);
+                mbar_wait_bounded(tma_bar, 0);
+            }
             return;
         }
     } else {
@@ -584,7 +653,9 @@ __global__ void __launch_bounds__(kZThreads, sizeof(T) == 4 ? 4 : 1) k2_zpencil(
         else z_mf<T, 2>(B, A, d.F3, d.I3);
         __syncthreads();
         // psir <- V psir, epot += V psir^2 (orbitals/potential.f90:1011-1031);
-        // per-thread partial sum in T, one FP64 conversion per thread
+        // per-thread partial sum in T, one FP64 conversion per thread (which
+        // z values a thread sums depends on the block size, so the energy's
+        // rounding does too)
         const TV *V = o.pot_ptr ? (const TV *)o.pot_ptr : pot + o.pot;
         T ep = T(0);
         constexpr int U = 4;   // potential loads in flight per thread
@@ -677,9 +748,9 @@ __device__ __forceinline__ void k3_item(const LrDev *__restrict__ lrs, const Orb
                                         const int *__restrict__ pre, int norb, const T *__restrict__ scratch,
                                         TO *__restrict__ hpsi, double *__restrict__ part_kin, int part_stride,
                                         int accumulate, const double *__restrict__ cprec, int it, T *sc,
-                                        double *red, T *bslice)
+                                        double *red, T *bslice, const TO *__restrict__ dotv)
 {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
+    extern __shared__ __align__(128) unsigned char smem_raw[];
     constexpr int SEG = Seg<T>::v;
     {
         const int oi = find_owner(pre, norb, it);   // item = (orbital, wavelet plane kz)
@@ -792,19 +863,25 @@ __device__ __forceinline__ void k3_item(const LrDev *__restrict__ lrs, const Orb
             }
         }
         __syncthreads();
+        // e: the kinetic energy partial (MODE_LOCHAM) or <d | A d> (MODE_PRECOND)
         double e = 0.0;
+        double *ek = MODE == MODE_PRECOND ? nullptr : &e;
         const double sx = -0.5 / ((0.5 * L.hgrid[0]) * (0.5 * L.hgrid[0]));
         const double sy = -0.5 / ((0.5 * L.hgrid[1]) * (0.5 * L.hgrid[1]));
-        pass_kin<T, SEG, true, true>(B, A, rows_geom(d.F2, pitch), d.F1, d.p1, sx, T(0), &e);   // += K_x P
+        pass_kin<T, SEG, true, true>(B, A, rows_geom(d.F2, pitch), d.F1, d.p1, sx, T(0), ek);   // += K_x P
         __syncthreads();
-        pass_kin<T, SEG, true>(B, A, cols_geom(d.F1, pitch), d.F2, d.p2, sy, T(0), &e);   // += K_y P
+        // += K_y P: the lines along y are the plane's columns, side by side
+        // (F1 is even): FP32 takes them in pairs with packed FMAs
+        if constexpr (sizeof(T) == 4) pass2_kin<kPairSeg, true>(B, A, PairGeom{d.F1 / 2, pitch, pitch}, d.F2, d.p2, sy, 0.f, ek);
+        else pass_kin<T, SEG, true>(B, A, cols_geom(d.F1, pitch), d.F2, d.p2, sy, T(0), ek);
         __syncthreads();
         pass_ana<T, SEG, true>(A, B, xpose_geom(d.F2, pitch, d.pitchT(d.F2)), d.N1, d.H1, d.p1);   // A_x: F1 -> G1, into B^T
         __syncthreads();
         pass_ana<T, SEG, true>(B, A, xpose_geom(d.G1, d.pitchT(d.F2), pitch), d.N2, d.H2, d.p2);   // A_y: F2 -> G2, into A
         __syncthreads();
-        scatter_plane<T, TO>(A, pitch, L, kz, out_ptr(o, hpsi), accumulate != 0,
-                             MODE == MODE_PRECOND ? sc : nullptr);
+        scatter_plane<T, TO, MODE == MODE_PRECOND>(A, pitch, L, kz, out_ptr(o, hpsi), accumulate != 0,
+                                                   MODE == MODE_PRECOND ? sc : nullptr,
+                                                   dotv ? dotv + o.psi : nullptr, e);
         const double s = block_sum(e, red);
         // slots 0 .. ntx1*nty1-1 belong to the z kernel's chain-1 tiles
         const int slot = ((d.F1 + TX - 1) / TX) * ((d.F2 + TY - 1) / TY) + kz;
@@ -821,20 +898,21 @@ __global__ void __launch_bounds__(NT, plane_min_blocks(sizeof(T) == 4, PERSIST, 
                                                                    const T *__restrict__ scratch, TO *__restrict__ hpsi,
                                                                    double *__restrict__ part_kin, int part_stride,
                                                                    int accumulate, const double *__restrict__ cprec,
-                                                                   T *gtmp, long long gstride)
+                                                                   T *gtmp, long long gstride,
+                                                                   const TO *__restrict__ dotv)
 {
     __shared__ double red[32];
     __shared__ T sc[8];
     if (!PERSIST) {
         k3_item<T, TO, ALLPER, MODE>(lrs, orbs, pre, norb, scratch, hpsi, part_kin, part_stride, accumulate, cprec,
-                                     blockIdx.x, sc, red, nullptr);
+                                     blockIdx.x, sc, red, nullptr, dotv);
         return;
     }
     const int nwork = pre[norb];
     for (int it = blockIdx.x; it < nwork; it += gridDim.x) {
         __syncthreads();  // the previous item is done with A, B, sc and red
         k3_item<T, TO, ALLPER, MODE>(lrs, orbs, pre, norb, scratch, hpsi, part_kin, part_stride, accumulate, cprec,
-                                     it, sc, red, gtmp + (size_t)blockIdx.x * gstride);
+                                     it, sc, red, gtmp + (size_t)blockIdx.x * gstride, dotv);
     }
 }
 
@@ -872,7 +950,7 @@ __global__ void __launch_bounds__(kZThreads) kd_density(const LrDev *__restrict_
                                                         const T *__restrict__ scratch, const double *__restrict__ hfac,
                                                         double *__restrict__ part)
 {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
+    extern __shared__ __align__(128) unsigned char smem_raw[];
     // MAXP accumulators per thread: I3 * TC <= MAXP * kZThreads
     // item = (chunk, tile of the I1 x I2 plane, row-major)
     const int chunk = find_owner(pre, nchunk, blockIdx.x);
@@ -886,7 +964,6 @@ __global__ void __launch_bounds__(kZThreads) kd_density(const LrDev *__restrict_
     const int zl = max(d.G3, max(d.F3, d.I3));
     T *A = reinterpret_cast<T *>(smem_raw);
     T *B = A + zl * TC;
-    constexpr int SEG = Seg<T>::v;
     const int W = d.I1, H = d.I2;
     const size_t plane = (size_t)W * H;
     // thread t owns tile column c = t % TC at z = t / TC + k ZS
@@ -966,21 +1043,37 @@ static __global__ void k_density_reduce(const int *__restrict__ group_chunk_star
 // Batched CG vector kernels (OpenCL/Preconditioner.c:130-195 with per-orbital
 // scalars kept on the device).  Vectors are [psi_c | psi_f] per orbital at
 // off[o], len[o] values; grid.y = orbital, grid.x = chunks of the vector.
+// With VEC the values move 16 bytes per access (a scalar head up to the first
+// 16-byte boundary of the orbital's range, then groups of 16 bytes, then a
+// scalar tail); the launcher takes VEC when every vector of the call starts on
+// a 16-byte boundary, so that all of them split alike.  Each thread's terms
+// and the block sums come in a fixed order: the reductions are deterministic.
 constexpr int kCgChunks = 16;
 
-template <class T>
-__global__ void k_cg_dot(const long long *__restrict__ off, const int *__restrict__ len, const T *__restrict__ x,
-                         const T *__restrict__ y, double *__restrict__ part)
+template <class T> struct alignas(16) Lanes {
+    static constexpr int n = 16 / (int)sizeof(T);
+    T v[n];
+};
+template <class T> __device__ __forceinline__ Lanes<T> ldv(const T *p) { return *reinterpret_cast<const Lanes<T> *>(p); }
+template <class T> __device__ __forceinline__ void stv(T *p, const Lanes<T> &a) { *reinterpret_cast<Lanes<T> *>(p) = a; }
+
+// e(i) for single values, g(i) for the 16-byte group starting at value i
+template <class T, bool VEC, class E1, class EG>
+__device__ __forceinline__ void cg_range(const T *p, int n, E1 &&e, EG &&g)
 {
-    __shared__ double red[32];
-    const int o = blockIdx.y;
-    const long long b = off[o];
-    const int n = len[o];
-    double s = 0.0;
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
-        s += (double)x[b + i] * (double)y[b + i];
-    const double t = block_sum(s, red);
-    if (threadIdx.x == 0) part[o * kCgChunks + blockIdx.x] = t;
+    const int tid = blockIdx.x * blockDim.x + threadIdx.x, nt = gridDim.x * blockDim.x;
+    if constexpr (!VEC) {
+        for (int i = tid; i < n; i += nt) e(i);
+    } else {
+        constexpr int E = Lanes<T>::n;
+        const int mis = (int)((reinterpret_cast<uintptr_t>(p) / sizeof(T)) % E);
+        int head = mis ? E - mis : 0;
+        head = head < n ? head : n;
+        const int nv = (n - head) / E, t0 = head + nv * E;
+        if (tid < head) e(tid);
+        for (int j = tid; j < nv; j += nt) g(head + j * E);
+        for (int i = t0 + tid; i < n; i += nt) e(i);
+    }
 }
 
 // out[o] = sum of its chunk partials (fixed order); optionally copy into hist
@@ -995,30 +1088,42 @@ static __global__ void k_cg_sum(int norb, const double *__restrict__ part, doubl
     if (hist) hist[o] = s;
 }
 
-// r = b - Ax; d = r
-template <class T>
-// r = b - A x, d = r, and the chunk partials of <r|r> (the order of k_cg_dot)
+// r = b - A x and the chunk partials of <r|r> (the first direction d = r is
+// formed by the next K1)
+template <class T, bool VEC>
 __global__ void k_cg_init(const long long *__restrict__ off, const int *__restrict__ len, const T *__restrict__ b,
-                          const T *__restrict__ ax, T *__restrict__ r, T *__restrict__ d, double *__restrict__ part)
+                          const T *__restrict__ ax, T *__restrict__ r, double *__restrict__ part)
 {
     __shared__ double red[32];
     const int o = blockIdx.y;
     const long long base = off[o];
+    const T *bo = b + base, *ao = ax + base;
+    T *ro = r + base;
     double s = 0.0;
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < len[o]; i += gridDim.x * blockDim.x) {
-        const T v = b[base + i] - ax[base + i];
-        r[base + i] = v;
-        d[base + i] = v;
-        s += (double)v * (double)v;
-    }
+    cg_range<T, VEC>(
+        bo, len[o],
+        [&](int i) {
+            const T v = bo[i] - ao[i];
+            ro[i] = v;
+            s += (double)v * (double)v;
+        },
+        [&](int i) {
+            Lanes<T> v = ldv(bo + i);
+            const Lanes<T> a = ldv(ao + i);
+#pragma unroll
+            for (int k = 0; k < Lanes<T>::n; ++k) {
+                v.v[k] -= a.v[k];
+                s += (double)v.v[k] * (double)v.v[k];
+            }
+            stv(ro + i, v);
+        });
     const double t = block_sum(s, red);
     if (threadIdx.x == 0) part[o * kCgChunks + blockIdx.x] = t;
 }
 
-// alpha = rr/dAd; x += alpha d; if (update_r) r -= alpha Ad
-template <class T>
-// x += alpha d, r -= alpha A d, and the chunk partials of the new <r|r>
-// (the order of k_cg_dot)
+// alpha = rr / dAd; x += alpha d, r -= alpha A d, and the chunk partials of
+// the new <r|r>
+template <class T, bool VEC>
 __global__ void k_cg_step(const long long *__restrict__ off, const int *__restrict__ len,
                           const double *__restrict__ rr, const double *__restrict__ dad, T *__restrict__ x,
                           const T *__restrict__ d, T *__restrict__ r, const T *__restrict__ ad,
@@ -1027,28 +1132,32 @@ __global__ void k_cg_step(const long long *__restrict__ off, const int *__restri
     __shared__ double red[32];
     const int o = blockIdx.y;
     const long long base = off[o];
+    T *xo = x + base, *ro = r + base;
+    const T *dn = d + base, *ao = ad + base;
     const T alpha = (T)(rr[o] / dad[o]);
     double s = 0.0;
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < len[o]; i += gridDim.x * blockDim.x) {
-        x[base + i] = fma(alpha, d[base + i], x[base + i]);
-        const T v = fma(-alpha, ad[base + i], r[base + i]);
-        r[base + i] = v;
-        s += (double)v * (double)v;
-    }
+    cg_range<T, VEC>(
+        xo, len[o],
+        [&](int i) {
+            xo[i] = fma(alpha, dn[i], xo[i]);
+            const T v = fma(-alpha, ao[i], ro[i]);
+            ro[i] = v;
+            s += (double)v * (double)v;
+        },
+        [&](int i) {
+            Lanes<T> xv = ldv(xo + i), rv = ldv(ro + i);
+            const Lanes<T> dv = ldv(dn + i), av = ldv(ao + i);
+#pragma unroll
+            for (int k = 0; k < Lanes<T>::n; ++k) {
+                xv.v[k] = fma(alpha, dv.v[k], xv.v[k]);
+                rv.v[k] = fma(-alpha, av.v[k], rv.v[k]);
+                s += (double)rv.v[k] * (double)rv.v[k];
+            }
+            stv(xo + i, xv);
+            stv(ro + i, rv);
+        });
     const double t = block_sum(s, red);
     if (threadIdx.x == 0) part[o * kCgChunks + blockIdx.x] = t;
-}
-
-// beta = rr_new/rr; d = beta d + r; rr = rr_new
-template <class T>
-__global__ void k_cg_dir(const long long *__restrict__ off, const int *__restrict__ len, double *__restrict__ rr,
-                         const double *__restrict__ rr_new, T *__restrict__ d, const T *__restrict__ r)
-{
-    const int o = blockIdx.y;
-    const long long base = off[o];
-    const T beta = (T)(rr_new[o] / rr[o]);
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < len[o]; i += gridDim.x * blockDim.x)
-        d[base + i] = fma(beta, d[base + i], r[base + i]);
 }
 
 static __global__ void k_copy_scalars(int n, const double *__restrict__ a, double *__restrict__ b)
@@ -1057,8 +1166,9 @@ static __global__ void k_copy_scalars(int n, const double *__restrict__ a, doubl
     if (i < n) b[i] = a[i];
 }
 
-// x *= D^-1/2 per component (scale_psi_d, OpenCL/Uncompress.c:596)
-template <class T>
+// x *= D^-1/2 per component (scale_psi_d, OpenCL/Uncompress.c:596): value i
+// is coarse below nvctr_c, else fine component 1 + (i - nvctr_c) % 7
+template <class T, bool VEC>
 __global__ void k_cg_scale(const LrDev *__restrict__ lrs, const OrbDev *__restrict__ orbs,
                            const long long *__restrict__ off, const int *__restrict__ len,
                            const double *__restrict__ cprec, T *__restrict__ x)
@@ -1069,12 +1179,22 @@ __global__ void k_cg_scale(const LrDev *__restrict__ lrs, const OrbDev *__restri
     T sc[8];
 #pragma unroll
     for (int k = 0; k < 8; ++k) sc[k] = (T)prec_scal(L, cprec[o], k);
-    const long long base = off[o];
+    T *xo = x + off[o];
     const int nc = L.nvctr_c;
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < len[o]; i += gridDim.x * blockDim.x) {
-        const int k = i < nc ? 0 : 1 + (i - nc) % 7;
-        x[base + i] *= sc[k];
-    }
+    auto comp = [&](int i) { return i < nc ? 0 : 1 + (i - nc) % 7; };
+    cg_range<T, VEC>(
+        xo, len[o], [&](int i) { xo[i] *= sc[comp(i)]; },
+        [&](int i) {
+            Lanes<T> v = ldv(xo + i);
+            int k = comp(i);
+#pragma unroll
+            for (int j = 0; j < Lanes<T>::n; ++j) {
+                v.v[j] *= sc[k];
+                // the next value's component: coarse until nvctr_c, then 1..7 cyclically
+                k = (i + j + 1 < nc) ? 0 : (k == 0 || k == 7 ? 1 : k + 1);
+            }
+            stv(xo + i, v);
+        });
 }
 
 // ---------------------------------------------------------------------------
@@ -1155,24 +1275,47 @@ static void zmaps(const Plan &p, T *scratch, ZMaps &m)
 // K1 / K3 launch with the plane configuration of the batch
 template <class T, class TI, bool ALLPER, int MODE>
 static cudaError_t run_k1(const Plan &p, const PlaneCfg &pc, const TI *psi, T *scratch, const double *cprec, T *gtmp,
-                          cudaStream_t st)
+                          cudaStream_t st, CgIo<T> cg = CgIo<T>{nullptr, nullptr, nullptr, nullptr, 0})
 {
     cudaError_t err;
     auto k = k1_for<T, TI, ALLPER, MODE>(pc);
     if ((err = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pc.smem))) return err;
-    k<<<pc.grid, pc.threads, pc.smem, st>>>(p.d_lr, p.d_orb, p.d_pre13, p.norb, psi, scratch, cprec, gtmp, pc.gstride);
+    k<<<pc.grid, pc.threads, pc.smem, st>>>(p.d_lr, p.d_orb, p.d_pre13, p.norb, psi, scratch, cprec, gtmp, pc.gstride,
+                                            cg);
     return cudaSuccess;
 }
 
 template <class T, class TO, bool ALLPER, int MODE>
 static cudaError_t run_k3(const Plan &p, const PlaneCfg &pc, const T *scratch, TO *out, double *part_kin,
-                          int part_stride, int accumulate, const double *cprec, T *gtmp, cudaStream_t st)
+                          int part_stride, int accumulate, const double *cprec, T *gtmp, cudaStream_t st,
+                          const TO *dotv = nullptr)
 {
     cudaError_t err;
     auto k = k3_for<T, TO, ALLPER, MODE>(pc);
     if ((err = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pc.smem))) return err;
     k<<<pc.grid, pc.threads, pc.smem, st>>>(p.d_lr, p.d_orb, p.d_pre13, p.norb, scratch, out, part_kin, part_stride,
-                                            accumulate, cprec, gtmp, pc.gstride);
+                                            accumulate, cprec, gtmp, pc.gstride, dotv);
+    return cudaSuccess;
+}
+
+// K2 launch with the block size zt (FP32: 256, 320 or 384; FP64: 256)
+template <class T, class TV, bool ALLPER, int CHAIN>
+static cudaError_t run_k2(int zt, int nwork, size_t sm2, const Plan &p, const int *pre, const TV *pot, T *scratch,
+                          double *part_pot, double *part_kin, int part_stride, const CUtensorMap &m_in,
+                          const CUtensorMap &m_out, int tma, cudaStream_t st)
+{
+    auto k = k2_zpencil<T, TV, ALLPER, CHAIN, kZThreads>;
+    if constexpr (sizeof(T) == 4) {
+        if (zt == 320) k = k2_zpencil<T, TV, ALLPER, CHAIN, 320>;
+        else if (zt == 384) k = k2_zpencil<T, TV, ALLPER, CHAIN, 384>;
+        else zt = kZThreads;
+    } else {
+        zt = kZThreads;
+    }
+    cudaError_t err;
+    if ((err = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm2))) return err;
+    k<<<nwork, zt, sm2, st>>>(p.d_lr, p.d_orb, pre, p.norb, pot, scratch, part_pot, part_kin, part_stride, m_in,
+                              m_out, tma);
     return cudaSuccess;
 }
 
@@ -1196,10 +1339,6 @@ static cudaError_t launch_locham_bc(const Plan &p, const TIO *psi, const TIO *po
     const size_t sm2 = p.smem2[fp] + kZExtra;
     T *gtmp = pc.global_b ? scratch + p.scratch_elems : nullptr;
     cudaError_t err;
-    auto k2 = k2_zpencil<T, TIO, ALLPER, 0>;
-    auto k2k = k2_zpencil<T, TIO, ALLPER, 1>;
-    if ((err = cudaFuncSetAttribute(k2, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm2))) return err;
-    if ((err = cudaFuncSetAttribute(k2k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm2))) return err;
     cudaMemsetAsync(part_pot, 0, sizeof(double) * (size_t)p.norb * p.part_stride, st);
     cudaMemsetAsync(part_kin, 0, sizeof(double) * (size_t)p.norb * p.part_stride, st);
     ZMaps zm;
@@ -1208,10 +1347,11 @@ static cudaError_t launch_locham_bc(const Plan &p, const TIO *psi, const TIO *po
     if (ev) cudaEventRecord(ev[0], st);
     if ((err = run_k1<T, TIO, ALLPER, MODE_LOCHAM>(p, pc, psi, scratch, nullptr, gtmp, st))) return err;
     if (ev) cudaEventRecord(ev[1], st);
-    k2<<<p.n_work2, kZThreads, sm2, st>>>(p.d_lr, p.d_orb, p.d_pre2, p.norb, pot, scratch, part_pot, part_kin,
-                                          p.part_stride, zm.q, zm.q, zm.ok);
-    k2k<<<p.n_work2p, kZThreads, sm2, st>>>(p.d_lr, p.d_orb, p.d_pre2p, p.norb, pot, scratch, part_pot, part_kin,
-                                            p.part_stride, zm.p, zm.z, zm.ok);
+    if ((err = run_k2<T, TIO, ALLPER, 0>(p.z_threads[fp], p.n_work2, sm2, p, p.d_pre2, pot, scratch, part_pot,
+                                         part_kin, p.part_stride, zm.q, zm.q, zm.ok, st)) ||
+        (err = run_k2<T, TIO, ALLPER, 1>(p.z_threads[fp], p.n_work2p, sm2, p, p.d_pre2p, pot, scratch, part_pot,
+                                         part_kin, p.part_stride, zm.p, zm.z, zm.ok, st)))
+        return err;
     if (ev) cudaEventRecord(ev[2], st);
     if ((err = run_k3<T, TIO, ALLPER, MODE_LOCHAM>(p, pc, scratch, hpsi, part_kin, p.part_stride, accumulate, nullptr,
                                                    gtmp, st)))
@@ -1281,59 +1421,90 @@ template cudaError_t launch_locden<double>(const Plan &, const double *, const d
                                            double *, cudaStream_t);
 #endif
 
-// preconditioner operator y = D^-1/2 A (c + T) S D^-1/2 x for every orbital
+// preconditioner operator y = D^-1/2 A (c + T) S D^-1/2 x for every orbital;
+// cg.dir: x is the CG direction, formed by K1 (see CgIo); dotpart: K3's
+// partials of <x | y> per plane (zeroed here first), or null
 template <class T, bool ALLPER>
 static cudaError_t launch_prec_apply_bc(const Plan &p, const T *x, T *y, const double *cprec, T *scratch,
-                                        cudaStream_t st)
+                                        cudaStream_t st, const CgIo<T> &cg, double *dotpart)
 {
     const int fp = sizeof(T) == 8 ? 1 : 0;
-    const PlaneCfg pc = plane_cfg(p, fp, p.n_work13);
+    PlaneCfg pc = plane_cfg(p, fp, p.n_work13);
+    if (!pc.global_b) pc.threads = p.plane_threads_pre[fp];
     const size_t sm2 = p.smem2[fp] + kZExtra;
     T *gtmp = pc.global_b ? scratch + p.scratch_elems : nullptr;
     cudaError_t err;
-    auto k2 = k2_zpencil<T, T, ALLPER, 1>;
-    if ((err = cudaFuncSetAttribute(k2, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm2))) return err;
-    if ((err = run_k1<T, T, ALLPER, MODE_PRECOND>(p, pc, x, scratch, cprec, gtmp, st))) return err;
+    if ((err = run_k1<T, T, ALLPER, MODE_PRECOND>(p, pc, x, scratch, cprec, gtmp, st, cg))) return err;
     ZMaps zm;
     zmaps(p, scratch, zm);
-    k2<<<p.n_work2p, kZThreads, sm2, st>>>(p.d_lr, p.d_orb, p.d_pre2p, p.norb, (const T *)nullptr, scratch,
-                                           nullptr, nullptr, 0, zm.p, zm.z, zm.ok);
-    if ((err = run_k3<T, T, ALLPER, MODE_PRECOND>(p, pc, scratch, y, nullptr, 0, 0, cprec, gtmp, st))) return err;
+    if ((err = run_k2<T, T, ALLPER, 1>(p.z_threads_pre[fp], p.n_work2p, sm2, p, p.d_pre2p, (const T *)nullptr, scratch,
+                                       nullptr, nullptr, 0, zm.p, zm.z, zm.ok, st)))
+        return err;
+    if (dotpart) cudaMemsetAsync(dotpart, 0, sizeof(double) * (size_t)p.norb * p.part_stride, st);
+    if ((err = run_k3<T, T, ALLPER, MODE_PRECOND>(p, pc, scratch, y, dotpart, dotpart ? p.part_stride : 0, 0, cprec,
+                                                  gtmp, st, dotpart ? x : nullptr)))
+        return err;
+    return cudaGetLastError();
+}
+
+// out[o] = the sum of orbital o's stride partial slots, in slot order
+static __global__ void k_cg_sum_slots(int norb, const double *__restrict__ part, int stride, double *__restrict__ out)
+{
+    const int o = blockIdx.x * blockDim.x + threadIdx.x;
+    if (o >= norb) return;
+    double s = 0.0;
+    for (int k = 0; k < stride; ++k) s += part[(size_t)o * stride + k];
+    out[o] = s;
+}
+
+static bool aligned16(const void *p) { return !(reinterpret_cast<uintptr_t>(p) & 15); }
+
+// The recurrence of Preconditioner.c:130-195 with two of its vector passes
+// folded into the operator's kernels: K1 forms the direction
+// d = r / d = beta d + r while gathering it, K3 accumulates <d | A d> while
+// scattering A d.  Per iteration: apply (K1, K2, K3), alpha = rr / dAd, the
+// x and r updates with the new <r|r> (k_cg_step), then rr <- rr_new once
+// the next K1 has read both.
+template <class T, bool VEC, class Apply>
+static cudaError_t cg_loop(const Plan &p, int ncong, const double *cprec, T *x, const T *b, T *r, T *dvec, T *ad,
+                           double *rr, double *dad, double *rrn, double *part, double *dotpart, double *hist,
+                           Apply &&apply, cudaStream_t st)
+{
+    const dim3 vg(kCgChunks, p.norb);
+    const int sg = (p.norb + 127) / 128;
+    cudaError_t err;
+    if ((err = apply(x, ad, CgIo<T>{nullptr, nullptr, nullptr, nullptr, 0}, nullptr))) return err;
+    k_cg_init<T, VEC><<<vg, 256, 0, st>>>(p.d_orb_off, p.d_orb_len, b, ad, r, part);
+    k_cg_sum<<<sg, 128, 0, st>>>(p.norb, part, rr, hist);
+    for (int it = 0; it < ncong; ++it) {
+        if ((err = apply(dvec, ad, CgIo<T>{dvec, r, rr, rrn, it == 0 ? 1 : 2}, dotpart))) return err;
+        if (it > 0) k_copy_scalars<<<sg, 128, 0, st>>>(p.norb, rrn, rr);
+        k_cg_sum_slots<<<sg, 128, 0, st>>>(p.norb, dotpart, p.part_stride, dad);
+        k_cg_step<T, VEC><<<vg, 256, 0, st>>>(p.d_orb_off, p.d_orb_len, rr, dad, x, dvec, r, ad, part);
+        k_cg_sum<<<sg, 128, 0, st>>>(p.norb, part, rrn, hist ? hist + (size_t)(it + 1) * p.norb : nullptr);
+    }
+    k_cg_scale<T, VEC><<<vg, 256, 0, st>>>(p.d_lr, p.d_orb, p.d_orb_off, p.d_orb_len, cprec, x);
     return cudaGetLastError();
 }
 
 // Batched CG of ocl_preconditioner_generic: x (in: initial guess, out:
-// preconditioned), b right-hand side; work: r, d, ad vectors; scal: 5*norb
-// doubles + kCgChunks*norb partials; hist (optional): (ncong+1)*norb squared
-// residual norms, entry 0 the initial one.
+// preconditioned), b right-hand side; work: r, d, ad vectors; scal:
+// (5 + kCgChunks + part_stride) * norb doubles (scalars, chunk partials of
+// the vector kernels, K3's per-plane partials of <d|Ad>); hist (optional):
+// (ncong+1)*norb squared residual norms, entry 0 the initial one.
 template <class T>
 cudaError_t launch_precond(const Plan &p, int ncong, const double *cprec, T *x, const T *b, T *r, T *dvec, T *ad,
                            T *scratch, double *scal, double *hist, cudaStream_t st)
 {
     double *rr = scal, *dad = scal + p.norb, *rrn = scal + 2 * p.norb, *part = scal + 5 * p.norb;
-    const dim3 vg(kCgChunks, p.norb);
-    auto apply = [&](const T *in, T *out) {
-        return p.all_periodic ? launch_prec_apply_bc<T, true>(p, in, out, cprec, scratch, st)
-                              : launch_prec_apply_bc<T, false>(p, in, out, cprec, scratch, st);
+    double *dotpart = part + (size_t)kCgChunks * p.norb;
+    auto apply = [&](const T *in, T *out, const CgIo<T> &cg, double *dp) {
+        return p.all_periodic ? launch_prec_apply_bc<T, true>(p, in, out, cprec, scratch, st, cg, dp)
+                              : launch_prec_apply_bc<T, false>(p, in, out, cprec, scratch, st, cg, dp);
     };
-    cudaError_t err;
-    if ((err = apply(x, ad))) return err;
-    k_cg_init<T><<<vg, 256, 0, st>>>(p.d_orb_off, p.d_orb_len, b, ad, r, dvec, part);
-    k_cg_sum<<<(p.norb + 127) / 128, 128, 0, st>>>(p.norb, part, rr, hist);
-    for (int it = 0; it < ncong; ++it) {
-        if ((err = apply(dvec, ad))) return err;
-        k_cg_dot<T><<<vg, 256, 0, st>>>(p.d_orb_off, p.d_orb_len, dvec, ad, part);
-        k_cg_sum<<<(p.norb + 127) / 128, 128, 0, st>>>(p.norb, part, dad, nullptr);
-        k_cg_step<T><<<vg, 256, 0, st>>>(p.d_orb_off, p.d_orb_len, rr, dad, x, dvec, r, ad, part);
-        k_cg_sum<<<(p.norb + 127) / 128, 128, 0, st>>>(p.norb, part, rrn,
-                                                      hist ? hist + (size_t)(it + 1) * p.norb : nullptr);
-        if (it != ncong - 1) {
-            k_cg_dir<T><<<vg, 256, 0, st>>>(p.d_orb_off, p.d_orb_len, rr, rrn, dvec, r);
-            k_copy_scalars<<<(p.norb + 127) / 128, 128, 0, st>>>(p.norb, rrn, rr);
-        }
-    }
-    k_cg_scale<T><<<vg, 256, 0, st>>>(p.d_lr, p.d_orb, p.d_orb_off, p.d_orb_len, cprec, x);
-    return cudaGetLastError();
+    const bool vec = aligned16(x) && aligned16(b) && aligned16(r) && aligned16(dvec) && aligned16(ad);
+    return vec ? cg_loop<T, true>(p, ncong, cprec, x, b, r, dvec, ad, rr, dad, rrn, part, dotpart, hist, apply, st)
+               : cg_loop<T, false>(p, ncong, cprec, x, b, r, dvec, ad, rr, dad, rrn, part, dotpart, hist, apply, st);
 }
 #ifdef WVLH_FUSED_F32
 template cudaError_t launch_precond<float>(const Plan &, int, const double *, float *, const float *, float *, float *,

@@ -150,6 +150,9 @@ struct Plan {
     long long plane_elems = 0;     // elements of plane buffer A (rows x pitch)
     long long planeB_elems = 0;    // elements of buffer B (a plane or a transposed plane)
     int plane_threads[2] = {kPlaneThreads, kPlaneThreads};   // plane-kernel CTA size (float, double)
+    int plane_threads_pre[2] = {kPlaneThreads, kPlaneThreads};   // the same for the preconditioner operator
+    int z_threads[2] = {kZThreads, kZThreads};       // z-kernel CTA size (FP32: 256, 320 or 384)
+    int z_threads_pre[2] = {kZThreads, kZThreads};   // the same for the preconditioner operator
     size_t smem2[2] = {0, 0};
     int pitch_max = 0, rows_max = 0, zlen_max = 0;
     // scratch elements per orbital when every orbital lies in one region (the

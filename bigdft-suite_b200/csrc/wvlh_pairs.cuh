@@ -234,13 +234,20 @@ __device__ __forceinline__ void pass2_kin(const float *src, float *dst, const Pa
     constexpr int NLAG = kKinLags;
     const float scale = (float)scale_d;
     const int nseg = (L + SEG - 1) / SEG;
+    // interior segments (window inside the line, all outputs in it) take
+    // plain loads and no per-output tests; the others wrap or zero-pad
+    auto interior = [&](int s) {
+        const int p0 = s * SEG - 14;
+        return p0 >= 0 && p0 + W <= L;
+    };
     double e = 0.0;
-    for_items(g.npairs, nseg, [&](int lp, int s) {
+    for_items2(g.npairs, nseg, interior, [&](int lp, int s, auto int_t) {
+        constexpr bool INT = decltype(int_t)::value;
         const float *in = src + 2 * lp;
         const int q0 = s * SEG;
         const int p0 = q0 - 14;
-        const bool interior = p0 >= 0 && p0 + W <= L;
-        const int nout = min(SEG, L - q0);
+        const int nout = INT ? SEG : min(SEG, L - q0);
+        const float *b = in + p0 * g.src_ps;
         float2 conv[SEG], lag[NLAG], hist[NLAG];
 #pragma unroll
         for (int t = 0; t < SEG; ++t) conv[t] = P::zero();
@@ -248,7 +255,7 @@ __device__ __forceinline__ void pass2_kin(const float *src, float *dst, const Pa
         for (int l = 0; l < NLAG; ++l) lag[l] = P::zero();
 #pragma unroll
         for (int k = 0; k < W; ++k) {
-            const float2 x = load_point2(in, g.src_ps, p0 + k, L, per, interior);
+            const float2 x = INT ? ld2(b + k * g.src_ps) : load_point2(in, g.src_ps, p0 + k, L, per, false);
 #pragma unroll
             for (int t = 0; t < SEG; ++t) {
                 const int l = k - 14 - t;   // tap offset of this value for output t
@@ -258,7 +265,7 @@ __device__ __forceinline__ void pass2_kin(const float *src, float *dst, const Pa
             for (int j = NLAG - 1; j > 0; --j) hist[j] = hist[j - 1];
             hist[0] = x;
             // outputs of this segment: window positions 14 .. 14 + nout - 1
-            if (k >= 14 && k < 14 + SEG && k - 14 < nout) {
+            if (k >= 14 && k < 14 + SEG && (INT || k - 14 < nout)) {
 #pragma unroll
                 for (int l = 0; l < NLAG; ++l) lag[l] = P::fmav(x, hist[l], lag[l]);
             }
@@ -266,7 +273,7 @@ __device__ __forceinline__ void pass2_kin(const float *src, float *dst, const Pa
         float2 es = P::zero();
 #pragma unroll
         for (int t = 0; t < SEG; ++t) {
-            if (t < nout) {
+            if (INT || t < nout) {
                 const int q = q0 + t;
                 const float2 xq = ld2(in + q * g.src_ps);
                 es = P::fmav(xq, conv[t], es);

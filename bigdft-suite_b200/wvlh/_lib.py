@@ -84,6 +84,8 @@ WVLH_SYMBOLS = [
     "wvlh_locham_graph_create", "wvlh_graph_launch", "wvlh_graph_destroy",
     "wvlh_nlpsp_create", "wvlh_nlpsp_apply", "wvlh_nlpsp_destroy", "wvlh_subspace_matrix", "wvlh_panel_apply",
     "wvlh_batch_autotune",
+    "wvlh_batch_autotune_precond",
+    "wvlh_batch_block_sizes",
     "wvlh_psolver_periodic",
     "wvlh_xc_lda",
     "wvlh_ks_potential_periodic",
@@ -158,6 +160,9 @@ def lib():
     L.wvlh_subspace_matrix.argtypes = [vp, C.c_int, C.c_int, C.c_int64, C.c_int64, vp, vp, vp]
     L.wvlh_batch_autotune.argtypes = [vp, C.c_int, vp, vp, vp, vp, vp, C.c_int, C.POINTER(C.c_int),
                                       C.POINTER(C.c_int), C.POINTER(C.c_double), C.POINTER(C.c_int)]
+    L.wvlh_batch_block_sizes.argtypes = [vp, C.POINTER(C.c_int)]
+    L.wvlh_batch_autotune_precond.argtypes = [vp, C.c_int, C.c_int, vp, vp, vp, C.c_int, C.POINTER(C.c_int), vp,
+                                              vp, C.POINTER(C.c_int)]
     L.wvlh_panel_apply.argtypes = [vp, C.c_int, C.c_int64, C.c_int64, vp, C.c_int, C.c_double, vp, C.c_double, vp]
     L.wvlh_psolver_periodic.argtypes = [vp, C.POINTER(C.c_int), C.POINTER(C.c_double), vp, vp, C.c_double, vp]
     L.wvlh_xc_lda.argtypes = [vp, C.c_int64, vp, vp, C.c_int, C.c_double, vp]

@@ -141,6 +141,31 @@ class Batch:
                                         int(reps), C.byref(chosen), cand, ms, C.byref(n)), "wvlh_batch_autotune")
         return chosen.value, {int(cand[k]): float(ms[k]) for k in range(n.value)}
 
+    def autotune_precond(self, x, rhs, cprec, ncong, reps=2):
+        """Measure the plane kernels' block sizes on this batch's
+        preconditioner (wvlh_batch_autotune_precond: ncong CG iterations per
+        timed call; x is overwritten) and keep the fastest; returns (chosen,
+        {block size: ms per call})."""
+        torch = self.ctx.torch
+        prec = {torch.float32: 32, torch.float64: 64}.get(x.dtype)
+        if prec is None or rhs.dtype != x.dtype:
+            raise WvlhError("x and rhs must both be float32 or float64")
+        c = torch.as_tensor(cprec, dtype=torch.float64, device=x.device).contiguous()
+        chosen, n = C.c_int(), C.c_int()
+        cand, ms = (C.c_int * 5)(), (C.c_double * 5)()
+        check(lib().wvlh_batch_autotune_precond(self.h, prec, int(ncong), _ptr(c), _ptr(x), _ptr(rhs), int(reps),
+                                                C.byref(chosen), cand, ms, C.byref(n)),
+              "wvlh_batch_autotune_precond")
+        return chosen.value, {int(cand[k]): float(ms[k]) for k in range(n.value)}
+
+    def block_sizes(self):
+        """The CTA sizes the batch launches with (wvlh_batch_block_sizes):
+        {"locham": {"plane": (fp32, fp64), "z": (fp32, fp64)}, "precond": ...}."""
+        v = (C.c_int * 8)()
+        check(lib().wvlh_batch_block_sizes(self.h, v), "wvlh_batch_block_sizes")
+        return {"locham": {"plane": (v[0], v[1]), "z": (v[2], v[3])},
+                "precond": {"plane": (v[4], v[5]), "z": (v[6], v[7])}}
+
     def locham_graph(self, psi, pot, hpsi, ekin, epot, accumulate=False):
         """Capture locham(psi, pot, hpsi, ekin, epot) into a CUDA graph; replay
         it with .launch() (the tensors must stay alive and in place)."""

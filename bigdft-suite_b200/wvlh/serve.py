@@ -401,9 +401,24 @@ class Server:
 
 
 def latency_stats(reqs):
-    """p50 / p99 / mean latency (ms) and served coarse cells of completed requests."""
-    lat = np.array([r.latency for r in reqs if r.latency is not None]) * 1e3
-    if len(lat) == 0:
+    """p50 / p99 / mean latency (ms) of completed requests, split into the
+    time queued before their launch and the time from launch to completion
+    (kernels, plus any launch of the other slot ahead of them on the
+    device); "tail" gives the mean of both parts and the mean orbital count
+    over the requests at or above the p99 latency, against all requests."""
+    done = [r for r in reqs if r.latency is not None]
+    if not done:
         return {"n": 0}
-    return {"n": int(len(lat)), "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
-            "mean_ms": float(lat.mean()), "max_ms": float(lat.max())}
+    lat = np.array([r.latency for r in done]) * 1e3
+    wait = np.array([r.t_launch - r.t_arrival for r in done]) * 1e3
+    run = lat - wait
+    norb = np.array([r.client.norb for r in done], dtype=float)
+    p99 = float(np.percentile(lat, 99))
+    top = lat >= p99
+    return {"n": int(len(lat)), "p50_ms": float(np.percentile(lat, 50)), "p99_ms": p99,
+            "mean_ms": float(lat.mean()), "max_ms": float(lat.max()),
+            "queued_p50_ms": float(np.percentile(wait, 50)), "queued_p99_ms": float(np.percentile(wait, 99)),
+            "launched_p50_ms": float(np.percentile(run, 50)), "launched_p99_ms": float(np.percentile(run, 99)),
+            "tail": {"requests": int(top.sum()), "queued_mean_ms": float(wait[top].mean()),
+                     "launched_mean_ms": float(run[top].mean()), "orbitals_mean": float(norb[top].mean()),
+                     "orbitals_mean_all": float(norb.mean())}}

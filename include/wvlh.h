@@ -527,6 +527,18 @@ int wvlh_ks_potential_spin(wvlh_ctx *ctx, int free_bc, const int n[3], const dou
  * many were timed. */
 int wvlh_batch_autotune(wvlh_batch *batch, int precision, const void *psi, const void *pot, void *hpsi,
                         double *ekin, double *epot, int reps, int *chosen, int *cand, double *ms, int *ncand);
+/* The same measured choice for the preconditioner operator of
+ * wvlh_precond_batched (ncong CG iterations per timed call on the caller's
+ * x and rhs; x is overwritten), kept apart from the local Hamiltonian's: the
+ * preconditioner's plane kernels run fewer passes per plane.  Packed batches
+ * only, as wvlh_precond_batched. */
+int wvlh_batch_autotune_precond(wvlh_batch *batch, int precision, int ncong, const double *cprec, void *x,
+                                const void *rhs, int reps, int *chosen, int *cand, double *ms, int *ncand);
+/* The block sizes the batch launches with: {plane kernels FP32, FP64, z kernel
+ * FP32, FP64} of the local Hamiltonian (its plane sizes serve the density as
+ * well), then the same four of the preconditioner.  The autotuners above also time the FP32 z kernel's
+ * sizes (256, 320, 384) after the plane kernels' pick. */
+int wvlh_batch_block_sizes(const wvlh_batch *batch, int *sizes8);
 /* FP64, one kernel per 1D pass (the OpenCL backend's structure) */
 int wvlh_locham_plain_batched(wvlh_batch *batch, const double *psi, const double *pot, double *hpsi,
                               double *ekin, double *epot);

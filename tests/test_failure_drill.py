@@ -55,7 +55,7 @@ def _worker(rank, world, port, sport, leaver, mode, out):
 @pytest.mark.parametrize("world,leaver", [(2, 1), (3, 2)])
 def test_rank_leaving_between_steps_is_reported(world, leaver):
     import torch.distributed as dist
-    mgr = mp.Manager()
+    mgr = mp.get_context("spawn").Manager()
     out = mgr.dict()
     sport = _free_port()
     server = dist.TCPStore("127.0.0.1", sport, is_master=True, wait_for_workers=False,
@@ -76,7 +76,7 @@ def test_collective_waiting_for_a_dead_rank_times_out():
     """Without the monitor the survivor enters the step's all-reduce; the
     process group's 4 s timeout ends it with an error on the host."""
     import torch.distributed as dist
-    mgr = mp.Manager()
+    mgr = mp.get_context("spawn").Manager()
     out = mgr.dict()
     sport = _free_port()
     server = dist.TCPStore("127.0.0.1", sport, is_master=True, wait_for_workers=False,

@@ -131,3 +131,34 @@ def test_density_long_z_pencils(oracle, torch_cuda, wctx, dtype_name, tol):
     for o in range(3):
         ref = oracle.locden(desc(oracle, lr), rows[o][:lr.nvctr_c], rows[o][lr.nvctr_c:], hfac[o], ref)
     assert rel(rho.cpu().numpy(), ref) < tol
+
+
+@pytest.mark.parametrize("dtype_name", ["float64", "float32"])
+def test_precond_autotune_keeps_results(torch_cuda, wctx, dtype_name):
+    """wvlh_batch_autotune_precond times each compiled block size of the plane
+    kernels on the batch's own preconditioner and keeps the fastest; the
+    preconditioned vectors depend on the pick only through the summation order
+    of <d|Ad>, which K3 accumulates per thread while it scatters A d."""
+    torch = torch_cuda
+    lrs = [region((10, 9, 11), (1, 1, 1), 5), region((7, 8, 6), (0, 0, 0), 6)]
+    orb_lr = np.array([0, 1, 0], np.int32)
+    b = Batch(wctx, lrs, orb_lr)
+    rng = np.random.default_rng(12)
+    cprec = np.array([0.8, 1.1, 0.6])
+    dt = getattr(torch, dtype_name)
+    rhs = torch.tensor(rng.uniform(-1, 1, b.psi_size), dtype=dt, device="cuda")
+    x0, h0 = b.precond(rhs.clone(), rhs, cprec, 3)
+    x0, h0 = x0.clone(), h0.clone()
+    pick, times = b.autotune_precond(rhs.clone(), rhs, cprec, 3, reps=1)
+    assert pick in times and len(times) >= 4 and all(t > 0 for t in times.values())
+    bs = b.block_sizes()["precond"]
+    assert bs["plane"][0 if dtype_name == "float32" else 1] == pick and bs["z"][0] in (256, 320, 384)
+    x1, h1 = b.precond(rhs.clone(), rhs, cprec, 3)
+    torch.cuda.synchronize()
+    tol = 1e-13 if dtype_name == "float64" else 1e-5
+    assert ((x1.double() - x0.double()).norm() / x0.double().norm()).item() <= tol
+    assert ((h1 - h0).abs() / h0.abs()).max().item() <= 10 * tol
+    x2, h2 = b.precond(rhs.clone(), rhs, cprec, 3)
+    torch.cuda.synchronize()
+    assert torch.equal(x2, x1) and torch.equal(h2, h1)   # deterministic for a given block size
+    b.close()

@@ -228,8 +228,10 @@ def test_fp64_large_planes_match_oracle(oracle, torch_cuda, wctx, N, per, dens):
 @pytest.mark.parametrize("dtype_name,tol", [("float64", 1e-13), ("float32", 1e-6)])
 def test_autotune_times_every_block_size_and_keeps_results(oracle, torch_cuda, wctx, dtype_name, tol):
     """wvlh_batch_autotune times each compiled block size of the plane kernels
-    on the batch's own locham and keeps the fastest; the result does not
-    depend on the pick (beyond the energies' summation order)."""
+    (then, FP32, of the z kernel) on the batch's own locham and keeps the
+    fastest; Hpsi does not depend on the pick, the energies only through their
+    summation order (FP32: the z kernel's per-thread partial sums of E_pot
+    change with its block size, an FP32-rounding difference)."""
     torch = torch_cuda
     lrs = [case((12, 10, 9), (0, 0, 0), 0.6, seed=1)[0], case((10, 11, 12), (1, 1, 1), 0.5, seed=2)[0]]
     rng = np.random.default_rng(4)
@@ -241,8 +243,12 @@ def test_autotune_times_every_block_size_and_keeps_results(oracle, torch_cuda, w
     h0, e0, p0 = h0.clone(), e0.clone(), p0.clone()
     pick, times = b.autotune(psi, pot, reps=1)
     assert pick in times and len(times) >= 4 and all(t > 0 for t in times.values())
+    bs = b.block_sizes()["locham"]
+    assert bs["plane"][0 if dtype_name == "float32" else 1] == pick
+    assert bs["z"][0] in (256, 320, 384) and bs["z"][1] == 256
     h1, e1, p1 = b.locham(psi, pot)
     torch.cuda.synchronize()
     assert ((h1 - h0).norm() / h0.norm()).item() <= tol
-    assert ((e1 - e0).abs() / e0.abs()).max().item() <= 1e-12 and ((p1 - p0).abs() / p0.abs()).max().item() <= 1e-12
+    etol = 1e-12 if dtype_name == "float64" else 1e-7
+    assert ((e1 - e0).abs() / e0.abs()).max().item() <= etol and ((p1 - p0).abs() / p0.abs()).max().item() <= etol
     b.close()

@@ -189,6 +189,8 @@ def test_poisson_replay_completes(torch_cuda):
     reqs = srv.replay(poisson_arrivals(5e4, 60, len(cl), seed=3))
     st = latency_stats(reqs)
     assert st["n"] == 60 and 0 < st["p50_ms"] <= st["p99_ms"]
+    assert 0 <= st["queued_p50_ms"] <= st["queued_p99_ms"] and 0 < st["launched_p50_ms"] <= st["launched_p99_ms"]
+    assert st["tail"]["requests"] >= 1 and st["tail"]["orbitals_mean"] > 0
     assert srv.launches < 60   # requests were batched
     srv.close()
 

@@ -48,7 +48,7 @@ def _worker(rank, world, port, out):
 
 @pytest.mark.parametrize("world", [2, 3])
 def test_energy_and_density_exchanges(world):
-    mgr = mp.Manager()
+    mgr = mp.get_context("spawn").Manager()
     out = mgr.dict()
     mp.spawn(_worker, args=(world, _free_port(), out), nprocs=world, join=True)
     data = [_rank_data(r) for r in range(world)]
@@ -110,7 +110,7 @@ def _ov_worker(rank, world, port, out):
 
 @pytest.mark.parametrize("world", [2, 3])
 def test_overlap_transposition_and_allreduce(world):
-    mgr = mp.Manager()
+    mgr = mp.get_context("spawn").Manager()
     out = mgr.dict()
     mp.spawn(_ov_worker, args=(world, _free_port(), out), nprocs=world, join=True)
     psi = _ov_psi(world).numpy()
