@@ -337,6 +337,10 @@ def leg_free_regions(torch, ctx, dev, nlr=1024, seed=2):
     tuned = {nm: b.autotune(ps, pt, hh, e[0], e[1], reps=1)[0]
              for nm, ps, pt, hh in (("fp32", psi32, pot32, h32), ("fp64", psi64, pot64, h64))}
     ms32 = _timed(torch, lambda: b.locham(psi32, pot32, h32, e[0], e[1]), 5)
+    # the same call captured once into a CUDA graph and replayed (one launch a step)
+    gr = b.locham_graph(psi32, pot32, h32, e[0], e[1])
+    ms32_graph = _timed(torch, gr.launch, 5)
+    gr.close()
     ms64 = _timed(torch, lambda: b.locham(psi64, pot64, h64, e[2], e[3]), 3)
     de = max((e[0] - e[2]).abs().max().item(), (e[1] - e[3]).abs().max().item())
     ms_plain = _timed(torch, lambda: b.locham_plain(psi64, pot64, h64, e[2], e[3]), 1)
@@ -354,7 +358,8 @@ def leg_free_regions(torch, ctx, dev, nlr=1024, seed=2):
                                 [e[k + 1][o].item() for o in sample])
     out = {"workload": "%d free-BC regions, coarse 20..40 per dim, fine ellipsoid 0.4, 1 orbital each" % nlr,
            "err_vs_oracle": err, "plane_threads_measured": tuned,
-           "coarse_cells": int(cells), "fp32_fused": {"value": cells / (ms32 * 1e-3), "ms": ms32},
+           "coarse_cells": int(cells), "fp32_fused": {"value": cells / (ms32 * 1e-3), "ms": ms32,
+                                                      "graph_replay_ms": ms32_graph},
            "fp64_fused": {"value": cells / (ms64 * 1e-3), "ms": ms64},
            "fp64_plain": {"value": cells / (ms_plain * 1e-3), "ms": ms_plain},
            "speedup_fp32_vs_fp64_plain": ms_plain / ms32, "energy_err_ha_fp32_vs_fp64": de}
@@ -388,11 +393,12 @@ def leg_precond(torch, ctx, dev, n=40, norb=512, ncong=5, seed=3):
     for nm, x, r in (("fp32", x32, r32), ("fp64", x64, r64)):
         # measured block size of the preconditioner's plane kernels (untimed)
         pick, by_size = b.autotune_precond(x, r, cprec, ncong, reps=1)
+        zpick = b.block_sizes()["precond"]["z"][0 if nm == "fp32" else 1]
         ms = _timed(torch, lambda: run(x, r), 3)
         _, hist = run(x, r)
         torch.cuda.synchronize()
         res[nm] = {"ms": ms, "value": norb * lr.coarse_cells / (ms * 1e-3), "hist": hist.cpu().numpy(),
-                   "plane_threads": pick, "ms_by_block_size": by_size}
+                   "plane_threads": pick, "z_threads": zpick, "ms_by_block_size": by_size}
     h32, h64 = res["fp32"].pop("hist"), res["fp64"].pop("hist")
     rel = np.abs(h32 - h64) / np.abs(h64)
     # two orbitals through the oracle's CG (x0 = b = r): x relative L2 and the
@@ -784,7 +790,8 @@ def main():
     for nm, ps, pt in (("fp32", psi32, pot32), ("fp64", psi64, pot64)):
         hh = torch.empty_like(ps)
         pick, times = batch.autotune(ps, pt, hh, ek, ep, reps=2)
-        tuned[nm] = {"plane_threads": pick, "ms_by_block_size": times}
+        tuned[nm] = {"plane_threads": pick, "ms_by_block_size": times,
+                     "z_threads": batch.block_sizes()["locham"]["z"][0 if nm == "fp32" else 1]}
         del hh
 
     def step():

@@ -360,8 +360,10 @@ __device__ __forceinline__ void pass_mf(const T *src, T *dst, const LineGeom g, 
 // with scale = -1/(2h^2) (cshift: the preconditioner's c of (T + c),
 // OpenCL/Preconditioner.c:108); ekin += src(q) * scale * conv in FP64.
 // UNIT: source and destination lines are unit-stride rows starting on a point
-// pair (window and full output segments move as point pairs).
-template <class T, int SEG, bool ACC, bool UNIT = false>
+// pair (window and full output segments move as point pairs).  EN: compute
+// the energy (else ekin is left alone); ACCS (with ACC): dst(q) also gains
+// cshift src(q).
+template <class T, int SEG, bool ACC, bool UNIT = false, bool EN = true, bool ACCS = false>
 __device__ __forceinline__ void pass_kin(const T *src, T *dst, const LineGeom g, int L, int per, double scale_d, T cshift,
                          double *ekin)
 {
@@ -385,17 +387,17 @@ __device__ __forceinline__ void pass_kin(const T *src, T *dst, const LineGeom g,
         for (int t = 0; t < SEG; ++t) {
             T conv = Filt<T>::kin(0) * x[t + 14];
             [[maybe_unused]] T lo = T(0);
-            if constexpr (sizeof(T) == 4) lo = Filt<T>::kin_lo(0) * x[t + 14];
+            if constexpr (EN && sizeof(T) == 4) lo = Filt<T>::kin_lo(0) * x[t + 14];
 #pragma unroll
             for (int l = 1; l <= 14; ++l) {
                 const T pr = x[t + 14 + l] + x[t + 14 - l];
                 conv = fma(Filt<T>::kin(l), pr, conv);
-                if constexpr (sizeof(T) == 4) {
+                if constexpr (EN && sizeof(T) == 4) {
                     if (l <= 5) lo = fma(Filt<T>::kin_lo(l), pr, lo);
                 }
             }
             const int q = q0 + t;
-            if (FULL || q < L) {
+            if (EN && (FULL || q < L)) {
                 es = fma(x[t + 14], conv, es);
                 if constexpr (sizeof(T) == 4) el = fma(x[t + 14], lo, el);
             }
@@ -407,8 +409,13 @@ __device__ __forceinline__ void pass_kin(const T *src, T *dst, const LineGeom g,
                         using V = typename Pair<T>::type;
                         V *o = reinterpret_cast<V *>(out + q - 1);
                         V v;
-                        if (ACC) v = *o;
-                        else {
+                        if (ACC) {
+                            v = *o;
+                            if (ACCS) {
+                                v.x = fma(cshift, x[t + 13], v.x);
+                                v.y = fma(cshift, x[t + 14], v.y);
+                            }
+                        } else {
                             v.x = cshift * x[t + 13];
                             v.y = cshift * x[t + 14];
                         }
@@ -420,13 +427,14 @@ __device__ __forceinline__ void pass_kin(const T *src, T *dst, const LineGeom g,
                     }
                 }
             } else if (FULL || q < L) {
-                const T base = ACC ? out[q * g.dst_ps] : cshift * x[t + 14];
+                const T base = ACC ? (ACCS ? fma(cshift, x[t + 14], out[q * g.dst_ps]) : out[q * g.dst_ps])
+                                   : cshift * x[t + 14];
                 out[q * g.dst_ps] = fma(scale, conv, base);
             }
         }
-        e += ((double)es + (double)el) * scale_d;
+        if (EN) e += ((double)es + (double)el) * scale_d;
     });
-    if (ekin) *ekin += e;
+    if (EN && ekin) *ekin += e;
 }
 
 // ---------------------------------------------------------------- reductions

@@ -156,11 +156,12 @@ __device__ void gather_plane(T *A, int pitch, const LrDev &L, int kz, const TI *
 // Inverse of gather_plane: write (or add into) the compressed output.
 template <class T, class TO, int S3, bool DOT = false>
 __device__ __forceinline__ void scatter_plane_s(const T *A, int pitch, const LrDev &L, int i3, TO *out, bool accumulate,
-                                                const T *sc, const TO *dotv, double &dot)
+                                                const T *sc, const T *D, int dpitch, double &dot)
 {
     const int H1 = half_off(L.N[0]), H2 = half_off(L.N[1]);
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-    // dotv (optional): dot += <dotv | written values> over this plane's values
+    // D (DOT): a plane of the vector to dot with, gathered at row pitch
+    // dpitch; dot += <D | written values> over this plane's values
     if (!S3) {
         const T s0 = sc ? sc[0] : T(1);
         const int a = L.plane_c[i3], b = L.plane_c[i3 + 1];
@@ -169,12 +170,11 @@ __device__ __forceinline__ void scatter_plane_s(const T *A, int pitch, const LrD
             for (int t = lane; t < d.z; t += 32) {
                 const TO v = (TO)(A[d.y * pitch + d.x + t] * s0);
                 out[d.w + t] = accumulate ? out[d.w + t] + v : v;
-                if (DOT && dotv) dot += (double)v * (double)dotv[d.w + t];
+                if (DOT) dot += (double)v * (double)D[d.y * dpitch + d.x + t];
             }
         }
     }
     TO *pf = out + L.nvctr_c;
-    const TO *df = DOT && dotv ? dotv + L.nvctr_c : nullptr;
     const int a = L.plane_f[i3], b = L.plane_f[i3 + 1];
     for (int sg = a + warp; sg < b; sg += nw) {
         const int4 d = L.seg_f[sg];
@@ -186,7 +186,7 @@ __device__ __forceinline__ void scatter_plane_s(const T *A, int pitch, const LrD
                 if (fs3(c) != S3) continue;
                 const TO v = (TO)(A[(fs2(c) * H2 + d.y) * pitch + fs1(c) * H1 + d.x + t] * (sc ? sc[c] : T(1)));
                 dst[c - 1] = accumulate ? dst[c - 1] + v : v;
-                if (DOT && df) dot += (double)v * (double)df[i + c - 1];
+                if (DOT) dot += (double)v * (double)D[(fs2(c) * H2 + d.y) * dpitch + fs1(c) * H1 + d.x + t];
             }
         }
     }
@@ -194,10 +194,10 @@ __device__ __forceinline__ void scatter_plane_s(const T *A, int pitch, const LrD
 
 template <class T, class TO, bool DOT = false>
 __device__ void scatter_plane(const T *A, int pitch, const LrDev &L, int kz, TO *out, bool accumulate, const T *sc,
-                              const TO *dotv, double &dot)
+                              const T *D, int dpitch, double &dot)
 {
-    if (kz >= L.N[2]) scatter_plane_s<T, TO, 1, DOT>(A, pitch, L, kz - L.N[2], out, accumulate, sc, dotv, dot);
-    else scatter_plane_s<T, TO, 0, DOT>(A, pitch, L, kz, out, accumulate, sc, dotv, dot);
+    if (kz >= L.N[2]) scatter_plane_s<T, TO, 1, DOT>(A, pitch, L, kz - L.N[2], out, accumulate, sc, D, dpitch, dot);
+    else scatter_plane_s<T, TO, 0, DOT>(A, pitch, L, kz, out, accumulate, sc, D, dpitch, dot);
 }
 
 // Rows of `cols` points walked as point pairs: warp w takes rows w, w + nwarps,
@@ -396,36 +396,43 @@ template <class T> struct CgIo {
     int dir;
 };
 
-// gather_plane_s with the direction update: every coefficient of the plane
-// is read from d and r once, updated, written back to d and stored scaled
+// The direction update on one gathered plane: A holds d (or zeros when
+// first), R the residual r of the same positions at row pitch rpitch = G1
+// (dense, so it fits in the transposed-plane buffer); every coefficient
+// position of the plane gets v = r (first) or beta d + r, written back to d
+// in global memory and into A scaled by D^-1/2.
 template <class T, int S3>
-__device__ __forceinline__ void gather_plane_dir_s(T *A, int pitch, const LrDev &L, int i3, T *d, const T *r,
-                                                   T beta, bool first, const T *sc)
+__device__ __forceinline__ void cg_dir_plane_s(T *A, int pitch, const T *R, int rpitch, const LrDev &L, int i3,
+                                               T *__restrict__ d, T beta, bool first, const T *sc)
 {
     const int H1 = half_off(L.N[0]), H2 = half_off(L.N[1]);
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-    auto upd = [&](size_t i) {
-        const T v = first ? r[i] : fma(beta, d[i], r[i]);
-        d[i] = v;
-        return v;
-    };
     if (!S3) {
         const int a = L.plane_c[i3], b = L.plane_c[i3 + 1];
         for (int sg = a + warp; sg < b; sg += nw) {
             const int4 q = L.seg_c[sg];
-            for (int t = lane; t < q.z; t += 32) A[q.y * pitch + q.x + t] = upd(q.w + t) * sc[0];
+            for (int t = lane; t < q.z; t += 32) {
+                const int pa = q.y * pitch + q.x + t, pr = q.y * rpitch + q.x + t;
+                const T v = first ? R[pr] : fma(beta, A[pa], R[pr]);
+                d[q.w + t] = v;
+                A[pa] = v * sc[0];
+            }
         }
     }
-    const size_t f0 = L.nvctr_c;
+    T *df = d + L.nvctr_c;
     const int a = L.plane_f[i3], b = L.plane_f[i3 + 1];
     for (int sg = a + warp; sg < b; sg += nw) {
         const int4 q = L.seg_f[sg];
         for (int t = lane; t < q.z; t += 32) {
-            const size_t i = f0 + 7 * (size_t)(q.w + t);
+            T *dst = df + 7 * (size_t)(q.w + t);
 #pragma unroll
             for (int c = 1; c <= 7; ++c) {
                 if (fs3(c) != S3) continue;
-                A[(fs2(c) * H2 + q.y) * pitch + fs1(c) * H1 + q.x + t] = upd(i + c - 1) * sc[c];
+                const int pa = (fs2(c) * H2 + q.y) * pitch + fs1(c) * H1 + q.x + t;
+                const int pr = (fs2(c) * H2 + q.y) * rpitch + fs1(c) * H1 + q.x + t;
+                const T v = first ? R[pr] : fma(beta, A[pa], R[pr]);
+                dst[c - 1] = v;
+                A[pa] = v * sc[c];
             }
         }
     }
@@ -462,13 +469,21 @@ __device__ __forceinline__ void k1_item(const LrDev *__restrict__ lrs, const Orb
         if (MODE == MODE_PRECOND && threadIdx.x < 8) sc[threadIdx.x] = (T)prec_scal(L, cprec[oi], threadIdx.x);
         zero_region(A, d.G2, pitch);
         __syncthreads();
-        if (MODE == MODE_PRECOND && cg.dir) {
-            // the CG direction, updated and scaled on the way in
+        if (MODE == MODE_PRECOND && cg.dir && std::is_same<T, TI>::value) {
+            // the CG direction, updated and scaled on the way in: d and r of
+            // the plane arrive by cp.async (d into A, r into B at pitch G1,
+            // which the transposed-plane buffer always holds)
             T *dv = cg.d + o.psi;
-            const T *rv = cg.r + o.psi;
-            const T beta = cg.dir == 1 ? T(0) : (T)(cg.rrn[oi] / cg.rr[oi]);
-            if (kz >= d.N3) gather_plane_dir_s<T, 1>(A, pitch, L, kz - d.N3, dv, rv, beta, cg.dir == 1, sc);
-            else gather_plane_dir_s<T, 0>(A, pitch, L, kz, dv, rv, beta, cg.dir == 1, sc);
+            const bool first = cg.dir == 1;
+            const T beta = first ? T(0) : (T)(cg.rrn[oi] / cg.rr[oi]);
+            if (!first) gather_plane_async<T>(A, pitch, L, kz, dv);
+            // (B in a global slice: plain loads, cp.async writes shared memory only)
+            if (bslice) gather_plane<T, T>(B, d.G1, L, kz, cg.r + o.psi, nullptr);
+            else gather_plane_async<T>(B, d.G1, L, kz, cg.r + o.psi);
+            cp_async_wait_all();
+            __syncthreads();
+            if (kz >= d.N3) cg_dir_plane_s<T, 1>(A, pitch, B, d.G1, L, kz - d.N3, dv, beta, first, sc);
+            else cg_dir_plane_s<T, 0>(A, pitch, B, d.G1, L, kz, dv, beta, first, sc);
         } else if constexpr (std::is_same<T, TI>::value) {
             gather_plane_async<T>(A, pitch, L, kz, in_ptr(o, psi));
             cp_async_wait_all();
@@ -545,12 +560,12 @@ __device__ __forceinline__ void z_mf(const T *src, T *dst, int Lin, int Lout)
     if constexpr (sizeof(T) == 4) pass2_mf<kPairSeg, MODE>(src, dst, PairGeom{TC / 2, TC, TC}, Lin, Lout);
     else pass_mf<T, Seg<T>::v, MODE>(src, dst, LineGeom{TC, 1, TC, 1, TC}, Lin, Lout);
 }
-template <class T>
+template <class T, bool EN = true>
 __device__ __forceinline__ void z_kin(const T *src, T *dst, int L, int per, double scale, double *e)
 {
     if constexpr (sizeof(T) == 4)
-        pass2_kin<kPairSeg, false>(src, dst, PairGeom{TC / 2, TC, TC}, L, per, scale, 0.f, e);
-    else pass_kin<T, Seg<T>::v, false>(src, dst, LineGeom{TC, 1, TC, 1, TC}, L, per, scale, T(0), e);
+        pass2_kin<kPairSeg, false, EN>(src, dst, PairGeom{TC / 2, TC, TC}, L, per, scale, 0.f, e);
+    else pass_kin<T, Seg<T>::v, false, false, EN>(src, dst, LineGeom{TC, 1, TC, 1, TC}, L, per, scale, T(0), e);
 }
 
 // ---------------------------------------------------------------------------
@@ -576,7 +591,9 @@ __global__ void __launch_bounds__(NT, z_min_blocks(sizeof(T) == 4, NT)) k2_zpenc
     extern __shared__ __align__(128) unsigned char smem_raw[];
     // item = (orbital, tile): chain 0 tiles the I1 x I2 plane of Q, chain 1
     // the F1 x F2 plane of P, row-major; pre is the chain's own prefix table
-    constexpr int chain = CHAIN;
+    // CHAIN 2: chain 1 without the energy (the preconditioner's operator)
+    constexpr int chain = CHAIN == 2 ? 1 : CHAIN;
+    constexpr bool EN = CHAIN != 2;
     const int oi = find_owner(pre, norb, blockIdx.x);
     const int jj = blockIdx.x - pre[oi];   // tile index, also the energy slot
     const OrbDev o = orbs[oi];
@@ -708,7 +725,7 @@ __global__ void __launch_bounds__(NT, z_min_blocks(sizeof(T) == 4, NT)) k2_zpenc
         z_ana<T>(B, A, d.N3, d.p3);                               // A_z: F3 -> G3
     } else {
         const double scale = -0.5 / ((0.5 * L.hgrid[2]) * (0.5 * L.hgrid[2]));
-        z_kin<T>(B, A, d.F3, d.p3, scale, &e);                    // K_z X
+        z_kin<T, EN>(B, A, d.F3, d.p3, scale, &e);                // K_z X
         __syncthreads();
         z_ana<T>(A, B, d.N3, d.p3);                               // A_z: F3 -> G3
         __syncthreads();
@@ -735,9 +752,11 @@ __global__ void __launch_bounds__(NT, z_min_blocks(sizeof(T) == 4, NT)) k2_zpenc
             for (int z = zs; z < d.G3; z += ZS) gz[(size_t)z * plane + colofs] = A[z * TC + col];
         }
     }
-    const double s = block_sum(e, red);
-    if (threadIdx.x == 0 && part_kin)
-        (chain == 0 ? part_pot : part_kin)[(size_t)oi * part_stride + jj] = s;
+    if constexpr (EN) {
+        const double s = block_sum(e, red);
+        if (threadIdx.x == 0 && part_kin)
+            (chain == 0 ? part_pot : part_kin)[(size_t)oi * part_stride + jj] = s;
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -829,34 +848,16 @@ __device__ __forceinline__ void k3_item(const LrDev *__restrict__ lrs, const Orb
                 }
                 cp_async_wait_all();
             } else if (MODE == MODE_PRECOND && !bslice) {
-                // P -> B and Z2 -> A asynchronously, then A = c P + Z2
+                // P -> B and Z2 -> A asynchronously (the x kinetic pass adds c P)
                 load_plane_async(B, pitch, d.F2, d.F1, p);
                 load_plane_async(A, pitch, d.F2, d.F1, z2);
                 cp_async_wait_all();
-                __syncthreads();
-                if (!(d.F1 & 1)) {
-                    using V = typename Pair<T>::type;
-                    for_row_pairs(d.F2, d.F1, [&](int r, int c) {
-                        V *a = reinterpret_cast<V *>(A + r * pitch + c);
-                        const V b = *reinterpret_cast<const V *>(B + r * pitch + c);
-                        V w = *a;
-                        w.x = fma(cshift, b.x, w.x);
-                        w.y = fma(cshift, b.y, w.y);
-                        *a = w;
-                    });
-                } else {
-                    RowCol q(d.F1);
-                    for (int i = threadIdx.x; i < nf; i += blockDim.x, q.next()) {
-                        const int e = q.r * pitch + q.c;
-                        A[e] = fma(cshift, B[e], A[e]);
-                    }
-                }
             } else {
                 RowCol q(d.F1);
                 for (int i = threadIdx.x; i < nf; i += blockDim.x, q.next()) {
                     const int e = q.r * pitch + q.c;
                     const T pv = p[i];
-                    if (MODE == MODE_PRECOND) A[e] = fma(cshift, pv, z2[i]);
+                    if (MODE == MODE_PRECOND) A[e] = z2[i];
                     else A[e] += z2[i];
                     B[e] = pv;
                 }
@@ -864,24 +865,34 @@ __device__ __forceinline__ void k3_item(const LrDev *__restrict__ lrs, const Orb
         }
         __syncthreads();
         // e: the kinetic energy partial (MODE_LOCHAM) or <d | A d> (MODE_PRECOND)
+        // (the preconditioner's operator has no energy: its kinetic passes
+        // are compiled without the energy terms, and its x pass adds c P)
+        constexpr bool EN = MODE != MODE_PRECOND;
         double e = 0.0;
-        double *ek = MODE == MODE_PRECOND ? nullptr : &e;
         const double sx = -0.5 / ((0.5 * L.hgrid[0]) * (0.5 * L.hgrid[0]));
         const double sy = -0.5 / ((0.5 * L.hgrid[1]) * (0.5 * L.hgrid[1]));
-        pass_kin<T, SEG, true, true>(B, A, rows_geom(d.F2, pitch), d.F1, d.p1, sx, T(0), ek);   // += K_x P
+        pass_kin<T, SEG, true, true, EN, !EN>(B, A, rows_geom(d.F2, pitch), d.F1, d.p1, sx, cshift, &e);   // += K_x P
         __syncthreads();
         // += K_y P: the lines along y are the plane's columns, side by side
         // (F1 is even): FP32 takes them in pairs with packed FMAs
-        if constexpr (sizeof(T) == 4) pass2_kin<kPairSeg, true>(B, A, PairGeom{d.F1 / 2, pitch, pitch}, d.F2, d.p2, sy, 0.f, ek);
-        else pass_kin<T, SEG, true>(B, A, cols_geom(d.F1, pitch), d.F2, d.p2, sy, T(0), ek);
+        if constexpr (sizeof(T) == 4) pass2_kin<kPairSeg, true, EN>(B, A, PairGeom{d.F1 / 2, pitch, pitch}, d.F2, d.p2, sy, 0.f, &e);
+        else pass_kin<T, SEG, true, false, EN>(B, A, cols_geom(d.F1, pitch), d.F2, d.p2, sy, T(0), &e);
         __syncthreads();
         pass_ana<T, SEG, true>(A, B, xpose_geom(d.F2, pitch, d.pitchT(d.F2)), d.N1, d.H1, d.p1);   // A_x: F1 -> G1, into B^T
         __syncthreads();
         pass_ana<T, SEG, true>(B, A, xpose_geom(d.G1, d.pitchT(d.F2), pitch), d.N2, d.H2, d.p2);   // A_y: F2 -> G2, into A
         __syncthreads();
-        scatter_plane<T, TO, MODE == MODE_PRECOND>(A, pitch, L, kz, out_ptr(o, hpsi), accumulate != 0,
-                                                   MODE == MODE_PRECOND ? sc : nullptr,
-                                                   dotv ? dotv + o.psi : nullptr, e);
+        if (MODE == MODE_PRECOND && dotv) {
+            // the plane of d for <d | A d>, into the free buffer B at pitch G1
+            if (bslice) gather_plane<T, TO>(B, d.G1, L, kz, dotv + o.psi, nullptr);
+            else gather_plane_async<T>(B, d.G1, L, kz, (const T *)(dotv + o.psi));
+            cp_async_wait_all();
+            __syncthreads();
+            scatter_plane<T, TO, true>(A, pitch, L, kz, out_ptr(o, hpsi), accumulate != 0, sc, B, d.G1, e);
+        } else {
+            scatter_plane<T, TO, false>(A, pitch, L, kz, out_ptr(o, hpsi), accumulate != 0,
+                                        MODE == MODE_PRECOND ? sc : nullptr, nullptr, 0, e);
+        }
         const double s = block_sum(e, red);
         // slots 0 .. ntx1*nty1-1 belong to the z kernel's chain-1 tiles
         const int slot = ((d.F1 + TX - 1) / TX) * ((d.F2 + TY - 1) / TY) + kz;
@@ -1437,7 +1448,7 @@ static cudaError_t launch_prec_apply_bc(const Plan &p, const T *x, T *y, const d
     if ((err = run_k1<T, T, ALLPER, MODE_PRECOND>(p, pc, x, scratch, cprec, gtmp, st, cg))) return err;
     ZMaps zm;
     zmaps(p, scratch, zm);
-    if ((err = run_k2<T, T, ALLPER, 1>(p.z_threads_pre[fp], p.n_work2p, sm2, p, p.d_pre2p, (const T *)nullptr, scratch,
+    if ((err = run_k2<T, T, ALLPER, 2>(p.z_threads_pre[fp], p.n_work2p, sm2, p, p.d_pre2p, (const T *)nullptr, scratch,
                                        nullptr, nullptr, 0, zm.p, zm.z, zm.ok, st)))
         return err;
     if (dotpart) cudaMemsetAsync(dotpart, 0, sizeof(double) * (size_t)p.norb * p.part_stride, st);

@@ -225,7 +225,7 @@ __device__ __forceinline__ void pass2_mf(const float *src, float *dst, const Pai
 // line, periodic or zero-padded, that is lo(0) C(0) + 2 sum_{l>0} lo(l) C(l)
 // with C(l) = sum_q x(q) x(q-l), which each segment accumulates for its own
 // outputs q from the window, for the kKinLags largest taps.
-template <int SEG, bool ACC>
+template <int SEG, bool ACC, bool EN = true>
 __device__ __forceinline__ void pass2_kin(const float *src, float *dst, const PairGeom g, int L, int per, double scale_d,
                                           float cshift, double *ekin)
 {
@@ -261,6 +261,7 @@ __device__ __forceinline__ void pass2_kin(const float *src, float *dst, const Pa
                 const int l = k - 14 - t;   // tap offset of this value for output t
                 if (l >= -14 && l <= 14) conv[t] = P::fma(Filt<float>::kin(l < 0 ? -l : l), x, conv[t]);
             }
+            if constexpr (!EN) continue;
 #pragma unroll
             for (int j = NLAG - 1; j > 0; --j) hist[j] = hist[j - 1];
             hist[0] = x;
@@ -275,20 +276,26 @@ __device__ __forceinline__ void pass2_kin(const float *src, float *dst, const Pa
         for (int t = 0; t < SEG; ++t) {
             if (INT || t < nout) {
                 const int q = q0 + t;
-                const float2 xq = ld2(in + q * g.src_ps);
-                es = P::fmav(xq, conv[t], es);
                 float *o = dst + 2 * lp + q * g.dst_ps;
-                const float2 base = ACC ? ld2(o) : P::mul(cshift, xq);
+                float2 base;
+                if constexpr (ACC) {
+                    base = ld2(o);
+                } else {
+                    base = P::mul(cshift, ld2(in + q * g.src_ps));
+                }
+                if constexpr (EN) es = P::fmav(ld2(in + q * g.src_ps), conv[t], es);
                 st2(o, P::fma(scale, conv[t], base));
             }
         }
-        double el = (double)Filt<float>::kin_lo(0) * ((double)lag[0].x + (double)lag[0].y);
+        if constexpr (EN) {
+            double el = (double)Filt<float>::kin_lo(0) * ((double)lag[0].x + (double)lag[0].y);
 #pragma unroll
-        for (int l = 1; l < NLAG; ++l)
-            el += 2.0 * (double)Filt<float>::kin_lo(l) * ((double)lag[l].x + (double)lag[l].y);
-        e += ((double)es.x + (double)es.y + el) * scale_d;
+            for (int l = 1; l < NLAG; ++l)
+                el += 2.0 * (double)Filt<float>::kin_lo(l) * ((double)lag[l].x + (double)lag[l].y);
+            e += ((double)es.x + (double)es.y + el) * scale_d;
+        }
     });
-    if (ekin) *ekin += e;
+    if (EN && ekin) *ekin += e;
 }
 
 }  // namespace wvlh
