@@ -162,3 +162,25 @@ def test_precond_autotune_keeps_results(torch_cuda, wctx, dtype_name):
     torch.cuda.synchronize()
     assert torch.equal(x2, x1) and torch.equal(h2, h1)   # deterministic for a given block size
     b.close()
+
+
+@pytest.mark.parametrize("N,per", [((64, 64, 8), (1, 1, 1)), ((48, 46, 6), (0, 0, 0))])
+def test_precond_large_planes_match_oracle(oracle, torch_cuda, wctx, N, per):
+    """FP64 boxes whose two planes exceed a block's shared memory keep the
+    second plane in a global slice per CTA: the CG direction update and the
+    <d|Ad> staging then go through that slice instead of shared memory."""
+    torch = torch_cuda
+    lr = region(N, per, 13, 0.5)
+    b = Batch(wctx, [lr, lr], np.zeros(2, np.int32))
+    rng = np.random.default_rng(14)
+    cprec = np.array([0.8, 1.2])
+    rows = [rng.uniform(-1, 1, lr.ncoeff) for _ in range(2)]
+    x = torch.tensor(layout(b, [lr], [0, 0], rows), dtype=torch.float64, device="cuda")
+    rhs = x.clone()
+    x, hist = b.precond(x, rhs, cprec, 3)
+    torch.cuda.synchronize()
+    xg, hist = x.cpu().numpy(), hist.cpu().numpy()
+    for o in range(2):
+        ref, rn = oracle.precond(desc(oracle, lr), [0.5 * h for h in lr.hgrid], cprec[o], 3, rows[o], rows[o])
+        assert rel(xg[b.psi_offset(o):b.psi_offset(o) + lr.ncoeff], ref) < 1e-13
+        assert np.allclose(hist[:, o], rn, rtol=1e-12, atol=0)
