@@ -33,9 +33,8 @@ template <> struct PV<float> {
     static __device__ __forceinline__ V zero() { return make_float2(0.f, 0.f); }
 };
 
-// taps whose FP32 rounding residual the pair passes carry (see above)
-constexpr double kSynSeedTap = 0.1;
-constexpr double kMfSeedTap = 0.5;
+// the pair passes seed the taps kSynSeedTap / kMfSeedTap select
+// (wvlh_common.cuh), as the one-line passes do
 constexpr int kKinLags = 3;
 
 // outputs per line of one thread's segment: eight outputs share a window of
@@ -261,14 +260,15 @@ __device__ __forceinline__ void pass2_kin(const float *src, float *dst, const Pa
                 const int l = k - 14 - t;   // tap offset of this value for output t
                 if (l >= -14 && l <= 14) conv[t] = P::fma(Filt<float>::kin(l < 0 ? -l : l), x, conv[t]);
             }
-            if constexpr (!EN) continue;
+            if constexpr (EN) {
 #pragma unroll
-            for (int j = NLAG - 1; j > 0; --j) hist[j] = hist[j - 1];
-            hist[0] = x;
-            // outputs of this segment: window positions 14 .. 14 + nout - 1
-            if (k >= 14 && k < 14 + SEG && (INT || k - 14 < nout)) {
+                for (int j = NLAG - 1; j > 0; --j) hist[j] = hist[j - 1];
+                hist[0] = x;
+                // outputs of this segment: window positions 14 .. 14 + nout - 1
+                if (k >= 14 && k < 14 + SEG && (INT || k - 14 < nout)) {
 #pragma unroll
-                for (int l = 0; l < NLAG; ++l) lag[l] = P::fmav(x, hist[l], lag[l]);
+                    for (int l = 0; l < NLAG; ++l) lag[l] = P::fmav(x, hist[l], lag[l]);
+                }
             }
         }
         float2 es = P::zero();
