@@ -247,7 +247,8 @@ __device__ __forceinline__ void pass2_kin(const float *src, float *dst, const Pa
         const int p0 = q0 - 14;
         const int nout = INT ? SEG : min(SEG, L - q0);
         const float *b = in + p0 * g.src_ps;
-        float2 conv[SEG], lag[NLAG], hist[NLAG];
+        float2 conv[SEG], lag[NLAG];
+        [[maybe_unused]] float2 hist[NLAG];
 #pragma unroll
         for (int t = 0; t < SEG; ++t) conv[t] = P::zero();
 #pragma unroll
