@@ -331,8 +331,11 @@ __device__ __forceinline__ void pass_ana(const T *src, T *dst, const LineGeom g,
 
 // ---------------------------------------------------------------- magic filter
 // MODE 0: mf periodic, 1: mft periodic, 2: mf grow (F -> F+15), 3: mft shrink (F+15 -> F)
-template <class T, int SEG, int MODE, bool UNIT = false>
-__device__ __forceinline__ void pass_mf(const T *src, T *dst, const LineGeom g, int Lin, int Lout)
+// ADDG: every output also gains addg[line + q * addg_ps] (a plane in global
+// memory, read as the outputs are stored)
+template <class T, int SEG, int MODE, bool UNIT = false, bool ADDG = false>
+__device__ __forceinline__ void pass_mf(const T *src, T *dst, const LineGeom g, int Lin, int Lout,
+                                        const T *__restrict__ addg = nullptr, int addg_ps = 0)
 {
     constexpr int W = SEG + 15;
     constexpr int shift = MODE == 0 ? -8 : MODE == 1 ? -7 : MODE == 2 ? -15 : 0;
@@ -360,7 +363,10 @@ __device__ __forceinline__ void pass_mf(const T *src, T *dst, const LineGeom g, 
 #pragma unroll
             for (int k = 0; k < 16; ++k) acc = fma(Filt<T>::mf(rev ? 15 - k : k), x[t + k], acc);
             const int q = q0 + t;
-            if (FULL || q < Lout) out[q * g.dst_ps] = acc;
+            if (FULL || q < Lout) {
+                if constexpr (ADDG) acc += addg[line + q * addg_ps];
+                out[q * g.dst_ps] = acc;
+            }
         }
     });
 }
@@ -389,27 +395,31 @@ __device__ __forceinline__ void pass_kin(const T *src, T *dst, const LineGeom g,
         const int q0 = s * SEG;
         T x[W];
         load_window_g<T, W, -14, UNIT>(x, in, g.src_ps, q0, L, per);
-        // per-segment partial sums of x.conv (and of x.lo in FP32), converted
-        // to FP64 once per segment; the rounding of these short sums is unbiased
-        T es = T(0), el = T(0);
+        // per-segment partial sums of x.conv, converted to FP64 once per
+        // segment (the rounding of these short sums is unbiased); in FP32 the
+        // taps' rounding residuals lo(l) enter E_kin through the lag sums
+        // C(l) = sum_q x(q) x(q-l) of the three largest taps, lo(0) C(0) +
+        // 2 sum lo(l) C(l), which over whole lines equals the per-output
+        // correction (as the line-pair kinetic pass does)
+        T es = T(0);
+        [[maybe_unused]] T c0 = T(0), c1 = T(0), c2 = T(0);
         T prev = T(0);
 #pragma unroll
         for (int t = 0; t < SEG; ++t) {
             T conv = Filt<T>::kin(0) * x[t + 14];
-            [[maybe_unused]] T lo = T(0);
-            if constexpr (EN && sizeof(T) == 4) lo = Filt<T>::kin_lo(0) * x[t + 14];
 #pragma unroll
             for (int l = 1; l <= 14; ++l) {
                 const T pr = x[t + 14 + l] + x[t + 14 - l];
                 conv = fma(Filt<T>::kin(l), pr, conv);
-                if constexpr (EN && sizeof(T) == 4) {
-                    if (l <= 5) lo = fma(Filt<T>::kin_lo(l), pr, lo);
-                }
             }
             const int q = q0 + t;
             if (EN && (FULL || q < L)) {
                 es = fma(x[t + 14], conv, es);
-                if constexpr (sizeof(T) == 4) el = fma(x[t + 14], lo, el);
+                if constexpr (sizeof(T) == 4) {
+                    c0 = fma(x[t + 14], x[t + 14], c0);
+                    c1 = fma(x[t + 14], x[t + 13], c1);
+                    c2 = fma(x[t + 14], x[t + 12], c2);
+                }
             }
             // unit-stride rows store each point pair once both are formed (a
             // clipped segment of an even line ends on a whole pair)
@@ -442,7 +452,13 @@ __device__ __forceinline__ void pass_kin(const T *src, T *dst, const LineGeom g,
                 out[q * g.dst_ps] = fma(scale, conv, base);
             }
         }
-        if (EN) e += ((double)es + (double)el) * scale_d;
+        if constexpr (EN) {
+            double el = 0.0;
+            if constexpr (sizeof(T) == 4)
+                el = (double)Filt<T>::kin_lo(0) * (double)c0 +
+                     2.0 * ((double)Filt<T>::kin_lo(1) * (double)c1 + (double)Filt<T>::kin_lo(2) * (double)c2);
+            e += ((double)es + el) * scale_d;
+        }
     });
     if (EN && ekin) *ekin += e;
 }

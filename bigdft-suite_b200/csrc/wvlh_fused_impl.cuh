@@ -792,8 +792,10 @@ __device__ __forceinline__ void k3_item(const LrDev *__restrict__ lrs, const Orb
             if (d.p1) pass_mf<T, SEG, 1, true>(A, B, xpose_geom(d.I2, pitch, d.pitchT(d.I2)), d.I1, d.F1);   // Mt_x into B^T
             else pass_mf<T, SEG, 3, true>(A, B, xpose_geom(d.I2, pitch, d.pitchT(d.I2)), d.I1, d.F1);
             __syncthreads();
-            if (d.p2) pass_mf<T, SEG, 1, true>(B, A, xpose_geom(d.F1, d.pitchT(d.I2), pitch), d.I2, d.F2);   // Mt_y into A
-            else pass_mf<T, SEG, 3, true>(B, A, xpose_geom(d.F1, d.pitchT(d.I2), pitch), d.I2, d.F2);
+            // Mt_y into A, plus Z2 (read from global memory as the outputs are stored)
+            const T *z2 = scratch + o.sZ + (size_t)kz * d.F2 * d.F1;
+            if (d.p2) pass_mf<T, SEG, 1, true, true>(B, A, xpose_geom(d.F1, d.pitchT(d.I2), pitch), d.I2, d.F2, z2, d.F1);
+            else pass_mf<T, SEG, 3, true, true>(B, A, xpose_geom(d.F1, d.pitchT(d.I2), pitch), d.I2, d.F2, z2, d.F1);
             __syncthreads();
         }
         {
@@ -801,51 +803,8 @@ __device__ __forceinline__ void k3_item(const LrDev *__restrict__ lrs, const Orb
             const T *p = scratch + o.sP + (size_t)kz * d.F2 * d.F1;
             const int nf = d.F2 * d.F1;
             if (MODE != MODE_PRECOND && !bslice) {
-                // P -> B asynchronously while Z2 is added into A, 4 loads in flight
+                // P -> B (Z2 is already in A)
                 load_plane_async(B, pitch, d.F2, d.F1, p);
-                constexpr int U = 4;
-                if (pair_rows(d.F1, z2)) {
-                    // point pairs: pair i = (row q.r, column 2 q.c) of the dense Z2 plane
-                    using V = typename Pair<T>::type;
-                    const int npair = nf >> 1;
-                    RowCol q(d.F1 >> 1);
-                    for (int i0 = threadIdx.x; i0 < npair; i0 += U * blockDim.x) {
-                        V v[U];
-#pragma unroll
-                        for (int u = 0; u < U; ++u) {
-                            const int i = i0 + u * blockDim.x;
-                            v[u].x = T(0);
-                            v[u].y = T(0);
-                            if (i < npair) v[u] = *reinterpret_cast<const V *>(z2 + 2 * i);
-                        }
-#pragma unroll
-                        for (int u = 0; u < U; ++u) {
-                            if (i0 + u * (int)blockDim.x < npair) {
-                                V *a = reinterpret_cast<V *>(A + q.r * pitch + 2 * q.c);
-                                V w = *a;
-                                w.x += v[u].x;
-                                w.y += v[u].y;
-                                *a = w;
-                            }
-                            q.next();
-                        }
-                    }
-                } else {
-                    RowCol q(d.F1);
-                    for (int i0 = threadIdx.x; i0 < nf; i0 += U * blockDim.x) {
-                        T v[U];
-#pragma unroll
-                        for (int u = 0; u < U; ++u) {
-                            const int i = i0 + u * blockDim.x;
-                            v[u] = i < nf ? z2[i] : T(0);
-                        }
-#pragma unroll
-                        for (int u = 0; u < U; ++u) {
-                            if (i0 + u * (int)blockDim.x < nf) A[q.r * pitch + q.c] += v[u];
-                            q.next();
-                        }
-                    }
-                }
                 cp_async_wait_all();
             } else if (MODE == MODE_PRECOND && !bslice) {
                 // P -> B and Z2 -> A asynchronously (the x kinetic pass adds c P)
@@ -857,8 +816,7 @@ __device__ __forceinline__ void k3_item(const LrDev *__restrict__ lrs, const Orb
                 for (int i = threadIdx.x; i < nf; i += blockDim.x, q.next()) {
                     const int e = q.r * pitch + q.c;
                     const T pv = p[i];
-                    if (MODE == MODE_PRECOND) A[e] = z2[i];
-                    else A[e] += z2[i];
+                    if (MODE == MODE_PRECOND) A[e] = z2[i];   // (MODE_LOCHAM: Z2 came with Mt_y)
                     B[e] = pv;
                 }
             }
