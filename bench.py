@@ -862,7 +862,7 @@ def main():
         # DRAM traffic of each kernel (dram__bytes_read.sum + dram__bytes_write.sum) from ncu
         # captures of one call over 48 orbitals of this 48^3 FP32 workload, scaled by the orbitals
         # of this launch (the traffic grows in proportion to them); z kernels: both chains
-        traffic48 = [453.271296e6, 582.952960e6, 657.630208e6]
+        traffic48 = [453.519104e6, 582.610688e6, 656.173312e6]
         traffic = traffic48[dom] / 48 * norb if (dom < 3 and n == 48) else None
         step_s = ms / args.steps * 1e-3
         extras["roofline"] = {"bound": "hbm", "achieved": ach, "peak": hbm, "unit": "GB/s", "frac": ach / hbm,
