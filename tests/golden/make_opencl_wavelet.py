@@ -1,0 +1,109 @@
+"""Writes opencl_wavelet.npz: outputs of the reference's OpenCL periodic
+wavelet synthesis and analysis kernels (bigdft/src/OpenCL/Wavelet_Generator.cpp:
+syn1dKernel_d, ana1dKernel_d), evaluated on seeded lines.
+
+The kernels exist only as source text that the generator pastes into an
+OpenCL program; there is no OpenCL runtime here.  This script reads the
+generator's scalar filter macros and replays their multiply-add statements in
+their own order, with the indexing of the kernels that use them:
+
+  * analysis (`filter(ci,di,tmp)` in generate_ana_filter, used by
+    generate_ana1dKernel): for coarse output i of a line of 2n fine points,
+    tmp[m] = psi[(2 i - 7 + m) mod 2n]; out[i] = ci, out[i + n] = di;
+  * synthesis (`filter(tmp1,tmp2)` in generate_syn_filter, used by
+    generate_syn1dKernel): tmp1 points at s[i - 4] and tmp2 at w[i - 4] of the
+    line's two halves (s = psi[0:n], w = psi[n:2n], periodic in the coarse
+    index); the macro starts tmp1b = tmp1, tmp2b = tmp2 + 8 and walks them
+    with ++ / --; out[2 i] = se, out[2 i + 1] = so.
+
+`mad(a, b, c)` is evaluated as a * b + c in FP64.  The file holds, per line
+length n, the input line and the two kernels' outputs.
+
+Run from the repository root:
+  WVLH_REFERENCE_ROOT=<reference tree> python tests/golden/make_opencl_wavelet.py
+"""
+import os
+import re
+import sys
+from pathlib import Path
+
+import numpy as np
+
+NUM = r"([-+]?[0-9]*\.?[0-9]+(?:[eE][-+]?[0-9]+)?)"
+
+
+def macro(text, head):
+    """Body of the first `#define <head>` macro of the generator's text."""
+    i = text.index("#define " + head)
+    j = text.find("#define", i + 1)
+    k = text.find('";', i)
+    end = min(x for x in (j, k) if x > 0)
+    return text[i + len("#define " + head):end]
+
+
+def ana_program(text):
+    body = macro(text, "filter(ci,di,tmp)")
+    prog = [(v, int(m), float(c)) for v, m, c, v2 in
+            re.findall(r"(ci|di)\s*=\s*mad\(\s*tmp\[\s*(\d+)\s*\]\s*,\s*" + NUM + r"\s*,\s*(ci|di)\s*\)", body)]
+    assert len(prog) == 32, len(prog)
+    return prog
+
+
+def syn_program(text):
+    body = macro(text, "filter(tmp1,tmp2)")
+    st = re.findall(r"(se|so)\s*=\s*mad\(\s*\*\s*(tmp1b|tmp2b)\s*(\+\+|--)?\s*,\s*" + NUM + r"\s*,\s*(se|so)\s*\)", body)
+    init = dict(re.findall(r"(tmp[12]b)\s*=\s*tmp[12]\s*(?:\+\s*(\d+))?\s*;", body.replace("__local double *", "")))
+    start = {"tmp1b": int(init.get("tmp1b") or 0), "tmp2b": int(init.get("tmp2b") or 0)}
+    prog = [(v, p, inc, float(c)) for v, p, inc, c, v2 in st]
+    assert len(prog) == 32 and set(init) == {"tmp1b", "tmp2b"}, (len(prog), init)
+    return prog, start
+
+
+def ana_line(prog, x):
+    n = len(x) // 2
+    out = np.zeros(2 * n)
+    for i in range(n):
+        tmp = [x[(2 * i - 7 + m) % (2 * n)] for m in range(16)]
+        acc = {"ci": 0.0, "di": 0.0}
+        for v, m, c in prog:
+            acc[v] = tmp[m] * c + acc[v]
+        out[i], out[i + n] = acc["ci"], acc["di"]
+    return out
+
+
+def syn_line(prog, start, x):
+    n = len(x) // 2
+    s, w = x[:n], x[n:]
+    out = np.zeros(2 * n)
+    for i in range(n):
+        pos = {"tmp1b": start["tmp1b"], "tmp2b": start["tmp2b"]}
+        src = {"tmp1b": s, "tmp2b": w}
+        acc = {"se": 0.0, "so": 0.0}
+        for v, p, inc, c in prog:
+            acc[v] = src[p][(i - 4 + pos[p]) % n] * c + acc[v]
+            pos[p] += 1 if inc == "++" else -1 if inc == "--" else 0
+        out[2 * i], out[2 * i + 1] = acc["se"], acc["so"]
+    return out
+
+
+def main():
+    root = os.environ.get("WVLH_REFERENCE_ROOT") or (sys.argv[1] if len(sys.argv) > 1 else None)
+    if not root:
+        sys.exit("set WVLH_REFERENCE_ROOT to the reference tree")
+    text = (Path(root) / "bigdft/src/OpenCL/Wavelet_Generator.cpp").read_text()
+    ana = ana_program(text)
+    syn, start = syn_program(text)
+    rng = np.random.default_rng(2024)
+    out = {}
+    for n in (8, 9, 13, 16, 24):
+        x = rng.uniform(-1, 1, 2 * n)
+        out["x_%d" % n] = x
+        out["ana_%d" % n] = ana_line(ana, x)
+        out["syn_%d" % n] = syn_line(syn, start, x)
+    dst = Path(__file__).resolve().parent / "opencl_wavelet.npz"
+    np.savez(dst, **out)
+    print("wrote", dst, "syn start", start)
+
+
+if __name__ == "__main__":
+    main()

@@ -11,7 +11,11 @@ recompute CPU references from random inputs), so the oracle is pinned by:
     wavelet-basis a/b/c/e filters of ConvolkineticT) agreeing to 1e-15;
   * the reference's Fortran chain (daub_to_isf_locham + isf_to_daub_kinetic)
     and its OpenCL composition (ocl_fulllocham_generic) agreeing;
-  * an analytic known answer: the kinetic energy of a Gaussian.
+  * an analytic known answer: the kinetic energy of a Gaussian;
+  * the reference's OpenCL periodic synthesis and analysis kernels
+    (OpenCL/Wavelet_Generator.cpp), whose multiply-add statements
+    tests/golden/make_opencl_wavelet.py replays from the generator's source
+    text into tests/golden/opencl_wavelet.npz.
 """
 import ctypes as C
 from pathlib import Path
@@ -264,3 +268,25 @@ def test_wavelet_kinetic_matches_reference_sse(oracle, N, fc, ff, cprecr):
             full[nfl[2]:nfu[2] + 1, nfl[1]:nfu[1] + 1, nfl[0]:nfu[0] + 1] = rf
             got, want = full[mf].ravel(), yf + cprecr * f
         assert np.abs(got - want).max() <= 2e-6 * np.abs(want).max(), part
+
+
+def test_syn_ana_match_reference_opencl_kernels(oracle):
+    """The oracle's periodic synthesis and analysis (syn_rot_per / ana_rot_per,
+    convolut_simple_per.f90) against the reference's OpenCL syn1dKernel_d /
+    ana1dKernel_d arithmetic on the same lines (golden file), to FP64 rounding;
+    with the reference tree present, the golden file is re-derived first."""
+    gold = np.load(GOLD / "opencl_wavelet.npz")
+    if (REFERENCE / "bigdft").exists():
+        import importlib.util
+        spec = importlib.util.spec_from_file_location("mk", GOLD / "make_opencl_wavelet.py")
+        mk = importlib.util.module_from_spec(spec)
+        spec.loader.exec_module(mk)
+        text = (REFERENCE / "bigdft/src/OpenCL/Wavelet_Generator.cpp").read_text()
+        ana, (syn, start) = mk.ana_program(text), mk.syn_program(text)
+    for n in (8, 9, 13, 16, 24):
+        x = gold["x_%d" % n]
+        if (REFERENCE / "bigdft").exists():
+            assert np.array_equal(mk.ana_line(ana, x), gold["ana_%d" % n])
+            assert np.array_equal(mk.syn_line(syn, start, x), gold["syn_%d" % n])
+        assert np.abs(oracle.ana_rot_per(n - 1, 1, x) - gold["ana_%d" % n]).max() < 1e-15
+        assert np.abs(oracle.syn_rot_per(n - 1, 1, x) - gold["syn_%d" % n]).max() < 1e-15
