@@ -1,6 +1,8 @@
-"""Writes opencl_wavelet.npz: outputs of the reference's OpenCL periodic
+"""Writes opencl_kernels.npz: outputs of the reference's OpenCL periodic
 wavelet synthesis and analysis kernels (bigdft/src/OpenCL/Wavelet_Generator.cpp:
-syn1dKernel_d, ana1dKernel_d), evaluated on seeded lines.
+syn1dKernel_d, ana1dKernel_d) and fine-grid kinetic kernel
+(bigdft/src/OpenCL/Kinetic_Generator.cpp: kinetic1dKernel_d), evaluated on
+seeded lines.
 
 The kernels exist only as source text that the generator pastes into an
 OpenCL program; there is no OpenCL runtime here.  This script reads the
@@ -14,13 +16,17 @@ their own order, with the indexing of the kernels that use them:
     generate_syn1dKernel): tmp1 points at s[i - 4] and tmp2 at w[i - 4] of the
     line's two halves (s = psi[0:n], w = psi[n:2n], periodic in the coarse
     index); the macro starts tmp1b = tmp1, tmp2b = tmp2 + 8 and walks them
-    with ++ / --; out[2 i] = se, out[2 i + 1] = so.
+    with ++ / --; out[2 i] = se, out[2 i + 1] = so;
+  * kinetic (`filter1(tt,tmp)` in generate_filters, with the FILT1_* values
+    of generate_header, used by generate_kinetic1dKernel): for fine point i of
+    a line of n points, tmp[m] = x[(i + m) mod n]; the kernel writes
+    y_in + scale * conv, of which the file keeps conv.
 
 `mad(a, b, c)` is evaluated as a * b + c in FP64.  The file holds, per line
 length n, the input line and the two kernels' outputs.
 
 Run from the repository root:
-  WVLH_REFERENCE_ROOT=<reference tree> python tests/golden/make_opencl_wavelet.py
+  WVLH_REFERENCE_ROOT=<reference tree> python tests/golden/make_opencl_kernels.py
 """
 import os
 import re
@@ -59,6 +65,29 @@ def syn_program(text):
     return prog, start
 
 
+def kin_program(text):
+    filt = {int(k): float(v) for k, v in re.findall(r"#define FILT1_(\d+)\s+" + NUM, text)}
+    body = macro(text, "filter1(tt,tmp)")
+    prog = []
+    for a, b, k in re.findall(r"tt\s*=\s*mad\(\s*tmp\[\s*(-?\d+)\s*\](?:\s*\+\s*tmp\[\s*(-?\d+)\s*\])?\s*,"
+                              r"\s*FILT1_(\d+)\s*,\s*tt\s*\)", body):
+        prog.append((int(a), None if b == "" else int(b), filt[int(k)]))
+    assert len(prog) == 15 and len(filt) == 15, (len(prog), len(filt))
+    return prog
+
+
+def kin_line(prog, x):
+    n = len(x)
+    out = np.zeros(n)
+    for i in range(n):
+        tt = 0.0
+        for a, b, c in prog:
+            v = x[(i + a) % n] if b is None else x[(i + a) % n] + x[(i + b) % n]
+            tt = v * c + tt
+        out[i] = tt
+    return out
+
+
 def ana_line(prog, x):
     n = len(x) // 2
     out = np.zeros(2 * n)
@@ -93,6 +122,7 @@ def main():
     text = (Path(root) / "bigdft/src/OpenCL/Wavelet_Generator.cpp").read_text()
     ana = ana_program(text)
     syn, start = syn_program(text)
+    kin = kin_program((Path(root) / "bigdft/src/OpenCL/Kinetic_Generator.cpp").read_text())
     rng = np.random.default_rng(2024)
     out = {}
     for n in (8, 9, 13, 16, 24):
@@ -100,7 +130,8 @@ def main():
         out["x_%d" % n] = x
         out["ana_%d" % n] = ana_line(ana, x)
         out["syn_%d" % n] = syn_line(syn, start, x)
-    dst = Path(__file__).resolve().parent / "opencl_wavelet.npz"
+        out["kin_%d" % n] = kin_line(kin, x)   # on the 2n fine points of the same line
+    dst = Path(__file__).resolve().parent / "opencl_kernels.npz"
     np.savez(dst, **out)
     print("wrote", dst, "syn start", start)
 

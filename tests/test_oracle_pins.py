@@ -12,10 +12,10 @@ recompute CPU references from random inputs), so the oracle is pinned by:
   * the reference's Fortran chain (daub_to_isf_locham + isf_to_daub_kinetic)
     and its OpenCL composition (ocl_fulllocham_generic) agreeing;
   * an analytic known answer: the kinetic energy of a Gaussian;
-  * the reference's OpenCL periodic synthesis and analysis kernels
-    (OpenCL/Wavelet_Generator.cpp), whose multiply-add statements
-    tests/golden/make_opencl_wavelet.py replays from the generator's source
-    text into tests/golden/opencl_wavelet.npz.
+  * the reference's OpenCL periodic synthesis, analysis and fine-grid kinetic
+    kernels (OpenCL/Wavelet_Generator.cpp, Kinetic_Generator.cpp), whose
+    multiply-add statements tests/golden/make_opencl_kernels.py replays from
+    the generators' source text into tests/golden/opencl_kernels.npz.
 """
 import ctypes as C
 from pathlib import Path
@@ -270,23 +270,34 @@ def test_wavelet_kinetic_matches_reference_sse(oracle, N, fc, ff, cprecr):
         assert np.abs(got - want).max() <= 2e-6 * np.abs(want).max(), part
 
 
-def test_syn_ana_match_reference_opencl_kernels(oracle):
+def test_syn_ana_kinetic_match_reference_opencl_kernels(oracle):
     """The oracle's periodic synthesis and analysis (syn_rot_per / ana_rot_per,
-    convolut_simple_per.f90) against the reference's OpenCL syn1dKernel_d /
-    ana1dKernel_d arithmetic on the same lines (golden file), to FP64 rounding;
-    with the reference tree present, the golden file is re-derived first."""
-    gold = np.load(GOLD / "opencl_wavelet.npz")
-    if (REFERENCE / "bigdft").exists():
+    convolut_simple_per.f90) and fine-grid kinetic filter (the x part of
+    wo_kinetic_generic on a line) against the reference's OpenCL
+    syn1dKernel_d / ana1dKernel_d / kinetic1dKernel_d arithmetic on the same
+    lines (golden file), to FP64 rounding; with the reference tree present the
+    golden file is re-derived first."""
+    gold = np.load(GOLD / "opencl_kernels.npz")
+    have_ref = (REFERENCE / "bigdft").exists()
+    if have_ref:
         import importlib.util
-        spec = importlib.util.spec_from_file_location("mk", GOLD / "make_opencl_wavelet.py")
+        spec = importlib.util.spec_from_file_location("mk", GOLD / "make_opencl_kernels.py")
         mk = importlib.util.module_from_spec(spec)
         spec.loader.exec_module(mk)
         text = (REFERENCE / "bigdft/src/OpenCL/Wavelet_Generator.cpp").read_text()
         ana, (syn, start) = mk.ana_program(text), mk.syn_program(text)
+        kin = mk.kin_program((REFERENCE / "bigdft/src/OpenCL/Kinetic_Generator.cpp").read_text())
+    L = oracle.lib()
     for n in (8, 9, 13, 16, 24):
         x = gold["x_%d" % n]
-        if (REFERENCE / "bigdft").exists():
+        if have_ref:
             assert np.array_equal(mk.ana_line(ana, x), gold["ana_%d" % n])
             assert np.array_equal(mk.syn_line(syn, start, x), gold["syn_%d" % n])
+            assert np.array_equal(mk.kin_line(kin, x), gold["kin_%d" % n])
         assert np.abs(oracle.ana_rot_per(n - 1, 1, x) - gold["ana_%d" % n]).max() < 1e-15
         assert np.abs(oracle.syn_rot_per(n - 1, 1, x) - gold["syn_%d" % n]).max() < 1e-15
+        # kinetic of a line of 2n points: a (2n, 1, 1) periodic box with unit
+        # spacing adds -1/2 conv along x (the one-point y and z lines add 0)
+        y, e = np.zeros(2 * n), C.c_double()
+        L.wo_kinetic_generic(2 * n, 1, 1, np.ones(3, np.int32), np.ones(3), np.ascontiguousarray(x), y, C.byref(e))
+        assert np.abs(-2.0 * y - gold["kin_%d" % n]).max() < 1e-14 * np.abs(gold["kin_%d" % n]).max()
