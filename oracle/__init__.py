@@ -13,11 +13,16 @@ cites the reference lines it follows.  Parity pins:
   (``bigdft/src/convolutions-c/MagicFilter_sse.c``) compiled into
   ``oracle/_ref`` (see ``Makefile``), and against golden vectors generated
   from it (``tests/golden``);
-* the rest is pinned by the reference's mathematical known-answer checks
-  (orthonormality of DB16, analysis after synthesis = identity, magic-filter
-  adjointness, kinetic symmetry, agreement of the fine-grid kinetic with the
-  wavelet-basis ``ConvolkineticT`` filters, analytic Laplacian of a Gaussian),
-  since the reference stores no golden vectors for this path.
+* the wavelet-basis kinetic operator against the reference's SSE C
+  (``bigdft/src/orbitals/convolut_ib_sse.c``), also compiled into ``oracle/_ref``;
+* synthesis and analysis (periodic and free) and the fine-grid kinetic filter
+  against the arithmetic of the reference's OpenCL kernels, replayed from the
+  kernel generators' source text into golden vectors
+  (``tests/golden/make_opencl_kernels.py``);
+* and by the reference's mathematical known-answer checks (orthonormality of
+  DB16, analysis after synthesis = identity, magic-filter adjointness,
+  kinetic symmetry, agreement of the fine-grid kinetic with the wavelet-basis
+  ``ConvolkineticT`` filters, analytic Laplacian of a Gaussian).
 """
 import ctypes as C
 import os

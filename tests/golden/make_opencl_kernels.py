@@ -17,6 +17,11 @@ their own order, with the indexing of the kernels that use them:
     line's two halves (s = psi[0:n], w = psi[n:2n], periodic in the coarse
     index); the macro starts tmp1b = tmp1, tmp2b = tmp2 + 8 and walks them
     with ++ / --; out[2 i] = se, out[2 i + 1] = so;
+  * free-BC synthesis (`filter_grow(tmp1,tmp2)`, used by
+    generate_syngrow1dKernel): Nc coarse points grow to Nc + 7 output pairs,
+    tmp1 / tmp2 at s[i - 7] / w[i - 7] (zero outside), out[2 i] = so,
+    out[2 i + 1] = se; free-BC analysis (the analysis macro in
+    generate_anashrink1dKernel): tmp[m] = y[2 i + m] of 2 Nc + 14 points;
   * kinetic (`filter1(tt,tmp)` in generate_filters, with the FILT1_* values
     of generate_header, used by generate_kinetic1dKernel): for fine point i of
     a line of n points, tmp[m] = x[(i + m) mod n]; the kernel writes
@@ -55,8 +60,8 @@ def ana_program(text):
     return prog
 
 
-def syn_program(text):
-    body = macro(text, "filter(tmp1,tmp2)")
+def syn_program(text, head="filter(tmp1,tmp2)"):
+    body = macro(text, head)
     st = re.findall(r"(se|so)\s*=\s*mad\(\s*\*\s*(tmp1b|tmp2b)\s*(\+\+|--)?\s*,\s*" + NUM + r"\s*,\s*(se|so)\s*\)", body)
     init = dict(re.findall(r"(tmp[12]b)\s*=\s*tmp[12]\s*(?:\+\s*(\d+))?\s*;", body.replace("__local double *", "")))
     start = {"tmp1b": int(init.get("tmp1b") or 0), "tmp2b": int(init.get("tmp2b") or 0)}
@@ -115,6 +120,39 @@ def syn_line(prog, start, x):
     return out
 
 
+def syngrow_line(prog, start, x):
+    """syngrow1dKernel_d: coarse inputs s, w of Nc points each (zero outside),
+    n = Nc + 7 output pairs; tmp1 at s[i - 7], tmp2 at w[i - 7]."""
+    nc = len(x) // 2
+    s, w = x[:nc], x[nc:]
+    n = nc + 7
+    out = np.zeros(2 * n)
+    for i in range(n):
+        pos = {"tmp1b": start["tmp1b"], "tmp2b": start["tmp2b"]}
+        src = {"tmp1b": s, "tmp2b": w}
+        acc = {"se": 0.0, "so": 0.0}
+        for v, p, inc, c in prog:
+            k = i - 7 + pos[p]
+            val = src[p][k] if 0 <= k < nc else 0.0
+            acc[v] = val * c + acc[v]
+            pos[p] += 1 if inc == "++" else -1 if inc == "--" else 0
+        out[2 * i], out[2 * i + 1] = acc["so"], acc["se"]
+    return out
+
+
+def anashrink_line(prog, y):
+    """anashrink1dKernel_d: 2 Nc + 14 fine inputs, Nc coarse outputs;
+    tmp[m] = y[2 i + m]."""
+    nc = (len(y) - 14) // 2
+    out = np.zeros(2 * nc)
+    for i in range(nc):
+        acc = {"ci": 0.0, "di": 0.0}
+        for v, m, c in prog:
+            acc[v] = y[2 * i + m] * c + acc[v]
+        out[i], out[i + nc] = acc["ci"], acc["di"]
+    return out
+
+
 def main():
     root = os.environ.get("WVLH_REFERENCE_ROOT") or (sys.argv[1] if len(sys.argv) > 1 else None)
     if not root:
@@ -123,6 +161,7 @@ def main():
     ana = ana_program(text)
     syn, start = syn_program(text)
     kin = kin_program((Path(root) / "bigdft/src/OpenCL/Kinetic_Generator.cpp").read_text())
+    grow, gstart = syn_program(text, "filter_grow(tmp1,tmp2)")
     rng = np.random.default_rng(2024)
     out = {}
     for n in (8, 9, 13, 16, 24):
@@ -131,6 +170,10 @@ def main():
         out["ana_%d" % n] = ana_line(ana, x)
         out["syn_%d" % n] = syn_line(syn, start, x)
         out["kin_%d" % n] = kin_line(kin, x)   # on the 2n fine points of the same line
+        out["grow_%d" % n] = syngrow_line(grow, gstart, x)   # free BC: n coarse points grow to 2n + 14
+        yg = rng.uniform(-1, 1, 2 * n + 14)
+        out["yg_%d" % n] = yg
+        out["shrink_%d" % n] = anashrink_line(ana, yg)
     dst = Path(__file__).resolve().parent / "opencl_kernels.npz"
     np.savez(dst, **out)
     print("wrote", dst, "syn start", start)
