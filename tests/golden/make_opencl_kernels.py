@@ -1,7 +1,8 @@
 """Writes opencl_kernels.npz: outputs of the reference's OpenCL periodic
 wavelet synthesis and analysis kernels (bigdft/src/OpenCL/Wavelet_Generator.cpp:
 syn1dKernel_d, ana1dKernel_d) and fine-grid kinetic kernel
-(bigdft/src/OpenCL/Kinetic_Generator.cpp: kinetic1dKernel_d), evaluated on
+(bigdft/src/OpenCL/Kinetic_Generator.cpp: kinetic1dKernel_d) and free-BC
+magic filters (bigdft/src/OpenCL/MagicFilter_Generator.cpp), evaluated on
 seeded lines.
 
 The kernels exist only as source text that the generator pastes into an
@@ -22,6 +23,10 @@ their own order, with the indexing of the kernels that use them:
     tmp1 / tmp2 at s[i - 7] / w[i - 7] (zero outside), out[2 i] = so,
     out[2 i + 1] = se; free-BC analysis (the analysis macro in
     generate_anashrink1dKernel): tmp[m] = y[2 i + m] of 2 Nc + 14 points;
+  * free-BC magic filter (`filter(tmp)` / `filter_reverse(tmp)` of
+    MagicFilter_Generator.cpp with its FILT* values, used by
+    generate_magicfiltergrow1dKernel / generate_magicfiltershrink1dKernel):
+    growing, tmp[k] = x[i - 15 + k] (zero outside); shrinking, tmp[k] = y[i + k];
   * kinetic (`filter1(tt,tmp)` in generate_filters, with the FILT1_* values
     of generate_header, used by generate_kinetic1dKernel): for fine point i of
     a line of n points, tmp[m] = x[(i + m) mod n]; the kernel writes
@@ -68,6 +73,43 @@ def syn_program(text, head="filter(tmp1,tmp2)"):
     prog = [(v, p, inc, float(c)) for v, p, inc, c, v2 in st]
     assert len(prog) == 32 and set(init) == {"tmp1b", "tmp2b"}, (len(prog), init)
     return prog, start
+
+
+def mf_program(text, head):
+    """Tap values of a magic-filter macro (`filter(tmp)` or `filter_reverse(tmp)`
+    of MagicFilter_Generator.cpp) in the order its statements apply them to
+    tmp[0], tmp[1], ..."""
+    filt = {int(k): float(v) for k, v in re.findall(r"#define FILT(\d+)\s+" + NUM, text)}
+    body = macro(text, head)
+    order = [int(k) for k in re.findall(r"tt\s*=\s*mad\(\s*\*tmp\+\+\s*,\s*FILT(\d+)\s*,\s*tt\s*\)", body)]
+    assert len(order) == 16 and len(filt) == 16, (len(order), len(filt))
+    return [filt[k] for k in order]
+
+
+def mfgrow_line(taps, x):
+    """magicfiltergrow1dKernel_d: Lf inputs (zero outside), Lf + 15 outputs;
+    tmp[k] = x[i - 15 + k]."""
+    lf = len(x)
+    out = np.zeros(lf + 15)
+    for i in range(lf + 15):
+        tt = 0.0
+        for k, c in enumerate(taps):
+            j = i - 15 + k
+            tt = (x[j] if 0 <= j < lf else 0.0) * c + tt
+        out[i] = tt
+    return out
+
+
+def mfshrink_line(taps, y):
+    """magicfiltershrink1dKernel_d: Lf + 15 inputs, Lf outputs; tmp[k] = y[i + k]."""
+    lf = len(y) - 15
+    out = np.zeros(lf)
+    for i in range(lf):
+        tt = 0.0
+        for k, c in enumerate(taps):
+            tt = y[i + k] * c + tt
+        out[i] = tt
+    return out
 
 
 def kin_program(text):
@@ -162,6 +204,8 @@ def main():
     syn, start = syn_program(text)
     kin = kin_program((Path(root) / "bigdft/src/OpenCL/Kinetic_Generator.cpp").read_text())
     grow, gstart = syn_program(text, "filter_grow(tmp1,tmp2)")
+    mtext = (Path(root) / "bigdft/src/OpenCL/MagicFilter_Generator.cpp").read_text()
+    mf_fwd, mf_rev = mf_program(mtext, "filter(tmp)"), mf_program(mtext, "filter_reverse(tmp)")
     rng = np.random.default_rng(2024)
     out = {}
     for n in (8, 9, 13, 16, 24):
@@ -174,6 +218,10 @@ def main():
         yg = rng.uniform(-1, 1, 2 * n + 14)
         out["yg_%d" % n] = yg
         out["shrink_%d" % n] = anashrink_line(ana, yg)
+        out["mfgrow_%d" % n] = mfgrow_line(mf_fwd, x)        # 2n fine points grow by 15
+        ym = rng.uniform(-1, 1, 2 * n + 15)
+        out["ym_%d" % n] = ym
+        out["mfshrink_%d" % n] = mfshrink_line(mf_rev, ym)
     dst = Path(__file__).resolve().parent / "opencl_kernels.npz"
     np.savez(dst, **out)
     print("wrote", dst, "syn start", start)

@@ -273,10 +273,12 @@ def test_wavelet_kinetic_matches_reference_sse(oracle, N, fc, ff, cprecr):
 def test_syn_ana_kinetic_match_reference_opencl_kernels(oracle):
     """The oracle's synthesis and analysis, periodic (syn_rot_per /
     ana_rot_per, convolut_simple_per.f90) and free (syn_grow_rot /
-    ana_shrink_rot), and its fine-grid kinetic filter (the x part of
+    ana_shrink_rot), its free-BC magic filters (mf_grow_rot / mf_shrink_rot)
+    and its fine-grid kinetic filter (the x part of
     wo_kinetic_generic on a line) against the reference's OpenCL
     syn1dKernel_d / ana1dKernel_d / syngrow1dKernel_d / anashrink1dKernel_d /
-    kinetic1dKernel_d arithmetic on the same
+    magicfiltergrow1dKernel_d / magicfiltershrink1dKernel_d / kinetic1dKernel_d
+    arithmetic on the same
     lines (golden file), to FP64 rounding; with the reference tree present the
     golden file is re-derived first."""
     gold = np.load(GOLD / "opencl_kernels.npz")
@@ -290,6 +292,8 @@ def test_syn_ana_kinetic_match_reference_opencl_kernels(oracle):
         ana, (syn, start) = mk.ana_program(text), mk.syn_program(text)
         kin = mk.kin_program((REFERENCE / "bigdft/src/OpenCL/Kinetic_Generator.cpp").read_text())
         grow, gstart = mk.syn_program(text, "filter_grow(tmp1,tmp2)")
+        mtext = (REFERENCE / "bigdft/src/OpenCL/MagicFilter_Generator.cpp").read_text()
+        mf_fwd, mf_rev = mk.mf_program(mtext, "filter(tmp)"), mk.mf_program(mtext, "filter_reverse(tmp)")
     L = oracle.lib()
     for n in (8, 9, 13, 16, 24):
         x = gold["x_%d" % n]
@@ -299,11 +303,16 @@ def test_syn_ana_kinetic_match_reference_opencl_kernels(oracle):
             assert np.array_equal(mk.kin_line(kin, x), gold["kin_%d" % n])
             assert np.array_equal(mk.syngrow_line(grow, gstart, x), gold["grow_%d" % n])
             assert np.array_equal(mk.anashrink_line(ana, gold["yg_%d" % n]), gold["shrink_%d" % n])
+            assert np.array_equal(mk.mfgrow_line(mf_fwd, x), gold["mfgrow_%d" % n])
+            assert np.array_equal(mk.mfshrink_line(mf_rev, gold["ym_%d" % n]), gold["mfshrink_%d" % n])
         assert np.abs(oracle.ana_rot_per(n - 1, 1, x) - gold["ana_%d" % n]).max() < 1e-15
         assert np.abs(oracle.syn_rot_per(n - 1, 1, x) - gold["syn_%d" % n]).max() < 1e-15
         # free BC: n coarse points grow to 2n + 14 fine ones and shrink back
         assert np.abs(oracle.syn_grow_rot(n, 1, x) - gold["grow_%d" % n]).max() < 1e-15
         assert np.abs(oracle.ana_shrink_rot(n, 1, gold["yg_%d" % n]) - gold["shrink_%d" % n]).max() < 1e-15
+        # free-BC magic filter: 2n fine points grow by 15 and shrink back
+        assert np.abs(oracle.mf_grow_rot(2 * n, 1, x) - gold["mfgrow_%d" % n]).max() < 1e-15
+        assert np.abs(oracle.mf_shrink_rot(2 * n, 1, gold["ym_%d" % n]) - gold["mfshrink_%d" % n]).max() < 1e-15
         # kinetic of a line of 2n points: a (2n, 1, 1) periodic box with unit
         # spacing adds -1/2 conv along x (the one-point y and z lines add 0)
         y, e = np.zeros(2 * n), C.c_double()
