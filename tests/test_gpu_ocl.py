@@ -124,6 +124,39 @@ def test_1d_passes_match_oracle(oracle, q):
         assert rel(y.reshape(ndat, lout), yref) < 1e-14, name
 
 
+def test_1d_passes_match_reference_opencl_kernels(q):
+    """The drop-in 1D kernels on the lines of tests/golden/opencl_kernels.npz,
+    whose outputs replay the reference's own OpenCL kernels (syn1d, ana1d,
+    syngrow1d, anashrink1d, magicfiltergrow1d, magicfiltershrink1d, kinetic1d;
+    see tests/golden/make_opencl_kernels.py): FP64, to rounding."""
+    from pathlib import Path
+    gold = np.load(Path(__file__).resolve().parent / "golden" / "opencl_kernels.npz")
+    buf_in, buf_out = q.buffer(8 * 4096), q.buffer(8 * 4096)
+    wx, wy = q.buffer(8 * 4096), q.buffer(8 * 4096)
+    one = ocl._u(1)
+    for n in (8, 9, 13, 16, 24):
+        x, yg, ym = gold["x_%d" % n], gold["yg_%d" % n], gold["ym_%d" % n]
+        cases = [("syn1d_d_", n, x, "syn"), ("ana1d_d_", n, x, "ana"), ("syngrow1d_d_", n, x, "grow"),
+                 ("anashrink1d_d_", n, yg, "shrink"), ("magicfiltergrow1d_d_", 2 * n, x, "mfgrow"),
+                 ("magicfiltershrink1d_d_", 2 * n, ym, "mfshrink")]
+        for name, narg, xin, key in cases:
+            ref = gold["%s_%d" % (key, n)]
+            q.write(buf_in, np.ascontiguousarray(xin))
+            q.call(name, ocl._u(narg), one, buf_in.ref, buf_out.ref)
+            y = np.empty(len(ref))
+            q.read(buf_out, y)
+            assert np.abs(y - ref).max() <= 1e-14 * np.abs(ref).max(), (name, n)
+        # kinetic1d: y = c x - K x / (2 h^2); with c = 0 and h = 1 the filter is -2 y
+        ref = gold["kin_%d" % n]
+        q.write(buf_in, np.ascontiguousarray(x))
+        h, c0, e = C.c_double(1.0), C.c_double(0.0), C.c_double()
+        q.call("kinetic1d_d_", ocl._u(2 * n), one, C.byref(h), C.byref(c0), buf_in.ref, buf_out.ref, wx.ref,
+               wy.ref, C.byref(e))
+        y = np.empty(2 * n)
+        q.read(buf_out, y)
+        assert np.abs(-2.0 * y - ref).max() <= 1e-14 * np.abs(ref).max(), ("kinetic1d_d_", n)
+
+
 def test_dot_and_axpy(q):
     rng = np.random.default_rng(6)
     n = 100003
