@@ -154,14 +154,12 @@ __device__ void gather_plane(T *A, int pitch, const LrDev &L, int kz, const TI *
 }
 
 // Inverse of gather_plane: write (or add into) the compressed output.
-template <class T, class TO, int S3, bool DOT = false>
+template <class T, class TO, int S3>
 __device__ __forceinline__ void scatter_plane_s(const T *A, int pitch, const LrDev &L, int i3, TO *out, bool accumulate,
-                                                const T *sc, const T *D, int dpitch, double &dot)
+                                                const T *sc)
 {
     const int H1 = half_off(L.N[0]), H2 = half_off(L.N[1]);
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-    // D (DOT): a plane of the vector to dot with, gathered at row pitch
-    // dpitch; dot += <D | written values> over this plane's values
     if (!S3) {
         const T s0 = sc ? sc[0] : T(1);
         const int a = L.plane_c[i3], b = L.plane_c[i3 + 1];
@@ -170,7 +168,6 @@ __device__ __forceinline__ void scatter_plane_s(const T *A, int pitch, const LrD
             for (int t = lane; t < d.z; t += 32) {
                 const TO v = (TO)(A[d.y * pitch + d.x + t] * s0);
                 out[d.w + t] = accumulate ? out[d.w + t] + v : v;
-                if (DOT) dot += (double)v * (double)D[d.y * dpitch + d.x + t];
             }
         }
     }
@@ -186,18 +183,16 @@ __device__ __forceinline__ void scatter_plane_s(const T *A, int pitch, const LrD
                 if (fs3(c) != S3) continue;
                 const TO v = (TO)(A[(fs2(c) * H2 + d.y) * pitch + fs1(c) * H1 + d.x + t] * (sc ? sc[c] : T(1)));
                 dst[c - 1] = accumulate ? dst[c - 1] + v : v;
-                if (DOT) dot += (double)v * (double)D[(fs2(c) * H2 + d.y) * dpitch + fs1(c) * H1 + d.x + t];
             }
         }
     }
 }
 
-template <class T, class TO, bool DOT = false>
-__device__ void scatter_plane(const T *A, int pitch, const LrDev &L, int kz, TO *out, bool accumulate, const T *sc,
-                              const T *D, int dpitch, double &dot)
+template <class T, class TO>
+__device__ void scatter_plane(const T *A, int pitch, const LrDev &L, int kz, TO *out, bool accumulate, const T *sc)
 {
-    if (kz >= L.N[2]) scatter_plane_s<T, TO, 1, DOT>(A, pitch, L, kz - L.N[2], out, accumulate, sc, D, dpitch, dot);
-    else scatter_plane_s<T, TO, 0, DOT>(A, pitch, L, kz, out, accumulate, sc, D, dpitch, dot);
+    if (kz >= L.N[2]) scatter_plane_s<T, TO, 1>(A, pitch, L, kz - L.N[2], out, accumulate, sc);
+    else scatter_plane_s<T, TO, 0>(A, pitch, L, kz, out, accumulate, sc);
 }
 
 // Rows of `cols` points walked as point pairs: warp w takes rows w, w + nwarps,
@@ -387,8 +382,9 @@ __host__ __device__ constexpr int plane_min_blocks(bool fp32, bool persist, int 
 // CG vectors the preconditioner's plane kernels fold in (MODE_PRECOND): K1
 // forms the search direction while it gathers it (dir 1: d = r, the first
 // iteration; dir 2: d = beta d + r with beta = rrn / rr, in T), and
-// writes d back; K3 accumulates <d | A d> over the values it scatters, into
-// one partial per plane.  dir 0 / d null: plain gather / scatter.
+// writes d back; K3 accumulates <d | A d> of its plane, into one partial per
+// plane (as <P | W> of the fine planes it holds, since analysis is the
+// transpose of synthesis).  dir 0 / d null: plain gather / scatter.
 template <class T> struct CgIo {
     T *d;
     const T *r;
@@ -836,21 +832,22 @@ __device__ __forceinline__ void k3_item(const LrDev *__restrict__ lrs, const Orb
         if constexpr (sizeof(T) == 4) pass2_kin<kPairSeg, true, EN>(B, A, PairGeom{d.F1 / 2, pitch, pitch}, d.F2, d.p2, sy, 0.f, &e);
         else pass_kin<T, SEG, true, false, EN>(B, A, cols_geom(d.F1, pitch), d.F2, d.p2, sy, T(0), &e);
         __syncthreads();
+        if (MODE == MODE_PRECOND && dotv) {
+            // <d | A d> of this plane without reading d: analysis is the
+            // transpose of synthesis, so <d, D^-1/2 A_x A_y W> = <P, W> with
+            // P = S_x S_y D^-1/2 d (in B) and W the fine plane now in A
+            RowCol q(d.F1);
+            for (int i = threadIdx.x; i < d.F2 * d.F1; i += blockDim.x, q.next()) {
+                const int el = q.r * pitch + q.c;
+                e = fma((double)B[el], (double)A[el], e);
+            }
+            __syncthreads();   // A_x overwrites B
+        }
         pass_ana<T, SEG, true>(A, B, xpose_geom(d.F2, pitch, d.pitchT(d.F2)), d.N1, d.H1, d.p1);   // A_x: F1 -> G1, into B^T
         __syncthreads();
         pass_ana<T, SEG, true>(B, A, xpose_geom(d.G1, d.pitchT(d.F2), pitch), d.N2, d.H2, d.p2);   // A_y: F2 -> G2, into A
         __syncthreads();
-        if (MODE == MODE_PRECOND && dotv) {
-            // the plane of d for <d | A d>, into the free buffer B at pitch G1
-            if (bslice) gather_plane<T, TO>(B, d.G1, L, kz, dotv + o.psi, nullptr);
-            else gather_plane_async<T>(B, d.G1, L, kz, (const T *)(dotv + o.psi));
-            cp_async_wait_all();
-            __syncthreads();
-            scatter_plane<T, TO, true>(A, pitch, L, kz, out_ptr(o, hpsi), accumulate != 0, sc, B, d.G1, e);
-        } else {
-            scatter_plane<T, TO, false>(A, pitch, L, kz, out_ptr(o, hpsi), accumulate != 0,
-                                        MODE == MODE_PRECOND ? sc : nullptr, nullptr, 0, e);
-        }
+        scatter_plane<T, TO>(A, pitch, L, kz, out_ptr(o, hpsi), accumulate != 0, MODE == MODE_PRECOND ? sc : nullptr);
         const double s = block_sum(e, red);
         // slots 0 .. ntx1*nty1-1 belong to the z kernel's chain-1 tiles
         const int slot = ((d.F1 + TX - 1) / TX) * ((d.F2 + TY - 1) / TY) + kz;
