@@ -1413,14 +1413,17 @@ static cudaError_t launch_prec_apply_bc(const Plan &p, const T *x, T *y, const d
     return cudaGetLastError();
 }
 
-// out[o] = the sum of orbital o's stride partial slots, in slot order
+// out[o] = the sum of orbital o's stride partial slots: one warp per
+// orbital, lane l summing slots l, l + 32, ... then a fixed shuffle tree
+// (deterministic)
 static __global__ void k_cg_sum_slots(int norb, const double *__restrict__ part, int stride, double *__restrict__ out)
 {
-    const int o = blockIdx.x * blockDim.x + threadIdx.x;
+    const int o = blockIdx.x;
     if (o >= norb) return;
     double s = 0.0;
-    for (int k = 0; k < stride; ++k) s += part[(size_t)o * stride + k];
-    out[o] = s;
+    for (int k = threadIdx.x; k < stride; k += 32) s += part[(size_t)o * stride + k];
+    s = warp_sum(s);
+    if (threadIdx.x == 0) out[o] = s;
 }
 
 static bool aligned16(const void *p) { return !(reinterpret_cast<uintptr_t>(p) & 15); }
@@ -1445,7 +1448,7 @@ static cudaError_t cg_loop(const Plan &p, int ncong, const double *cprec, T *x, 
     for (int it = 0; it < ncong; ++it) {
         if ((err = apply(dvec, ad, CgIo<T>{dvec, r, rr, rrn, it == 0 ? 1 : 2}, dotpart))) return err;
         if (it > 0) k_copy_scalars<<<sg, 128, 0, st>>>(p.norb, rrn, rr);
-        k_cg_sum_slots<<<sg, 128, 0, st>>>(p.norb, dotpart, p.part_stride, dad);
+        k_cg_sum_slots<<<p.norb, 32, 0, st>>>(p.norb, dotpart, p.part_stride, dad);
         k_cg_step<T, VEC><<<vg, 256, 0, st>>>(p.d_orb_off, p.d_orb_len, rr, dad, x, dvec, r, ad, part);
         k_cg_sum<<<sg, 128, 0, st>>>(p.norb, part, rrn, hist ? hist + (size_t)(it + 1) * p.norb : nullptr);
     }
