@@ -1,7 +1,8 @@
 """GPU parity of the periodic Poisson solver (wvlh_psolver_periodic: cuFFT and
 the library's ISF kernel multiply) with the oracle's numpy restatement of the
 reference's periodic PSolver: potential within 1e-13 of its magnitude, the
-Hartree energy within 1e-12, on random and analytic densities."""
+Hartree energy within 1e-12, on random and analytic densities; grid lengths
+with prime factors 2, 3, 5, 7 and 11 and a long axis of 250 points."""
 import numpy as np
 import pytest
 
@@ -14,7 +15,10 @@ pytestmark = pytest.mark.gpu
 
 
 @pytest.mark.parametrize("n,h", [((32, 32, 32), (0.3, 0.3, 0.3)), ((48, 40, 36), (0.21, 0.25, 0.27)),
-                                 ((96, 96, 96), (0.225, 0.225, 0.225))])
+                                 ((96, 96, 96), (0.225, 0.225, 0.225)),
+                                 ((50, 30, 20), (0.3, 0.28, 0.26)),      # factors 5 and 3
+                                 ((250, 16, 18), (0.1, 0.3, 0.3)),       # a long axis
+                                 ((28, 42, 22), (0.3, 0.3, 0.3))])       # factors 7 and 11
 def test_matches_oracle_random_density(oracle, torch_cuda, wctx, n, h):
     torch = torch_cuda
     rng = np.random.default_rng(n[0])
