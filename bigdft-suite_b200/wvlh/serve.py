@@ -170,8 +170,9 @@ class Server:
         waits for admission.  psi: (norb, ncoeff) array (host or device) or
         None for seeded uniform(-1, 1) rows drawn on the device; pot: ISF
         potential or None for zero.  Raises AdmissionError if the client can
-        never fit (its resident bytes above the capacity, or one request's
-        scratch above a slot's share)."""
+        never fit (its resident bytes above the capacity, one request's
+        scratch above a slot's share, or more orbitals than a launch holds:
+        max_orbitals sizes each slot's energy and occupation buffers)."""
         c = Client(id=len(self.clients), locreg=locreg, norb=int(norb), occ=np.full(int(norb), float(occ)))
         c.coarse_cells = locreg.coarse_cells * c.norb
         c.resident_bytes = client_bytes(locreg, c.norb, self.elem)
@@ -179,6 +180,9 @@ class Server:
         if c.resident_bytes > self.capacity:
             raise AdmissionError("client %d needs %d resident bytes, capacity %d"
                                  % (c.id, c.resident_bytes, self.capacity))
+        if c.norb > self.max_orbitals:
+            raise AdmissionError("client %d has %d orbitals, a launch holds at most %d"
+                                 % (c.id, c.norb, self.max_orbitals))
         if c.scratch_bytes > self.scratch_per_slot:
             raise AdmissionError("client %d: one request needs %d scratch bytes, a slot has %d"
                                  % (c.id, c.scratch_bytes, self.scratch_per_slot))

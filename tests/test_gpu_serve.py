@@ -182,6 +182,26 @@ def test_admission_by_hbm_budget(torch_cuda):
     srv.close()
 
 
+def test_launch_orbital_cap(torch_cuda):
+    """A client with more orbitals than a launch holds is refused; with
+    max_orbitals at the largest client every launch stays within the slots'
+    buffers and the requests complete."""
+    from wvlh.serve import AdmissionError
+    specs = small_clients()
+    big = max(n for _, n in specs)
+    srv = Server(precision=32, hbm_budget=8e9, n_slots=2, scratch_per_slot=2e9, max_orbitals=big - 1)
+    lr, n = next((lr, n) for lr, n in specs if n == big)
+    with pytest.raises(AdmissionError, match="orbitals"):
+        srv.register(lr, n)
+    srv.close()
+    srv = Server(precision=32, hbm_budget=8e9, n_slots=2, scratch_per_slot=2e9, max_orbitals=big)
+    cl = [srv.register(lr, n, seed=i) for i, (lr, n) in enumerate(specs)]
+    reqs = srv.replay(poisson_arrivals(5e4, 40, len(cl), seed=5))
+    assert all(r.t_done is not None for r in reqs)
+    assert all(np.isfinite(r.ekin) for r in reqs if r.kind == "H")
+    srv.close()
+
+
 def test_poisson_replay_completes(torch_cuda):
     specs = small_clients()
     srv = Server(precision=32, hbm_budget=8e9, n_slots=2, scratch_per_slot=2e9)
