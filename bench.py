@@ -680,7 +680,11 @@ def leg_serve(torch, dev, precision, nreq=300, loads=(0.3, 0.5, 0.7)):
     orbitals), requests 50/50 Hpsi and density; capacity from a burst of one
     request of each kind per client, then Poisson arrivals swept over loads x
     capacity.  The headline p50/p99 are those of the highest load whose
-    served rate kept up with the offered rate (within 5 %)."""
+    served rate kept up with the rate the sample's arrivals actually came at
+    (requests over the last arrival time; within 5 %: the span of a few
+    hundred Poisson arrivals varies by several per cent around the nominal
+    rate, which a comparison with the nominal rate would read as falling
+    behind)."""
     from wvlh import workloads as W
     from wvlh.serve import Server, latency_stats
     specs = W.serving_clients()
@@ -697,20 +701,23 @@ def leg_serve(torch, dev, precision, nreq=300, loads=(0.3, 0.5, 0.7)):
     sweep = []
     n0, k0 = srv.launches, srv.kernel_launches
     for i, load in enumerate(loads):
+        arrivals = W.poisson_arrivals(load * cap, nreq, len(cl), seed=11 + i)
         t = time.perf_counter()
-        reqs = srv.replay(W.poisson_arrivals(load * cap, nreq, len(cl), seed=11 + i))
+        reqs = srv.replay(arrivals)
         dt = time.perf_counter() - t
         st = latency_stats(reqs)
-        sweep.append({"load": load, "offered_req_s": load * cap, "served_req_s": len(reqs) / dt,
+        sweep.append({"load": load, "offered_req_s": load * cap, "arrival_req_s": len(arrivals) / arrivals[-1][0],
+                      "served_req_s": len(reqs) / dt,
                       "served_cells_s": sum(cells[r.client.id] for r in reqs) / dt,
                       "p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"], "mean_ms": st["mean_ms"],
                       "queued_p50_ms": st["queued_p50_ms"], "queued_p99_ms": st["queued_p99_ms"],
                       "launched_p50_ms": st["launched_p50_ms"], "launched_p99_ms": st["launched_p99_ms"],
                       "tail": st["tail"]})
-    kept = [w for w in sweep if w["served_req_s"] >= 0.95 * w["offered_req_s"]]
+    kept = [w for w in sweep if w["served_req_s"] >= 0.95 * w["arrival_req_s"]]
     head = kept[-1] if kept else sweep[0]
     out = {"clients": len(cl), "resident_gb": srv.resident / 1e9, "capacity_req_s": cap,
            "capacity_cells_s": cap_cells, "sustained_load": head["load"], "offered_req_s": head["offered_req_s"],
+           "arrival_req_s": head["arrival_req_s"],
            "served_req_s": head["served_req_s"], "served_cells_s": head["served_cells_s"],
            "p50_ms": head["p50_ms"], "p99_ms": head["p99_ms"], "mean_ms": head["mean_ms"],
            "queued_p99_ms": head["queued_p99_ms"], "launched_p99_ms": head["launched_p99_ms"], "tail": head["tail"],
