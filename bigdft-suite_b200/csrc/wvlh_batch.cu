@@ -597,12 +597,16 @@ static int batch_usable(const wvlh_batch *b)
     return WVLH_OK;
 }
 
+// dynamic shared memory a block of the current device may ask for (its
+// opt-in limit less 1 KB for the kernels' static arrays), 0 when the limit
+// cannot be read
 static size_t sm_limit()
 {
     int dev = 0, v = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
-    return (size_t)v;
+    if (cudaGetDevice(&dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess || v <= 1024)
+        return 0;
+    return (size_t)v - 1024;
 }
 
 extern "C" int wvlh_locham_batched(wvlh_batch *b, int precision, const void *psi, const void *pot, void *hpsi,
@@ -617,7 +621,8 @@ extern "C" int wvlh_locham_batched(wvlh_batch *b, int precision, const void *psi
     CK(cudaSetDevice(c->device));
     const Plan &p = b->plan;
     const int fp = precision == 64;
-    const size_t lim = sm_limit() - 1024;
+    const size_t lim = sm_limit();
+    if (!lim) return fail(WVLH_ERR_CUDA);
     if ((size_t)p.plane_elems * (fp ? 8 : 4) > lim || p.smem2[fp] > lim) return fail(WVLH_ERR_TOO_LARGE);
     if ((rc = c->scratch.ensure((p.scratch_elems + plane_tmp_elems(p, fp)) * (fp ? 8 : 4))) ||
         (rc = c->part_pot.ensure(sizeof(double) * (size_t)p.norb * p.part_stride)) ||
@@ -698,7 +703,8 @@ extern "C" int wvlh_locden_batched(wvlh_batch *b, int precision, const void *psi
     CK(cudaSetDevice(c->device));
     const Plan &p = b->plan;
     const int fp = precision == 64;
-    const size_t lim = sm_limit() - 1024;
+    const size_t lim = sm_limit();
+    if (!lim) return fail(WVLH_ERR_CUDA);
     if ((size_t)p.plane_elems * (fp ? 8 : 4) > lim || p.smem2[fp] > lim) return fail(WVLH_ERR_TOO_LARGE);
     if ((rc = c->scratch.ensure((p.scratch_elems + plane_tmp_elems(p, fp)) * (fp ? 8 : 4))) ||
         (rc = c->den_part.ensure(sizeof(double) * (size_t)p.part_den_elems)))
@@ -720,7 +726,8 @@ extern "C" int wvlh_precond_batched(wvlh_batch *b, int precision, int ncong, con
     CK(cudaSetDevice(c->device));
     const Plan &p = b->plan;
     const int fp = precision == 64;
-    const size_t lim = sm_limit() - 1024;
+    const size_t lim = sm_limit();
+    if (!lim) return fail(WVLH_ERR_CUDA);
     if ((size_t)p.plane_elems * (fp ? 8 : 4) > lim || p.smem2[fp] > lim) return fail(WVLH_ERR_TOO_LARGE);
     const size_t es = fp ? 8 : 4;
     const size_t nv = (size_t)p.psi_total * es;
@@ -980,7 +987,8 @@ extern "C" int wvlh_locham_batched_host(wvlh_batch *b, int precision, const void
     const Plan &p = b->plan;
     const size_t npsi = (size_t)p.psi_total * es, npot = (size_t)pot_extent(b) * es;
     const size_t ne = sizeof(double) * p.norb;
-    const size_t lim = sm_limit() - 1024;
+    const size_t lim = sm_limit();
+    if (!lim) return fail(WVLH_ERR_CUDA);
     if ((size_t)p.plane_elems * es > lim || p.smem2[fp] > lim) return fail(WVLH_ERR_TOO_LARGE);
     int rc;
     if ((rc = c->io_psi.ensure(npsi)) || (rc = c->io_hpsi.ensure(npsi)) || (rc = c->io_pot.ensure(npot)) ||
@@ -1284,7 +1292,8 @@ extern "C" int wvlh_locham_graph_create(wvlh_batch *b, int precision, const void
     CK(cudaSetDevice(c->device));
     const Plan &p = b->plan;
     const int fp = precision == 64;
-    const size_t lim = sm_limit() - 1024;
+    const size_t lim = sm_limit();
+    if (!lim) return fail(WVLH_ERR_CUDA);
     if ((size_t)p.plane_elems * (fp ? 8 : 4) > lim || p.smem2[fp] > lim) return fail(WVLH_ERR_TOO_LARGE);
     wvlh_graph *g = new wvlh_graph();
     g->ctx = c;
